@@ -1,0 +1,380 @@
+/*
+ * ref_harness.cpp -- TEST INFRASTRUCTURE (the oracle), never part of the product.
+ *
+ * Drives the reference LS-STAG-3D CPU/OpenMP code (compiled from its own
+ * headers by oracle/build_ref.sh) on the synthetic cases the product is
+ * measured on, and dumps everything the parity tests compare against:
+ *   geometry (cell types, theta, delta, VOF, 1/M_x,y,z), the Laplace CSR
+ *   (laplace_discrete_operator.h:107-686, fixPoint :809-821), the right-hand
+ *   side, the multigrid hierarchy (coarse_grid.h:93-106: P, R, A_H, ADLJ
+ *   factors, coarse LU), one V-cycle (multigrid_solver.h:48-75), one
+ *   MG-FGMRES solve (fgmres_interface.h:78-142) and one ILU(0)-BiCGStab
+ *   solve (bicgstab_interface.h:76-111).
+ *
+ * Geometry: a uniform staggered grid built through the reference's own zoned
+ * mesh (ls_stag_mesh.h) with a single zone, and the reference's level-set
+ * machinery (FlowTaskDescription::buildBaseMesh, flow_task_description.h).
+ * The level set is evaluated exactly like calcLevelSetSphere
+ * (flow_sphere_task_description.h:57-74): at the upper cell corner, phi > 0
+ * inside a body; several bodies are merged by max (i.e. min of |x-c|-r).
+ *
+ * Usage: ref_harness <config.txt> <outdir>
+ * The config is a whitespace separated key/value list written by
+ * oracle/ref_runner.py.  Every dumped array is raw little-endian binary with
+ * a line in <outdir>/manifest.txt: "<name> <dtype> <count>".
+ */
+#include "stdafx.h"
+#include "TimeSteppingMethod/time_stepping_method_interface.h"
+#include "Base/Solvers/BiCGStab/ilu_bicgstab.h"
+#include <chrono>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <vector>
+
+using namespace LS_STAG;
+
+namespace {
+
+struct Body {
+    int kind = 0;          // 0 sphere, 1 ellipsoid
+    double c[3] = {0, 0, 0};
+    double r = 0.0;        // sphere radius
+    double ax[3] = {1, 1, 1};   // ellipsoid semi-axes
+    double rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};  // body frame = rot * (x - c)
+    double phi(double x, double y, double z) const
+    {
+        const double qx = x - c[0], qy = y - c[1], qz = z - c[2];
+        if (kind == 0) return r - sqrt(qx * qx + qy * qy + qz * qz);
+        const double bx = rot[0] * qx + rot[1] * qy + rot[2] * qz;
+        const double by = rot[3] * qx + rot[4] * qy + rot[5] * qz;
+        const double bz = rot[6] * qx + rot[7] * qy + rot[8] * qz;
+        const double s = sqrt((bx / ax[0]) * (bx / ax[0]) + (by / ax[1]) * (by / ax[1]) +
+                              (bz / ax[2]) * (bz / ax[2]));
+        // scaled distance-like function, zero on the surface, > 0 inside
+        const double amin = std::min(ax[0], std::min(ax[1], ax[2]));
+        return (1.0 - s) * amin;
+    }
+    void bbox(double lo[3], double hi[3]) const
+    {
+        const double e = (kind == 0) ? r : std::max(ax[0], std::max(ax[1], ax[2]));
+        for (int d = 0; d < 3; d++) { lo[d] = c[d] - e; hi[d] = c[d] + e; }
+    }
+};
+
+struct Config {
+    std::map<std::string, std::string> kv;
+    std::vector<Body> bodies;
+    double get(const std::string& k, double d) const
+    {
+        auto it = kv.find(k);
+        return it == kv.end() ? d : atof(it->second.c_str());
+    }
+    std::string gets(const std::string& k, const std::string& d) const
+    {
+        auto it = kv.find(k);
+        return it == kv.end() ? d : it->second;
+    }
+};
+
+Config readConfig(const char* path)
+{
+    Config c;
+    std::ifstream in(path);
+    std::string key;
+    while (in >> key) {
+        if (key == "body") {
+            Body b;
+            in >> b.kind >> b.c[0] >> b.c[1] >> b.c[2];
+            if (b.kind == 0) in >> b.r;
+            else {
+                in >> b.ax[0] >> b.ax[1] >> b.ax[2];
+                for (int i = 0; i < 9; i++) in >> b.rot[i];
+            }
+            c.bodies.push_back(b);
+        } else {
+            std::string v;
+            in >> v;
+            c.kv[key] = v;
+        }
+    }
+    return c;
+}
+
+/* Uniform-grid flow task over bodies given by level sets.  Subclasses the
+   reference FlowTaskDescription exactly like FlowSphereTaskDescription does
+   (flow_sphere_task_description.h:41-153), replacing the zoned step table
+   with one zone of step h in every direction. */
+struct HarnessTask : FlowTaskDescription {
+    LSSTAGMesh mesh;
+    int gN, gM, gK;
+    double hx, hy, hz;
+    std::vector<Body> bodies;
+    HarnessTask()
+        : FlowTaskDescription(AIRFOIL_SPHERE, MOTION_NO, (LSSTAGUniformMesh*)&mesh, sizeof(HarnessTask)),
+          gN(8), gM(8), gK(8), hx(1), hy(1), hz(1)
+    {
+        discontin = 0;
+        ibCount = 1;
+        useNNM = 0;
+        needXYMesh = 0;
+        useTM = 0;
+        continueSolveTask = 0;
+        PeriodPrintSol = 1e30;
+        PeriodPrintRotor = 0.0;
+        PeriodSaveState = 1e30;
+    }
+    void calcNodesCount() override
+    {
+        mesh.baseMesh.N = gN;
+        mesh.baseMesh.M = gM;
+        mesh.baseMesh.K = gK;
+    }
+    void initMeshParams() override
+    {
+        FlowTaskDescription::initMeshParams();
+        for (int k = 0; k < LSSTAGMesh::ZONES_COUNT; k++) mesh.zone[k].set(0, 0, 0);
+        mesh.zone[3].x = gN;  // ZONE_ORDER_X[3] = 0 -> deltaCurZone[0].x
+        mesh.zone[2].y = gM;  // deltaOrder[0][2] = 0 -> deltaCurZone[0].y
+        mesh.zone[2].z = gK;
+        for (int d = 0; d < LSSTAGMesh::DELTA_COUNT; d++) mesh.deltaCurZone[d].set(hx, hy, hz);
+        mesh.maxCountCutCells = gN * gM * gK;
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (const Body& b : bodies) {
+            double l[3], h[3];
+            b.bbox(l, h);
+            for (int d = 0; d < 3; d++) { lo[d] = std::min(lo[d], l[d]); hi[d] = std::max(hi[d], h[d]); }
+        }
+        // LS block as in FlowSphereTaskDescription::initMeshParams, kept >= 5
+        // cells from the walls: buildBaseMesh widens it by 3 and the row walks
+        // of calcTypeOfCells (flow_task_description.h) need >= 2 plain cells
+        // on each side of the widened block.  Bodies must lie inside it.
+        mesh.hs = std::max(5, (int)floor(lo[0] / hx));
+        mesh.hf = std::min(gN - 5, (int)floor(hi[0] / hx) + 1);
+        mesh.vs = std::max(5, (int)floor(lo[1] / hy));
+        mesh.vf = std::min(gM - 5, (int)floor(hi[1] / hy) + 1);
+        H_BASE = 1.0;
+    }
+    void buildLS(const int zs, const int zf, const int vs, const int vf, const int hs, const int hf) override
+    {
+        const int N = mesh.baseMesh.N, NM = N * mesh.baseMesh.M;
+        for (int k = zs; k < zf; k++)
+            for (int j = vs; j < vf; j++) {
+                // same point walk as calcLevelSetSphere: corner = node + delta/2, then += delta.x
+                int num = NM * k + N * j + hs;
+                coordinate p = mesh.nodes[num];
+                coordinate* d = mesh.delta + num;
+                p.add(0.5 * d->x, 0.5 * d->y, 0.5 * d->z);
+                for (int end = NM * k + N * j + hf; num < end; num++) {
+                    double f = -1e300;
+                    for (const Body& b : bodies) f = std::max(f, b.phi(p.x, p.y, p.z));
+                    mesh.phi[num] = f;
+                    d++;
+                    p.x += d->x;
+                }
+            }
+    }
+};
+
+struct Dumper {
+    std::string dir;
+    std::ofstream man;
+    explicit Dumper(const std::string& d) : dir(d), man(d + "/manifest.txt") {}
+    template <typename T>
+    void put(const std::string& name, const T* p, long n, const char* dt)
+    {
+        std::ofstream f(dir + "/" + name + ".bin", std::ios::binary);
+        f.write((const char*)p, sizeof(T) * n);
+        man << name << " " << dt << " " << n << "\n";
+        man.flush();
+    }
+    void d(const std::string& name, const double* p, long n) { put(name, p, n, "f8"); }
+    void i(const std::string& name, const int* p, long n) { put(name, p, n, "i4"); }
+    void csr(const std::string& name, SparseMatrix* A)
+    {
+        const int n = A->NMK;
+        const int nnz = A->Number[n];
+        i(name + "_rowptr", A->Number, n + 1);
+        i(name + "_col", A->Portrait, nnz);
+        d(name + "_val", A->Cell, nnz);
+        int dims[4] = {A->m_N, A->m_M, A->m_K, A->NMK};
+        i(name + "_dims", dims, 4);
+    }
+    void scalar(const std::string& name, double v) { d(name, &v, 1); }
+};
+
+double now_s()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+/* Same accessors as the reference's private members need: MultiGridSolver
+   exposes grids/LU publicly through CoarseGridsHierarchy. */
+void dumpHierarchy(Dumper& out, MultiGridSolver& mg)
+{
+    int nl = mg.numMG;
+    out.i("mg_nlev", &nl, 1);
+    for (int l = 0; l < nl; l++) {
+        CoarseGrid& g = mg.grids[l];
+        std::string p = "mg" + std::to_string(l) + "_";
+        out.csr(p + "P", &g.P);
+        out.csr(p + "R", (SparseMatrix*)&g.R);
+        out.csr(p + "AH", (SparseMatrix*)&g.AH);
+        int par[3] = {g.oddN, g.oddM, g.oddK};
+        out.i(p + "odd", par, 3);
+        const int n = g.m_A->NMK;
+        SmootherADLJ& s = g.ADLJ;
+        out.d(p + "xc", s.ADLJ_x.c, n - 1);
+        out.d(p + "xd", s.ADLJ_x.d, n);
+        out.d(p + "xe", s.ADLJ_x.e, n - 1);
+        out.d(p + "yc", s.ADLJ_y.c, n - 1);
+        out.d(p + "yd", s.ADLJ_y.d, n);
+        out.d(p + "ye", s.ADLJ_y.e, n - 1);
+        out.d(p + "zc", s.ADLJ_z.c, n - 1);
+        out.d(p + "zd", s.ADLJ_z.d, n);
+        out.d(p + "ze", s.ADLJ_z.e, n - 1);
+    }
+}
+
+}  // namespace
+
+int main(int argc, char** argv)
+{
+    if (argc < 3) {
+        fprintf(stderr, "usage: %s config outdir\n", argv[0]);
+        return 2;
+    }
+    Config cfg = readConfig(argv[1]);
+    const std::string outdir = argv[2];
+    const int threads = (int)cfg.get("threads", 0);
+    if (threads > 0) omp_set_num_threads(threads);
+
+    HarnessTask* task = new HarnessTask;
+    task->gN = (int)cfg.get("N", 16);
+    task->gM = (int)cfg.get("M", 16);
+    task->gK = (int)cfg.get("K", 16);
+    task->hx = cfg.get("hx", 1.0 / task->gN);
+    task->hy = cfg.get("hy", 1.0 / task->gM);
+    task->hz = cfg.get("hz", 1.0 / task->gK);
+    task->bodies = cfg.bodies;
+    task->Re = cfg.get("Re", 100.0);
+    task->t = cfg.get("dt", 0.01);
+    task->T_end = cfg.get("T_end", 1.0);
+    task->nu = task->V_BASE * task->L_BASE / task->Re;
+    task->FGMRES_RESTART_NUM_P = (int)cfg.get("restart", 30);
+    task->MAX_ITER = (int)cfg.get("max_it", 200);
+    task->n_post = (int)cfg.get("n_post", BaseTaskDescription::DEFAULT_N_POST);
+    task->outputDirectoryFull = outdir + "/";
+
+    Dumper out(outdir);
+    double curTime = 0.0;
+    int it = 1;
+    double t0 = now_s();
+    task->init(&curTime);
+    SetSolutions* sol = new SetSolutions;
+    sol->init(task, &it);
+    task->initSol(&(sol->current), &(sol->prediction), &(sol->previous));
+    PoissonDiscreteEquation* pEq = new PoissonDiscreteEquation;
+    pEq->set(task, &(sol->prediction.p));
+    double t_setup = now_s() - t0;
+
+    LSSTAGUniformMesh* m = task->m_mesh;
+    const int N = m->baseMesh.N, M = m->baseMesh.M, K = m->baseMesh.K;
+    const long n = (long)N * M * K;
+    int dims[3] = {N, M, K};
+    out.i("dims", dims, 3);
+    out.scalar("t_setup_s", t_setup);
+
+    const int dumpGeom = (int)cfg.get("dump_geometry", 1);
+    if (dumpGeom) {
+        out.i("celltype", (const int*)m->baseMesh.typeOfCell, n);
+        out.d("theta", (const double*)m->theta, 3 * n);
+        out.d("alpha", (const double*)m->alpha, 3 * n);
+        out.d("delta", (const double*)m->delta, 3 * n);
+        out.d("phi", m->phi, n);
+        out.d("vof", m->baseMesh.VOF, n);
+        out.d("inv_mx", m->xMesh.inv_VOF, (long)m->xMesh.NMK);
+        out.d("inv_my", m->yMesh.inv_VOF, (long)m->yMesh.NMK);
+        out.d("inv_mz", m->zMesh.inv_VOF, (long)m->zMesh.NMK);
+        out.d("flux", pEq->A.flux, n);
+    }
+    SparseMatrix* A = (SparseMatrix*)&pEq->A;
+    if ((int)cfg.get("dump_matrix", 1)) out.csr("A", A);
+    int pins[2] = {pEq->A.fixPointNum, pEq->A.fixPointFlowNum};
+    out.i("pins", pins, 2);
+
+    // Right-hand side: read from file when given (written by the runner).
+    std::vector<double> b(n, 0.0);
+    const std::string rhsPath = cfg.gets("rhs", "");
+    if (rhsPath.empty()) return 0;
+    {
+        std::ifstream f(rhsPath, std::ios::binary);
+        f.read((char*)b.data(), sizeof(double) * n);
+        if (!f) { fprintf(stderr, "cannot read rhs %s\n", rhsPath.c_str()); return 3; }
+    }
+    double bnorm = 0.0;
+    for (long i = 0; i < n; i++) bnorm += b[i] * b[i];
+    bnorm = sqrt(bnorm);
+    const double rel = cfg.get("rel_tol", 1e-10);
+    const double eps = cfg.get("abs_tol", rel * bnorm);
+    out.scalar("eps", eps);
+
+    const int reps = (int)cfg.get("repeats", 1);
+    // --- one V-cycle of the reference multigrid (a standalone instance with
+    //     the same task parameters as the MGFGMRES preconditioner) ---
+    if ((int)cfg.get("dump_mg", 0)) {
+        // heap-allocated and intentionally not destroyed: the reference's
+        // hierarchy destructors are not safe for a second instance.
+        MultiGridSolver* mg = new MultiGridSolver;
+        mg->set(A, task);
+        dumpHierarchy(out, *mg);
+        std::vector<double> x(n, 0.0);
+        mg->solve(b.data(), x.data());
+        out.d("vcycle_x", x.data(), n);
+    }
+    // --- MG-FGMRES ---
+    if ((int)cfg.get("fgmres", 1)) {
+        MGFGMRES& s = pEq->solver;
+        s.eps = eps;
+        std::vector<double> ts;
+        for (int r = 0; r < reps; r++) {
+            std::copy(b.begin(), b.end(), pEq->m_right);
+            std::fill(pEq->m_sol, pEq->m_sol + n, 0.0);
+            double t1 = now_s();
+            int iters = s.solve();
+            ts.push_back(now_s() - t1);
+            if (r == reps - 1) {
+                out.d("fgmres_x", pEq->m_sol, n);
+                out.i("fgmres_it", &iters, 1);
+                out.scalar("fgmres_norm_r", s.norm_r);
+            }
+        }
+        out.d("fgmres_time_s", ts.data(), (long)ts.size());
+    }
+    // --- ILU(0)-BiCGStab (bicgstab_interface.h / ilu_bicgstab.h) ---
+    if ((int)cfg.get("bicgstab", 0)) {
+        ILUBiCGStab& s = *new ILUBiCGStab;  // not destroyed (see above)
+        std::vector<double> x(n, 0.0), bb(b);
+        double tset = now_s();
+        s.set(A, bb.data(), x.data(), task);
+        tset = now_s() - tset;
+        s.eps = eps;
+        std::vector<double> ts;
+        for (int r = 0; r < reps; r++) {
+            std::fill(x.begin(), x.end(), 0.0);
+            double t1 = now_s();
+            int iters = s.solve();
+            ts.push_back(now_s() - t1);
+            if (r == reps - 1) {
+                out.d("bicgstab_x", x.data(), n);
+                out.i("bicgstab_it", &iters, 1);
+                out.scalar("bicgstab_norm_r", s.norm_r);
+            }
+        }
+        out.d("bicgstab_time_s", ts.data(), (long)ts.size());
+        out.scalar("bicgstab_setup_s", tset);
+    }
+    int nthreads = omp_get_max_threads();
+    out.i("omp_threads", &nthreads, 1);
+    return 0;
+}

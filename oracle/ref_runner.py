@@ -1,0 +1,93 @@
+"""TEST INFRASTRUCTURE: run the reference-backed harness binary
+(``oracle/_ref/ref_harness``, built by ``oracle/build_ref.sh`` from the
+reference's own sources) and load what it dumps.
+
+Only tests, the fixture generator and bench.py's CPU-baseline leg use this
+module; the product never does.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_BIN = os.path.join(HERE, "_ref", "ref_harness")
+
+
+def available() -> bool:
+    return os.path.isfile(REF_BIN) and os.access(REF_BIN, os.X_OK)
+
+
+@dataclass
+class Case:
+    """Uniform box [0, N*hx] x [0, M*hy] x [0, K*hz] with level-set bodies."""
+    N: int
+    M: int
+    K: int
+    hx: float
+    hy: float
+    hz: float
+    spheres: list = field(default_factory=list)      # (cx, cy, cz, r)
+    ellipsoids: list = field(default_factory=list)   # (c[3], axes[3], rot[3x3])
+
+    def config_lines(self):
+        lines = [f"N {self.N}", f"M {self.M}", f"K {self.K}",
+                 f"hx {self.hx!r}", f"hy {self.hy!r}", f"hz {self.hz!r}"]
+        for (cx, cy, cz, r) in self.spheres:
+            lines.append(f"body 0 {cx!r} {cy!r} {cz!r} {r!r}")
+        for (c, ax, rot) in self.ellipsoids:
+            rr = " ".join(repr(float(v)) for v in np.asarray(rot).reshape(-1))
+            lines.append(f"body 1 {float(c[0])!r} {float(c[1])!r} {float(c[2])!r} "
+                         f"{float(ax[0])!r} {float(ax[1])!r} {float(ax[2])!r} {rr}")
+        return lines
+
+
+def load_dir(d: str) -> dict:
+    out = {}
+    with open(os.path.join(d, "manifest.txt")) as f:
+        for line in f:
+            name, dt, n = line.split()
+            out[name] = np.fromfile(os.path.join(d, name + ".bin"), dtype=np.dtype(dt), count=int(n))
+    return out
+
+
+def run(case: Case, rhs: np.ndarray | None = None, *, threads: int = 0, workdir: str | None = None,
+        timeout: float = 3600, **opts) -> dict:
+    """Run the harness once.  ``opts`` become config keys (restart, max_it,
+    rel_tol, abs_tol, fgmres, bicgstab, dump_mg, dump_geometry, dump_matrix,
+    repeats, n_post)."""
+    if not available():
+        raise FileNotFoundError(REF_BIN)
+    own = workdir is None
+    d = tempfile.mkdtemp(prefix="lsg_ref_") if own else workdir
+    os.makedirs(d, exist_ok=True)
+    lines = case.config_lines()
+    if threads:
+        lines.append(f"threads {threads}")
+    for k, v in opts.items():
+        lines.append(f"{k} {v!r}" if isinstance(v, float) else f"{k} {v}")
+    if rhs is not None:
+        p = os.path.join(d, "rhs.in")
+        np.ascontiguousarray(rhs, dtype=np.float64).tofile(p)
+        lines.append(f"rhs {p}")
+    cfg = os.path.join(d, "case.cfg")
+    with open(cfg, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    subprocess.run([REF_BIN, cfg, d], check=True, timeout=timeout,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
+    res = load_dir(d)
+    if own:
+        import shutil
+        shutil.rmtree(d, ignore_errors=True)
+    return res
+
+
+def csr(res: dict, name: str):
+    """(rowptr, col, val, (N, M, K)) of a dumped CSR matrix."""
+    dims = res[name + "_dims"]
+    return (res[name + "_rowptr"], res[name + "_col"], res[name + "_val"],
+            (int(dims[0]), int(dims[1]), int(dims[2])))
