@@ -1,0 +1,77 @@
+"""Generate the golden fixtures in this directory from the reference's own
+solver (oracle/_ref/ref_harness, built by oracle/build_ref.sh from the
+reference sources).  Run from the repository root:
+
+    python tests/golden/make_golden.py
+
+Each fixture is a compressed .npz holding the case's Laplace CSR exactly as
+the reference assembles it (laplace_discrete_operator.h), the seeded
+right-hand side, and the reference's outputs: its multigrid hierarchy
+(P, R, A_H, factored ADLJ tridiagonals), one V-cycle, one MG-FGMRES(30) solve
+and one ILU(0)-BiCGStab solve to a 1e-10 relative residual.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "ls-stag-3d_parallel_b200"))
+
+import ref_runner as rr  # noqa: E402
+from lsstag_b200 import synth  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def cases():
+    """(name, Case, rhs seed).  Small grids whose coarsening visits the
+    even-even-even, even-even-odd and odd-odd-odd transfer classes."""
+    out = []
+    h = 1.0 / 16
+    out.append(("sphere16", rr.Case(16, 16, 16, h, h, h,
+                                    spheres=[(0.5 + 0.3 * h, 0.5 + 0.2 * h, 0.5 + 0.1 * h, 0.18)]), 5))
+    h = 1.0 / 20
+    out.append(("sphere20x12x10", rr.Case(20, 12, 10, h, h, h,
+                                          spheres=[(0.5 + 0.3 * h, 0.3 + 0.2 * h, 0.25 + 0.1 * h, 0.09)]), 6))
+    h = 1.0 / 24
+    sph = synth.four_spheres(3, rmin=0.05, rmax=0.1, cmin=0.4, cmax=0.6)
+    out.append(("spheres4_24", rr.Case(24, 24, 24, h, h, h, spheres=sph), 7))
+    return out
+
+
+def main():
+    if not rr.available():
+        sys.exit("oracle/_ref/ref_harness missing: run oracle/build_ref.sh first")
+    for name, case, seed in cases():
+        g = rr.run(case, threads=1)
+        rp, col, val, dims = rr.csr(g, "A")
+        mask = synth.connected_fluid(rp, col, val, g["pins"])
+        b = synth.poisson_rhs(seed, g["celltype"], g["pins"], mask)
+        r = rr.run(case, b, threads=1, fgmres=1, bicgstab=1, dump_mg=1, dump_geometry=0,
+                   restart=30, rel_tol=1e-10, max_it=200)
+        keep = {"dims": np.array(dims), "A_rowptr": rp, "A_col": col, "A_val": val,
+                "pins": g["pins"], "celltype": g["celltype"], "b": b, "eps": r["eps"],
+                "vcycle_x": r["vcycle_x"], "fgmres_x": r["fgmres_x"], "fgmres_it": r["fgmres_it"],
+                "fgmres_norm_r": r["fgmres_norm_r"], "bicgstab_x": r["bicgstab_x"],
+                "bicgstab_it": r["bicgstab_it"], "bicgstab_norm_r": r["bicgstab_norm_r"],
+                "mg_nlev": r["mg_nlev"]}
+        for l in range(int(r["mg_nlev"][0])):
+            for m in ("P", "R", "AH"):
+                for part in ("rowptr", "col", "val", "dims"):
+                    keep[f"mg{l}_{m}_{part}"] = r[f"mg{l}_{m}_{part}"]
+            keep[f"mg{l}_odd"] = r[f"mg{l}_odd"]
+            for d in "xyz":
+                for part in "cde":
+                    keep[f"mg{l}_{d}{part}"] = r[f"mg{l}_{d}{part}"]
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **keep)
+        print(f"{path}: n={len(b)} fgmres_it={int(r['fgmres_it'][0])} "
+              f"bicgstab_it={int(r['bicgstab_it'][0])} size={os.path.getsize(path)} B")
+
+
+if __name__ == "__main__":
+    main()
