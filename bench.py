@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 pressure-Poisson projection solver.
+
+Workload (one "step" = one complete solve from x = 0):
+  standalone cut-cell pressure-Poisson system on the unit cube at 256^3 with
+  four seeded immersed spheres, Neumann walls and the reference's two pinned
+  rows; FGMRES(30) right-preconditioned with the reference-shaped multigrid
+  (Galerkin coarse operators, ADLJ z/y/x line smoother, V(0,3)), solved to a
+  relative residual of 1e-10 (absolute eps = 1e-10 * ||b||, the reference's
+  stopping rule on the implicit residual).
+  value     = ms per solve with the FP32 multigrid preconditioner inside FP64
+              FGMRES with iterative refinement (device time, CUDA events on
+              the solver's stream), inputs resident in HBM;
+  fp64_ms   = the same solve with the FP64 multigrid (the plain FP64 GPU solve);
+  e2e       = the FP32-preconditioned solve through the C ABI with host
+              buffers (b, x in, x out, pinned host memory), copies timed;
+  roofline  = the dominant kernel's algorithmic bytes / its event-timed
+              duration against the measured HBM copy bandwidth;
+  cpu_baseline = the reference's own MG-FGMRES (oracle/_ref, OpenMP on all
+              host cores) on the same operator and right-hand side.
+Multi-GPU: replicas only (each rank solves its own copy; no collectives on the
+data path); the timed region is bracketed by a barrier and the max over ranks
+is reported.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size 256]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ls-stag-3d_parallel_b200"))
+
+METRIC = "Poisson ms/solve at 256³ to 1e-10: FP32-MG vs FP64 on 1 B200; HBM % peak"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_hbm_gbs():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [v.strip() for v in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(k)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier_max(pg, value: float, local: int) -> float:
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def reference_solve_ms(P, dims, b, threads, repeats):
+    """Reference MG-FGMRES(30) on the host cores: per-solve seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner as rr
+    r = rr.run_planes(P, dims, b, threads=threads, fgmres=1, bicgstab=0, restart=30, rel_tol=1e-10,
+                      max_it=200, repeats=repeats, timeout=3600)
+    return [1e3 * t for t in r["fgmres_time_s"]], int(r["fgmres_it"][0]), int(r["omp_threads"][0])
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    from lsstag_b200 import cases
+    P, dims, pins, b = cases.load(args.size)
+    threads = os.cpu_count() or 1
+    cfg = config_dict(args, world)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner as rr
+    if not rr.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built (needs the "
+                          "reference sources at build time)"}))
+        return 0
+    warm = min(args.warmup, 1)
+    times, it, th = reference_solve_ms(P, dims, b, threads, warm + args.steps)
+    timed = times[warm:]
+    ms = sum(timed) / len(timed)
+    out = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms/solve", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+           "iterations": it,
+           "cpu_baseline": {"value": ms, "unit": "ms/solve", "cores": th, "kind": "reference",
+                            "sample": f"{len(timed)} full {args.size}^3 MG-FGMRES(30) solves to 1e-10 "
+                                      f"(reference LS-STAG-3D OpenMP build, {th} threads)"},
+           "e2e": {"value": ms, "unit": "ms/solve", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def config_dict(args, world):
+    return {"workload": f"poisson_spheres4_{args.size}^3_mgfgmres30_rel1e-10",
+            "grid": [args.size] * 3, "bodies": "4 seeded spheres (seed 3), Neumann walls, 2 pinned rows",
+            "krylov": "FGMRES(30) FP64, modified Gram-Schmidt",
+            "precond": "Galerkin MG, ADLJ z/y/x line smoother V(0,3), omega 0.805",
+            "l2": "inputs larger than L2 (operator 0.94 GB FP64 + Krylov basis)",
+            "parallelism": "replicas" if world > 1 else "single GPU"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
+    world, rank, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        rc = run_reference_arm(args, world, rank)
+        if pg is not None:
+            pg.destroy_process_group()
+        return rc
+
+    import numpy as np
+    import torch
+
+    from lsstag_b200 import _lib as L
+    from lsstag_b200 import cases
+    from lsstag_b200 import solver as S
+
+    torch.cuda.set_device(local)
+    P, dims, pins, b = cases.load(args.size)
+    n = b.size
+    bnorm = float(np.linalg.norm(b))
+    task = S.Task(eps=1e-10 * bnorm, MAX_ITER=200, FGMRES_RESTART_NUM=30)
+    dev = f"cuda:{local}"
+    b_dev = torch.from_numpy(b).to(dev)
+    results = {}
+    for name, prec in (("fp32", L.FP32), ("fp64", L.FP64)):
+        s = S.MGFGMRES(device=local, mg_precision=prec)
+        s.set_planes(P, dims, task)
+        x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+        st = L.Stats()
+        def one():
+            x_dev.zero_()
+            torch.cuda.synchronize()
+            s.ctx.check(s.ctx.lib.lsg_solve_device(s.ctx.h, L.C.c_void_p(b_dev.data_ptr()),
+                                                   L.C.c_void_p(x_dev.data_ptr()), L.C.byref(st)))
+            return st.ms, st.iterations, st.kernel_launches, st.bytes, st.true_residual, st.norm_r
+        for _ in range(args.warmup):
+            one()
+        barrier(pg)
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local) if name == "fp32" else None
+        if sampler:
+            sampler.__enter__()
+        recs = [one() for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.__exit__()
+        barrier(pg)
+        ms = sum(r[0] for r in recs)
+        ms_max = barrier_max(pg, ms, local)
+        results[name] = {"ms_total": ms_max, "ms_per_solve": ms_max / args.steps, "it": recs[-1][1],
+                         "launches": sum(r[2] for r in recs), "bytes": recs[-1][3], "true_res": recs[-1][4],
+                         "norm_r": recs[-1][5], "x": x_dev.cpu().numpy(), "clocks": sampler.summary() if sampler else None}
+        if name == "fp32":
+            # dominant-kernel roofline (finest-level smoother/residual kernels)
+            prof = {}
+            nv = recs[-1][1]
+            per_solve = {0: 3 * nv, 1: 3 * nv, 2: 3 * nv, 3: 9 * nv}
+            names = {0: "adlj_xline_fp32", 1: "adlj_yline_fp32", 2: "adlj_zline_fp32", 3: "residual7_fp32"}
+            for k in (0, 1, 2, 3):
+                msk = L.C.c_double(0)
+                byk = L.C.c_double(0)
+                s.ctx.check(s.ctx.lib.lsg_profile_kernel(s.ctx.h, k, 20, L.C.byref(msk), L.C.byref(byk)))
+                prof[k] = (msk.value, byk.value, per_solve[k] * msk.value)
+            results["prof"] = {names[k]: {"ms": v[0], "bytes": v[1], "gbs": v[1] / v[0] / 1e6, "ms_per_solve": v[2]}
+                               for k, v in prof.items()}
+            kdom = max(prof, key=lambda k: prof[k][2])
+            results["dominant"] = (names[kdom], prof[kdom])
+            # e2e through the C ABI with pinned host buffers
+            bh = torch.from_numpy(b).pin_memory()
+            xh = torch.zeros(n, dtype=torch.float64).pin_memory()
+            e2e = []
+            for rep in range(args.warmup + args.steps):
+                xh.zero_()
+                t0 = time.perf_counter()
+                s.ctx.check(s.ctx.lib.lsg_solve(s.ctx.h, L.C.cast(bh.data_ptr(), L.C.POINTER(L.C.c_double)),
+                                                L.C.cast(xh.data_ptr(), L.C.POINTER(L.C.c_double)), L.C.byref(st)))
+                if rep >= args.warmup:
+                    e2e.append(1e3 * (time.perf_counter() - t0))
+            results["e2e_ms"] = barrier_max(pg, sum(e2e), local) / args.steps
+        s.close()
+        del x_dev
+    x32, x64 = results["fp32"]["x"], results["fp64"]["x"]
+    err = float(np.linalg.norm(x32 - x64) / np.linalg.norm(x64))
+    peak, peak_kind = measured_hbm_gbs()
+    dname, (dms, dbytes, _) = results["dominant"]
+    achieved = dbytes / dms / 1e6
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.isfile(tp):
+        try:
+            with open(tp) as f:
+                tj = json.load(f)
+            traffic = tj.get(dname, {}).get(f"traffic_bytes_per_launch_{args.size}")
+        except Exception:
+            traffic = None
+    value = results["fp32"]["ms_total"] / (args.steps * world)
+    out = {
+        "metric": METRIC, "value": value, "unit": "ms/solve", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": results["fp32"]["ms_per_solve"], "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (multigrid) / f64 (Krylov)", "data": "synthetic",
+        "config": config_dict(args, world),
+        "fp64_ms_per_solve": results["fp64"]["ms_per_solve"],
+        "speedup_fp32mg_vs_fp64": results["fp64"]["ms_per_solve"] / results["fp32"]["ms_per_solve"],
+        "iterations": {"fp32": results["fp32"]["it"], "fp64": results["fp64"]["it"]},
+        "true_rel_residual": {"fp32": results["fp32"]["true_res"] / bnorm, "fp64": results["fp64"]["true_res"] / bnorm},
+        "rel_l2_fp32_vs_fp64": err,
+        "solve_algorithmic_gbs": results["fp32"]["bytes"] / results["fp32"]["ms_per_solve"] / 1e6,
+        "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": dbytes, "ms_per_launch": dms},
+        "kernels": results["prof"],
+        "e2e": {"value": results["e2e_ms"] / world, "unit": "ms/solve", "h2d_bytes_per_step": 2 * 8 * n,
+                "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": results["fp32"]["launches"],
+        "clocks": results["fp32"]["clocks"],
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import ref_runner as rr
+            if rr.available():
+                threads = os.cpu_count() or 1
+                times, it, th = reference_solve_ms(P, dims, b, threads, 1)
+                out["cpu_baseline"] = {"value": times[0], "unit": "ms/solve", "cores": th, "kind": "reference",
+                                       "iterations": it,
+                                       "sample": f"one full {args.size}^3 MG-FGMRES(30) solve to 1e-10 on the same "
+                                                 f"operator and right-hand side (reference OpenMP build, {th} threads)"}
+            else:
+                out["cpu_baseline"] = None
+        except Exception as e:  # report, do not hide
+            out["cpu_baseline"] = {"error": str(e)}
+    if rank == 0:
+        print(json.dumps(out))
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,173 @@
+/*
+ * lsstag_b200.h -- C ABI of the B200 (sm_100a) pressure-Poisson projection
+ * solver for LS-STAG-3D.
+ *
+ * The library replaces the reference's iterative solvers for the pressure
+ * correction system: the drop-in point is the reference's
+ *     IterativeSolverInterface::set(SparseMatrix* A, double* b, double* x,
+ *                                   BaseTaskDescription* task)   (Base/Solvers/iterative_solver_interface.h:46-55)
+ *     IterativeSolverInterface::solve()                          (:45, FGMRES fgmres_interface.h:78-142,
+ *                                                                  BiCGStab bicgstab_interface.h:76-111)
+ *     IterativeSolverInterface::rebuildPreconditioner()          (:38, mg_fgmres.h:40-44, ilu_bicgstab.h:50-54)
+ * An adapter class implementing that interface calls, in order,
+ *     lsg_set_matrix_csr (set: the operator the equation assembled),
+ *     lsg_setup          (set / rebuildPreconditioner: MG hierarchy or ILU(0)),
+ *     lsg_solve          (solve: x updated in place, returns iterations).
+ *
+ * Conventions
+ *   - cells are numbered  i + N*(j + M*k)  (x fastest), as in the reference;
+ *   - the operator is given as the reference's CSR (Number/Portrait/Cell,
+ *     Base/SparseMatrix/sparse_matrix.h:220-228), 32-bit indices, FP64 values;
+ *     every row may hold only the cell itself and its six face neighbours;
+ *   - host pointers unless the function name ends in _device;
+ *   - every call returns an lsg status; 0 is success, > 0 a solver outcome,
+ *     < 0 an error (lsg_last_error gives the text);
+ *   - one context per device and per operator; a context is not thread safe;
+ *     all work of a context runs on its own CUDA stream.
+ */
+#ifndef LSSTAG_B200_H
+#define LSSTAG_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define LSG_OK 0
+#define LSG_NOT_CONVERGED 1   /* iteration cap reached (reference: silent MAX_ITER) */
+#define LSG_BREAKDOWN 2       /* zero/NaN norm met by a reduction */
+#define LSG_ERR_ARG (-1)
+#define LSG_ERR_CUDA (-2)
+#define LSG_ERR_NOMEM (-3)
+#define LSG_ERR_STATE (-4)    /* call order violated (e.g. solve before setup) */
+#define LSG_ERR_PATTERN (-5)  /* operator entry outside the 7-point stencil */
+#define LSG_ERR_SINGULAR (-6)
+
+/* lsg_options.method */
+#define LSG_METHOD_FGMRES 0
+#define LSG_METHOD_BICGSTAB 1
+/* lsg_options.precond */
+#define LSG_PC_MG 0
+#define LSG_PC_ILU0 1
+#define LSG_PC_NONE 2
+/* lsg_options.mg_precision */
+#define LSG_FP64 0
+#define LSG_FP32 1
+/* lsg_options.smoother */
+#define LSG_SMOOTHER_ADLJ 0   /* reference: damped z,y,x line Jacobi */
+#define LSG_SMOOTHER_RBGS 1   /* red-black point Gauss-Seidel (new variant) */
+
+typedef struct lsg_options {
+    int method;          /* LSG_METHOD_*; reference default FGMRES */
+    int precond;         /* LSG_PC_*; reference default MG */
+    int mg_precision;    /* LSG_FP64 (reference) or LSG_FP32 (mixed precision) */
+    int smoother;        /* LSG_SMOOTHER_* */
+    int n_pre;           /* pre-smoothing sweeps (reference 0) */
+    int n_post;          /* post-smoothing sweeps (reference 3) */
+    int max_levels;      /* coarse levels; <= 0: the reference's GridLevels rule */
+    int restart;         /* FGMRES restart length (reference FGMRES_RESTART_NUM_P) */
+    int max_it;          /* iteration cap (reference MAX_ITER = 200) */
+    int zline_reference; /* 1: z-line smoother reads its first right-hand side
+                            where the reference does (smoother_adlj_z.h:54-58) */
+    double eps;          /* absolute stopping tolerance (reference semantics) */
+    double omega;        /* ADLJ damping (reference 0.805) */
+    int reserved[8];
+} lsg_options;
+
+typedef struct lsg_stats {
+    int iterations;       /* reference IterativeSolverInterface::it */
+    int status;           /* LSG_OK / LSG_NOT_CONVERGED / LSG_BREAKDOWN */
+    double norm_r;        /* reference norm_r: implicit residual at exit */
+    double true_residual; /* ||b - A x||_2 recomputed in FP64 at exit */
+    double ms;            /* device time of the solve (CUDA events) */
+    double bytes;         /* algorithmic HBM bytes the solve moved */
+    int vcycles;          /* preconditioner applications */
+    int pad;
+    long long kernel_launches; /* CUDA kernels this library launched in the solve */
+    int reserved[4];
+} lsg_stats;
+
+typedef struct lsg_ctx lsg_ctx;
+
+/* Fill *o with the reference defaults (MG-FGMRES, FP64, ADLJ V(0,3),
+   omega 0.805, restart 30, max_it 200, eps 1e-5). */
+void lsg_default_options(lsg_options* o);
+
+/* Create a context on CUDA device `device`.  Replaces the construction of
+   MGFGMRES / ILUBiCGStab (mg_fgmres.h:33-52, ilu_bicgstab.h:33-64). */
+int lsg_create(int device, lsg_ctx** out);
+int lsg_destroy(lsg_ctx* ctx);
+/* Text of the last error of this context (static storage of the context). */
+const char* lsg_last_error(const lsg_ctx* ctx);
+
+/* Set the operator: the reference's CSR of the N x M x K cell-centred
+   Laplace operator (LaplaceDiscreteOperator, laplace_discrete_operator.h:107-686
+   with the pinned rows of fixPoint :809-821).  Replaces the matrix half of
+   IterativeSolverInterface::set (iterative_solver_interface.h:46-55). */
+int lsg_set_matrix_csr(lsg_ctx* ctx, int N, int M, int K, const int* rowptr, const int* col,
+                       const double* val);
+/* Same with device pointers (the reference's CUDA build keeps its CSR in
+   device memory, Base/MeshFunctions/array.h). */
+int lsg_set_matrix_csr_device(lsg_ctx* ctx, int N, int M, int K, const int* rowptr, const int* col,
+                              const double* val, long long nnz);
+
+/* Set the operator from its seven coefficient planes, the structured form of
+   the same CSR: planes[s*n + i] is row i's coefficient toward the cell at
+   offset s = 0..6 = (0,0,-1), (0,-1,0), (-1,0,0), (0,0,0), (1,0,0), (0,1,0),
+   (0,0,1)  (the column order b, s, w, p, e, n, t of the reference's CSR,
+   laplace_discrete_operator.h:130-136).  Coefficients toward cells outside
+   the grid must be 0.  Host pointer, 7*N*M*K doubles. */
+int lsg_set_matrix_stencil7(lsg_ctx* ctx, int N, int M, int K, const double* planes);
+
+/* Build the preconditioner for the current operator (multigrid hierarchy:
+   MultiGridSolver::set multigrid_solver.h:76-101 / CoarseGrid::set
+   coarse_grid.h:93-106; or ILU(0): ILUDecompositionSparseMatrix::decompose
+   ilu_decomposition_sparse_matrix.h:138-148).  Call again after
+   lsg_set_matrix_csr to rebuild (rebuildPreconditioner). */
+int lsg_setup(lsg_ctx* ctx, const lsg_options* opts);
+
+/* Solve A x = b; x holds the initial guess on entry and the solution on exit
+   (IterativeSolverInterface::solve).  Host buffers of N*M*K doubles. */
+int lsg_solve(lsg_ctx* ctx, const double* b, double* x, lsg_stats* stats);
+/* Same with device buffers (no host copies). */
+int lsg_solve_device(lsg_ctx* ctx, const double* b, double* x, lsg_stats* stats);
+
+/* y = A x with the stored operator (RealValuedMeshFunction::mvProd,
+   real_valued_mesh_function.h:81-88).  Host buffers. */
+int lsg_apply(lsg_ctx* ctx, const double* x, double* y);
+/* x = M^{-1} b: one application of the configured preconditioner
+   (MultiGridSolver::solve multigrid_solver.h:48-75 or the ILU(0) solves).
+   Host buffers; for the FP32 multigrid the result is the FP32 cycle rounded
+   to FP64. */
+int lsg_precond_apply(lsg_ctx* ctx, const double* b, double* x);
+
+/* Multigrid introspection for parity checks.  Level 0 is the fine grid. */
+int lsg_mg_num_levels(const lsg_ctx* ctx);  /* coarse levels (GridLevels), or < 0 */
+int lsg_mg_level_dims(const lsg_ctx* ctx, int level, int dims[3]);
+/* Level operator as CSR with columns sorted (rowptr n+1, col/val nnz).
+   Call with col == NULL to get *nnz only. */
+int lsg_mg_level_csr(lsg_ctx* ctx, int level, int* rowptr, int* col, double* val, long long* nnz);
+/* Factored line tridiagonal of `dir` ('x', 'y', 'z') on `level` in the
+   reference's storage order (TriDiagonalMatrix c, d, e after triLU,
+   tridiagonal_matrix.h:45-67): c and e hold n-1 values, d holds n. */
+int lsg_mg_level_tridiag(lsg_ctx* ctx, int level, char dir, double* c, double* d, double* e);
+
+/* Time one kernel of the solve path on the context's stream with CUDA
+   events (after a warm-up launch): `which` = 0/1/2 the finest-level x/y/z
+   line solve of the multigrid smoother, 3 the finest-level residual update
+   r -= A c, 4 the FP64 operator apply fused with a dot product (Krylov).
+   Returns the mean duration of one launch and the algorithmic HBM bytes one
+   launch moves (compulsory traffic of its inputs and outputs).  Needs
+   lsg_setup with the multigrid preconditioner. */
+int lsg_profile_kernel(lsg_ctx* ctx, int which, int reps, double* ms_per_launch, double* bytes_per_launch);
+
+/* Library build string (version, arch). */
+const char* lsg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LSSTAG_B200_H */

@@ -1,0 +1,667 @@
+// Device kernels of the B200 pressure-Poisson solver.
+//
+// Every kernel is bandwidth bound (<= 0.25 flop/B); they are written for
+// coalesced, vectorisable streaming of the SoA coefficient planes with the
+// stencil neighbours served from L1/L2, and for deterministic reductions
+// (block partials summed by the last block in a fixed order).
+#pragma once
+
+#include "lsg_internal.cuh"
+
+namespace lsg {
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+struct OffList {
+    int n;
+    int center;
+    signed char o[125][3];
+};
+
+__device__ __forceinline__ void cell_xyz(long long i, int N, int NM, int& x, int& y, int& z)
+{
+    z = (int)(i / NM);
+    int r = (int)(i - (long long)z * NM);
+    y = r / N;
+    x = r - y * N;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic block + grid reduction of NS values.  Every block writes its
+// partial sums; the last block to finish adds them in block order and writes
+// out[s].  blockDim.x must be a multiple of 32 and <= 1024.
+template <int NS>
+__device__ void grid_reduce(double (&v)[NS], double* partial, unsigned int* counter, double* out)
+{
+    __shared__ double sh[32][NS];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        double t = warp_sum(v[s]);
+        if (lane == 0) sh[wid][s] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            double t = 0.0;
+            for (int w = 0; w < nw; w++) t += sh[w][s];
+            partial[(size_t)blockIdx.x * NS + s] = t;
+        }
+        __threadfence();
+        unsigned int prev = atomicAdd(counter, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double acc[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) acc[s] = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) acc[s] += ((volatile double*)partial)[(size_t)b * NS + s];
+    }
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        double t = warp_sum(acc[s]);
+        if (lane == 0) sh[wid][s] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            double t = 0.0;
+            for (int w = 0; w < nw; w++) t += sh[w][s];
+            out[s] = t;
+        }
+        *counter = 0u;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// operator assembly
+// ---------------------------------------------------------------------------
+
+// Scatter the reference's CSR rows into the 7 coefficient planes (b, s, w, p,
+// e, n, t).  Entries of one row with the same column add up, like the CSR
+// product does.  err[0] = 1 + first bad row when an entry is not one of the
+// six face neighbours or the cell itself.
+__global__ void k_csr_to_stencil7(int N, int M, int K, const int* __restrict__ rowptr,
+                                  const int* __restrict__ col, const double* __restrict__ val,
+                                  double* __restrict__ coef, int* err)
+{
+    const long long n = (long long)N * M * K;
+    const int NM = N * M;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        cell_xyz(i, N, NM, x, y, z);
+        for (int e = rowptr[i]; e < rowptr[i + 1]; e++) {
+            const long long j = col[e];
+            int slot = -1;
+            if (j >= 0 && j < n) {
+                int jx, jy, jz;
+                cell_xyz(j, N, NM, jx, jy, jz);
+                const int dx = jx - x, dy = jy - y, dz = jz - z;
+                if (dx == 0 && dy == 0 && dz == -1) slot = 0;
+                else if (dx == 0 && dy == -1 && dz == 0) slot = 1;
+                else if (dx == -1 && dy == 0 && dz == 0) slot = 2;
+                else if (dx == 0 && dy == 0 && dz == 0) slot = 3;
+                else if (dx == 1 && dy == 0 && dz == 0) slot = 4;
+                else if (dx == 0 && dy == 1 && dz == 0) slot = 5;
+                else if (dx == 0 && dy == 0 && dz == 1) slot = 6;
+            }
+            if (slot < 0) {
+                atomicCAS(err, 0, (int)(i + 1));
+                continue;
+            }
+            coef[(size_t)slot * n + i] += val[e];
+        }
+    }
+}
+
+template <typename Tout, typename Tin>
+__global__ void k_convert(long long n, const Tin* __restrict__ a, Tout* __restrict__ b)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        b[i] = (Tout)a[i];
+}
+
+// ---------------------------------------------------------------------------
+// stencil applies
+// ---------------------------------------------------------------------------
+
+// Fine 7-point residual update  r -= A x  (mode 0),  y = A x  (mode 1).
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_apply7(int N, int M, int K, const T* __restrict__ coef,
+                                                 const T* __restrict__ x, T* __restrict__ r)
+{
+    const long long n = (long long)N * M * K;
+    const int NM = N * M;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int ix, iy, iz;
+        cell_xyz(i, N, NM, ix, iy, iz);
+        T acc = coef[3 * n + i] * x[i];
+        if (iz > 0) acc += coef[i] * x[i - NM];
+        if (iy > 0) acc += coef[n + i] * x[i - N];
+        if (ix > 0) acc += coef[2 * n + i] * x[i - 1];
+        if (ix < N - 1) acc += coef[4 * n + i] * x[i + 1];
+        if (iy < M - 1) acc += coef[5 * n + i] * x[i + N];
+        if (iz < K - 1) acc += coef[6 * n + i] * x[i + NM];
+        if (MODE == 0) r[i] -= acc;
+        else r[i] = acc;
+    }
+}
+
+// Box-stencil (coarse Galerkin operator) residual update r -= A x (mode 0)
+// or y = A x (mode 1).
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_applybox(int N, int M, int K, OffList ol, const T* __restrict__ coef,
+                                                   const T* __restrict__ x, T* __restrict__ r)
+{
+    const long long n = (long long)N * M * K;
+    const int NM = N * M;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int ix, iy, iz;
+        cell_xyz(i, N, NM, ix, iy, iz);
+        T acc = 0;
+        for (int o = 0; o < ol.n; o++) {
+            const int jx = ix + ol.o[o][0], jy = iy + ol.o[o][1], jz = iz + ol.o[o][2];
+            if (jx < 0 || jx >= N || jy < 0 || jy >= M || jz < 0 || jz >= K) continue;
+            acc += coef[(size_t)o * n + i] * x[i + ol.o[o][0] + (long long)ol.o[o][1] * N + (long long)ol.o[o][2] * NM];
+        }
+        if (MODE == 0) r[i] -= acc;
+        else r[i] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// transfers (structured tensor-product operators, one 1-D table per axis)
+// ---------------------------------------------------------------------------
+// Prolongation table per fine index f: two (coarse index, weight) pairs.
+struct PTab {
+    const int* c;      // 2 per fine index
+    const float* w;    // 2 per fine index (exact binary fractions)
+};
+// Restriction table per coarse index: up to 4 (fine index, weight) pairs.
+struct RTab {
+    const int* f;      // 4 per coarse index, -1 = unused
+    const float* w;
+};
+
+// ch = P cHH and c = ch  (the prolongation plus the copy c.copy(m_ch) of
+// MultiGridSolver::solve, multigrid_solver.h:65-66)
+template <typename T>
+__global__ void k_prolong(int N, int M, int K, int Nc, int Mc, PTab px, PTab py, PTab pz,
+                          const T* __restrict__ coarse, T* __restrict__ ch, T* __restrict__ c)
+{
+    const long long n = (long long)N * M * K;
+    const int NM = N * M, NMc = Nc * Mc;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        cell_xyz(i, N, NM, x, y, z);
+        T acc = 0;
+#pragma unroll
+        for (int a = 0; a < 2; a++) {
+            const float wz = pz.w[2 * z + a];
+            if (wz == 0.f) continue;
+            const int cz = pz.c[2 * z + a];
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                const float wy = py.w[2 * y + b];
+                if (wy == 0.f) continue;
+                const int cy = py.c[2 * y + b];
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const float wx = px.w[2 * x + q];
+                    if (wx == 0.f) continue;
+                    const int cx = px.c[2 * x + q];
+                    acc += (T)(wz * wy * wx) * coarse[(long long)cz * NMc + cy * Nc + cx];
+                }
+            }
+        }
+        ch[i] = acc;
+        c[i] = acc;
+    }
+}
+
+// coarse = R fine.  agglomerate: 1/8 of the 2x2x2 block (even-even-even
+// class, summed in the reference's CSR order); otherwise R = P^T via tables.
+template <typename T>
+__global__ void k_restrict(int Nc, int Mc, int Kc, int N, int M, bool agglomerate, RTab rx, RTab ry, RTab rz,
+                           const T* __restrict__ fine, T* __restrict__ coarse)
+{
+    const long long nc = (long long)Nc * Mc * Kc;
+    const int NMc = Nc * Mc, NM = N * M;
+    for (long long I = blockIdx.x * (long long)blockDim.x + threadIdx.x; I < nc;
+         I += (long long)gridDim.x * blockDim.x) {
+        int X, Y, Z;
+        cell_xyz(I, Nc, NMc, X, Y, Z);
+        T acc = 0;
+        if (agglomerate) {
+            const long long f0 = (long long)(2 * Z) * NM + (2 * Y) * N + 2 * X;
+            const T w = (T)0.125;
+            acc += w * fine[f0];
+            acc += w * fine[f0 + 1];
+            acc += w * fine[f0 + N];
+            acc += w * fine[f0 + N + 1];
+            acc += w * fine[f0 + NM];
+            acc += w * fine[f0 + NM + 1];
+            acc += w * fine[f0 + NM + N];
+            acc += w * fine[f0 + NM + N + 1];
+        } else {
+            for (int a = 0; a < 4; a++) {
+                const int fz = rz.f[4 * Z + a];
+                if (fz < 0) continue;
+                const float wz = rz.w[4 * Z + a];
+                for (int b = 0; b < 4; b++) {
+                    const int fy = ry.f[4 * Y + b];
+                    if (fy < 0) continue;
+                    const float wy = ry.w[4 * Y + b];
+                    for (int q = 0; q < 4; q++) {
+                        const int fx = rx.f[4 * X + q];
+                        if (fx < 0) continue;
+                        acc += (T)(wz * wy * rx.w[4 * X + q]) * fine[(long long)fz * NM + fy * N + fx];
+                    }
+                }
+            }
+        }
+        coarse[I] = acc;
+    }
+}
+
+// Galerkin coarse operator A_H = R A P for one coarse cell per thread.  The
+// box of the coarse stencil is (2rx+1)(2ry+1)(2rz+1), offsets ordered
+// z-major, then y, then x (all in [-r, r]).  A is a box/offset-list stencil
+// on the fine level.  Accumulation is in FP64.
+__global__ void k_galerkin(int N, int M, int K, OffList fol, const double* __restrict__ Af, int Nc, int Mc,
+                           int Kc, int crx, int cry, int crz, bool agglomerate, PTab px, PTab py, PTab pz,
+                           RTab rx, RTab ry, RTab rz, double* __restrict__ Ac)
+{
+    const long long n = (long long)N * M * K;
+    const long long nc = (long long)Nc * Mc * Kc;
+    const int NMc = Nc * Mc;
+    const int bx = 2 * crx + 1, by = 2 * cry + 1;
+    const int nbox = bx * by * (2 * crz + 1);
+    for (long long I = blockIdx.x * (long long)blockDim.x + threadIdx.x; I < nc;
+         I += (long long)gridDim.x * blockDim.x) {
+        int X, Y, Z;
+        cell_xyz(I, Nc, NMc, X, Y, Z);
+        double box[125];
+        for (int q = 0; q < nbox; q++) box[q] = 0.0;
+        // support of row I of R: 1-D lists
+        int fxl[4], fyl[4], fzl[4];
+        double wxl[4], wyl[4], wzl[4];
+        int nx = 0, ny = 0, nz = 0;
+        if (agglomerate) {
+            fxl[0] = 2 * X; fxl[1] = 2 * X + 1; wxl[0] = wxl[1] = 0.5; nx = 2;
+            fyl[0] = 2 * Y; fyl[1] = 2 * Y + 1; wyl[0] = wyl[1] = 0.5; ny = 2;
+            fzl[0] = 2 * Z; fzl[1] = 2 * Z + 1; wzl[0] = wzl[1] = 0.5; nz = 2;
+        } else {
+            for (int a = 0; a < 4; a++) {
+                if (rx.f[4 * X + a] >= 0) { fxl[nx] = rx.f[4 * X + a]; wxl[nx++] = rx.w[4 * X + a]; }
+                if (ry.f[4 * Y + a] >= 0) { fyl[ny] = ry.f[4 * Y + a]; wyl[ny++] = ry.w[4 * Y + a]; }
+                if (rz.f[4 * Z + a] >= 0) { fzl[nz] = rz.f[4 * Z + a]; wzl[nz++] = rz.w[4 * Z + a]; }
+            }
+        }
+        for (int a = 0; a < nz; a++)
+            for (int b = 0; b < ny; b++)
+                for (int q = 0; q < nx; q++) {
+                    const int fx = fxl[q], fy = fyl[b], fz = fzl[a];
+                    const double rw = wzl[a] * wyl[b] * wxl[q];
+                    const long long f = (long long)fz * N * M + (long long)fy * N + fx;
+                    for (int o = 0; o < fol.n; o++) {
+                        const int gx = fx + fol.o[o][0], gy = fy + fol.o[o][1], gz = fz + fol.o[o][2];
+                        if (gx < 0 || gx >= N || gy < 0 || gy >= M || gz < 0 || gz >= K) continue;
+                        const double a_fg = Af[(size_t)o * n + f];
+                        if (a_fg == 0.0) continue;
+                        const double ra = rw * a_fg;
+                        for (int s = 0; s < 2; s++) {
+                            const float wz = pz.w[2 * gz + s];
+                            if (wz == 0.f) continue;
+                            const int dz = pz.c[2 * gz + s] - Z;
+                            for (int t = 0; t < 2; t++) {
+                                const float wy = py.w[2 * gy + t];
+                                if (wy == 0.f) continue;
+                                const int dy = py.c[2 * gy + t] - Y;
+                                for (int u = 0; u < 2; u++) {
+                                    const float wx = px.w[2 * gx + u];
+                                    if (wx == 0.f) continue;
+                                    const int dx = px.c[2 * gx + u] - X;
+                                    const int q2 = ((dz + crz) * by + (dy + cry)) * bx + (dx + crx);
+                                    box[q2] += ra * ((double)wz * (double)wy * (double)wx);
+                                }
+                            }
+                        }
+                    }
+                }
+        for (int q = 0; q < nbox; q++) Ac[(size_t)q * nc + I] = box[q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ADLJ line splitting
+// ---------------------------------------------------------------------------
+// Raw line tridiagonals (natural layout): for each stencil neighbour whose
+// flat column equals i-NM, i-N, i-1, i, i+1, i+N, i+NM the value goes to the
+// matching slot, exactly as SmootherADLJ::_k_build matches CSR columns
+// (smoother_adlj.h:40-86).  lo_d[i] = coupling to the previous cell of the
+// d-line of i, up_d[i] = to the next one, dg = diagonal (shared).
+__global__ void k_adlj_extract(int N, int M, int K, OffList ol, const double* __restrict__ A,
+                               double* __restrict__ dg, double* __restrict__ xlo, double* __restrict__ xup,
+                               double* __restrict__ ylo, double* __restrict__ yup,
+                               double* __restrict__ zlo, double* __restrict__ zup)
+{
+    const long long n = (long long)N * M * K;
+    const int NM = N * M;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int ix, iy, iz;
+        cell_xyz(i, N, NM, ix, iy, iz);
+        double d = 0, xl = 0, xu = 0, yl = 0, yu = 0, zl = 0, zu = 0;
+        for (int o = 0; o < ol.n; o++) {
+            const int jx = ix + ol.o[o][0], jy = iy + ol.o[o][1], jz = iz + ol.o[o][2];
+            if (jx < 0 || jx >= N || jy < 0 || jy >= M || jz < 0 || jz >= K) continue;
+            const long long delta = ol.o[o][0] + (long long)ol.o[o][1] * N + (long long)ol.o[o][2] * NM;
+            const double v = A[(size_t)o * n + i];
+            if (delta == -NM) zl = v;
+            else if (delta == -N) yl = v;
+            else if (delta == -1) xl = v;
+            else if (delta == 0) d = v;
+            else if (delta == 1) xu = v;
+            else if (delta == N) yu = v;
+            else if (delta == NM) zu = v;
+        }
+        dg[i] = d;
+        xlo[i] = xl; xup[i] = xu;
+        ylo[i] = yl; yup[i] = yu;
+        zlo[i] = zl; zup[i] = zu;
+    }
+}
+
+__global__ void k_absmax(long long n, const double* __restrict__ a, double* partial, unsigned int* counter,
+                         double* out)
+{
+    double m = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(a[i]));
+    // max-reduce through the same partial buffer
+    __shared__ double sh[32];
+    __shared__ bool last;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t = fmax(t, sh[w]);
+        partial[blockIdx.x] = t;
+        __threadfence();
+        last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double t = 0.0;
+        for (int b = 0; b < (int)gridDim.x; b++) t = fmax(t, ((volatile double*)partial)[b]);
+        *out = t;
+        *counter = 0u;
+    }
+}
+
+// Geometry of the lines of one direction in natural indexing:
+//   cell of line l at position t = start(l) + t * stride
+struct LineGeom {
+    int N, M, K;
+    int dir;        // 0 x, 1 y, 2 z
+    __host__ __device__ long long nlines() const { return dir == 0 ? (long long)M * K : (dir == 1 ? (long long)N * K : (long long)N * M); }
+    __host__ __device__ int len() const { return dir == 0 ? N : (dir == 1 ? M : K); }
+};
+
+__device__ __forceinline__ long long line_start(const LineGeom& g, long long l)
+{
+    if (g.dir == 0) return l * g.N;                                        // l = y + M z
+    if (g.dir == 1) {                                                      // l = x + N z
+        const long long z = l / g.N, x = l - z * g.N;
+        return z * (long long)g.N * g.M + x;
+    }
+    return l;                                                              // l = x + N y
+}
+__device__ __forceinline__ long long line_stride(const LineGeom& g)
+{
+    return g.dir == 0 ? 1 : (g.dir == 1 ? g.N : (long long)g.N * g.M);
+}
+
+// Per-line LU of the line tridiagonals (TriDiagonalMatrix::triLU,
+// tridiagonal_matrix.h:45-67) when no coupling crosses line ends: each line
+// starts afresh.  dinv <- inverse pivots (0 below tiny), up <- up * dinv.
+__global__ void k_trilu_lines(LineGeom g, const double* __restrict__ tinyp, const double* __restrict__ lo,
+                              double* __restrict__ dinv, double* __restrict__ up)
+{
+    const long long nl = g.nlines();
+    const int L = g.len();
+    const long long st = line_stride(g);
+    const double tiny = *tinyp;
+    for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < nl;
+         l += (long long)gridDim.x * blockDim.x) {
+        long long i = line_start(g, l);
+        double aux = dinv[i];
+        double dprev = (fabs(aux) < tiny) ? 0.0 : 1.0 / aux;
+        dinv[i] = dprev;
+        for (int t = 1; t < L; t++) {
+            const long long ip = i;
+            i += st;
+            const double e = up[ip] * dprev;
+            up[ip] = e;
+            aux = dinv[i] - lo[i] * e;
+            dprev = (fabs(aux) < tiny) ? 0.0 : 1.0 / aux;
+            dinv[i] = dprev;
+        }
+        up[i] *= dprev;   // coupling across the line end (zero unless aliased)
+    }
+}
+
+// Serial LU over the whole direction order, for levels whose line ends are
+// coupled (a dimension too small for the stencil, see k_adlj_extract).
+__global__ void k_trilu_serial(LineGeom g, const double* __restrict__ tinyp, const double* __restrict__ lo,
+                               double* __restrict__ dinv, double* __restrict__ up)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const double tiny = *tinyp;
+    const long long nl = g.nlines();
+    const int L = g.len();
+    const long long st = line_stride(g);
+    double dprev = 0.0;
+    long long ip = -1;
+    for (long long l = 0; l < nl; l++) {
+        long long i = line_start(g, l);
+        for (int t = 0; t < L; t++, i += st) {
+            double aux = dinv[i];
+            if (ip >= 0) {
+                const double e = up[ip] * dprev;
+                up[ip] = e;
+                aux -= lo[i] * e;
+            }
+            dprev = (fabs(aux) < tiny) ? 0.0 : 1.0 / aux;
+            dinv[i] = dprev;
+            ip = i;
+        }
+    }
+}
+
+// Flags coupling across line ends: lo(start of line l+1) * up(end of line l).
+__global__ void k_line_coupling(LineGeom g, const double* __restrict__ lo, const double* __restrict__ up,
+                                int* flag)
+{
+    const long long nl = g.nlines();
+    const int L = g.len();
+    const long long st = line_stride(g);
+    for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l + 1 < nl;
+         l += (long long)gridDim.x * blockDim.x) {
+        const long long iend = line_start(g, l) + (long long)(L - 1) * st;
+        const long long inext = line_start(g, l + 1);
+        if (lo[inext] != 0.0 && up[iend] != 0.0) atomicOr(flag, 1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ADLJ line solves:  c = omega * T^{-1} r ;  ch += c
+// ---------------------------------------------------------------------------
+
+// y- and z-lines: one thread per line, neighbouring threads on neighbouring x
+// (coalesced).  The forward sweep stores into c, the backward sweep finishes
+// it in place.  quirk_first >= 0: natural index base of the z-line first
+// right-hand side as the reference reads it (y*N*K + x), see header.
+template <typename T>
+__global__ void __launch_bounds__(128) k_tdma_strided(LineGeom g, bool zquirk, const T* __restrict__ lo,
+                                                       const T* __restrict__ dinv, const T* __restrict__ up,
+                                                       const T* __restrict__ r, T* __restrict__ c,
+                                                       T* __restrict__ ch, T omega)
+{
+    const long long nl = g.nlines();
+    const int L = g.len();
+    const long long st = line_stride(g);
+    for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < nl;
+         l += (long long)gridDim.x * blockDim.x) {
+        const long long i0 = line_start(g, l);
+        long long i = i0;
+        T rhs0;
+        if (zquirk) {
+            // line l = x + N*y; the reference reads right_member[y*N*K + x]
+            const long long y = l / g.N, x = l - y * g.N;
+            rhs0 = r[y * (long long)g.N * g.K + x];
+        } else {
+            rhs0 = r[i];
+        }
+        T yv = rhs0 * dinv[i];
+        c[i] = yv;
+        for (int t = 1; t < L; t++) {
+            i += st;
+            yv = (r[i] - lo[i] * yv) * dinv[i];
+            c[i] = yv;
+        }
+        // backward: x_t = y_t - up_t x_{t+1}
+        T xv = yv;
+        T cv = omega * xv;
+        c[i] = cv;
+        ch[i] += cv;
+        for (int t = L - 2; t >= 0; t--) {
+            i -= st;
+            xv = c[i] - up[i] * xv;
+            cv = omega * xv;
+            c[i] = cv;
+            ch[i] += cv;
+        }
+    }
+}
+
+// x-lines: one warp per line.  The forward recurrence y_t = D_t r_t -
+// D_t lo_t y_{t-1} and the backward one x_t = y_t - up_t x_{t+1} are affine;
+// each round of 32 consecutive cells is solved by a warp scan of affine maps
+// (a, b) o (a', b') = (a + b a', b b'), carrying the last value between rounds.
+template <typename T>
+__global__ void __launch_bounds__(256) k_tdma_xwarp(int N, long long nlines, const T* __restrict__ lo,
+                                                     const T* __restrict__ dinv, const T* __restrict__ up,
+                                                     const T* __restrict__ r, T* __restrict__ c,
+                                                     T* __restrict__ ch, T omega)
+{
+    const int lane = threadIdx.x & 31;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int rounds = (N + 31) >> 5;
+    for (long long l = warp; l < nlines; l += nwarps) {
+        const long long base = l * N;
+        T carry = 0;
+        for (int rd = 0; rd < rounds; rd++) {
+            const int t = rd * 32 + lane;
+            T a = 0, b = 1;
+            if (t < N) {
+                const long long i = base + t;
+                const T D = dinv[i];
+                a = r[i] * D;
+                b = (t == 0) ? (T)0 : -lo[i] * D;
+            }
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const T a2 = __shfl_up_sync(0xffffffffu, a, o);
+                const T b2 = __shfl_up_sync(0xffffffffu, b, o);
+                if (lane >= o) {
+                    a = a + b * a2;
+                    b = b * b2;
+                }
+            }
+            const T yv = a + b * carry;
+            if (t < N) c[base + t] = yv;
+            carry = __shfl_sync(0xffffffffu, yv, 31);
+        }
+        __syncwarp();
+        carry = 0;
+        for (int rd = 0; rd < rounds; rd++) {
+            const int t = N - 1 - (rd * 32 + lane);
+            T a = 0, b = 1;
+            if (t >= 0) {
+                const long long i = base + t;
+                a = c[i];
+                b = (t == N - 1) ? (T)0 : -up[i];
+            }
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const T a2 = __shfl_up_sync(0xffffffffu, a, o);
+                const T b2 = __shfl_up_sync(0xffffffffu, b, o);
+                if (lane >= o) {
+                    a = a + b * a2;
+                    b = b * b2;
+                }
+            }
+            const T xv = a + b * carry;
+            carry = __shfl_sync(0xffffffffu, xv, 31);
+            if (t >= 0) {
+                const long long i = base + t;
+                const T cv = omega * xv;
+                c[i] = cv;
+                ch[i] += cv;
+            }
+        }
+    }
+}
+
+// Coarsest-grid solve with the stored scaled/permuted LU factors
+// (LUDecompositionSparseMatrix DirectGauss/InverseGauss,
+// lu_decomposition_sparse_matrix.h:238-259): one thread, n is tiny.
+template <typename T>
+__global__ void k_coarse_solve(int n, const double* __restrict__ L, const double* __restrict__ U,
+                               const double* __restrict__ scale, const int* __restrict__ perm,
+                               const T* __restrict__ b, T* __restrict__ ch, double* __restrict__ work)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double* y = work;
+    double* z = work + n;
+    for (int i = 0; i < n; i++) {
+        double aux = scale[perm[i]] * (double)b[perm[i]];
+        for (int j = 0; j < i; j++) aux -= L[i * n + j] * y[j];
+        y[i] = aux;
+    }
+    for (int i = n - 1; i >= 0; i--) {
+        double aux = y[i];
+        for (int j = i + 1; j < n; j++) aux -= U[i * n + j] * z[j];
+        z[i] = aux / U[i * n + i];
+    }
+    for (int i = 0; i < n; i++) ch[i] = (T)(scale[i] * z[i]);
+}
+
+}  // namespace lsg

@@ -1,0 +1,1326 @@
+// Host orchestration and C ABI of the B200 pressure-Poisson solver.
+//
+// Replaces the reference's MGFGMRES / ILUBiCGStab solvers
+// (Base/Solvers/FGMRES/mg_fgmres.h, Base/Solvers/BiCGStab/ilu_bicgstab.h)
+// behind IterativeSolverInterface (Base/Solvers/iterative_solver_interface.h).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "lsg_ilu.cuh"
+#include "lsg_krylov.cuh"
+
+namespace lsg {
+
+long long g_launches = 0;
+
+// ---------------------------------------------------------------------------
+// host-side tables and helpers
+// ---------------------------------------------------------------------------
+static int grid_levels(int N, int M, int K)
+{
+    // CoarseGridsHierarchy::GridLevels (coarse_grids_hierarchy.h:73-81)
+    double aux = (double)std::min(std::min(N, M), K);
+    int n = 0;
+    while (aux > 2.0) {
+        aux *= 0.5;
+        n++;
+    }
+    return n;
+}
+
+static int coarse_count(int nf, bool& odd)
+{
+    // CoarseGrid::nodesCount (coarse_grid.h:62-69)
+    odd = std::fmod((double)nf, 2.0) > 1e-5;
+    return odd ? (nf + 1) / 2 : nf / 2;
+}
+
+// 1-D prolongation table: for each fine index two (coarse, weight) pairs.
+static void prolong_table(int nf, std::vector<int>& c, std::vector<float>& w)
+{
+    bool odd;
+    const int nc = coarse_count(nf, odd);
+    c.assign(2 * nf, 0);
+    w.assign(2 * nf, 0.f);
+    for (int f = 0; f < nf; f++) {
+        const int I = f / 2;
+        int c0 = 0, c1 = 0;
+        float w0 = 0.f, w1 = 0.f;
+        if (odd) {
+            if (f % 2 == 0) { c0 = I; w0 = 1.f; }
+            else { c0 = I; w0 = 0.5f; c1 = I + 1; w1 = 0.5f; }
+        } else {
+            if (f == 0) { c0 = 0; w0 = 1.f; }
+            else if (f == nf - 1) { c0 = nc - 1; w0 = 1.f; }
+            else if (f % 2 == 0) { c0 = I - 1; w0 = 0.25f; c1 = I; w1 = 0.75f; }
+            else { c0 = I; w0 = 0.75f; c1 = I + 1; w1 = 0.25f; }
+        }
+        c[2 * f] = c0; w[2 * f] = w0;
+        c[2 * f + 1] = c1; w[2 * f + 1] = w1;
+    }
+}
+
+// 1-D restriction table R = P^T: for each coarse index up to 4 (fine, w).
+static void restrict_table(int nf, std::vector<int>& f4, std::vector<float>& w4)
+{
+    bool odd;
+    const int nc = coarse_count(nf, odd);
+    std::vector<int> pc;
+    std::vector<float> pw;
+    prolong_table(nf, pc, pw);
+    f4.assign(4 * nc, -1);
+    w4.assign(4 * nc, 0.f);
+    std::vector<int> cnt(nc, 0);
+    for (int f = 0; f < nf; f++)
+        for (int a = 0; a < 2; a++) {
+            if (pw[2 * f + a] == 0.f) continue;
+            const int I = pc[2 * f + a];
+            f4[4 * I + cnt[I]] = f;
+            w4[4 * I + cnt[I]] = pw[2 * f + a];
+            cnt[I]++;
+        }
+}
+
+// Radius of the Galerkin coarse stencil in one dimension.
+static int coarse_radius(int rf, bool odd, bool agglomerate)
+{
+    std::vector<int> rs, ps;
+    if (agglomerate) rs = {0, 1};
+    else if (odd) rs = {-1, 0, 1};
+    else rs = {-1, 0, 1, 2};
+    if (odd) ps = {-1, 0, 1};
+    else ps = {-1, 0, 1, 2};
+    int rc = 0;
+    for (int sr : rs)
+        for (int a = -rf; a <= rf; a++)
+            for (int sp : ps) {
+                const int v = sr + a - sp;
+                if (v % 2 == 0) rc = std::max(rc, std::abs(v / 2));
+            }
+    return rc;
+}
+
+static OffList make_offlist(const std::vector<int>& off)
+{
+    OffList ol;
+    std::memset(&ol, 0, sizeof(ol));
+    ol.n = (int)off.size() / 3;
+    ol.center = -1;
+    for (int o = 0; o < ol.n; o++) {
+        for (int d = 0; d < 3; d++) ol.o[o][d] = (signed char)off[3 * o + d];
+        if (off[3 * o] == 0 && off[3 * o + 1] == 0 && off[3 * o + 2] == 0) ol.center = o;
+    }
+    return ol;
+}
+
+static const int kFine7[21] = {0, 0, -1, 0, -1, 0, -1, 0, 0, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1};
+
+// ---------------------------------------------------------------------------
+// multigrid level storage (FP64 master copy; FP32 shadow for mixed precision)
+// ---------------------------------------------------------------------------
+struct TransferTabs {
+    DevBuf<int> pc[3];
+    DevBuf<float> pw[3];
+    DevBuf<int> rf[3];
+    DevBuf<float> rw[3];
+    PTab P(int d) const { return PTab{pc[d].p, pw[d].p}; }
+    RTab R(int d) const { return RTab{rf[d].p, rw[d].p}; }
+};
+
+template <typename T>
+struct LevelT {
+    Dims d;
+    std::vector<int> off;     // 3 * noff
+    OffList ol;
+    const T* A = nullptr;     // noff * n coefficient planes
+    DevBuf<T> Aown;
+    DevBuf<T> lo[3], dinv[3], up[3];
+    DevBuf<T> r, c, ch;
+};
+
+struct MGData {
+    int L = 0;                // coarse levels
+    std::vector<Dims> dims;   // L + 1
+    std::vector<TransferTabs> tabs;   // L (level l -> l+1)
+    std::vector<bool> agg;            // L
+    std::vector<LevelT<double>> l64;  // L + 1 (operators, factors for l < L)
+    std::vector<LevelT<float>> l32;
+    // coarsest LU
+    int nc = 0;
+    DevBuf<double> dL, dU, dscale, dwork;
+    DevBuf<int> dperm;
+    bool fp32 = false;
+};
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct Context {
+    int device = 0;
+    cudaStream_t s = nullptr;
+    std::string err;
+    Dims d;
+    long long n = 0;
+    DevBuf<double> A7;        // fine operator, 7 planes (b s w p e n t)
+    bool have_matrix = false, have_setup = false;
+    lsg_options opt;
+    MGData mg;
+    Reducer red;
+    DevBuf<double> scal;      // misc device scalars (64)
+    // Krylov storage
+    int restart = 0;
+    DevBuf<double> V, Z, w, xd, bd, coefs, t1, t2, t3, t4;
+    DevBuf<KrylovScalars> ks;
+    int* hflag = nullptr;
+    double* hnorm = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevBuf<float> v32;        // FP32 preconditioner right-hand side
+    // ILU(0)
+    DevBuf<double> iluL, iluU;        // 3 lower planes (b s w) / 4 planes (p e n t), U diagonal = plane 0
+    bool have_ilu = false;
+    double bytes = 0;
+    int vcycles = 0;
+};
+
+}  // namespace lsg
+
+struct lsg_ctx {
+    lsg::Context c;
+};
+
+namespace lsg {
+
+static void ilu_apply(Context& C, const double* b, double* x);
+
+// ---------------------------------------------------------------------------
+// multigrid setup
+// ---------------------------------------------------------------------------
+static void upload_tabs(TransferTabs& t, const Dims& f, cudaStream_t s)
+{
+    const int nf[3] = {f.N, f.M, f.K};
+    for (int d = 0; d < 3; d++) {
+        std::vector<int> pc, rf;
+        std::vector<float> pw, rw;
+        prolong_table(nf[d], pc, pw);
+        restrict_table(nf[d], rf, rw);
+        t.pc[d].alloc(pc.size());
+        t.pw[d].alloc(pw.size());
+        t.rf[d].alloc(rf.size());
+        t.rw[d].alloc(rw.size());
+        LSG_CUDA(cudaMemcpyAsync(t.pc[d].p, pc.data(), pc.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        LSG_CUDA(cudaMemcpyAsync(t.pw[d].p, pw.data(), pw.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+        LSG_CUDA(cudaMemcpyAsync(t.rf[d].p, rf.data(), rf.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        LSG_CUDA(cudaMemcpyAsync(t.rw[d].p, rw.data(), rw.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    }
+}
+
+// Scaled partial-pivoting dense LU of the coarsest operator, a restatement
+// of LUDecompositionSparseMatrix::initScalePerm/calcLU
+// (Base/SparseMatrix/Decomposition/lu_decomposition_sparse_matrix.h:66-215).
+// A is row-major dense; first_col0[i] tells whether the first stored CSR
+// entry of row i is in column 0 (the first pivot search only looks there).
+static void coarse_lu(int n, const std::vector<double>& A, const std::vector<char>& first_col0,
+                      std::vector<double>& L, std::vector<double>& U, std::vector<double>& scale,
+                      std::vector<int>& perm)
+{
+    L.assign((size_t)n * n, 0.0);
+    U.assign((size_t)n * n, 0.0);
+    scale.assign(n, 1.0);
+    perm.resize(n);
+    double maxabs = 0.0;
+    for (int i = 0; i < n; i++) {
+        const double dg = std::fabs(A[(size_t)i * n + i]);
+        scale[i] = (dg > 1e-5) ? 1.0 / std::sqrt(dg) : 1.0;
+        perm[i] = i;
+        for (int j = 0; j < n; j++) maxabs = std::max(maxabs, std::fabs(A[(size_t)i * n + j]));
+    }
+    const double tiny = 1e-13 * maxabs;
+    double maxv = 0.0;
+    int piv = 0;
+    for (int i = 0; i < n; i++) {
+        if (!first_col0[i]) continue;
+        const double v = std::fabs(A[(size_t)i * n] * scale[i] * scale[0]);
+        if (v > maxv) { maxv = v; piv = i; }
+    }
+    if (piv != 0) std::swap(perm[0], perm[piv]);
+    {
+        const int p0 = perm[0];
+        for (int j = 0; j < n; j++) U[j] = A[(size_t)p0 * n + j] * scale[p0] * scale[j];
+        double u00 = U[0];
+        if (std::fabs(u00) < tiny) u00 = (u00 < 0) ? -tiny : tiny;
+        U[0] = u00;
+        const double inv = scale[0] / u00;
+        for (int k = 1; k < n; k++) L[(size_t)k * n] = A[(size_t)perm[k] * n] * scale[perm[k]] * inv;
+        L[0] = 1.0;
+    }
+    std::vector<double> col(n, 0.0);
+    for (int i = 1; i < n; i++) {
+        maxv = 0.0;
+        piv = i;
+        const double si = scale[i];
+        for (int k = i; k < n; k++) {
+            double s = 0.0;
+            for (int t = 0; t < i; t++) s += L[(size_t)k * n + t] * U[(size_t)t * n + i];
+            const double val = A[(size_t)perm[k] * n + i] * scale[perm[k]] * si - s;
+            col[k] = val;
+            if (std::fabs(val) > maxv) { maxv = std::fabs(val); piv = k; }
+        }
+        if (piv != i) {
+            std::swap(perm[i], perm[piv]);
+            for (int t = 0; t < i; t++) std::swap(L[(size_t)i * n + t], L[(size_t)piv * n + t]);
+            std::swap(col[i], col[piv]);
+        }
+        const int pi = perm[i];
+        const double sp = scale[pi];
+        for (int j = i; j < n; j++) {
+            double s = 0.0;
+            for (int t = 0; t < i; t++) s += L[(size_t)i * n + t] * U[(size_t)t * n + j];
+            U[(size_t)i * n + j] = A[(size_t)pi * n + j] * sp * scale[j] - s;
+        }
+        double uii = U[(size_t)i * n + i];
+        if (std::fabs(uii) < tiny) uii = (uii < 0) ? -tiny : tiny;
+        U[(size_t)i * n + i] = uii;
+        const double inv = 1.0 / uii;
+        for (int k = i + 1; k < n; k++) L[(size_t)k * n + i] = col[k] * inv;
+        L[(size_t)i * n + i] = 1.0;
+    }
+}
+
+template <typename T>
+static void alloc_vectors(LevelT<T>& lv)
+{
+    const long long n = lv.d.n();
+    lv.r.alloc(n);
+    lv.c.alloc(n);
+    lv.ch.alloc(n);
+}
+
+static void mg_setup(Context& C)
+{
+    MGData& mg = C.mg;
+    const lsg_options& o = C.opt;
+    cudaStream_t s = C.s;
+    int L = grid_levels(C.d.N, C.d.M, C.d.K);
+    if (o.max_levels > 0) L = std::min(L, o.max_levels);
+    LSG_REQUIRE(L >= 1, LSG_ERR_ARG, "grid too small for a multigrid hierarchy (min dimension <= 2)");
+    mg.L = L;
+    mg.dims.assign(L + 1, Dims());
+    mg.tabs.clear();
+    mg.tabs.resize(L);
+    mg.agg.assign(L, false);
+    mg.l64.clear();
+    mg.l64.resize(L + 1);
+    mg.dims[0] = C.d;
+    mg.l64[0].d = C.d;
+    mg.l64[0].off.assign(kFine7, kFine7 + 21);
+    mg.l64[0].ol = make_offlist(mg.l64[0].off);
+    mg.l64[0].A = C.A7.p;
+    std::vector<int> rad = {1, 1, 1};
+    for (int l = 0; l < L; l++) {
+        const Dims f = mg.dims[l];
+        bool oN, oM, oK;
+        Dims c;
+        c.N = coarse_count(f.N, oN);
+        c.M = coarse_count(f.M, oM);
+        c.K = coarse_count(f.K, oK);
+        mg.dims[l + 1] = c;
+        const bool agg = !oN && !oM && !oK;
+        mg.agg[l] = agg;
+        upload_tabs(mg.tabs[l], f, s);
+        const int crx = coarse_radius(rad[0], oN, agg), cry = coarse_radius(rad[1], oM, agg),
+                  crz = coarse_radius(rad[2], oK, agg);
+        LSG_REQUIRE((2 * crx + 1) * (2 * cry + 1) * (2 * crz + 1) <= 125, LSG_ERR_ARG, "coarse stencil too wide");
+        LevelT<double>& cl = mg.l64[l + 1];
+        cl.d = c;
+        cl.off.clear();
+        for (int dz = -crz; dz <= crz; dz++)
+            for (int dy = -cry; dy <= cry; dy++)
+                for (int dx = -crx; dx <= crx; dx++) {
+                    cl.off.push_back(dx);
+                    cl.off.push_back(dy);
+                    cl.off.push_back(dz);
+                }
+        cl.ol = make_offlist(cl.off);
+        cl.Aown.alloc((size_t)cl.ol.n * c.n());
+        cl.A = cl.Aown.p;
+        const TransferTabs& t = mg.tabs[l];
+        k_galerkin<<<grid_for(c.n(), 128), 128, 0, s>>>(f.N, f.M, f.K, mg.l64[l].ol, mg.l64[l].A, c.N, c.M, c.K, crx,
+                                                        cry, crz, agg, t.P(0), t.P(1), t.P(2), t.R(0), t.R(1), t.R(2),
+                                                        cl.Aown.p);
+        LSG_CHECK_LAUNCH();
+        rad = {crx, cry, crz};
+    }
+    // ADLJ line factors of every smoothed level
+    double* tinyp = C.scal.p;
+    int* flag = (int*)(C.scal.p + 8);
+    for (int l = 0; l < L; l++) {
+        LevelT<double>& lv = mg.l64[l];
+        const long long n = lv.d.n();
+        for (int d = 0; d < 3; d++) {
+            lv.lo[d].alloc(n);
+            lv.dinv[d].alloc(n);
+            lv.up[d].alloc(n);
+        }
+        k_adlj_extract<<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.ol, lv.A, lv.dinv[0].p, lv.lo[0].p,
+                                                       lv.up[0].p, lv.lo[1].p, lv.up[1].p, lv.lo[2].p, lv.up[2].p);
+        LSG_CHECK_LAUNCH();
+        LSG_CUDA(cudaMemcpyAsync(lv.dinv[1].p, lv.dinv[0].p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        LSG_CUDA(cudaMemcpyAsync(lv.dinv[2].p, lv.dinv[0].p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        // tiny = max(1e-5 * max|d|, 1e-12)   (tridiagonal_matrix.h:49-57)
+        k_absmax<<<grid_for(n, 256, Reducer::kMaxBlocks), 256, 0, s>>>(n, lv.dinv[0].p, C.red.partial.p,
+                                                                      C.red.counter.p, tinyp);
+        LSG_CHECK_LAUNCH();
+        double maxabs = 0.0;
+        LSG_CUDA(cudaMemcpyAsync(&maxabs, tinyp, sizeof(double), cudaMemcpyDeviceToHost, s));
+        LSG_CUDA(cudaStreamSynchronize(s));
+        double tiny = 1e-5 * maxabs;
+        if (tiny < 1e-12) tiny = 1e-12;
+        LSG_CUDA(cudaMemcpyAsync(tinyp, &tiny, sizeof(double), cudaMemcpyHostToDevice, s));
+        for (int d = 0; d < 3; d++) {
+            LineGeom g{lv.d.N, lv.d.M, lv.d.K, d};
+            LSG_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
+            k_line_coupling<<<grid_for(g.nlines(), 256), 256, 0, s>>>(g, lv.lo[d].p, lv.up[d].p, flag);
+            LSG_CHECK_LAUNCH();
+            int coupled = 0;
+            LSG_CUDA(cudaMemcpyAsync(&coupled, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+            LSG_CUDA(cudaStreamSynchronize(s));
+            if (coupled)
+                k_trilu_serial<<<1, 1, 0, s>>>(g, tinyp, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p);
+            else
+                k_trilu_lines<<<grid_for(g.nlines(), 128), 128, 0, s>>>(g, tinyp, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p);
+            LSG_CHECK_LAUNCH();
+        }
+        alloc_vectors(lv);
+    }
+    alloc_vectors(mg.l64[L]);
+    // coarsest dense LU on the host
+    {
+        LevelT<double>& cl = mg.l64[L];
+        const int nc = (int)cl.d.n();
+        LSG_REQUIRE(nc <= 4096, LSG_ERR_ARG, "coarsest level too large for the dense LU");
+        const int no = cl.ol.n;
+        std::vector<double> box((size_t)no * nc);
+        LSG_CUDA(cudaMemcpyAsync(box.data(), cl.A, box.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        LSG_CUDA(cudaStreamSynchronize(s));
+        std::vector<double> A((size_t)nc * nc, 0.0);
+        std::vector<char> first0(nc, 0);
+        const int N = cl.d.N, M = cl.d.M, K = cl.d.K, NM = N * M;
+        for (int i = 0; i < nc; i++) {
+            const int z = i / NM, y = (i - z * NM) / N, x = i - z * NM - y * N;
+            int firstcol = nc;
+            for (int q = 0; q < no; q++) {
+                const int jx = x + cl.off[3 * q], jy = y + cl.off[3 * q + 1], jz = z + cl.off[3 * q + 2];
+                if (jx < 0 || jx >= N || jy < 0 || jy >= M || jz < 0 || jz >= K) continue;
+                const int j = jx + jy * N + jz * NM;
+                A[(size_t)i * nc + j] += box[(size_t)q * nc + i];
+                firstcol = std::min(firstcol, j);   // structural pattern (sorted CSR)
+            }
+            first0[i] = (firstcol == 0);
+        }
+        std::vector<double> Lh, Uh, sc;
+        std::vector<int> pm;
+        coarse_lu(nc, A, first0, Lh, Uh, sc, pm);
+        mg.nc = nc;
+        mg.dL.alloc(Lh.size());
+        mg.dU.alloc(Uh.size());
+        mg.dscale.alloc(nc);
+        mg.dperm.alloc(nc);
+        mg.dwork.alloc(2 * (size_t)nc);
+        LSG_CUDA(cudaMemcpyAsync(mg.dL.p, Lh.data(), Lh.size() * 8, cudaMemcpyHostToDevice, s));
+        LSG_CUDA(cudaMemcpyAsync(mg.dU.p, Uh.data(), Uh.size() * 8, cudaMemcpyHostToDevice, s));
+        LSG_CUDA(cudaMemcpyAsync(mg.dscale.p, sc.data(), sc.size() * 8, cudaMemcpyHostToDevice, s));
+        LSG_CUDA(cudaMemcpyAsync(mg.dperm.p, pm.data(), pm.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        LSG_CUDA(cudaStreamSynchronize(s));
+    }
+    // FP32 shadow hierarchy
+    mg.fp32 = (o.mg_precision == LSG_FP32);
+    mg.l32.clear();
+    if (mg.fp32) {
+        mg.l32.resize(L + 1);
+        for (int l = 0; l <= L; l++) {
+            LevelT<double>& a = mg.l64[l];
+            LevelT<float>& b = mg.l32[l];
+            b.d = a.d;
+            b.off = a.off;
+            b.ol = a.ol;
+            const long long n = a.d.n();
+            b.Aown.alloc((size_t)a.ol.n * n);
+            b.A = b.Aown.p;
+            k_convert<float, double><<<grid_for((long long)a.ol.n * n, 256), 256, 0, s>>>((long long)a.ol.n * n, a.A, b.Aown.p);
+            LSG_CHECK_LAUNCH();
+            if (l < L) {
+                for (int d = 0; d < 3; d++) {
+                    b.lo[d].alloc(n);
+                    b.dinv[d].alloc(n);
+                    b.up[d].alloc(n);
+                    k_convert<float, double><<<grid_for(n, 256), 256, 0, s>>>(n, a.lo[d].p, b.lo[d].p);
+                    k_convert<float, double><<<grid_for(n, 256), 256, 0, s>>>(n, a.dinv[d].p, b.dinv[d].p);
+                    k_convert<float, double><<<grid_for(n, 256), 256, 0, s>>>(n, a.up[d].p, b.up[d].p);
+                    LSG_CHECK_LAUNCH();
+                }
+            }
+            alloc_vectors(b);
+        }
+    }
+    LSG_CUDA(cudaStreamSynchronize(s));
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle (MultiGridSolver::solve, multigrid_solver.h:48-75).
+// Input: right-hand side already in lev[0].r.  Output: lev[0].ch.
+// ---------------------------------------------------------------------------
+template <typename T>
+static void apply_resid(const LevelT<T>& lv, const T* x, T* r, cudaStream_t s, int mode)
+{
+    const long long n = lv.d.n();
+    if (lv.ol.n == 7 && lv.off[0] == 0 && lv.off[2] == -1) {
+        if (mode == 0)
+            k_apply7<T, 0><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.A, x, r);
+        else
+            k_apply7<T, 1><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.A, x, r);
+    } else {
+        if (mode == 0)
+            k_applybox<T, 0><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.ol, lv.A, x, r);
+        else
+            k_applybox<T, 1><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.ol, lv.A, x, r);
+    }
+    LSG_CHECK_LAUNCH();
+}
+
+template <typename T>
+static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStream_t s)
+{
+    const Dims& g = lv.d;
+    if (d == 0) {
+        const long long nl = (long long)g.M * g.K;
+        const int blocks = grid_for(nl * 32, 256, 148 * 64);
+        k_tdma_xwarp<T><<<blocks, 256, 0, s>>>(g.N, nl, lv.lo[0].p, lv.dinv[0].p, lv.up[0].p, lv.r.p, lv.c.p,
+                                               lv.ch.p, omega);
+    } else {
+        LineGeom lg{g.N, g.M, g.K, d};
+        k_tdma_strided<T><<<grid_for(lg.nlines(), 128, 148 * 64), 128, 0, s>>>(
+            lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, lv.ch.p, omega);
+    }
+    LSG_CHECK_LAUNCH();
+}
+
+template <typename T>
+static void vcycle(Context& C, std::vector<LevelT<T>>& lev)
+{
+    MGData& mg = C.mg;
+    cudaStream_t s = C.s;
+    const int L = mg.L;
+    for (int l = 0; l < L; l++) {
+        const Dims& f = lev[l].d;
+        const Dims& c = lev[l + 1].d;
+        const TransferTabs& t = mg.tabs[l];
+        k_restrict<T><<<grid_for(c.n(), 256), 256, 0, s>>>(c.N, c.M, c.K, f.N, f.M, mg.agg[l], t.R(0), t.R(1), t.R(2),
+                                                          lev[l].r.p, lev[l + 1].r.p);
+        LSG_CHECK_LAUNCH();
+    }
+    k_coarse_solve<T><<<1, 32, 0, s>>>(mg.nc, mg.dL.p, mg.dU.p, mg.dscale.p, mg.dperm.p, lev[L].r.p, lev[L].ch.p,
+                                       mg.dwork.p);
+    LSG_CHECK_LAUNCH();
+    const T omega = (T)C.opt.omega;
+    const bool zq = C.opt.zline_reference != 0;
+    for (int l = L - 1; l >= 0; l--) {
+        LevelT<T>& lv = lev[l];
+        const Dims& f = lv.d;
+        const TransferTabs& t = mg.tabs[l];
+        k_prolong<T><<<grid_for(f.n(), 256), 256, 0, s>>>(f.N, f.M, f.K, lev[l + 1].d.N, lev[l + 1].d.M, t.P(0), t.P(1),
+                                                         t.P(2), lev[l + 1].ch.p, lv.ch.p, lv.c.p);
+        LSG_CHECK_LAUNCH();
+        for (int it = 0; it < C.opt.n_post; it++) {
+            const int order[3] = {2, 1, 0};       // SmootherADLJ::solve: z, y, x
+            for (int q = 0; q < 3; q++) {
+                apply_resid<T>(lv, lv.c.p, lv.r.p, s, 0);   // calcRes: r -= A c
+                line_solve<T>(lv, order[q], zq, omega, s);  // c = omega T^-1 r ; ch += c
+            }
+        }
+    }
+    C.vcycles++;
+}
+
+// Algorithmic bytes of one V-cycle with element size w (documented model).
+static double vcycle_bytes(const MGData& mg, int n_post, double w)
+{
+    double b = 0;
+    for (int l = 0; l <= mg.L; l++) {
+        const double n = (double)mg.dims[l].n();
+        const double noff = (l == 0) ? 7.0 : (double)mg.l64[l].ol.n;
+        if (l < mg.L) {
+            b += (1.0 + 0.125) * w * n;                      // restriction read fine + write coarse
+            b += (0.125 + 2.0) * w * n;                      // prolongation read coarse + write ch, c
+            // per direction: residual (r rw, c, A) + line solve (r, lo, dinv, up, c w r w, ch rw)
+            b += 3.0 * n_post * ((2.0 + 1.0 + noff) + (1.0 + 3.0 + 3.0 + 2.0)) * w * n;
+        }
+    }
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// preconditioner application z = M^{-1} v  (v FP64 on the device)
+// ---------------------------------------------------------------------------
+static void precond_apply(Context& C, const double* v, double* z)
+{
+    cudaStream_t s = C.s;
+    const long long n = C.n;
+    if (C.opt.precond == LSG_PC_NONE) {
+        LSG_CUDA(cudaMemcpyAsync(z, v, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        return;
+    }
+    if (C.opt.precond == LSG_PC_ILU0) {
+        ilu_apply(C, v, z);
+        return;
+    }
+    if (C.mg.fp32) {
+        auto& lev = C.mg.l32;
+        k_convert<float, double><<<grid_for(n, 256), 256, 0, s>>>(n, v, lev[0].r.p);
+        LSG_CHECK_LAUNCH();
+        vcycle<float>(C, lev);
+        k_convert<double, float><<<grid_for(n, 256), 256, 0, s>>>(n, lev[0].ch.p, z);
+        LSG_CHECK_LAUNCH();
+    } else {
+        auto& lev = C.mg.l64;
+        LSG_CUDA(cudaMemcpyAsync(lev[0].r.p, v, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        vcycle<double>(C, lev);
+        LSG_CUDA(cudaMemcpyAsync(z, lev[0].ch.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FGMRES (FGMRESInterface::solve, fgmres_interface.h:78-142)
+// ---------------------------------------------------------------------------
+static void launch_givens(Context& C, int j)
+{
+    k_givens<<<1, 32, 0, C.s>>>(C.ks.p, j, 65, C.opt.eps, C.opt.max_it, C.hflag, C.hnorm);
+    LSG_CHECK_LAUNCH();
+}
+
+static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
+{
+    cudaStream_t s = C.s;
+    const long long n = C.n;
+    const Dims& d = C.d;
+    const int m = C.restart;
+    const int gb = grid_for(n, 256, Reducer::kMaxBlocks);
+    double* part = C.red.partial.p;
+    unsigned int* cnt = C.red.counter.p;
+    KrylovScalars* ks = C.ks.p;
+    const double w8 = 8.0;
+    double bytes = 0;
+    // norm_r = ||b - A x||  ; w = b - A x
+    k_residual7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.A7.p, x, b, C.w.p, part, cnt, &ks->normW2);
+    LSG_CHECK_LAUNCH();
+    bytes += 10 * w8 * n;
+    double nrm2 = 0;
+    LSG_CUDA(cudaMemcpyAsync(&nrm2, &ks->normW2, sizeof(double), cudaMemcpyDeviceToHost, s));
+    LSG_CUDA(cudaStreamSynchronize(s));
+    double norm_r = std::sqrt(nrm2);
+    int it = 0;
+    int status = LSG_OK;
+    if (norm_r > C.opt.eps) {
+        it = 1;
+        // initialise device scalars: norm_r, invNormW = 1/norm_r, it
+        KrylovScalars h;
+        std::memset(&h, 0, sizeof(h));
+        h.norm_r = norm_r;
+        h.invNormW = 1.0 / norm_r;
+        h.it = 1;
+        LSG_CUDA(cudaMemcpyAsync(ks, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+        bool finished = false;
+        while (!finished) {
+            int jlast = m - 1;
+            for (int j = 0; j < m; j++) {
+                double* vj = C.V.p + (size_t)j * n;
+                double* zj = C.Z.p + (size_t)j * n;
+                // v_j = w / ||w|| (also the preconditioner input)
+                if (C.mg.fp32 && C.opt.precond == LSG_PC_MG) {
+                    k_scale_copy<float><<<grid_for(n, 256), 256, 0, s>>>(n, C.w.p, &ks->invNormW, vj, C.mg.l32[0].r.p);
+                    LSG_CHECK_LAUNCH();
+                    vcycle<float>(C, C.mg.l32);
+                    k_convert<double, float><<<grid_for(n, 256), 256, 0, s>>>(n, C.mg.l32[0].ch.p, zj);
+                    LSG_CHECK_LAUNCH();
+                    bytes += (8 + 8 + 4) * (double)n + vcycle_bytes(C.mg, C.opt.n_post, 4.0) + 12.0 * n;
+                } else {
+                    k_scale_copy<double><<<grid_for(n, 256), 256, 0, s>>>(n, C.w.p, &ks->invNormW, vj, C.t1.p);
+                    LSG_CHECK_LAUNCH();
+                    precond_apply(C, C.t1.p, zj);
+                    bytes += 24.0 * n + (C.opt.precond == LSG_PC_MG ? vcycle_bytes(C.mg, C.opt.n_post, 8.0) + 32.0 * n : 0);
+                }
+                // w = A z_j ; H[0,j] = (w, v_0)
+                double* Hj = ks->H + (size_t)j * 65;
+                k_spmv_dot7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.A7.p, zj, C.V.p, C.w.p, part, cnt, Hj);
+                LSG_CHECK_LAUNCH();
+                bytes += 10 * w8 * n;
+                // modified Gram-Schmidt: w -= h_i v_i ; h_{i+1} = (w, v_{i+1}); last: ||w||^2
+                for (int i = 1; i <= j + 1; i++) {
+                    const bool last = (i == j + 1);
+                    k_mgs_step<<<gb, 256, 0, s>>>(n, Hj + (i - 1), C.V.p + (size_t)(i - 1) * n,
+                                                 last ? C.w.p : C.V.p + (size_t)i * n, C.w.p, last, part, cnt,
+                                                 last ? &ks->normW2 : Hj + i);
+                    LSG_CHECK_LAUNCH();
+                    bytes += (last ? 3 : 4) * w8 * n;
+                }
+                launch_givens(C, j);
+                LSG_CUDA(cudaStreamSynchronize(s));
+                const int flag = *(volatile int*)C.hflag;
+                if (flag == 2) {
+                    jlast = j;
+                    finished = true;
+                    break;
+                }
+            }
+            // x += Z y   (solUpdate)
+            k_backsub<<<1, 32, 0, s>>>(ks, jlast, 65, C.coefs.p);
+            LSG_CHECK_LAUNCH();
+            k_multi_axpy<<<grid_for(n, 256), 256, 0, s>>>(n, jlast + 1, C.coefs.p, C.Z.p, x);
+            LSG_CHECK_LAUNCH();
+            bytes += (jlast + 3) * w8 * n;
+            const bool refine = (C.opt.mg_precision == LSG_FP32 && C.opt.precond == LSG_PC_MG);
+            if (!finished || refine) {
+                // w = b - A x: the next cycle's first direction
+                // (fgmres_interface.h:136-138)
+                k_residual7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.A7.p, x, b, C.w.p, part, cnt, C.scal.p + 16);
+                LSG_CHECK_LAUNCH();
+                bytes += 10 * w8 * n;
+                KrylovScalars hs;
+                double tr2 = 0;
+                LSG_CUDA(cudaMemcpyAsync(&hs, ks, sizeof(hs), cudaMemcpyDeviceToHost, s));
+                LSG_CUDA(cudaMemcpyAsync(&tr2, C.scal.p + 16, sizeof(double), cudaMemcpyDeviceToHost, s));
+                LSG_CUDA(cudaStreamSynchronize(s));
+                // FP64 reference semantics restart with the implicit norm |gamma|;
+                // with the FP32 preconditioner the restart is an iterative
+                // refinement step from the true FP64 residual, and the solve only
+                // ends when that true residual meets eps.
+                double g = refine ? std::sqrt(tr2) : std::fabs(hs.norm_r);
+                if (finished) {
+                    if (!(g > C.opt.eps) || !(hs.it < C.opt.max_it) || hs.breakdown) {
+                        hs.norm_r = g;
+                        LSG_CUDA(cudaMemcpyAsync(ks, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
+                        break;
+                    }
+                    finished = false;
+                    hs.it++;
+                }
+                hs.norm_r = g;
+                hs.invNormW = 1.0 / g;
+                hs.done = 0;
+                LSG_CUDA(cudaMemcpyAsync(ks, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
+            }
+        }
+        KrylovScalars hs;
+        LSG_CUDA(cudaMemcpyAsync(&hs, ks, sizeof(hs), cudaMemcpyDeviceToHost, s));
+        LSG_CUDA(cudaStreamSynchronize(s));
+        it = hs.it;
+        norm_r = hs.norm_r;
+        if (hs.breakdown) status = LSG_BREAKDOWN;
+        else if (!(norm_r <= C.opt.eps)) status = LSG_NOT_CONVERGED;
+    }
+    if (st) {
+        st->iterations = it;
+        st->norm_r = norm_r;
+        st->status = status;
+    }
+    C.bytes += bytes;
+    return status;
+}
+
+}  // namespace lsg
+
+namespace lsg {
+
+// ---------------------------------------------------------------------------
+// ILU(0): pivots by hyperplane sweeps, level-scheduled solves in a CUDA graph
+// ---------------------------------------------------------------------------
+
+static void ilu_setup(Context& C)
+{
+    const Dims& d = C.d;
+    LSG_REQUIRE(d.N >= 3 && d.M >= 3 && d.K >= 3, LSG_ERR_ARG, "ILU(0) needs N, M, K >= 3");
+    const long long n = C.n;
+    C.iluU.alloc(n);
+    C.iluL.alloc(3 * n);
+    const int planes = d.N + d.M + d.K - 2;
+    const int blocks = grid_for((long long)d.N * d.M, 256);
+    for (int lv = 0; lv < planes; lv++) {
+        k_ilu_pivots<<<blocks, 256, 0, C.s>>>(lv, d.N, d.M, d.K, C.A7.p, C.iluU.p);
+    }
+    LSG_CHECK_LAUNCH();
+    k_ilu_lower<<<grid_for(n, 256), 256, 0, C.s>>>(d.N, d.M, d.K, C.A7.p, C.iluU.p, C.iluL.p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    C.have_ilu = true;
+}
+
+// x = U^{-1} L^{-1} b ; uses C.t4 for the intermediate
+static void ilu_apply(Context& C, const double* b, double* x)
+{
+    const Dims& d = C.d;
+    const int planes = d.N + d.M + d.K - 2;
+    const int blocks = grid_for((long long)d.N * d.M, 256);
+    double* y = C.t4.p;
+    for (int lv = 0; lv < planes; lv++)
+        k_ilu_fwd<<<blocks, 256, 0, C.s>>>(lv, d.N, d.M, d.K, C.iluL.p, b, y);
+    for (int lv = planes - 1; lv >= 0; lv--)
+        k_ilu_bwd<<<blocks, 256, 0, C.s>>>(lv, d.N, d.M, d.K, C.A7.p, C.iluU.p, y, x);
+    LSG_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------
+// BiCGStab (BiCGStabInterface::solve, bicgstab_interface.h:76-111)
+// ---------------------------------------------------------------------------
+static int bicgstab(Context& C, double* x, const double* b, lsg_stats* st)
+{
+    cudaStream_t s = C.s;
+    const long long n = C.n;
+    const Dims& d = C.d;
+    const int gb = grid_for(n, 256, Reducer::kMaxBlocks);
+    double* part = C.red.partial.p;
+    unsigned int* cnt = C.red.counter.p;
+    double* sc = C.scal.p + 24;   // 8 scalars
+    double* r = C.w.p;
+    double* rr = C.V.p;
+    double* p = C.V.p + n;
+    double* y = C.Z.p;
+    double* z = C.Z.p + n;
+    double* nu = C.t1.p;
+    double* sv = C.t2.p;
+    double* t = C.t3.p;
+    double bytes = 0;
+    int it = 1;
+    k_residual7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.A7.p, x, b, r, part, cnt, sc + 5);
+    LSG_CHECK_LAUNCH();
+    bytes += 80.0 * n;
+    double nr2 = 0;
+    LSG_CUDA(cudaMemcpyAsync(&nr2, sc + 5, 8, cudaMemcpyDeviceToHost, s));
+    LSG_CUDA(cudaStreamSynchronize(s));
+    double norm_r = std::sqrt(nr2);
+    int status = LSG_OK;
+    if (norm_r > C.opt.eps) {
+        LSG_CUDA(cudaMemcpyAsync(rr, r, n * 8, cudaMemcpyDeviceToDevice, s));
+        LSG_CUDA(cudaMemcpyAsync(p, r, n * 8, cudaMemcpyDeviceToDevice, s));
+        do {
+            precond_apply(C, p, y);
+            k_bicg_nu<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.A7.p, y, nu, rr, r, part, cnt, sc);
+            LSG_CHECK_LAUNCH();
+            k_bicg_s<<<grid_for(n, 256), 256, 0, s>>>(n, sc, nu, r, sv);
+            LSG_CHECK_LAUNCH();
+            precond_apply(C, sv, z);
+            k_bicg_t<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.A7.p, z, t, sv, part, cnt, sc + 2);
+            LSG_CHECK_LAUNCH();
+            k_bicg_upd<<<gb, 256, 0, s>>>(n, sc, y, z, x, t, r, sv, rr, part, cnt, sc + 4);
+            LSG_CHECK_LAUNCH();
+            k_bicg_p<<<gb, 256, 0, s>>>(n, sc, p, nu, r, part, cnt, sc + 5);
+            LSG_CHECK_LAUNCH();
+            LSG_CUDA(cudaMemcpyAsync(&nr2, sc + 5, 8, cudaMemcpyDeviceToHost, s));
+            LSG_CUDA(cudaStreamSynchronize(s));
+            norm_r = std::sqrt(nr2);
+            it++;
+            bytes += 8.0 * n * (10 + 4 + 10 + 10 + 5) + (C.opt.precond == LSG_PC_ILU0 ? 2 * 8.0 * n * 12 : 0.0);
+            if (std::isnan(norm_r)) {
+                status = LSG_BREAKDOWN;
+                break;
+            }
+        } while (norm_r > C.opt.eps && it < C.opt.max_it);
+        if (status == LSG_OK && !(norm_r <= C.opt.eps)) status = LSG_NOT_CONVERGED;
+    }
+    if (st) {
+        st->iterations = it;
+        st->norm_r = norm_r;
+        st->status = status;
+    }
+    C.bytes += bytes;
+    return status;
+}
+
+static void krylov_alloc(Context& C)
+{
+    const long long n = C.n;
+    const int m = std::max(2, std::min(C.opt.restart, 64));
+    C.restart = m;
+    C.V.alloc((size_t)m * n);
+    C.Z.alloc((size_t)m * n);
+    C.w.alloc(n);
+    C.t1.alloc(n);
+    C.t2.alloc(n);
+    C.t3.alloc(n);
+    C.t4.alloc(n);
+    C.xd.alloc(n);
+    C.bd.alloc(n);
+    C.coefs.alloc(64);
+}
+
+static double true_residual(Context& C, const double* x, const double* b)
+{
+    const Dims& d = C.d;
+    k_residual7<<<grid_for(C.n, 256, Reducer::kMaxBlocks), 256, 0, C.s>>>(d.N, d.M, d.K, C.A7.p, x, b, C.t1.p,
+                                                                       C.red.partial.p, C.red.counter.p,
+                                                                       C.scal.p + 40);
+    LSG_CHECK_LAUNCH();
+    double r2 = 0;
+    LSG_CUDA(cudaMemcpyAsync(&r2, C.scal.p + 40, 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return std::sqrt(r2);
+}
+
+static int solve_device(Context& C, const double* b, double* x, lsg_stats* st)
+{
+    LSG_REQUIRE(C.have_setup, LSG_ERR_STATE, "lsg_setup must be called before solving");
+    C.bytes = 0;
+    C.vcycles = 0;
+    const long long l0 = g_launches;
+    LSG_CUDA(cudaEventRecord(C.ev0, C.s));
+    int rc;
+    if (C.opt.method == LSG_METHOD_BICGSTAB) rc = bicgstab(C, x, b, st);
+    else rc = fgmres(C, x, b, st);
+    LSG_CUDA(cudaEventRecord(C.ev1, C.s));
+    LSG_CUDA(cudaEventSynchronize(C.ev1));
+    float ms = 0;
+    LSG_CUDA(cudaEventElapsedTime(&ms, C.ev0, C.ev1));
+    if (st) {
+        st->ms = ms;
+        st->bytes = C.bytes;
+        st->vcycles = C.vcycles;
+        st->kernel_launches = g_launches - l0;
+        st->true_residual = true_residual(C, x, b);
+    }
+    return rc;
+}
+
+}  // namespace lsg
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace lsg;
+
+#define LSG_API_BEGIN \
+    try {
+#define LSG_API_END(ctxp)                                   \
+    }                                                       \
+    catch (const lsg::Error& e)                             \
+    {                                                       \
+        if (ctxp) (ctxp)->c.err = e.msg;                     \
+        return e.code;                                      \
+    }                                                       \
+    catch (const std::exception& e)                         \
+    {                                                       \
+        if (ctxp) (ctxp)->c.err = e.what();                  \
+        return LSG_ERR_ARG;                                 \
+    }
+
+extern "C" {
+
+void lsg_default_options(lsg_options* o)
+{
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->method = LSG_METHOD_FGMRES;
+    o->precond = LSG_PC_MG;
+    o->mg_precision = LSG_FP64;
+    o->smoother = LSG_SMOOTHER_ADLJ;
+    o->n_pre = 0;
+    o->n_post = 3;
+    o->max_levels = 0;
+    o->restart = 30;
+    o->max_it = 200;
+    o->zline_reference = 1;
+    o->eps = 1e-5;
+    o->omega = 0.805;
+}
+
+const char* lsg_version(void) { return "lsstag_b200 1.0 (sm_100a)"; }
+
+int lsg_create(int device, lsg_ctx** out)
+{
+    if (!out) return LSG_ERR_ARG;
+    *out = nullptr;
+    lsg_ctx* h = new (std::nothrow) lsg_ctx;
+    if (!h) return LSG_ERR_NOMEM;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    C.device = device;
+    LSG_CUDA(cudaSetDevice(device));
+    LSG_CUDA(cudaStreamCreateWithFlags(&C.s, cudaStreamNonBlocking));
+    LSG_CUDA(cudaEventCreate(&C.ev0));
+    LSG_CUDA(cudaEventCreate(&C.ev1));
+    C.red.init();
+    C.scal.alloc(64);
+    LSG_CUDA(cudaMemset(C.scal.p, 0, C.scal.bytes()));
+    C.ks.alloc(1);
+    LSG_CUDA(cudaHostAlloc((void**)&C.hflag, 64, cudaHostAllocMapped));
+    C.hnorm = (double*)((char*)C.hflag + 8);
+    lsg_default_options(&C.opt);
+    *out = h;
+    return LSG_OK;
+    }
+    catch (const lsg::Error& e)
+    {
+        fprintf(stderr, "lsg_create: %s\n", e.msg.c_str());
+        delete h;
+        return e.code;
+    }
+}
+
+int lsg_destroy(lsg_ctx* h)
+{
+    if (!h) return LSG_OK;
+    Context& C = h->c;
+    cudaSetDevice(C.device);
+    if (C.s) cudaStreamSynchronize(C.s);
+    if (C.hflag) cudaFreeHost(C.hflag);
+    if (C.ev0) cudaEventDestroy(C.ev0);
+    if (C.ev1) cudaEventDestroy(C.ev1);
+    cudaStream_t s = C.s;
+    delete h;   // DevBuf destructors free device memory
+    if (s) cudaStreamDestroy(s);
+    return LSG_OK;
+}
+
+const char* lsg_last_error(const lsg_ctx* h) { return h ? h->c.err.c_str() : "null context"; }
+
+static int set_matrix_impl(lsg_ctx* h, int N, int M, int K, const int* rowptr, const int* col, const double* val,
+                           long long nnz, bool host)
+{
+    Context& C = h->c;
+    LSG_REQUIRE(N >= 1 && M >= 1 && K >= 1, LSG_ERR_ARG, "grid dimensions must be positive");
+    LSG_REQUIRE(rowptr && col && val, LSG_ERR_ARG, "null CSR pointer");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const long long n = (long long)N * M * K;
+    LSG_REQUIRE(n < (1LL << 31), LSG_ERR_ARG, "grid too large for 32-bit CSR indices");
+    DevBuf<int> drp, dcol;
+    DevBuf<double> dval;
+    const int* prp = rowptr;
+    const int* pcol = col;
+    const double* pval = val;
+    if (host) {
+        nnz = rowptr[n];
+        LSG_REQUIRE(nnz >= 0, LSG_ERR_ARG, "negative nnz");
+        drp.alloc(n + 1);
+        dcol.alloc(nnz > 0 ? nnz : 1);
+        dval.alloc(nnz > 0 ? nnz : 1);
+        LSG_CUDA(cudaMemcpyAsync(drp.p, rowptr, (n + 1) * sizeof(int), cudaMemcpyHostToDevice, C.s));
+        LSG_CUDA(cudaMemcpyAsync(dcol.p, col, nnz * sizeof(int), cudaMemcpyHostToDevice, C.s));
+        LSG_CUDA(cudaMemcpyAsync(dval.p, val, nnz * sizeof(double), cudaMemcpyHostToDevice, C.s));
+        prp = drp.p;
+        pcol = dcol.p;
+        pval = dval.p;
+    }
+    C.d.N = N;
+    C.d.M = M;
+    C.d.K = K;
+    C.n = n;
+    C.A7.alloc(7 * n);
+    LSG_CUDA(cudaMemsetAsync(C.A7.p, 0, C.A7.bytes(), C.s));
+    int* err = (int*)(C.scal.p + 8);
+    LSG_CUDA(cudaMemsetAsync(err, 0, sizeof(int), C.s));
+    k_csr_to_stencil7<<<grid_for(n, 256), 256, 0, C.s>>>(N, M, K, prp, pcol, pval, C.A7.p, err);
+    LSG_CHECK_LAUNCH();
+    int e = 0;
+    LSG_CUDA(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    if (e != 0) {
+        C.have_matrix = false;
+        throw Error{LSG_ERR_PATTERN, "row " + std::to_string(e - 1) +
+                                         " holds an entry that is not the cell or one of its six face neighbours"};
+    }
+    C.have_matrix = true;
+    C.have_setup = false;
+    return LSG_OK;
+}
+
+int lsg_set_matrix_csr(lsg_ctx* h, int N, int M, int K, const int* rowptr, const int* col, const double* val)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    return set_matrix_impl(h, N, M, K, rowptr, col, val, -1, true);
+    LSG_API_END(h)
+}
+
+int lsg_set_matrix_csr_device(lsg_ctx* h, int N, int M, int K, const int* rowptr, const int* col,
+                              const double* val, long long nnz)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    return set_matrix_impl(h, N, M, K, rowptr, col, val, nnz, false);
+    LSG_API_END(h)
+}
+
+int lsg_set_matrix_stencil7(lsg_ctx* h, int N, int M, int K, const double* planes)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(N >= 1 && M >= 1 && K >= 1, LSG_ERR_ARG, "grid dimensions must be positive");
+    LSG_REQUIRE(planes, LSG_ERR_ARG, "null planes");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const long long n = (long long)N * M * K;
+    LSG_REQUIRE(n < (1LL << 31), LSG_ERR_ARG, "grid too large");
+    C.d.N = N;
+    C.d.M = M;
+    C.d.K = K;
+    C.n = n;
+    C.A7.alloc(7 * n);
+    LSG_CUDA(cudaMemcpyAsync(C.A7.p, planes, 7 * n * sizeof(double), cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    C.have_matrix = true;
+    C.have_setup = false;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_setup(lsg_ctx* h, const lsg_options* opts)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.have_matrix, LSG_ERR_STATE, "lsg_set_matrix_csr must be called before lsg_setup");
+    LSG_CUDA(cudaSetDevice(C.device));
+    if (opts) C.opt = *opts;
+    LSG_REQUIRE(C.opt.method == LSG_METHOD_FGMRES || C.opt.method == LSG_METHOD_BICGSTAB, LSG_ERR_ARG, "bad method");
+    LSG_REQUIRE(C.opt.precond >= 0 && C.opt.precond <= 2, LSG_ERR_ARG, "bad preconditioner");
+    LSG_REQUIRE(C.opt.restart >= 1 && C.opt.restart <= 64, LSG_ERR_ARG, "restart must be in [1, 64]");
+    LSG_REQUIRE(C.opt.max_it >= 1, LSG_ERR_ARG, "max_it must be >= 1");
+    LSG_REQUIRE(C.opt.n_post >= 0 && C.opt.n_post <= 16, LSG_ERR_ARG, "n_post must be in [0, 16]");
+    LSG_REQUIRE(C.opt.smoother == LSG_SMOOTHER_ADLJ, LSG_ERR_ARG, "smoother not supported");
+    C.have_setup = false;
+    if (C.opt.precond == LSG_PC_MG) mg_setup(C);
+    if (C.opt.precond == LSG_PC_ILU0) ilu_setup(C);
+    krylov_alloc(C);
+    C.have_setup = true;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_solve_device(lsg_ctx* h, const double* b, double* x, lsg_stats* st)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(b && x, LSG_ERR_ARG, "null vector");
+    LSG_CUDA(cudaSetDevice(C.device));
+    if (st) std::memset(st, 0, sizeof(*st));
+    return solve_device(C, b, x, st);
+    LSG_API_END(h)
+}
+
+int lsg_solve(lsg_ctx* h, const double* b, double* x, lsg_stats* st)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(b && x, LSG_ERR_ARG, "null vector");
+    LSG_REQUIRE(C.have_setup, LSG_ERR_STATE, "lsg_setup must be called before solving");
+    LSG_CUDA(cudaSetDevice(C.device));
+    if (st) std::memset(st, 0, sizeof(*st));
+    const size_t bytes = (size_t)C.n * sizeof(double);
+    LSG_CUDA(cudaMemcpyAsync(C.bd.p, b, bytes, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(C.xd.p, x, bytes, cudaMemcpyHostToDevice, C.s));
+    const int rc = solve_device(C, C.bd.p, C.xd.p, st);
+    LSG_CUDA(cudaMemcpyAsync(x, C.xd.p, bytes, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return rc;
+    LSG_API_END(h)
+}
+
+int lsg_apply(lsg_ctx* h, const double* x, double* y)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.have_matrix, LSG_ERR_STATE, "no operator set");
+    LSG_REQUIRE(x && y, LSG_ERR_ARG, "null vector");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const long long n = C.n;
+    DevBuf<double> dx, dy;
+    dx.alloc(n);
+    dy.alloc(n);
+    LSG_CUDA(cudaMemcpyAsync(dx.p, x, n * 8, cudaMemcpyHostToDevice, C.s));
+    k_apply7<double, 1><<<grid_for(n, 256), 256, 0, C.s>>>(C.d.N, C.d.M, C.d.K, C.A7.p, dx.p, dy.p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaMemcpyAsync(y, dy.p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_precond_apply(lsg_ctx* h, const double* b, double* x)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.have_setup, LSG_ERR_STATE, "lsg_setup must be called first");
+    LSG_REQUIRE(b && x, LSG_ERR_ARG, "null vector");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const long long n = C.n;
+    LSG_CUDA(cudaMemcpyAsync(C.bd.p, b, n * 8, cudaMemcpyHostToDevice, C.s));
+    precond_apply(C, C.bd.p, C.xd.p);
+    LSG_CUDA(cudaMemcpyAsync(x, C.xd.p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_mg_num_levels(const lsg_ctx* h)
+{
+    if (!h || !h->c.have_setup || h->c.opt.precond != LSG_PC_MG) return LSG_ERR_STATE;
+    return h->c.mg.L;
+}
+
+int lsg_mg_level_dims(const lsg_ctx* h, int level, int dims[3])
+{
+    if (!h || !dims) return LSG_ERR_ARG;
+    const Context& C = h->c;
+    if (!C.have_setup || C.opt.precond != LSG_PC_MG) return LSG_ERR_STATE;
+    if (level < 0 || level > C.mg.L) return LSG_ERR_ARG;
+    dims[0] = C.mg.dims[level].N;
+    dims[1] = C.mg.dims[level].M;
+    dims[2] = C.mg.dims[level].K;
+    return LSG_OK;
+}
+
+int lsg_mg_level_csr(lsg_ctx* h, int level, int* rowptr, int* col, double* val, long long* nnz)
+{
+    if (!h || !nnz) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.have_setup && C.opt.precond == LSG_PC_MG, LSG_ERR_STATE, "no multigrid hierarchy");
+    LSG_REQUIRE(level >= 0 && level <= C.mg.L, LSG_ERR_ARG, "bad level");
+    const LevelT<double>& lv = C.mg.l64[level];
+    const long long n = lv.d.n();
+    const int no = lv.ol.n;
+    std::vector<double> box((size_t)no * n);
+    LSG_CUDA(cudaMemcpyAsync(box.data(), lv.A, box.size() * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    const int N = lv.d.N, M = lv.d.M, K = lv.d.K, NM = N * M;
+    std::vector<std::pair<long long, double>> row;
+    long long cntnz = 0;
+    for (long long i = 0; i < n; i++) {
+        const int z = (int)(i / NM), y = (int)((i - (long long)z * NM) / N), x = (int)(i - (long long)z * NM - (long long)y * N);
+        row.clear();
+        for (int q = 0; q < no; q++) {
+            const int jx = x + lv.off[3 * q], jy = y + lv.off[3 * q + 1], jz = z + lv.off[3 * q + 2];
+            if (jx < 0 || jx >= N || jy < 0 || jy >= M || jz < 0 || jz >= K) continue;
+            const double v = box[(size_t)q * n + i];
+            if (level == 0 && v == 0.0 && !(lv.off[3 * q] == 0 && lv.off[3 * q + 1] == 0 && lv.off[3 * q + 2] == 0)) continue;
+            row.push_back({jx + (long long)jy * N + (long long)jz * NM, v});
+        }
+        std::sort(row.begin(), row.end());
+        if (rowptr) rowptr[i] = (int)cntnz;
+        if (col)
+            for (auto& e : row) {
+                col[cntnz] = (int)e.first;
+                val[cntnz] = e.second;
+                cntnz++;
+            }
+        else
+            cntnz += (long long)row.size();
+    }
+    if (rowptr) rowptr[n] = (int)cntnz;
+    *nnz = cntnz;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_mg_level_tridiag(lsg_ctx* h, int level, char dir, double* c, double* d, double* e)
+{
+    if (!h || !c || !d || !e) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.have_setup && C.opt.precond == LSG_PC_MG, LSG_ERR_STATE, "no multigrid hierarchy");
+    LSG_REQUIRE(level >= 0 && level < C.mg.L, LSG_ERR_ARG, "level has no smoother");
+    const int di = (dir == 'x') ? 0 : (dir == 'y') ? 1 : (dir == 'z') ? 2 : -1;
+    LSG_REQUIRE(di >= 0, LSG_ERR_ARG, "dir must be 'x', 'y' or 'z'");
+    const LevelT<double>& lv = C.mg.l64[level];
+    const long long n = lv.d.n();
+    std::vector<double> lo(n), dv(n), up(n);
+    LSG_CUDA(cudaMemcpyAsync(lo.data(), lv.lo[di].p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dv.data(), lv.dinv[di].p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaMemcpyAsync(up.data(), lv.up[di].p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    // map natural -> the direction's storage order (SmootherADLJy::initOrder,
+    // smoother_adlj_y.h:51-59; SmootherADLJz::initOrderZ, smoother_adlj_z.h:34-43)
+    const int N = lv.d.N, M = lv.d.M, K = lv.d.K;
+    long long pos = 0;
+    auto nat = [&](long long q) -> long long {
+        if (di == 0) return q;
+        if (di == 1) {   // q = z*N*M + x*M + y
+            const long long z = q / ((long long)N * M), r = q - z * N * M, x = r / M, y = r - x * M;
+            return x + N * (y + M * z);
+        }
+        const long long y = q / ((long long)N * K), r = q - y * N * K, x = r / K, z = r - x * K;   // q = y*N*K + x*K + z
+        return x + N * (y + M * z);
+    };
+    for (pos = 0; pos < n; pos++) {
+        const long long i = nat(pos);
+        d[pos] = dv[i];
+        if (pos + 1 < n) {
+            e[pos] = up[i];
+            c[pos] = lo[nat(pos + 1)];
+        }
+    }
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, double* bytes_per_launch)
+{
+    if (!h || !ms_per_launch || !bytes_per_launch || reps < 1) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.have_setup && C.opt.precond == LSG_PC_MG, LSG_ERR_STATE, "needs the multigrid setup");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const bool f32 = C.mg.fp32;
+    const double w = f32 ? 4.0 : 8.0;
+    const long long n = C.n;
+    auto launch = [&]() {
+        if (which >= 0 && which <= 2) {
+            if (f32) line_solve<float>(C.mg.l32[0], which, C.opt.zline_reference != 0, (float)C.opt.omega, C.s);
+            else line_solve<double>(C.mg.l64[0], which, C.opt.zline_reference != 0, C.opt.omega, C.s);
+        } else if (which == 3) {
+            if (f32) apply_resid<float>(C.mg.l32[0], C.mg.l32[0].c.p, C.mg.l32[0].r.p, C.s, 0);
+            else apply_resid<double>(C.mg.l64[0], C.mg.l64[0].c.p, C.mg.l64[0].r.p, C.s, 0);
+        } else if (which == 4) {
+            k_spmv_dot7<<<grid_for(n, 256, Reducer::kMaxBlocks), 256, 0, C.s>>>(
+                C.d.N, C.d.M, C.d.K, C.A7.p, C.Z.p, C.V.p, C.w.p, C.red.partial.p, C.red.counter.p, C.scal.p + 48);
+            LSG_CHECK_LAUNCH();
+        } else {
+            throw Error{LSG_ERR_ARG, "unknown kernel id"};
+        }
+    };
+    double bytes;
+    if (which <= 2) bytes = 7.0 * w * n;              // r, lo, dinv, up, ch read; c, ch written
+    else if (which == 3) bytes = 10.0 * w * n;        // 7 planes + c + r read/write
+    else bytes = 10.0 * 8.0 * n;                      // 7 planes + z + v0 read, w written
+    // defined inputs for the timed launches
+    if (f32) {
+        LSG_CUDA(cudaMemsetAsync(C.mg.l32[0].r.p, 0, n * 4, C.s));
+        LSG_CUDA(cudaMemsetAsync(C.mg.l32[0].c.p, 0, n * 4, C.s));
+        LSG_CUDA(cudaMemsetAsync(C.mg.l32[0].ch.p, 0, n * 4, C.s));
+    } else {
+        LSG_CUDA(cudaMemsetAsync(C.mg.l64[0].r.p, 0, n * 8, C.s));
+        LSG_CUDA(cudaMemsetAsync(C.mg.l64[0].c.p, 0, n * 8, C.s));
+        LSG_CUDA(cudaMemsetAsync(C.mg.l64[0].ch.p, 0, n * 8, C.s));
+    }
+    if (which == 4) {
+        LSG_CUDA(cudaMemsetAsync(C.Z.p, 0, n * 8, C.s));
+        LSG_CUDA(cudaMemsetAsync(C.V.p, 0, n * 8, C.s));
+    }
+    launch();
+    LSG_CUDA(cudaEventRecord(C.ev0, C.s));
+    for (int r = 0; r < reps; r++) launch();
+    LSG_CUDA(cudaEventRecord(C.ev1, C.s));
+    LSG_CUDA(cudaEventSynchronize(C.ev1));
+    float ms = 0;
+    LSG_CUDA(cudaEventElapsedTime(&ms, C.ev0, C.ev1));
+    *ms_per_launch = ms / reps;
+    *bytes_per_launch = bytes;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+}  // extern "C"

@@ -1,0 +1,139 @@
+"""ctypes binding of liblsstag_b200.so (the C ABI in include/lsstag_b200.h).
+
+The library is built in-tree (ls-stag-3d_parallel_b200/lib) by the package
+Makefile.  There is no fallback: importing this module without the built
+library, or calling it without a CUDA device, raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "liblsstag_b200.so")
+
+LSG_OK = 0
+LSG_NOT_CONVERGED = 1
+LSG_BREAKDOWN = 2
+LSG_ERR_ARG = -1
+LSG_ERR_CUDA = -2
+LSG_ERR_NOMEM = -3
+LSG_ERR_STATE = -4
+LSG_ERR_PATTERN = -5
+
+METHOD_FGMRES, METHOD_BICGSTAB = 0, 1
+PC_MG, PC_ILU0, PC_NONE = 0, 1, 2
+FP64, FP32 = 0, 1
+SMOOTHER_ADLJ, SMOOTHER_RBGS = 0, 1
+
+
+class Options(C.Structure):
+    _fields_ = [("method", C.c_int), ("precond", C.c_int), ("mg_precision", C.c_int), ("smoother", C.c_int),
+                ("n_pre", C.c_int), ("n_post", C.c_int), ("max_levels", C.c_int), ("restart", C.c_int),
+                ("max_it", C.c_int), ("zline_reference", C.c_int), ("eps", C.c_double), ("omega", C.c_double),
+                ("reserved", C.c_int * 8)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("norm_r", C.c_double),
+                ("true_residual", C.c_double), ("ms", C.c_double), ("bytes", C.c_double),
+                ("vcycles", C.c_int), ("pad", C.c_int), ("kernel_launches", C.c_longlong),
+                ("reserved", C.c_int * 4)]
+
+
+EXPORTS = [
+    "lsg_default_options", "lsg_create", "lsg_destroy", "lsg_last_error", "lsg_set_matrix_csr",
+    "lsg_set_matrix_csr_device", "lsg_set_matrix_stencil7", "lsg_setup", "lsg_solve", "lsg_solve_device", "lsg_apply",
+    "lsg_precond_apply", "lsg_mg_num_levels", "lsg_mg_level_dims", "lsg_mg_level_csr",
+    "lsg_mg_level_tridiag", "lsg_profile_kernel", "lsg_version",
+]
+
+_lib = None
+
+
+class LsgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"lsstag_b200 error {code}: {msg}")
+        self.code = code
+
+
+def load() -> C.CDLL:
+    """Load the shared library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.isfile(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} not built (run make in {PKG_ROOT})")
+    lib = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    ip = C.POINTER(C.c_int)
+    dp = C.POINTER(C.c_double)
+    lib.lsg_default_options.argtypes = [C.POINTER(Options)]
+    lib.lsg_default_options.restype = None
+    lib.lsg_create.argtypes = [C.c_int, C.POINTER(P)]
+    lib.lsg_destroy.argtypes = [P]
+    lib.lsg_last_error.argtypes = [P]
+    lib.lsg_last_error.restype = C.c_char_p
+    lib.lsg_set_matrix_csr.argtypes = [P, C.c_int, C.c_int, C.c_int, ip, ip, dp]
+    lib.lsg_set_matrix_csr_device.argtypes = [P, C.c_int, C.c_int, C.c_int, P, P, P, C.c_longlong]
+    lib.lsg_set_matrix_stencil7.argtypes = [P, C.c_int, C.c_int, C.c_int, dp]
+    lib.lsg_setup.argtypes = [P, C.POINTER(Options)]
+    lib.lsg_solve.argtypes = [P, dp, dp, C.POINTER(Stats)]
+    lib.lsg_solve_device.argtypes = [P, P, P, C.POINTER(Stats)]
+    lib.lsg_apply.argtypes = [P, dp, dp]
+    lib.lsg_precond_apply.argtypes = [P, dp, dp]
+    lib.lsg_mg_num_levels.argtypes = [P]
+    lib.lsg_mg_level_dims.argtypes = [P, C.c_int, ip]
+    lib.lsg_mg_level_csr.argtypes = [P, C.c_int, ip, ip, dp, C.POINTER(C.c_longlong)]
+    lib.lsg_mg_level_tridiag.argtypes = [P, C.c_int, C.c_char, dp, dp, dp]
+    lib.lsg_profile_kernel.argtypes = [P, C.c_int, C.c_int, dp, dp]
+    lib.lsg_version.restype = C.c_char_p
+    _lib = lib
+    return lib
+
+
+def default_options(**over) -> Options:
+    o = Options()
+    load().lsg_default_options(C.byref(o))
+    for k, v in over.items():
+        setattr(o, k, v)
+    return o
+
+
+def dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def iptr(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class Context:
+    """Owns one lsg_ctx (one device, one operator)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        self.h = C.c_void_p()
+        rc = self.lib.lsg_create(device, C.byref(self.h))
+        if rc != LSG_OK:
+            raise LsgError(rc, "lsg_create failed (no usable CUDA device?)")
+
+    def check(self, rc):
+        if rc < 0:
+            raise LsgError(rc, self.lib.lsg_last_error(self.h).decode())
+        return rc
+
+    def close(self):
+        if self.h:
+            self.lib.lsg_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

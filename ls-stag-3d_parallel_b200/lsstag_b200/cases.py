@@ -1,0 +1,62 @@
+"""The synthetic pressure-Poisson cases the solver is measured on.
+
+Standalone Poisson solve on the unit cube with four immersed spheres (radii
+U[0.05, 0.15], centres U[0.2, 0.8]^3, seeded, see synth.four_spheres) and
+homogeneous Neumann walls with the reference's two pinned rows.  Each case
+file holds the cut-cell Laplace operator that the reference's own
+LaplaceDiscreteOperator assembles for that geometry
+(laplace_discrete_operator.h:107-686, fixPoint :809-821), stored as seven
+coefficient planes (b, s, w, p, e, n, t) in a compressed .npz; the files are
+produced by cases/make_cases.py.  The right-hand side is generated here from
+the seed (synth.poisson_rhs).
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+from . import synth
+
+CASE_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "cases")
+
+
+def case_path(n: int, seed: int = 3) -> str:
+    return os.path.join(CASE_DIR, f"spheres4_seed{seed}_{n}.npz")
+
+
+def planes_to_csr(P: np.ndarray, dims):
+    """CSR (rowptr, col, val) with every in-grid neighbour of each row."""
+    N, M, K = dims
+    n = N * M * K
+    NM = N * M
+    i = np.arange(n)
+    x = i % N
+    y = (i // N) % M
+    z = i // NM
+    offs = [-NM, -N, -1, 0, 1, N, NM]
+    ok = [z > 0, y > 0, x > 0, np.ones(n, bool), x < N - 1, y < M - 1, z < K - 1]
+    cols = np.stack([np.where(ok[s], i + offs[s], -1) for s in range(7)], axis=1)
+    vals = P.T
+    mask = cols >= 0
+    rowptr = np.concatenate([[0], np.cumsum(mask.sum(axis=1))]).astype(np.int32)
+    return rowptr, cols[mask].astype(np.int32), vals[mask].astype(np.float64)
+
+
+def fluid_mask_from_planes(P: np.ndarray, dims, pins) -> np.ndarray:
+    rowptr, col, val = planes_to_csr(P, dims)
+    return synth.connected_fluid(rowptr, col, val, pins)
+
+
+def load(n: int, seed: int = 3):
+    """(planes (7, n^3), dims, pins, rhs) of the n^3 four-sphere case."""
+    with np.load(case_path(n, seed)) as f:
+        P = f["planes"].astype(np.float64)
+        dims = tuple(int(v) for v in f["dims"])
+        pins = f["pins"].astype(np.int64)
+        celltype = f["solid"]
+    mask = fluid_mask_from_planes(P, dims, pins)
+    # celltype stand-in: solid cells (0) vs the rest (1)
+    ct = np.where(celltype, 0, 1)
+    b = synth.poisson_rhs(seed, ct, pins, mask)
+    return P, dims, pins, b

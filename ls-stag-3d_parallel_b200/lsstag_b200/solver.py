@@ -1,0 +1,175 @@
+"""Python mirror of the reference's iterative-solver interface for the
+pressure-Poisson system, backed by the B200 C ABI.
+
+The reference drives its solvers through
+``IterativeSolverInterface{set(A, b, x, task); solve() -> it; norm_r;
+rebuildPreconditioner()}`` (Base/Solvers/iterative_solver_interface.h:31-73)
+with the concrete classes ``MGFGMRES`` (Base/Solvers/FGMRES/mg_fgmres.h) and
+``ILUBiCGStab`` (Base/Solvers/BiCGStab/ilu_bicgstab.h).  The classes below keep
+those names, argument meanings and results: ``set`` takes the operator in the
+reference's CSR form plus the task parameters (``eps`` absolute tolerance,
+``MAX_ITER``, ``FGMRES_RESTART_NUM``), ``solve`` updates ``x`` in place and
+returns the iteration count, and ``norm_r`` / ``it`` hold the final implicit
+residual and iteration count.  Errors raise instead of the reference's silent
+behaviour; a capped solve is reported through ``status``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+
+@dataclass
+class Task:
+    """The task fields the reference's solvers read (base_task_description.h:391-416)."""
+    eps: float = 1e-5
+    MAX_ITER: int = 200
+    FGMRES_RESTART_NUM: int = 30
+    n_post: int = 3
+
+
+class IterativeSolver:
+    """Common part of the solver classes (IterativeSolverInterface)."""
+
+    method = L.METHOD_FGMRES
+    precond = L.PC_MG
+
+    def __init__(self, device: int = 0, mg_precision: int = L.FP64, zline_reference: bool = True,
+                 max_levels: int = 0, omega: float = 0.805):
+        self.ctx = L.Context(device)
+        self.mg_precision = mg_precision
+        self.zline_reference = zline_reference
+        self.max_levels = max_levels
+        self.omega = omega
+        self.it = 1
+        self.norm_r = 0.0
+        self.eps = 1e-5
+        self.status = L.LSG_OK
+        self.stats = L.Stats()
+        self._b = None
+        self._x = None
+
+    # -- IterativeSolverInterface::set ------------------------------------
+    def set(self, A, b: np.ndarray | None = None, x: np.ndarray | None = None, task: Task | None = None):
+        """A = (rowptr, col, val, (N, M, K)) in the reference's CSR layout."""
+        rowptr, col, val, dims = A
+        task = task or Task()
+        self.task = task
+        self.eps = float(task.eps)
+        self._rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        self._col = np.ascontiguousarray(col, dtype=np.int32)
+        self._val = np.ascontiguousarray(val, dtype=np.float64)
+        self.dims = tuple(int(v) for v in dims)
+        N, M, K = self.dims
+        self.ctx.check(self.ctx.lib.lsg_set_matrix_csr(self.ctx.h, N, M, K, L.iptr(self._rowptr), L.iptr(self._col),
+                                                       L.dptr(self._val)))
+        self._setup()
+        self._b, self._x = b, x
+
+    def set_planes(self, planes: np.ndarray, dims, task: Task | None = None):
+        """Same as set() with the operator as seven coefficient planes
+        (b, s, w, p, e, n, t) of shape (7, N*M*K)."""
+        self.task = task or Task()
+        self.eps = float(self.task.eps)
+        self._planes = np.ascontiguousarray(planes, dtype=np.float64)
+        self.dims = tuple(int(v) for v in dims)
+        N, M, K = self.dims
+        self.ctx.check(self.ctx.lib.lsg_set_matrix_stencil7(self.ctx.h, N, M, K, L.dptr(self._planes)))
+        self._setup()
+
+    def options(self) -> L.Options:
+        return L.default_options(method=self.method, precond=self.precond, mg_precision=self.mg_precision,
+                                 restart=int(self.task.FGMRES_RESTART_NUM), max_it=int(self.task.MAX_ITER),
+                                 n_post=int(self.task.n_post), eps=float(self.eps),
+                                 zline_reference=int(self.zline_reference), max_levels=int(self.max_levels),
+                                 omega=float(self.omega))
+
+    def _setup(self):
+        o = self.options()
+        self.ctx.check(self.ctx.lib.lsg_setup(self.ctx.h, L.C.byref(o)))
+
+    # -- IterativeSolverInterface::rebuildPreconditioner -------------------
+    def rebuildPreconditioner(self):
+        self._setup()
+
+    # -- IterativeSolverInterface::solve -----------------------------------
+    def solve(self, b: np.ndarray | None = None, x: np.ndarray | None = None) -> int:
+        b = self._b if b is None else b
+        x = self._x if x is None else x
+        if b is None or x is None:
+            raise ValueError("solve needs b and x (given here or to set)")
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        if not (x.dtype == np.float64 and x.flags.c_contiguous):
+            raise ValueError("x must be a C-contiguous float64 array (updated in place)")
+        if self.eps != self.task.eps:
+            self._setup()
+        rc = self.ctx.check(self.ctx.lib.lsg_solve(self.ctx.h, L.dptr(bb), L.dptr(x), L.C.byref(self.stats)))
+        self.status = rc
+        self.it = self.stats.iterations
+        self.norm_r = self.stats.norm_r
+        return self.it
+
+    # -- helpers used by the parity tests -----------------------------------
+    def apply(self, x: np.ndarray) -> np.ndarray:
+        y = np.empty_like(x, dtype=np.float64)
+        self.ctx.check(self.ctx.lib.lsg_apply(self.ctx.h, L.dptr(np.ascontiguousarray(x, dtype=np.float64)),
+                                              L.dptr(y)))
+        return y
+
+    def precondition(self, b: np.ndarray) -> np.ndarray:
+        x = np.empty(b.size, dtype=np.float64)
+        self.ctx.check(self.ctx.lib.lsg_precond_apply(self.ctx.h, L.dptr(np.ascontiguousarray(b, dtype=np.float64)),
+                                                      L.dptr(x)))
+        return x
+
+    def num_levels(self) -> int:
+        return self.ctx.check(self.ctx.lib.lsg_mg_num_levels(self.ctx.h))
+
+    def level_dims(self, level: int):
+        d = np.zeros(3, dtype=np.int32)
+        self.ctx.check(self.ctx.lib.lsg_mg_level_dims(self.ctx.h, level, L.iptr(d)))
+        return tuple(int(v) for v in d)
+
+    def level_csr(self, level: int):
+        nnz = L.C.c_longlong(0)
+        self.ctx.check(self.ctx.lib.lsg_mg_level_csr(self.ctx.h, level, None, None, None, L.C.byref(nnz)))
+        n = int(np.prod(self.level_dims(level)))
+        rp = np.zeros(n + 1, dtype=np.int32)
+        col = np.zeros(max(1, nnz.value), dtype=np.int32)
+        val = np.zeros(max(1, nnz.value), dtype=np.float64)
+        self.ctx.check(self.ctx.lib.lsg_mg_level_csr(self.ctx.h, level, L.iptr(rp), L.iptr(col), L.dptr(val),
+                                                     L.C.byref(nnz)))
+        return rp, col[: nnz.value], val[: nnz.value]
+
+    def level_tridiag(self, level: int, direction: str):
+        n = int(np.prod(self.level_dims(level)))
+        c = np.zeros(max(1, n - 1))
+        d = np.zeros(n)
+        e = np.zeros(max(1, n - 1))
+        self.ctx.check(self.ctx.lib.lsg_mg_level_tridiag(self.ctx.h, level, direction.encode(), L.dptr(c), L.dptr(d),
+                                                         L.dptr(e)))
+        return c[: n - 1], d, e[: n - 1]
+
+    def close(self):
+        self.ctx.close()
+
+
+class MGFGMRES(IterativeSolver):
+    """FGMRES with the multigrid preconditioner (mg_fgmres.h:33-52)."""
+    method = L.METHOD_FGMRES
+    precond = L.PC_MG
+
+
+class ILUBiCGStab(IterativeSolver):
+    """BiCGStab with the ILU(0) preconditioner (ilu_bicgstab.h:33-64)."""
+    method = L.METHOD_BICGSTAB
+    precond = L.PC_ILU0
+
+
+class ILUFGMRES(IterativeSolver):
+    """FGMRES with the ILU(0) preconditioner (ilu_fgmres.h:33-64)."""
+    method = L.METHOD_FGMRES
+    precond = L.PC_ILU0

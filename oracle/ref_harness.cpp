@@ -236,6 +236,85 @@ void dumpHierarchy(Dumper& out, MultiGridSolver& mg)
     }
 }
 
+/* Reference solvers on an operator given as seven coefficient planes
+   (b, s, w, p, e, n, t of the reference's CSR order; raw f8 file of 7*n
+   values) and a right-hand side: the CPU-baseline mode.  The CSR holds every
+   in-grid neighbour (explicit zeros included), like the reference's portrait
+   for fluid rows (sym_discrete_operator.h). */
+int solvePlanes(const Config& cfg, const std::string& outdir)
+{
+    const int N = (int)cfg.get("N", 0), M = (int)cfg.get("M", 0), K = (int)cfg.get("K", 0);
+    const long n = (long)N * M * K;
+    std::vector<double> planes(7 * n), b(n);
+    {
+        std::ifstream f(cfg.gets("planes_in", ""), std::ios::binary);
+        f.read((char*)planes.data(), sizeof(double) * 7 * n);
+        std::ifstream g(cfg.gets("rhs", ""), std::ios::binary);
+        g.read((char*)b.data(), sizeof(double) * n);
+        if (!f || !g) { fprintf(stderr, "cannot read planes/rhs\n"); return 3; }
+    }
+    const int NM = N * M;
+    const int offs[7] = {-NM, -N, -1, 0, 1, N, NM};
+    SparseMatrix* A = new SparseMatrix;
+    A->set(N, M, K, (int)n);
+    std::vector<int> cols;
+    std::vector<double> vals;
+    cols.reserve(7 * n);
+    vals.reserve(7 * n);
+    A->Number[0] = 0;
+    for (long i = 0; i < n; i++) {
+        const int z = (int)(i / NM), y = (int)((i - (long)z * NM) / N), x = (int)(i - (long)z * NM - (long)y * N);
+        const bool ok[7] = {z > 0, y > 0, x > 0, true, x < N - 1, y < M - 1, z < K - 1};
+        for (int s = 0; s < 7; s++)
+            if (ok[s]) { cols.push_back((int)(i + offs[s])); vals.push_back(planes[(size_t)s * n + i]); }
+        A->Number[i + 1] = (int)cols.size();
+    }
+    A->resize();
+    A->maxElemCount = A->elemCount;
+    A->reserve();
+    std::copy(cols.begin(), cols.end(), A->Portrait);
+    std::copy(vals.begin(), vals.end(), A->Cell);
+    HarnessTask* task = new HarnessTask;
+    task->FGMRES_RESTART_NUM = (int)cfg.get("restart", 30);
+    task->MAX_ITER = (int)cfg.get("max_it", 200);
+    task->n_post = (int)cfg.get("n_post", BaseTaskDescription::DEFAULT_N_POST);
+    double bnorm = 0.0;
+    for (long i = 0; i < n; i++) bnorm += b[i] * b[i];
+    bnorm = sqrt(bnorm);
+    task->eps = cfg.get("abs_tol", cfg.get("rel_tol", 1e-10) * bnorm);
+    Dumper out(outdir);
+    out.scalar("eps", task->eps);
+    const int reps = (int)cfg.get("repeats", 1);
+    std::vector<double> x(n, 0.0);
+    const char* names[2] = {"fgmres", "bicgstab"};
+    for (int which = 0; which < 2; which++) {
+        if (!(int)cfg.get(names[which], which == 0 ? 1 : 0)) continue;
+        IterativeSolverInterface* s = which == 0 ? (IterativeSolverInterface*)new MGFGMRES
+                                                 : (IterativeSolverInterface*)new ILUBiCGStab;
+        double tset = now_s();
+        s->set(A, b.data(), x.data(), task);
+        tset = now_s() - tset;
+        s->eps = task->eps;
+        std::vector<double> ts;
+        int iters = 0;
+        for (int r = 0; r < reps; r++) {
+            std::fill(x.begin(), x.end(), 0.0);
+            double t1 = now_s();
+            iters = s->solve();
+            ts.push_back(now_s() - t1);
+        }
+        std::string p = names[which];
+        out.d(p + "_x", x.data(), n);
+        out.i(p + "_it", &iters, 1);
+        out.scalar(p + "_norm_r", s->norm_r);
+        out.d(p + "_time_s", ts.data(), (long)ts.size());
+        out.scalar(p + "_setup_s", tset);
+    }
+    int nthreads = omp_get_max_threads();
+    out.i("omp_threads", &nthreads, 1);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv)
@@ -248,6 +327,7 @@ int main(int argc, char** argv)
     const std::string outdir = argv[2];
     const int threads = (int)cfg.get("threads", 0);
     if (threads > 0) omp_set_num_threads(threads);
+    if (!cfg.gets("planes_in", "").empty()) return solvePlanes(cfg, outdir);
 
     HarnessTask* task = new HarnessTask;
     task->gN = (int)cfg.get("N", 16);

@@ -91,3 +91,48 @@ def csr(res: dict, name: str):
     dims = res[name + "_dims"]
     return (res[name + "_rowptr"], res[name + "_col"], res[name + "_val"],
             (int(dims[0]), int(dims[1]), int(dims[2])))
+
+
+def run_planes(planes: np.ndarray, dims, rhs: np.ndarray, *, threads: int = 0, timeout: float = 3600,
+               **opts) -> dict:
+    """Reference MG-FGMRES / ILU-BiCGStab (opts fgmres=1, bicgstab=0/1) on an
+    operator given as seven coefficient planes (b, s, w, p, e, n, t)."""
+    if not available():
+        raise FileNotFoundError(REF_BIN)
+    import shutil
+    d = tempfile.mkdtemp(prefix="lsg_refp_")
+    try:
+        pp = os.path.join(d, "planes.in")
+        bp = os.path.join(d, "rhs.in")
+        np.ascontiguousarray(planes, dtype=np.float64).tofile(pp)
+        np.ascontiguousarray(rhs, dtype=np.float64).tofile(bp)
+        N, M, K = dims
+        lines = [f"N {N}", f"M {M}", f"K {K}", f"planes_in {pp}", f"rhs {bp}"]
+        if threads:
+            lines.append(f"threads {threads}")
+        for k, v in opts.items():
+            lines.append(f"{k} {v!r}" if isinstance(v, float) else f"{k} {v}")
+        cfg = os.path.join(d, "case.cfg")
+        with open(cfg, "w") as f:
+            f.write("\n".join(lines) + "\n")
+        subprocess.run([REF_BIN, cfg, d], check=True, timeout=timeout, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.PIPE)
+        return load_dir(d)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def csr_to_planes(rowptr, col, val, dims) -> np.ndarray:
+    """Seven coefficient planes (b, s, w, p, e, n, t) of a 7-point CSR."""
+    N, M, K = dims
+    n = N * M * K
+    NM = N * M
+    rows = np.repeat(np.arange(n), np.diff(rowptr))
+    dlt = col.astype(np.int64) - rows
+    slot = np.select([dlt == -NM, dlt == -N, dlt == -1, dlt == 0, dlt == 1, dlt == N, dlt == NM],
+                     [0, 1, 2, 3, 4, 5, 6], -1)
+    if np.any(slot < 0):
+        raise ValueError("not a 7-point operator")
+    P = np.zeros((7, n))
+    np.add.at(P, (slot, rows), val)
+    return P
