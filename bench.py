@@ -232,8 +232,10 @@ def main():
         sampler = ClockSampler(local) if name == "fp32" else None
         if sampler:
             sampler.__enter__()
+        torch.cuda.nvtx.range_push(f"lsg_{name}_timed")   # ncu --nvtx-include lsg_fp32_timed/
         recs = [one() for _ in range(args.steps)]
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         if sampler:
             sampler.__exit__()
         barrier(pg)
@@ -246,9 +248,10 @@ def main():
             # dominant-kernel roofline (finest-level smoother/residual kernels)
             prof = {}
             nv = recs[-1][1]
-            per_solve = {0: 3 * nv, 1: 3 * nv, 2: 3 * nv, 3: 9 * nv}
-            names = {0: "adlj_xline_fp32", 1: "adlj_yline_fp32", 2: "adlj_zline_fp32", 3: "residual7_fp32"}
-            for k in (0, 1, 2, 3):
+            per_solve = {0: 3 * nv, 1: 3 * nv, 2: 3 * nv, 3: 9 * nv, 5: 9 * nv}
+            names = {0: "adlj_xline_fp32", 1: "adlj_yline_fp32", 2: "adlj_zline_fp32", 3: "residual7_fp32",
+                     5: "residual27_level1_fp32"}
+            for k in (0, 1, 2, 3, 5):
                 msk = L.C.c_double(0)
                 byk = L.C.c_double(0)
                 s.ctx.check(s.ctx.lib.lsg_profile_kernel(s.ctx.h, k, 20, L.C.byref(msk), L.C.byref(byk)))

@@ -157,7 +157,8 @@ int lsg_mg_level_tridiag(lsg_ctx* ctx, int level, char dir, double* c, double* d
 /* Time one kernel of the solve path on the context's stream with CUDA
    events (after a warm-up launch): `which` = 0/1/2 the finest-level x/y/z
    line solve of the multigrid smoother, 3 the finest-level residual update
-   r -= A c, 4 the FP64 operator apply fused with a dot product (Krylov).
+   r -= A c, 4 the FP64 operator apply fused with a dot product (Krylov),
+   5 the residual update of the first coarse level (Galerkin stencil).
    Returns the mean duration of one launch and the algorithmic HBM bytes one
    launch moves (compulsory traffic of its inputs and outputs).  Needs
    lsg_setup with the multigrid preconditioner. */

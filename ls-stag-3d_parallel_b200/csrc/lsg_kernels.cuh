@@ -188,6 +188,232 @@ __global__ void __launch_bounds__(256) k_applybox(int N, int M, int K, OffList o
     }
 }
 
+// 27-point box stencil (radius 1 in every dimension, the Galerkin operator of
+// the even-even-even and odd-odd-odd coarsenings): offsets unrolled, plane
+// q = ((dz+1)*3 + (dy+1))*3 + (dx+1).
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_apply27(int N, int M, int K, const T* __restrict__ coef,
+                                                  const T* __restrict__ x, T* __restrict__ r)
+{
+    const long long n = (long long)N * M * K;
+    const int NM = N * M;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int ix, iy, iz;
+        cell_xyz(i, N, NM, ix, iy, iz);
+        T acc = 0;
+        const bool interior = ix > 0 && ix < N - 1 && iy > 0 && iy < M - 1 && iz > 0 && iz < K - 1;
+        if (interior) {
+#pragma unroll
+            for (int dz = -1; dz <= 1; dz++)
+#pragma unroll
+                for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+                    for (int dx = -1; dx <= 1; dx++) {
+                        const int q = ((dz + 1) * 3 + (dy + 1)) * 3 + (dx + 1);
+                        acc += coef[(size_t)q * n + i] * x[i + dx + (long long)dy * N + (long long)dz * NM];
+                    }
+        } else {
+#pragma unroll
+            for (int dz = -1; dz <= 1; dz++)
+#pragma unroll
+                for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+                    for (int dx = -1; dx <= 1; dx++) {
+                        const int jx = ix + dx, jy = iy + dy, jz = iz + dz;
+                        if (jx < 0 || jx >= N || jy < 0 || jy >= M || jz < 0 || jz >= K) continue;
+                        const int q = ((dz + 1) * 3 + (dy + 1)) * 3 + (dx + 1);
+                        acc += coef[(size_t)q * n + i] * x[i + dx + (long long)dy * N + (long long)dz * NM];
+                    }
+        }
+        if (MODE == 0) r[i] -= acc;
+        else r[i] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// row-dictionary operators: cls[i] indexes a table of the distinct
+// coefficient rows (row-major, NOFF values per row).  Bit-identical rows share
+// one entry, so a level whose rows are mostly uniform streams 4 bytes of
+// operator per cell instead of NOFF coefficients; the table stays in L1/L2.
+// ---------------------------------------------------------------------------
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_apply7d(int N, int M, int K, const int* __restrict__ cls,
+                                                  const T* __restrict__ dict, const T* __restrict__ x,
+                                                  T* __restrict__ r)
+{
+    const long long n = (long long)N * M * K;
+    const int NM = N * M;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int ix, iy, iz;
+        cell_xyz(i, N, NM, ix, iy, iz);
+        const T* a = dict + (size_t)cls[i] * 7;
+        T acc = a[3] * x[i];
+        if (iz > 0) acc += a[0] * x[i - NM];
+        if (iy > 0) acc += a[1] * x[i - N];
+        if (ix > 0) acc += a[2] * x[i - 1];
+        if (ix < N - 1) acc += a[4] * x[i + 1];
+        if (iy < M - 1) acc += a[5] * x[i + N];
+        if (iz < K - 1) acc += a[6] * x[i + NM];
+        if (MODE == 0) r[i] -= acc;
+        else r[i] = acc;
+    }
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_apply27d(int N, int M, int K, const int* __restrict__ cls,
+                                                   const T* __restrict__ dict, const T* __restrict__ x,
+                                                   T* __restrict__ r)
+{
+    const long long n = (long long)N * M * K;
+    const int NM = N * M;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int ix, iy, iz;
+        cell_xyz(i, N, NM, ix, iy, iz);
+        const T* a = dict + (size_t)cls[i] * 27;
+        T acc = 0;
+        const bool interior = ix > 0 && ix < N - 1 && iy > 0 && iy < M - 1 && iz > 0 && iz < K - 1;
+        if (interior) {
+#pragma unroll
+            for (int dz = -1; dz <= 1; dz++)
+#pragma unroll
+                for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+                    for (int dx = -1; dx <= 1; dx++) {
+                        const int q = ((dz + 1) * 3 + (dy + 1)) * 3 + (dx + 1);
+                        acc += a[q] * x[i + dx + (long long)dy * N + (long long)dz * NM];
+                    }
+        } else {
+#pragma unroll
+            for (int dz = -1; dz <= 1; dz++)
+#pragma unroll
+                for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+                    for (int dx = -1; dx <= 1; dx++) {
+                        const int jx = ix + dx, jy = iy + dy, jz = iz + dz;
+                        if (jx < 0 || jx >= N || jy < 0 || jy >= M || jz < 0 || jz >= K) continue;
+                        const int q = ((dz + 1) * 3 + (dy + 1)) * 3 + (dx + 1);
+                        acc += a[q] * x[i + dx + (long long)dy * N + (long long)dz * NM];
+                    }
+        }
+        if (MODE == 0) r[i] -= acc;
+        else r[i] = acc;
+    }
+}
+
+// z-marching variants: a 32 x 8 thread tile covers (x, y); each thread walks a
+// chunk of ZC planes, keeping the z-neighbours of its column in registers.
+// No integer division; rows of the same class hit the same L1 lines.
+constexpr int kZChunk = 16;
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_apply7z(int N, int M, int K, const int* __restrict__ cls,
+                                                  const T* __restrict__ dict, const T* __restrict__ x,
+                                                  T* __restrict__ r)
+{
+    const int ix = blockIdx.x * 32 + threadIdx.x;
+    const int iy = blockIdx.y * 8 + threadIdx.y;
+    if (ix >= N || iy >= M) return;
+    const long long NM = (long long)N * M;
+    const int z0 = blockIdx.z * kZChunk;
+    const int z1 = min(z0 + kZChunk, K);
+    long long i = ix + (long long)N * iy + NM * z0;
+    T xm = (z0 > 0) ? x[i - NM] : (T)0;
+    T xc = x[i];
+    const bool hasw = ix > 0, hase = ix < N - 1, hass = iy > 0, hasn = iy < M - 1;
+    for (int z = z0; z < z1; z++, i += NM) {
+        const T xp = (z < K - 1) ? x[i + NM] : (T)0;
+        const T* a = dict + (size_t)cls[i] * 7;
+        T acc = a[3] * xc;
+        acc += a[0] * xm;          // zero coefficient below the bottom wall
+        if (hass) acc += a[1] * x[i - N];
+        if (hasw) acc += a[2] * x[i - 1];
+        if (hase) acc += a[4] * x[i + 1];
+        if (hasn) acc += a[5] * x[i + N];
+        acc += a[6] * xp;
+        if (MODE == 0) r[i] -= acc;
+        else r[i] = acc;
+        xm = xc;
+        xc = xp;
+    }
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_apply27z(int N, int M, int K, const int* __restrict__ cls,
+                                                   const T* __restrict__ dict, const T* __restrict__ x,
+                                                   T* __restrict__ r)
+{
+    const int ix = blockIdx.x * 32 + threadIdx.x;
+    const int iy = blockIdx.y * 8 + threadIdx.y;
+    if (ix >= N || iy >= M) return;
+    const long long NM = (long long)N * M;
+    const int z0 = blockIdx.z * kZChunk;
+    const int z1 = min(z0 + kZChunk, K);
+    const long long col = ix + (long long)N * iy;
+    bool ok[9];
+    int off[9];
+#pragma unroll
+    for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+        for (int dx = -1; dx <= 1; dx++) {
+            const int q = (dy + 1) * 3 + (dx + 1);
+            ok[q] = (ix + dx >= 0) && (ix + dx < N) && (iy + dy >= 0) && (iy + dy < M);
+            off[q] = dx + dy * N;
+        }
+    // plane values of the 3x3 column neighbourhood at z-1, z, z+1
+    T pm[9], pc[9], pp[9];
+    auto load_plane = [&](int z, T* p) {
+#pragma unroll
+        for (int q = 0; q < 9; q++) p[q] = (z >= 0 && z < K && ok[q]) ? x[col + NM * z + off[q]] : (T)0;
+    };
+    load_plane(z0 - 1, pm);
+    load_plane(z0, pc);
+    for (int z = z0; z < z1; z++) {
+        load_plane(z + 1, pp);
+        const long long i = col + NM * z;
+        const T* a = dict + (size_t)cls[i] * 27;
+        T acc = 0;
+#pragma unroll
+        for (int q = 0; q < 9; q++) acc += a[q] * pm[q];
+#pragma unroll
+        for (int q = 0; q < 9; q++) acc += a[9 + q] * pc[q];
+#pragma unroll
+        for (int q = 0; q < 9; q++) acc += a[18 + q] * pp[q];
+        if (MODE == 0) r[i] -= acc;
+        else r[i] = acc;
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            pm[q] = pc[q];
+            pc[q] = pp[q];
+        }
+    }
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_applyboxd(int N, int M, int K, OffList ol, const int* __restrict__ cls,
+                                                    const T* __restrict__ dict, const T* __restrict__ x,
+                                                    T* __restrict__ r)
+{
+    const long long n = (long long)N * M * K;
+    const int NM = N * M;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int ix, iy, iz;
+        cell_xyz(i, N, NM, ix, iy, iz);
+        const T* a = dict + (size_t)cls[i] * ol.n;
+        T acc = 0;
+        for (int o = 0; o < ol.n; o++) {
+            const int jx = ix + ol.o[o][0], jy = iy + ol.o[o][1], jz = iz + ol.o[o][2];
+            if (jx < 0 || jx >= N || jy < 0 || jy >= M || jz < 0 || jz >= K) continue;
+            acc += a[o] * x[i + ol.o[o][0] + (long long)ol.o[o][1] * N + (long long)ol.o[o][2] * NM];
+        }
+        if (MODE == 0) r[i] -= acc;
+        else r[i] = acc;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // transfers (structured tensor-product operators, one 1-D table per axis)
 // ---------------------------------------------------------------------------
@@ -527,45 +753,78 @@ __global__ void k_line_coupling(LineGeom g, const double* __restrict__ lo, const
 // (coalesced).  The forward sweep stores into c, the backward sweep finishes
 // it in place.  quirk_first >= 0: natural index base of the z-line first
 // right-hand side as the reference reads it (y*N*K + x), see header.
+// The sweeps run in chunks of U cells: all loads of a chunk are issued before
+// its dependent recurrence, so each thread keeps 3U loads in flight (the
+// recurrence itself is latency bound, one FMA chain per line).
 template <typename T>
 __global__ void __launch_bounds__(128) k_tdma_strided(LineGeom g, bool zquirk, const T* __restrict__ lo,
                                                        const T* __restrict__ dinv, const T* __restrict__ up,
                                                        const T* __restrict__ r, T* __restrict__ c,
                                                        T* __restrict__ ch, T omega)
 {
+    constexpr int U = 8;
     const long long nl = g.nlines();
     const int L = g.len();
     const long long st = line_stride(g);
     for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < nl;
          l += (long long)gridDim.x * blockDim.x) {
         const long long i0 = line_start(g, l);
-        long long i = i0;
         T rhs0;
         if (zquirk) {
             // line l = x + N*y; the reference reads right_member[y*N*K + x]
             const long long y = l / g.N, x = l - y * g.N;
             rhs0 = r[y * (long long)g.N * g.K + x];
         } else {
-            rhs0 = r[i];
+            rhs0 = r[i0];
         }
-        T yv = rhs0 * dinv[i];
-        c[i] = yv;
-        for (int t = 1; t < L; t++) {
-            i += st;
-            yv = (r[i] - lo[i] * yv) * dinv[i];
-            c[i] = yv;
+        // forward: y_t = (r_t - lo_t y_{t-1}) * dinv_t, stored in c
+        T yv = 0;
+        for (int t0 = 0; t0 < L; t0 += U) {
+            T rr[U], ll[U], dd[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int t = t0 + u;
+                if (t < L) {
+                    const long long i = i0 + (long long)t * st;
+                    rr[u] = (t == 0) ? rhs0 : r[i];
+                    ll[u] = lo[i];
+                    dd[u] = dinv[i];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int t = t0 + u;
+                if (t < L) {
+                    yv = (t == 0) ? rr[u] * dd[u] : (rr[u] - ll[u] * yv) * dd[u];
+                    c[i0 + (long long)t * st] = yv;
+                }
+            }
         }
-        // backward: x_t = y_t - up_t x_{t+1}
-        T xv = yv;
-        T cv = omega * xv;
-        c[i] = cv;
-        ch[i] += cv;
-        for (int t = L - 2; t >= 0; t--) {
-            i -= st;
-            xv = c[i] - up[i] * xv;
-            cv = omega * xv;
-            c[i] = cv;
-            ch[i] += cv;
+        // backward: x_t = y_t - up_t x_{t+1};  c = omega x ; ch += c
+        T xv = 0;
+        for (int t1 = L - 1; t1 >= 0; t1 -= U) {
+            T yy[U], uu[U], hh[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int t = t1 - u;
+                if (t >= 0) {
+                    const long long i = i0 + (long long)t * st;
+                    yy[u] = c[i];
+                    uu[u] = up[i];
+                    hh[u] = ch[i];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int t = t1 - u;
+                if (t >= 0) {
+                    xv = (t == L - 1) ? yy[u] : yy[u] - uu[u] * xv;
+                    const T cv = omega * xv;
+                    const long long i = i0 + (long long)t * st;
+                    c[i] = cv;
+                    ch[i] = hh[u] + cv;
+                }
+            }
         }
     }
 }
@@ -587,14 +846,26 @@ __global__ void __launch_bounds__(256) k_tdma_xwarp(int N, long long nlines, con
     for (long long l = warp; l < nlines; l += nwarps) {
         const long long base = l * N;
         T carry = 0;
+        // forward, with the next round's loads issued before this round's scan
+        T nr = 0, nd = 1, nl = 0;
+        if (lane < N) {
+            nr = r[base + lane];
+            nd = dinv[base + lane];
+            nl = lo[base + lane];
+        }
         for (int rd = 0; rd < rounds; rd++) {
             const int t = rd * 32 + lane;
+            const T rv = nr, D = nd, lv = nl;
+            const int tn = t + 32;
+            if (tn < N) {
+                nr = r[base + tn];
+                nd = dinv[base + tn];
+                nl = lo[base + tn];
+            }
             T a = 0, b = 1;
             if (t < N) {
-                const long long i = base + t;
-                const T D = dinv[i];
-                a = r[i] * D;
-                b = (t == 0) ? (T)0 : -lo[i] * D;
+                a = rv * D;
+                b = (t == 0) ? (T)0 : -lv * D;
             }
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -611,13 +882,28 @@ __global__ void __launch_bounds__(256) k_tdma_xwarp(int N, long long nlines, con
         }
         __syncwarp();
         carry = 0;
+        T ny = 0, nu = 0, nh = 0;
+        {
+            const int t = N - 1 - lane;
+            if (t >= 0) {
+                ny = c[base + t];
+                nu = up[base + t];
+                nh = ch[base + t];
+            }
+        }
         for (int rd = 0; rd < rounds; rd++) {
             const int t = N - 1 - (rd * 32 + lane);
+            const T yv = ny, uv = nu, hv = nh;
+            const int tn = t - 32;
+            if (tn >= 0) {
+                ny = c[base + tn];
+                nu = up[base + tn];
+                nh = ch[base + tn];
+            }
             T a = 0, b = 1;
             if (t >= 0) {
-                const long long i = base + t;
-                a = c[i];
-                b = (t == N - 1) ? (T)0 : -up[i];
+                a = yv;
+                b = (t == N - 1) ? (T)0 : -uv;
             }
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -631,10 +917,9 @@ __global__ void __launch_bounds__(256) k_tdma_xwarp(int N, long long nlines, con
             const T xv = a + b * carry;
             carry = __shfl_sync(0xffffffffu, xv, 31);
             if (t >= 0) {
-                const long long i = base + t;
                 const T cv = omega * xv;
-                c[i] = cv;
-                ch[i] += cv;
+                c[base + t] = cv;
+                ch[base + t] = hv + cv;
             }
         }
     }

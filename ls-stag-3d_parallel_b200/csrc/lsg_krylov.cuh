@@ -12,7 +12,7 @@ namespace lsg {
 
 // w = b - A x  and  out[0] = ||w||^2   (setProductWithResidual,
 // real_valued_mesh_function.h:203-211, 245-256)
-__global__ void __launch_bounds__(256) k_residual7(int N, int M, int K, const double* __restrict__ coef,
+__global__ void __launch_bounds__(256) k_residual7(int N, int M, int K, const int* __restrict__ cls, const double* __restrict__ dict,
                                                     const double* __restrict__ x, const double* __restrict__ b,
                                                     double* __restrict__ w, double* partial,
                                                     unsigned int* counter, double* out)
@@ -24,13 +24,14 @@ __global__ void __launch_bounds__(256) k_residual7(int N, int M, int K, const do
          i += (long long)gridDim.x * blockDim.x) {
         int ix, iy, iz;
         cell_xyz(i, N, NM, ix, iy, iz);
-        double acc = coef[3 * n + i] * x[i];
-        if (iz > 0) acc += coef[i] * x[i - NM];
-        if (iy > 0) acc += coef[n + i] * x[i - N];
-        if (ix > 0) acc += coef[2 * n + i] * x[i - 1];
-        if (ix < N - 1) acc += coef[4 * n + i] * x[i + 1];
-        if (iy < M - 1) acc += coef[5 * n + i] * x[i + N];
-        if (iz < K - 1) acc += coef[6 * n + i] * x[i + NM];
+        const double* a = dict + (size_t)cls[i] * 7;
+        double acc = a[3] * x[i];
+        if (iz > 0) acc += a[0] * x[i - NM];
+        if (iy > 0) acc += a[1] * x[i - N];
+        if (ix > 0) acc += a[2] * x[i - 1];
+        if (ix < N - 1) acc += a[4] * x[i + 1];
+        if (iy < M - 1) acc += a[5] * x[i + N];
+        if (iz < K - 1) acc += a[6] * x[i + NM];
         const double v = b[i] - acc;
         w[i] = v;
         s[0] += v * v;
@@ -38,9 +39,10 @@ __global__ void __launch_bounds__(256) k_residual7(int N, int M, int K, const do
     grid_reduce<1>(s, partial, counter, out);
 }
 
-// w = A z  and  H[0,j] = (w, v0)
-__global__ void __launch_bounds__(256) k_spmv_dot7(int N, int M, int K, const double* __restrict__ coef,
-                                                    const double* __restrict__ z, const double* __restrict__ v0,
+// w = A z  and  H[0,j] = (w, v0)   (z in FP64, or FP32 widened exactly)
+template <typename Tz>
+__global__ void __launch_bounds__(256) k_spmv_dot7(int N, int M, int K, const int* __restrict__ cls, const double* __restrict__ dict,
+                                                    const Tz* __restrict__ z, const double* __restrict__ v0,
                                                     double* __restrict__ w, double* partial,
                                                     unsigned int* counter, double* out)
 {
@@ -51,13 +53,14 @@ __global__ void __launch_bounds__(256) k_spmv_dot7(int N, int M, int K, const do
          i += (long long)gridDim.x * blockDim.x) {
         int ix, iy, iz;
         cell_xyz(i, N, NM, ix, iy, iz);
-        double acc = coef[3 * n + i] * z[i];
-        if (iz > 0) acc += coef[i] * z[i - NM];
-        if (iy > 0) acc += coef[n + i] * z[i - N];
-        if (ix > 0) acc += coef[2 * n + i] * z[i - 1];
-        if (ix < N - 1) acc += coef[4 * n + i] * z[i + 1];
-        if (iy < M - 1) acc += coef[5 * n + i] * z[i + N];
-        if (iz < K - 1) acc += coef[6 * n + i] * z[i + NM];
+        const double* a = dict + (size_t)cls[i] * 7;
+        double acc = a[3] * (double)z[i];
+        if (iz > 0) acc += a[0] * (double)z[i - NM];
+        if (iy > 0) acc += a[1] * (double)z[i - N];
+        if (ix > 0) acc += a[2] * (double)z[i - 1];
+        if (ix < N - 1) acc += a[4] * (double)z[i + 1];
+        if (iy < M - 1) acc += a[5] * (double)z[i + N];
+        if (iz < K - 1) acc += a[6] * (double)z[i + NM];
         w[i] = acc;
         s[0] += acc * v0[i];
     }
@@ -155,8 +158,9 @@ __global__ void k_backsub(KrylovScalars* ks, int last, int ldh, double* coef)
 }
 
 // x += sum_k coef_k z_k over nz basis vectors (stride n).
+template <typename Tz>
 __global__ void __launch_bounds__(256) k_multi_axpy(long long n, int nz, const double* __restrict__ coef,
-                                                     const double* __restrict__ Z, double* __restrict__ x)
+                                                     const Tz* __restrict__ Z, double* __restrict__ x)
 {
     __shared__ double cf[64];
     if (threadIdx.x < nz) cf[threadIdx.x] = coef[threadIdx.x];
@@ -165,7 +169,7 @@ __global__ void __launch_bounds__(256) k_multi_axpy(long long n, int nz, const d
          i += (long long)gridDim.x * blockDim.x) {
         double acc = x[i];
         // the reference adds z_last first and z_0 last
-        for (int k = nz - 1; k >= 0; k--) acc += Z[(size_t)k * n + i] * cf[k];
+        for (int k = nz - 1; k >= 0; k--) acc += (double)Z[(size_t)k * n + i] * cf[k];
         x[i] = acc;
     }
 }
@@ -191,7 +195,7 @@ __global__ void __launch_bounds__(256) k_dot2(long long n, const double* __restr
 // sc[3] = (t, t), sc[4] = (rr, r_new), sc[5] = ||r_new||^2.
 //
 // nu = A y ;  sc[0] = (rr, r) ; sc[1] = (rr, nu)
-__global__ void __launch_bounds__(256) k_bicg_nu(int N, int M, int K, const double* __restrict__ coef,
+__global__ void __launch_bounds__(256) k_bicg_nu(int N, int M, int K, const int* __restrict__ cls, const double* __restrict__ dict,
                                                   const double* __restrict__ y, double* __restrict__ nu,
                                                   const double* __restrict__ rr, const double* __restrict__ r,
                                                   double* partial, unsigned int* counter, double* sc)
@@ -203,13 +207,14 @@ __global__ void __launch_bounds__(256) k_bicg_nu(int N, int M, int K, const doub
          i += (long long)gridDim.x * blockDim.x) {
         int ix, iy, iz;
         cell_xyz(i, N, NM, ix, iy, iz);
-        double acc = coef[3 * n + i] * y[i];
-        if (iz > 0) acc += coef[i] * y[i - NM];
-        if (iy > 0) acc += coef[n + i] * y[i - N];
-        if (ix > 0) acc += coef[2 * n + i] * y[i - 1];
-        if (ix < N - 1) acc += coef[4 * n + i] * y[i + 1];
-        if (iy < M - 1) acc += coef[5 * n + i] * y[i + N];
-        if (iz < K - 1) acc += coef[6 * n + i] * y[i + NM];
+        const double* a = dict + (size_t)cls[i] * 7;
+        double acc = a[3] * y[i];
+        if (iz > 0) acc += a[0] * y[i - NM];
+        if (iy > 0) acc += a[1] * y[i - N];
+        if (ix > 0) acc += a[2] * y[i - 1];
+        if (ix < N - 1) acc += a[4] * y[i + 1];
+        if (iy < M - 1) acc += a[5] * y[i + N];
+        if (iz < K - 1) acc += a[6] * y[i + NM];
         nu[i] = acc;
         s[0] += rr[i] * r[i];
         s[1] += rr[i] * acc;
@@ -232,7 +237,7 @@ __global__ void k_bicg_s(long long n, const double* __restrict__ sc, double* __r
 }
 
 // t = A z ; sc[2] = (t, s) ; sc[3] = (t, t)
-__global__ void __launch_bounds__(256) k_bicg_t(int N, int M, int K, const double* __restrict__ coef,
+__global__ void __launch_bounds__(256) k_bicg_t(int N, int M, int K, const int* __restrict__ cls, const double* __restrict__ dict,
                                                  const double* __restrict__ z, double* __restrict__ t,
                                                  const double* __restrict__ sv, double* partial,
                                                  unsigned int* counter, double* sc2)
@@ -244,13 +249,14 @@ __global__ void __launch_bounds__(256) k_bicg_t(int N, int M, int K, const doubl
          i += (long long)gridDim.x * blockDim.x) {
         int ix, iy, iz;
         cell_xyz(i, N, NM, ix, iy, iz);
-        double acc = coef[3 * n + i] * z[i];
-        if (iz > 0) acc += coef[i] * z[i - NM];
-        if (iy > 0) acc += coef[n + i] * z[i - N];
-        if (ix > 0) acc += coef[2 * n + i] * z[i - 1];
-        if (ix < N - 1) acc += coef[4 * n + i] * z[i + 1];
-        if (iy < M - 1) acc += coef[5 * n + i] * z[i + N];
-        if (iz < K - 1) acc += coef[6 * n + i] * z[i + NM];
+        const double* a = dict + (size_t)cls[i] * 7;
+        double acc = a[3] * z[i];
+        if (iz > 0) acc += a[0] * z[i - NM];
+        if (iy > 0) acc += a[1] * z[i - N];
+        if (ix > 0) acc += a[2] * z[i - 1];
+        if (ix < N - 1) acc += a[4] * z[i + 1];
+        if (iy < M - 1) acc += a[5] * z[i + N];
+        if (iz < K - 1) acc += a[6] * z[i + NM];
         t[i] = acc;
         s[0] += acc * sv[i];
         s[1] += acc * acc;

@@ -135,8 +135,14 @@ struct LevelT {
     Dims d;
     std::vector<int> off;     // 3 * noff
     OffList ol;
-    const T* A = nullptr;     // noff * n coefficient planes
+    const T* A = nullptr;     // noff * n coefficient planes (setup; FP64 master only)
     DevBuf<T> Aown;
+    // solve-time operator: per-cell row class + table of distinct rows
+    const int* cls = nullptr;
+    DevBuf<int> clsown;
+    const T* dict = nullptr;
+    DevBuf<T> dictown;
+    int nclass = 0;
     DevBuf<T> lo[3], dinv[3], up[3];
     DevBuf<T> r, c, ch;
 };
@@ -165,6 +171,9 @@ struct Context {
     Dims d;
     long long n = 0;
     DevBuf<double> A7;        // fine operator, 7 planes (b s w p e n t)
+    DevBuf<int> cls0;         // fine operator as row classes + distinct rows
+    DevBuf<double> dict0;
+    int nclass0 = 0;
     bool have_matrix = false, have_setup = false;
     lsg_options opt;
     MGData mg;
@@ -177,7 +186,7 @@ struct Context {
     int* hflag = nullptr;
     double* hnorm = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    DevBuf<float> v32;        // FP32 preconditioner right-hand side
+    DevBuf<float> Z32;        // FP32 preconditioned basis (FP32 multigrid)
     // ILU(0)
     DevBuf<double> iluL, iluU;        // 3 lower planes (b s w) / 4 planes (p e n t), U diagonal = plane 0
     bool have_ilu = false;
@@ -194,6 +203,84 @@ struct lsg_ctx {
 namespace lsg {
 
 static void ilu_apply(Context& C, const double* b, double* x);
+
+// ---------------------------------------------------------------------------
+// row dictionary of an operator given as noff coefficient planes
+// ---------------------------------------------------------------------------
+__global__ void k_planes_to_rows(int noff, long long n, const double* __restrict__ planes, double* __restrict__ rows)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        for (int o = 0; o < noff; o++) rows[i * noff + o] = planes[(size_t)o * n + i];
+}
+
+// Assign every row a class id (first-seen order) and collect the distinct
+// rows; rows are compared bit for bit, so the format is lossless.
+static int build_dict(cudaStream_t s, const double* planes, int noff, long long n, DevBuf<int>& cls,
+                      DevBuf<double>& dict)
+{
+    DevBuf<double> rows;
+    rows.alloc((size_t)noff * n);
+    k_planes_to_rows<<<grid_for(n, 256), 256, 0, s>>>(noff, n, planes, rows.p);
+    LSG_CHECK_LAUNCH();
+    std::vector<double> h((size_t)noff * n);
+    LSG_CUDA(cudaMemcpyAsync(h.data(), rows.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    LSG_CUDA(cudaStreamSynchronize(s));
+    rows.release();
+    std::vector<int> hc(n);
+    std::vector<long long> first;        // row index of each class
+    size_t cap = 1 << 12;
+    std::vector<int> slot(cap, -1);
+    const size_t rowbytes = (size_t)noff * sizeof(double);
+    auto hash_row = [&](long long i) {
+        const uint64_t* w = (const uint64_t*)(h.data() + (size_t)i * noff);
+        uint64_t x = 0x9E3779B97F4A7C15ull;
+        for (int o = 0; o < noff; o++) {
+            x ^= w[o] + 0x9E3779B97F4A7C15ull + (x << 6) + (x >> 2);
+            x *= 0xBF58476D1CE4E5B9ull;
+            x ^= x >> 31;
+        }
+        return x;
+    };
+    for (long long i = 0; i < n; i++) {
+        if (first.size() * 2 >= cap) {
+            cap *= 2;
+            slot.assign(cap, -1);
+            for (size_t c = 0; c < first.size(); c++) {
+                size_t q = hash_row(first[c]) & (cap - 1);
+                while (slot[q] >= 0) q = (q + 1) & (cap - 1);
+                slot[q] = (int)c;
+            }
+        }
+        size_t q = hash_row(i) & (cap - 1);
+        const double* ri = h.data() + (size_t)i * noff;
+        int id = -1;
+        while (slot[q] >= 0) {
+            const int c = slot[q];
+            if (std::memcmp(ri, h.data() + (size_t)first[c] * noff, rowbytes) == 0) {
+                id = c;
+                break;
+            }
+            q = (q + 1) & (cap - 1);
+        }
+        if (id < 0) {
+            id = (int)first.size();
+            first.push_back(i);
+            slot[q] = id;
+        }
+        hc[i] = id;
+    }
+    const int nclass = (int)first.size();
+    std::vector<double> hd((size_t)nclass * noff);
+    for (int c = 0; c < nclass; c++)
+        std::memcpy(hd.data() + (size_t)c * noff, h.data() + (size_t)first[c] * noff, rowbytes);
+    cls.alloc(n);
+    dict.alloc(hd.size());
+    LSG_CUDA(cudaMemcpyAsync(cls.p, hc.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+    LSG_CUDA(cudaMemcpyAsync(dict.p, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    LSG_CUDA(cudaStreamSynchronize(s));
+    return nclass;
+}
 
 // ---------------------------------------------------------------------------
 // multigrid setup
@@ -318,6 +405,9 @@ static void mg_setup(Context& C)
     mg.l64[0].off.assign(kFine7, kFine7 + 21);
     mg.l64[0].ol = make_offlist(mg.l64[0].off);
     mg.l64[0].A = C.A7.p;
+    mg.l64[0].cls = C.cls0.p;
+    mg.l64[0].dict = C.dict0.p;
+    mg.l64[0].nclass = C.nclass0;
     std::vector<int> rad = {1, 1, 1};
     for (int l = 0; l < L; l++) {
         const Dims f = mg.dims[l];
@@ -351,6 +441,9 @@ static void mg_setup(Context& C)
                                                         cry, crz, agg, t.P(0), t.P(1), t.P(2), t.R(0), t.R(1), t.R(2),
                                                         cl.Aown.p);
         LSG_CHECK_LAUNCH();
+        cl.nclass = build_dict(s, cl.A, cl.ol.n, c.n(), cl.clsown, cl.dictown);
+        cl.cls = cl.clsown.p;
+        cl.dict = cl.dictown.p;
         rad = {crx, cry, crz};
     }
     // ADLJ line factors of every smoothed level
@@ -447,9 +540,12 @@ static void mg_setup(Context& C)
             b.off = a.off;
             b.ol = a.ol;
             const long long n = a.d.n();
-            b.Aown.alloc((size_t)a.ol.n * n);
-            b.A = b.Aown.p;
-            k_convert<float, double><<<grid_for((long long)a.ol.n * n, 256), 256, 0, s>>>((long long)a.ol.n * n, a.A, b.Aown.p);
+            b.cls = a.cls;
+            b.nclass = a.nclass;
+            const long long nd = (long long)a.nclass * a.ol.n;
+            b.dictown.alloc(nd);
+            b.dict = b.dictown.p;
+            k_convert<float, double><<<grid_for(nd, 256), 256, 0, s>>>(nd, a.dict, b.dictown.p);
             LSG_CHECK_LAUNCH();
             if (l < L) {
                 for (int d = 0; d < 3; d++) {
@@ -476,39 +572,48 @@ template <typename T>
 static void apply_resid(const LevelT<T>& lv, const T* x, T* r, cudaStream_t s, int mode)
 {
     const long long n = lv.d.n();
+    const dim3 zb(32, 8), zg((lv.d.N + 31) / 32, (lv.d.M + 7) / 8, (lv.d.K + kZChunk - 1) / kZChunk);
     if (lv.ol.n == 7 && lv.off[0] == 0 && lv.off[2] == -1) {
         if (mode == 0)
-            k_apply7<T, 0><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.A, x, r);
+            k_apply7z<T, 0><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.cls, lv.dict, x, r);
         else
-            k_apply7<T, 1><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.A, x, r);
+            k_apply7z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.cls, lv.dict, x, r);
+    } else if (lv.ol.n == 27) {
+        if (mode == 0)
+            k_apply27z<T, 0><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.cls, lv.dict, x, r);
+        else
+            k_apply27z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.cls, lv.dict, x, r);
     } else {
         if (mode == 0)
-            k_applybox<T, 0><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.ol, lv.A, x, r);
+            k_applyboxd<T, 0><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.ol, lv.cls, lv.dict, x, r);
         else
-            k_applybox<T, 1><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.ol, lv.A, x, r);
+            k_applyboxd<T, 1><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.ol, lv.cls, lv.dict, x, r);
     }
     LSG_CHECK_LAUNCH();
 }
 
 template <typename T>
-static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStream_t s)
+static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStream_t s, T* ch = nullptr)
 {
+    if (!ch) ch = const_cast<T*>(lv.ch.p);
     const Dims& g = lv.d;
     if (d == 0) {
         const long long nl = (long long)g.M * g.K;
         const int blocks = grid_for(nl * 32, 256, 148 * 64);
         k_tdma_xwarp<T><<<blocks, 256, 0, s>>>(g.N, nl, lv.lo[0].p, lv.dinv[0].p, lv.up[0].p, lv.r.p, lv.c.p,
-                                               lv.ch.p, omega);
+                                               ch, omega);
     } else {
         LineGeom lg{g.N, g.M, g.K, d};
         k_tdma_strided<T><<<grid_for(lg.nlines(), 128, 148 * 64), 128, 0, s>>>(
-            lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, lv.ch.p, omega);
+            lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, ch, omega);
     }
     LSG_CHECK_LAUNCH();
 }
 
+// ch0: where the finest-level correction (the preconditioned vector) goes;
+// nullptr = the level's own buffer.
 template <typename T>
-static void vcycle(Context& C, std::vector<LevelT<T>>& lev)
+static void vcycle(Context& C, std::vector<LevelT<T>>& lev, T* ch0 = nullptr)
 {
     MGData& mg = C.mg;
     cudaStream_t s = C.s;
@@ -530,14 +635,15 @@ static void vcycle(Context& C, std::vector<LevelT<T>>& lev)
         LevelT<T>& lv = lev[l];
         const Dims& f = lv.d;
         const TransferTabs& t = mg.tabs[l];
+        T* chl = (l == 0 && ch0) ? ch0 : lv.ch.p;
         k_prolong<T><<<grid_for(f.n(), 256), 256, 0, s>>>(f.N, f.M, f.K, lev[l + 1].d.N, lev[l + 1].d.M, t.P(0), t.P(1),
-                                                         t.P(2), lev[l + 1].ch.p, lv.ch.p, lv.c.p);
+                                                         t.P(2), lev[l + 1].ch.p, chl, lv.c.p);
         LSG_CHECK_LAUNCH();
         for (int it = 0; it < C.opt.n_post; it++) {
             const int order[3] = {2, 1, 0};       // SmootherADLJ::solve: z, y, x
             for (int q = 0; q < 3; q++) {
-                apply_resid<T>(lv, lv.c.p, lv.r.p, s, 0);   // calcRes: r -= A c
-                line_solve<T>(lv, order[q], zq, omega, s);  // c = omega T^-1 r ; ch += c
+                apply_resid<T>(lv, lv.c.p, lv.r.p, s, 0);        // calcRes: r -= A c
+                line_solve<T>(lv, order[q], zq, omega, s, chl);  // c = omega T^-1 r ; ch += c
             }
         }
     }
@@ -550,12 +656,12 @@ static double vcycle_bytes(const MGData& mg, int n_post, double w)
     double b = 0;
     for (int l = 0; l <= mg.L; l++) {
         const double n = (double)mg.dims[l].n();
-        const double noff = (l == 0) ? 7.0 : (double)mg.l64[l].ol.n;
         if (l < mg.L) {
             b += (1.0 + 0.125) * w * n;                      // restriction read fine + write coarse
             b += (0.125 + 2.0) * w * n;                      // prolongation read coarse + write ch, c
-            // per direction: residual (r rw, c, A) + line solve (r, lo, dinv, up, c w r w, ch rw)
-            b += 3.0 * n_post * ((2.0 + 1.0 + noff) + (1.0 + 3.0 + 3.0 + 2.0)) * w * n;
+            // per direction: residual (r rw, c; row class 4 B; the distinct-row
+            // table is L2 resident) + line solve (r, lo, dinv, up, ch read; c, ch written)
+            b += 3.0 * n_post * ((3.0 * w + 4.0) + 7.0 * w) * n;
         }
     }
     return b;
@@ -613,9 +719,9 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
     const double w8 = 8.0;
     double bytes = 0;
     // norm_r = ||b - A x||  ; w = b - A x
-    k_residual7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.A7.p, x, b, C.w.p, part, cnt, &ks->normW2);
+    k_residual7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, x, b, C.w.p, part, cnt, &ks->normW2);
     LSG_CHECK_LAUNCH();
-    bytes += 10 * w8 * n;
+    bytes += (3 * w8 + 4) * n;
     double nrm2 = 0;
     LSG_CUDA(cudaMemcpyAsync(&nrm2, &ks->normW2, sizeof(double), cudaMemcpyDeviceToHost, s));
     LSG_CUDA(cudaStreamSynchronize(s));
@@ -638,13 +744,16 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
                 double* vj = C.V.p + (size_t)j * n;
                 double* zj = C.Z.p + (size_t)j * n;
                 // v_j = w / ||w|| (also the preconditioner input)
-                if (C.mg.fp32 && C.opt.precond == LSG_PC_MG) {
+                const bool z32 = C.mg.fp32 && C.opt.precond == LSG_PC_MG;
+                float* zj32 = z32 ? C.Z32.p + (size_t)j * n : nullptr;
+                if (z32) {
+                    // the FP32 cycle writes z_j directly; it is kept in FP32
+                    // (exactly representable in FP64, so the Arnoldi relation
+                    // w = A z_j below holds for the stored z_j)
                     k_scale_copy<float><<<grid_for(n, 256), 256, 0, s>>>(n, C.w.p, &ks->invNormW, vj, C.mg.l32[0].r.p);
                     LSG_CHECK_LAUNCH();
-                    vcycle<float>(C, C.mg.l32);
-                    k_convert<double, float><<<grid_for(n, 256), 256, 0, s>>>(n, C.mg.l32[0].ch.p, zj);
-                    LSG_CHECK_LAUNCH();
-                    bytes += (8 + 8 + 4) * (double)n + vcycle_bytes(C.mg, C.opt.n_post, 4.0) + 12.0 * n;
+                    vcycle<float>(C, C.mg.l32, zj32);
+                    bytes += (8 + 8 + 4) * (double)n + vcycle_bytes(C.mg, C.opt.n_post, 4.0);
                 } else {
                     k_scale_copy<double><<<grid_for(n, 256), 256, 0, s>>>(n, C.w.p, &ks->invNormW, vj, C.t1.p);
                     LSG_CHECK_LAUNCH();
@@ -653,9 +762,14 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
                 }
                 // w = A z_j ; H[0,j] = (w, v_0)
                 double* Hj = ks->H + (size_t)j * 65;
-                k_spmv_dot7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.A7.p, zj, C.V.p, C.w.p, part, cnt, Hj);
+                if (z32)
+                    k_spmv_dot7<float><<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, zj32, C.V.p, C.w.p, part,
+                                                          cnt, Hj);
+                else
+                    k_spmv_dot7<double><<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, zj, C.V.p, C.w.p, part,
+                                                           cnt, Hj);
                 LSG_CHECK_LAUNCH();
-                bytes += 10 * w8 * n;
+                bytes += (3 * w8 + 4) * n;
                 // modified Gram-Schmidt: w -= h_i v_i ; h_{i+1} = (w, v_{i+1}); last: ||w||^2
                 for (int i = 1; i <= j + 1; i++) {
                     const bool last = (i == j + 1);
@@ -677,16 +791,19 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
             // x += Z y   (solUpdate)
             k_backsub<<<1, 32, 0, s>>>(ks, jlast, 65, C.coefs.p);
             LSG_CHECK_LAUNCH();
-            k_multi_axpy<<<grid_for(n, 256), 256, 0, s>>>(n, jlast + 1, C.coefs.p, C.Z.p, x);
+            if (C.mg.fp32 && C.opt.precond == LSG_PC_MG)
+                k_multi_axpy<float><<<grid_for(n, 256), 256, 0, s>>>(n, jlast + 1, C.coefs.p, C.Z32.p, x);
+            else
+                k_multi_axpy<double><<<grid_for(n, 256), 256, 0, s>>>(n, jlast + 1, C.coefs.p, C.Z.p, x);
             LSG_CHECK_LAUNCH();
             bytes += (jlast + 3) * w8 * n;
             const bool refine = (C.opt.mg_precision == LSG_FP32 && C.opt.precond == LSG_PC_MG);
             if (!finished || refine) {
                 // w = b - A x: the next cycle's first direction
                 // (fgmres_interface.h:136-138)
-                k_residual7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.A7.p, x, b, C.w.p, part, cnt, C.scal.p + 16);
+                k_residual7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, x, b, C.w.p, part, cnt, C.scal.p + 16);
                 LSG_CHECK_LAUNCH();
-                bytes += 10 * w8 * n;
+                bytes += (3 * w8 + 4) * n;
                 KrylovScalars hs;
                 double tr2 = 0;
                 LSG_CUDA(cudaMemcpyAsync(&hs, ks, sizeof(hs), cudaMemcpyDeviceToHost, s));
@@ -792,7 +909,7 @@ static int bicgstab(Context& C, double* x, const double* b, lsg_stats* st)
     double* t = C.t3.p;
     double bytes = 0;
     int it = 1;
-    k_residual7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.A7.p, x, b, r, part, cnt, sc + 5);
+    k_residual7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, x, b, r, part, cnt, sc + 5);
     LSG_CHECK_LAUNCH();
     bytes += 80.0 * n;
     double nr2 = 0;
@@ -805,12 +922,12 @@ static int bicgstab(Context& C, double* x, const double* b, lsg_stats* st)
         LSG_CUDA(cudaMemcpyAsync(p, r, n * 8, cudaMemcpyDeviceToDevice, s));
         do {
             precond_apply(C, p, y);
-            k_bicg_nu<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.A7.p, y, nu, rr, r, part, cnt, sc);
+            k_bicg_nu<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, y, nu, rr, r, part, cnt, sc);
             LSG_CHECK_LAUNCH();
             k_bicg_s<<<grid_for(n, 256), 256, 0, s>>>(n, sc, nu, r, sv);
             LSG_CHECK_LAUNCH();
             precond_apply(C, sv, z);
-            k_bicg_t<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.A7.p, z, t, sv, part, cnt, sc + 2);
+            k_bicg_t<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, z, t, sv, part, cnt, sc + 2);
             LSG_CHECK_LAUNCH();
             k_bicg_upd<<<gb, 256, 0, s>>>(n, sc, y, z, x, t, r, sv, rr, part, cnt, sc + 4);
             LSG_CHECK_LAUNCH();
@@ -843,7 +960,13 @@ static void krylov_alloc(Context& C)
     const int m = std::max(2, std::min(C.opt.restart, 64));
     C.restart = m;
     C.V.alloc((size_t)m * n);
-    C.Z.alloc((size_t)m * n);
+    if (C.opt.mg_precision == LSG_FP32 && C.opt.precond == LSG_PC_MG && C.opt.method == LSG_METHOD_FGMRES) {
+        C.Z.alloc(2 * n);          // BiCGStab-sized scratch only
+        C.Z32.alloc((size_t)m * n);
+    } else {
+        C.Z.alloc((size_t)std::max(m, 2) * n);
+        C.Z32.release();
+    }
     C.w.alloc(n);
     C.t1.alloc(n);
     C.t2.alloc(n);
@@ -857,7 +980,7 @@ static void krylov_alloc(Context& C)
 static double true_residual(Context& C, const double* x, const double* b)
 {
     const Dims& d = C.d;
-    k_residual7<<<grid_for(C.n, 256, Reducer::kMaxBlocks), 256, 0, C.s>>>(d.N, d.M, d.K, C.A7.p, x, b, C.t1.p,
+    k_residual7<<<grid_for(C.n, 256, Reducer::kMaxBlocks), 256, 0, C.s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, x, b, C.t1.p,
                                                                        C.red.partial.p, C.red.counter.p,
                                                                        C.scal.p + 40);
     LSG_CHECK_LAUNCH();
@@ -1028,6 +1151,7 @@ static int set_matrix_impl(lsg_ctx* h, int N, int M, int K, const int* rowptr, c
         throw Error{LSG_ERR_PATTERN, "row " + std::to_string(e - 1) +
                                          " holds an entry that is not the cell or one of its six face neighbours"};
     }
+    C.nclass0 = build_dict(C.s, C.A7.p, 7, n, C.cls0, C.dict0);
     C.have_matrix = true;
     C.have_setup = false;
     return LSG_OK;
@@ -1067,6 +1191,7 @@ int lsg_set_matrix_stencil7(lsg_ctx* h, int N, int M, int K, const double* plane
     C.A7.alloc(7 * n);
     LSG_CUDA(cudaMemcpyAsync(C.A7.p, planes, 7 * n * sizeof(double), cudaMemcpyHostToDevice, C.s));
     LSG_CUDA(cudaStreamSynchronize(C.s));
+    C.nclass0 = build_dict(C.s, C.A7.p, 7, n, C.cls0, C.dict0);
     C.have_matrix = true;
     C.have_setup = false;
     return LSG_OK;
@@ -1140,7 +1265,7 @@ int lsg_apply(lsg_ctx* h, const double* x, double* y)
     dx.alloc(n);
     dy.alloc(n);
     LSG_CUDA(cudaMemcpyAsync(dx.p, x, n * 8, cudaMemcpyHostToDevice, C.s));
-    k_apply7<double, 1><<<grid_for(n, 256), 256, 0, C.s>>>(C.d.N, C.d.M, C.d.K, C.A7.p, dx.p, dy.p);
+    k_apply7d<double, 1><<<grid_for(n, 256), 256, 0, C.s>>>(C.d.N, C.d.M, C.d.K, C.cls0.p, C.dict0.p, dx.p, dy.p);
     LSG_CHECK_LAUNCH();
     LSG_CUDA(cudaMemcpyAsync(y, dy.p, n * 8, cudaMemcpyDeviceToHost, C.s));
     LSG_CUDA(cudaStreamSynchronize(C.s));
@@ -1284,9 +1409,13 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
         } else if (which == 3) {
             if (f32) apply_resid<float>(C.mg.l32[0], C.mg.l32[0].c.p, C.mg.l32[0].r.p, C.s, 0);
             else apply_resid<double>(C.mg.l64[0], C.mg.l64[0].c.p, C.mg.l64[0].r.p, C.s, 0);
+        } else if (which == 5) {
+            LSG_REQUIRE(C.mg.L >= 2, LSG_ERR_STATE, "no smoothed coarse level");
+            if (f32) apply_resid<float>(C.mg.l32[1], C.mg.l32[1].c.p, C.mg.l32[1].r.p, C.s, 0);
+            else apply_resid<double>(C.mg.l64[1], C.mg.l64[1].c.p, C.mg.l64[1].r.p, C.s, 0);
         } else if (which == 4) {
-            k_spmv_dot7<<<grid_for(n, 256, Reducer::kMaxBlocks), 256, 0, C.s>>>(
-                C.d.N, C.d.M, C.d.K, C.A7.p, C.Z.p, C.V.p, C.w.p, C.red.partial.p, C.red.counter.p, C.scal.p + 48);
+            k_spmv_dot7<double><<<grid_for(n, 256, Reducer::kMaxBlocks), 256, 0, C.s>>>(
+                C.d.N, C.d.M, C.d.K, C.cls0.p, C.dict0.p, C.Z.p, C.V.p, C.w.p, C.red.partial.p, C.red.counter.p, C.scal.p + 48);
             LSG_CHECK_LAUNCH();
         } else {
             throw Error{LSG_ERR_ARG, "unknown kernel id"};
@@ -1294,9 +1423,20 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
     };
     double bytes;
     if (which <= 2) bytes = 7.0 * w * n;              // r, lo, dinv, up, ch read; c, ch written
-    else if (which == 3) bytes = 10.0 * w * n;        // 7 planes + c + r read/write
-    else bytes = 10.0 * 8.0 * n;                      // 7 planes + z + v0 read, w written
+    else if (which == 3) bytes = (3.0 * w + 4.0) * n; // c, r read/write, row class
+    else if (which == 5) bytes = (3.0 * w + 4.0) * (double)C.mg.dims[1].n();
+    else bytes = (3.0 * 8.0 + 4.0) * n;               // z, v0 read, w written, row class
     // defined inputs for the timed launches
+    if (which == 5) {
+        const long long n1 = C.mg.dims[1].n();
+        if (f32) {
+            LSG_CUDA(cudaMemsetAsync(C.mg.l32[1].r.p, 0, n1 * 4, C.s));
+            LSG_CUDA(cudaMemsetAsync(C.mg.l32[1].c.p, 0, n1 * 4, C.s));
+        } else {
+            LSG_CUDA(cudaMemsetAsync(C.mg.l64[1].r.p, 0, n1 * 8, C.s));
+            LSG_CUDA(cudaMemsetAsync(C.mg.l64[1].c.p, 0, n1 * 8, C.s));
+        }
+    }
     if (f32) {
         LSG_CUDA(cudaMemsetAsync(C.mg.l32[0].r.p, 0, n * 4, C.s));
         LSG_CUDA(cudaMemsetAsync(C.mg.l32[0].c.p, 0, n * 4, C.s));
