@@ -306,10 +306,12 @@ __global__ void __launch_bounds__(256) k_apply27d(int N, int M, int K, const int
 // z-marching variants: a 32 x 8 thread tile covers (x, y); each thread walks a
 // chunk of ZC planes, keeping the z-neighbours of its column in registers.
 // No integer division; rows of the same class hit the same L1 lines.
-constexpr int kZChunk = 16;
+// z planes per thread: long chunks on big levels (register reuse), short
+// ones on coarse levels (parallelism).
+inline int zchunk_for(long long n) { return n >= (8LL << 20) ? 16 : (n >= (1LL << 20) ? 4 : 2); }
 
 template <typename T, int MODE>
-__global__ void __launch_bounds__(256) k_apply7z(int N, int M, int K, const int* __restrict__ cls,
+__global__ void __launch_bounds__(256) k_apply7z(int N, int M, int K, int zc, const int* __restrict__ cls,
                                                   const T* __restrict__ dict, const T* __restrict__ x,
                                                   T* __restrict__ r)
 {
@@ -317,8 +319,8 @@ __global__ void __launch_bounds__(256) k_apply7z(int N, int M, int K, const int*
     const int iy = blockIdx.y * 8 + threadIdx.y;
     if (ix >= N || iy >= M) return;
     const long long NM = (long long)N * M;
-    const int z0 = blockIdx.z * kZChunk;
-    const int z1 = min(z0 + kZChunk, K);
+    const int z0 = blockIdx.z * zc;
+    const int z1 = min(z0 + zc, K);
     long long i = ix + (long long)N * iy + NM * z0;
     T xm = (z0 > 0) ? x[i - NM] : (T)0;
     T xc = x[i];
@@ -341,7 +343,7 @@ __global__ void __launch_bounds__(256) k_apply7z(int N, int M, int K, const int*
 }
 
 template <typename T, int MODE>
-__global__ void __launch_bounds__(256) k_apply27z(int N, int M, int K, const int* __restrict__ cls,
+__global__ void __launch_bounds__(256) k_apply27z(int N, int M, int K, int zc, const int* __restrict__ cls,
                                                    const T* __restrict__ dict, const T* __restrict__ x,
                                                    T* __restrict__ r)
 {
@@ -349,8 +351,8 @@ __global__ void __launch_bounds__(256) k_apply27z(int N, int M, int K, const int
     const int iy = blockIdx.y * 8 + threadIdx.y;
     if (ix >= N || iy >= M) return;
     const long long NM = (long long)N * M;
-    const int z0 = blockIdx.z * kZChunk;
-    const int z1 = min(z0 + kZChunk, K);
+    const int z0 = blockIdx.z * zc;
+    const int z1 = min(z0 + zc, K);
     const long long col = ix + (long long)N * iy;
     bool ok[9];
     int off[9];
@@ -777,18 +779,34 @@ __global__ void __launch_bounds__(128) k_tdma_strided(LineGeom g, bool zquirk, c
         } else {
             rhs0 = r[i0];
         }
-        // forward: y_t = (r_t - lo_t y_{t-1}) * dinv_t, stored in c
+        // forward: y_t = (r_t - lo_t y_{t-1}) * dinv_t, stored in c.  The loads
+        // of chunk k+1 are issued before the recurrence of chunk k.
         T yv = 0;
+        T rr[U], ll[U], dd[U], rn[U], ln[U], dn[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (u < L) {
+                const long long i = i0 + (long long)u * st;
+                rn[u] = (u == 0) ? rhs0 : r[i];
+                ln[u] = lo[i];
+                dn[u] = dinv[i];
+            }
+        }
         for (int t0 = 0; t0 < L; t0 += U) {
-            T rr[U], ll[U], dd[U];
 #pragma unroll
             for (int u = 0; u < U; u++) {
-                const int t = t0 + u;
+                rr[u] = rn[u];
+                ll[u] = ln[u];
+                dd[u] = dn[u];
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int t = t0 + U + u;
                 if (t < L) {
                     const long long i = i0 + (long long)t * st;
-                    rr[u] = (t == 0) ? rhs0 : r[i];
-                    ll[u] = lo[i];
-                    dd[u] = dinv[i];
+                    rn[u] = r[i];
+                    ln[u] = lo[i];
+                    dn[u] = dinv[i];
                 }
             }
 #pragma unroll
@@ -802,23 +820,40 @@ __global__ void __launch_bounds__(128) k_tdma_strided(LineGeom g, bool zquirk, c
         }
         // backward: x_t = y_t - up_t x_{t+1};  c = omega x ; ch += c
         T xv = 0;
-        for (int t1 = L - 1; t1 >= 0; t1 -= U) {
-            T yy[U], uu[U], hh[U];
+        T yy[U], uu[U], hh[U], yn[U], un[U], hn[U];
+        const int tl = L - 1;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int t = tl - u;
+            if (t >= 0) {
+                const long long i = i0 + (long long)t * st;
+                yn[u] = (u == 0) ? yv : c[i];
+                un[u] = up[i];
+                hn[u] = ch[i];
+            }
+        }
+        for (int t1 = tl; t1 >= 0; t1 -= U) {
 #pragma unroll
             for (int u = 0; u < U; u++) {
-                const int t = t1 - u;
+                yy[u] = yn[u];
+                uu[u] = un[u];
+                hh[u] = hn[u];
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int t = t1 - U - u;
                 if (t >= 0) {
                     const long long i = i0 + (long long)t * st;
-                    yy[u] = c[i];
-                    uu[u] = up[i];
-                    hh[u] = ch[i];
+                    yn[u] = c[i];
+                    un[u] = up[i];
+                    hn[u] = ch[i];
                 }
             }
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const int t = t1 - u;
                 if (t >= 0) {
-                    xv = (t == L - 1) ? yy[u] : yy[u] - uu[u] * xv;
+                    xv = (t == tl) ? yy[u] : yy[u] - uu[u] * xv;
                     const T cv = omega * xv;
                     const long long i = i0 + (long long)t * st;
                     c[i] = cv;

@@ -572,17 +572,18 @@ template <typename T>
 static void apply_resid(const LevelT<T>& lv, const T* x, T* r, cudaStream_t s, int mode)
 {
     const long long n = lv.d.n();
-    const dim3 zb(32, 8), zg((lv.d.N + 31) / 32, (lv.d.M + 7) / 8, (lv.d.K + kZChunk - 1) / kZChunk);
+    const int zc = zchunk_for(n);
+    const dim3 zb(32, 8), zg((lv.d.N + 31) / 32, (lv.d.M + 7) / 8, (lv.d.K + zc - 1) / zc);
     if (lv.ol.n == 7 && lv.off[0] == 0 && lv.off[2] == -1) {
         if (mode == 0)
-            k_apply7z<T, 0><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.cls, lv.dict, x, r);
+            k_apply7z<T, 0><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict, x, r);
         else
-            k_apply7z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.cls, lv.dict, x, r);
+            k_apply7z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict, x, r);
     } else if (lv.ol.n == 27) {
         if (mode == 0)
-            k_apply27z<T, 0><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.cls, lv.dict, x, r);
+            k_apply27z<T, 0><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict, x, r);
         else
-            k_apply27z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.cls, lv.dict, x, r);
+            k_apply27z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict, x, r);
     } else {
         if (mode == 0)
             k_applyboxd<T, 0><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.ol, lv.cls, lv.dict, x, r);
