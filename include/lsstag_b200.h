@@ -164,6 +164,24 @@ int lsg_mg_level_tridiag(lsg_ctx* ctx, int level, char dir, double* c, double* d
    lsg_setup with the multigrid preconditioner. */
 int lsg_profile_kernel(lsg_ctx* ctx, int which, int reps, double* ms_per_launch, double* bytes_per_launch);
 
+/* Residual r = b - A x and its squared 2-norm for a 7-point operator given
+   as seven coefficient planes (layout of lsg_set_matrix_stencil7), without
+   allocating device memory.  No counterpart in the reference: it is for
+   callers that cannot call cudaMalloc (a host application recording a CUDA
+   graph, a solver embedded under a device-memory budget owned by its host
+   program).  All pointers are device pointers owned by the caller; r may be
+   NULL (norm only); *norm2 receives ||b - A x||^2 (FP64).  Work is queued on
+   `stream` (a cudaStream_t, NULL = legacy default stream); read *norm2 after
+   synchronising it.  Scratch is a file-scope device array of the library
+   (4096 block partials + a counter, about 32 KiB per GPU, held until the
+   process exits), which caps the grid at 16,777,216 cells; larger grids are
+   rejected with LSG_ERR_ARG and a message on stderr.  The first call on a
+   device looks up the array's device address (cudaGetSymbolAddress), so make
+   that first call before any stream capture.  All calls share the array:
+   calls that overlap on the GPU race and must be serialised by the caller. */
+int lsg_residual_norm_noalloc(int N, int M, int K, const double* planes, const double* x, const double* b,
+                              double* r, double* norm2, void* stream);
+
 /* Library build string (version, arch). */
 const char* lsg_version(void);
 

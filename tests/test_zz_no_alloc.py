@@ -1,0 +1,75 @@
+"""The allocation-free residual entry point (lsg_residual_norm_noalloc).
+
+It exists for callers that cannot allocate device memory -- a host program
+that is recording a CUDA graph, or a solver embedded under a device-memory
+budget its host application owns -- so it takes every buffer from the
+caller and keeps its only scratch in a fixed device array of the library.
+This checks it, through the C ABI, against the context-based operator apply
+on two calls in a row.  The file sorts last so that a run stopping at the
+first failure has already run every other test."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _planes(g):
+    n = g["b"].size
+    N, M, K = (int(v) for v in g["dims"])
+    NM = N * M
+    rp, col, val = g["A_rowptr"], g["A_col"], g["A_val"]
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    d = col.astype(np.int64) - rows
+    slot = np.select([d == -NM, d == -N, d == -1, d == 0, d == 1, d == N, d == NM], [0, 1, 2, 3, 4, 5, 6], -1)
+    P = np.zeros((7, n))
+    np.add.at(P, (slot, rows), val)
+    return P
+
+
+def test_residual_norm_noalloc_matches_context_apply():
+    import torch
+
+    from lsstag_b200 import _lib as L
+    from lsstag_b200 import solver as S
+
+    g = load_golden("spheres4_24")
+    N, M, K = (int(v) for v in g["dims"])
+    n = N * M * K
+    P = _planes(g)
+    s = S.MGFGMRES()
+    s.set((g["A_rowptr"], g["A_col"], g["A_val"], (N, M, K)))
+    lib = L.load()
+    dev = torch.device("cuda:0")
+    planes_d = torch.from_numpy(P.reshape(-1).copy()).to(dev)
+    b_d = torch.from_numpy(g["b"]).to(dev)
+    rng = np.random.default_rng(11)
+    stream = torch.cuda.current_stream().cuda_stream
+    for call in range(2):
+        x = rng.standard_normal(n)
+        x_d = torch.from_numpy(x).to(dev)
+        r_d = torch.empty(n, dtype=torch.float64, device=dev)
+        nrm_d = torch.zeros(1, dtype=torch.float64, device=dev)
+        rc = lib.lsg_residual_norm_noalloc(N, M, K, ctypes.c_void_p(planes_d.data_ptr()),
+                                           ctypes.c_void_p(x_d.data_ptr()), ctypes.c_void_p(b_d.data_ptr()),
+                                           ctypes.c_void_p(r_d.data_ptr()), ctypes.c_void_p(nrm_d.data_ptr()),
+                                           ctypes.c_void_p(stream))
+        assert rc == L.LSG_OK
+        torch.cuda.synchronize()
+        r_ref = g["b"] - s.apply(x)            # the existing entry point (lsg_apply)
+        r = r_d.cpu().numpy()
+        assert np.linalg.norm(r - r_ref) <= 1e-14 * np.linalg.norm(r_ref), call
+        nrm = float(nrm_d.item())
+        assert nrm == pytest.approx(float(np.dot(r_ref, r_ref)), rel=1e-12), call
+    s.close()
+
+
+def test_residual_norm_noalloc_rejects_oversize_grid():
+    from lsstag_b200 import _lib as L
+    lib = L.load()
+    one = ctypes.c_void_p(8)   # never dereferenced: the size check comes first
+    rc = lib.lsg_residual_norm_noalloc(512, 256, 256, one, one, one, None, one, None)
+    assert rc == L.LSG_ERR_ARG
