@@ -176,7 +176,7 @@ def run_reference_arm(args, world, rank):
 def config_dict(args, world):
     return {"workload": f"poisson_spheres4_{args.size}^3_mgfgmres30_rel1e-10",
             "grid": [args.size] * 3, "bodies": "4 seeded spheres (seed 3), Neumann walls, 2 pinned rows",
-            "krylov": "FGMRES(30) FP64, modified Gram-Schmidt",
+            "krylov": f"FGMRES({getattr(args, 'restart', 30)}) FP64, modified Gram-Schmidt ({getattr(args, 'gs', 'mgs')} form)",
             "precond": "Galerkin MG, ADLJ z/y/x line smoother V(0,3), omega 0.805",
             "l2": "inputs larger than L2 (operator 0.94 GB FP64 + Krylov basis)",
             "parallelism": "replicas" if world > 1 else "single GPU"}
@@ -190,6 +190,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--restart", type=int, default=30, help="FGMRES restart length (30 = the measured workload)")
+    ap.add_argument("--gs", default="mgs", choices=["mgs", "lowsync"],
+                    help="Gram-Schmidt form: the reference's pass-per-vector MGS (default) or the "
+                         "low-synchronisation form of the same projections")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
     world, rank, local, pg = dist_setup(args)
@@ -210,12 +214,13 @@ def main():
     P, dims, pins, b = cases.load(args.size)
     n = b.size
     bnorm = float(np.linalg.norm(b))
-    task = S.Task(eps=1e-10 * bnorm, MAX_ITER=200, FGMRES_RESTART_NUM=30)
+    task = S.Task(eps=1e-10 * bnorm, MAX_ITER=200, FGMRES_RESTART_NUM=args.restart)
     dev = f"cuda:{local}"
     b_dev = torch.from_numpy(b).to(dev)
     results = {}
+    gs = L.GS_LOWSYNC if args.gs == "lowsync" else L.GS_MGS
     for name, prec in (("fp32", L.FP32), ("fp64", L.FP64)):
-        s = S.MGFGMRES(device=local, mg_precision=prec)
+        s = S.MGFGMRES(device=local, mg_precision=prec, gram_schmidt=gs)
         s.set_planes(P, dims, task)
         x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
         st = L.Stats()

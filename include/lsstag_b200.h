@@ -55,6 +55,9 @@ extern "C" {
 /* lsg_options.mg_precision */
 #define LSG_FP64 0
 #define LSG_FP32 1
+/* lsg_options.gram_schmidt */
+#define LSG_GS_MGS 0
+#define LSG_GS_LOWSYNC 1
 /* lsg_options.smoother */
 #define LSG_SMOOTHER_ADLJ 0   /* reference: damped z,y,x line Jacobi */
 #define LSG_SMOOTHER_RBGS 1   /* red-black point Gauss-Seidel (new variant) */
@@ -73,7 +76,12 @@ typedef struct lsg_options {
                             where the reference does (smoother_adlj_z.h:54-58) */
     double eps;          /* absolute stopping tolerance (reference semantics) */
     double omega;        /* ADLJ damping (reference 0.805) */
-    int reserved[8];
+    int gram_schmidt;    /* LSG_GS_MGS: modified Gram-Schmidt, one pass per basis
+                            vector (reference, fgmres_interface.h:97-102);
+                            LSG_GS_LOWSYNC: the same MGS projections computed as
+                            h = (I + L)^{-1} V^T w with L the strictly lower part of
+                            V^T V (inverse compact WY form), two passes per step */
+    int reserved[7];
 } lsg_options;
 
 typedef struct lsg_stats {

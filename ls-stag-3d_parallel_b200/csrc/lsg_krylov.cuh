@@ -159,7 +159,7 @@ __global__ void k_backsub(KrylovScalars* ks, int last, int ldh, double* coef)
 
 // x += sum_k coef_k z_k over nz basis vectors (stride n).
 template <typename Tz>
-__global__ void __launch_bounds__(256) k_multi_axpy(long long n, int nz, const double* __restrict__ coef,
+__global__ void __launch_bounds__(256) k_multi_axpy(long long n, long long ld, int nz, const double* __restrict__ coef,
                                                      const Tz* __restrict__ Z, double* __restrict__ x)
 {
     __shared__ double cf[64];
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(256) k_multi_axpy(long long n, int nz, const d
          i += (long long)gridDim.x * blockDim.x) {
         double acc = x[i];
         // the reference adds z_last first and z_0 last
-        for (int k = nz - 1; k >= 0; k--) acc += (double)Z[(size_t)k * n + i] * cf[k];
+        for (int k = nz - 1; k >= 0; k--) acc += (double)Z[(size_t)k * ld + i] * cf[k];
         x[i] = acc;
     }
 }
@@ -308,6 +308,128 @@ __global__ void __launch_bounds__(256) k_bicg_p(long long n, const double* __res
         s[0] += rv * rv;
     }
     grid_reduce<1>(s, partial, counter, sc5);
+}
+
+}  // namespace lsg
+
+namespace lsg {
+
+// ---------------------------------------------------------------------------
+// Low-synchronisation MGS (inverse compact WY form).  For the basis
+// V = [v_0 .. v_j] the MGS coefficients satisfy (I + L) h = V^T w with L the
+// strictly lower part of V^T V; both right-hand sides come from one pass.
+// ---------------------------------------------------------------------------
+constexpr int kGsMaxVec = 64;
+
+// Block-level sum of nv values per thread into partial[block * stride + q];
+// the last block sums the partials in block order into out[q].
+__device__ void grid_reduce_n(double* vals, int nv, double* partial, int stride, unsigned int* counter,
+                              double* out)
+{
+    __shared__ double sh[32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int q = 0; q < nv; q++) {
+        double t = warp_sum(vals[q]);
+        if (lane == 0) sh[wid] = t;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double u = 0.0;
+            for (int w = 0; w < nw; w++) u += sh[w];
+            partial[(size_t)blockIdx.x * stride + q] = u;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int q = wid; q < nv; q += nw) {
+        double acc = 0.0;
+        for (int b = lane; b < (int)gridDim.x; b += 32) acc += ((volatile double*)partial)[(size_t)b * stride + q];
+        acc = warp_sum(acc);
+        if (lane == 0) out[q] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *counter = 0u;
+}
+
+// One pass over V[0..j] and w:  s[k] = (v_k, w), k <= j;  g[k] = (v_k, v_j), k < j.
+// out = s[0..j], g[0..j-1] (2j+1 values).
+template <int NV>
+__global__ void __launch_bounds__(256) k_gs_dots(long long n, long long ld, int j, const double* __restrict__ V,
+                                                  const double* __restrict__ w, double* partial,
+                                                  unsigned int* counter, double* out)
+{
+    double sacc[NV], gacc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        sacc[k] = 0.0;
+        gacc[k] = 0.0;
+    }
+    const double* vj = V + (size_t)j * ld;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double wi = w[i], vji = vj[i];
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            if (k <= j) {
+                const double vk = (k == j) ? vji : V[(size_t)k * ld + i];
+                sacc[k] += vk * wi;
+                if (k < j) gacc[k] += vk * vji;
+            }
+        }
+    }
+    double vals[2 * NV];
+    int nv = 0;
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+        if (k <= j) vals[nv++] = sacc[k];
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+        if (k < j) vals[nv++] = gacc[k];
+    grid_reduce_n(vals, nv, partial, 2 * kGsMaxVec, counter, out);
+}
+
+// Triangular correction on one thread: store row j of L (from g), solve
+// (I + L) h = s, write h into Hessenberg column j.
+__global__ void k_gs_tri(KrylovScalars* ks, int j, int ldh, const double* __restrict__ sg, double* __restrict__ Lrows)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double* s = sg;
+    const double* g = sg + (j + 1);
+    for (int k = 0; k < j; k++) Lrows[(size_t)j * kGsMaxVec + k] = g[k];
+    double* H = ks->H + (size_t)j * ldh;
+    for (int i = 0; i <= j; i++) {
+        double h = s[i];
+        for (int k = 0; k < i; k++) h -= Lrows[(size_t)i * kGsMaxVec + k] * H[k];
+        H[i] = h;
+    }
+}
+
+// w -= sum_k h_k v_k (k <= j) and ||w||^2.
+template <int NV>
+__global__ void __launch_bounds__(256) k_gs_update(long long n, long long ld, int j, const double* __restrict__ V,
+                                                    const double* __restrict__ h, double* __restrict__ w,
+                                                    double* partial, unsigned int* counter, double* out)
+{
+    __shared__ double hs[NV];
+    if (threadIdx.x < NV) hs[threadIdx.x] = (threadIdx.x <= j) ? h[threadIdx.x] : 0.0;
+    __syncthreads();
+    double s[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        double acc = w[i];
+#pragma unroll
+        for (int k = 0; k < NV; k++)
+            if (k <= j) acc -= hs[k] * V[(size_t)k * ld + i];
+        w[i] = acc;
+        s[0] += acc * acc;
+    }
+    grid_reduce<1>(s, partial, counter, out);
 }
 
 }  // namespace lsg

@@ -181,12 +181,14 @@ struct Context {
     DevBuf<double> scal;      // misc device scalars (64)
     // Krylov storage
     int restart = 0;
+    long long ldv = 0;        // stride between basis vectors (n padded off a power of two)
     DevBuf<double> V, Z, w, xd, bd, coefs, t1, t2, t3, t4;
     DevBuf<KrylovScalars> ks;
     int* hflag = nullptr;
     double* hnorm = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DevBuf<float> Z32;        // FP32 preconditioned basis (FP32 multigrid)
+    DevBuf<double> gs_partial, gs_sg, gs_L;   // low-synchronisation Gram-Schmidt
     // ILU(0)
     DevBuf<double> iluL, iluU;        // 3 lower planes (b s w) / 4 planes (p e n t), U diagonal = plane 0
     bool have_ilu = false;
@@ -707,6 +709,29 @@ static void launch_givens(Context& C, int j)
     LSG_CHECK_LAUNCH();
 }
 
+// Low-synchronisation MGS for Arnoldi step j: one pass for V^T w and the new
+// row of V^T V, a triangular correction, one update pass (with ||w||^2).
+template <int NV>
+static void gs_lowsync_t(Context& C, int j, int gb, double* Hj)
+{
+    const long long n = C.n;
+    k_gs_dots<NV><<<gb, 256, 0, C.s>>>(n, C.ldv, j, C.V.p, C.w.p, C.gs_partial.p, C.red.counter.p, C.gs_sg.p);
+    LSG_CHECK_LAUNCH();
+    k_gs_tri<<<1, 32, 0, C.s>>>(C.ks.p, j, 65, C.gs_sg.p, C.gs_L.p);
+    LSG_CHECK_LAUNCH();
+    k_gs_update<NV><<<gb, 256, 0, C.s>>>(n, C.ldv, j, C.V.p, Hj, C.w.p, C.red.partial.p, C.red.counter.p,
+                                         &C.ks.p->normW2);
+    LSG_CHECK_LAUNCH();
+}
+
+static void gs_lowsync(Context& C, int j, int gb, double* Hj)
+{
+    if (j < 8) gs_lowsync_t<8>(C, j, gb, Hj);
+    else if (j < 16) gs_lowsync_t<16>(C, j, gb, Hj);
+    else if (j < 32) gs_lowsync_t<32>(C, j, gb, Hj);
+    else gs_lowsync_t<64>(C, j, gb, Hj);
+}
+
 static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
 {
     cudaStream_t s = C.s;
@@ -742,11 +767,11 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
         while (!finished) {
             int jlast = m - 1;
             for (int j = 0; j < m; j++) {
-                double* vj = C.V.p + (size_t)j * n;
-                double* zj = C.Z.p + (size_t)j * n;
+                double* vj = C.V.p + (size_t)j * C.ldv;
+                double* zj = C.Z.p + (size_t)j * C.ldv;
                 // v_j = w / ||w|| (also the preconditioner input)
                 const bool z32 = C.mg.fp32 && C.opt.precond == LSG_PC_MG;
-                float* zj32 = z32 ? C.Z32.p + (size_t)j * n : nullptr;
+                float* zj32 = z32 ? C.Z32.p + (size_t)j * C.ldv : nullptr;
                 if (z32) {
                     // the FP32 cycle writes z_j directly; it is kept in FP32
                     // (exactly representable in FP64, so the Arnoldi relation
@@ -771,14 +796,19 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
                                                            cnt, Hj);
                 LSG_CHECK_LAUNCH();
                 bytes += (3 * w8 + 4) * n;
-                // modified Gram-Schmidt: w -= h_i v_i ; h_{i+1} = (w, v_{i+1}); last: ||w||^2
-                for (int i = 1; i <= j + 1; i++) {
-                    const bool last = (i == j + 1);
-                    k_mgs_step<<<gb, 256, 0, s>>>(n, Hj + (i - 1), C.V.p + (size_t)(i - 1) * n,
-                                                 last ? C.w.p : C.V.p + (size_t)i * n, C.w.p, last, part, cnt,
-                                                 last ? &ks->normW2 : Hj + i);
-                    LSG_CHECK_LAUNCH();
-                    bytes += (last ? 3 : 4) * w8 * n;
+                if (C.opt.gram_schmidt == LSG_GS_LOWSYNC) {
+                    gs_lowsync(C, j, gb, Hj);
+                    bytes += (2.0 * j + 5.0) * w8 * n;
+                } else {
+                    // modified Gram-Schmidt: w -= h_i v_i ; h_{i+1} = (w, v_{i+1}); last: ||w||^2
+                    for (int i = 1; i <= j + 1; i++) {
+                        const bool last = (i == j + 1);
+                        k_mgs_step<<<gb, 256, 0, s>>>(n, Hj + (i - 1), C.V.p + (size_t)(i - 1) * C.ldv,
+                                                     last ? C.w.p : C.V.p + (size_t)i * C.ldv, C.w.p, last, part, cnt,
+                                                     last ? &ks->normW2 : Hj + i);
+                        LSG_CHECK_LAUNCH();
+                        bytes += (last ? 3 : 4) * w8 * n;
+                    }
                 }
                 launch_givens(C, j);
                 LSG_CUDA(cudaStreamSynchronize(s));
@@ -793,9 +823,9 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
             k_backsub<<<1, 32, 0, s>>>(ks, jlast, 65, C.coefs.p);
             LSG_CHECK_LAUNCH();
             if (C.mg.fp32 && C.opt.precond == LSG_PC_MG)
-                k_multi_axpy<float><<<grid_for(n, 256), 256, 0, s>>>(n, jlast + 1, C.coefs.p, C.Z32.p, x);
+                k_multi_axpy<float><<<grid_for(n, 256), 256, 0, s>>>(n, C.ldv, jlast + 1, C.coefs.p, C.Z32.p, x);
             else
-                k_multi_axpy<double><<<grid_for(n, 256), 256, 0, s>>>(n, jlast + 1, C.coefs.p, C.Z.p, x);
+                k_multi_axpy<double><<<grid_for(n, 256), 256, 0, s>>>(n, C.ldv, jlast + 1, C.coefs.p, C.Z.p, x);
             LSG_CHECK_LAUNCH();
             bytes += (jlast + 3) * w8 * n;
             const bool refine = (C.opt.mg_precision == LSG_FP32 && C.opt.precond == LSG_PC_MG);
@@ -902,9 +932,9 @@ static int bicgstab(Context& C, double* x, const double* b, lsg_stats* st)
     double* sc = C.scal.p + 24;   // 8 scalars
     double* r = C.w.p;
     double* rr = C.V.p;
-    double* p = C.V.p + n;
+    double* p = C.V.p + C.ldv;
     double* y = C.Z.p;
-    double* z = C.Z.p + n;
+    double* z = C.Z.p + C.ldv;
     double* nu = C.t1.p;
     double* sv = C.t2.p;
     double* t = C.t3.p;
@@ -960,12 +990,16 @@ static void krylov_alloc(Context& C)
     const long long n = C.n;
     const int m = std::max(2, std::min(C.opt.restart, 64));
     C.restart = m;
-    C.V.alloc((size_t)m * n);
+    // vectors n*8 bytes apart alias in the memory system when n is a power of
+    // two; an odd multiple of 256 bytes of padding spreads them
+    C.ldv = ((n + 31) / 32) * 32 + 96;
+    const long long ldv = C.ldv;
+    C.V.alloc((size_t)m * ldv);
     if (C.opt.mg_precision == LSG_FP32 && C.opt.precond == LSG_PC_MG && C.opt.method == LSG_METHOD_FGMRES) {
-        C.Z.alloc(2 * n);          // BiCGStab-sized scratch only
-        C.Z32.alloc((size_t)m * n);
+        C.Z.alloc(2 * ldv);        // BiCGStab-sized scratch only
+        C.Z32.alloc((size_t)m * ldv);
     } else {
-        C.Z.alloc((size_t)std::max(m, 2) * n);
+        C.Z.alloc((size_t)std::max(m, 2) * ldv);
         C.Z32.release();
     }
     C.w.alloc(n);
@@ -976,6 +1010,11 @@ static void krylov_alloc(Context& C)
     C.xd.alloc(n);
     C.bd.alloc(n);
     C.coefs.alloc(64);
+    if (C.opt.gram_schmidt == LSG_GS_LOWSYNC) {
+        C.gs_partial.alloc((size_t)Reducer::kMaxBlocks * 2 * kGsMaxVec);
+        C.gs_sg.alloc(2 * kGsMaxVec);
+        C.gs_L.alloc((size_t)kGsMaxVec * kGsMaxVec);
+    }
 }
 
 static double true_residual(Context& C, const double* x, const double* b)

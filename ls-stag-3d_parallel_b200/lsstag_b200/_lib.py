@@ -27,13 +27,14 @@ METHOD_FGMRES, METHOD_BICGSTAB = 0, 1
 PC_MG, PC_ILU0, PC_NONE = 0, 1, 2
 FP64, FP32 = 0, 1
 SMOOTHER_ADLJ, SMOOTHER_RBGS = 0, 1
+GS_MGS, GS_LOWSYNC = 0, 1
 
 
 class Options(C.Structure):
     _fields_ = [("method", C.c_int), ("precond", C.c_int), ("mg_precision", C.c_int), ("smoother", C.c_int),
                 ("n_pre", C.c_int), ("n_post", C.c_int), ("max_levels", C.c_int), ("restart", C.c_int),
                 ("max_it", C.c_int), ("zline_reference", C.c_int), ("eps", C.c_double), ("omega", C.c_double),
-                ("reserved", C.c_int * 8)]
+                ("gram_schmidt", C.c_int), ("reserved", C.c_int * 7)]
 
 
 class Stats(C.Structure):

@@ -81,6 +81,20 @@ def test_mg_fgmres_fp64(golden):
     s.close()
 
 
+def test_mg_fgmres_lowsync_gram_schmidt(golden):
+    """The low-synchronisation form of MGS computes the same projections:
+    iterations within +-1 and the FP64 solution within 1e-10."""
+    from lsstag_b200 import _lib as L
+    _, g = golden
+    s = _solver(g, gram_schmidt=L.GS_LOWSYNC)
+    x = np.zeros_like(g["b"])
+    it = s.solve(g["b"], x)
+    assert abs(it - int(g["fgmres_it"][0])) <= 1
+    ref = g["fgmres_x"]
+    assert np.linalg.norm(x - ref) <= 1e-10 * np.linalg.norm(ref)
+    s.close()
+
+
 def test_mg_fgmres_fp32_preconditioner(golden):
     """Mixed precision: FP32 V-cycle inside FP64 FGMRES with iterative
     refinement.  Stated tolerance: the FP64 true residual meets eps and the
