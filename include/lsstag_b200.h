@@ -129,6 +129,22 @@ int lsg_set_matrix_csr_device(lsg_ctx* ctx, int N, int M, int K, const int* rowp
    the grid must be 0.  Host pointer, 7*N*M*K doubles. */
 int lsg_set_matrix_stencil7(lsg_ctx* ctx, int N, int M, int K, const double* planes);
 
+/* Assemble the operator on the GPU from the cut-cell geometry, the
+   restatement of LaplaceDiscreteOperator::calcLap + fixPoint
+   (laplace_discrete_operator.h:107-686, :809-821): celltype[n] (CellTypes
+   codes, cut_cells.h:26-168), theta/delta[3n] (per-cell x,y,z face fractions
+   and cell sizes, the reference's coord<double> layout), inv_mx/my/mz the
+   inverse staggered masses on the x-grid ((N-1)MK), y-grid (N(M-1)K) and
+   z-grid (NM(K-1)) (LSSTAGUniformMesh xMesh/yMesh/zMesh inv_VOF), pin0/pin1
+   the two rows made identity (N-1 and NM-1 for the flow task).  Host
+   pointers.  The result is bit-identical to the reference's CSR values. */
+int lsg_set_matrix_geometry(lsg_ctx* ctx, int N, int M, int K, const int* celltype, const double* theta,
+                            const double* delta, const double* inv_mx, const double* inv_my, const double* inv_mz,
+                            long long pin0, long long pin1);
+/* Copy the current operator out as seven planes (layout of
+   lsg_set_matrix_stencil7).  Host pointer, 7*N*M*K doubles. */
+int lsg_get_matrix_stencil7(lsg_ctx* ctx, double* planes);
+
 /* Build the preconditioner for the current operator (multigrid hierarchy:
    MultiGridSolver::set multigrid_solver.h:76-101 / CoarseGrid::set
    coarse_grid.h:93-106; or ILU(0): ILUDecompositionSparseMatrix::decompose
@@ -150,6 +166,22 @@ int lsg_apply(lsg_ctx* ctx, const double* x, double* y);
    Host buffers; for the FP32 multigrid the result is the FP32 cycle rounded
    to FP64. */
 int lsg_precond_apply(lsg_ctx* ctx, const double* b, double* x);
+
+/* Adjoint (no counterpart in the reference, which has no adjoint; built for
+   gradient-based use of the pressure solve).
+   lsg_apply_transpose: y = A^T x, the transposed cut-cell stencil (row i of
+     A^T holds column i of A).
+   lsg_solve_adjoint: A^T lambda = g with the same method, preconditioner
+     construction and options as the forward solve, applied to A^T (the
+     multigrid hierarchy is rebuilt from A^T on first use); lambda holds the
+     initial guess on entry.  For J(x) with A x = b, dJ/db = lambda when
+     g = dJ/dx.
+   lsg_operator_gradient: grad[s*n + i] = -lambda_i x_{i + off_s} = dJ/dA for
+     the seven planes of lsg_set_matrix_stencil7 (0 toward outside cells).
+   Host buffers. */
+int lsg_apply_transpose(lsg_ctx* ctx, const double* x, double* y);
+int lsg_solve_adjoint(lsg_ctx* ctx, const double* g, double* lambda, lsg_stats* stats);
+int lsg_operator_gradient(lsg_ctx* ctx, const double* lambda, const double* x, double* grad);
 
 /* Multigrid introspection for parity checks.  Level 0 is the fine grid. */
 int lsg_mg_num_levels(const lsg_ctx* ctx);  /* coarse levels (GridLevels), or < 0 */

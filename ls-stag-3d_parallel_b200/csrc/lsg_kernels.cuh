@@ -985,3 +985,108 @@ __global__ void k_coarse_solve(int n, const double* __restrict__ L, const double
 }
 
 }  // namespace lsg
+
+namespace lsg {
+
+// ---------------------------------------------------------------------------
+// Cut-cell Laplace operator from the geometry (restatement of
+// LaplaceDiscreteOperator::calcLap, laplace_discrete_operator.h:107-686, and
+// fixPointFlow :809-821).  Face coefficient  a_f = (theta_f dS_f)^2 / M_f
+// with the face fraction of the shared face (west/south/bottom read from the
+// neighbour's east/north/top), 1/M from the staggered x/y/z grids; a fully
+// fluid cell uses dS_f^2 / M_f; the faces on the box walls named by a
+// boundary cell type are absent; diagonal = -(a_b + a_s + a_w + a_e + a_n +
+// a_t) summed in that order; a solid cell has only PLUS_TINY on the diagonal;
+// the two pinned rows become identity rows.  Planes: b s w p e n t.
+// Cell type codes (cut_cells.h): SolidCell 0, FluidCell 11111111, box
+// boundary types -2 .. -27.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int absent_faces(int type)
+{
+    // bit 0 b, 1 s, 2 w, 3 e, 4 n, 5 t
+    constexpr int B = 1, S = 2, W = 4, E = 8, Nn = 16, T = 32;
+    switch (type) {
+    case -2: return T;
+    case -3: return B;
+    case -4: return Nn;
+    case -5: return S;
+    case -6: return E;
+    case -7: return W;
+    case -8: return T | Nn;
+    case -9: return T | S;
+    case -10: return T | E;
+    case -11: return T | W;
+    case -12: return B | Nn;
+    case -13: return B | S;
+    case -14: return B | E;
+    case -15: return B | W;
+    case -16: return Nn | E;
+    case -17: return Nn | W;
+    case -18: return S | E;
+    case -19: return S | W;
+    case -20: return T | Nn | E;
+    case -21: return T | Nn | W;
+    case -22: return T | S | E;
+    case -23: return T | S | W;
+    case -24: return B | Nn | E;
+    case -25: return B | Nn | W;
+    case -26: return B | S | E;
+    case -27: return B | S | W;
+    default: return 0;
+    }
+}
+
+__global__ void k_laplace_from_geometry(int N, int M, int K, const int* __restrict__ type,
+                                        const double* __restrict__ theta, const double* __restrict__ delta,
+                                        const double* __restrict__ inv_mx, const double* __restrict__ inv_my,
+                                        const double* __restrict__ inv_mz, long long pin0, long long pin1,
+                                        double* __restrict__ planes)
+{
+    const long long n = (long long)N * M * K;
+    const long long NM = (long long)N * M;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        double a[7] = {0, 0, 0, 0, 0, 0, 0};
+        const int ty = type[i];
+        if (i == pin0 || i == pin1) {
+            a[3] = 1.0;
+        } else if (ty == 0) {
+            a[3] = 1e-16;                                   // PLUS_TINY
+        } else {
+            const int iz = (int)(i / NM);
+            const long long rem = i - (long long)iz * NM;
+            const int iy = (int)(rem / N);
+            const long long numX = i - iy - (long long)iz * M;   // x-grid cell east of i
+            const long long numY = i - (long long)iz * N;        // y-grid cell north of i
+            const double dx = delta[3 * i], dy = delta[3 * i + 1], dz = delta[3 * i + 2];
+            const double dyz = dy * dz, dxz = dx * dz, dxy = dx * dy;
+            const int miss = absent_faces(ty);
+            const bool fluid = (ty == 11111111);
+            double ab = 0, as = 0, aw = 0, ae = 0, an = 0, at = 0;
+            auto coef = [&](double th, double ds, double inv) {
+                const double aux = fluid ? ds : th * ds;
+                return aux * aux * inv;
+            };
+            if (!(miss & 1)) ab = coef(theta[3 * (i - NM) + 2], dxy, inv_mz[i - NM]);
+            if (!(miss & 2)) as = coef(theta[3 * (i - N) + 1], dxz, inv_my[numY - N]);
+            if (!(miss & 4)) aw = coef(theta[3 * (i - 1)], dyz, inv_mx[numX - 1]);
+            if (!(miss & 8)) ae = coef(theta[3 * i], dyz, inv_mx[numX]);
+            if (!(miss & 16)) an = coef(theta[3 * i + 1], dxz, inv_my[numY]);
+            if (!(miss & 32)) at = coef(theta[3 * i + 2], dxy, inv_mz[i]);
+            double dg = 0.0;
+            bool first = true;
+            const double vals[6] = {ab, as, aw, ae, an, at};
+#pragma unroll
+            for (int f = 0; f < 6; f++) {
+                if (miss & (1 << f)) continue;
+                dg = first ? -vals[f] : dg - vals[f];
+                first = false;
+            }
+            a[0] = ab; a[1] = as; a[2] = aw; a[3] = dg; a[4] = ae; a[5] = an; a[6] = at;
+        }
+#pragma unroll
+        for (int s = 0; s < 7; s++) planes[(size_t)s * n + i] = a[s];
+    }
+}
+
+}  // namespace lsg

@@ -194,6 +194,10 @@ struct Context {
     bool have_ilu = false;
     double bytes = 0;
     int vcycles = 0;
+    bool own_stream = true;
+    // adjoint: a second solver state for the transposed operator, built on
+    // first use and dropped whenever the operator changes
+    std::unique_ptr<Context> adj;
 };
 
 }  // namespace lsg
@@ -882,6 +886,58 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
 namespace lsg {
 
 // ---------------------------------------------------------------------------
+// adjoint pieces: transposed stencil, operator-coefficient gradient
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool nbr7(int s, int x, int y, int z, int N, int M, int K, long long& off, long long NM)
+{
+    switch (s) {
+    case 0: off = -NM; return z > 0;
+    case 1: off = -N; return y > 0;
+    case 2: off = -1; return x > 0;
+    case 3: off = 0; return true;
+    case 4: off = 1; return x < N - 1;
+    case 5: off = N; return y < M - 1;
+    default: off = NM; return z < K - 1;
+    }
+}
+
+// AT[s][i] = A[6-s][i + off_s]: row i of A^T holds column i of A (the
+// neighbour's coefficient pointing back, b<->t, s<->n, w<->e).
+__global__ void k_transpose7(int N, int M, int K, const double* __restrict__ A, double* __restrict__ AT)
+{
+    const long long n = (long long)N * M * K;
+    const long long NM = (long long)N * M;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        cell_xyz(i, N, (int)NM, x, y, z);
+        for (int sl = 0; sl < 7; sl++) {
+            long long off;
+            const bool ok = nbr7(sl, x, y, z, N, M, K, off, NM);
+            AT[(size_t)sl * n + i] = ok ? A[(size_t)(6 - sl) * n + i + off] : 0.0;
+        }
+    }
+}
+
+// grad[s][i] = -lambda_i x_{i+off_s}: dJ/dA for J(x(A)) with A^T lambda = dJ/dx
+__global__ void k_operator_grad7(int N, int M, int K, const double* __restrict__ lam, const double* __restrict__ x,
+                                 double* __restrict__ grad)
+{
+    const long long n = (long long)N * M * K;
+    const long long NM = (long long)N * M;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int xx, y, z;
+        cell_xyz(i, N, (int)NM, xx, y, z);
+        for (int sl = 0; sl < 7; sl++) {
+            long long off;
+            const bool ok = nbr7(sl, xx, y, z, N, M, K, off, NM);
+            grad[(size_t)sl * n + i] = ok ? -lam[i] * x[i + off] : 0.0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // ILU(0): pivots by hyperplane sweeps, level-scheduled solves in a CUDA graph
 // ---------------------------------------------------------------------------
 
@@ -1054,6 +1110,71 @@ static int solve_device(Context& C, const double* b, double* x, lsg_stats* st)
     return rc;
 }
 
+static void context_init(Context& C, int device, cudaStream_t stream)
+{
+    C.device = device;
+    LSG_CUDA(cudaSetDevice(device));
+    if (stream) {
+        C.s = stream;
+        C.own_stream = false;
+    } else {
+        LSG_CUDA(cudaStreamCreateWithFlags(&C.s, cudaStreamNonBlocking));
+        C.own_stream = true;
+    }
+    LSG_CUDA(cudaEventCreate(&C.ev0));
+    LSG_CUDA(cudaEventCreate(&C.ev1));
+    C.red.init();
+    C.scal.alloc(64);
+    LSG_CUDA(cudaMemset(C.scal.p, 0, C.scal.bytes()));
+    C.ks.alloc(1);
+    LSG_CUDA(cudaHostAlloc((void**)&C.hflag, 64, cudaHostAllocMapped));
+    C.hnorm = (double*)((char*)C.hflag + 8);
+    lsg_default_options(&C.opt);
+}
+
+// Frees what the DevBuf members do not own; returns the stream to destroy.
+static cudaStream_t context_release(Context& C)
+{
+    if (C.adj) {
+        context_release(*C.adj);
+        C.adj.reset();
+    }
+    if (C.s) cudaStreamSynchronize(C.s);
+    if (C.hflag) cudaFreeHost(C.hflag);
+    C.hflag = nullptr;
+    if (C.ev0) cudaEventDestroy(C.ev0);
+    if (C.ev1) cudaEventDestroy(C.ev1);
+    C.ev0 = C.ev1 = nullptr;
+    return C.own_stream ? C.s : nullptr;
+}
+
+// The transposed operator's solver state, with the forward solver's options.
+static Context& adjoint_context(Context& C)
+{
+    LSG_REQUIRE(C.have_setup, LSG_ERR_STATE, "lsg_setup must be called before the adjoint");
+    if (!C.adj) {
+        std::unique_ptr<Context> a(new Context);
+        context_init(*a, C.device, C.s);
+        a->d = C.d;
+        a->n = C.n;
+        a->A7.alloc(7 * C.n);
+        k_transpose7<<<grid_for(C.n, 256), 256, 0, C.s>>>(C.d.N, C.d.M, C.d.K, C.A7.p, a->A7.p);
+        LSG_CHECK_LAUNCH();
+        a->nclass0 = build_dict(C.s, a->A7.p, 7, C.n, a->cls0, a->dict0);
+        a->have_matrix = true;
+        C.adj = std::move(a);
+    }
+    Context& A = *C.adj;
+    if (!A.have_setup || std::memcmp(&A.opt, &C.opt, sizeof(lsg_options)) != 0) {
+        A.opt = C.opt;
+        if (A.opt.precond == LSG_PC_MG) mg_setup(A);
+        if (A.opt.precond == LSG_PC_ILU0) ilu_setup(A);
+        krylov_alloc(A);
+        A.have_setup = true;
+    }
+    return A;
+}
+
 }  // namespace lsg
 
 // ===========================================================================
@@ -1104,41 +1225,24 @@ int lsg_create(int device, lsg_ctx** out)
     *out = nullptr;
     lsg_ctx* h = new (std::nothrow) lsg_ctx;
     if (!h) return LSG_ERR_NOMEM;
-    LSG_API_BEGIN
-    Context& C = h->c;
-    C.device = device;
-    LSG_CUDA(cudaSetDevice(device));
-    LSG_CUDA(cudaStreamCreateWithFlags(&C.s, cudaStreamNonBlocking));
-    LSG_CUDA(cudaEventCreate(&C.ev0));
-    LSG_CUDA(cudaEventCreate(&C.ev1));
-    C.red.init();
-    C.scal.alloc(64);
-    LSG_CUDA(cudaMemset(C.scal.p, 0, C.scal.bytes()));
-    C.ks.alloc(1);
-    LSG_CUDA(cudaHostAlloc((void**)&C.hflag, 64, cudaHostAllocMapped));
-    C.hnorm = (double*)((char*)C.hflag + 8);
-    lsg_default_options(&C.opt);
-    *out = h;
-    return LSG_OK;
-    }
-    catch (const lsg::Error& e)
-    {
+    try {
+        context_init(h->c, device, nullptr);
+    } catch (const lsg::Error& e) {
         fprintf(stderr, "lsg_create: %s\n", e.msg.c_str());
+        cudaStream_t s = context_release(h->c);
         delete h;
+        if (s) cudaStreamDestroy(s);
         return e.code;
     }
+    *out = h;
+    return LSG_OK;
 }
 
 int lsg_destroy(lsg_ctx* h)
 {
     if (!h) return LSG_OK;
-    Context& C = h->c;
-    cudaSetDevice(C.device);
-    if (C.s) cudaStreamSynchronize(C.s);
-    if (C.hflag) cudaFreeHost(C.hflag);
-    if (C.ev0) cudaEventDestroy(C.ev0);
-    if (C.ev1) cudaEventDestroy(C.ev1);
-    cudaStream_t s = C.s;
+    cudaSetDevice(h->c.device);
+    cudaStream_t s = context_release(h->c);
     delete h;   // DevBuf destructors free device memory
     if (s) cudaStreamDestroy(s);
     return LSG_OK;
@@ -1192,6 +1296,10 @@ static int set_matrix_impl(lsg_ctx* h, int N, int M, int K, const int* rowptr, c
                                          " holds an entry that is not the cell or one of its six face neighbours"};
     }
     C.nclass0 = build_dict(C.s, C.A7.p, 7, n, C.cls0, C.dict0);
+    if (C.adj) {
+        context_release(*C.adj);
+        C.adj.reset();
+    }
     C.have_matrix = true;
     C.have_setup = false;
     return LSG_OK;
@@ -1232,8 +1340,72 @@ int lsg_set_matrix_stencil7(lsg_ctx* h, int N, int M, int K, const double* plane
     LSG_CUDA(cudaMemcpyAsync(C.A7.p, planes, 7 * n * sizeof(double), cudaMemcpyHostToDevice, C.s));
     LSG_CUDA(cudaStreamSynchronize(C.s));
     C.nclass0 = build_dict(C.s, C.A7.p, 7, n, C.cls0, C.dict0);
+    if (C.adj) {
+        context_release(*C.adj);
+        C.adj.reset();
+    }
     C.have_matrix = true;
     C.have_setup = false;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_set_matrix_geometry(lsg_ctx* h, int N, int M, int K, const int* celltype, const double* theta,
+                            const double* delta, const double* inv_mx, const double* inv_my, const double* inv_mz,
+                            long long pin0, long long pin1)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(N >= 2 && M >= 2 && K >= 2, LSG_ERR_ARG, "grid dimensions must be >= 2");
+    LSG_REQUIRE(celltype && theta && delta && inv_mx && inv_my && inv_mz, LSG_ERR_ARG, "null geometry array");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const long long n = (long long)N * M * K;
+    LSG_REQUIRE(n < (1LL << 31), LSG_ERR_ARG, "grid too large");
+    const long long nx = (long long)(N - 1) * M * K, ny = (long long)N * (M - 1) * K, nz = (long long)N * M * (K - 1);
+    DevBuf<int> dt;
+    DevBuf<double> dth, dde, dmx, dmy, dmz;
+    dt.alloc(n);
+    dth.alloc(3 * n);
+    dde.alloc(3 * n);
+    dmx.alloc(nx);
+    dmy.alloc(ny);
+    dmz.alloc(nz);
+    LSG_CUDA(cudaMemcpyAsync(dt.p, celltype, n * sizeof(int), cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dth.p, theta, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dde.p, delta, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dmx.p, inv_mx, nx * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dmy.p, inv_my, ny * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dmz.p, inv_mz, nz * 8, cudaMemcpyHostToDevice, C.s));
+    C.d.N = N;
+    C.d.M = M;
+    C.d.K = K;
+    C.n = n;
+    C.A7.alloc(7 * n);
+    k_laplace_from_geometry<<<grid_for(n, 256), 256, 0, C.s>>>(N, M, K, dt.p, dth.p, dde.p, dmx.p, dmy.p, dmz.p,
+                                                              pin0, pin1, C.A7.p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    C.nclass0 = build_dict(C.s, C.A7.p, 7, n, C.cls0, C.dict0);
+    if (C.adj) {
+        context_release(*C.adj);
+        C.adj.reset();
+    }
+    C.have_matrix = true;
+    C.have_setup = false;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_get_matrix_stencil7(lsg_ctx* h, double* planes)
+{
+    if (!h || !planes) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.have_matrix, LSG_ERR_STATE, "no operator set");
+    LSG_CUDA(cudaSetDevice(C.device));
+    LSG_CUDA(cudaMemcpyAsync(planes, C.A7.p, 7 * C.n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
     return LSG_OK;
     LSG_API_END(h)
 }
@@ -1428,6 +1600,72 @@ int lsg_mg_level_tridiag(lsg_ctx* h, int level, char dir, double* c, double* d, 
             c[pos] = lo[nat(pos + 1)];
         }
     }
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_apply_transpose(lsg_ctx* h, const double* x, double* y)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.have_matrix, LSG_ERR_STATE, "no operator set");
+    LSG_REQUIRE(x && y, LSG_ERR_ARG, "null vector");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const long long n = C.n;
+    DevBuf<double> AT, dx, dy;
+    AT.alloc(7 * n);
+    dx.alloc(n);
+    dy.alloc(n);
+    k_transpose7<<<grid_for(n, 256), 256, 0, C.s>>>(C.d.N, C.d.M, C.d.K, C.A7.p, AT.p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaMemcpyAsync(dx.p, x, n * 8, cudaMemcpyHostToDevice, C.s));
+    k_apply7<double, 1><<<grid_for(n, 256), 256, 0, C.s>>>(C.d.N, C.d.M, C.d.K, AT.p, dx.p, dy.p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaMemcpyAsync(y, dy.p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_solve_adjoint(lsg_ctx* h, const double* g, double* lambda, lsg_stats* st)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(g && lambda, LSG_ERR_ARG, "null vector");
+    LSG_CUDA(cudaSetDevice(C.device));
+    Context& A = adjoint_context(C);
+    if (st) std::memset(st, 0, sizeof(*st));
+    const size_t bytes = (size_t)A.n * sizeof(double);
+    LSG_CUDA(cudaMemcpyAsync(A.bd.p, g, bytes, cudaMemcpyHostToDevice, A.s));
+    LSG_CUDA(cudaMemcpyAsync(A.xd.p, lambda, bytes, cudaMemcpyHostToDevice, A.s));
+    const int rc = solve_device(A, A.bd.p, A.xd.p, st);
+    LSG_CUDA(cudaMemcpyAsync(lambda, A.xd.p, bytes, cudaMemcpyDeviceToHost, A.s));
+    LSG_CUDA(cudaStreamSynchronize(A.s));
+    return rc;
+    LSG_API_END(h)
+}
+
+int lsg_operator_gradient(lsg_ctx* h, const double* lambda, const double* x, double* grad)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.have_matrix, LSG_ERR_STATE, "no operator set");
+    LSG_REQUIRE(lambda && x && grad, LSG_ERR_ARG, "null vector");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const long long n = C.n;
+    DevBuf<double> dl, dx, dg;
+    dl.alloc(n);
+    dx.alloc(n);
+    dg.alloc(7 * n);
+    LSG_CUDA(cudaMemcpyAsync(dl.p, lambda, n * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dx.p, x, n * 8, cudaMemcpyHostToDevice, C.s));
+    k_operator_grad7<<<grid_for(n, 256), 256, 0, C.s>>>(C.d.N, C.d.M, C.d.K, dl.p, dx.p, dg.p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaMemcpyAsync(grad, dg.p, 7 * n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
     return LSG_OK;
     LSG_API_END(h)
 }

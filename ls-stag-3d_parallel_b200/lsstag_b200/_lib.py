@@ -48,7 +48,9 @@ EXPORTS = [
     "lsg_default_options", "lsg_create", "lsg_destroy", "lsg_last_error", "lsg_set_matrix_csr",
     "lsg_set_matrix_csr_device", "lsg_set_matrix_stencil7", "lsg_setup", "lsg_solve", "lsg_solve_device", "lsg_apply",
     "lsg_precond_apply", "lsg_mg_num_levels", "lsg_mg_level_dims", "lsg_mg_level_csr",
-    "lsg_mg_level_tridiag", "lsg_profile_kernel", "lsg_residual_norm_noalloc", "lsg_version",
+    "lsg_mg_level_tridiag", "lsg_profile_kernel", "lsg_residual_norm_noalloc", "lsg_apply_transpose",
+    "lsg_solve_adjoint", "lsg_operator_gradient", "lsg_set_matrix_geometry", "lsg_get_matrix_stencil7",
+    "lsg_version",
 ]
 
 _lib = None
@@ -91,6 +93,12 @@ def load() -> C.CDLL:
     lib.lsg_mg_level_tridiag.argtypes = [P, C.c_int, C.c_char, dp, dp, dp]
     lib.lsg_profile_kernel.argtypes = [P, C.c_int, C.c_int, dp, dp]
     lib.lsg_residual_norm_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, P, P, P, P, P, P]
+    lib.lsg_apply_transpose.argtypes = [P, dp, dp]
+    lib.lsg_solve_adjoint.argtypes = [P, dp, dp, C.POINTER(Stats)]
+    lib.lsg_operator_gradient.argtypes = [P, dp, dp, dp]
+    lib.lsg_set_matrix_geometry.argtypes = [P, C.c_int, C.c_int, C.c_int, ip, dp, dp, dp, dp, dp, C.c_longlong,
+                                            C.c_longlong]
+    lib.lsg_get_matrix_stencil7.argtypes = [P, dp]
     lib.lsg_version.restype = C.c_char_p
     _lib = lib
     return lib

@@ -81,6 +81,30 @@ class IterativeSolver:
         self.ctx.check(self.ctx.lib.lsg_set_matrix_stencil7(self.ctx.h, N, M, K, L.dptr(self._planes)))
         self._setup()
 
+    def set_geometry(self, geom: dict, dims, pins, task: Task | None = None, setup: bool = True):
+        """Same as set() with the operator assembled on the GPU from the
+        cut-cell geometry (celltype, theta, delta, inv_mx, inv_my, inv_mz)."""
+        self.task = task or Task()
+        self.eps = float(self.task.eps)
+        g = {k: np.ascontiguousarray(geom[k], dtype=np.float64) for k in ("theta", "delta", "inv_mx", "inv_my",
+                                                                          "inv_mz")}
+        ct = np.ascontiguousarray(geom["celltype"], dtype=np.int32)
+        self._geom = (g, ct)
+        self.dims = tuple(int(v) for v in dims)
+        N, M, K = self.dims
+        self.ctx.check(self.ctx.lib.lsg_set_matrix_geometry(self.ctx.h, N, M, K, L.iptr(ct), L.dptr(g["theta"]),
+                                                            L.dptr(g["delta"]), L.dptr(g["inv_mx"]),
+                                                            L.dptr(g["inv_my"]), L.dptr(g["inv_mz"]),
+                                                            int(pins[0]), int(pins[1])))
+        if setup:
+            self._setup()
+
+    def planes(self) -> np.ndarray:
+        n = int(np.prod(self.dims))
+        P = np.empty((7, n))
+        self.ctx.check(self.ctx.lib.lsg_get_matrix_stencil7(self.ctx.h, L.dptr(P)))
+        return P
+
     def options(self) -> L.Options:
         return L.default_options(method=self.method, precond=self.precond, mg_precision=self.mg_precision,
                                  restart=int(self.task.FGMRES_RESTART_NUM), max_it=int(self.task.MAX_ITER),
@@ -125,6 +149,28 @@ class IterativeSolver:
         self.ctx.check(self.ctx.lib.lsg_precond_apply(self.ctx.h, L.dptr(np.ascontiguousarray(b, dtype=np.float64)),
                                                       L.dptr(x)))
         return x
+
+    # -- adjoint --------------------------------------------------------------
+    def apply_transpose(self, x: np.ndarray) -> np.ndarray:
+        y = np.empty(x.size, dtype=np.float64)
+        self.ctx.check(self.ctx.lib.lsg_apply_transpose(self.ctx.h, L.dptr(np.ascontiguousarray(x, dtype=np.float64)),
+                                                        L.dptr(y)))
+        return y
+
+    def solve_adjoint(self, g: np.ndarray, lam: np.ndarray | None = None) -> np.ndarray:
+        """lambda with A^T lambda = g (same method/preconditioner on A^T)."""
+        lam = np.zeros(g.size) if lam is None else lam
+        self.adj_stats = L.Stats()
+        self.ctx.check(self.ctx.lib.lsg_solve_adjoint(self.ctx.h, L.dptr(np.ascontiguousarray(g, dtype=np.float64)),
+                                                      L.dptr(lam), L.C.byref(self.adj_stats)))
+        return lam
+
+    def operator_gradient(self, lam: np.ndarray, x: np.ndarray) -> np.ndarray:
+        """dJ/dA over the seven coefficient planes: -lambda_i x_{i+off}."""
+        g = np.empty((7, x.size))
+        self.ctx.check(self.ctx.lib.lsg_operator_gradient(self.ctx.h, L.dptr(np.ascontiguousarray(lam)),
+                                                          L.dptr(np.ascontiguousarray(x)), L.dptr(g)))
+        return g
 
     def num_levels(self) -> int:
         return self.ctx.check(self.ctx.lib.lsg_mg_num_levels(self.ctx.h))

@@ -134,5 +134,5 @@ def csr_to_planes(rowptr, col, val, dims) -> np.ndarray:
     if np.any(slot < 0):
         raise ValueError("not a 7-point operator")
     P = np.zeros((7, n))
-    np.add.at(P, (slot, rows), val)
+    P[slot, rows] = val          # assignment keeps the sign of a stored -0.0
     return P

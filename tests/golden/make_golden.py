@@ -54,6 +54,8 @@ def main():
         r = rr.run(case, b, threads=1, fgmres=1, bicgstab=1, dump_mg=1, dump_geometry=0,
                    restart=30, rel_tol=1e-10, max_it=200)
         keep = {"dims": np.array(dims), "A_rowptr": rp, "A_col": col, "A_val": val,
+                "theta": g["theta"], "delta": g["delta"], "inv_mx": g["inv_mx"], "inv_my": g["inv_my"],
+                "inv_mz": g["inv_mz"], "flux": g["flux"],
                 "pins": g["pins"], "celltype": g["celltype"], "b": b, "eps": r["eps"],
                 "vcycle_x": r["vcycle_x"], "fgmres_x": r["fgmres_x"], "fgmres_it": r["fgmres_it"],
                 "fgmres_norm_r": r["fgmres_norm_r"], "bicgstab_x": r["bicgstab_x"],
