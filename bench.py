@@ -191,9 +191,10 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--restart", type=int, default=30, help="FGMRES restart length (30 = the measured workload)")
-    ap.add_argument("--gs", default="mgs", choices=["mgs", "lowsync"],
-                    help="Gram-Schmidt form: the reference's pass-per-vector MGS (default) or the "
-                         "low-synchronisation form of the same projections")
+    ap.add_argument("--gs", default="lowsync", choices=["mgs", "lowsync"],
+                    help="Gram-Schmidt form of both arms: the low-synchronisation form of the MGS "
+                         "projections (default; two passes over the basis per step) or the reference's "
+                         "pass-per-vector MGS")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
     world, rank, local, pg = dist_setup(args)

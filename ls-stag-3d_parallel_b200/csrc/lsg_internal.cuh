@@ -143,13 +143,14 @@ struct Hierarchy {
 // reductions: deterministic two-stage (block partials + last-block sum)
 // ---------------------------------------------------------------------------
 struct Reducer {
-    static constexpr int kMaxBlocks = 2048;
+    static constexpr int kMaxBlocks = 2048;   // default grid cap of the one-thread-per-cell kernels
+    static constexpr int kCapBlocks = 8192;   // most blocks any reducing launch may use
     static constexpr int kSlots = 4;
-    DevBuf<double> partial;       // kMaxBlocks * kSlots
+    DevBuf<double> partial;       // kCapBlocks * kSlots
     DevBuf<unsigned int> counter; // one per concurrent reduction site
     void init()
     {
-        partial.alloc((size_t)kMaxBlocks * kSlots);
+        partial.alloc((size_t)kCapBlocks * kSlots);
         counter.alloc(64);
         LSG_CUDA(cudaMemset(counter.p, 0, counter.bytes()));
     }

@@ -19,13 +19,55 @@ struct OffList {
     signed char o[125][3];
 };
 
+// Cell coordinates of a flat index (x fastest).  Grids hold fewer than 2^31
+// cells, so 32-bit unsigned division suffices.
 __device__ __forceinline__ void cell_xyz(long long i, int N, int NM, int& x, int& y, int& z)
 {
-    z = (int)(i / NM);
-    int r = (int)(i - (long long)z * NM);
-    y = r / N;
-    x = r - y * N;
+    const unsigned u = (unsigned)i;
+    z = (int)(u / (unsigned)NM);
+    const unsigned r = u - (unsigned)z * (unsigned)NM;
+    y = (int)(r / (unsigned)N);
+    x = (int)(r - (unsigned)y * (unsigned)N);
 }
+
+// Division by a run-time invariant d >= 1 of numerators below 2^31 by one
+// multiply-high and shifts (Granlund & Montgomery, "Division by invariant
+// integers using multiplication", PLDI 1994, fig. 4.1):
+//   l = ceil(log2 d),  m = floor(2^32 (2^l - d) / d) + 1,
+//   t = mulhi(m, n),   q = (t + ((n - t) >> min(l,1))) >> max(l-1,0).
+// Built once per thread, used for every cell the thread visits.
+struct FDiv {
+    unsigned d, m;
+    int s1, s2;
+    __device__ explicit FDiv(unsigned dd) : d(dd)
+    {
+        int l = 0;
+        while (l < 31 && (1u << l) < dd) l++;
+        m = (unsigned)((((unsigned long long)((1ull << l) - dd)) << 32) / dd + 1);
+        s1 = l < 1 ? l : 1;
+        s2 = l - 1 > 0 ? l - 1 : 0;
+    }
+    __device__ __forceinline__ unsigned div(unsigned n) const
+    {
+        const unsigned t = __umulhi(m, n);
+        return (t + ((n - t) >> s1)) >> s2;
+    }
+};
+
+struct CellIndex {
+    FDiv dN, dNM;
+    __device__ CellIndex(int N, int NM) : dN((unsigned)N), dNM((unsigned)NM) {}
+    __device__ __forceinline__ void xyz(long long i, int& x, int& y, int& z) const
+    {
+        const unsigned u = (unsigned)i;
+        const unsigned zz = dNM.div(u);
+        const unsigned r = u - zz * dNM.d;
+        const unsigned yy = dN.div(r);
+        z = (int)zz;
+        y = (int)yy;
+        x = (int)(r - yy * dN.d);
+    }
+};
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v)
@@ -37,39 +79,54 @@ __device__ __forceinline__ T warp_sum(T v)
 
 // Deterministic block + grid reduction of NS values.  Every block writes its
 // partial sums; the last block to finish adds them in block order and writes
-// out[s].  blockDim.x must be a multiple of 32 and <= 1024.
+// out[s].  Blocks of 1-3 dimensions with a multiple of 32 threads (<= 1024),
+// grids of 1-3 dimensions; blocks and threads are taken in linear order.
 template <int NS>
 __device__ void grid_reduce(double (&v)[NS], double* partial, unsigned int* counter, double* out)
 {
     __shared__ double sh[32][NS];
     __shared__ bool last;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthr = blockDim.x * blockDim.y * blockDim.z;
+    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
+    const int lane = tid & 31, wid = tid >> 5, nw = nthr >> 5;
 #pragma unroll
     for (int s = 0; s < NS; s++) {
         double t = warp_sum(v[s]);
         if (lane == 0) sh[wid][s] = t;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
 #pragma unroll
         for (int s = 0; s < NS; s++) {
             double t = 0.0;
             for (int w = 0; w < nw; w++) t += sh[w][s];
-            partial[(size_t)blockIdx.x * NS + s] = t;
+            partial[(size_t)bid * NS + s] = t;
         }
         __threadfence();
         unsigned int prev = atomicAdd(counter, 1u);
-        last = (prev == gridDim.x - 1);
+        last = (prev == nblk - 1);
     }
     __syncthreads();
     if (!last) return;
     __threadfence();
+    // partials read past L1 (__ldcg), two blocks per step so loads overlap
     double acc[NS];
 #pragma unroll
     for (int s = 0; s < NS; s++) acc[s] = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+    int b = tid;
+    for (; b + nthr < (int)nblk; b += 2 * nthr) {
 #pragma unroll
-        for (int s = 0; s < NS; s++) acc[s] += ((volatile double*)partial)[(size_t)b * NS + s];
+        for (int s = 0; s < NS; s++) {
+            const double p0 = __ldcg(partial + (size_t)b * NS + s);
+            const double p1 = __ldcg(partial + (size_t)(b + nthr) * NS + s);
+            acc[s] += p0 + p1;
+        }
+    }
+    for (; b < (int)nblk; b += nthr) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) acc[s] += __ldcg(partial + (size_t)b * NS + s);
     }
 #pragma unroll
     for (int s = 0; s < NS; s++) {
@@ -77,7 +134,7 @@ __device__ void grid_reduce(double (&v)[NS], double* partial, unsigned int* coun
         if (lane == 0) sh[wid][s] = t;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
 #pragma unroll
         for (int s = 0; s < NS; s++) {
             double t = 0.0;
@@ -310,50 +367,103 @@ __global__ void __launch_bounds__(256) k_apply27d(int N, int M, int K, const int
 // ones on coarse levels (parallelism).
 inline int zchunk_for(long long n) { return n >= (8LL << 20) ? 16 : (n >= (1LL << 20) ? 4 : 2); }
 
+// 7-point apply marching along z: a thread owns one (x, y) column of a
+// z-chunk and keeps x at z-1, z, z+1 in registers.  The loads of U z-steps
+// (class index, r, the four lateral neighbours and the next plane) are all
+// issued before the arithmetic of those steps, so each thread has U cells of
+// loads in flight.  Terms are summed p, b, s, w, e, n, t.
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) k_apply7z(int N, int M, int K, int zc, const int* __restrict__ cls,
                                                   const T* __restrict__ dict, const T* __restrict__ x,
                                                   T* __restrict__ r)
 {
+    constexpr int U = 4;
     const int ix = blockIdx.x * 32 + threadIdx.x;
     const int iy = blockIdx.y * 8 + threadIdx.y;
     if (ix >= N || iy >= M) return;
-    const long long NM = (long long)N * M;
+    const int NM = N * M;                                  // grids hold fewer than 2^31 cells
     const int z0 = blockIdx.z * zc;
     const int z1 = min(z0 + zc, K);
-    long long i = ix + (long long)N * iy + NM * z0;
+    int i = ix + N * iy + NM * z0;
     T xm = (z0 > 0) ? x[i - NM] : (T)0;
     T xc = x[i];
     const bool hasw = ix > 0, hase = ix < N - 1, hass = iy > 0, hasn = iy < M - 1;
-    for (int z = z0; z < z1; z++, i += NM) {
-        const T xp = (z < K - 1) ? x[i + NM] : (T)0;
-        const T* a = dict + (size_t)cls[i] * 7;
-        T acc = a[3] * xc;
-        acc += a[0] * xm;          // zero coefficient below the bottom wall
-        if (hass) acc += a[1] * x[i - N];
-        if (hasw) acc += a[2] * x[i - 1];
-        if (hase) acc += a[4] * x[i + 1];
-        if (hasn) acc += a[5] * x[i + N];
-        acc += a[6] * xp;
-        if (MODE == 0) r[i] -= acc;
-        else r[i] = acc;
-        xm = xc;
-        xc = xp;
+    for (int zb = z0; zb < z1; zb += U, i += U * NM) {
+        int cl[U];
+        T rv[U], xs[U], xw[U], xe[U], xn[U], xp[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int z = zb + u;
+            const int ii = (z < z1) ? i + u * NM : i;       // steps past the chunk reload a valid cell
+            cl[u] = cls[ii];
+            rv[u] = (MODE == 0) ? r[ii] : (T)0;
+            xs[u] = hass ? x[ii - N] : (T)0;
+            xw[u] = hasw ? x[ii - 1] : (T)0;
+            xe[u] = hase ? x[ii + 1] : (T)0;
+            xn[u] = hasn ? x[ii + N] : (T)0;
+            xp[u] = (z < K - 1) ? x[ii + NM] : (T)0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (zb + u < z1) {
+                const T* a = dict + (size_t)cl[u] * 7;
+                T acc = a[3] * xc;
+                acc += a[0] * xm;          // zero coefficient below the bottom wall
+                if (hass) acc += a[1] * xs[u];
+                if (hasw) acc += a[2] * xw[u];
+                if (hase) acc += a[4] * xe[u];
+                if (hasn) acc += a[5] * xn[u];
+                acc += a[6] * xp[u];
+                const int ii = i + u * NM;
+                if (MODE == 0) r[ii] = rv[u] - acc;
+                else r[ii] = acc;
+                xm = xc;
+                xc = xp[u];
+            }
+        }
     }
 }
 
+// Row of 27 coefficients stored with stride 28, read as 16-byte vectors.
+template <typename T>
+__device__ __forceinline__ void load_row28(const T* __restrict__ p, T (&a)[28])
+{
+    if constexpr (sizeof(T) == 4) {
+        const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+        for (int k = 0; k < 7; k++) {
+            const float4 v = __ldg(q + k);
+            a[4 * k] = v.x;
+            a[4 * k + 1] = v.y;
+            a[4 * k + 2] = v.z;
+            a[4 * k + 3] = v.w;
+        }
+    } else {
+        const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+        for (int k = 0; k < 14; k++) {
+            const double2 v = __ldg(q + k);
+            a[2 * k] = v.x;
+            a[2 * k + 1] = v.y;
+        }
+    }
+}
+
+// 27-point apply (Galerkin levels) marching along z.  dict28 holds each
+// distinct row with stride 28 (the 27 box coefficients in z, y, x order and a
+// zero), so a row is seven (FP32) or fourteen (FP64) vector loads.
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) k_apply27z(int N, int M, int K, int zc, const int* __restrict__ cls,
-                                                   const T* __restrict__ dict, const T* __restrict__ x,
+                                                   const T* __restrict__ dict28, const T* __restrict__ x,
                                                    T* __restrict__ r)
 {
     const int ix = blockIdx.x * 32 + threadIdx.x;
     const int iy = blockIdx.y * 8 + threadIdx.y;
     if (ix >= N || iy >= M) return;
-    const long long NM = (long long)N * M;
+    const int NM = N * M;                                  // grids hold fewer than 2^31 cells
     const int z0 = blockIdx.z * zc;
     const int z1 = min(z0 + zc, K);
-    const long long col = ix + (long long)N * iy;
+    const int col = ix + N * iy;
     bool ok[9];
     int off[9];
 #pragma unroll
@@ -367,15 +477,25 @@ __global__ void __launch_bounds__(256) k_apply27z(int N, int M, int K, int zc, c
     // plane values of the 3x3 column neighbourhood at z-1, z, z+1
     T pm[9], pc[9], pp[9];
     auto load_plane = [&](int z, T* p) {
+        const bool zin = z >= 0 && z < K;
 #pragma unroll
-        for (int q = 0; q < 9; q++) p[q] = (z >= 0 && z < K && ok[q]) ? x[col + NM * z + off[q]] : (T)0;
+        for (int q = 0; q < 9; q++) p[q] = (zin && ok[q]) ? x[col + NM * z + off[q]] : (T)0;
     };
     load_plane(z0 - 1, pm);
     load_plane(z0, pc);
+    int cn = cls[col + NM * z0];
+    T rn = (MODE == 0) ? r[col + NM * z0] : (T)0;
     for (int z = z0; z < z1; z++) {
+        const int i = col + NM * z;
+        const int cl = cn;
+        const T rv = rn;
         load_plane(z + 1, pp);
-        const long long i = col + NM * z;
-        const T* a = dict + (size_t)cls[i] * 27;
+        if (z + 1 < z1) {                                  // next step's class and residual, one step ahead
+            cn = cls[i + NM];
+            if (MODE == 0) rn = r[i + NM];
+        }
+        T a[28];
+        load_row28(dict28 + (size_t)cl * 28, a);
         T acc = 0;
 #pragma unroll
         for (int q = 0; q < 9; q++) acc += a[q] * pm[q];
@@ -383,13 +503,23 @@ __global__ void __launch_bounds__(256) k_apply27z(int N, int M, int K, int zc, c
         for (int q = 0; q < 9; q++) acc += a[9 + q] * pc[q];
 #pragma unroll
         for (int q = 0; q < 9; q++) acc += a[18 + q] * pp[q];
-        if (MODE == 0) r[i] -= acc;
+        if (MODE == 0) r[i] = rv - acc;
         else r[i] = acc;
 #pragma unroll
         for (int q = 0; q < 9; q++) {
             pm[q] = pc[q];
             pc[q] = pp[q];
         }
+    }
+}
+
+__global__ void k_pad_rows(long long nrows, int w, int wpad, const double* __restrict__ src, double* __restrict__ dst)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nrows * wpad;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long row = e / wpad;
+        const int k = (int)(e - row * wpad);
+        dst[e] = k < w ? src[row * w + k] : 0.0;
     }
 }
 
@@ -432,36 +562,57 @@ struct RTab {
 
 // ch = P cHH and c = ch  (the prolongation plus the copy c.copy(m_ch) of
 // MultiGridSolver::solve, multigrid_solver.h:65-66)
-template <typename T>
-__global__ void k_prolong(int N, int M, int K, int Nc, int Mc, PTab px, PTab py, PTab pz,
-                          const T* __restrict__ coarse, T* __restrict__ ch, T* __restrict__ c)
+template <typename T, int ZC>
+__global__ void __launch_bounds__(256) k_prolong(int N, int M, int K, int Nc, int Mc, PTab px, PTab py, PTab pz,
+                                                 const T* __restrict__ coarse, T* __restrict__ ch, T* __restrict__ c)
 {
-    const long long n = (long long)N * M * K;
-    const int NM = N * M, NMc = Nc * Mc;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        int x, y, z;
-        cell_xyz(i, N, NM, x, y, z);
-        T acc = 0;
+    // block (32, 8) over (x, y); each thread ZC consecutive z.  All gathers of
+    // the ZC cells are issued before any is summed (unused table slots hold
+    // index 0 and weight 0, so every address is valid); the sum skips zero
+    // weights and runs in the row order of P (z, y, x ascending).
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    if (x >= N || y >= M) return;
+    const int z0 = blockIdx.z * ZC;
+    const int NMc = Nc * Mc;
+    float wx[2], wy[2];
+    int ox[2], oy[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        wx[q] = px.w[2 * x + q];
+        ox[q] = px.c[2 * x + q];
+        wy[q] = py.w[2 * y + q];
+        oy[q] = py.c[2 * y + q] * Nc;
+    }
+    T g[ZC][8];
+    float wz[ZC][2];
+#pragma unroll
+    for (int u = 0; u < ZC; u++) {
+        const int z = min(z0 + u, K - 1);
 #pragma unroll
         for (int a = 0; a < 2; a++) {
-            const float wz = pz.w[2 * z + a];
-            if (wz == 0.f) continue;
-            const int cz = pz.c[2 * z + a];
+            wz[u][a] = pz.w[2 * z + a];
+            const int oz = pz.c[2 * z + a] * NMc;
 #pragma unroll
-            for (int b = 0; b < 2; b++) {
-                const float wy = py.w[2 * y + b];
-                if (wy == 0.f) continue;
-                const int cy = py.c[2 * y + b];
+            for (int b = 0; b < 2; b++)
 #pragma unroll
-                for (int q = 0; q < 2; q++) {
-                    const float wx = px.w[2 * x + q];
-                    if (wx == 0.f) continue;
-                    const int cx = px.c[2 * x + q];
-                    acc += (T)(wz * wy * wx) * coarse[(long long)cz * NMc + cy * Nc + cx];
-                }
-            }
+                for (int q = 0; q < 2; q++) g[u][4 * a + 2 * b + q] = coarse[oz + oy[b] + ox[q]];
         }
+    }
+#pragma unroll
+    for (int u = 0; u < ZC; u++) {
+        const int z = z0 + u;
+        if (z >= K) break;
+        T acc = 0;
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++)
+#pragma unroll
+                for (int q = 0; q < 2; q++)
+                    if (wz[u][a] != 0.f && wy[b] != 0.f && wx[q] != 0.f)
+                        acc += (T)(wz[u][a] * wy[b] * wx[q]) * g[u][4 * a + 2 * b + q];
+        const int i = x + N * (y + M * z);                 // grids hold fewer than 2^31 cells
         ch[i] = acc;
         c[i] = acc;
     }
@@ -475,10 +626,11 @@ __global__ void k_restrict(int Nc, int Mc, int Kc, int N, int M, bool agglomerat
 {
     const long long nc = (long long)Nc * Mc * Kc;
     const int NMc = Nc * Mc, NM = N * M;
+    const CellIndex ci(Nc, NMc);
     for (long long I = blockIdx.x * (long long)blockDim.x + threadIdx.x; I < nc;
          I += (long long)gridDim.x * blockDim.x) {
         int X, Y, Z;
-        cell_xyz(I, Nc, NMc, X, Y, Z);
+        ci.xyz(I, X, Y, Z);
         T acc = 0;
         if (agglomerate) {
             const long long f0 = (long long)(2 * Z) * NM + (2 * Y) * N + 2 * X;
@@ -859,6 +1011,107 @@ __global__ void __launch_bounds__(128) k_tdma_strided(LineGeom g, bool zquirk, c
                     c[i] = cv;
                     ch[i] = hh[u] + cv;
                 }
+            }
+        }
+    }
+}
+
+// y- and z-lines, segmented.  A CTA holds W neighbouring lines (consecutive
+// x, so each warp load is a contiguous row piece) split into S = ceil(L/SEG)
+// segments, one thread per (line, segment).  Every thread issues all loads of
+// its segment (r, lo, dinv, up, ch) before any arithmetic, so the whole line
+// is one memory round trip.  Within a segment the forward recurrence
+//   y_t = (r_t - lo_t y_{t-1}) dinv_t
+// is kept as affine maps of the value entering the segment, y_t = A_t + B_t y_in,
+// and the backward one x_t = y_t - up_t x_{t+1} as x_t = G_t + H_t x_out; the
+// S segment maps of a line are chained through shared memory.
+template <typename T, int SEG, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_tdma_seg(LineGeom g, bool zquirk, const T* __restrict__ lo,
+                                                         const T* __restrict__ dinv, const T* __restrict__ up,
+                                                         const T* __restrict__ r, T* __restrict__ c,
+                                                         T* __restrict__ ch, T omega)
+{
+    extern __shared__ __align__(16) unsigned char seg_smem[];
+    const int W = blockDim.x, S = blockDim.y;
+    T* sA = reinterpret_cast<T*>(seg_smem);
+    T* sB = sA + W * S;
+    const int w = threadIdx.x, sg = threadIdx.y;
+    const int L = g.len();
+    const long long st = line_stride(g);
+    const int gx = (g.N + W - 1) / W;
+    const int row = blockIdx.x / gx;                       // z for y-lines, y for z-lines
+    const int x = (blockIdx.x - row * gx) * W + w;
+    const bool valid = x < g.N;
+    const int xs = valid ? x : g.N - 1;                    // idle lanes load a valid line, store nothing
+    const long long i0 = line_start(g, (long long)row * g.N + xs);
+    const int t0 = sg * SEG;
+    T rv[SEG], lv[SEG], dv[SEG], uv[SEG], hv[SEG];
+#pragma unroll
+    for (int u = 0; u < SEG; u++) {
+        const int t = min(t0 + u, L - 1);
+        const long long i = i0 + (long long)t * st;
+        rv[u] = r[i];
+        lv[u] = lo[i];
+        dv[u] = dinv[i];
+        uv[u] = up[i];
+        hv[u] = ch[i];
+    }
+    if (zquirk && sg == 0) rv[0] = r[(long long)row * g.N * g.K + xs];   // reference z-line quirk (y*N*K + x)
+    // forward, relative to y_in
+    T a = 0, b = 1;
+#pragma unroll
+    for (int u = 0; u < SEG; u++) {
+        const int t = t0 + u;
+        if (t < L) {
+            if (t == 0) {
+                a = rv[u] * dv[u];
+                b = 0;
+            } else {
+                a = (rv[u] - lv[u] * a) * dv[u];
+                b = -(lv[u] * b) * dv[u];
+            }
+        }
+        rv[u] = a;
+        lv[u] = b;
+    }
+    sA[sg * W + w] = a;
+    sB[sg * W + w] = b;
+    __syncthreads();
+    T yin = 0;
+    for (int q = 0; q < sg; q++) yin = sA[q * W + w] + sB[q * W + w] * yin;
+    __syncthreads();
+    // backward, relative to x_out
+    T gg = 0, hh = 1;
+#pragma unroll
+    for (int u = SEG - 1; u >= 0; u--) {
+        const int t = t0 + u;
+        if (t < L) {
+            const T yv = rv[u] + lv[u] * yin;
+            if (t == L - 1) {
+                gg = yv;
+                hh = 0;
+            } else {
+                gg = yv - uv[u] * gg;
+                hh = -(uv[u] * hh);
+            }
+        }
+        rv[u] = gg;
+        lv[u] = hh;
+    }
+    sA[sg * W + w] = gg;
+    sB[sg * W + w] = hh;
+    __syncthreads();
+    T xo = 0;
+    for (int q = S - 1; q > sg; q--) xo = sA[q * W + w] + sB[q * W + w] * xo;
+    if (valid) {
+#pragma unroll
+        for (int u = 0; u < SEG; u++) {
+            const int t = t0 + u;
+            if (t < L) {
+                const long long i = i0 + (long long)t * st;
+                const T cv = omega * (rv[u] + lv[u] * xo);
+                c[i] = cv;
+                ch[i] = hv[u] + cv;
             }
         }
     }

@@ -19,11 +19,12 @@ __global__ void __launch_bounds__(256) k_residual7(int N, int M, int K, const in
 {
     const long long n = (long long)N * M * K;
     const int NM = N * M;
+    const CellIndex ci(N, NM);
     double s[1] = {0.0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         int ix, iy, iz;
-        cell_xyz(i, N, NM, ix, iy, iz);
+        ci.xyz(i, ix, iy, iz);
         const double* a = dict + (size_t)cls[i] * 7;
         double acc = a[3] * x[i];
         if (iz > 0) acc += a[0] * x[i - NM];
@@ -48,11 +49,12 @@ __global__ void __launch_bounds__(256) k_spmv_dot7(int N, int M, int K, const in
 {
     const long long n = (long long)N * M * K;
     const int NM = N * M;
+    const CellIndex ci(N, NM);
     double s[1] = {0.0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         int ix, iy, iz;
-        cell_xyz(i, N, NM, ix, iy, iz);
+        ci.xyz(i, ix, iy, iz);
         const double* a = dict + (size_t)cls[i] * 7;
         double acc = a[3] * (double)z[i];
         if (iz > 0) acc += a[0] * (double)z[i - NM];
@@ -63,6 +65,74 @@ __global__ void __launch_bounds__(256) k_spmv_dot7(int N, int M, int K, const in
         if (iz < K - 1) acc += a[6] * (double)z[i + NM];
         w[i] = acc;
         s[0] += acc * v0[i];
+    }
+    grid_reduce<1>(s, partial, counter, out);
+}
+
+// Krylov 7-point products on the fine grid, marching along z like k_apply7z
+// (U z-steps of loads in flight per thread) and fused with one dot product:
+//   MODE 0:  w = A z,      out = (w, v)      (Arnoldi: first MGS coefficient)
+//   MODE 1:  w = v - A z,  out = (w, w)      (residual and its squared norm)
+// z is FP64, or FP32 widened exactly.  Terms are summed p, b, s, w, e, n, t.
+template <typename Tz, int MODE>
+__global__ void __launch_bounds__(256) k_krylov7z(int N, int M, int K, int zc, const int* __restrict__ cls,
+                                                   const double* __restrict__ dict, const Tz* __restrict__ z,
+                                                   const double* __restrict__ v, double* __restrict__ w,
+                                                   double* partial, unsigned int* counter, double* out)
+{
+    constexpr int U = 4;
+    double s[1] = {0.0};
+    const int ix = blockIdx.x * 32 + threadIdx.x;
+    const int iy = blockIdx.y * 8 + threadIdx.y;
+    if (ix < N && iy < M) {
+        const int NM = N * M;                              // grids hold fewer than 2^31 cells
+        const int z0 = blockIdx.z * zc;
+        const int z1 = min(z0 + zc, K);
+        int i = ix + N * iy + NM * z0;
+        Tz xm = (z0 > 0) ? z[i - NM] : (Tz)0;
+        Tz xc = z[i];
+        const bool hasw = ix > 0, hase = ix < N - 1, hass = iy > 0, hasn = iy < M - 1;
+        for (int zb = z0; zb < z1; zb += U, i += U * NM) {
+            int cl[U];
+            double vv[U];
+            Tz xs[U], xw[U], xe[U], xn[U], xp[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int zz = zb + u;
+                const int ii = (zz < z1) ? i + u * NM : i;
+                cl[u] = cls[ii];
+                vv[u] = v[ii];
+                xs[u] = hass ? z[ii - N] : (Tz)0;
+                xw[u] = hasw ? z[ii - 1] : (Tz)0;
+                xe[u] = hase ? z[ii + 1] : (Tz)0;
+                xn[u] = hasn ? z[ii + N] : (Tz)0;
+                xp[u] = (zz < K - 1) ? z[ii + NM] : (Tz)0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (zb + u < z1) {
+                    const double* a = dict + (size_t)cl[u] * 7;
+                    double acc = a[3] * (double)xc;
+                    acc += a[0] * (double)xm;
+                    if (hass) acc += a[1] * (double)xs[u];
+                    if (hasw) acc += a[2] * (double)xw[u];
+                    if (hase) acc += a[4] * (double)xe[u];
+                    if (hasn) acc += a[5] * (double)xn[u];
+                    acc += a[6] * (double)xp[u];
+                    const int ii = i + u * NM;
+                    if (MODE == 0) {
+                        w[ii] = acc;
+                        s[0] += acc * vv[u];
+                    } else {
+                        const double t = vv[u] - acc;
+                        w[ii] = t;
+                        s[0] += t * t;
+                    }
+                    xm = xc;
+                    xc = xp[u];
+                }
+            }
+        }
     }
     grid_reduce<1>(s, partial, counter, out);
 }
@@ -202,11 +272,12 @@ __global__ void __launch_bounds__(256) k_bicg_nu(int N, int M, int K, const int*
 {
     const long long n = (long long)N * M * K;
     const int NM = N * M;
+    const CellIndex ci(N, NM);
     double s[2] = {0.0, 0.0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         int ix, iy, iz;
-        cell_xyz(i, N, NM, ix, iy, iz);
+        ci.xyz(i, ix, iy, iz);
         const double* a = dict + (size_t)cls[i] * 7;
         double acc = a[3] * y[i];
         if (iz > 0) acc += a[0] * y[i - NM];
@@ -244,11 +315,12 @@ __global__ void __launch_bounds__(256) k_bicg_t(int N, int M, int K, const int* 
 {
     const long long n = (long long)N * M * K;
     const int NM = N * M;
+    const CellIndex ci(N, NM);
     double s[2] = {0.0, 0.0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         int ix, iy, iz;
-        cell_xyz(i, N, NM, ix, iy, iz);
+        ci.xyz(i, ix, iy, iz);
         const double* a = dict + (size_t)cls[i] * 7;
         double acc = a[3] * z[i];
         if (iz > 0) acc += a[0] * z[i - NM];
@@ -321,79 +393,6 @@ namespace lsg {
 // ---------------------------------------------------------------------------
 constexpr int kGsMaxVec = 64;
 
-// Block-level sum of nv values per thread into partial[block * stride + q];
-// the last block sums the partials in block order into out[q].
-__device__ void grid_reduce_n(double* vals, int nv, double* partial, int stride, unsigned int* counter,
-                              double* out)
-{
-    __shared__ double sh[32];
-    __shared__ bool last;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int q = 0; q < nv; q++) {
-        double t = warp_sum(vals[q]);
-        if (lane == 0) sh[wid] = t;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double u = 0.0;
-            for (int w = 0; w < nw; w++) u += sh[w];
-            partial[(size_t)blockIdx.x * stride + q] = u;
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        __threadfence();
-        last = (atomicAdd(counter, 1u) == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    for (int q = wid; q < nv; q += nw) {
-        double acc = 0.0;
-        for (int b = lane; b < (int)gridDim.x; b += 32) acc += ((volatile double*)partial)[(size_t)b * stride + q];
-        acc = warp_sum(acc);
-        if (lane == 0) out[q] = acc;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) *counter = 0u;
-}
-
-// One pass over V[0..j] and w:  s[k] = (v_k, w), k <= j;  g[k] = (v_k, v_j), k < j.
-// out = s[0..j], g[0..j-1] (2j+1 values).
-template <int NV>
-__global__ void __launch_bounds__(256) k_gs_dots(long long n, long long ld, int j, const double* __restrict__ V,
-                                                  const double* __restrict__ w, double* partial,
-                                                  unsigned int* counter, double* out)
-{
-    double sacc[NV], gacc[NV];
-#pragma unroll
-    for (int k = 0; k < NV; k++) {
-        sacc[k] = 0.0;
-        gacc[k] = 0.0;
-    }
-    const double* vj = V + (size_t)j * ld;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
-        const double wi = w[i], vji = vj[i];
-#pragma unroll
-        for (int k = 0; k < NV; k++) {
-            if (k <= j) {
-                const double vk = (k == j) ? vji : V[(size_t)k * ld + i];
-                sacc[k] += vk * wi;
-                if (k < j) gacc[k] += vk * vji;
-            }
-        }
-    }
-    double vals[2 * NV];
-    int nv = 0;
-#pragma unroll
-    for (int k = 0; k < NV; k++)
-        if (k <= j) vals[nv++] = sacc[k];
-#pragma unroll
-    for (int k = 0; k < NV; k++)
-        if (k < j) vals[nv++] = gacc[k];
-    grid_reduce_n(vals, nv, partial, 2 * kGsMaxVec, counter, out);
-}
-
 // Triangular correction on one thread: store row j of L (from g), solve
 // (I + L) h = s, write h into Hessenberg column j.
 __global__ void k_gs_tri(KrylovScalars* ks, int j, int ldh, const double* __restrict__ sg, double* __restrict__ Lrows)
@@ -410,22 +409,112 @@ __global__ void k_gs_tri(KrylovScalars* ks, int j, int ldh, const double* __rest
     }
 }
 
-// w -= sum_k h_k v_k (k <= j) and ||w||^2.
-template <int NV>
-__global__ void __launch_bounds__(256) k_gs_update(long long n, long long ld, int j, const double* __restrict__ V,
+// One pass over V[0..j] and w for the low-synchronisation Gram-Schmidt:
+// s_k = (v_k, w) for k <= j and g_k = (v_k, v_j) for k < j; out = s_0..s_j,
+// g_0..g_{j-1}.  A block is 32 lanes (consecutive cells) by one warp per group
+// of four basis vectors: each warp streams only its own vectors, while w and
+// v_j are shared by the warps of the block through L1.  Per-block sums go to
+// partial[block][q]; the last block to finish adds them in block order.
+__global__ void __launch_bounds__(512) k_gs_dots2(long long n, long long ld, int j, const double* __restrict__ V,
+                                                  const double* __restrict__ w, double* partial,
+                                                  unsigned int* counter, double* out)
+{
+    constexpr int VW = 4;
+    const int lane = threadIdx.x, grp = threadIdx.y;
+    const int k0 = grp * VW;
+    const int nk = max(0, min(VW, j + 1 - k0));
+    double sa[VW], ga[VW];
+#pragma unroll
+    for (int q = 0; q < VW; q++) {
+        sa[q] = 0.0;
+        ga[q] = 0.0;
+    }
+    const double* vj = V + (size_t)j * ld;
+    // each block streams one contiguous range of cells, 128 per warp step
+    // (four 32-cell pieces, all loads of a step issued before the sums)
+    const long long chunk = ((n + gridDim.x - 1) / gridDim.x + 127) / 128 * 128;
+    const long long beg = (long long)blockIdx.x * chunk, end = min(n, beg + chunk);
+    for (long long i0 = beg + lane; i0 < end; i0 += 128) {
+        double wv[4], vv[4], av[VW][4];
+#pragma unroll
+        for (int p = 0; p < 4; p++) {
+            const long long i = i0 + 32 * p;
+            const bool in = i < end;
+            wv[p] = in ? w[i] : 0.0;
+            vv[p] = in ? vj[i] : 0.0;
+#pragma unroll
+            for (int q = 0; q < VW; q++) av[q][p] = (in && q < nk) ? V[(size_t)(k0 + q) * ld + i] : 0.0;
+        }
+#pragma unroll
+        for (int p = 0; p < 4; p++)
+#pragma unroll
+            for (int q = 0; q < VW; q++) {
+                sa[q] += av[q][p] * wv[p];
+                ga[q] += av[q][p] * vv[p];
+            }
+    }
+    const int pstride = 2 * kGsMaxVec;
+#pragma unroll
+    for (int q = 0; q < VW; q++) {
+        sa[q] = warp_sum(sa[q]);
+        ga[q] = warp_sum(ga[q]);
+    }
+    if (lane == 0) {
+        for (int q = 0; q < nk; q++) {
+            const int k = k0 + q;
+            partial[(size_t)blockIdx.x * pstride + k] = sa[q];
+            if (k < j) partial[(size_t)blockIdx.x * pstride + j + 1 + k] = ga[q];
+        }
+        __threadfence();
+    }
+    __shared__ bool last;
+    __syncthreads();
+    if (lane == 0 && grp == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // final sums: one warp per value, four independent L2 loads in flight per lane
+    const int nv = 2 * j + 1;
+    for (int q = grp; q < nv; q += blockDim.y) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int b = lane;
+        for (; b + 96 < (int)gridDim.x; b += 128) {
+            a0 += __ldcg(partial + (size_t)b * pstride + q);
+            a1 += __ldcg(partial + (size_t)(b + 32) * pstride + q);
+            a2 += __ldcg(partial + (size_t)(b + 64) * pstride + q);
+            a3 += __ldcg(partial + (size_t)(b + 96) * pstride + q);
+        }
+        for (; b < (int)gridDim.x; b += 32) a0 += __ldcg(partial + (size_t)b * pstride + q);
+        const double acc = warp_sum((a0 + a1) + (a2 + a3));
+        if (lane == 0) out[q] = acc;
+    }
+    __syncthreads();
+    if (lane == 0 && grp == 0) *counter = 0u;
+}
+
+// w -= sum_{k<=j} h_k v_k and ||w||^2, the basis vectors read four at a time.
+__global__ void __launch_bounds__(256) k_gs_update2(long long n, long long ld, int j, const double* __restrict__ V,
                                                     const double* __restrict__ h, double* __restrict__ w,
                                                     double* partial, unsigned int* counter, double* out)
 {
-    __shared__ double hs[NV];
-    if (threadIdx.x < NV) hs[threadIdx.x] = (threadIdx.x <= j) ? h[threadIdx.x] : 0.0;
+    __shared__ double hs[kGsMaxVec];
+    for (int t = threadIdx.x; t <= j; t += blockDim.x) hs[t] = h[t];
     __syncthreads();
     double s[1] = {0.0};
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    const long long chunk = ((n + gridDim.x - 1) / gridDim.x + blockDim.x - 1) / blockDim.x * blockDim.x;
+    const long long beg = (long long)blockIdx.x * chunk, end = min(n, beg + chunk);
+    for (long long i = beg + threadIdx.x; i < end; i += blockDim.x) {
         double acc = w[i];
-#pragma unroll
-        for (int k = 0; k < NV; k++)
-            if (k <= j) acc -= hs[k] * V[(size_t)k * ld + i];
+        int k = 0;
+        for (; k + 4 <= j + 1; k += 4) {
+            const double v0 = V[(size_t)k * ld + i], v1 = V[(size_t)(k + 1) * ld + i];
+            const double v2 = V[(size_t)(k + 2) * ld + i], v3 = V[(size_t)(k + 3) * ld + i];
+            acc -= hs[k] * v0;
+            acc -= hs[k + 1] * v1;
+            acc -= hs[k + 2] * v2;
+            acc -= hs[k + 3] * v3;
+        }
+        for (; k <= j; k++) acc -= hs[k] * V[(size_t)k * ld + i];
         w[i] = acc;
         s[0] += acc * acc;
     }

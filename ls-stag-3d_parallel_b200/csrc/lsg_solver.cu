@@ -142,6 +142,7 @@ struct LevelT {
     DevBuf<int> clsown;
     const T* dict = nullptr;
     DevBuf<T> dictown;
+    DevBuf<T> dict28;         // 27-point levels: rows padded to stride 28 for vector loads
     int nclass = 0;
     DevBuf<T> lo[3], dinv[3], up[3];
     DevBuf<T> r, c, ch;
@@ -450,6 +451,11 @@ static void mg_setup(Context& C)
         cl.nclass = build_dict(s, cl.A, cl.ol.n, c.n(), cl.clsown, cl.dictown);
         cl.cls = cl.clsown.p;
         cl.dict = cl.dictown.p;
+        if (cl.ol.n == 27) {
+            cl.dict28.alloc((size_t)cl.nclass * 28);
+            k_pad_rows<<<grid_for((long long)cl.nclass * 28, 256), 256, 0, s>>>(cl.nclass, 27, 28, cl.dict, cl.dict28.p);
+            LSG_CHECK_LAUNCH();
+        }
         rad = {crx, cry, crz};
     }
     // ADLJ line factors of every smoothed level
@@ -553,6 +559,12 @@ static void mg_setup(Context& C)
             b.dict = b.dictown.p;
             k_convert<float, double><<<grid_for(nd, 256), 256, 0, s>>>(nd, a.dict, b.dictown.p);
             LSG_CHECK_LAUNCH();
+            if (a.ol.n == 27) {
+                const long long n28 = (long long)a.nclass * 28;
+                b.dict28.alloc(n28);
+                k_convert<float, double><<<grid_for(n28, 256), 256, 0, s>>>(n28, a.dict28.p, b.dict28.p);
+                LSG_CHECK_LAUNCH();
+            }
             if (l < L) {
                 for (int d = 0; d < 3; d++) {
                     b.lo[d].alloc(n);
@@ -585,11 +597,11 @@ static void apply_resid(const LevelT<T>& lv, const T* x, T* r, cudaStream_t s, i
             k_apply7z<T, 0><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict, x, r);
         else
             k_apply7z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict, x, r);
-    } else if (lv.ol.n == 27) {
+    } else if (lv.ol.n == 27 && lv.dict28.p) {
         if (mode == 0)
-            k_apply27z<T, 0><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict, x, r);
+            k_apply27z<T, 0><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict28.p, x, r);
         else
-            k_apply27z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict, x, r);
+            k_apply27z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict28.p, x, r);
     } else {
         if (mode == 0)
             k_applyboxd<T, 0><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.ol, lv.cls, lv.dict, x, r);
@@ -611,8 +623,21 @@ static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStr
                                                ch, omega);
     } else {
         LineGeom lg{g.N, g.M, g.K, d};
-        k_tdma_strided<T><<<grid_for(lg.nlines(), 128, 148 * 64), 128, 0, s>>>(
-            lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, ch, omega);
+        constexpr int SEG = 8;
+        constexpr int MAXT = sizeof(T) == 4 ? 512 : 256;
+        const int S = (lg.len() + SEG - 1) / SEG;
+        if (S * 8 <= MAXT) {
+            // W lines per CTA: as many as fit MAXT threads, at most 32 (one warp row)
+            int W = 8;
+            while (W < 32 && 2 * W * S <= MAXT) W *= 2;
+            const long long blocks = (long long)((g.N + W - 1) / W) * (d == 1 ? g.K : g.M);
+            const size_t smem = 2 * (size_t)W * S * sizeof(T);
+            k_tdma_seg<T, SEG, MAXT, 2><<<(unsigned)blocks, dim3(W, S), smem, s>>>(
+                lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, ch, omega);
+        } else {
+            k_tdma_strided<T><<<grid_for(lg.nlines(), 128, 148 * 64), 128, 0, s>>>(
+                lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, ch, omega);
+        }
     }
     LSG_CHECK_LAUNCH();
 }
@@ -643,8 +668,9 @@ static void vcycle(Context& C, std::vector<LevelT<T>>& lev, T* ch0 = nullptr)
         const Dims& f = lv.d;
         const TransferTabs& t = mg.tabs[l];
         T* chl = (l == 0 && ch0) ? ch0 : lv.ch.p;
-        k_prolong<T><<<grid_for(f.n(), 256), 256, 0, s>>>(f.N, f.M, f.K, lev[l + 1].d.N, lev[l + 1].d.M, t.P(0), t.P(1),
-                                                         t.P(2), lev[l + 1].ch.p, chl, lv.c.p);
+        constexpr int PZ = 4;
+        k_prolong<T, PZ><<<dim3((f.N + 31) / 32, (f.M + 7) / 8, (f.K + PZ - 1) / PZ), dim3(32, 8), 0, s>>>(
+            f.N, f.M, f.K, lev[l + 1].d.N, lev[l + 1].d.M, t.P(0), t.P(1), t.P(2), lev[l + 1].ch.p, chl, lv.c.p);
         LSG_CHECK_LAUNCH();
         for (int it = 0; it < C.opt.n_post; it++) {
             const int order[3] = {2, 1, 0};       // SmootherADLJ::solve: z, y, x
@@ -715,32 +741,53 @@ static void launch_givens(Context& C, int j)
 
 // Low-synchronisation MGS for Arnoldi step j: one pass for V^T w and the new
 // row of V^T V, a triangular correction, one update pass (with ||w||^2).
-template <int NV>
-static void gs_lowsync_t(Context& C, int j, int gb, double* Hj)
+// Fine-grid Krylov product fused with one dot (k_krylov7z): MODE 0 w = A z,
+// out = (w, v); MODE 1 w = v - A z, out = ||w||^2.  The z-chunk is sized so the
+// grid has at most 4096 blocks; wider grids use the one-thread-per-cell kernels.
+template <typename Tz, int MODE>
+static void krylov7(Context& C, const Tz* z, const double* v, double* w, double* out)
 {
-    const long long n = C.n;
-    k_gs_dots<NV><<<gb, 256, 0, C.s>>>(n, C.ldv, j, C.V.p, C.w.p, C.gs_partial.p, C.red.counter.p, C.gs_sg.p);
-    LSG_CHECK_LAUNCH();
-    k_gs_tri<<<1, 32, 0, C.s>>>(C.ks.p, j, 65, C.gs_sg.p, C.gs_L.p);
-    LSG_CHECK_LAUNCH();
-    k_gs_update<NV><<<gb, 256, 0, C.s>>>(n, C.ldv, j, C.V.p, Hj, C.w.p, C.red.partial.p, C.red.counter.p,
-                                         &C.ks.p->normW2);
+    const Dims& d = C.d;
+    const long long gx = (d.N + 31) / 32, gy = (d.M + 7) / 8;
+    constexpr long long cap = 4096;
+    if (gx * gy <= cap) {
+        int zc = zchunk_for(C.n);
+        while (gx * gy * ((d.K + zc - 1) / zc) > cap) zc *= 2;
+        const dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)((d.K + zc - 1) / zc));
+        k_krylov7z<Tz, MODE><<<grid, dim3(32, 8), 0, C.s>>>(d.N, d.M, d.K, zc, C.cls0.p, C.dict0.p, z, v, w,
+                                                             C.red.partial.p, C.red.counter.p, out);
+    } else {
+        const int gb = grid_for(C.n, 256, Reducer::kMaxBlocks);
+        if constexpr (MODE == 0)
+            k_spmv_dot7<Tz><<<gb, 256, 0, C.s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, z, v, w, C.red.partial.p,
+                                                 C.red.counter.p, out);
+        else
+            k_residual7<<<gb, 256, 0, C.s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, z, v, w, C.red.partial.p,
+                                             C.red.counter.p, out);
+    }
     LSG_CHECK_LAUNCH();
 }
 
 static void gs_lowsync(Context& C, int j, int gb, double* Hj)
 {
-    if (j < 8) gs_lowsync_t<8>(C, j, gb, Hj);
-    else if (j < 16) gs_lowsync_t<16>(C, j, gb, Hj);
-    else if (j < 32) gs_lowsync_t<32>(C, j, gb, Hj);
-    else gs_lowsync_t<64>(C, j, gb, Hj);
+    const long long n = C.n;
+    // about 32 resident warps per SM whatever the number of vector groups
+    const int groups = (j + 4) / 4;
+    const int gd = (int)std::min<long long>((n + 127) / 128, std::max(148, 148 * 32 / groups));
+    k_gs_dots2<<<gd, dim3(32, (j + 4) / 4), 0, C.s>>>(n, C.ldv, j, C.V.p, C.w.p, C.gs_partial.p, C.red.counter.p,
+                                                      C.gs_sg.p);
+    LSG_CHECK_LAUNCH();
+    k_gs_tri<<<1, 32, 0, C.s>>>(C.ks.p, j, 65, C.gs_sg.p, C.gs_L.p);
+    LSG_CHECK_LAUNCH();
+    k_gs_update2<<<gb, 256, 0, C.s>>>(n, C.ldv, j, C.V.p, Hj, C.w.p, C.red.partial.p, C.red.counter.p,
+                                      &C.ks.p->normW2);
+    LSG_CHECK_LAUNCH();
 }
 
 static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
 {
     cudaStream_t s = C.s;
     const long long n = C.n;
-    const Dims& d = C.d;
     const int m = C.restart;
     const int gb = grid_for(n, 256, Reducer::kMaxBlocks);
     double* part = C.red.partial.p;
@@ -749,8 +796,7 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
     const double w8 = 8.0;
     double bytes = 0;
     // norm_r = ||b - A x||  ; w = b - A x
-    k_residual7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, x, b, C.w.p, part, cnt, &ks->normW2);
-    LSG_CHECK_LAUNCH();
+    krylov7<double, 1>(C, x, b, C.w.p, &ks->normW2);
     bytes += (3 * w8 + 4) * n;
     double nrm2 = 0;
     LSG_CUDA(cudaMemcpyAsync(&nrm2, &ks->normW2, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -792,13 +838,8 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
                 }
                 // w = A z_j ; H[0,j] = (w, v_0)
                 double* Hj = ks->H + (size_t)j * 65;
-                if (z32)
-                    k_spmv_dot7<float><<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, zj32, C.V.p, C.w.p, part,
-                                                          cnt, Hj);
-                else
-                    k_spmv_dot7<double><<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, zj, C.V.p, C.w.p, part,
-                                                           cnt, Hj);
-                LSG_CHECK_LAUNCH();
+                if (z32) krylov7<float, 0>(C, zj32, C.V.p, C.w.p, Hj);
+                else krylov7<double, 0>(C, zj, C.V.p, C.w.p, Hj);
                 bytes += (3 * w8 + 4) * n;
                 if (C.opt.gram_schmidt == LSG_GS_LOWSYNC) {
                     gs_lowsync(C, j, gb, Hj);
@@ -836,8 +877,7 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
             if (!finished || refine) {
                 // w = b - A x: the next cycle's first direction
                 // (fgmres_interface.h:136-138)
-                k_residual7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, x, b, C.w.p, part, cnt, C.scal.p + 16);
-                LSG_CHECK_LAUNCH();
+                krylov7<double, 1>(C, x, b, C.w.p, C.scal.p + 16);
                 bytes += (3 * w8 + 4) * n;
                 KrylovScalars hs;
                 double tr2 = 0;
@@ -996,8 +1036,7 @@ static int bicgstab(Context& C, double* x, const double* b, lsg_stats* st)
     double* t = C.t3.p;
     double bytes = 0;
     int it = 1;
-    k_residual7<<<gb, 256, 0, s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, x, b, r, part, cnt, sc + 5);
-    LSG_CHECK_LAUNCH();
+    krylov7<double, 1>(C, x, b, r, sc + 5);
     bytes += 80.0 * n;
     double nr2 = 0;
     LSG_CUDA(cudaMemcpyAsync(&nr2, sc + 5, 8, cudaMemcpyDeviceToHost, s));
@@ -1067,7 +1106,7 @@ static void krylov_alloc(Context& C)
     C.bd.alloc(n);
     C.coefs.alloc(64);
     if (C.opt.gram_schmidt == LSG_GS_LOWSYNC) {
-        C.gs_partial.alloc((size_t)Reducer::kMaxBlocks * 2 * kGsMaxVec);
+        C.gs_partial.alloc((size_t)148 * 32 * 2 * kGsMaxVec);
         C.gs_sg.alloc(2 * kGsMaxVec);
         C.gs_L.alloc((size_t)kGsMaxVec * kGsMaxVec);
     }
@@ -1075,11 +1114,7 @@ static void krylov_alloc(Context& C)
 
 static double true_residual(Context& C, const double* x, const double* b)
 {
-    const Dims& d = C.d;
-    k_residual7<<<grid_for(C.n, 256, Reducer::kMaxBlocks), 256, 0, C.s>>>(d.N, d.M, d.K, C.cls0.p, C.dict0.p, x, b, C.t1.p,
-                                                                       C.red.partial.p, C.red.counter.p,
-                                                                       C.scal.p + 40);
-    LSG_CHECK_LAUNCH();
+    krylov7<double, 1>(C, x, b, C.t1.p, C.scal.p + 40);
     double r2 = 0;
     LSG_CUDA(cudaMemcpyAsync(&r2, C.scal.p + 40, 8, cudaMemcpyDeviceToHost, C.s));
     LSG_CUDA(cudaStreamSynchronize(C.s));
@@ -1692,9 +1727,7 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
             if (f32) apply_resid<float>(C.mg.l32[1], C.mg.l32[1].c.p, C.mg.l32[1].r.p, C.s, 0);
             else apply_resid<double>(C.mg.l64[1], C.mg.l64[1].c.p, C.mg.l64[1].r.p, C.s, 0);
         } else if (which == 4) {
-            k_spmv_dot7<double><<<grid_for(n, 256, Reducer::kMaxBlocks), 256, 0, C.s>>>(
-                C.d.N, C.d.M, C.d.K, C.cls0.p, C.dict0.p, C.Z.p, C.V.p, C.w.p, C.red.partial.p, C.red.counter.p, C.scal.p + 48);
-            LSG_CHECK_LAUNCH();
+            krylov7<double, 0>(C, C.Z.p, C.V.p, C.w.p, C.scal.p + 48);
         } else {
             throw Error{LSG_ERR_ARG, "unknown kernel id"};
         }
