@@ -378,6 +378,33 @@ int main(int argc, char** argv)
         out.d("inv_mz", m->zMesh.inv_VOF, (long)m->zMesh.NMK);
         out.d("flux", pEq->A.flux, n);
     }
+    // projection operators: divergence rows on the base grid
+    // (poisson_discrete_equation.h Dx/Dy/Dz), gradient rows on the staggered
+    // grids (GradientDiscreteOperatorX/Y/Z as the momentum equations build
+    // them, helmholtz_discrete_equation.h set()), staggered cell types
+    GradientDiscreteOperatorX* gx = nullptr;   // not destroyed (see below)
+    GradientDiscreteOperatorY* gy = nullptr;
+    GradientDiscreteOperatorZ* gz = nullptr;
+    const bool wantProj = (int)cfg.get("dump_projection", 0) || (int)cfg.get("projection", 0);
+    if (wantProj) {
+        gx = new GradientDiscreteOperatorX;
+        gy = new GradientDiscreteOperatorY;
+        gz = new GradientDiscreteOperatorZ;
+        gx->initMeshParams(&m->xMesh, m);
+        gy->initMeshParams(&m->yMesh, m);
+        gz->initMeshParams(&m->zMesh, m);
+    }
+    if ((int)cfg.get("dump_projection", 0)) {
+        out.i("xtype", (const int*)m->xMesh.typeOfCell, (long)m->xMesh.NMK);
+        out.i("ytype", (const int*)m->yMesh.typeOfCell, (long)m->yMesh.NMK);
+        out.i("ztype", (const int*)m->zMesh.typeOfCell, (long)m->zMesh.NMK);
+        out.csr("Dx", (SparseMatrix*)&pEq->Dx);
+        out.csr("Dy", (SparseMatrix*)&pEq->Dy);
+        out.csr("Dz", (SparseMatrix*)&pEq->Dz);
+        out.csr("Gx", (SparseMatrix*)gx);
+        out.csr("Gy", (SparseMatrix*)gy);
+        out.csr("Gz", (SparseMatrix*)gz);
+    }
     SparseMatrix* A = (SparseMatrix*)&pEq->A;
     if ((int)cfg.get("dump_matrix", 1)) out.csr("A", A);
     int pins[2] = {pEq->A.fixPointNum, pEq->A.fixPointFlowNum};
@@ -399,6 +426,43 @@ int main(int argc, char** argv)
     const double eps = cfg.get("abs_tol", rel * bnorm);
     out.scalar("eps", eps);
 
+    // --- one pressure projection of the time step (TimeSteppingMethod::step:
+    //     pEq.solve() then sol.correction()) on predicted velocities read from
+    //     files: the right-hand side (PoissonDiscreteEquation::recalcRightMember),
+    //     the MG-FGMRES pressure correction and the corrected fields ---
+    if ((int)cfg.get("projection", 0)) {
+        task->tScaleP = -1.0;                     // no start-up pressure scaling
+        const double coefP = 1.5 / task->t;       // HelmholtzDiscreteEquation::coef (BDF2)
+        sol->set((SparseMatrix*)gx, (SparseMatrix*)gy, (SparseMatrix*)gz, coefP);
+        double *pu, *pv, *pw, *pp, *cu, *cv, *cw, *cp;
+        sol->prediction.getCopy(pu, pv, pw, pp);
+        sol->current.getCopy(cu, cv, cw, cp);
+        auto readv = [&](const char* key, double* dst, long cnt) {
+            std::ifstream f(cfg.gets(key, ""), std::ios::binary);
+            f.read((char*)dst, sizeof(double) * cnt);
+            return (bool)f;
+        };
+        if (!readv("proj_u", pu, m->xMesh.NMK) || !readv("proj_v", pv, m->yMesh.NMK) ||
+            !readv("proj_w", pw, m->zMesh.NMK) || !readv("proj_p", cp, n)) {
+            fprintf(stderr, "cannot read projection inputs\n");
+            return 3;
+        }
+        std::fill(pp, pp + n, 0.0);
+        pEq->solver.eps = eps;
+        pEq->solve();
+        out.d("proj_b", pEq->m_right, n);
+        out.d("proj_phi", pp, n);
+        int pit = pEq->solver.it;
+        out.i("proj_it", &pit, 1);
+        sol->correction();
+        out.d("proj_u_out", cu, m->xMesh.NMK);
+        out.d("proj_v_out", cv, m->yMesh.NMK);
+        out.d("proj_w_out", cw, m->zMesh.NMK);
+        out.d("proj_p_out", cp, n);
+        out.scalar("proj_coef", coefP);
+        out.scalar("proj_vbase", task->V_BASE);
+        return 0;
+    }
     const int reps = (int)cfg.get("repeats", 1);
     // --- one V-cycle of the reference multigrid (a standalone instance with
     //     the same task parameters as the MGFGMRES preconditioner) ---

@@ -136,3 +136,37 @@ def csr_to_planes(rowptr, col, val, dims) -> np.ndarray:
     P = np.zeros((7, n))
     P[slot, rows] = val          # assignment keeps the sign of a stored -0.0
     return P
+
+
+def run_projection(case: Case, u: np.ndarray, v: np.ndarray, w: np.ndarray, p: np.ndarray, abs_tol: float, *,
+                   threads: int = 1, timeout: float = 3600, **opts) -> dict:
+    """One pressure projection of the reference's time step on given predicted
+    velocities u (x-grid), v (y-grid), w (z-grid) and pressure p: right-hand
+    side, MG-FGMRES pressure correction to the absolute tolerance abs_tol, and
+    the corrected u, v, w, p (harness ``projection`` mode)."""
+    if not available():
+        raise FileNotFoundError(REF_BIN)
+    d = tempfile.mkdtemp(prefix="lsg_proj_")
+    try:
+        lines = case.config_lines()
+        if threads:
+            lines.append(f"threads {threads}")
+        for k, val in opts.items():
+            lines.append(f"{k} {val!r}" if isinstance(val, float) else f"{k} {val}")
+        for key, arr in (("proj_u", u), ("proj_v", v), ("proj_w", w), ("proj_p", p)):
+            path = os.path.join(d, key + ".in")
+            np.ascontiguousarray(arr, dtype=np.float64).tofile(path)
+            lines.append(f"{key} {path}")
+        n = case.N * case.M * case.K
+        rhs = os.path.join(d, "rhs.in")
+        np.zeros(n).tofile(rhs)
+        lines += [f"rhs {rhs}", f"abs_tol {float(abs_tol)!r}", "projection 1", "dump_projection 1"]
+        cfg = os.path.join(d, "case.cfg")
+        with open(cfg, "w") as f:
+            f.write("\n".join(lines) + "\n")
+        subprocess.run([REF_BIN, cfg, d], check=True, timeout=timeout, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.PIPE)
+        return load_dir(d)
+    finally:
+        import shutil
+        shutil.rmtree(d, ignore_errors=True)
