@@ -145,6 +145,44 @@ int lsg_set_matrix_geometry(lsg_ctx* ctx, int N, int M, int K, const int* cellty
    lsg_set_matrix_stencil7).  Host pointer, 7*N*M*K doubles. */
 int lsg_get_matrix_stencil7(lsg_ctx* ctx, double* planes);
 
+/* ---- pressure projection of the time step -----------------------------
+   Both calls use the geometry given to lsg_set_matrix_geometry (kept on the
+   device).  Fields: u on the x-grid ((N-1)MK), v on the y-grid (N(M-1)K), w on
+   the z-grid (NM(K-1)), base-grid fields (flux, b, phi, p) NMK, x fastest.
+   Results equal the reference's bit for bit. */
+
+/* Staggered cell types (LSSTAGUniformMesh xMesh/yMesh/zMesh typeOfCell),
+   needed by lsg_projection_correct.  Host pointers. */
+int lsg_set_staggered_types(lsg_ctx* ctx, const int* xtype, const int* ytype, const int* ztype);
+
+/* b = Dx u + Dy v + Dz w + flux with b[pin0] = b[pin1] = 0: the right-hand
+   side of the pressure equation, PoissonDiscreteEquation::recalcRightMember
+   (DiscreteEquations/poisson_discrete_equation.h:145-159) with the divergence
+   operators DivergenceDiscreteOperatorX/Y/Z
+   (DiscreteOperators/Divergence/divergence_discrete_operator_x.h:119-159,
+   _y.h:92-121, _z.h:86-111) applied from the geometry.  Host pointers. */
+int lsg_projection_rhs(lsg_ctx* ctx, const double* u, const double* v, const double* w, const double* flux,
+                       double* b);
+/* Same on device pointers (the context's device, its stream). */
+int lsg_projection_rhs_device(lsg_ctx* ctx, const double* u, const double* v, const double* w, const double* flux,
+                              double* b);
+
+/* Velocity and pressure update after the pressure solve, SetSolutions::
+   correction (Base/set_solutions.h:215-237): u = inv_VOF_x (Gx phi) + us
+   (gradient GradientDiscreteOperatorX/Y/Z, DiscreteOperators/Gradient/
+   gradient_discrete_operator_x.h:58-77, _y.h:52-74, _z.h:45-62), likewise v, w;
+   with outflow != 0 the east outflow and bottom/top backflow clamps
+   (corrOutFlow / corrOutFlowTB, :87-118, :297-304; vbase = V_BASE); then
+   p += phi * coef (coef = 1.5/dt for the BDF2 step).  phi is not modified
+   (the reference scales its copy in place).  Host pointers; u/v/w are outputs
+   and may alias us/vs/ws. */
+int lsg_projection_correct(lsg_ctx* ctx, const double* phi, const double* us, const double* vs, const double* ws,
+                           double* u, double* v, double* w, double* p, double coef, double vbase, int outflow);
+/* Same on device pointers. */
+int lsg_projection_correct_device(lsg_ctx* ctx, const double* phi, const double* us, const double* vs,
+                                  const double* ws, double* u, double* v, double* w, double* p, double coef,
+                                  double vbase, int outflow);
+
 /* Build the preconditioner for the current operator (multigrid hierarchy:
    MultiGridSolver::set multigrid_solver.h:76-101 / CoarseGrid::set
    coarse_grid.h:93-106; or ILU(0): ILUDecompositionSparseMatrix::decompose

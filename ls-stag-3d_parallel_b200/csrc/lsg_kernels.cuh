@@ -1117,6 +1117,133 @@ __global__ void __launch_bounds__(MAXT, MINB) k_tdma_seg(LineGeom g, bool zquirk
     }
 }
 
+// x-lines of power-of-two length L = P * SEG (P <= 32 lanes per line): every
+// thread owns SEG consecutive cells of a line and reads them with 16-byte
+// vector loads (all loads before any arithmetic, one memory round trip).  The
+// segment maps y = A + B y_in (forward) and x = G + H x_out (backward) are
+// chained across the P lanes of a line by warp shuffle scans of width P, so a
+// line costs one scan each way instead of one per 32 cells, and the forward
+// values never leave registers.
+template <typename T, int SEG>
+__device__ __forceinline__ void load_seg(const T* __restrict__ p, T (&v)[SEG])
+{
+    if constexpr (sizeof(T) == 4) {
+        static_assert(SEG % 4 == 0, "FP32 segments are whole float4s");
+#pragma unroll
+        for (int k = 0; k < SEG / 4; k++) {
+            const float4 q = *reinterpret_cast<const float4*>(p + 4 * k);
+            v[4 * k] = q.x;
+            v[4 * k + 1] = q.y;
+            v[4 * k + 2] = q.z;
+            v[4 * k + 3] = q.w;
+        }
+    } else {
+        static_assert(SEG % 2 == 0, "FP64 segments are whole double2s");
+#pragma unroll
+        for (int k = 0; k < SEG / 2; k++) {
+            const double2 q = *reinterpret_cast<const double2*>(p + 2 * k);
+            v[2 * k] = q.x;
+            v[2 * k + 1] = q.y;
+        }
+    }
+}
+
+template <typename T, int SEG>
+__device__ __forceinline__ void store_seg(T* __restrict__ p, const T (&v)[SEG])
+{
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int k = 0; k < SEG / 4; k++)
+            *reinterpret_cast<float4*>(p + 4 * k) = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < SEG / 2; k++) *reinterpret_cast<double2*>(p + 2 * k) = make_double2(v[2 * k], v[2 * k + 1]);
+    }
+}
+
+template <typename T, int SEG>
+__global__ void __launch_bounds__(256) k_tdma_xseg(int L, int P, long long nlines, const T* __restrict__ lo,
+                                                    const T* __restrict__ dinv, const T* __restrict__ up,
+                                                    const T* __restrict__ r, T* __restrict__ c, T* __restrict__ ch,
+                                                    T omega)
+{
+    // whole warps stay in the loop so every shuffle has its full group
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long line = tid / P;
+    const int q = (int)(tid - line * P);
+    const bool valid = line < nlines;
+    const long long base = (valid ? line : 0) * L + (long long)q * SEG;
+    T rv[SEG], lv[SEG], dv[SEG], uv[SEG], hv[SEG];
+    load_seg<T, SEG>(r + base, rv);
+    load_seg<T, SEG>(lo + base, lv);
+    load_seg<T, SEG>(dinv + base, dv);
+    load_seg<T, SEG>(up + base, uv);
+    load_seg<T, SEG>(ch + base, hv);
+    // forward: y_t = (r_t - lo_t y_{t-1}) dinv_t relative to the segment input
+    T a = 0, b = 1;
+#pragma unroll
+    for (int u = 0; u < SEG; u++) {
+        if (q == 0 && u == 0) {
+            a = rv[0] * dv[0];
+            b = 0;
+        } else {
+            a = (rv[u] - lv[u] * a) * dv[u];
+            b = -(lv[u] * b) * dv[u];
+        }
+        rv[u] = a;
+        lv[u] = b;
+    }
+    // inclusive scan of the segment maps over the P lanes of the line
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        if (o >= P) break;
+        const T a2 = __shfl_up_sync(0xffffffffu, a, o, P);
+        const T b2 = __shfl_up_sync(0xffffffffu, b, o, P);
+        if (q >= o) {
+            a = a + b * a2;
+            b = b * b2;
+        }
+    }
+    T yin = __shfl_up_sync(0xffffffffu, a, 1, P);
+    if (q == 0) yin = 0;
+    // backward: x_t = y_t - up_t x_{t+1} relative to the segment output
+    T g = 0, hh = 1;
+#pragma unroll
+    for (int u = SEG - 1; u >= 0; u--) {
+        const T yv = rv[u] + lv[u] * yin;
+        if (q == P - 1 && u == SEG - 1) {
+            g = yv;
+            hh = 0;
+        } else {
+            g = yv - uv[u] * g;
+            hh = -(uv[u] * hh);
+        }
+        rv[u] = g;
+        lv[u] = hh;
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        if (o >= P) break;
+        const T g2 = __shfl_down_sync(0xffffffffu, g, o, P);
+        const T h2 = __shfl_down_sync(0xffffffffu, hh, o, P);
+        if (q + o < P) {
+            g = g + hh * g2;
+            hh = hh * h2;
+        }
+    }
+    T xout = __shfl_down_sync(0xffffffffu, g, 1, P);
+    if (q == P - 1) xout = 0;
+    if (!valid) return;
+#pragma unroll
+    for (int u = 0; u < SEG; u++) {
+        const T cv = omega * (rv[u] + lv[u] * xout);
+        rv[u] = cv;
+        hv[u] = hv[u] + cv;
+    }
+    store_seg<T, SEG>(c + base, rv);
+    store_seg<T, SEG>(ch + base, hv);
+}
+
 // x-lines: one warp per line.  The forward recurrence y_t = D_t r_t -
 // D_t lo_t y_{t-1} and the backward one x_t = y_t - up_t x_{t+1} are affine;
 // each round of 32 consecutive cells is solved by a warp scan of affine maps
@@ -1254,7 +1381,7 @@ namespace lsg {
 // Cell type codes (cut_cells.h): SolidCell 0, FluidCell 11111111, box
 // boundary types -2 .. -27.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int absent_faces(int type)
+__host__ __device__ inline int absent_faces(int type)
 {
     // bit 0 b, 1 s, 2 w, 3 e, 4 n, 5 t
     constexpr int B = 1, S = 2, W = 4, E = 8, Nn = 16, T = 32;

@@ -1,0 +1,181 @@
+// Pressure projection of the time step on the GPU: the divergence right-hand
+// side of the pressure equation and the velocity/pressure update, computed
+// from the cut-cell geometry without assembling the reference's CSR operators.
+//
+// The reference evaluates these products on the CPU as separate IEEE multiply
+// and add operations, so the kernels use __dmul_rn / __dadd_rn (no fused
+// multiply-add) in the reference's order and reproduce its results bit for
+// bit.
+#pragma once
+
+#include "lsg_kernels.cuh"
+
+namespace lsg {
+
+// CellTypes families (Base/LS_STAG_Mesh/cut_cells.h:142-167) by which border
+// of the domain a cell lies on.
+__device__ __forceinline__ bool fam_e(int t) { return t == -6 || t == -16 || t == -18 || t == -10 || t == -14 || t == -20 || t == -22 || t == -24 || t == -26; }
+__device__ __forceinline__ bool fam_w(int t) { return t == -7 || t == -17 || t == -19 || t == -11 || t == -15 || t == -21 || t == -23 || t == -25 || t == -27; }
+__device__ __forceinline__ bool fam_n(int t) { return t == -4 || t == -16 || t == -17 || t == -8 || t == -12 || t == -20 || t == -21 || t == -24 || t == -25; }
+__device__ __forceinline__ bool fam_s(int t) { return t == -5 || t == -18 || t == -19 || t == -9 || t == -13 || t == -22 || t == -23 || t == -26 || t == -27; }
+__device__ __forceinline__ bool fam_t(int t) { return t == -2 || t == -8 || t == -9 || t == -10 || t == -11 || t == -20 || t == -21 || t == -22 || t == -23; }
+__device__ __forceinline__ bool fam_b(int t) { return t == -3 || t == -12 || t == -13 || t == -14 || t == -15 || t == -24 || t == -25 || t == -26 || t == -27; }
+
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+
+// b = Dx u + flux + Dy v + Dz w (PoissonDiscreteEquation::recalcRightMember,
+// DiscreteEquations/poisson_discrete_equation.h:145-159):
+//   aux = Dx u;  b = (aux + flux) + Dy v;  b += Dz w;  b[pin0] = b[pin1] = 0,
+// each product summed from its initial value in the row's column order
+// (RealValuedMeshFunction::mvProd, real_valued_mesh_function.h:81-106).  The
+// rows are DivergenceDiscreteOperatorX/Y/Z::calcD*
+// (DiscreteOperators/Divergence/divergence_discrete_operator_x.h:119-159,
+// _y.h:92-121, _z.h:86-111): -theta dS on the lower face, +theta dS on the
+// upper face, one face on a domain-border cell, one zero entry on a solid
+// cell.  The cell types must be consistent with the grid (border families on
+// the border layers); lsg_set_matrix_geometry checks that before any launch.
+__global__ void __launch_bounds__(256) k_projection_rhs(int N, int M, int K, const int* __restrict__ type,
+                                                        const double* __restrict__ theta,
+                                                        const double* __restrict__ delta,
+                                                        const double* __restrict__ flux, const double* __restrict__ u,
+                                                        const double* __restrict__ v, const double* __restrict__ w,
+                                                        long long pin0, long long pin1, double* __restrict__ b)
+{
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= N || y >= M) return;
+    const long long NM = (long long)N * M;
+    const long long i = x + (long long)N * y + NM * z;
+    const int t = type[i];
+    const double dx = delta[3 * i], dy = delta[3 * i + 1], dz = delta[3 * i + 2];
+    const long long numX = i - y - (long long)z * M;          // x-face east of the cell
+    const long long numY = i - (long long)z * N;              // y-face north of the cell
+    // Dx u (divergence_discrete_operator_x.h:119-159)
+    double aux;
+    if (t == 0) {
+        aux = add(0.0, mul(0.0, u[x == 0 ? numX : numX - 1]));
+    } else if (fam_e(t)) {
+        aux = add(0.0, mul(mul(mul(-theta[3 * (i - 1)], dy), dz), u[numX - 1]));
+    } else if (fam_w(t)) {
+        aux = add(0.0, mul(mul(mul(theta[3 * i], dy), dz), u[numX]));
+    } else {
+        const double dyz = mul(dy, dz);
+        aux = add(add(0.0, mul(mul(-theta[3 * (i - 1)], dyz), u[numX - 1])), mul(mul(theta[3 * i], dyz), u[numX]));
+    }
+    // (aux + flux) + Dy v (divergence_discrete_operator_y.h:92-121)
+    double r = add(aux, flux[i]);
+    if (t == 0) {
+        r = add(r, mul(0.0, v[y == 0 ? numY : numY - N]));
+    } else if (fam_n(t)) {
+        r = add(r, mul(mul(mul(-theta[3 * (i - N) + 1], dx), dz), v[numY - N]));
+    } else if (fam_s(t)) {
+        r = add(r, mul(mul(mul(theta[3 * i + 1], dx), dz), v[numY]));
+    } else {
+        const double dxz = mul(dx, dz);
+        r = add(add(r, mul(mul(-theta[3 * (i - N) + 1], dxz), v[numY - N])), mul(mul(theta[3 * i + 1], dxz), v[numY]));
+    }
+    // + Dz w (divergence_discrete_operator_z.h:86-111)
+    double q;
+    if (t == 0) {
+        q = add(0.0, mul(0.0, w[z == 0 ? i : i - NM]));
+    } else if (fam_b(t)) {
+        q = add(0.0, mul(mul(mul(theta[3 * i + 2], dx), dy), w[i]));
+    } else if (fam_t(t)) {
+        q = add(0.0, mul(mul(mul(-theta[3 * (i - NM) + 2], dx), dy), w[i - NM]));
+    } else {
+        const double dxy = mul(dx, dy);
+        q = add(add(0.0, mul(mul(-theta[3 * (i - NM) + 2], dxy), w[i - NM])), mul(mul(theta[3 * i + 2], dxy), w[i]));
+    }
+    r = add(r, q);
+    if (i == pin0 || i == pin1) r = 0.0;
+    b[i] = r;
+}
+
+// Velocity update on one staggered grid (SetSolutions::correction,
+// Base/set_solutions.h:215-237, with GradientDiscreteOperatorX/Y/Z::calc,
+// DiscreteOperators/Gradient/gradient_discrete_operator_x.h:58-77, _y.h:52-74,
+// _z.h:45-62):  out = (G phi) * inv_vof + pred, where the staggered cell f
+// between base cells P and E = P + step carries (+c at P, -c at E),
+// c = (theta_P[comp] * d1_P) * d2_P, and a solid staggered cell one zero
+// entry at P.  dir 0: x-grid (N-1)MK, 1: y-grid N(M-1)K, 2: z-grid NM(K-1).
+__global__ void __launch_bounds__(256) k_projection_velocity(int dir, int N, int M, int K, const int* __restrict__ stype,
+                                                             const double* __restrict__ theta,
+                                                             const double* __restrict__ delta,
+                                                             const double* __restrict__ inv_vof,
+                                                             const double* __restrict__ phi,
+                                                             const double* __restrict__ pred,
+                                                             double* __restrict__ out)
+{
+    const int Ns = N - (dir == 0), Ms = M - (dir == 1);     // blockIdx.z runs over the K - (dir == 2) layers
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= Ns || y >= Ms) return;
+    const long long f = x + (long long)Ns * (y + (long long)Ms * z);
+    const long long p = x + (long long)N * (y + (long long)M * z);      // base cell below the face
+    const long long step = dir == 0 ? 1 : (dir == 1 ? N : (long long)N * M);
+    double g;
+    if (stype[f] == 0) {
+        g = add(0.0, mul(0.0, phi[p]));
+    } else {
+        // d1, d2: the two cell sizes across the face (y, z for x; x, z for y; x, y for z)
+        const double d1 = delta[3 * p + (dir == 0 ? 1 : 0)];
+        const double d2 = delta[3 * p + (dir == 2 ? 1 : 2)];
+        const double c = mul(mul(theta[3 * p + dir], d1), d2);
+        g = add(add(0.0, mul(c, phi[p])), mul(-c, phi[p + step]));
+    }
+    out[f] = add(mul(g, inv_vof[f]), pred[f]);
+}
+
+// Outflow clamp at the east boundary (SetSolutions::corrOutFlow,
+// Base/set_solutions.h:87-106) over y in [1, M-1), z in [1, K-1): where the
+// last two x-faces of a row carry backflow (u < 0) they are reset to vbase and
+// the matching v and w faces to zero.
+__global__ void k_outflow_east(int N, int M, int K, double vbase, double* __restrict__ u, double* __restrict__ v,
+                               double* __restrict__ w)
+{
+    const int y = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = 1 + blockIdx.y;
+    if (y >= M - 1 || z >= K - 1) return;
+    const long long NM = (long long)N * M;
+    const long long num = (long long)(y + 1) * N - 1 + z * NM;
+    long long num2 = num - y - 1 - (long long)z * M;
+    const long long num3 = num - (long long)z * N;
+    if (u[num2] < 0.0) {
+        u[num2] = vbase;
+        v[num3] = 0.0;
+        w[num] = 0.0;
+    }
+    num2--;
+    if (u[num2] < 0.0) {
+        u[num2] = vbase;
+        v[num3 - 1] = 0.0;
+        w[num - 1] = 0.0;
+    }
+}
+
+// Anti-backflow clamp on the bottom and top z-face layers
+// (SetSolutions::corrOutFlowTB, Base/set_solutions.h:111-118) over
+// x in [1, N), y in [1, M).
+__global__ void k_outflow_tb(int N, int M, int K, double* __restrict__ w)
+{
+    const int x = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = 1 + blockIdx.y;
+    if (x >= N || y >= M) return;
+    const long long num = x + (long long)y * N;
+    const long long top = num + (long long)(K - 2) * N * M;
+    if (w[num] > 0.0) w[num] = 0.0;
+    if (w[top] < 0.0) w[top] = 0.0;
+}
+
+// p += phi * coef (prediction.p *= coef; current.p += prediction.p).
+__global__ void k_pressure_update(long long n, double coef, const double* __restrict__ phi, double* __restrict__ p)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        p[i] = add(p[i], mul(phi[i], coef));
+}
+
+}  // namespace lsg

@@ -6,11 +6,13 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <memory>
 
 #include "lsg_ilu.cuh"
 #include "lsg_krylov.cuh"
+#include "lsg_projection.cuh"
 
 namespace lsg {
 
@@ -199,6 +201,15 @@ struct Context {
     // adjoint: a second solver state for the transposed operator, built on
     // first use and dropped whenever the operator changes
     std::unique_ptr<Context> adj;
+    // cut-cell geometry kept on the device by lsg_set_matrix_geometry (the
+    // projection kernels read it); staggered cell types from
+    // lsg_set_staggered_types
+    struct Geometry {
+        DevBuf<int> type, stype[3];
+        DevBuf<double> theta, delta, inv[3];
+        long long pin0 = -1, pin1 = -1;
+        bool have = false, have_stypes = false;
+    } geo;
 };
 
 }  // namespace lsg
@@ -618,9 +629,20 @@ static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStr
     const Dims& g = lv.d;
     if (d == 0) {
         const long long nl = (long long)g.M * g.K;
-        const int blocks = grid_for(nl * 32, 256, 148 * 64);
-        k_tdma_xwarp<T><<<blocks, 256, 0, s>>>(g.N, nl, lv.lo[0].p, lv.dinv[0].p, lv.up[0].p, lv.r.p, lv.c.p,
-                                               ch, omega);
+        constexpr int SEG = 8;
+        const int P = g.N / SEG;
+        // whole lines per warp, 16-byte aligned segments: power-of-two lengths 8..256
+        const bool pow2 = g.N >= SEG && (g.N & (g.N - 1)) == 0 && P <= 32;
+        const bool aligned = ((reinterpret_cast<uintptr_t>(ch) | reinterpret_cast<uintptr_t>(lv.c.p)) & 15) == 0;
+        if (pow2 && aligned) {
+            const long long threads = nl * P;
+            k_tdma_xseg<T, SEG><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
+                g.N, P, nl, lv.lo[0].p, lv.dinv[0].p, lv.up[0].p, lv.r.p, lv.c.p, ch, omega);
+        } else {
+            const int blocks = grid_for(nl * 32, 256, 148 * 64);
+            k_tdma_xwarp<T><<<blocks, 256, 0, s>>>(g.N, nl, lv.lo[0].p, lv.dinv[0].p, lv.up[0].p, lv.r.p, lv.c.p,
+                                                   ch, omega);
+        }
     } else {
         LineGeom lg{g.N, g.M, g.K, d};
         constexpr int SEG = 8;
@@ -1291,6 +1313,7 @@ static int set_matrix_impl(lsg_ctx* h, int N, int M, int K, const int* rowptr, c
     Context& C = h->c;
     LSG_REQUIRE(N >= 1 && M >= 1 && K >= 1, LSG_ERR_ARG, "grid dimensions must be positive");
     LSG_REQUIRE(rowptr && col && val, LSG_ERR_ARG, "null CSR pointer");
+    C.geo.have = C.geo.have_stypes = false;    // geometry of an earlier operator no longer applies
     LSG_CUDA(cudaSetDevice(C.device));
     const long long n = (long long)N * M * K;
     LSG_REQUIRE(n < (1LL << 31), LSG_ERR_ARG, "grid too large for 32-bit CSR indices");
@@ -1364,6 +1387,7 @@ int lsg_set_matrix_stencil7(lsg_ctx* h, int N, int M, int K, const double* plane
     Context& C = h->c;
     LSG_REQUIRE(N >= 1 && M >= 1 && K >= 1, LSG_ERR_ARG, "grid dimensions must be positive");
     LSG_REQUIRE(planes, LSG_ERR_ARG, "null planes");
+    C.geo.have = C.geo.have_stypes = false;    // geometry of an earlier operator no longer applies
     LSG_CUDA(cudaSetDevice(C.device));
     const long long n = (long long)N * M * K;
     LSG_REQUIRE(n < (1LL << 31), LSG_ERR_ARG, "grid too large");
@@ -1385,6 +1409,29 @@ int lsg_set_matrix_stencil7(lsg_ctx* h, int N, int M, int K, const double* plane
     LSG_API_END(h)
 }
 
+// Every face a row reads must exist: a cell whose type keeps a face (fluid,
+// cut or border family without that face) may not lie on the matching domain
+// border.  Checked on the host before the geometry reaches any kernel.
+static void check_cell_types(int N, int M, int K, const int* t)
+{
+    const long long NM = (long long)N * M;
+    for (int z = 0; z < K; z++)
+        for (int y = 0; y < M; y++)
+            for (int x = 0; x < N; x++) {
+                const long long i = x + N * (long long)y + NM * z;
+                if (t[i] == 0) continue;
+                const int miss = absent_faces(t[i]);
+                const bool ok = ((miss & 1) || z > 0) && ((miss & 2) || y > 0) && ((miss & 4) || x > 0) &&
+                                ((miss & 8) || x < N - 1) && ((miss & 16) || y < M - 1) && ((miss & 32) || z < K - 1);
+                if (!ok) {
+                    char buf[160];
+                    std::snprintf(buf, sizeof buf, "cell type %d at (%d, %d, %d) keeps a face outside the grid", t[i], x,
+                                  y, z);
+                    throw Error{LSG_ERR_ARG, buf};
+                }
+            }
+}
+
 int lsg_set_matrix_geometry(lsg_ctx* h, int N, int M, int K, const int* celltype, const double* theta,
                             const double* delta, const double* inv_mx, const double* inv_my, const double* inv_mz,
                             long long pin0, long long pin1)
@@ -1394,31 +1441,36 @@ int lsg_set_matrix_geometry(lsg_ctx* h, int N, int M, int K, const int* celltype
     Context& C = h->c;
     LSG_REQUIRE(N >= 2 && M >= 2 && K >= 2, LSG_ERR_ARG, "grid dimensions must be >= 2");
     LSG_REQUIRE(celltype && theta && delta && inv_mx && inv_my && inv_mz, LSG_ERR_ARG, "null geometry array");
-    LSG_CUDA(cudaSetDevice(C.device));
     const long long n = (long long)N * M * K;
     LSG_REQUIRE(n < (1LL << 31), LSG_ERR_ARG, "grid too large");
+    LSG_REQUIRE(pin0 >= -1 && pin0 < n && pin1 >= -1 && pin1 < n, LSG_ERR_ARG, "pinned row outside the grid");
+    check_cell_types(N, M, K, celltype);
+    LSG_CUDA(cudaSetDevice(C.device));
     const long long nx = (long long)(N - 1) * M * K, ny = (long long)N * (M - 1) * K, nz = (long long)N * M * (K - 1);
-    DevBuf<int> dt;
-    DevBuf<double> dth, dde, dmx, dmy, dmz;
-    dt.alloc(n);
-    dth.alloc(3 * n);
-    dde.alloc(3 * n);
-    dmx.alloc(nx);
-    dmy.alloc(ny);
-    dmz.alloc(nz);
-    LSG_CUDA(cudaMemcpyAsync(dt.p, celltype, n * sizeof(int), cudaMemcpyHostToDevice, C.s));
-    LSG_CUDA(cudaMemcpyAsync(dth.p, theta, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
-    LSG_CUDA(cudaMemcpyAsync(dde.p, delta, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
-    LSG_CUDA(cudaMemcpyAsync(dmx.p, inv_mx, nx * 8, cudaMemcpyHostToDevice, C.s));
-    LSG_CUDA(cudaMemcpyAsync(dmy.p, inv_my, ny * 8, cudaMemcpyHostToDevice, C.s));
-    LSG_CUDA(cudaMemcpyAsync(dmz.p, inv_mz, nz * 8, cudaMemcpyHostToDevice, C.s));
+    Context::Geometry& g = C.geo;
+    g.have = false;
+    g.have_stypes = false;
+    g.type.alloc(n);
+    g.theta.alloc(3 * n);
+    g.delta.alloc(3 * n);
+    g.inv[0].alloc(nx);
+    g.inv[1].alloc(ny);
+    g.inv[2].alloc(nz);
+    LSG_CUDA(cudaMemcpyAsync(g.type.p, celltype, n * sizeof(int), cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(g.theta.p, theta, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(g.delta.p, delta, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(g.inv[0].p, inv_mx, nx * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(g.inv[1].p, inv_my, ny * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(g.inv[2].p, inv_mz, nz * 8, cudaMemcpyHostToDevice, C.s));
+    g.pin0 = pin0;
+    g.pin1 = pin1;
     C.d.N = N;
     C.d.M = M;
     C.d.K = K;
     C.n = n;
     C.A7.alloc(7 * n);
-    k_laplace_from_geometry<<<grid_for(n, 256), 256, 0, C.s>>>(N, M, K, dt.p, dth.p, dde.p, dmx.p, dmy.p, dmz.p,
-                                                              pin0, pin1, C.A7.p);
+    k_laplace_from_geometry<<<grid_for(n, 256), 256, 0, C.s>>>(N, M, K, g.type.p, g.theta.p, g.delta.p, g.inv[0].p,
+                                                              g.inv[1].p, g.inv[2].p, pin0, pin1, C.A7.p);
     LSG_CHECK_LAUNCH();
     LSG_CUDA(cudaStreamSynchronize(C.s));
     C.nclass0 = build_dict(C.s, C.A7.p, 7, n, C.cls0, C.dict0);
@@ -1426,8 +1478,163 @@ int lsg_set_matrix_geometry(lsg_ctx* h, int N, int M, int K, const int* celltype
         context_release(*C.adj);
         C.adj.reset();
     }
+    g.have = true;
     C.have_matrix = true;
     C.have_setup = false;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_set_staggered_types(lsg_ctx* h, const int* xtype, const int* ytype, const int* ztype)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have, LSG_ERR_STATE, "no geometry set (lsg_set_matrix_geometry)");
+    LSG_REQUIRE(xtype && ytype && ztype, LSG_ERR_ARG, "null type array");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const long long cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
+                              (long long)d.N * d.M * (d.K - 1)};
+    const int* src[3] = {xtype, ytype, ztype};
+    for (int k = 0; k < 3; k++) {
+        C.geo.stype[k].alloc(cnt[k]);
+        LSG_CUDA(cudaMemcpyAsync(C.geo.stype[k].p, src[k], cnt[k] * sizeof(int), cudaMemcpyHostToDevice, C.s));
+    }
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    C.geo.have_stypes = true;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+static void projection_rhs(Context& C, const double* u, const double* v, const double* w, const double* flux, double* b)
+{
+    const Dims& d = C.d;
+    const Context::Geometry& g = C.geo;
+    k_projection_rhs<<<dim3((d.N + 31) / 32, (d.M + 7) / 8, d.K), dim3(32, 8), 0, C.s>>>(
+        d.N, d.M, d.K, g.type.p, g.theta.p, g.delta.p, flux, u, v, w, g.pin0, g.pin1, b);
+    LSG_CHECK_LAUNCH();
+}
+
+static void projection_correct(Context& C, const double* phi, const double* const pred[3], double* const out[3],
+                               double* p, double coef, double vbase, bool outflow)
+{
+    const Dims& d = C.d;
+    const Context::Geometry& g = C.geo;
+    for (int dir = 0; dir < 3; dir++) {
+        const int Ns = d.N - (dir == 0), Ms = d.M - (dir == 1), Ks = d.K - (dir == 2);
+        k_projection_velocity<<<dim3((Ns + 31) / 32, (Ms + 7) / 8, Ks), dim3(32, 8), 0, C.s>>>(
+            dir, d.N, d.M, d.K, g.stype[dir].p, g.theta.p, g.delta.p, g.inv[dir].p, phi, pred[dir], out[dir]);
+        LSG_CHECK_LAUNCH();
+    }
+    if (outflow) {
+        if (d.M > 2 && d.K > 2) {
+            k_outflow_east<<<dim3((d.M - 2 + 127) / 128, d.K - 2), 128, 0, C.s>>>(d.N, d.M, d.K, vbase, out[0], out[1],
+                                                                                 out[2]);
+            LSG_CHECK_LAUNCH();
+        }
+        k_outflow_tb<<<dim3((d.N - 1 + 127) / 128, d.M - 1), 128, 0, C.s>>>(d.N, d.M, d.K, out[2]);
+        LSG_CHECK_LAUNCH();
+    }
+    k_pressure_update<<<grid_for(C.n, 256), 256, 0, C.s>>>(C.n, coef, phi, p);
+    LSG_CHECK_LAUNCH();
+}
+
+int lsg_projection_rhs_device(lsg_ctx* h, const double* u, const double* v, const double* w, const double* flux,
+                              double* b)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have, LSG_ERR_STATE, "no geometry set (lsg_set_matrix_geometry)");
+    LSG_REQUIRE(u && v && w && flux && b, LSG_ERR_ARG, "null field");
+    LSG_CUDA(cudaSetDevice(C.device));
+    projection_rhs(C, u, v, w, flux, b);
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_projection_rhs(lsg_ctx* h, const double* u, const double* v, const double* w, const double* flux, double* b)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have, LSG_ERR_STATE, "no geometry set (lsg_set_matrix_geometry)");
+    LSG_REQUIRE(u && v && w && flux && b, LSG_ERR_ARG, "null field");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const long long n = C.n, cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
+                                       (long long)d.N * d.M * (d.K - 1)};
+    DevBuf<double> du, dv, dw, df, db;
+    du.alloc(cnt[0]);
+    dv.alloc(cnt[1]);
+    dw.alloc(cnt[2]);
+    df.alloc(n);
+    db.alloc(n);
+    LSG_CUDA(cudaMemcpyAsync(du.p, u, cnt[0] * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dv.p, v, cnt[1] * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dw.p, w, cnt[2] * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(df.p, flux, n * 8, cudaMemcpyHostToDevice, C.s));
+    projection_rhs(C, du.p, dv.p, dw.p, df.p, db.p);
+    LSG_CUDA(cudaMemcpyAsync(b, db.p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_projection_correct_device(lsg_ctx* h, const double* phi, const double* us, const double* vs, const double* ws,
+                                  double* u, double* v, double* w, double* p, double coef, double vbase, int outflow)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(phi && us && vs && ws && u && v && w && p, LSG_ERR_ARG, "null field");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const double* pred[3] = {us, vs, ws};
+    double* out[3] = {u, v, w};
+    projection_correct(C, phi, pred, out, p, coef, vbase, outflow != 0);
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_projection_correct(lsg_ctx* h, const double* phi, const double* us, const double* vs, const double* ws,
+                           double* u, double* v, double* w, double* p, double coef, double vbase, int outflow)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(phi && us && vs && ws && u && v && w && p, LSG_ERR_ARG, "null field");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const long long n = C.n, cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
+                                       (long long)d.N * d.M * (d.K - 1)};
+    DevBuf<double> dphi, dp, dpred[3], dout[3];
+    dphi.alloc(n);
+    dp.alloc(n);
+    const double* hpred[3] = {us, vs, ws};
+    double* hout[3] = {u, v, w};
+    LSG_CUDA(cudaMemcpyAsync(dphi.p, phi, n * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dp.p, p, n * 8, cudaMemcpyHostToDevice, C.s));
+    const double* pred[3];
+    double* out[3];
+    for (int k = 0; k < 3; k++) {
+        dpred[k].alloc(cnt[k]);
+        dout[k].alloc(cnt[k]);
+        LSG_CUDA(cudaMemcpyAsync(dpred[k].p, hpred[k], cnt[k] * 8, cudaMemcpyHostToDevice, C.s));
+        pred[k] = dpred[k].p;
+        out[k] = dout[k].p;
+    }
+    projection_correct(C, dphi.p, pred, out, dp.p, coef, vbase, outflow != 0);
+    for (int k = 0; k < 3; k++)
+        LSG_CUDA(cudaMemcpyAsync(hout[k], dout[k].p, cnt[k] * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaMemcpyAsync(p, dp.p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
     return LSG_OK;
     LSG_API_END(h)
 }

@@ -50,7 +50,8 @@ EXPORTS = [
     "lsg_precond_apply", "lsg_mg_num_levels", "lsg_mg_level_dims", "lsg_mg_level_csr",
     "lsg_mg_level_tridiag", "lsg_profile_kernel", "lsg_residual_norm_noalloc", "lsg_apply_transpose",
     "lsg_solve_adjoint", "lsg_operator_gradient", "lsg_set_matrix_geometry", "lsg_get_matrix_stencil7",
-    "lsg_version",
+    "lsg_set_staggered_types", "lsg_projection_rhs", "lsg_projection_rhs_device", "lsg_projection_correct",
+    "lsg_projection_correct_device", "lsg_version",
 ]
 
 _lib = None
@@ -99,6 +100,11 @@ def load() -> C.CDLL:
     lib.lsg_set_matrix_geometry.argtypes = [P, C.c_int, C.c_int, C.c_int, ip, dp, dp, dp, dp, dp, C.c_longlong,
                                             C.c_longlong]
     lib.lsg_get_matrix_stencil7.argtypes = [P, dp]
+    lib.lsg_set_staggered_types.argtypes = [P, ip, ip, ip]
+    lib.lsg_projection_rhs.argtypes = [P, dp, dp, dp, dp, dp]
+    lib.lsg_projection_rhs_device.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.lsg_projection_correct.argtypes = [P, dp, dp, dp, dp, dp, dp, dp, dp, C.c_double, C.c_double, C.c_int]
+    lib.lsg_projection_correct_device.argtypes = [P] + [C.c_void_p] * 8 + [C.c_double, C.c_double, C.c_int]
     lib.lsg_version.restype = C.c_char_p
     _lib = lib
     return lib

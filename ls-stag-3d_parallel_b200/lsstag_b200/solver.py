@@ -99,6 +99,29 @@ class IterativeSolver:
         if setup:
             self._setup()
 
+    # -- pressure projection (needs set_geometry) -----------------------------
+    def set_staggered_types(self, xtype, ytype, ztype):
+        self._stypes = tuple(np.ascontiguousarray(t, dtype=np.int32) for t in (xtype, ytype, ztype))
+        self.ctx.check(self.ctx.lib.lsg_set_staggered_types(self.ctx.h, *(L.iptr(t) for t in self._stypes)))
+
+    def projection_rhs(self, u, v, w, flux) -> np.ndarray:
+        """b = Dx u + Dy v + Dz w + flux, b[pins] = 0 (recalcRightMember)."""
+        args = [np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, w, flux)]
+        b = np.empty(int(np.prod(self.dims)))
+        self.ctx.check(self.ctx.lib.lsg_projection_rhs(self.ctx.h, *(L.dptr(a) for a in args), L.dptr(b)))
+        return b
+
+    def projection_correct(self, phi, us, vs, ws, p, coef, vbase, outflow=True):
+        """(u, v, w, p) after SetSolutions::correction; p is updated in place."""
+        ins = [np.ascontiguousarray(a, dtype=np.float64) for a in (phi, us, vs, ws)]
+        outs = [np.empty_like(a) for a in ins[1:]]
+        if not (p.dtype == np.float64 and p.flags.c_contiguous):
+            raise ValueError("p must be a C-contiguous float64 array (updated in place)")
+        self.ctx.check(self.ctx.lib.lsg_projection_correct(self.ctx.h, *(L.dptr(a) for a in ins),
+                                                           *(L.dptr(a) for a in outs), L.dptr(p), float(coef),
+                                                           float(vbase), int(bool(outflow))))
+        return outs[0], outs[1], outs[2], p
+
     def planes(self) -> np.ndarray:
         n = int(np.prod(self.dims))
         P = np.empty((7, n))

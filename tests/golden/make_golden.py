@@ -8,7 +8,10 @@ Each fixture is a compressed .npz holding the case's Laplace CSR exactly as
 the reference assembles it (laplace_discrete_operator.h), the seeded
 right-hand side, and the reference's outputs: its multigrid hierarchy
 (P, R, A_H, factored ADLJ tridiagonals), one V-cycle, one MG-FGMRES(30) solve
-and one ILU(0)-BiCGStab solve to a 1e-10 relative residual.
+and one ILU(0)-BiCGStab solve to a 1e-10 relative residual; the projection
+operators (divergence Dx/Dy/Dz, gradient Gx/Gy/Gz, staggered cell types) and
+one pressure projection of the time step (right-hand side, MG-FGMRES pressure
+correction, corrected u, v, w, p) on seeded predicted fields.
 """
 from __future__ import annotations
 
@@ -21,6 +24,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "ls-stag-3d_parallel_b200"))
 
+import lsg_oracle as lo  # noqa: E402
 import ref_runner as rr  # noqa: E402
 from lsstag_b200 import synth  # noqa: E402
 
@@ -61,6 +65,26 @@ def main():
                 "fgmres_norm_r": r["fgmres_norm_r"], "bicgstab_x": r["bicgstab_x"],
                 "bicgstab_it": r["bicgstab_it"], "bicgstab_norm_r": r["bicgstab_norm_r"],
                 "mg_nlev": r["mg_nlev"]}
+        # one pressure projection on seeded predicted velocities and pressure
+        N, M, K = dims
+        gp = rr.run(case, threads=1, dump_projection=1)
+        rng = np.random.default_rng(100 + seed)
+        pu = 1.0 + 0.1 * rng.standard_normal((N - 1) * M * K)
+        pv = 0.1 * rng.standard_normal(N * (M - 1) * K)
+        pw = 0.1 * rng.standard_normal(N * M * (K - 1))
+        pp = rng.standard_normal(N * M * K)
+        D = tuple(rr.csr(gp, k)[:3] for k in ("Dx", "Dy", "Dz"))
+        bproj = lo.projection_rhs(D, pu, pv, pw, gp["flux"], gp["pins"])
+        pr = rr.run_projection(case, pu, pv, pw, pp, 1e-10 * float(np.linalg.norm(bproj)))
+        for k in ("xtype", "ytype", "ztype"):
+            keep[k] = gp[k]
+        for m in ("Dx", "Dy", "Dz", "Gx", "Gy", "Gz"):
+            for part in ("rowptr", "col", "val"):
+                keep[f"{m}_{part}"] = gp[f"{m}_{part}"]
+        keep.update(proj_u_in=pu, proj_v_in=pv, proj_w_in=pw, proj_p_in=pp)
+        for k in ("proj_b", "proj_phi", "proj_it", "proj_u_out", "proj_v_out", "proj_w_out", "proj_p_out", "proj_coef",
+                  "proj_vbase"):
+            keep[k] = pr[k]
         for l in range(int(r["mg_nlev"][0])):
             for m in ("P", "R", "AH"):
                 for part in ("rowptr", "col", "val", "dims"):
