@@ -75,12 +75,12 @@ __global__ void __launch_bounds__(256) k_spmv_dot7(int N, int M, int K, const in
 //   MODE 1:  w = v - A z,  out = (w, w)      (residual and its squared norm)
 // z is FP64, or FP32 widened exactly.  Terms are summed p, b, s, w, e, n, t.
 template <typename Tz, int MODE>
-__global__ void __launch_bounds__(256) k_krylov7z(int N, int M, int K, int zc, const int* __restrict__ cls,
+__global__ void __launch_bounds__(256, 3) k_krylov7z(int N, int M, int K, int zc, const int* __restrict__ cls,
                                                    const double* __restrict__ dict, const Tz* __restrict__ z,
                                                    const double* __restrict__ v, double* __restrict__ w,
                                                    double* partial, unsigned int* counter, double* out)
 {
-    constexpr int U = 4;
+    constexpr int U = sizeof(Tz) == 4 ? 8 : 4;            // z-steps of DRAM loads in flight per thread
     double s[1] = {0.0};
     const int ix = blockIdx.x * 32 + threadIdx.x;
     const int iy = blockIdx.y * 8 + threadIdx.y;
@@ -93,33 +93,32 @@ __global__ void __launch_bounds__(256) k_krylov7z(int N, int M, int K, int zc, c
         Tz xc = z[i];
         const bool hasw = ix > 0, hase = ix < N - 1, hass = iy > 0, hasn = iy < M - 1;
         for (int zb = z0; zb < z1; zb += U, i += U * NM) {
+            // the streams from DRAM (class, v, next plane) for U steps first;
+            // the four lateral neighbours were just read by the adjacent
+            // threads and come from L1 inside the step
             int cl[U];
             double vv[U];
-            Tz xs[U], xw[U], xe[U], xn[U], xp[U];
+            Tz xp[U];
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const int zz = zb + u;
                 const int ii = (zz < z1) ? i + u * NM : i;
                 cl[u] = cls[ii];
                 vv[u] = v[ii];
-                xs[u] = hass ? z[ii - N] : (Tz)0;
-                xw[u] = hasw ? z[ii - 1] : (Tz)0;
-                xe[u] = hase ? z[ii + 1] : (Tz)0;
-                xn[u] = hasn ? z[ii + N] : (Tz)0;
                 xp[u] = (zz < K - 1) ? z[ii + NM] : (Tz)0;
             }
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 if (zb + u < z1) {
+                    const int ii = i + u * NM;
                     const double* a = dict + (size_t)cl[u] * 7;
                     double acc = a[3] * (double)xc;
                     acc += a[0] * (double)xm;
-                    if (hass) acc += a[1] * (double)xs[u];
-                    if (hasw) acc += a[2] * (double)xw[u];
-                    if (hase) acc += a[4] * (double)xe[u];
-                    if (hasn) acc += a[5] * (double)xn[u];
+                    if (hass) acc += a[1] * (double)z[ii - N];
+                    if (hasw) acc += a[2] * (double)z[ii - 1];
+                    if (hase) acc += a[4] * (double)z[ii + 1];
+                    if (hasn) acc += a[5] * (double)z[ii + N];
                     acc += a[6] * (double)xp[u];
-                    const int ii = i + u * NM;
                     if (MODE == 0) {
                         w[ii] = acc;
                         s[0] += acc * vv[u];

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <memory>
 
+#include "lsg_coarse.cuh"
 #include "lsg_ilu.cuh"
 #include "lsg_krylov.cuh"
 #include "lsg_projection.cuh"
@@ -162,6 +163,11 @@ struct MGData {
     DevBuf<double> dL, dU, dscale, dwork;
     DevBuf<int> dperm;
     bool fp32 = false;
+    // lower part of the cycle fused into k_vcycle_tail from level tail_l0 on
+    // (-1: every level runs as separate kernels)
+    int tail_l0 = -1;
+    DevBuf<TailArgs<double>> tail64;
+    DevBuf<TailArgs<float>> tail32;
 };
 
 // ---------------------------------------------------------------------------
@@ -403,6 +409,85 @@ static void alloc_vectors(LevelT<T>& lv)
     lv.ch.alloc(n);
 }
 
+// First level from which the rest of the cycle fits the one-CTA tail kernel:
+// every level from there down holds at most kTailMaxCells cells, and every
+// smoothed one is a 27-point Galerkin level.
+static int tail_first_level(const MGData& mg)
+{
+    const int L = mg.L;
+    if (L < 2) return -1;
+    int l0 = -1;
+    for (int l = L - 1; l >= 1; l--) {
+        const LevelT<double>& lv = mg.l64[l];
+        if (lv.d.n() > kTailMaxCells || lv.ol.n != 27 || !lv.dict28.p) break;
+        l0 = l;
+    }
+    if (l0 >= 0 && L - l0 + 1 > kTailMaxLevels) return -1;
+    return l0;
+}
+
+template <typename T>
+static void fill_tail(const MGData& mg, const std::vector<LevelT<T>>& lev, int l0, const Context& C, TailArgs<T>& A)
+{
+    std::memset(&A, 0, sizeof(A));
+    const int L = mg.L;
+    A.nlev = L - l0 + 1;
+    for (int l = l0; l <= L; l++) {
+        TailLevel<T>& t = A.lev[l - l0];
+        const LevelT<T>& lv = lev[l];
+        t.N = lv.d.N;
+        t.M = lv.d.M;
+        t.K = lv.d.K;
+        t.cls = lv.cls;
+        t.dict28 = lv.dict28.p;
+        for (int d = 0; d < 3; d++) {
+            t.lo[d] = lv.lo[d].p;
+            t.dinv[d] = lv.dinv[d].p;
+            t.up[d] = lv.up[d].p;
+        }
+        t.r = const_cast<T*>(lv.r.p);
+        t.c = const_cast<T*>(lv.c.p);
+        t.ch = const_cast<T*>(lv.ch.p);
+        if (l < L) {
+            const TransferTabs& tb = mg.tabs[l];
+            t.px = tb.P(0);
+            t.py = tb.P(1);
+            t.pz = tb.P(2);
+            t.rx = tb.R(0);
+            t.ry = tb.R(1);
+            t.rz = tb.R(2);
+            t.agg = mg.agg[l] ? 1 : 0;
+        }
+    }
+    A.nc = mg.nc;
+    A.L = mg.dL.p;
+    A.U = mg.dU.p;
+    A.scale = mg.dscale.p;
+    A.perm = mg.dperm.p;
+    A.work = mg.dwork.p;
+    A.n_post = C.opt.n_post;
+    A.zquirk = C.opt.zline_reference != 0;
+    A.omega = (T)C.opt.omega;
+}
+
+static void tail_setup(Context& C)
+{
+    MGData& mg = C.mg;
+    mg.tail_l0 = tail_first_level(mg);
+    if (mg.tail_l0 < 0) return;
+    TailArgs<double> a64;
+    fill_tail<double>(mg, mg.l64, mg.tail_l0, C, a64);
+    mg.tail64.alloc(1);
+    LSG_CUDA(cudaMemcpyAsync(mg.tail64.p, &a64, sizeof(a64), cudaMemcpyHostToDevice, C.s));
+    if (mg.fp32) {
+        TailArgs<float> a32;
+        fill_tail<float>(mg, mg.l32, mg.tail_l0, C, a32);
+        mg.tail32.alloc(1);
+        LSG_CUDA(cudaMemcpyAsync(mg.tail32.p, &a32, sizeof(a32), cudaMemcpyHostToDevice, C.s));
+    }
+    LSG_CUDA(cudaStreamSynchronize(C.s));    // the host copies of the arguments go out of scope
+}
+
 static void mg_setup(Context& C)
 {
     MGData& mg = C.mg;
@@ -590,6 +675,7 @@ static void mg_setup(Context& C)
             alloc_vectors(b);
         }
     }
+    tail_setup(C);
     LSG_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -672,7 +758,8 @@ static void vcycle(Context& C, std::vector<LevelT<T>>& lev, T* ch0 = nullptr)
     MGData& mg = C.mg;
     cudaStream_t s = C.s;
     const int L = mg.L;
-    for (int l = 0; l < L; l++) {
+    const int lt = mg.tail_l0;              // levels lt..L run inside k_vcycle_tail
+    for (int l = 0; l < (lt >= 0 ? lt : L); l++) {
         const Dims& f = lev[l].d;
         const Dims& c = lev[l + 1].d;
         const TransferTabs& t = mg.tabs[l];
@@ -680,12 +767,17 @@ static void vcycle(Context& C, std::vector<LevelT<T>>& lev, T* ch0 = nullptr)
                                                           lev[l].r.p, lev[l + 1].r.p);
         LSG_CHECK_LAUNCH();
     }
-    k_coarse_solve<T><<<1, 32, 0, s>>>(mg.nc, mg.dL.p, mg.dU.p, mg.dscale.p, mg.dperm.p, lev[L].r.p, lev[L].ch.p,
-                                       mg.dwork.p);
+    if (lt >= 0) {
+        if constexpr (sizeof(T) == 8) k_vcycle_tail<double><<<1, kTailThreads, 0, s>>>(mg.tail64.p);
+        else k_vcycle_tail<float><<<1, kTailThreads, 0, s>>>(mg.tail32.p);
+    } else {
+        k_coarse_solve<T><<<1, 32, 0, s>>>(mg.nc, mg.dL.p, mg.dU.p, mg.dscale.p, mg.dperm.p, lev[L].r.p, lev[L].ch.p,
+                                           mg.dwork.p);
+    }
     LSG_CHECK_LAUNCH();
     const T omega = (T)C.opt.omega;
     const bool zq = C.opt.zline_reference != 0;
-    for (int l = L - 1; l >= 0; l--) {
+    for (int l = (lt >= 0 ? lt : L) - 1; l >= 0; l--) {
         LevelT<T>& lv = lev[l];
         const Dims& f = lv.d;
         const TransferTabs& t = mg.tabs[l];
