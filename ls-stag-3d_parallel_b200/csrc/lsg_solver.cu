@@ -715,15 +715,23 @@ static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStr
     const Dims& g = lv.d;
     if (d == 0) {
         const long long nl = (long long)g.M * g.K;
-        constexpr int SEG = 8;
-        const int P = g.N / SEG;
-        // whole lines per warp, 16-byte aligned segments: power-of-two lengths 8..256
-        const bool pow2 = g.N >= SEG && (g.N & (g.N - 1)) == 0 && P <= 32;
+        // whole lines per warp with 16-byte aligned segments: lengths SEG * P,
+        // P a power of two <= 32 (SEG 8: 8..256, SEG 12: 12..384)
+        auto xseg_p = [&](int seg) {
+            if (g.N % seg) return 0;
+            const int P = g.N / seg;
+            return (P <= 32 && (P & (P - 1)) == 0) ? P : 0;
+        };
         const bool aligned = ((reinterpret_cast<uintptr_t>(ch) | reinterpret_cast<uintptr_t>(lv.c.p)) & 15) == 0;
-        if (pow2 && aligned) {
-            const long long threads = nl * P;
-            k_tdma_xseg<T, SEG><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-                g.N, P, nl, lv.lo[0].p, lv.dinv[0].p, lv.up[0].p, lv.r.p, lv.c.p, ch, omega);
+        const int P8 = xseg_p(8), P12 = xseg_p(12);
+        if (aligned && P8) {
+            const long long threads = nl * P8;
+            k_tdma_xseg<T, 8><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
+                g.N, P8, nl, lv.lo[0].p, lv.dinv[0].p, lv.up[0].p, lv.r.p, lv.c.p, ch, omega);
+        } else if (aligned && P12) {
+            const long long threads = nl * P12;
+            k_tdma_xseg<T, 12><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
+                g.N, P12, nl, lv.lo[0].p, lv.dinv[0].p, lv.up[0].p, lv.r.p, lv.c.p, ch, omega);
         } else {
             const int blocks = grid_for(nl * 32, 256, 148 * 64);
             k_tdma_xwarp<T><<<blocks, 256, 0, s>>>(g.N, nl, lv.lo[0].p, lv.dinv[0].p, lv.up[0].p, lv.r.p, lv.c.p,
@@ -731,16 +739,29 @@ static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStr
         }
     } else {
         LineGeom lg{g.N, g.M, g.K, d};
-        constexpr int SEG = 8;
         constexpr int MAXT = sizeof(T) == 4 ? 512 : 256;
-        const int S = (lg.len() + SEG - 1) / SEG;
-        if (S * 8 <= MAXT) {
-            // W lines per CTA: as many as fit MAXT threads, at most 32 (one warp row)
+        const int L = lg.len();
+        const long long rows = d == 1 ? g.K : g.M;
+        // W lines per CTA (as many as fit MAXT threads, at most 32: one warp
+        // row of x) times S segments; the segment chain is sequential, so in
+        // FP32 longer segments (12 cells) are used where 8-cell ones would
+        // give more than 32 of them.  In FP64 the 12-cell segments need 166
+        // registers a thread, and at 384^3 the strided solve measured faster.
+        auto pick_w = [&](int S) {
             int W = 8;
             while (W < 32 && 2 * W * S <= MAXT) W *= 2;
-            const long long blocks = (long long)((g.N + W - 1) / W) * (d == 1 ? g.K : g.M);
-            const size_t smem = 2 * (size_t)W * S * sizeof(T);
-            k_tdma_seg<T, SEG, MAXT, 2><<<(unsigned)blocks, dim3(W, S), smem, s>>>(
+            return W;
+        };
+        const int S8 = (L + 7) / 8, S12 = (L + 11) / 12;
+        if (8 * S8 <= MAXT && (S8 <= 32 || 8 * S12 > MAXT)) {
+            const int W = pick_w(S8);
+            const long long blocks = (long long)((g.N + W - 1) / W) * rows;
+            k_tdma_seg<T, 8, MAXT, 2><<<(unsigned)blocks, dim3(W, S8), 2 * (size_t)W * S8 * sizeof(T), s>>>(
+                lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, ch, omega);
+        } else if (sizeof(T) == 4 && 8 * S12 <= MAXT) {
+            const int W = pick_w(S12);
+            const long long blocks = (long long)((g.N + W - 1) / W) * rows;
+            k_tdma_seg<T, 12, MAXT, 1><<<(unsigned)blocks, dim3(W, S12), 2 * (size_t)W * S12 * sizeof(T), s>>>(
                 lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, ch, omega);
         } else {
             k_tdma_strided<T><<<grid_for(lg.nlines(), 128, 148 * 64), 128, 0, s>>>(

@@ -54,8 +54,10 @@ class IterativeSolver:
         self._x = None
 
     # -- IterativeSolverInterface::set ------------------------------------
-    def set(self, A, b: np.ndarray | None = None, x: np.ndarray | None = None, task: Task | None = None):
-        """A = (rowptr, col, val, (N, M, K)) in the reference's CSR layout."""
+    def set(self, A, b: np.ndarray | None = None, x: np.ndarray | None = None, task: Task | None = None,
+            setup: bool = True):
+        """A = (rowptr, col, val, (N, M, K)) in the reference's CSR layout.
+        setup=False stores the operator only (for apply())."""
         rowptr, col, val, dims = A
         task = task or Task()
         self.task = task
@@ -67,7 +69,8 @@ class IterativeSolver:
         N, M, K = self.dims
         self.ctx.check(self.ctx.lib.lsg_set_matrix_csr(self.ctx.h, N, M, K, L.iptr(self._rowptr), L.iptr(self._col),
                                                        L.dptr(self._val)))
-        self._setup()
+        if setup:
+            self._setup()
         self._b, self._x = b, x
 
     def set_planes(self, planes: np.ndarray, dims, task: Task | None = None):

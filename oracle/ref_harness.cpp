@@ -354,6 +354,20 @@ int main(int argc, char** argv)
     SetSolutions* sol = new SetSolutions;
     sol->init(task, &it);
     task->initSol(&(sol->current), &(sol->prediction), &(sol->previous));
+    if ((int)cfg.get("operator_only", 0)) {
+        // the Laplace operator alone (LaplaceDiscreteOperator::init + build), without
+        // the pressure equation's solver set-up, whose multigrid hierarchy does not
+        // fit host memory on the largest grids
+        LaplaceDiscreteOperator* Aop = new LaplaceDiscreteOperator;   // not destroyed (see below)
+        Aop->init(task, &task->m_mesh->baseMesh);
+        LSSTAGUniformMesh* mm = task->m_mesh;
+        int dd[3] = {mm->baseMesh.N, mm->baseMesh.M, mm->baseMesh.K};
+        out.i("dims", dd, 3);
+        out.csr("A", (SparseMatrix*)Aop);
+        int pp[2] = {Aop->fixPointNum, Aop->fixPointFlowNum};
+        out.i("pins", pp, 2);
+        return 0;
+    }
     PoissonDiscreteEquation* pEq = new PoissonDiscreteEquation;
     pEq->set(task, &(sol->prediction.p));
     double t_setup = now_s() - t0;
@@ -430,6 +444,49 @@ int main(int argc, char** argv)
     //     pEq.solve() then sol.correction()) on predicted velocities read from
     //     files: the right-hand side (PoissonDiscreteEquation::recalcRightMember),
     //     the MG-FGMRES pressure correction and the corrected fields ---
+    // --- the momentum equations as the time step builds them
+    //     (TimeSteppingMethod::init: uEq/vEq/wEq.set): the Helmholtz operators
+    //     K (HelmholtzDiscreteOperatorX/Y/Z), the convective operators C
+    //     (ConvectiveDiscreteOperatorX/Y/Z, recalculated on the initial
+    //     velocity) and one solve of each K with the momentum solver
+    //     (ILUFGMRES) on a right-hand side read from a file ---
+    if ((int)cfg.get("momentum", 0)) {
+        HelmholtzDiscreteEquationX* ux = new HelmholtzDiscreteEquationX;   // not destroyed (see below)
+        HelmholtzDiscreteEquationY* vy = new HelmholtzDiscreteEquationY;
+        HelmholtzDiscreteEquationZ* wz = new HelmholtzDiscreteEquationZ;
+        ux->set(task, &(sol->prediction.u));
+        vy->set(task, &(sol->prediction.v));
+        wz->set(task, &(sol->prediction.w));
+        HelmholtzDiscreteEquation* eq[3] = {ux, vy, wz};
+        const char* nm[3] = {"x", "y", "z"};
+        const double meps = cfg.get("mom_rel_tol", 1e-10);
+        for (int d = 0; d < 3; d++) {
+            HelmholtzDiscreteEquation* e = eq[d];
+            const long ne = e->m_A->NMK;
+            out.csr(std::string("K") + nm[d], (SparseMatrix*)e->m_A);
+            out.csr(std::string("C") + nm[d], (SparseMatrix*)e->m_conv);
+            std::vector<double> rhs(ne, 0.0);
+            std::ifstream f(cfg.gets(std::string("mom_rhs_") + nm[d], ""), std::ios::binary);
+            f.read((char*)rhs.data(), sizeof(double) * ne);
+            if (!f) {
+                fprintf(stderr, "cannot read momentum rhs %s\n", nm[d]);
+                return 3;
+            }
+            double bn = 0.0;
+            for (double v : rhs) bn += v * v;
+            std::copy(rhs.begin(), rhs.end(), e->m_right);
+            std::fill(e->m_sol, e->m_sol + ne, 0.0);
+            e->solver.eps = meps * sqrt(bn);
+            int mit = e->solver.solve();
+            out.d(std::string("mom_x_") + nm[d], e->m_sol, ne);
+            out.i(std::string("mom_it_") + nm[d], &mit, 1);
+            out.scalar(std::string("mom_eps_") + nm[d], e->solver.eps);
+        }
+        int rs = task->FGMRES_RESTART_NUM, mi = task->MAX_ITER;
+        out.i("mom_restart", &rs, 1);
+        out.i("mom_max_it", &mi, 1);
+        return 0;
+    }
     if ((int)cfg.get("projection", 0)) {
         task->tScaleP = -1.0;                     // no start-up pressure scaling
         const double coefP = 1.5 / task->t;       // HelmholtzDiscreteEquation::coef (BDF2)

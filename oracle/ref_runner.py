@@ -170,3 +170,37 @@ def run_projection(case: Case, u: np.ndarray, v: np.ndarray, w: np.ndarray, p: n
     finally:
         import shutil
         shutil.rmtree(d, ignore_errors=True)
+
+
+def run_momentum(case: Case, rhs_xyz, rel_tol: float = 1e-10, *, threads: int = 1, timeout: float = 3600,
+                 **opts) -> dict:
+    """The reference's momentum equations for a case (harness ``momentum``
+    mode): Helmholtz operators Kx/Ky/Kz and convective operators Cx/Cy/Cz in
+    CSR form, and the momentum solver (ILU-FGMRES) on each K with the given
+    right-hand sides (x-, y-, z-grid) to rel_tol * ||rhs||."""
+    if not available():
+        raise FileNotFoundError(REF_BIN)
+    d = tempfile.mkdtemp(prefix="lsg_mom_")
+    try:
+        lines = case.config_lines()
+        if threads:
+            lines.append(f"threads {threads}")
+        for k, val in opts.items():
+            lines.append(f"{k} {val!r}" if isinstance(val, float) else f"{k} {val}")
+        for name, arr in zip("xyz", rhs_xyz):
+            path = os.path.join(d, f"mom_rhs_{name}.in")
+            np.ascontiguousarray(arr, dtype=np.float64).tofile(path)
+            lines.append(f"mom_rhs_{name} {path}")
+        n = case.N * case.M * case.K
+        rhs = os.path.join(d, "rhs.in")
+        np.zeros(n).tofile(rhs)
+        lines += [f"rhs {rhs}", "abs_tol 1.0", "momentum 1", f"mom_rel_tol {float(rel_tol)!r}"]
+        cfg = os.path.join(d, "case.cfg")
+        with open(cfg, "w") as f:
+            f.write("\n".join(lines) + "\n")
+        subprocess.run([REF_BIN, cfg, d], check=True, timeout=timeout, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.PIPE)
+        return load_dir(d)
+    finally:
+        import shutil
+        shutil.rmtree(d, ignore_errors=True)

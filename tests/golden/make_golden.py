@@ -11,7 +11,9 @@ right-hand side, and the reference's outputs: its multigrid hierarchy
 and one ILU(0)-BiCGStab solve to a 1e-10 relative residual; the projection
 operators (divergence Dx/Dy/Dz, gradient Gx/Gy/Gz, staggered cell types) and
 one pressure projection of the time step (right-hand side, MG-FGMRES pressure
-correction, corrected u, v, w, p) on seeded predicted fields.
+correction, corrected u, v, w, p) on seeded predicted fields; the momentum
+operators (Helmholtz Kx/Ky/Kz, convective Cx/Cy/Cz) and one ILU-FGMRES solve
+of each Helmholtz system.
 """
 from __future__ import annotations
 
@@ -85,6 +87,21 @@ def main():
         for k in ("proj_b", "proj_phi", "proj_it", "proj_u_out", "proj_v_out", "proj_w_out", "proj_p_out", "proj_coef",
                   "proj_vbase"):
             keep[k] = pr[k]
+        # the momentum equations: Helmholtz and convective operators on the
+        # staggered grids and one ILU-FGMRES solve of each Helmholtz system
+        # (right-hand side zero on solid staggered cells, like the pressure one)
+        mrhs = [rng.standard_normal((N - 1) * M * K) * (gp["xtype"] != 0),
+                rng.standard_normal(N * (M - 1) * K) * (gp["ytype"] != 0),
+                rng.standard_normal(N * M * (K - 1)) * (gp["ztype"] != 0)]
+        mr = rr.run_momentum(case, mrhs)
+        for d, rhs_d in zip("xyz", mrhs):
+            for m in ("K", "C"):
+                for part in ("rowptr", "col", "val", "dims"):
+                    keep[f"{m}{d}_{part}"] = mr[f"{m}{d}_{part}"]
+            keep[f"mom_rhs_{d}"] = rhs_d
+            for k in ("mom_x_", "mom_it_", "mom_eps_"):
+                keep[k + d] = mr[k + d]
+        keep["mom_restart"] = mr["mom_restart"]
         for l in range(int(r["mg_nlev"][0])):
             for m in ("P", "R", "AH"):
                 for part in ("rowptr", "col", "val", "dims"):

@@ -119,3 +119,21 @@ def test_oracle_projection_matches_reference(name):
                                        float(g["proj_vbase"][0]))
     for mine, key in ((u, "proj_u_out"), (v, "proj_v_out"), (w, "proj_w_out"), (p, "proj_p_out")):
         assert np.array_equal(mine.view(np.int64), g[key].view(np.int64)), key
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_oracle_momentum_ilu_fgmres(name):
+    """ILU(0)-FGMRES(13) on the reference's Helmholtz systems (the momentum
+    solver of each time step): the reference's iteration count and solution."""
+    g = load_golden(name)
+    for d in "xyz":
+        rp, col, val = g[f"K{d}_rowptr"], g[f"K{d}_col"], g[f"K{d}_val"]
+        n = rp.size - 1
+        A = sp.csr_matrix((val, col, rp), shape=(n, n))
+        LU = lo.ilu0(A)
+        b = g[f"mom_rhs_{d}"]
+        x, it, _ = lo.fgmres(A, b, np.zeros(n), lambda v: lo.ilu_solve(LU, v), float(g[f"mom_eps_{d}"][0]),
+                             int(g["mom_restart"][0]), 200)
+        assert it == int(g[f"mom_it_{d}"][0]), d
+        ref = g[f"mom_x_{d}"]
+        assert np.linalg.norm(x - ref) <= 1e-12 * np.linalg.norm(ref), d
