@@ -105,7 +105,10 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup(args):
+def dist_setup(args, backend: str = "nccl"):
+    """One process per GPU (replicas): rank/world from the torchrun
+    environment; the process group only carries the barrier and the max over
+    ranks of the timings (gloo on CPU for the host-side tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -115,8 +118,9 @@ def dist_setup(args):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
 
@@ -125,7 +129,8 @@ def barrier_max(pg, value: float, local: int) -> float:
     if pg is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dev = f"cuda:{local}" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 

@@ -151,6 +151,21 @@ int lsg_get_matrix_stencil7(lsg_ctx* ctx, double* planes);
    the z-grid (NM(K-1)), base-grid fields (flux, b, phi, p) NMK, x fastest.
    Results equal the reference's bit for bit. */
 
+/* Source term of the pressure equation, LaplaceDiscreteOperator::flux after
+   initMeshParams + calcFlux for a flow task with fixed bodies
+   (DiscreteOperators/WithFlux/Sym/laplace_discrete_operator.h:47-83, :687-808):
+   immersed-boundary term on cut cells, inflow profile, N/S and T/B wall
+   velocities, outflow from u.  side_type[3n] (the cell's e, n, t face types,
+   LSSTAGUniformMesh baseSideTypes, cut_sides.h SideTypes codes), vib[3n] (the
+   immersed-boundary velocity, v_ib), u_w[M*K] (inflow profile pU_W, index
+   y + M z), bc = {U_E, V_S, V_N, W_B, W_T} (host memory in both variants),
+   ux the x-grid velocity; flux[n] out.  Host pointers. */
+int lsg_laplace_flux(lsg_ctx* ctx, const int* side_type, const double* vib, const double* u_w, const double* bc,
+                     const double* ux, double* flux);
+/* Same with device pointers (bc stays a host array of five values). */
+int lsg_laplace_flux_device(lsg_ctx* ctx, const int* side_type, const double* vib, const double* u_w,
+                            const double* bc, const double* ux, double* flux);
+
 /* Staggered cell types (LSSTAGUniformMesh xMesh/yMesh/zMesh typeOfCell),
    needed by lsg_projection_correct.  Host pointers. */
 int lsg_set_staggered_types(lsg_ctx* ctx, const int* xtype, const int* ytype, const int* ztype);
@@ -178,6 +193,19 @@ int lsg_projection_rhs_device(lsg_ctx* ctx, const double* u, const double* v, co
    and may alias us/vs/ws. */
 int lsg_projection_correct(lsg_ctx* ctx, const double* phi, const double* us, const double* vs, const double* ws,
                            double* u, double* v, double* w, double* p, double coef, double vbase, int outflow);
+/* Adjoint of the projection step without the outflow clamps (the linear map
+   (u*, v*, w*, flux, p) -> (u, v, w, p) of lsg_projection_rhs, the pressure
+   solve and lsg_projection_correct with outflow = 0): given the cotangents of
+   the outputs, returns those of the inputs,
+     phi_bar = Gx^T S_x ubar_out + Gy^T S_y vbar_out + Gz^T S_z wbar_out + coef pbar_out,
+     A^T lambda = phi_bar (lsg_solve_adjoint's solver),  b_bar = lambda with the pins zeroed,
+     ubar = ubar_out + Dx^T b_bar (likewise v, w),  fluxbar = b_bar,
+   the pressure cotangent passing through unchanged.  No counterpart in the
+   reference (the north star's adjoint of the projection step).  Host
+   pointers; st receives the adjoint solve's statistics (may be NULL). */
+int lsg_projection_adjoint(lsg_ctx* ctx, const double* ubar_out, const double* vbar_out, const double* wbar_out,
+                           const double* pbar_out, double coef, double* ubar, double* vbar, double* wbar,
+                           double* fluxbar, lsg_stats* st);
 /* Same on device pointers. */
 int lsg_projection_correct_device(lsg_ctx* ctx, const double* phi, const double* us, const double* vs,
                                   const double* ws, double* u, double* v, double* w, double* p, double coef,

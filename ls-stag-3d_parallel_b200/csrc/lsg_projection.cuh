@@ -178,4 +178,195 @@ __global__ void k_pressure_update(long long n, double coef, const double* __rest
         p[i] = add(p[i], mul(phi[i], coef));
 }
 
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+// Source term of the pressure equation, LaplaceDiscreteOperator::flux after
+// initMeshParams + calcFlux for a flow task with fixed bodies
+// (DiscreteOperators/WithFlux/Sym/laplace_discrete_operator.h:47-83,
+// :687-808).  One thread per cell applies, in the reference's order:
+//   ibFlux (x in [1, N-2], y in [1, M-2]): 0 on fluid and solid cells; on cut
+//     cells -V_ib . (theta jump) dS over the cut faces (B/T border cells only
+//     when a face is cut, their z term left out; TW/TE/BW/BE edges untouched);
+//   initFlux: -U_W(y, z) dS at x = 0, U_E dS at x = N-1 (dS of the row's first
+//     cell);  addFluxNSp: -V_S dx dz at y = 0, +V_N dx dz at y = M-1 (dx of the
+//     y = 0 cell, dz of the layer's first cell);  addFluxTBp: -W_B theta_z dx dy
+//     at z = 0, +W_T theta_z dx dy at z = K-1 (dx of the z = 0 cell, dy of the
+//     row's first cell);
+//   setBaseFlux: x = N-1 overwritten by u(last x-face) dy dz (outflow).
+// (A cut-cell type on the bottom layer has no face below; its index is
+// clamped to the cell itself so that inconsistent input cannot read outside
+// the arrays.)
+__global__ void __launch_bounds__(256) k_laplace_flux(int N, int M, int K, const int* __restrict__ type,
+                                                      const int* __restrict__ side, const double* __restrict__ theta,
+                                                      const double* __restrict__ delta,
+                                                      const double* __restrict__ vib, const double* __restrict__ u_w,
+                                                      double U_E, double V_S, double V_N, double W_B, double W_T,
+                                                      const double* __restrict__ ux, double* __restrict__ flux)
+{
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= N || y >= M) return;
+    const long long NM = (long long)N * M;
+    const long long i = x + (long long)N * y + NM * z;
+    double f = 0.0;
+    if (y >= 1 && y <= M - 2 && x >= 1 && x <= N - 2) {
+        const int t = type[i];
+        const double dx = delta[3 * i], dy = delta[3 * i + 1], dz = delta[3 * i + 2];
+        const double vx = vib[3 * i], vy = vib[3 * i + 1], vz = vib[3 * i + 2];
+        if (t == 0 || t == 11111111) {
+            f = 0.0;
+        } else if (t == -3 || t == -2) {                       // B_Border, T_Border
+            bool cut = false;
+#pragma unroll
+            for (int c = 0; c < 3; c++) cut |= side[3 * i + c] > 0 && side[3 * i + c] < 1111;
+            f = cut ? mul(add(mul(mul(vx, sub(theta[3 * (i - 1)], theta[3 * i])), dy),
+                              mul(mul(vy, sub(theta[3 * (i - N) + 1], theta[3 * i + 1])), dx)),
+                          dz)
+                    : 0.0;
+        } else if (t == -11 || t == -10 || t == -15 || t == -14) {   // TW, TE, BW, BE edges: untouched
+        } else {
+            f = add(mul(add(mul(mul(vx, sub(theta[3 * (i - 1)], theta[3 * i])), dy),
+                            mul(mul(vy, sub(theta[3 * (i - N) + 1], theta[3 * i + 1])), dx)),
+                        dz),
+                    mul(mul(mul(vz, sub(theta[3 * (z > 0 ? i - NM : i) + 2], theta[3 * i + 2])), dx), dy));
+        }
+    }
+    const long long row0 = (long long)N * y + NM * z;          // first cell of the x-row
+    if (x == 0 || x == N - 1) {
+        const double dyz = mul(delta[3 * row0 + 1], delta[3 * row0 + 2]);
+        f = (x == 0) ? mul(-u_w[y + (long long)z * M], dyz) : mul(U_E, dyz);
+    }
+    if (y == 0 || y == M - 1) {
+        const double dz0 = delta[3 * (NM * z) + 2];
+        const double coef = mul(delta[3 * (x + NM * z)], dz0);
+        if (y == 0) f = sub(f, mul(coef, V_S));
+        if (y == M - 1) f = add(f, mul(coef, V_N));
+    }
+    if (z == 0 || z == K - 1) {
+        const long long b0 = (long long)N * y;                  // (x, y, 0) and its row start
+        const double coef = mul(delta[3 * b0 + 1], delta[3 * (b0 + x)]);
+        if (z == 0) f = sub(f, mul(mul(coef, theta[3 * i + 2]), W_B));
+        if (z == K - 1) f = add(f, mul(mul(coef, theta[3 * i + 2]), W_T));
+    }
+    if (x == N - 1) f = mul(mul(ux[i - 1 - y - (long long)z * M], delta[3 * i + 1]), delta[3 * i + 2]);
+    flux[i] = f;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint of the projection (outflow clamps off):
+//   b = Pi (Dx u + Dy v + Dz w + flux),  A phi = b,
+//   u' = u + S_x Gx phi (likewise v, w),  p' = p + coef phi,
+// Pi zeroing the pinned rows and S = diag(inv_vof).  Given the cotangents
+// (u'_bar, v'_bar, w'_bar, p'_bar):
+//   phi_bar = Gx^T S_x u'_bar + Gy^T S_y v'_bar + Gz^T S_z w'_bar + coef p'_bar,
+//   A^T lambda = phi_bar,  b_bar = Pi lambda,
+//   u_bar = u'_bar + Dx^T b_bar (likewise v, w),  flux_bar = b_bar,  p_bar = p'_bar.
+// The transposed operators are applied from the geometry like the forward ones.
+// ---------------------------------------------------------------------------
+
+// face coefficient of the gradient row of the staggered cell whose lower base
+// cell is P (GradientDiscreteOperator*::calc): c = (theta_P[dir] d1_P) d2_P
+__device__ __forceinline__ double grad_coef(int dir, const double* __restrict__ theta, const double* __restrict__ delta,
+                                            long long P)
+{
+    const double d1 = delta[3 * P + (dir == 0 ? 1 : 0)];
+    const double d2 = delta[3 * P + (dir == 2 ? 1 : 2)];
+    return theta[3 * P + dir] * d1 * d2;
+}
+
+// phi_bar at every base cell: sum over the cell's faces of +-c S u'_bar, plus coef p'_bar
+__global__ void __launch_bounds__(256) k_projection_adjoint_phi(int N, int M, int K, const int* __restrict__ xtype,
+                                                                const int* __restrict__ ytype,
+                                                                const int* __restrict__ ztype,
+                                                                const double* __restrict__ theta,
+                                                                const double* __restrict__ delta,
+                                                                const double* __restrict__ inv_x,
+                                                                const double* __restrict__ inv_y,
+                                                                const double* __restrict__ inv_z,
+                                                                const double* __restrict__ ub,
+                                                                const double* __restrict__ vb,
+                                                                const double* __restrict__ wb,
+                                                                const double* __restrict__ pb, double coef,
+                                                                double* __restrict__ phib)
+{
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= N || y >= M) return;
+    const long long NM = (long long)N * M;
+    const long long i = x + (long long)N * y + NM * z;
+    double acc = coef * pb[i];
+    // x-faces: east (P = i) and west (P = i - 1); x-grid index numX = i - y - z M
+    const long long fx = i - y - (long long)z * M;
+    if (x < N - 1 && xtype[fx] != 0) acc += grad_coef(0, theta, delta, i) * inv_x[fx] * ub[fx];
+    if (x > 0 && xtype[fx - 1] != 0) acc -= grad_coef(0, theta, delta, i - 1) * inv_x[fx - 1] * ub[fx - 1];
+    // y-faces: north (P = i) and south (P = i - N); y-grid index i - z N
+    const long long fy = i - (long long)z * N;
+    if (y < M - 1 && ytype[fy] != 0) acc += grad_coef(1, theta, delta, i) * inv_y[fy] * vb[fy];
+    if (y > 0 && ytype[fy - N] != 0) acc -= grad_coef(1, theta, delta, i - N) * inv_y[fy - N] * vb[fy - N];
+    // z-faces: top (P = i) and bottom (P = i - NM); z-grid index i
+    if (z < K - 1 && ztype[i] != 0) acc += grad_coef(2, theta, delta, i) * inv_z[i] * wb[i];
+    if (z > 0 && ztype[i - NM] != 0) acc -= grad_coef(2, theta, delta, i - NM) * inv_z[i - NM] * wb[i - NM];
+    phib[i] = acc;
+}
+
+// divergence entry of base cell P's row for its upper face (dir) and of cell
+// E's row for its lower face, as DivergenceDiscreteOperatorX/Y/Z::calcD* build
+// them (solid rows hold a zero; upper face: +theta_P dS on W/S/B-border rows
+// and interior rows; lower face: -theta_P dS on E/N/T-border and interior rows)
+__device__ __forceinline__ double div_upper(int dir, int t, const double* __restrict__ theta,
+                                            const double* __restrict__ delta, long long P)
+{
+    if (t == 0) return 0.0;
+    const double d0 = delta[3 * P], d1 = delta[3 * P + 1], d2 = delta[3 * P + 2];
+    const double th = theta[3 * P + dir];
+    if (dir == 0) return fam_w(t) ? th * d1 * d2 : th * (d1 * d2);
+    if (dir == 1) return fam_s(t) ? th * d0 * d2 : th * (d0 * d2);
+    return fam_b(t) ? th * d0 * d1 : th * (d0 * d1);
+}
+__device__ __forceinline__ double div_lower(int dir, int t, const double* __restrict__ theta,
+                                            const double* __restrict__ delta, long long E, long long P)
+{
+    if (t == 0) return 0.0;
+    const double d0 = delta[3 * E], d1 = delta[3 * E + 1], d2 = delta[3 * E + 2];
+    const double th = -theta[3 * P + dir];
+    if (dir == 0) return fam_e(t) ? th * d1 * d2 : th * (d1 * d2);
+    if (dir == 1) return fam_n(t) ? th * d0 * d2 : th * (d0 * d2);
+    return fam_t(t) ? th * d0 * d1 : th * (d0 * d1);
+}
+
+// u_bar = u'_bar + D^T b_bar on one staggered grid; b_bar is lambda with the
+// pinned rows zeroed
+__global__ void __launch_bounds__(256) k_projection_adjoint_vel(int dir, int N, int M, int K,
+                                                                const int* __restrict__ type,
+                                                                const double* __restrict__ theta,
+                                                                const double* __restrict__ delta,
+                                                                const double* __restrict__ lambda, long long pin0,
+                                                                long long pin1, const double* __restrict__ outbar,
+                                                                double* __restrict__ inbar)
+{
+    const int Ns = N - (dir == 0), Ms = M - (dir == 1);
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= Ns || y >= Ms) return;
+    const long long f = x + (long long)Ns * (y + (long long)Ms * z);
+    const long long P = x + (long long)N * (y + (long long)M * z);
+    const long long E = P + (dir == 0 ? 1 : (dir == 1 ? N : (long long)N * M));
+    const double bP = (P == pin0 || P == pin1) ? 0.0 : lambda[P];
+    const double bE = (E == pin0 || E == pin1) ? 0.0 : lambda[E];
+    inbar[f] = outbar[f] + div_upper(dir, type[P], theta, delta, P) * bP +
+               div_lower(dir, type[E], theta, delta, E, P) * bE;
+}
+
+// flux_bar = lambda with the pinned rows zeroed
+__global__ void k_pin_zero_copy(long long n, long long pin0, long long pin1, const double* __restrict__ lambda,
+                                double* __restrict__ out)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = (i == pin0 || i == pin1) ? 0.0 : lambda[i];
+}
+
 }  // namespace lsg

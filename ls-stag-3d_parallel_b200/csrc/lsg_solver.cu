@@ -1696,6 +1696,60 @@ int lsg_projection_rhs(lsg_ctx* h, const double* u, const double* v, const doubl
     LSG_API_END(h)
 }
 
+static void laplace_flux(Context& C, const int* side, const double* vib, const double* u_w, const double* bc,
+                         const double* ux, double* flux)
+{
+    const Dims& d = C.d;
+    const Context::Geometry& g = C.geo;
+    k_laplace_flux<<<dim3((d.N + 31) / 32, (d.M + 7) / 8, d.K), dim3(32, 8), 0, C.s>>>(
+        d.N, d.M, d.K, g.type.p, side, g.theta.p, g.delta.p, vib, u_w, bc[0], bc[1], bc[2], bc[3], bc[4], ux, flux);
+    LSG_CHECK_LAUNCH();
+}
+
+int lsg_laplace_flux_device(lsg_ctx* h, const int* side_type, const double* vib, const double* u_w, const double* bc,
+                            const double* ux, double* flux)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have, LSG_ERR_STATE, "no geometry set (lsg_set_matrix_geometry)");
+    LSG_REQUIRE(side_type && vib && u_w && bc && ux && flux, LSG_ERR_ARG, "null argument");
+    LSG_CUDA(cudaSetDevice(C.device));
+    laplace_flux(C, side_type, vib, u_w, bc, ux, flux);
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_laplace_flux(lsg_ctx* h, const int* side_type, const double* vib, const double* u_w, const double* bc,
+                     const double* ux, double* flux)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have, LSG_ERR_STATE, "no geometry set (lsg_set_matrix_geometry)");
+    LSG_REQUIRE(side_type && vib && u_w && bc && ux && flux, LSG_ERR_ARG, "null argument");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const long long n = C.n, nx = (long long)(d.N - 1) * d.M * d.K, nmk = (long long)d.M * d.K;
+    DevBuf<int> ds;
+    DevBuf<double> dv, dw, dux, df;
+    ds.alloc(3 * n);
+    dv.alloc(3 * n);
+    dw.alloc(nmk);
+    dux.alloc(nx);
+    df.alloc(n);
+    LSG_CUDA(cudaMemcpyAsync(ds.p, side_type, 3 * n * sizeof(int), cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dv.p, vib, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dw.p, u_w, nmk * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dux.p, ux, nx * 8, cudaMemcpyHostToDevice, C.s));
+    laplace_flux(C, ds.p, dv.p, dw.p, bc, dux.p, df.p);
+    LSG_CUDA(cudaMemcpyAsync(flux, df.p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
 int lsg_projection_correct_device(lsg_ctx* h, const double* phi, const double* us, const double* vs, const double* ws,
                                   double* u, double* v, double* w, double* p, double coef, double vbase, int outflow)
 {
@@ -1980,6 +2034,58 @@ int lsg_apply_transpose(lsg_ctx* h, const double* x, double* y)
     LSG_CUDA(cudaMemcpyAsync(y, dy.p, n * 8, cudaMemcpyDeviceToHost, C.s));
     LSG_CUDA(cudaStreamSynchronize(C.s));
     return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_projection_adjoint(lsg_ctx* h, const double* ubar_out, const double* vbar_out, const double* wbar_out,
+                           const double* pbar_out, double coef, double* ubar, double* vbar, double* wbar,
+                           double* fluxbar, lsg_stats* st)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(ubar_out && vbar_out && wbar_out && pbar_out && ubar && vbar && wbar && fluxbar, LSG_ERR_ARG,
+                "null field");
+    LSG_CUDA(cudaSetDevice(C.device));
+    Context& A = adjoint_context(C);
+    if (st) std::memset(st, 0, sizeof(*st));
+    const Dims& d = C.d;
+    const Context::Geometry& g = C.geo;
+    const long long n = C.n, cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
+                                       (long long)d.N * d.M * (d.K - 1)};
+    const double* hout[3] = {ubar_out, vbar_out, wbar_out};
+    double* hin[3] = {ubar, vbar, wbar};
+    DevBuf<double> dout[3], din[3], dp, df;
+    for (int k = 0; k < 3; k++) {
+        dout[k].alloc(cnt[k]);
+        din[k].alloc(cnt[k]);
+        LSG_CUDA(cudaMemcpyAsync(dout[k].p, hout[k], cnt[k] * 8, cudaMemcpyHostToDevice, C.s));
+    }
+    dp.alloc(n);
+    df.alloc(n);
+    LSG_CUDA(cudaMemcpyAsync(dp.p, pbar_out, n * 8, cudaMemcpyHostToDevice, C.s));
+    const dim3 blk(32, 8);
+    k_projection_adjoint_phi<<<dim3((d.N + 31) / 32, (d.M + 7) / 8, d.K), blk, 0, C.s>>>(
+        d.N, d.M, d.K, g.stype[0].p, g.stype[1].p, g.stype[2].p, g.theta.p, g.delta.p, g.inv[0].p, g.inv[1].p,
+        g.inv[2].p, dout[0].p, dout[1].p, dout[2].p, dp.p, coef, A.bd.p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaMemsetAsync(A.xd.p, 0, n * 8, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    const int rc = solve_device(A, A.bd.p, A.xd.p, st);
+    for (int dir = 0; dir < 3; dir++) {
+        const int Ns = d.N - (dir == 0), Ms = d.M - (dir == 1), Ks = d.K - (dir == 2);
+        k_projection_adjoint_vel<<<dim3((Ns + 31) / 32, (Ms + 7) / 8, Ks), blk, 0, C.s>>>(
+            dir, d.N, d.M, d.K, g.type.p, g.theta.p, g.delta.p, A.xd.p, g.pin0, g.pin1, dout[dir].p, din[dir].p);
+        LSG_CHECK_LAUNCH();
+        LSG_CUDA(cudaMemcpyAsync(hin[dir], din[dir].p, cnt[dir] * 8, cudaMemcpyDeviceToHost, C.s));
+    }
+    k_pin_zero_copy<<<grid_for(n, 256), 256, 0, C.s>>>(n, g.pin0, g.pin1, A.xd.p, df.p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaMemcpyAsync(fluxbar, df.p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return rc;
     LSG_API_END(h)
 }
 

@@ -107,6 +107,15 @@ class IterativeSolver:
         self._stypes = tuple(np.ascontiguousarray(t, dtype=np.int32) for t in (xtype, ytype, ztype))
         self.ctx.check(self.ctx.lib.lsg_set_staggered_types(self.ctx.h, *(L.iptr(t) for t in self._stypes)))
 
+    def laplace_flux(self, side_type, vib, u_w, bc, ux) -> np.ndarray:
+        """Pressure-equation source term (LaplaceDiscreteOperator flux);
+        bc = (U_E, V_S, V_N, W_B, W_T)."""
+        st = np.ascontiguousarray(side_type, dtype=np.int32)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (vib, u_w, bc, ux)]
+        f = np.empty(int(np.prod(self.dims)))
+        self.ctx.check(self.ctx.lib.lsg_laplace_flux(self.ctx.h, L.iptr(st), *(L.dptr(a) for a in arrs), L.dptr(f)))
+        return f
+
     def projection_rhs(self, u, v, w, flux) -> np.ndarray:
         """b = Dx u + Dy v + Dz w + flux, b[pins] = 0 (recalcRightMember)."""
         args = [np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, w, flux)]
@@ -124,6 +133,18 @@ class IterativeSolver:
                                                            *(L.dptr(a) for a in outs), L.dptr(p), float(coef),
                                                            float(vbase), int(bool(outflow))))
         return outs[0], outs[1], outs[2], p
+
+    def projection_adjoint(self, ubar_out, vbar_out, wbar_out, pbar_out, coef):
+        """Cotangents (ubar, vbar, wbar, fluxbar, pbar) of the inputs of the
+        projection step (outflow clamps off) from those of its outputs."""
+        ins = [np.ascontiguousarray(a, dtype=np.float64) for a in (ubar_out, vbar_out, wbar_out, pbar_out)]
+        outs = [np.empty_like(a) for a in ins[:3]]
+        fb = np.empty_like(ins[3])
+        self.adj_stats = L.Stats()
+        self.ctx.check(self.ctx.lib.lsg_projection_adjoint(self.ctx.h, *(L.dptr(a) for a in ins), float(coef),
+                                                           *(L.dptr(a) for a in outs), L.dptr(fb),
+                                                           L.C.byref(self.adj_stats)))
+        return outs[0], outs[1], outs[2], fb, ins[3].copy()
 
     def planes(self) -> np.ndarray:
         n = int(np.prod(self.dims))

@@ -354,6 +354,22 @@ int main(int argc, char** argv)
     SetSolutions* sol = new SetSolutions;
     sol->init(task, &it);
     task->initSol(&(sol->current), &(sol->prediction), &(sol->previous));
+    if ((int)cfg.get("flux_perturb", 0)) {
+        // nonzero boundary and immersed-boundary velocities, so that every term
+        // of the Laplace source (inflow profile, outflow, N/S and T/B walls,
+        // immersed boundary) contributes; all inputs are dumped below
+        LSSTAGUniformMesh* mm = task->m_mesh;
+        const long nb = (long)mm->baseMesh.N * mm->baseMesh.M * mm->baseMesh.K;
+        for (long j = 0; j < (long)mm->baseMesh.M * mm->baseMesh.K; j++) task->pU_W[j] = 1.0 + 0.1 * sin(0.37 * j);
+        task->U_E = 0.9;
+        task->V_S = 0.05;
+        task->V_N = -0.07;
+        task->W_B = 0.03;
+        task->W_T = -0.02;
+        for (long i = 0; i < nb; i++)
+            mm->v_ib[i].set(0.1 * sin(0.11 * i), 0.1 * cos(0.13 * i), 0.05 * sin(0.17 * i));
+        for (long i = 0; i < (long)mm->xMesh.NMK; i++) mm->m_Ux[i] = 1.0 + 0.2 * sin(0.29 * i);
+    }
     if ((int)cfg.get("operator_only", 0)) {
         // the Laplace operator alone (LaplaceDiscreteOperator::init + build), without
         // the pressure equation's solver set-up, whose multigrid hierarchy does not
@@ -391,6 +407,15 @@ int main(int argc, char** argv)
         out.d("inv_my", m->yMesh.inv_VOF, (long)m->yMesh.NMK);
         out.d("inv_mz", m->zMesh.inv_VOF, (long)m->zMesh.NMK);
         out.d("flux", pEq->A.flux, n);
+        // inputs of the Laplace source term (LaplaceDiscreteOperator::initFlux,
+        // ibFlux, setBaseFlux): face types, immersed-boundary velocity,
+        // boundary velocities and the x-velocity used for the outflow
+        out.i("side_type", (const int*)m->baseSideTypes, 3 * n);
+        out.d("vib", (const double*)m->v_ib, 3 * n);
+        out.d("u_w", task->pU_W, (long)M * K);
+        double bc[5] = {task->U_E, task->V_S, task->V_N, task->W_B, task->W_T};
+        out.d("bc_ue_vs_vn_wb_wt", bc, 5);
+        out.d("ux0", m->m_Ux, (long)m->xMesh.NMK);
     }
     // projection operators: divergence rows on the base grid
     // (poisson_discrete_equation.h Dx/Dy/Dz), gradient rows on the staggered

@@ -13,7 +13,8 @@ operators (divergence Dx/Dy/Dz, gradient Gx/Gy/Gz, staggered cell types) and
 one pressure projection of the time step (right-hand side, MG-FGMRES pressure
 correction, corrected u, v, w, p) on seeded predicted fields; the momentum
 operators (Helmholtz Kx/Ky/Kz, convective Cx/Cy/Cz) and one ILU-FGMRES solve
-of each Helmholtz system.
+of each Helmholtz system; the pressure-equation source term (flux) with
+nonzero boundary and immersed-boundary velocities.
 """
 from __future__ import annotations
 
@@ -102,6 +103,12 @@ def main():
             for k in ("mom_x_", "mom_it_", "mom_eps_"):
                 keep[k + d] = mr[k + d]
         keep["mom_restart"] = mr["mom_restart"]
+        # the pressure-equation source term with every contribution nonzero
+        # (harness flux_perturb: inflow profile, wall and immersed-boundary
+        # velocities, outflow u)
+        gf = rr.run(case, threads=1, flux_perturb=1)
+        for k in ("side_type", "vib", "u_w", "bc_ue_vs_vn_wb_wt", "ux0", "flux"):
+            keep["fluxp_" + k] = gf[k]
         for l in range(int(r["mg_nlev"][0])):
             for m in ("P", "R", "AH"):
                 for part in ("rowptr", "col", "val", "dims"):

@@ -80,3 +80,15 @@ def test_geometry_rejects_inconsistent_types():
     with pytest.raises(L.LsgError):
         s.set_geometry(geom, dims, g["pins"], setup=False)
     s.close()
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_laplace_flux_bitwise(name):
+    """GPU pressure-equation source term against the reference's flux, bit for
+    bit, with every contribution nonzero."""
+    g = load_golden(name)
+    s = _solver(g)
+    f = s.laplace_flux(g["fluxp_side_type"], g["fluxp_vib"], g["fluxp_u_w"], g["fluxp_bc_ue_vs_vn_wb_wt"],
+                       g["fluxp_ux0"])
+    assert np.array_equal(_bits(f), _bits(g["fluxp_flux"]))
+    s.close()
