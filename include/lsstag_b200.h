@@ -166,6 +166,21 @@ int lsg_laplace_flux(lsg_ctx* ctx, const int* side_type, const double* vib, cons
 int lsg_laplace_flux_device(lsg_ctx* ctx, const int* side_type, const double* vib, const double* u_w,
                             const double* bc, const double* ux, double* flux);
 
+/* Right-hand side of one momentum equation (dir 0: u on the x-grid, 1: v,
+   2: w) for a fixed-body flow, HelmholtzDiscreteEquation::recalcRightMember
+   (DiscreteEquations/helmholtz_discrete_equation.h:91-95, :213-254):
+     aux   = flux2 + C u   (C the convective operator of this step in the
+                            reference's CSR form, flux2 its source term),
+     right = ((-2 u + 0.5 u_prev) VOF) coef2 - ((G p + flux) + prev_aux) + 2 aux,
+   with G the pressure gradient applied from the geometry, flux the Helmholtz
+   operator's source term, coef2 = 1/dt; aux is returned as the next step's
+   prev_aux.  Bit-identical to the reference.  Host pointers (staggered-grid
+   vectors, p on the base grid). */
+int lsg_momentum_rhs(lsg_ctx* ctx, int dir, const int* rowptr, const int* col, const double* val,
+                     const double* flux2, const double* u, const double* uprev, const double* vof,
+                     const double* hflux, const double* p, const double* prev_aux, double coef2, double* right,
+                     double* aux);
+
 /* Staggered cell types (LSSTAGUniformMesh xMesh/yMesh/zMesh typeOfCell),
    needed by lsg_projection_correct.  Host pointers. */
 int lsg_set_staggered_types(lsg_ctx* ctx, const int* xtype, const int* ytype, const int* ztype);

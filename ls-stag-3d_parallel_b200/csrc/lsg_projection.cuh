@@ -23,6 +23,7 @@ __device__ __forceinline__ bool fam_b(int t) { return t == -3 || t == -12 || t =
 
 __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
 
 // b = Dx u + flux + Dy v + Dz w (PoissonDiscreteEquation::recalcRightMember,
 // DiscreteEquations/poisson_discrete_equation.h:145-159):
@@ -178,8 +179,6 @@ __global__ void k_pressure_update(long long n, double coef, const double* __rest
         p[i] = add(p[i], mul(phi[i], coef));
 }
 
-__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
-
 // Source term of the pressure equation, LaplaceDiscreteOperator::flux after
 // initMeshParams + calcFlux for a flow task with fixed bodies
 // (DiscreteOperators/WithFlux/Sym/laplace_discrete_operator.h:47-83,
@@ -251,6 +250,61 @@ __global__ void __launch_bounds__(256) k_laplace_flux(int N, int M, int K, const
     }
     if (x == N - 1) f = mul(mul(ux[i - 1 - y - (long long)z * M], delta[3 * i + 1]), delta[3 * i + 2]);
     flux[i] = f;
+}
+
+// Pressure gradient on one staggered grid, out = G p (the rows of
+// k_projection_velocity without the update): GradientDiscreteOperatorX/Y/Z
+// applied by RealValuedMeshFunction::mvProd.
+__global__ void __launch_bounds__(256) k_gradient_apply(int dir, int N, int M, int K, const int* __restrict__ stype,
+                                                        const double* __restrict__ theta,
+                                                        const double* __restrict__ delta,
+                                                        const double* __restrict__ p, double* __restrict__ out)
+{
+    const int Ns = N - (dir == 0), Ms = M - (dir == 1);     // blockIdx.z runs over the K - (dir == 2) layers
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= Ns || y >= Ms) return;
+    const long long f = x + (long long)Ns * (y + (long long)Ms * z);
+    const long long P = x + (long long)N * (y + (long long)M * z);
+    const long long step = dir == 0 ? 1 : (dir == 1 ? N : (long long)N * M);
+    if (stype[f] == 0) {
+        out[f] = add(0.0, mul(0.0, p[P]));
+    } else {
+        const double d1 = delta[3 * P + (dir == 0 ? 1 : 0)];
+        const double d2 = delta[3 * P + (dir == 2 ? 1 : 2)];
+        const double c = mul(mul(theta[3 * P + dir], d1), d2);
+        out[f] = add(add(0.0, mul(c, p[P])), mul(-c, p[P + step]));
+    }
+}
+
+// Right-hand side of one momentum equation for a fixed-body flow,
+// HelmholtzDiscreteEquation::recalcRightMember (DiscreteEquations/
+// helmholtz_discrete_equation.h:91-95, :213-254), one thread per staggered
+// cell: aux = flux2 + C u summed in the CSR row order of the convective
+// operator (ConvectiveDiscreteOperator*, rebuilt by the caller each step),
+// right = ((-2 u + 0.5 u_prev) VOF) coef2 - ((G p + flux) + prev_aux) + 2 aux;
+// aux is returned as the next step's prev_aux (Adams-Bashforth history).
+__global__ void __launch_bounds__(256) k_momentum_rhs(long long n, const int* __restrict__ rowptr,
+                                                      const int* __restrict__ col, const double* __restrict__ val,
+                                                      const double* __restrict__ flux2, const double* __restrict__ u,
+                                                      const double* __restrict__ uprev,
+                                                      const double* __restrict__ vof,
+                                                      const double* __restrict__ hflux,
+                                                      const double* __restrict__ prev_aux,
+                                                      const double* __restrict__ gp, double coef2,
+                                                      double* __restrict__ right, double* __restrict__ aux_out)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        double aux = flux2[i];
+        for (int e = rowptr[i]; e < rowptr[i + 1]; e++) aux = add(aux, mul(val[e], u[col[e]]));
+        double r = mul(mul(add(mul(-2.0, u[i]), mul(0.5, uprev[i])), vof[i]), coef2);
+        r = sub(r, add(add(gp[i], hflux[i]), prev_aux[i]));
+        r = add(r, mul(aux, 2.0));
+        right[i] = r;
+        aux_out[i] = aux;
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -1750,6 +1750,58 @@ int lsg_laplace_flux(lsg_ctx* h, const int* side_type, const double* vib, const 
     LSG_API_END(h)
 }
 
+int lsg_momentum_rhs(lsg_ctx* h, int dir, const int* rowptr, const int* col, const double* val, const double* flux2,
+                     const double* u, const double* uprev, const double* vof, const double* hflux, const double* p,
+                     const double* prev_aux, double coef2, double* right, double* aux)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z)");
+    LSG_REQUIRE(rowptr && col && val && flux2 && u && uprev && vof && hflux && p && prev_aux && right && aux,
+                LSG_ERR_ARG, "null argument");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const int Ns = d.N - (dir == 0), Ms = d.M - (dir == 1), Ks = d.K - (dir == 2);
+    const long long ns = (long long)Ns * Ms * Ks, n = C.n;
+    const long long nnz = rowptr[ns];
+    LSG_REQUIRE(rowptr[0] == 0 && nnz >= 0, LSG_ERR_ARG, "bad CSR row pointer");
+    for (long long i = 0; i < ns; i++)
+        LSG_REQUIRE(rowptr[i] <= rowptr[i + 1], LSG_ERR_ARG, "CSR row pointer not monotone");
+    for (long long e = 0; e < nnz; e++)
+        LSG_REQUIRE(col[e] >= 0 && col[e] < ns, LSG_ERR_ARG, "CSR column outside the staggered grid");
+    DevBuf<int> drp, dcol;
+    DevBuf<double> dval, dflux2, du, dup, dvof, dhf, dp, dprev, dgp, dr, da;
+    drp.alloc(ns + 1);
+    dcol.alloc(std::max<long long>(nnz, 1));
+    dval.alloc(std::max<long long>(nnz, 1));
+    for (DevBuf<double>* b : {&dflux2, &du, &dup, &dvof, &dhf, &dprev, &dgp, &dr, &da}) b->alloc(ns);
+    dp.alloc(n);
+    LSG_CUDA(cudaMemcpyAsync(drp.p, rowptr, (ns + 1) * sizeof(int), cudaMemcpyHostToDevice, C.s));
+    if (nnz) {
+        LSG_CUDA(cudaMemcpyAsync(dcol.p, col, nnz * sizeof(int), cudaMemcpyHostToDevice, C.s));
+        LSG_CUDA(cudaMemcpyAsync(dval.p, val, nnz * 8, cudaMemcpyHostToDevice, C.s));
+    }
+    const double* hsrc[6] = {flux2, u, uprev, vof, hflux, prev_aux};
+    DevBuf<double>* dst[6] = {&dflux2, &du, &dup, &dvof, &dhf, &dprev};
+    for (int k = 0; k < 6; k++) LSG_CUDA(cudaMemcpyAsync(dst[k]->p, hsrc[k], ns * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dp.p, p, n * 8, cudaMemcpyHostToDevice, C.s));
+    const Context::Geometry& g = C.geo;
+    k_gradient_apply<<<dim3((Ns + 31) / 32, (Ms + 7) / 8, Ks), dim3(32, 8), 0, C.s>>>(
+        dir, d.N, d.M, d.K, g.stype[dir].p, g.theta.p, g.delta.p, dp.p, dgp.p);
+    LSG_CHECK_LAUNCH();
+    k_momentum_rhs<<<grid_for(ns, 256), 256, 0, C.s>>>(ns, drp.p, dcol.p, dval.p, dflux2.p, du.p, dup.p, dvof.p, dhf.p,
+                                                       dprev.p, dgp.p, coef2, dr.p, da.p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaMemcpyAsync(right, dr.p, ns * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaMemcpyAsync(aux, da.p, ns * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
 int lsg_projection_correct_device(lsg_ctx* h, const double* phi, const double* us, const double* vs, const double* ws,
                                   double* u, double* v, double* w, double* p, double coef, double vbase, int outflow)
 {

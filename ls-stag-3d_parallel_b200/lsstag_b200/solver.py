@@ -116,6 +116,21 @@ class IterativeSolver:
         self.ctx.check(self.ctx.lib.lsg_laplace_flux(self.ctx.h, L.iptr(st), *(L.dptr(a) for a in arrs), L.dptr(f)))
         return f
 
+    def momentum_rhs(self, direction: int, Cconv, flux2, u, uprev, vof, hflux, p, prev_aux, coef2):
+        """(right, aux) of one momentum equation (HelmholtzDiscreteEquation::
+        recalcRightMember); Cconv = (rowptr, col, val) of the convective
+        operator; aux is the next step's prev_aux."""
+        rp = np.ascontiguousarray(Cconv[0], dtype=np.int32)
+        col = np.ascontiguousarray(Cconv[1], dtype=np.int32)
+        val = np.ascontiguousarray(Cconv[2], dtype=np.float64)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (flux2, u, uprev, vof, hflux, p, prev_aux)]
+        right = np.empty_like(arrs[1])
+        aux = np.empty_like(arrs[1])
+        self.ctx.check(self.ctx.lib.lsg_momentum_rhs(self.ctx.h, int(direction), L.iptr(rp), L.iptr(col), L.dptr(val),
+                                                     *(L.dptr(a) for a in arrs), float(coef2), L.dptr(right),
+                                                     L.dptr(aux)))
+        return right, aux
+
     def projection_rhs(self, u, v, w, flux) -> np.ndarray:
         """b = Dx u + Dy v + Dz w + flux, b[pins] = 0 (recalcRightMember)."""
         args = [np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, w, flux)]

@@ -510,6 +510,55 @@ int main(int argc, char** argv)
         int rs = task->FGMRES_RESTART_NUM, mi = task->MAX_ITER;
         out.i("mom_restart", &rs, 1);
         out.i("mom_max_it", &mi, 1);
+        if ((int)cfg.get("mom_step", 0)) {
+            // one momentum step of each equation (HelmholtzDiscreteEquation::
+            // solve: recalcRightMember + ILUFGMRES) on perturbed current and
+            // previous velocities and pressure.  The state left by set() (the
+            // convective product C(u0) u0 + flux2 as the previous term) is
+            // dumped first, then the inputs, the right-hand side and solution.
+            LSSTAGUniformMesh* mm = task->m_mesh;
+            double* cur[3] = {mm->m_Ux, mm->m_Uy, mm->m_Uz};
+            double* prv[3] = {mm->m_prevUx, mm->m_prevUy, mm->m_prevUz};
+            const double* vofs[3] = {mm->xMesh.VOF, mm->yMesh.VOF, mm->zMesh.VOF};
+            for (int d = 0; d < 3; d++) {
+                HelmholtzDiscreteEquation* e = eq[d];
+                const long ne = e->m_A->NMK;
+                out.csr(std::string("C0") + nm[d], (SparseMatrix*)e->m_conv);
+                out.d(std::string("flux2_0") + nm[d], e->m_conv->flux, ne);
+                out.d(std::string("u0") + nm[d], cur[d], ne);
+            }
+            const CellTypes* stype[3] = {mm->xMesh.typeOfCell, mm->yMesh.typeOfCell, mm->zMesh.typeOfCell};
+            for (int d = 0; d < 3; d++) {
+                const long ne = eq[d]->m_A->NMK;
+                for (long i = 0; i < ne; i++) {
+                    if (stype[d][i] == SolidCell) continue;     // velocities stay zero inside the bodies
+                    cur[d][i] += 0.05 * sin(0.07 * i + d);
+                    prv[d][i] = cur[d][i] - 0.01 * cos(0.05 * i + 2 * d);
+                }
+            }
+            for (long i = 0; i < n; i++) mm->m_P[i] = 0.3 * sin(0.013 * i);
+            out.d("mstep_p", mm->m_P, n);
+            for (int d = 0; d < 3; d++) {
+                HelmholtzDiscreteEquation* e = eq[d];
+                const long ne = e->m_A->NMK;
+                out.d(std::string("mstep_u_") + nm[d], cur[d], ne);
+                out.d(std::string("mstep_uprev_") + nm[d], prv[d], ne);
+                out.d(std::string("mstep_vof_") + nm[d], vofs[d], ne);
+                std::fill(e->m_sol, e->m_sol + ne, 0.0);
+                e->solver.eps = 1e-10;
+                e->solve();
+                out.csr(std::string("C1") + nm[d], (SparseMatrix*)e->m_conv);
+                out.d(std::string("flux2_1") + nm[d], e->m_conv->flux, ne);
+                out.d(std::string("mstep_hflux_") + nm[d], e->m_A->flux, ne);
+                out.d(std::string("mstep_rhs_") + nm[d], e->m_right, ne);
+                out.d(std::string("mstep_sol_") + nm[d], e->m_sol, ne);
+                int it = e->solver.it;
+                out.i(std::string("mstep_it_") + nm[d], &it, 1);
+                out.csr(std::string("K1") + nm[d], (SparseMatrix*)e->m_A);
+            }
+            double c2 = 1.0 / task->t;
+            out.scalar("mstep_coef2", c2);
+        }
         return 0;
     }
     if ((int)cfg.get("projection", 0)) {

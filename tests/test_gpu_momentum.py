@@ -55,3 +55,43 @@ def test_momentum_solve_matches_reference(name):
         ref = g[f"mom_x_{d}"]
         assert np.linalg.norm(x - ref) <= 1e-10 * np.linalg.norm(ref), d
         s.close()
+
+
+@pytest.mark.parametrize("name", ["sphere16", "sphere20x12x10"])
+def test_momentum_step_matches_reference(name):
+    """One momentum step on the GPU: the right-hand side (lsg_momentum_rhs,
+    gradient from the geometry, convective product in CSR order) equals the
+    reference's bit for bit; ILU-FGMRES(13) on it gives the reference's
+    iteration count (+-1) and solution (relative L2 <= 1e-10)."""
+    from lsstag_b200 import solver as S
+    g = load_golden(name)
+    dims = tuple(int(v) for v in g["dims"])
+    geo = S.MGFGMRES()
+    geom = {k: g[k] for k in ("celltype", "theta", "delta", "inv_mx", "inv_my", "inv_mz")}
+    geo.set_geometry(geom, dims, g["pins"], setup=False)
+    geo.set_staggered_types(g["xtype"], g["ytype"], g["ztype"])
+    for k, d in enumerate("xyz"):
+        # the history term left by set(): C(u0) u0 + flux2 in the reference's
+        # summation order (the aux output of the same kernel on the first state)
+        C0 = (g[f"C{d}_rowptr"], g[f"C{d}_col"], g[f"C{d}_val"])
+        _, prev = geo.momentum_rhs(k, C0, g["flux2_0" + d], g["u0" + d], g["u0" + d], g["mstep_vof_" + d],
+                                   g["mstep_hflux_" + d], g["mstep_p"], np.zeros_like(g["u0" + d]),
+                                   float(g["mstep_coef2"][0]))
+        n0 = C0[0].size - 1
+        ref_prev = sp.csr_matrix((C0[2], C0[1], C0[0]), shape=(n0, n0)) @ g["u0" + d] + g["flux2_0" + d]
+        assert np.linalg.norm(prev - ref_prev) <= 1e-13 * np.linalg.norm(ref_prev)
+        right, aux = geo.momentum_rhs(k, (g[f"C1{d}_rowptr"], g[f"C1{d}_col"], g[f"C1{d}_val"]),
+                                      g["flux2_1" + d], g["mstep_u_" + d], g["mstep_uprev_" + d],
+                                      g["mstep_vof_" + d], g["mstep_hflux_" + d], g["mstep_p"], prev,
+                                      float(g["mstep_coef2"][0]))
+        assert np.array_equal(right.view(np.int64), g["mstep_rhs_" + d].view(np.int64)), d
+        rp, col, val, sdims = _csr(g, "K" + d)
+        s = S.ILUFGMRES()
+        s.set((rp, col, val, sdims), task=S.Task(eps=1e-10, MAX_ITER=200, FGMRES_RESTART_NUM=int(g["mom_restart"][0])))
+        x = np.zeros(rp.size - 1)
+        it = s.solve(right, x)
+        assert abs(it - int(g["mstep_it_" + d][0])) <= 1, d
+        ref = g["mstep_sol_" + d]
+        assert np.linalg.norm(x - ref) <= 1e-10 * np.linalg.norm(ref), d
+        s.close()
+    geo.close()

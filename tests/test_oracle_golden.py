@@ -149,3 +149,29 @@ def test_oracle_laplace_flux_matches_reference(name):
     f = lo.laplace_flux(N, M, K, g["celltype"], g["fluxp_side_type"], g["theta"], g["delta"], g["fluxp_vib"],
                         g["fluxp_u_w"], *bc, g["fluxp_ux0"])
     assert np.array_equal(f.view(np.int64), g["fluxp_flux"].view(np.int64))
+
+
+@pytest.mark.parametrize("name", ["sphere16", "sphere20x12x10"])
+def test_oracle_momentum_step(name):
+    """One momentum step of each equation: the right-hand side restated from
+    its inputs equals the reference's bit for bit, and ILU-FGMRES(13) on it
+    gives the reference's iteration count and solution."""
+    g = load_golden(name)
+    for d, gname in zip("xyz", ("Gx", "Gy", "Gz")):
+        C0 = (g[f"C{d}_rowptr"], g[f"C{d}_col"], g[f"C{d}_val"])
+        C1 = (g[f"C1{d}_rowptr"], g[f"C1{d}_col"], g[f"C1{d}_val"])
+        G = (g[gname + "_rowptr"], g[gname + "_col"], g[gname + "_val"])
+        prev = lo._mv(C0, g["u0" + d], init=g["flux2_0" + d])
+        right, _ = lo.momentum_rhs(C1, g["flux2_1" + d], g["mstep_u_" + d], g["mstep_uprev_" + d],
+                                   g["mstep_vof_" + d], g["mstep_hflux_" + d], prev, G, g["mstep_p"],
+                                   float(g["mstep_coef2"][0]))
+        assert np.array_equal(right.view(np.int64), g["mstep_rhs_" + d].view(np.int64)), d
+        rp, col, val = g[f"K{d}_rowptr"], g[f"K{d}_col"], g[f"K{d}_val"]
+        n = rp.size - 1
+        A = sp.csr_matrix((val, col, rp), shape=(n, n))
+        LU = lo.ilu0(A)
+        x, it, _ = lo.fgmres(A, right, np.zeros(n), lambda v: lo.ilu_solve(LU, v), 1e-10,
+                             int(g["mom_restart"][0]), 200)
+        assert it == int(g["mstep_it_" + d][0]), d
+        ref = g["mstep_sol_" + d]
+        assert np.linalg.norm(x - ref) <= 1e-12 * np.linalg.norm(ref), d
