@@ -181,8 +181,24 @@ int lsg_momentum_rhs(lsg_ctx* ctx, int dir, const int* rowptr, const int* col, c
                      const double* hflux, const double* p, const double* prev_aux, double coef2, double* right,
                      double* aux);
 
+/* Convective operator of momentum component dir (0 x, 1 y, 2 z) applied
+   from the geometry: out = init + C(u) v on the dir-grid, C the operator
+   ConvectiveDiscreteOperatorX/Y/Z::calcConv* builds from the velocity
+   (ux, uy, uz) (DiscreteOperators/WithFlux/SkewSym/convective_discrete_operator_x.h:49-366,
+   _y.h, _z.h); init may be NULL (zero).  zconv_reference = 1 reproduces the
+   reference's x-velocity indexing in the z operator (M + 1 cells per row,
+   calcConvZ launched with M3 at convective_discrete_operator_z.h:772-773);
+   0 uses the grid's own row length.  Bit-identical to init + (the
+   reference's CSR) v.  Host pointers. */
+int lsg_convective_apply(lsg_ctx* ctx, int dir, const double* ux, const double* uy, const double* uz,
+                         const double* v, const double* init, double* out, int zconv_reference);
+/* Same on device pointers. */
+int lsg_convective_apply_device(lsg_ctx* ctx, int dir, const double* ux, const double* uy, const double* uz,
+                                const double* v, const double* init, double* out, int zconv_reference);
+
 /* Staggered cell types (LSSTAGUniformMesh xMesh/yMesh/zMesh typeOfCell),
-   needed by lsg_projection_correct.  Host pointers. */
+   needed by the staggered-grid entry points below.  Checked on the host like
+   the base types (a kept face must lie inside the grid).  Host pointers. */
 int lsg_set_staggered_types(lsg_ctx* ctx, const int* xtype, const int* ytype, const int* ztype);
 
 /* b = Dx u + Dy v + Dz w + flux with b[pin0] = b[pin1] = 0: the right-hand

@@ -307,6 +307,87 @@ __global__ void __launch_bounds__(256) k_momentum_rhs(long long n, const int* __
     }
 }
 
+// Convective operator of momentum component d applied from the geometry,
+// out = init + C(U) v on the d-grid (ConvectiveDiscreteOperatorX/Y/Z::calcConv*,
+// DiscreteOperators/WithFlux/SkewSym/convective_discrete_operator_x.h:49-366,
+// _y.h, _z.h, in the form of their generic cut-cell rows).  For the staggered
+// cell f between base cells P and Q = P + step_d, faces B, S, W, E, N, T:
+//   along d:  -/+ 0.25 A (theta_d(P) U_d[f] + theta_d(P - step_d | Q) U_d[f -/+ stride_d]),
+//             A = the product of P's two cell sizes across d;
+//   across d (direction e):  -/+ 0.25 h (delta_d(P) theta_e(.) U_e[face of P] + delta_d(Q) theta_e(.) U_e[face of Q]),
+//             h = P's cell size in the third direction, the faces below (theta of
+//             the cells below) or above P and Q;
+// faces absent for the staggered cell's type are left out, solid cells give
+// init.  With zquirk the z operator reads the x-velocity with M + 1 cells per
+// row, as the reference does (calcConvZ launched with M3,
+// convective_discrete_operator_z.h:772-773): its x-face indices are shifted
+// back by P's layer index.  Products and sums in the reference's order without
+// fused multiply-adds, so out is bit-identical to init + (its CSR) v.
+__device__ __forceinline__ long long face_index(int e, int N, int M, int x, int y, int z)
+{
+    const int Ne = N - (e == 0), Me = M - (e == 1);
+    return x + (long long)Ne * (y + (long long)Me * z);
+}
+
+__global__ void __launch_bounds__(256) k_convective_apply(int d, int N, int M, int K, const int* __restrict__ stype,
+                                                          const double* __restrict__ theta,
+                                                          const double* __restrict__ delta,
+                                                          const double* __restrict__ Ux, const double* __restrict__ Uy,
+                                                          const double* __restrict__ Uz, const double* __restrict__ v,
+                                                          const double* __restrict__ init, bool zquirk,
+                                                          double* __restrict__ out)
+{
+    const int Nd = N - (d == 0), Md = M - (d == 1);
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= Nd || y >= Md) return;
+    const long long f = x + (long long)Nd * (y + (long long)Md * z);
+    double acc = init ? init[f] : 0.0;
+    const int t = stype[f];
+    if (t != 0) {
+        const long long NM = (long long)N * M;
+        const long long step[3] = {1, N, NM};
+        const long long P = x + (long long)N * (y + (long long)M * z), Q = P + step[d];
+        const int qx = x + (d == 0), qy = y + (d == 1), qz = z + (d == 2);
+        const double* U[3] = {Ux, Uy, Uz};
+        const long long dstride = d == 0 ? 1 : (d == 1 ? Nd : (long long)Nd * Md);
+        const long long cols[6] = {-(long long)Nd * Md, -Nd, -1, 1, Nd, (long long)Nd * Md};
+        const int fdir[6] = {2, 1, 0, 0, 1, 2};
+        const int miss = absent_faces(t);
+        const double tx = mul(theta[3 * P + d], U[d][f]);
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            if (miss & (1 << k)) continue;
+            const bool upper = k >= 3;
+            const int e = fdir[k];
+            double coef;
+            if (e == d) {
+                const int o0 = d == 0 ? 1 : 0, o1 = d == 2 ? 1 : 2;
+                const double area = mul(delta[3 * P + o0], delta[3 * P + o1]);
+                const double th2 = upper ? theta[3 * Q + d] : theta[3 * (P - step[d]) + d];
+                const double u2 = upper ? U[d][f + dstride] : U[d][f - dstride];
+                coef = mul(mul(upper ? 0.25 : -0.25, area), add(tx, mul(th2, u2)));
+            } else {
+                const int third = 3 - d - e;
+                const double h = delta[3 * P + third];
+                const long long pc = upper ? P : P - step[e], qc = upper ? Q : Q - step[e];
+                // coordinates of the two cells whose e-faces are used
+                const int px = x - (!upper && e == 0), py = y - (!upper && e == 1), pz = z - (!upper && e == 2);
+                const int cx = qx - (!upper && e == 0), cy = qy - (!upper && e == 1), cz = qz - (!upper && e == 2);
+                const long long shift = (zquirk && d == 2 && e == 0) ? z : 0;
+                const long long fp = face_index(e, N, M, px, py, pz) - shift;
+                const long long fq = face_index(e, N, M, cx, cy, cz) - shift;
+                const double a = mul(mul(delta[3 * P + d], theta[3 * pc + e]), U[e][fp]);
+                const double b = mul(mul(delta[3 * Q + d], theta[3 * qc + e]), U[e][fq]);
+                coef = mul(mul(upper ? 0.25 : -0.25, h), add(a, b));
+            }
+            acc = add(acc, mul(coef, v[f + cols[k]]));
+        }
+    }
+    out[f] = acc;
+}
+
 // ---------------------------------------------------------------------------
 // Adjoint of the projection (outflow clamps off):
 //   b = Pi (Dx u + Dy v + Dz w + flux),  A phi = b,

@@ -1610,6 +1610,11 @@ int lsg_set_staggered_types(lsg_ctx* h, const int* xtype, const int* ytype, cons
     const long long cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
                               (long long)d.N * d.M * (d.K - 1)};
     const int* src[3] = {xtype, ytype, ztype};
+    // as for the base grid: a face kept by a staggered cell's type must lie inside its grid
+    for (int k = 0; k < 3; k++) {
+        const int Nd = d.N - (k == 0), Md = d.M - (k == 1), Kd = d.K - (k == 2);
+        check_cell_types(Nd, Md, Kd, src[k]);
+    }
     for (int k = 0; k < 3; k++) {
         C.geo.stype[k].alloc(cnt[k]);
         LSG_CUDA(cudaMemcpyAsync(C.geo.stype[k].p, src[k], cnt[k] * sizeof(int), cudaMemcpyHostToDevice, C.s));
@@ -1797,6 +1802,68 @@ int lsg_momentum_rhs(lsg_ctx* h, int dir, const int* rowptr, const int* col, con
     LSG_CHECK_LAUNCH();
     LSG_CUDA(cudaMemcpyAsync(right, dr.p, ns * 8, cudaMemcpyDeviceToHost, C.s));
     LSG_CUDA(cudaMemcpyAsync(aux, da.p, ns * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+static void convective_apply(Context& C, int dir, const double* ux, const double* uy, const double* uz, const double* v,
+                             const double* init, double* out, bool zquirk)
+{
+    const Dims& d = C.d;
+    const Context::Geometry& g = C.geo;
+    const int Ns = d.N - (dir == 0), Ms = d.M - (dir == 1), Ks = d.K - (dir == 2);
+    k_convective_apply<<<dim3((Ns + 31) / 32, (Ms + 7) / 8, Ks), dim3(32, 8), 0, C.s>>>(
+        dir, d.N, d.M, d.K, g.stype[dir].p, g.theta.p, g.delta.p, ux, uy, uz, v, init, zquirk, out);
+    LSG_CHECK_LAUNCH();
+}
+
+int lsg_convective_apply_device(lsg_ctx* h, int dir, const double* ux, const double* uy, const double* uz,
+                                const double* v, const double* init, double* out, int zconv_reference)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z)");
+    LSG_REQUIRE(ux && uy && uz && v && out, LSG_ERR_ARG, "null argument");
+    LSG_CUDA(cudaSetDevice(C.device));
+    convective_apply(C, dir, ux, uy, uz, v, init, out, zconv_reference != 0);
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_convective_apply(lsg_ctx* h, int dir, const double* ux, const double* uy, const double* uz, const double* v,
+                         const double* init, double* out, int zconv_reference)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z)");
+    LSG_REQUIRE(ux && uy && uz && v && out, LSG_ERR_ARG, "null argument");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const long long cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
+                              (long long)d.N * d.M * (d.K - 1)};
+    const double* hu[3] = {ux, uy, uz};
+    DevBuf<double> du[3], dv, di, dout;
+    for (int k = 0; k < 3; k++) {
+        du[k].alloc(cnt[k]);
+        LSG_CUDA(cudaMemcpyAsync(du[k].p, hu[k], cnt[k] * 8, cudaMemcpyHostToDevice, C.s));
+    }
+    dv.alloc(cnt[dir]);
+    dout.alloc(cnt[dir]);
+    LSG_CUDA(cudaMemcpyAsync(dv.p, v, cnt[dir] * 8, cudaMemcpyHostToDevice, C.s));
+    if (init) {
+        di.alloc(cnt[dir]);
+        LSG_CUDA(cudaMemcpyAsync(di.p, init, cnt[dir] * 8, cudaMemcpyHostToDevice, C.s));
+    }
+    convective_apply(C, dir, du[0].p, du[1].p, du[2].p, dv.p, init ? di.p : nullptr, dout.p, zconv_reference != 0);
+    LSG_CUDA(cudaMemcpyAsync(out, dout.p, cnt[dir] * 8, cudaMemcpyDeviceToHost, C.s));
     LSG_CUDA(cudaStreamSynchronize(C.s));
     return LSG_OK;
     LSG_API_END(h)

@@ -52,7 +52,7 @@ EXPORTS = [
     "lsg_solve_adjoint", "lsg_operator_gradient", "lsg_set_matrix_geometry", "lsg_get_matrix_stencil7",
     "lsg_set_staggered_types", "lsg_projection_rhs", "lsg_projection_rhs_device", "lsg_projection_correct",
     "lsg_projection_correct_device", "lsg_laplace_flux", "lsg_laplace_flux_device", "lsg_projection_adjoint",
-    "lsg_momentum_rhs", "lsg_version",
+    "lsg_momentum_rhs", "lsg_convective_apply", "lsg_convective_apply_device", "lsg_version",
 ]
 
 _lib = None
@@ -103,6 +103,8 @@ def load() -> C.CDLL:
     lib.lsg_get_matrix_stencil7.argtypes = [P, dp]
     lib.lsg_set_staggered_types.argtypes = [P, ip, ip, ip]
     lib.lsg_laplace_flux.argtypes = [P, ip, dp, dp, dp, dp, dp]
+    lib.lsg_convective_apply.argtypes = [P, C.c_int, dp, dp, dp, dp, dp, dp, C.c_int]
+    lib.lsg_convective_apply_device.argtypes = [P, C.c_int] + [C.c_void_p] * 6 + [C.c_int]
     lib.lsg_momentum_rhs.argtypes = [P, C.c_int, ip, ip, dp, dp, dp, dp, dp, dp, dp, dp, C.c_double, dp, dp]
     lib.lsg_projection_adjoint.argtypes = [P, dp, dp, dp, dp, C.c_double, dp, dp, dp, dp, C.POINTER(Stats)]
     lib.lsg_laplace_flux_device.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p, dp, C.c_void_p, C.c_void_p]

@@ -116,6 +116,18 @@ class IterativeSolver:
         self.ctx.check(self.ctx.lib.lsg_laplace_flux(self.ctx.h, L.iptr(st), *(L.dptr(a) for a in arrs), L.dptr(f)))
         return f
 
+    def convective_apply(self, direction: int, U, v, init=None, zconv_reference: bool = True) -> np.ndarray:
+        """init + C(U) v for momentum component direction, C the convective
+        operator built from the velocity U = (ux, uy, uz)."""
+        us = [np.ascontiguousarray(a, dtype=np.float64) for a in U]
+        vv = np.ascontiguousarray(v, dtype=np.float64)
+        ii = None if init is None else np.ascontiguousarray(init, dtype=np.float64)
+        out = np.empty_like(vv)
+        self.ctx.check(self.ctx.lib.lsg_convective_apply(self.ctx.h, int(direction), *(L.dptr(a) for a in us),
+                                                         L.dptr(vv), None if ii is None else L.dptr(ii),
+                                                         L.dptr(out), int(bool(zconv_reference))))
+        return out
+
     def momentum_rhs(self, direction: int, Cconv, flux2, u, uprev, vof, hflux, p, prev_aux, coef2):
         """(right, aux) of one momentum equation (HelmholtzDiscreteEquation::
         recalcRightMember); Cconv = (rowptr, col, val) of the convective
