@@ -182,7 +182,9 @@ def config_dict(args, world):
     return {"workload": f"poisson_spheres4_{args.size}^3_mgfgmres30_rel1e-10",
             "grid": [args.size] * 3, "bodies": "4 seeded spheres (seed 3), Neumann walls, 2 pinned rows",
             "krylov": f"FGMRES({getattr(args, 'restart', 30)}) FP64, modified Gram-Schmidt ({getattr(args, 'gs', 'mgs')} form)",
-            "precond": "Galerkin MG, ADLJ z/y/x line smoother V(0,3), omega 0.805",
+            "precond": ("Galerkin MG, red-black / 8-colour Gauss-Seidel V(2,2)"
+                        if getattr(args, "smoother", "adlj") == "rbgs"
+                        else "Galerkin MG, ADLJ z/y/x line smoother V(0,3), omega 0.805"),
             "l2": "inputs larger than L2 (operator 0.94 GB FP64 + Krylov basis)",
             "parallelism": "replicas" if world > 1 else "single GPU"}
 
@@ -196,6 +198,9 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--restart", type=int, default=30, help="FGMRES restart length (30 = the measured workload)")
+    ap.add_argument("--smoother", default="adlj", choices=["adlj", "rbgs"],
+                    help="multigrid smoother of both arms: the reference's ADLJ V(0,3) (default) or the "
+                         "red-black Gauss-Seidel V(2,2) variant")
     ap.add_argument("--gs", default="lowsync", choices=["mgs", "lowsync"],
                     help="Gram-Schmidt form of both arms: the low-synchronisation form of the MGS "
                          "projections (default; two passes over the basis per step) or the reference's "
@@ -220,13 +225,17 @@ def main():
     P, dims, pins, b = cases.load(args.size)
     n = b.size
     bnorm = float(np.linalg.norm(b))
-    task = S.Task(eps=1e-10 * bnorm, MAX_ITER=200, FGMRES_RESTART_NUM=args.restart)
+    task = S.Task(eps=1e-10 * bnorm, MAX_ITER=200, FGMRES_RESTART_NUM=args.restart,
+                  n_post=2 if args.smoother == "rbgs" else 3)
     dev = f"cuda:{local}"
     b_dev = torch.from_numpy(b).to(dev)
     results = {}
     gs = L.GS_LOWSYNC if args.gs == "lowsync" else L.GS_MGS
     for name, prec in (("fp32", L.FP32), ("fp64", L.FP64)):
-        s = S.MGFGMRES(device=local, mg_precision=prec, gram_schmidt=gs)
+        if args.smoother == "rbgs":
+            s = S.MGFGMRES(device=local, mg_precision=prec, gram_schmidt=gs, smoother=L.SMOOTHER_RBGS, n_pre=2)
+        else:
+            s = S.MGFGMRES(device=local, mg_precision=prec, gram_schmidt=gs)
         s.set_planes(P, dims, task)
         x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
         st = L.Stats()

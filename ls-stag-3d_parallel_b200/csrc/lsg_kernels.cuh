@@ -562,7 +562,7 @@ struct RTab {
 
 // ch = P cHH and c = ch  (the prolongation plus the copy c.copy(m_ch) of
 // MultiGridSolver::solve, multigrid_solver.h:65-66)
-template <typename T, int ZC>
+template <typename T, int ZC, bool ADD = false>
 __global__ void __launch_bounds__(256) k_prolong(int N, int M, int K, int Nc, int Mc, PTab px, PTab py, PTab pz,
                                                  const T* __restrict__ coarse, T* __restrict__ ch, T* __restrict__ c)
 {
@@ -613,8 +613,12 @@ __global__ void __launch_bounds__(256) k_prolong(int N, int M, int K, int Nc, in
                     if (wz[u][a] != 0.f && wy[b] != 0.f && wx[q] != 0.f)
                         acc += (T)(wz[u][a] * wy[b] * wx[q]) * g[u][4 * a + 2 * b + q];
         const int i = x + N * (y + M * z);                 // grids hold fewer than 2^31 cells
-        ch[i] = acc;
-        c[i] = acc;
+        if (ADD) {
+            ch[i] += acc;                                  // correction added to the smoothed iterate
+        } else {
+            ch[i] = acc;
+            c[i] = acc;
+        }
     }
 }
 
@@ -1467,6 +1471,105 @@ __global__ void k_laplace_from_geometry(int N, int M, int K, const int* __restri
 #pragma unroll
         for (int s = 0; s < 7; s++) planes[(size_t)s * n + i] = a[s];
     }
+}
+
+}  // namespace lsg
+
+namespace lsg {
+
+// ---------------------------------------------------------------------------
+// Multi-colour point Gauss-Seidel (the red-black smoother variant; no
+// counterpart in the reference, whose smoother is ADLJ).  One launch per
+// colour updates every cell of that colour in place,
+//   x_i = (b_i - sum_{j != i} a_ij x_j) * dinv_i,
+// dinv_i = 1 / a_ii, or 0 on rows whose pivot is below the level's tiny
+// threshold (solid and sealed cells keep their value).  Cells of one colour
+// never couple: 7-point rows use the parity of x + y + z (red-black), 27-point
+// box rows the parities of x, y and z (8 colours).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_gs_dinv(long long n, const double* __restrict__ diag, const double* __restrict__ tinyp,
+                          T* __restrict__ dinv)
+{
+    const double tiny = *tinyp;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double d = diag[i];
+        dinv[i] = (T)(fabs(d) < tiny ? 0.0 : 1.0 / d);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_gs_rb7(int N, int M, int K, int color, const int* __restrict__ cls,
+                                                const T* __restrict__ dict, const T* __restrict__ dinv,
+                                                const T* __restrict__ b, T* __restrict__ x)
+{
+    const int xh = blockIdx.x * 32 + threadIdx.x;
+    const int iy = blockIdx.y * 8 + threadIdx.y;
+    const int iz = blockIdx.z;
+    const int ix = 2 * xh + ((iy + iz + color) & 1);
+    if (ix >= N || iy >= M) return;
+    const int NM = N * M;
+    const int i = ix + N * iy + NM * iz;
+    const T di = dinv[i];
+    if (di == (T)0) return;
+    const T* a = dict + (size_t)cls[i] * 7;
+    T acc = b[i];
+    if (iz > 0) acc -= a[0] * x[i - NM];
+    if (iy > 0) acc -= a[1] * x[i - N];
+    if (ix > 0) acc -= a[2] * x[i - 1];
+    if (ix < N - 1) acc -= a[4] * x[i + 1];
+    if (iy < M - 1) acc -= a[5] * x[i + N];
+    if (iz < K - 1) acc -= a[6] * x[i + NM];
+    x[i] = acc * di;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_gs_box27(int N, int M, int K, int color, const int* __restrict__ cls,
+                                                  const T* __restrict__ dict28, const T* __restrict__ dinv,
+                                                  const T* __restrict__ b, T* __restrict__ x)
+{
+    const int ix = 2 * (blockIdx.x * 32 + threadIdx.x) + (color & 1);
+    const int iy = 2 * (blockIdx.y * 8 + threadIdx.y) + ((color >> 1) & 1);
+    const int iz = 2 * blockIdx.z + ((color >> 2) & 1);
+    if (ix >= N || iy >= M || iz >= K) return;
+    const int NM = N * M;
+    const int i = ix + N * iy + NM * iz;
+    const T di = dinv[i];
+    if (di == (T)0) return;
+    T a[28];
+    load_row28(dict28 + (size_t)cls[i] * 28, a);
+    T acc = b[i];
+#pragma unroll
+    for (int dz = -1; dz <= 1; dz++)
+#pragma unroll
+        for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+            for (int dx = -1; dx <= 1; dx++) {
+                if (dx == 0 && dy == 0 && dz == 0) continue;
+                const bool ok = ix + dx >= 0 && ix + dx < N && iy + dy >= 0 && iy + dy < M && iz + dz >= 0 &&
+                                iz + dz < K;
+                if (ok) acc -= a[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] * x[i + dz * NM + dy * N + dx];
+            }
+    x[i] = acc * di;
+}
+
+// damped point Jacobi for levels with wider (mixed-parity) stencils:
+// x += 0.8 dinv (b - A x), with t = b - A x computed by the caller
+template <typename T>
+__global__ void k_jacobi_update(long long n, const T* __restrict__ dinv, const T* __restrict__ t, T* __restrict__ x)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        x[i] += (T)0.8 * dinv[i] * t[i];
+}
+
+template <typename T>
+__global__ void k_sub_from(long long n, const T* __restrict__ b, T* __restrict__ t)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        t[i] = b[i] - t[i];
 }
 
 }  // namespace lsg

@@ -148,6 +148,7 @@ struct LevelT {
     DevBuf<T> dict28;         // 27-point levels: rows padded to stride 28 for vector loads
     int nclass = 0;
     DevBuf<T> lo[3], dinv[3], up[3];
+    DevBuf<T> gsdinv;         // Gauss-Seidel smoother: 1 / a_ii, 0 below the tiny pivot threshold
     DevBuf<T> r, c, ch;
 };
 
@@ -473,7 +474,7 @@ static void fill_tail(const MGData& mg, const std::vector<LevelT<T>>& lev, int l
 static void tail_setup(Context& C)
 {
     MGData& mg = C.mg;
-    mg.tail_l0 = tail_first_level(mg);
+    mg.tail_l0 = C.opt.smoother == LSG_SMOOTHER_ADLJ ? tail_first_level(mg) : -1;
     if (mg.tail_l0 < 0) return;
     TailArgs<double> a64;
     fill_tail<double>(mg, mg.l64, mg.tail_l0, C, a64);
@@ -580,6 +581,11 @@ static void mg_setup(Context& C)
         double tiny = 1e-5 * maxabs;
         if (tiny < 1e-12) tiny = 1e-12;
         LSG_CUDA(cudaMemcpyAsync(tinyp, &tiny, sizeof(double), cudaMemcpyHostToDevice, s));
+        if (o.smoother == LSG_SMOOTHER_RBGS) {           // point pivots from the diagonal, before the line LU
+            lv.gsdinv.alloc(n);
+            k_gs_dinv<double><<<grid_for(n, 256), 256, 0, s>>>(n, lv.dinv[0].p, tinyp, lv.gsdinv.p);
+            LSG_CHECK_LAUNCH();
+        }
         for (int d = 0; d < 3; d++) {
             LineGeom g{lv.d.N, lv.d.M, lv.d.K, d};
             LSG_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
@@ -659,6 +665,11 @@ static void mg_setup(Context& C)
                 const long long n28 = (long long)a.nclass * 28;
                 b.dict28.alloc(n28);
                 k_convert<float, double><<<grid_for(n28, 256), 256, 0, s>>>(n28, a.dict28.p, b.dict28.p);
+                LSG_CHECK_LAUNCH();
+            }
+            if (l < L && a.gsdinv.p) {
+                b.gsdinv.alloc(n);
+                k_convert<float, double><<<grid_for(n, 256), 256, 0, s>>>(n, a.gsdinv.p, b.gsdinv.p);
                 LSG_CHECK_LAUNCH();
             }
             if (l < L) {
@@ -771,11 +782,103 @@ static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStr
     LSG_CHECK_LAUNCH();
 }
 
+// One smoothing sweep of the multi-colour Gauss-Seidel variant on level lv:
+// colours in increasing order (forward) or decreasing order (backward, for
+// the post-smoothing of a symmetric cycle).
+template <typename T>
+static void gs_sweep(const LevelT<T>& lv, const T* b, T* x, bool backward, cudaStream_t s)
+{
+    const Dims& d = lv.d;
+    if (lv.ol.n == 7 && lv.off[0] == 0 && lv.off[2] == -1) {
+        const dim3 g((d.N / 2 + 1 + 31) / 32, (d.M + 7) / 8, d.K);
+        for (int q = 0; q < 2; q++) {
+            k_gs_rb7<T><<<g, dim3(32, 8), 0, s>>>(d.N, d.M, d.K, backward ? 1 - q : q, lv.cls, lv.dict,
+                                                  lv.gsdinv.p, b, x);
+            LSG_CHECK_LAUNCH();
+        }
+    } else if (lv.ol.n == 27 && lv.dict28.p) {
+        const dim3 g(((d.N + 1) / 2 + 31) / 32, ((d.M + 1) / 2 + 7) / 8, (d.K + 1) / 2);
+        for (int q = 0; q < 8; q++) {
+            k_gs_box27<T><<<g, dim3(32, 8), 0, s>>>(d.N, d.M, d.K, backward ? 7 - q : q, lv.cls, lv.dict28.p,
+                                                    lv.gsdinv.p, b, x);
+            LSG_CHECK_LAUNCH();
+        }
+    } else {
+        // wider stencils (mixed-parity coarsening): one damped Jacobi step
+        T* t = const_cast<T*>(lv.c.p);
+        const long long n = d.n();
+        apply_resid<T>(lv, x, t, s, 1);                 // t = A x
+        k_sub_from<T><<<grid_for(n, 256), 256, 0, s>>>(n, b, t);
+        LSG_CHECK_LAUNCH();
+        k_jacobi_update<T><<<grid_for(n, 256), 256, 0, s>>>(n, lv.gsdinv.p, t, x);
+        LSG_CHECK_LAUNCH();
+    }
+}
+
+// V(n_pre, n_post) cycle with the multi-colour Gauss-Seidel smoother (the
+// red-black variant): on the way down each level starts from zero, is
+// pre-smoothed, and restricts its residual; the coarsest level is solved by
+// the dense LU; on the way up the prolonged correction is added and
+// post-smoothed.  Same hierarchy, transfers and coarsest solve as the
+// reference-shaped cycle.
+template <typename T>
+static void vcycle_rb(Context& C, std::vector<LevelT<T>>& lev, T* ch0)
+{
+    MGData& mg = C.mg;
+    cudaStream_t s = C.s;
+    const int L = mg.L;
+    const int npre = C.opt.n_pre, npost = C.opt.n_post;
+    for (int l = 0; l < L; l++) {
+        LevelT<T>& lv = lev[l];
+        const Dims& f = lv.d;
+        const Dims& c = lev[l + 1].d;
+        T* x = (l == 0 && ch0) ? ch0 : lv.ch.p;
+        const T* res = lv.r.p;
+        if (npre > 0) {
+            LSG_CUDA(cudaMemsetAsync(x, 0, f.n() * sizeof(T), s));
+            for (int it = 0; it < npre; it++) gs_sweep<T>(lv, lv.r.p, x, false, s);
+            // residual r - A x into c
+            LSG_CUDA(cudaMemcpyAsync(lv.c.p, lv.r.p, f.n() * sizeof(T), cudaMemcpyDeviceToDevice, s));
+            apply_resid<T>(lv, x, lv.c.p, s, 0);
+            res = lv.c.p;
+        }
+        const TransferTabs& t = mg.tabs[l];
+        k_restrict<T><<<grid_for(c.n(), 256), 256, 0, s>>>(c.N, c.M, c.K, f.N, f.M, mg.agg[l], t.R(0), t.R(1), t.R(2),
+                                                          res, lev[l + 1].r.p);
+        LSG_CHECK_LAUNCH();
+    }
+    k_coarse_solve<T><<<1, 32, 0, s>>>(mg.nc, mg.dL.p, mg.dU.p, mg.dscale.p, mg.dperm.p, lev[L].r.p, lev[L].ch.p,
+                                       mg.dwork.p);
+    LSG_CHECK_LAUNCH();
+    for (int l = L - 1; l >= 0; l--) {
+        LevelT<T>& lv = lev[l];
+        const Dims& f = lv.d;
+        const TransferTabs& t = mg.tabs[l];
+        T* x = (l == 0 && ch0) ? ch0 : lv.ch.p;
+        constexpr int PZ = 4;
+        const dim3 pg((f.N + 31) / 32, (f.M + 7) / 8, (f.K + PZ - 1) / PZ);
+        if (npre > 0) {
+            k_prolong<T, PZ, true><<<pg, dim3(32, 8), 0, s>>>(f.N, f.M, f.K, lev[l + 1].d.N, lev[l + 1].d.M, t.P(0),
+                                                              t.P(1), t.P(2), lev[l + 1].ch.p, x, lv.c.p);
+        } else {
+            k_prolong<T, PZ><<<pg, dim3(32, 8), 0, s>>>(f.N, f.M, f.K, lev[l + 1].d.N, lev[l + 1].d.M, t.P(0), t.P(1),
+                                                        t.P(2), lev[l + 1].ch.p, x, lv.c.p);
+        }
+        LSG_CHECK_LAUNCH();
+        for (int it = 0; it < npost; it++) gs_sweep<T>(lv, lv.r.p, x, true, s);
+    }
+    C.vcycles++;
+}
+
 // ch0: where the finest-level correction (the preconditioned vector) goes;
 // nullptr = the level's own buffer.
 template <typename T>
 static void vcycle(Context& C, std::vector<LevelT<T>>& lev, T* ch0 = nullptr)
 {
+    if (C.opt.smoother == LSG_SMOOTHER_RBGS) {
+        vcycle_rb<T>(C, lev, ch0);
+        return;
+    }
     MGData& mg = C.mg;
     cudaStream_t s = C.s;
     const int L = mg.L;
@@ -819,17 +922,24 @@ static void vcycle(Context& C, std::vector<LevelT<T>>& lev, T* ch0 = nullptr)
 }
 
 // Algorithmic bytes of one V-cycle with element size w (documented model).
-static double vcycle_bytes(const MGData& mg, int n_post, double w)
+static double vcycle_bytes(const MGData& mg, const lsg_options& o, double w)
 {
     double b = 0;
     for (int l = 0; l <= mg.L; l++) {
         const double n = (double)mg.dims[l].n();
         if (l < mg.L) {
             b += (1.0 + 0.125) * w * n;                      // restriction read fine + write coarse
-            b += (0.125 + 2.0) * w * n;                      // prolongation read coarse + write ch, c
-            // per direction: residual (r rw, c; row class 4 B; the distinct-row
-            // table is L2 resident) + line solve (r, lo, dinv, up, ch read; c, ch written)
-            b += 3.0 * n_post * ((3.0 * w + 4.0) + 7.0 * w) * n;
+            b += (0.125 + 2.0) * w * n;                      // prolongation read coarse + write ch, c (or ch rw)
+            if (o.smoother == LSG_SMOOTHER_RBGS) {
+                // full colour sweep: b, x read, x written, row class 4 B; pre-smoothed
+                // levels also form their residual (copy 2w + apply 3w + 4)
+                b += (o.n_pre + o.n_post) * (3.0 * w + 4.0) * n;
+                if (o.n_pre > 0) b += (5.0 * w + 4.0) * n;
+            } else {
+                // per direction: residual (r rw, c; row class 4 B; the distinct-row
+                // table is L2 resident) + line solve (r, lo, dinv, up, ch read; c, ch written)
+                b += 3.0 * o.n_post * ((3.0 * w + 4.0) + 7.0 * w) * n;
+            }
         }
     }
     return b;
@@ -964,12 +1074,12 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
                     k_scale_copy<float><<<grid_for(n, 256), 256, 0, s>>>(n, C.w.p, &ks->invNormW, vj, C.mg.l32[0].r.p);
                     LSG_CHECK_LAUNCH();
                     vcycle<float>(C, C.mg.l32, zj32);
-                    bytes += (8 + 8 + 4) * (double)n + vcycle_bytes(C.mg, C.opt.n_post, 4.0);
+                    bytes += (8 + 8 + 4) * (double)n + vcycle_bytes(C.mg, C.opt, 4.0);
                 } else {
                     k_scale_copy<double><<<grid_for(n, 256), 256, 0, s>>>(n, C.w.p, &ks->invNormW, vj, C.t1.p);
                     LSG_CHECK_LAUNCH();
                     precond_apply(C, C.t1.p, zj);
-                    bytes += 24.0 * n + (C.opt.precond == LSG_PC_MG ? vcycle_bytes(C.mg, C.opt.n_post, 8.0) + 32.0 * n : 0);
+                    bytes += 24.0 * n + (C.opt.precond == LSG_PC_MG ? vcycle_bytes(C.mg, C.opt, 8.0) + 32.0 * n : 0);
                 }
                 // w = A z_j ; H[0,j] = (w, v_0)
                 double* Hj = ks->H + (size_t)j * 65;
@@ -1951,7 +2061,10 @@ int lsg_setup(lsg_ctx* h, const lsg_options* opts)
     LSG_REQUIRE(C.opt.restart >= 1 && C.opt.restart <= 64, LSG_ERR_ARG, "restart must be in [1, 64]");
     LSG_REQUIRE(C.opt.max_it >= 1, LSG_ERR_ARG, "max_it must be >= 1");
     LSG_REQUIRE(C.opt.n_post >= 0 && C.opt.n_post <= 16, LSG_ERR_ARG, "n_post must be in [0, 16]");
-    LSG_REQUIRE(C.opt.smoother == LSG_SMOOTHER_ADLJ, LSG_ERR_ARG, "smoother not supported");
+    LSG_REQUIRE(C.opt.smoother == LSG_SMOOTHER_ADLJ || C.opt.smoother == LSG_SMOOTHER_RBGS, LSG_ERR_ARG,
+                "smoother not supported");
+    LSG_REQUIRE(C.opt.n_pre >= 0 && C.opt.n_post >= 0 && (C.opt.smoother == LSG_SMOOTHER_RBGS || C.opt.n_pre == 0),
+                LSG_ERR_ARG, "pre-smoothing needs the Gauss-Seidel smoother (the ADLJ cycle is V(0, n_post))");
     C.have_setup = false;
     if (C.opt.precond == LSG_PC_MG) mg_setup(C);
     if (C.opt.precond == LSG_PC_ILU0) ilu_setup(C);

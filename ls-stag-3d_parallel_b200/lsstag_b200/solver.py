@@ -38,9 +38,12 @@ class IterativeSolver:
     precond = L.PC_MG
 
     def __init__(self, device: int = 0, mg_precision: int = L.FP64, zline_reference: bool = True,
-                 max_levels: int = 0, omega: float = 0.805, gram_schmidt: int = L.GS_MGS):
+                 max_levels: int = 0, omega: float = 0.805, gram_schmidt: int = L.GS_MGS,
+                 smoother: int = L.SMOOTHER_ADLJ, n_pre: int = 0):
         self.ctx = L.Context(device)
         self.mg_precision = mg_precision
+        self.smoother = smoother
+        self.n_pre = n_pre
         self.gram_schmidt = gram_schmidt
         self.zline_reference = zline_reference
         self.max_levels = max_levels
@@ -184,7 +187,8 @@ class IterativeSolver:
                                  restart=int(self.task.FGMRES_RESTART_NUM), max_it=int(self.task.MAX_ITER),
                                  n_post=int(self.task.n_post), eps=float(self.eps),
                                  zline_reference=int(self.zline_reference), max_levels=int(self.max_levels),
-                                 omega=float(self.omega), gram_schmidt=int(self.gram_schmidt))
+                                 omega=float(self.omega), gram_schmidt=int(self.gram_schmidt),
+                                 smoother=int(self.smoother), n_pre=int(self.n_pre))
 
     def _setup(self):
         o = self.options()
