@@ -124,6 +124,7 @@ struct HarnessTask : FlowTaskDescription {
         PeriodPrintRotor = 0.0;
         PeriodSaveState = 1e30;
     }
+    double loadsCoef() const { return fcoef; }
     void calcNodesCount() override
     {
         mesh.baseMesh.N = gN;
@@ -315,6 +316,79 @@ int solvePlanes(const Config& cfg, const std::string& outdir)
     return 0;
 }
 
+template <typename T>
+bool readRaw(const Config& cfg, const std::string& key, std::vector<T>& v, long cnt)
+{
+    v.assign(cnt, T(0));
+    const std::string path = cfg.gets(key, "");
+    if (path.empty()) return false;
+    std::ifstream f(path, std::ios::binary);
+    f.read((char*)v.data(), sizeof(T) * cnt);
+    return (bool)f;
+}
+
+/* The reference's per-cut-cell load kernel (LoadsCalculator::calc,
+   loads_calculator.h:79-1269) and its moment kernels (:1270-1291) evaluated
+   on arrays read from files: every cut-cell type is exercised on seeded
+   inputs, independently of which types a geometry happens to produce.  Also
+   runs the moment filter (ButterworthLowPassFilter, butterworth_low_pass_filter.h)
+   on a given signal. */
+int loadsProbe(const Config& cfg, const std::string& outdir)
+{
+    const int N = (int)cfg.get("N", 0), M = (int)cfg.get("M", 0), K = (int)cfg.get("K", 0);
+    const long n = (long)N * M * K;
+    const int count = (int)cfg.get("count", 0);
+    std::vector<int> type, cells;
+    std::vector<double> theta, delta, vib, vibyx, vibzy, dne, dtn, dmax, nodes, invv, p, ux, uy, uz, nucell, cc;
+    bool ok = readRaw(cfg, "lp_type", type, n) && readRaw(cfg, "lp_cells", cells, count) &&
+              readRaw(cfg, "lp_theta", theta, 3 * n) && readRaw(cfg, "lp_delta", delta, 3 * n) &&
+              readRaw(cfg, "lp_vib", vib, 3 * n) && readRaw(cfg, "lp_vibyx", vibyx, 3 * n) &&
+              readRaw(cfg, "lp_vibzy", vibzy, 3 * n) && readRaw(cfg, "lp_dne", dne, 3 * n) &&
+              readRaw(cfg, "lp_dtn", dtn, 3 * n) && readRaw(cfg, "lp_dmax", dmax, 3 * n) &&
+              readRaw(cfg, "lp_nodes", nodes, 3 * n) && readRaw(cfg, "lp_center", cc, 3) &&
+              readRaw(cfg, "lp_invv", invv, n) && readRaw(cfg, "lp_p", p, n) &&
+              readRaw(cfg, "lp_ux", ux, (long)(N - 1) * M * K) && readRaw(cfg, "lp_uy", uy, (long)N * (M - 1) * K) &&
+              readRaw(cfg, "lp_uz", uz, (long)N * M * (K - 1));
+    if (!ok) { fprintf(stderr, "cannot read loads probe inputs\n"); return 3; }
+    const bool haveNu = readRaw(cfg, "lp_nucell", nucell, n);
+    const double nu = cfg.get("nu", 0.01);
+    std::vector<tripletInt> list(count);
+    for (int i = 0; i < count; i++) {
+        const int num = cells[i], k = num / (N * M), j = (num - k * N * M) / N;
+        list[i].set(num - j - k * M, num - k * N, num);      // BaseTaskDescription::addCutCell
+    }
+    std::vector<double> fx(count), fy(count), fz(count), mz(count), mx(count), my(count);
+    auto C = [](std::vector<double>& v) { return (coordinate*)v.data(); };
+    for (int i = 0; i < count; i++)
+        LoadsCalculator::_k_calc(i, (const CellTypes*)type.data(), list.data(), fx.data(), fy.data(), fz.data(),
+                                 C(vib), C(vibyx), C(vibzy), C(delta), C(dne), C(dtn), C(dmax), C(theta),
+                                 ux.data(), uy.data(), uz.data(), p.data(), invv.data(),
+                                 haveNu ? nucell.data() : nullptr, nu, N, M, N * M);
+    for (int i = 0; i < count; i++) {
+        mz[i] = LoadsCalculator::_k_calcMoment(i, C(nodes), list.data(), fx.data(), fy.data(), C(cc));
+        mx[i] = LoadsCalculator::_k_calcMomentX(i, C(nodes), list.data(), fy.data(), fz.data(), C(cc));
+        my[i] = LoadsCalculator::_k_calcMomentY(i, C(nodes), list.data(), fx.data(), fz.data(), C(cc));
+    }
+    Dumper out(outdir);
+    out.d("fx", fx.data(), count);
+    out.d("fy", fy.data(), count);
+    out.d("fz", fz.data(), count);
+    out.d("mz", mz.data(), count);
+    out.d("mx", mx.data(), count);
+    out.d("my", my.data(), count);
+    const int ns = (int)cfg.get("filter_len", 0);
+    if (ns > 0) {
+        std::vector<double> sig;
+        if (!readRaw(cfg, "filter_in", sig, ns)) { fprintf(stderr, "cannot read filter input\n"); return 3; }
+        ButterworthLowPassFilter flt;
+        flt.init(cfg.get("dt", 0.01), DEFAULT_CUT_OFF_FREQUENCY, DEFAULT_SUPPRESSION_LEVEL);
+        std::vector<double> res(ns);
+        for (int i = 0; i < ns; i++) res[i] = flt.getValue(sig[i]);
+        out.d("filter_out", res.data(), ns);
+    }
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv)
@@ -328,6 +402,7 @@ int main(int argc, char** argv)
     const int threads = (int)cfg.get("threads", 0);
     if (threads > 0) omp_set_num_threads(threads);
     if (!cfg.gets("planes_in", "").empty()) return solvePlanes(cfg, outdir);
+    if ((int)cfg.get("loads_probe", 0)) return loadsProbe(cfg, outdir);
 
     HarnessTask* task = new HarnessTask;
     task->gN = (int)cfg.get("N", 16);
@@ -369,6 +444,61 @@ int main(int argc, char** argv)
         for (long i = 0; i < nb; i++)
             mm->v_ib[i].set(0.1 * sin(0.11 * i), 0.1 * cos(0.13 * i), 0.05 * sin(0.17 * i));
         for (long i = 0; i < (long)mm->xMesh.NMK; i++) mm->m_Ux[i] = 1.0 + 0.2 * sin(0.29 * i);
+    }
+    if ((int)cfg.get("loads", 0)) {
+        // LoadsCalculator::calculate (loads_calculator.h:1366-1377) over the
+        // cut cells the mesh build listed (BaseTaskDescription::addCutCell,
+        // base_task_description.h:127-132), on seeded velocities, pressure and
+        // immersed-boundary velocities (velocities stay zero inside the bodies)
+        LSSTAGUniformMesh* mm = task->m_mesh;
+        const int N = mm->baseMesh.N, M = mm->baseMesh.M, K = mm->baseMesh.K;
+        const long n = (long)N * M * K;
+        double* cur[3] = {mm->m_Ux, mm->m_Uy, mm->m_Uz};
+        const long ns[3] = {(long)mm->xMesh.NMK, (long)mm->yMesh.NMK, (long)mm->zMesh.NMK};
+        const CellTypes* st[3] = {mm->xMesh.typeOfCell, mm->yMesh.typeOfCell, mm->zMesh.typeOfCell};
+        for (int d = 0; d < 3; d++)
+            for (long i = 0; i < ns[d]; i++)
+                cur[d][i] = (st[d][i] == SolidCell) ? 0.0 : (d == 0 ? 1.0 : 0.0) + 0.2 * sin(0.07 * i + d);
+        for (long i = 0; i < n; i++) {
+            mm->m_P[i] = 0.3 * sin(0.013 * i);
+            mm->v_ib[i].set(0.02 * sin(0.11 * i), 0.02 * cos(0.13 * i), 0.01 * sin(0.17 * i));
+            mm->v_ib_yx[i].set(0.02 * cos(0.19 * i), 0.01 * sin(0.23 * i), 0.02 * cos(0.29 * i));
+            mm->v_ib_zy[i].set(0.01 * sin(0.31 * i), 0.02 * cos(0.37 * i), 0.01 * cos(0.41 * i));
+        }
+        LoadsCalculator& L = task->m_loads[0];
+        L.initSol();
+        L.calculate();
+        const int cnt = L.countCutCells;
+        std::vector<int> cells(cnt);
+        for (int i = 0; i < cnt; i++) cells[i] = L.OnAirfoil[i].z;
+        int dd[3] = {N, M, K};
+        out.i("dims", dd, 3);
+        out.i("cells", cells.data(), cnt);
+        out.d("fx", L.ForceX, cnt);
+        out.d("fy", L.ForceY, cnt);
+        out.d("fz", L.ForceZ, cnt);
+        double sc[9] = {L.F_aer_x, L.F_aer_y, L.F_aer_z, L.C_d, L.C_y, L.C_z,
+                        L.moment_aer, L.moment_x_aer, L.moment_y_aer};
+        out.d("sums", sc, 9);
+        double par[3] = {task->nu, task->loadsCoef(), task->t};
+        out.d("nu_fcoef_dt", par, 3);
+        out.i("celltype", (const int*)mm->baseMesh.typeOfCell, n);
+        out.d("theta", (const double*)mm->theta, 3 * n);
+        out.d("delta", (const double*)mm->delta, 3 * n);
+        out.d("inv_vof", mm->baseMesh.inv_VOF, n);
+        out.d("dmax", (const double*)mm->delta_ib_max, 3 * n);
+        out.d("dne", (const double*)mm->inv_delta_ib_ne, 3 * n);
+        out.d("dtn", (const double*)mm->inv_delta_ib_tn, 3 * n);
+        out.d("vib", (const double*)mm->v_ib, 3 * n);
+        out.d("vibyx", (const double*)mm->v_ib_yx, 3 * n);
+        out.d("vibzy", (const double*)mm->v_ib_zy, 3 * n);
+        out.d("nodes", (const double*)mm->nodes, 3 * n);
+        out.d("center", (const double*)mm->cur_C, 3);
+        out.d("ux", mm->m_Ux, ns[0]);
+        out.d("uy", mm->m_Uy, ns[1]);
+        out.d("uz", mm->m_Uz, ns[2]);
+        out.d("p", mm->m_P, n);
+        return 0;
     }
     if ((int)cfg.get("operator_only", 0)) {
         // the Laplace operator alone (LaplaceDiscreteOperator::init + build), without

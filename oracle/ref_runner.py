@@ -204,3 +204,44 @@ def run_momentum(case: Case, rhs_xyz, rel_tol: float = 1e-10, *, threads: int = 
     finally:
         import shutil
         shutil.rmtree(d, ignore_errors=True)
+
+
+def run_loads_probe(dims, inputs: dict, nu: float, *, filter_in=None, dt: float = 0.01,
+                    timeout: float = 600) -> dict:
+    """The reference's per-cut-cell load kernel (LoadsCalculator::calc) and
+    moment kernels on given arrays.  ``inputs`` holds type (int32 n), cells
+    (int32, base indices), theta, delta, vib, vibyx, vibzy, dne, dtn, dmax,
+    nodes (3n each, xyz interleaved), center (3), invv, p (n), ux, uy, uz (the
+    staggered grids) and optionally nucell (n).  ``filter_in`` runs the moment
+    filter on a signal."""
+    if not available():
+        raise FileNotFoundError(REF_BIN)
+    import shutil
+    d = tempfile.mkdtemp(prefix="lsg_refl_")
+    try:
+        N, M, K = dims
+        lines = [f"N {N}", f"M {M}", f"K {K}", "loads_probe 1", f"nu {nu!r}",
+                 f"count {len(inputs['cells'])}", f"dt {dt!r}"]
+        for k, v in inputs.items():
+            p = os.path.join(d, k + ".in")
+            dt_ = np.int32 if k in ("type", "cells") else np.float64
+            np.ascontiguousarray(v, dtype=dt_).tofile(p)
+            lines.append(f"lp_{k} {p}")
+        if filter_in is not None:
+            p = os.path.join(d, "filter.in")
+            np.ascontiguousarray(filter_in, dtype=np.float64).tofile(p)
+            lines += [f"filter_len {len(filter_in)}", f"filter_in {p}"]
+        cfg = os.path.join(d, "case.cfg")
+        with open(cfg, "w") as f:
+            f.write("\n".join(lines) + "\n")
+        subprocess.run([REF_BIN, cfg, d], check=True, timeout=timeout, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.PIPE)
+        return load_dir(d)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def run_loads(case: Case, *, threads: int = 1, timeout: float = 600, **opts) -> dict:
+    """LoadsCalculator::calculate on the case's cut cells, with the seeded
+    velocities, pressure and immersed-boundary velocities the harness sets."""
+    return run(case, threads=threads, timeout=timeout, loads=1, dump_geometry=0, **opts)
