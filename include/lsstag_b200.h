@@ -196,6 +196,62 @@ int lsg_convective_apply(lsg_ctx* ctx, int dir, const double* ux, const double* 
 int lsg_convective_apply_device(lsg_ctx* ctx, int dir, const double* ux, const double* uy, const double* uz,
                                 const double* v, const double* init, double* out, int zconv_reference);
 
+/* ---- loads on the immersed boundary (LoadsCalculator, loads_calculator.h) ---- */
+
+typedef struct lsg_loads_result {
+    double force[3];       /* F_aer_x, F_aer_y, F_aer_z: sums of the per-cut-cell forces */
+    double coef[3];        /* C_d, C_y, C_z = force * fcoef */
+    double moment_raw[3];  /* sums of the per-cell moments M_z, M_x, M_y (calcMoment, calcMomentX/Y) */
+    double moment[3];      /* the same after the moment low-pass filters
+                              (moment_aer, moment_x_aer, moment_y_aer) */
+    int count;             /* number of cut cells */
+} lsg_loads_result;
+
+/* The cut-cell list and the geometry the loads read, replacing
+   LoadsCalculator::set + the OnAirfoil list (loads_calculator.h:1298-1333;
+   BaseTaskDescription::addCutCell, base_task_description.h:127-132).  cells
+   holds the base-grid indices of the cut cells in the order the forces are
+   reported; the x/y-grid indices follow from them.  celltype, inv_vof (n)
+   and theta, delta, delta_ib_max, inv_delta_ib_ne, inv_delta_ib_tn, nodes
+   (3n, xyz interleaved, the reference's coordinate arrays) describe the
+   N x M x K base grid; center is the moment centre (cur_C).  fcoef scales
+   forces to coefficients; dt initialises the moment filters
+   (ButterworthLowPassFilter::init with the reference defaults).  A cut cell
+   on the outer layer of the grid is rejected.  Host pointers; the packed
+   records stay on the device until the next call. */
+int lsg_loads_set(lsg_ctx* ctx, int N, int M, int K, int count, const int* cells, const int* celltype,
+                  const double* theta, const double* delta, const double* inv_vof, const double* delta_ib_max,
+                  const double* inv_delta_ib_ne, const double* inv_delta_ib_tn, const double* nodes,
+                  const double* center, double fcoef, double dt);
+/* LoadsCalculator::calculate (loads_calculator.h:1366-1377, calc :79-1269):
+   per-cut-cell forces, their sums and coefficients, the moments and one step
+   of the moment filters.  ux, uy, uz are the staggered velocity grids, p the
+   pressure, vib / vib_yx / vib_zy the immersed-boundary velocities (3n);
+   nu_cell (n) replaces nu per cell when not NULL.  forces (3 * count: all x,
+   then all y, then all z) may be NULL.  Per-cell forces and moments are
+   bitwise equal to the reference's; the sums differ from its OpenMP sums by
+   summation order only.  With no cut cells nothing is computed (as in the
+   reference) and the filters do not advance.  Host pointers. */
+int lsg_loads_calculate(lsg_ctx* ctx, const double* ux, const double* uy, const double* uz, const double* p,
+                        const double* vib, const double* vib_yx, const double* vib_zy, const double* nu_cell,
+                        double nu, double* forces, lsg_loads_result* out);
+/* Same on device pointers (forces a device pointer or NULL; out on the host). */
+int lsg_loads_calculate_device(lsg_ctx* ctx, const double* ux, const double* uy, const double* uz, const double* p,
+                               const double* vib, const double* vib_yx, const double* vib_zy,
+                               const double* nu_cell, double nu, double* forces, lsg_loads_result* out);
+/* Restart the three moment filters with time step dt. */
+int lsg_loads_reset_filter(lsg_ctx* ctx, double dt);
+/* Gradient of J = weight[0] F_aer_x + weight[1] F_aer_y + weight[2] F_aer_z
+   with respect to ux, uy, uz and p (the forces are affine in them, so the
+   gradient depends on the geometry, nu and the weights only): the adjoint
+   of the loads for drag-based objectives.  No reference counterpart (the
+   reference has no adjoint).  Outputs are overwritten.  Host pointers. */
+int lsg_loads_adjoint(lsg_ctx* ctx, const double* weight, const double* nu_cell, double nu, double* g_ux,
+                      double* g_uy, double* g_uz, double* g_p);
+/* Same on device pointers (weight on the host). */
+int lsg_loads_adjoint_device(lsg_ctx* ctx, const double* weight, const double* nu_cell, double nu,
+                             double* g_ux, double* g_uy, double* g_uz, double* g_p);
+
 /* Staggered cell types (LSSTAGUniformMesh xMesh/yMesh/zMesh typeOfCell),
    needed by the staggered-grid entry points below.  Checked on the host like
    the base types (a kept face must lie inside the grid).  Host pointers. */

@@ -13,6 +13,7 @@
 #include "lsg_coarse.cuh"
 #include "lsg_ilu.cuh"
 #include "lsg_krylov.cuh"
+#include "lsg_loads.cuh"
 #include "lsg_projection.cuh"
 
 namespace lsg {
@@ -217,6 +218,20 @@ struct Context {
         long long pin0 = -1, pin1 = -1;
         bool have = false, have_stypes = false;
     } geo;
+    // cut-cell loads: packed per-cut-cell records from lsg_loads_set, the
+    // reduction scratch, and the state of the three moment filters
+    struct Loads {
+        int N = 0, M = 0, K = 0, count = 0;
+        DevBuf<double> g;
+        DevBuf<int> idx;
+        DevBuf<unsigned long long> desc;
+        DevBuf<double> partial, sums;
+        DevBuf<unsigned int> counter;
+        double center[3] = {0, 0, 0};
+        double fcoef = 0;
+        LoadsFilter filt[3];
+        bool have = false;
+    } loads;
 };
 
 }  // namespace lsg
@@ -2428,6 +2443,296 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
     LSG_CUDA(cudaEventElapsedTime(&ms, C.ev0, C.ev1));
     *ms_per_launch = ms / reps;
     *bytes_per_launch = bytes;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+
+// ---------------------------------------------------------------------------
+// cut-cell loads (LoadsCalculator, Base/loads_calculator.h)
+// ---------------------------------------------------------------------------
+int lsg_loads_set(lsg_ctx* h, int N, int M, int K, int count, const int* cells, const int* celltype,
+                  const double* theta, const double* delta, const double* inv_vof, const double* delta_ib_max,
+                  const double* inv_delta_ib_ne, const double* inv_delta_ib_tn, const double* nodes,
+                  const double* center, double fcoef, double dt)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(N >= 3 && M >= 3 && K >= 3, LSG_ERR_ARG, "grid must be at least 3 cells in every direction");
+    LSG_REQUIRE((long long)N * M * K < (1LL << 31), LSG_ERR_ARG, "grid too large for 32-bit cell indices");
+    LSG_REQUIRE(count >= 0, LSG_ERR_ARG, "negative cut-cell count");
+    LSG_REQUIRE(center && (count == 0 || (cells && celltype && theta && delta && inv_vof && delta_ib_max &&
+                                          inv_delta_ib_ne && inv_delta_ib_tn && nodes)),
+                LSG_ERR_ARG, "null argument");
+    LSG_REQUIRE(dt > 0, LSG_ERR_ARG, "time step must be positive (moment filter)");
+    LSG_CUDA(cudaSetDevice(C.device));
+    using namespace loads_desc;
+    const int NM = N * M;
+    const long long n = (long long)NM * K;
+    std::vector<double> g((size_t)LF_COUNT * count);
+    std::vector<int> idx(3 * (size_t)count);
+    std::vector<unsigned long long> desc(count, 0ull);
+    auto put = [&](int f, int i, double v) { g[(size_t)f * count + i] = v; };
+    for (int i = 0; i < count; i++) {
+        const int num = cells[i];
+        LSG_REQUIRE(num >= 0 && num < n, LSG_ERR_ARG, "cut cell index outside the grid");
+        const int k = num / NM, j = (num - k * NM) / N, x = num - k * NM - j * N;
+        LSG_REQUIRE(x >= 1 && x <= N - 2 && j >= 1 && j <= M - 2 && k >= 1 && k <= K - 2, LSG_ERR_ARG,
+                    "cut cell on the outer layer of the grid (its loads read the neighbours on both sides)");
+        idx[i] = num;
+        idx[count + i] = num - j - k * M;      // x-grid index (BaseTaskDescription::addCutCell)
+        idx[2 * count + i] = num - k * N;      // y-grid index
+        const double* t = theta + 3 * (size_t)num;
+        put(LF_TX, i, t[0]);
+        put(LF_TY, i, t[1]);
+        put(LF_TZ, i, t[2]);
+        put(LF_TXX, i, theta[3 * (size_t)(num - 1)]);
+        put(LF_TYY, i, theta[3 * (size_t)(num - N) + 1]);
+        put(LF_TZZ, i, theta[3 * (size_t)(num - NM) + 2]);
+        for (int c = 0; c < 3; c++) {
+            put(LF_DX + c, i, delta[3 * (size_t)num + c]);
+            put(LF_S0 + c, i, delta_ib_max[3 * (size_t)num + c]);
+            put(LF_NX + c, i, nodes[3 * (size_t)num + c]);
+        }
+        put(LF_VV, i, inv_vof[num]);
+        const uint8_t* sl = find(celltype[num]);
+        unsigned long long dsc = 0;
+        for (int s = 0; s < 6; s++) {
+            const unsigned b = sl ? sl[s] : 0u;
+            double dh = 0.0, db = 0.0;
+            if (b & Q) {
+                const int c = vel_of(s);
+                const int step = c == 0 ? 1 : (c == 1 ? N : NM);
+                const double* D = (b & TN) ? inv_delta_ib_tn : inv_delta_ib_ne;
+                dh = D[3 * (size_t)num + dist_of(s)];
+                db = (b & DHERE) ? dh : D[3 * (size_t)(num - step) + dist_of(s)];
+            }
+            put(LF_D + 2 * s, i, dh);
+            put(LF_D + 2 * s + 1, i, db);
+            dsc |= (unsigned long long)b << (8 * s);
+        }
+        desc[i] = dsc;
+    }
+    Context::Loads& L = C.loads;
+    L.have = false;
+    L.N = N;
+    L.M = M;
+    L.K = K;
+    L.count = count;
+    if (count > 0) {
+        L.g.alloc(g.size());
+        L.idx.alloc(idx.size());
+        L.desc.alloc(desc.size());
+        LSG_CUDA(cudaMemcpyAsync(L.g.p, g.data(), g.size() * 8, cudaMemcpyHostToDevice, C.s));
+        LSG_CUDA(cudaMemcpyAsync(L.idx.p, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, C.s));
+        LSG_CUDA(cudaMemcpyAsync(L.desc.p, desc.data(), desc.size() * 8, cudaMemcpyHostToDevice, C.s));
+    }
+    L.partial.alloc(1024 * 6);
+    L.sums.alloc(8);
+    if (!L.counter.p) {
+        L.counter.alloc(1);
+        LSG_CUDA(cudaMemsetAsync(L.counter.p, 0, sizeof(unsigned int), C.s));
+    }
+    for (int c = 0; c < 3; c++) {
+        L.center[c] = center[c];
+        L.filt[c].init(dt);
+    }
+    L.fcoef = fcoef;
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    L.have = true;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+static void loads_run(Context& C, const double* ux, const double* uy, const double* uz, const double* p,
+                      const double* vib, const double* vib_yx, const double* vib_zy, const double* nu_cell,
+                      double nu, double* fx, double* fy, double* fz, lsg_loads_result* out)
+{
+    Context::Loads& L = C.loads;
+    memset(out, 0, sizeof(*out));
+    out->count = L.count;
+    if (L.count == 0) return;     // calculate() leaves everything untouched without cut cells
+    LoadsArgs a;
+    a.count = L.count;
+    a.N = L.N;
+    a.NM = L.N * L.M;
+    a.g = L.g.p;
+    a.idx = L.idx.p;
+    a.desc = L.desc.p;
+    a.ux = ux;
+    a.uy = uy;
+    a.uz = uz;
+    a.p = p;
+    a.vib = vib;
+    a.vyx = vib_yx;
+    a.vzy = vib_zy;
+    a.nu_cell = nu_cell;
+    a.nu = nu;
+    a.cx = L.center[0];
+    a.cy = L.center[1];
+    a.cz = L.center[2];
+    a.fx = fx;
+    a.fy = fy;
+    a.fz = fz;
+    a.partial = L.partial.p;
+    a.counter = L.counter.p;
+    a.sums = L.sums.p;
+    const int grid = grid_for(L.count, 256, 1024);
+    k_loads<<<grid, 256, 0, C.s>>>(a);
+    LSG_CHECK_LAUNCH();
+    double s[6];
+    LSG_CUDA(cudaMemcpyAsync(s, L.sums.p, sizeof(s), cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    for (int c = 0; c < 3; c++) {
+        out->force[c] = s[c];
+        out->coef[c] = s[c] * L.fcoef;
+        out->moment_raw[c] = s[3 + c];
+        out->moment[c] = L.filt[c].step(s[3 + c]);
+    }
+}
+
+int lsg_loads_calculate_device(lsg_ctx* h, const double* ux, const double* uy, const double* uz, const double* p,
+                               const double* vib, const double* vib_yx, const double* vib_zy,
+                               const double* nu_cell, double nu, double* forces, lsg_loads_result* out)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.loads.have, LSG_ERR_STATE, "no cut-cell list set (lsg_loads_set)");
+    LSG_REQUIRE(ux && uy && uz && p && vib && vib_yx && vib_zy && out, LSG_ERR_ARG, "null argument");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const int cnt = C.loads.count;
+    loads_run(C, ux, uy, uz, p, vib, vib_yx, vib_zy, nu_cell, nu, forces, forces ? forces + cnt : nullptr,
+              forces ? forces + 2 * (size_t)cnt : nullptr, out);
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_loads_calculate(lsg_ctx* h, const double* ux, const double* uy, const double* uz, const double* p,
+                        const double* vib, const double* vib_yx, const double* vib_zy, const double* nu_cell,
+                        double nu, double* forces, lsg_loads_result* out)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    Context::Loads& L = C.loads;
+    LSG_REQUIRE(L.have, LSG_ERR_STATE, "no cut-cell list set (lsg_loads_set)");
+    LSG_REQUIRE(ux && uy && uz && p && vib && vib_yx && vib_zy && out, LSG_ERR_ARG, "null argument");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const long long N = L.N, M = L.M, K = L.K, n = N * M * K;
+    const long long nx = (N - 1) * M * K, ny = N * (M - 1) * K, nz = N * M * (K - 1);
+    DevBuf<double> du, dv, dw, dp, dvib, dyx, dzy, dnu, df;
+    du.alloc(nx);
+    dv.alloc(ny);
+    dw.alloc(nz);
+    dp.alloc(n);
+    dvib.alloc(3 * n);
+    dyx.alloc(3 * n);
+    dzy.alloc(3 * n);
+    LSG_CUDA(cudaMemcpyAsync(du.p, ux, nx * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dv.p, uy, ny * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dw.p, uz, nz * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dp.p, p, n * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dvib.p, vib, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dyx.p, vib_yx, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dzy.p, vib_zy, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+    if (nu_cell) {
+        dnu.alloc(n);
+        LSG_CUDA(cudaMemcpyAsync(dnu.p, nu_cell, n * 8, cudaMemcpyHostToDevice, C.s));
+    }
+    const size_t cnt = (size_t)L.count;
+    if (forces && cnt) df.alloc(3 * cnt);
+    loads_run(C, du.p, dv.p, dw.p, dp.p, dvib.p, dyx.p, dzy.p, nu_cell ? dnu.p : nullptr, nu, df.p,
+              df.p ? df.p + cnt : nullptr, df.p ? df.p + 2 * cnt : nullptr, out);
+    if (forces && cnt) {
+        LSG_CUDA(cudaMemcpyAsync(forces, df.p, 3 * cnt * 8, cudaMemcpyDeviceToHost, C.s));
+        LSG_CUDA(cudaStreamSynchronize(C.s));
+    }
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_loads_reset_filter(lsg_ctx* h, double dt)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    LSG_REQUIRE(dt > 0, LSG_ERR_ARG, "time step must be positive");
+    for (int c = 0; c < 3; c++) h->c.loads.filt[c].init(dt);
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+static void loads_adjoint_run(Context& C, const double* w, const double* nu_cell, double nu, double* gux,
+                              double* guy, double* guz, double* gp)
+{
+    Context::Loads& L = C.loads;
+    const long long N = L.N, M = L.M, K = L.K, n = N * M * K;
+    LSG_CUDA(cudaMemsetAsync(gux, 0, (N - 1) * M * K * 8, C.s));
+    LSG_CUDA(cudaMemsetAsync(guy, 0, N * (M - 1) * K * 8, C.s));
+    LSG_CUDA(cudaMemsetAsync(guz, 0, N * M * (K - 1) * 8, C.s));
+    LSG_CUDA(cudaMemsetAsync(gp, 0, n * 8, C.s));
+    if (L.count == 0) return;
+    LoadsAdjArgs a;
+    a.count = L.count;
+    a.N = L.N;
+    a.NM = L.N * L.M;
+    a.g = L.g.p;
+    a.idx = L.idx.p;
+    a.desc = L.desc.p;
+    a.nu_cell = nu_cell;
+    a.nu = nu;
+    for (int c = 0; c < 3; c++) a.w[c] = w[c];
+    a.gux = gux;
+    a.guy = guy;
+    a.guz = guz;
+    a.gp = gp;
+    k_loads_adjoint<<<grid_for(L.count, 256, 1024), 256, 0, C.s>>>(a);
+    LSG_CHECK_LAUNCH();
+}
+
+int lsg_loads_adjoint_device(lsg_ctx* h, const double* weight, const double* nu_cell, double nu, double* g_ux,
+                             double* g_uy, double* g_uz, double* g_p)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.loads.have, LSG_ERR_STATE, "no cut-cell list set (lsg_loads_set)");
+    LSG_REQUIRE(weight && g_ux && g_uy && g_uz && g_p, LSG_ERR_ARG, "null argument");
+    LSG_CUDA(cudaSetDevice(C.device));
+    loads_adjoint_run(C, weight, nu_cell, nu, g_ux, g_uy, g_uz, g_p);
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_loads_adjoint(lsg_ctx* h, const double* weight, const double* nu_cell, double nu, double* g_ux,
+                      double* g_uy, double* g_uz, double* g_p)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    Context::Loads& L = C.loads;
+    LSG_REQUIRE(L.have, LSG_ERR_STATE, "no cut-cell list set (lsg_loads_set)");
+    LSG_REQUIRE(weight && g_ux && g_uy && g_uz && g_p, LSG_ERR_ARG, "null argument");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const long long N = L.N, M = L.M, K = L.K, n = N * M * K;
+    const long long nx = (N - 1) * M * K, ny = N * (M - 1) * K, nz = N * M * (K - 1);
+    DevBuf<double> gx, gy, gz, gpd, dnu;
+    gx.alloc(nx);
+    gy.alloc(ny);
+    gz.alloc(nz);
+    gpd.alloc(n);
+    if (nu_cell) {
+        dnu.alloc(n);
+        LSG_CUDA(cudaMemcpyAsync(dnu.p, nu_cell, n * 8, cudaMemcpyHostToDevice, C.s));
+    }
+    loads_adjoint_run(C, weight, nu_cell ? dnu.p : nullptr, nu, gx.p, gy.p, gz.p, gpd.p);
+    LSG_CUDA(cudaMemcpyAsync(g_ux, gx.p, nx * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaMemcpyAsync(g_uy, gy.p, ny * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaMemcpyAsync(g_uz, gz.p, nz * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaMemcpyAsync(g_p, gpd.p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
     return LSG_OK;
     LSG_API_END(h)
 }

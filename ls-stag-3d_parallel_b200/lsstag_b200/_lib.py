@@ -53,9 +53,18 @@ EXPORTS = [
     "lsg_set_staggered_types", "lsg_projection_rhs", "lsg_projection_rhs_device", "lsg_projection_correct",
     "lsg_projection_correct_device", "lsg_laplace_flux", "lsg_laplace_flux_device", "lsg_projection_adjoint",
     "lsg_momentum_rhs", "lsg_convective_apply", "lsg_convective_apply_device", "lsg_version",
+    "lsg_loads_set", "lsg_loads_calculate", "lsg_loads_calculate_device", "lsg_loads_reset_filter",
+    "lsg_loads_adjoint", "lsg_loads_adjoint_device",
 ]
 
 _lib = None
+
+
+class LoadsResult(C.Structure):
+    """lsg_loads_result: sums of the cut-cell forces, coefficients, raw and
+    filtered moments (M_z, M_x, M_y)."""
+    _fields_ = [("force", C.c_double * 3), ("coef", C.c_double * 3), ("moment_raw", C.c_double * 3),
+                ("moment", C.c_double * 3), ("count", C.c_int)]
 
 
 class LsgError(RuntimeError):
@@ -112,6 +121,14 @@ def load() -> C.CDLL:
     lib.lsg_projection_rhs_device.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.lsg_projection_correct.argtypes = [P, dp, dp, dp, dp, dp, dp, dp, dp, C.c_double, C.c_double, C.c_int]
     lib.lsg_projection_correct_device.argtypes = [P] + [C.c_void_p] * 8 + [C.c_double, C.c_double, C.c_int]
+    lib.lsg_loads_set.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip] + [dp] * 8 + [C.c_double,
+                                                                                             C.c_double]
+    lib.lsg_loads_calculate.argtypes = [P] + [dp] * 8 + [C.c_double, dp, C.POINTER(LoadsResult)]
+    lib.lsg_loads_calculate_device.argtypes = [P] + [C.c_void_p] * 8 + [C.c_double, C.c_void_p,
+                                                                        C.POINTER(LoadsResult)]
+    lib.lsg_loads_reset_filter.argtypes = [P, C.c_double]
+    lib.lsg_loads_adjoint.argtypes = [P, dp, dp, C.c_double, dp, dp, dp, dp]
+    lib.lsg_loads_adjoint_device.argtypes = [P, dp, C.c_void_p, C.c_double] + [C.c_void_p] * 4
     lib.lsg_version.restype = C.c_char_p
     _lib = lib
     return lib
