@@ -196,6 +196,27 @@ int lsg_convective_apply(lsg_ctx* ctx, int dir, const double* ux, const double* 
 int lsg_convective_apply_device(lsg_ctx* ctx, int dir, const double* ux, const double* uy, const double* uz,
                                 const double* v, const double* init, double* out, int zconv_reference);
 
+/* The momentum operator of direction dir (0 x, 1 y, 2 z) assembled on the
+   GPU from the cut-cell geometry and set as the context's operator (a 7-point
+   operator on the staggered grid of N-1 x M x K, N x M-1 x K or N x M x K-1
+   cells), replacing HelmholtzDiscreteOperatorX/Y/Z::build/calcElem
+   (DiscreteOperators/WithFlux/Sym/helmholtz_discrete_operator_x.h:98-686,
+   _y.h:92-…, _z.h:90-…) with the outflow terms of addPlusOutFlow
+   (helmholtz_discrete_operator_base.h:50-58).  stype are the staggered cell
+   types; theta, alpha, delta, delta_ib_en/ws/nb/st, inv_delta_ib_ne/tn (3n,
+   xyz interleaved) and inv_vof (n) describe the N x M x K base grid; vof are
+   the staggered cell volumes (the reference's M_x/M_y/M_z); nu the
+   viscosity, coef the time-integration coefficient (COEF_INTEGR_TIME, 1.5/dt
+   for BDF2); is_flow selects the flow-task boundary conditions (outflow on
+   E, slip T/B walls).  Entries agree with the reference to rounding (fluid
+   and cut-cell rows bitwise); read back with lsg_get_matrix_stencil7, solve
+   with lsg_setup (ILU(0) preconditioner) + lsg_solve.  Host pointers. */
+int lsg_set_matrix_helmholtz(lsg_ctx* ctx, int dir, int N, int M, int K, const int* stype, const double* theta,
+                             const double* alpha, const double* delta, const double* inv_vof, const double* vof,
+                             const double* delta_ib_en, const double* delta_ib_ws, const double* delta_ib_nb,
+                             const double* delta_ib_st, const double* inv_delta_ib_ne, const double* inv_delta_ib_tn,
+                             double nu, double coef, int is_flow);
+
 /* ---- loads on the immersed boundary (LoadsCalculator, loads_calculator.h) ---- */
 
 typedef struct lsg_loads_result {

@@ -1,0 +1,264 @@
+// Momentum (Helmholtz) operators assembled on the GPU from the cut-cell
+// geometry: K_d = -(coef) M_d + nu * (cut-cell Laplacian on the staggered
+// d-grid) with the box-boundary, immersed-boundary and outflow terms of
+// HelmholtzDiscreteOperatorX/Y/Z::calcHelm* (DiscreteOperators/WithFlux/Sym/
+// helmholtz_discrete_operator_x.h:98-686, _y.h:92-…, _z.h:90-…) and
+// addPlusOutFlow/setPlusOutFlow* (helmholtz_discrete_operator_base.h:50-58,
+// _x.h:732-737, _y.h:736-742, _z.h:726-732).
+//
+// The reference writes one formula block per cell type (fluid, solid, six
+// borders, twelve edges, eight corners, cut cells); here every row comes from
+// one face model of the staggered cell:
+//   * lateral face (direction l != d, lower or upper): coefficient
+//       nu dperp (theta_l(Q) da + theta_l(Q+up) da') alpha_r(Q) / (t_d dl + theta_d(nb) dl(nb)),
+//     Q the cell owning the face, nb the neighbour across it, r the third
+//     direction; for a fluid cell (dperp nu (da' + da)) / (dl + theta_d(nb) dl(nb));
+//   * axial face: nu t_d (dl1 dl2)^2 / V of the base cell on that side
+//     (nu (dl1 dl2)^2 / V for a fluid cell), entry scaled by the neighbour's
+//     theta_d;
+//   * cut cells (and some borders, below) drop a lateral face whose edge
+//     fraction alpha is below 1e-5 and add the immersed-boundary term of
+//     that direction pair instead.
+// The per-type differences of the reference are flags of that model:
+//   * a face on the box side is not an entry; on the outflow side (E) the
+//     coefficient stays in the diagonal, on the inflow side (W) it is dropped;
+//   * walls: lateral N/S walls of the x and z operators and T/B walls of the
+//     x and y operators (the latter only for tasks other than flows) add the
+//     upper lateral numerator at the cell over t_d dl; the N/S walls of the y
+//     operator keep the axial coefficient without the t_d factor, the T/B
+//     walls of the z operator (non-flow tasks) keep it with the factor;
+//   * T/B borders of all three operators gate their lateral faces like cut
+//     cells; the immersed-boundary terms they add follow the reference's
+//     conditions (x: T adds the z pair when alpha_y(P) or the b face is
+//     gated, B when the t face is; y: only the face it keeps; z: both pairs);
+//   * y-operator edges and corners with a T/B wall evaluate the wall term
+//     after the reference has overwritten dx by dx dz, and its TE/TW/BE/BW
+//     edges after dyy has become nu t_y (dx dz)^2 (values reproduced).
+// Fluid and cut-cell rows use the reference's operation order (bitwise); the
+// box-boundary rows agree to rounding (their diagonal sums are taken in the
+// cut-cell order).
+#pragma once
+
+#include "lsg_kernels.cuh"
+
+namespace lsg {
+
+struct HelmGeom {
+    int N, M, K;                   // base grid
+    int d;                         // 0 x, 1 y, 2 z operator
+    const int* stype;              // staggered cell types
+    const double* theta;           // 3n
+    const double* alpha;           // 3n
+    const double* delta;           // 3n
+    const double* inv_vof;         // n (base cells)
+    const double* vof;             // staggered cell volumes
+    const double* dib_en;          // 3n immersed-boundary distances
+    const double* dib_ws;
+    const double* dib_nb;
+    const double* dib_st;
+    const double* inv_dib_ne;      // 3n inverse distances
+    const double* inv_dib_tn;
+    double nu, coef;
+    int is_flow;
+    double* planes;                // 7 * ns: b s w p e n t
+};
+
+__device__ __forceinline__ double h_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double h_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double h_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double h_div(double a, double b) { return __ddiv_rn(a, b); }
+
+// immersed-boundary term of operator d for the lateral pair in direction l
+__device__ __forceinline__ double helm_ib(const HelmGeom& g, int l, long long P, long long up)
+{
+    const double* A;
+    const double* B;
+    const double* I;
+    int c, ci;
+    if (g.d == 0) {
+        A = g.dib_en; B = g.dib_ws; I = g.inv_dib_ne;
+        c = (l == 1) ? 1 : 0;
+        ci = (l == 1) ? 1 : 2;
+    } else if (g.d == 1) {
+        if (l == 0) { A = g.dib_en; B = g.dib_ws; I = g.inv_dib_ne; c = 2; ci = 0; }
+        else { A = g.dib_nb; B = g.dib_st; I = g.inv_dib_tn; c = 0; ci = 2; }
+    } else {
+        A = g.dib_st; B = g.dib_nb; I = g.inv_dib_tn;
+        c = (l == 0) ? 2 : 1;
+        ci = (l == 0) ? 0 : 1;
+    }
+    return h_mul(h_mul(g.nu, h_add(A[3 * P + c], B[3 * (P + up) + c])), I[3 * P + ci]);
+}
+
+__global__ void __launch_bounds__(256) k_helmholtz_from_geometry(HelmGeom g)
+{
+    const int d = g.d;
+    const int N = g.N, M = g.M;
+    const long long NM = (long long)N * M;
+    const int Ns = N - (d == 0), Ms = M - (d == 1), Ks = g.K - (d == 2);
+    const long long ns = (long long)Ns * Ms * Ks;
+    const long long step[3] = {1, N, NM};
+    const long long up = step[d];
+    const int l0 = d == 0 ? 1 : 0, l1 = d == 2 ? 1 : 2;      // lateral directions, lower first
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ns;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % Ns);
+        const long long rest = i / Ns;
+        const int y = (int)(rest % Ms), z = (int)(rest / Ms);
+        const long long P = x + (long long)N * (y + (long long)M * z);
+        const int t = g.stype[i];
+        double e[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (t == 0) {
+            e[3] = 1e-16;                                      // PLUS_TINY
+        } else {
+            const int miss = absent_faces(t);
+            // face bits of absent_faces by (axis, side)
+            auto bit = [](int ax, int side) {
+                return ax == 0 ? (side < 0 ? 4 : 8) : (ax == 1 ? (side < 0 ? 2 : 16) : (side < 0 ? 1 : 32));
+            };
+            const bool fluid = (t == 11111111);
+            const bool cut = t > 0 && !fluid;
+            const bool tb_border = (t == -2 || t == -3);
+            const bool gating = cut || tb_border;
+            const double* th = g.theta;
+            const double* de = g.delta;
+            const double* al = g.alpha;
+            const double ta = th[3 * P + d];
+            const double da = de[3 * P + d], da2 = de[3 * (P + up) + d];
+            double kl[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+            bool gated[3][2] = {{false, false}, {false, false}, {false, false}};
+            for (int q = 0; q < 2; q++) {
+                const int l = q == 0 ? l0 : l1;
+                const int r = 3 - d - l;
+                const long long sl = step[l];
+                const double dperp = de[3 * P + r];
+                for (int s = 0; s < 2; s++) {
+                    const int side = s == 0 ? -1 : 1;
+                    const bool on_box = (miss & bit(l, side)) != 0;
+                    // the outflow face (E) stays in the diagonal of the y and z operators
+                    if (on_box && !(l == 0 && side > 0)) continue;
+                    const long long Q = side < 0 ? P - sl : P;
+                    const long long nb = side < 0 ? P - sl : P + sl;
+                    const double den_n = h_mul(th[3 * nb + d], de[3 * nb + l]);
+                    if (fluid) {
+                        const double aux = h_mul(dperp, h_mul(g.nu, h_add(da2, da)));
+                        kl[l][s] = h_div(aux, h_add(de[3 * P + l], den_n));
+                    } else {
+                        const double a = al[3 * Q + r];
+                        if (gating && a < 1e-5) {
+                            gated[l][s] = true;
+                            continue;
+                        }
+                        const double aux = h_mul(dperp, g.nu);
+                        const double num =
+                            h_mul(h_mul(aux, h_add(h_mul(th[3 * Q + l], da), h_mul(th[3 * (Q + up) + l], da2))), a);
+                        kl[l][s] = h_div(num, h_add(h_mul(ta, de[3 * P + l]), den_n));
+                    }
+                }
+            }
+            // axial coefficients
+            const double A = h_mul(de[3 * P + l0], de[3 * P + l1]);
+            const double f0 = fluid ? h_mul(h_mul(g.nu, A), A) : h_mul(h_mul(h_mul(g.nu, ta), A), A);
+            const double kax_lo = h_mul(f0, g.inv_vof[P]);
+            const double kax_hi = h_mul(f0, g.inv_vof[P + up]);
+            // immersed-boundary terms
+            double ib = 0.0;
+            const bool ib_l0 = gated[l0][0] || gated[l0][1];
+            // the x operator's T border also adds the z pair when alpha_y of the cell is below 1e-5
+            const bool ib_l1 = gated[l1][0] || gated[l1][1] || (d == 0 && t == -2 && al[3 * P + 1] < 1e-5);
+            if (ib_l0) ib = helm_ib(g, l0, P, up);
+            if (ib_l1) ib = h_add(ib, helm_ib(g, l1, P, up));
+            // entries
+            const bool lo_box = (miss & bit(d, -1)) != 0, hi_box = (miss & bit(d, 1)) != 0;
+            if (!lo_box) e[d == 0 ? 2 : (d == 1 ? 1 : 0)] = h_mul(kax_lo, th[3 * (P - up) + d]);
+            if (!hi_box) e[d == 0 ? 4 : (d == 1 ? 5 : 6)] = h_mul(kax_hi, th[3 * (P + up) + d]);
+            const int slot_lo[3] = {2, 1, 0}, slot_hi[3] = {4, 5, 6};
+            for (int q = 0; q < 2; q++) {
+                const int l = q == 0 ? l0 : l1;
+                if (!(miss & bit(l, -1))) e[slot_lo[l]] = kl[l][0];
+                if (!(miss & bit(l, 1))) e[slot_hi[l]] = kl[l][1];
+            }
+            // diagonal
+            double dg = -h_mul(g.coef, g.vof[i]);
+            if (fluid) {
+                // CSR order b s w e n t (the reference's fluid rows)
+                const double kk[6] = {d == 2 ? kax_lo : kl[2][0], d == 1 ? kax_lo : kl[1][0],
+                                      d == 0 ? kax_lo : kl[0][0], d == 0 ? kax_hi : kl[0][1],
+                                      d == 1 ? kax_hi : kl[1][1], d == 2 ? kax_hi : kl[2][1]};
+                const int fb[6] = {1, 2, 4, 8, 16, 32};
+                for (int f = 0; f < 6; f++)
+                    if (!(miss & fb[f])) dg = h_sub(dg, kk[f]);
+            } else {
+                // lateral lower faces, the axial pair, lateral upper faces, then
+                // walls and immersed-boundary terms (the reference's cut-cell order)
+                dg = h_sub(dg, kl[l1][0]);
+                dg = h_sub(dg, kl[l0][0]);
+                double ax = 0.0;
+                bool any_ax = false;
+                double ax_plain = 0.0;
+                for (int s = 0; s < 2; s++) {
+                    const int side = s == 0 ? -1 : 1;
+                    const double kv = s == 0 ? kax_lo : kax_hi;
+                    if (!(miss & bit(d, side))) {
+                        ax = any_ax ? h_add(ax, kv) : kv;
+                        any_ax = true;
+                    } else if (d == 0 && side > 0) {
+                        ax = any_ax ? h_add(ax, kv) : kv;         // outflow face of the x operator
+                        any_ax = true;
+                    } else if (d == 1) {
+                        ax_plain = h_add(ax_plain, kv);            // y: N/S wall keeps the coefficient
+                    } else if (d == 2 && !g.is_flow) {
+                        ax = any_ax ? h_add(ax, kv) : kv;          // z: T/B wall of a non-flow task
+                        any_ax = true;
+                    }
+                }
+                if (any_ax) dg = h_sub(dg, h_mul(ax, ta));
+                dg = h_sub(dg, kl[l0][1]);
+                dg = h_sub(dg, kl[l1][1]);
+                dg = h_sub(dg, ax_plain);
+                // lateral walls
+                for (int q = 0; q < 2; q++) {
+                    const int l = q == 0 ? l0 : l1;
+                    const int r = 3 - d - l;
+                    for (int s = 0; s < 2; s++) {
+                        const int side = s == 0 ? -1 : 1;
+                        if (!(miss & bit(l, side))) continue;
+                        const bool ns_wall = (l == 1) && (d == 0 || d == 2);
+                        const bool tb_wall = (l == 2) && (d == 0 || d == 1) && !g.is_flow;
+                        if (!ns_wall && !tb_wall) continue;
+                        const bool checked = !(d == 2 && (t == -4 || t == -5));
+                        if (checked && !(ta > 1e-5)) continue;
+                        double dr = de[3 * P + r];
+                        double d2 = da2;
+                        if (d == 1 && l == 2 && t <= -8) {
+                            dr = h_mul(dr, de[3 * P + 2]);
+                            if (t == -10 || t == -11 || t == -14 || t == -15) d2 = h_mul(h_mul(h_mul(g.nu, ta), dr), dr);
+                        }
+                        const double num = h_mul(h_mul(h_mul(dr, g.nu),
+                                                       h_add(h_mul(th[3 * P + l], da), h_mul(th[3 * (P + up) + l], d2))),
+                                                 al[3 * P + r]);
+                        dg = h_sub(dg, h_div(num, h_mul(ta, de[3 * P + l])));
+                    }
+                }
+                dg = h_sub(dg, ib);
+            }
+            if (g.is_flow && (miss & 8)) {
+                // convective outflow on the last cell of each row
+                double po;
+                if (d == 0) {
+                    const long long Pb = P + 1;
+                    po = h_div(h_mul(h_mul(g.nu, de[3 * Pb + 1]), de[3 * Pb + 2]), de[3 * Pb]);
+                } else if (d == 1) {
+                    po = h_div(h_mul(h_mul(g.nu, h_add(de[3 * P + 1], de[3 * (P + N) + 1])), de[3 * P + 2]), de[3 * P]);
+                } else {
+                    po = h_div(h_mul(h_mul(g.nu, h_add(de[3 * P + 2], de[3 * (P + NM) + 2])), de[3 * P + 1]), de[3 * P]);
+                }
+                dg = h_add(dg, po);
+            }
+            e[3] = dg;
+        }
+        for (int f = 0; f < 7; f++) g.planes[(size_t)f * ns + i] = e[f];
+    }
+}
+
+}  // namespace lsg

@@ -13,6 +13,7 @@
 #include "lsg_coarse.cuh"
 #include "lsg_ilu.cuh"
 #include "lsg_krylov.cuh"
+#include "lsg_helmholtz.cuh"
 #include "lsg_loads.cuh"
 #include "lsg_projection.cuh"
 
@@ -1717,6 +1718,83 @@ int lsg_set_matrix_geometry(lsg_ctx* h, int N, int M, int K, const int* celltype
         C.adj.reset();
     }
     g.have = true;
+    C.have_matrix = true;
+    C.have_setup = false;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_set_matrix_helmholtz(lsg_ctx* h, int dir, int N, int M, int K, const int* stype, const double* theta,
+                             const double* alpha, const double* delta, const double* inv_vof, const double* vof,
+                             const double* delta_ib_en, const double* delta_ib_ws, const double* delta_ib_nb,
+                             const double* delta_ib_st, const double* inv_delta_ib_ne, const double* inv_delta_ib_tn,
+                             double nu, double coef, int is_flow)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z)");
+    LSG_REQUIRE(N >= 3 && M >= 3 && K >= 3, LSG_ERR_ARG, "grid must be at least 3 cells in every direction");
+    LSG_REQUIRE(stype && theta && alpha && delta && inv_vof && vof && delta_ib_en && delta_ib_ws && delta_ib_nb &&
+                    delta_ib_st && inv_delta_ib_ne && inv_delta_ib_tn,
+                LSG_ERR_ARG, "null geometry array");
+    const long long n = (long long)N * M * K;
+    LSG_REQUIRE(n < (1LL << 31), LSG_ERR_ARG, "grid too large");
+    const int Ns = N - (dir == 0), Ms = M - (dir == 1), Ks = K - (dir == 2);
+    const long long ns = (long long)Ns * Ms * Ks;
+    // a face kept by a staggered cell's type must lie inside the staggered grid
+    check_cell_types(Ns, Ms, Ks, stype);
+    C.geo.have = C.geo.have_stypes = false;    // geometry of an earlier operator no longer applies
+    LSG_CUDA(cudaSetDevice(C.device));
+    DevBuf<int> dt;
+    DevBuf<double> dth, dal, dde, dinv, dvof, den, dws, dnb, dst, dne, dtn;
+    dt.alloc(ns);
+    LSG_CUDA(cudaMemcpyAsync(dt.p, stype, ns * sizeof(int), cudaMemcpyHostToDevice, C.s));
+    const double* src3[9] = {theta, alpha, delta, delta_ib_en, delta_ib_ws, delta_ib_nb, delta_ib_st,
+                             inv_delta_ib_ne, inv_delta_ib_tn};
+    DevBuf<double>* dst3[9] = {&dth, &dal, &dde, &den, &dws, &dnb, &dst, &dne, &dtn};
+    for (int a = 0; a < 9; a++) {
+        dst3[a]->alloc(3 * n);
+        LSG_CUDA(cudaMemcpyAsync(dst3[a]->p, src3[a], 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+    }
+    dinv.alloc(n);
+    dvof.alloc(ns);
+    LSG_CUDA(cudaMemcpyAsync(dinv.p, inv_vof, n * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dvof.p, vof, ns * 8, cudaMemcpyHostToDevice, C.s));
+    C.d.N = Ns;
+    C.d.M = Ms;
+    C.d.K = Ks;
+    C.n = ns;
+    C.A7.alloc(7 * ns);
+    HelmGeom g;
+    g.N = N;
+    g.M = M;
+    g.K = K;
+    g.d = dir;
+    g.stype = dt.p;
+    g.theta = dth.p;
+    g.alpha = dal.p;
+    g.delta = dde.p;
+    g.inv_vof = dinv.p;
+    g.vof = dvof.p;
+    g.dib_en = den.p;
+    g.dib_ws = dws.p;
+    g.dib_nb = dnb.p;
+    g.dib_st = dst.p;
+    g.inv_dib_ne = dne.p;
+    g.inv_dib_tn = dtn.p;
+    g.nu = nu;
+    g.coef = coef;
+    g.is_flow = is_flow ? 1 : 0;
+    g.planes = C.A7.p;
+    k_helmholtz_from_geometry<<<grid_for(ns, 256), 256, 0, C.s>>>(g);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    C.nclass0 = build_dict(C.s, C.A7.p, 7, ns, C.cls0, C.dict0);
+    if (C.adj) {
+        context_release(*C.adj);
+        C.adj.reset();
+    }
     C.have_matrix = true;
     C.have_setup = false;
     return LSG_OK;

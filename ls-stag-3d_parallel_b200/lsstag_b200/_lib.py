@@ -54,7 +54,7 @@ EXPORTS = [
     "lsg_projection_correct_device", "lsg_laplace_flux", "lsg_laplace_flux_device", "lsg_projection_adjoint",
     "lsg_momentum_rhs", "lsg_convective_apply", "lsg_convective_apply_device", "lsg_version",
     "lsg_loads_set", "lsg_loads_calculate", "lsg_loads_calculate_device", "lsg_loads_reset_filter",
-    "lsg_loads_adjoint", "lsg_loads_adjoint_device",
+    "lsg_loads_adjoint", "lsg_loads_adjoint_device", "lsg_set_matrix_helmholtz",
 ]
 
 _lib = None
@@ -121,6 +121,8 @@ def load() -> C.CDLL:
     lib.lsg_projection_rhs_device.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.lsg_projection_correct.argtypes = [P, dp, dp, dp, dp, dp, dp, dp, dp, C.c_double, C.c_double, C.c_int]
     lib.lsg_projection_correct_device.argtypes = [P] + [C.c_void_p] * 8 + [C.c_double, C.c_double, C.c_int]
+    lib.lsg_set_matrix_helmholtz.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, ip] + [dp] * 11 + [
+        C.c_double, C.c_double, C.c_int]
     lib.lsg_loads_set.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip] + [dp] * 8 + [C.c_double,
                                                                                              C.c_double]
     lib.lsg_loads_calculate.argtypes = [P] + [dp] * 8 + [C.c_double, dp, C.POINTER(LoadsResult)]

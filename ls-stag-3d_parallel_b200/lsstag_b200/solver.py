@@ -105,6 +105,29 @@ class IterativeSolver:
         if setup:
             self._setup()
 
+    def set_helmholtz(self, direction: int, geom: dict, base_dims, nu: float, coef: float, is_flow: bool = True,
+                      task: Task | None = None, setup: bool = True):
+        """The momentum operator of one direction (HelmholtzDiscreteOperator
+        X/Y/Z) assembled on the GPU from the geometry and set as this
+        solver's operator.  geom holds stype (the staggered cell types),
+        theta, alpha, delta, inv_vof, vof (staggered volumes), dib_en,
+        dib_ws, dib_nb, dib_st, inv_dib_ne, inv_dib_tn; base_dims = (N, M, K)."""
+        self.task = task or Task()
+        self.eps = float(self.task.eps)
+        keys = ("theta", "alpha", "delta", "inv_vof", "vof", "dib_en", "dib_ws", "dib_nb", "dib_st", "inv_dib_ne",
+                "inv_dib_tn")
+        g = {k: np.ascontiguousarray(geom[k], dtype=np.float64).reshape(-1) for k in keys}
+        st = np.ascontiguousarray(geom["stype"], dtype=np.int32)
+        self._helm = (g, st)
+        N, M, K = (int(v) for v in base_dims)
+        d = int(direction)
+        self.dims = (N - (d == 0), M - (d == 1), K - (d == 2))
+        self.ctx.check(self.ctx.lib.lsg_set_matrix_helmholtz(self.ctx.h, d, N, M, K, L.iptr(st),
+                                                             *(L.dptr(g[k]) for k in keys), float(nu), float(coef),
+                                                             int(bool(is_flow))))
+        if setup:
+            self._setup()
+
     # -- pressure projection (needs set_geometry) -----------------------------
     def set_staggered_types(self, xtype, ytype, ztype):
         self._stypes = tuple(np.ascontiguousarray(t, dtype=np.int32) for t in (xtype, ytype, ztype))

@@ -29,6 +29,7 @@
 #include <chrono>
 #include <fstream>
 #include <map>
+#include <random>
 #include <sstream>
 #include <vector>
 
@@ -444,6 +445,85 @@ int main(int argc, char** argv)
         for (long i = 0; i < nb; i++)
             mm->v_ib[i].set(0.1 * sin(0.11 * i), 0.1 * cos(0.13 * i), 0.05 * sin(0.17 * i));
         for (long i = 0; i < (long)mm->xMesh.NMK; i++) mm->m_Ux[i] = 1.0 + 0.2 * sin(0.29 * i);
+    }
+    if ((int)cfg.get("helm", 0)) {
+        // the momentum operators as the time step builds them
+        // (HelmholtzDiscreteOperatorX/Y/Z::init -> build: calcFlux, calcHelm*,
+        // the outflow terms), optionally on seeded geometry arrays: face and
+        // edge fractions (some alpha exactly 0, so that the immersed-boundary
+        // branches run on every cell type), cell volumes and the
+        // immersed-boundary distances are replaced, the cell types are kept
+        LSSTAGUniformMesh* mm = task->m_mesh;
+        const int N = mm->baseMesh.N, M = mm->baseMesh.M, K = mm->baseMesh.K;
+        const long n = (long)N * M * K;
+        const long ns[3] = {(long)mm->xMesh.NMK, (long)mm->yMesh.NMK, (long)mm->zMesh.NMK};
+        if ((int)cfg.get("helm_random", 0)) {
+            std::mt19937_64 rng((unsigned long long)cfg.get("seed", 1));
+            std::uniform_real_distribution<double> U(0.0, 1.0);
+            auto frac = [&](double pz, double p1) {
+                const double r = U(rng);
+                if (r < pz) return 0.0;
+                if (r < pz + p1) return 1.0;
+                return 0.05 + 0.95 * U(rng);
+            };
+            for (long i = 0; i < n; i++) {
+                mm->theta[i].set(frac(0.0, 0.2), frac(0.0, 0.2), frac(0.0, 0.2));
+                mm->alpha[i].set(frac(0.15, 0.2), frac(0.15, 0.2), frac(0.15, 0.2));
+                mm->baseMesh.inv_VOF[i] = 0.5 + 1.5 * U(rng);
+                coordinate* arr[6] = {mm->delta_ib_en, mm->delta_ib_ws, mm->delta_ib_nb, mm->delta_ib_st,
+                                      mm->inv_delta_ib_ne, mm->inv_delta_ib_tn};
+                for (int a = 0; a < 6; a++) arr[a][i].set(0.1 + U(rng), 0.1 + U(rng), 0.1 + U(rng));
+            }
+            double* vofs[3] = {mm->xMesh.VOF, mm->yMesh.VOF, mm->zMesh.VOF};
+            for (int d = 0; d < 3; d++)
+                for (long i = 0; i < ns[d]; i++) vofs[d][i] = 0.2 + 0.8 * U(rng);
+        }
+        // the operators of a task that is not a flow (no outflow terms, walls on T/B)
+        if ((int)cfg.get("helm_noflow", 0)) task->id = BaseTaskDescription::TASK_UNKNOWN;
+        HelmholtzDiscreteOperatorX* kx = new HelmholtzDiscreteOperatorX;   // not destroyed (see below)
+        HelmholtzDiscreteOperatorY* ky = new HelmholtzDiscreteOperatorY;
+        HelmholtzDiscreteOperatorZ* kz = new HelmholtzDiscreteOperatorZ;
+        kx->init(task, &mm->xMesh);
+        ky->init(task, &mm->yMesh);
+        kz->init(task, &mm->zMesh);
+        int dd[3] = {N, M, K};
+        out.i("dims", dd, 3);
+        out.csr("Kx", (SparseMatrix*)kx);
+        out.csr("Ky", (SparseMatrix*)ky);
+        out.csr("Kz", (SparseMatrix*)kz);
+        out.d("hflux_x", kx->flux, ns[0]);
+        out.d("hflux_y", ky->flux, ns[1]);
+        out.d("hflux_z", kz->flux, ns[2]);
+        out.i("xtype", (const int*)mm->xMesh.typeOfCell, ns[0]);
+        out.i("ytype", (const int*)mm->yMesh.typeOfCell, ns[1]);
+        out.i("ztype", (const int*)mm->zMesh.typeOfCell, ns[2]);
+        out.i("celltype", (const int*)mm->baseMesh.typeOfCell, n);
+        out.i("side_type", (const int*)mm->baseSideTypes, 3 * n);
+        out.d("theta", (const double*)mm->theta, 3 * n);
+        out.d("alpha", (const double*)mm->alpha, 3 * n);
+        out.d("delta", (const double*)mm->delta, 3 * n);
+        out.d("inv_vof", mm->baseMesh.inv_VOF, n);
+        out.d("vof_x", mm->xMesh.VOF, ns[0]);
+        out.d("vof_y", mm->yMesh.VOF, ns[1]);
+        out.d("vof_z", mm->zMesh.VOF, ns[2]);
+        out.d("dib_en", (const double*)mm->delta_ib_en, 3 * n);
+        out.d("dib_ws", (const double*)mm->delta_ib_ws, 3 * n);
+        out.d("dib_nb", (const double*)mm->delta_ib_nb, 3 * n);
+        out.d("dib_st", (const double*)mm->delta_ib_st, 3 * n);
+        out.d("inv_dib_ne", (const double*)mm->inv_delta_ib_ne, 3 * n);
+        out.d("inv_dib_tn", (const double*)mm->inv_delta_ib_tn, 3 * n);
+        out.d("vib", (const double*)mm->v_ib, 3 * n);
+        out.d("vibyx", (const double*)mm->v_ib_yx, 3 * n);
+        out.d("vibzy", (const double*)mm->v_ib_zy, 3 * n);
+        out.d("u_w", task->pU_W, (long)M * K);
+        double par[4] = {task->nu, task->COEF_INTEGR_TIME, (double)(task->id == BaseTaskDescription::TASK_FLOW), task->t};
+        out.d("nu_coef_isflow_dt", par, 4);
+        // U_W U_E U_S U_N U_B U_T, V_W V_E V_S V_N V_B V_T, W_W W_E W_S W_N W_B W_T
+        double bc[18] = {task->U_W, task->U_E, task->U_S, task->U_N, task->U_B, task->U_T,
+                         task->V_W, task->V_E, task->V_S, task->V_N, task->V_B, task->V_T,
+                         task->W_W, task->W_E, task->W_S, task->W_N, task->W_B, task->W_T};
+        out.d("bc", bc, 18);
+        return 0;
     }
     if ((int)cfg.get("loads", 0)) {
         // LoadsCalculator::calculate (loads_calculator.h:1366-1377) over the
