@@ -217,6 +217,24 @@ int lsg_set_matrix_helmholtz(lsg_ctx* ctx, int dir, int N, int M, int K, const i
                              const double* delta_ib_st, const double* inv_delta_ib_ne, const double* inv_delta_ib_tn,
                              double nu, double coef, int is_flow);
 
+/* Source term of the momentum operator of direction dir as build() leaves
+   it (HelmholtzDiscreteOperatorX/Y/Z::initInFlowFlux: inFlowFluxHelm*,
+   addFluxNS*, addFluxTB*; helmholtz_discrete_operator_x.h:50-96, :750-758,
+   _y.h, _z.h): the inflow value on the x = 0 cells, then the S/N and B/T wall
+   terms.  bc = (U_W U_E U_S U_N U_B U_T, V_W V_E V_S V_N V_B V_T, W_W W_E
+   W_S W_N W_B W_T), u_w the x-inflow profile (M*K, the reference's pU_W).
+   With ib != 0 the immersed-boundary term (ibFluxHelmX/Y/Z, :687-731, run by
+   the reference for moving bodies) is written over rows 1 .. Ms-2 as the
+   reference does; the arrays after `ib` are then required (NULL allowed
+   otherwise).  Bitwise equal to the reference.  Host pointers; flux holds
+   the staggered grid's cells. */
+int lsg_helmholtz_flux(lsg_ctx* ctx, int dir, int N, int M, int K, const int* stype, const double* delta,
+                       const double* u_w, const double* bc, double nu, int ib, const int* side_type,
+                       const double* theta, const double* alpha, const double* inv_vof, const double* delta_ib_en,
+                       const double* delta_ib_ws, const double* delta_ib_nb, const double* delta_ib_st,
+                       const double* inv_delta_ib_ne, const double* inv_delta_ib_tn, const double* vib,
+                       const double* vib_yx, const double* vib_zy, double* flux);
+
 /* ---- loads on the immersed boundary (LoadsCalculator, loads_calculator.h) ---- */
 
 typedef struct lsg_loads_result {

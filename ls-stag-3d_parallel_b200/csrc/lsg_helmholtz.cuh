@@ -262,3 +262,155 @@ __global__ void __launch_bounds__(256) k_helmholtz_from_geometry(HelmGeom g)
 }
 
 }  // namespace lsg
+
+namespace lsg {
+
+// Source term of the momentum operator of direction d as build() leaves it
+// (initInFlowFlux: inFlowFluxHelm*, addFluxNS*, addFluxTB*,
+// helmholtz_discrete_operator_x.h:50-96 and :750-758, _y.h, _z.h), one thread
+// per staggered cell: the inflow value on x = 0 is assigned, then the S/N
+// wall terms and the B/T wall terms (non-solid cells) are added, in that
+// order.  The T/B terms are present for flow tasks too (the reference builds
+// them before it marks the operator as having an outflow).  The reference's
+// index choices are kept: the N-row terms use the S row's dx and dz, the x
+// operator's N coefficient reads dy at base index (N-1)(M-1)+zNM, the y
+// operator's T coefficient reads dz at base (y, y, K-1).
+// With ib != 0 the immersed-boundary term (ibFluxHelmX/Y/Z, :687-731) is then
+// written over rows 1 .. Ms-2: cut cells, and T/B borders with a cut face,
+// get it; every other cell of those rows gets 0.
+struct HelmFluxArgs {
+    HelmGeom g;
+    const int* side_type;         // 3n (ib only)
+    const double* vib;            // 3n (ib only)
+    const double* vyx;
+    const double* vzy;
+    const double* u_w;            // x-inflow profile, M*K
+    double bc[18];                // U_W U_E U_S U_N U_B U_T, V_*, W_*
+    int ib;
+    double* flux;
+};
+
+__device__ __forceinline__ bool helm_cut_face(const int* sd, long long P)
+{
+    const int a = sd[3 * P], b = sd[3 * P + 1], c = sd[3 * P + 2];
+    return (a > 0 && a < 1111) || (b > 0 && b < 1111) || (c > 0 && c < 1111);
+}
+
+__global__ void __launch_bounds__(256) k_helmholtz_flux(HelmFluxArgs a)
+{
+    const HelmGeom& g = a.g;
+    const int d = g.d;
+    const int N = g.N, M = g.M, K = g.K;
+    const long long NM = (long long)N * M;
+    const int Ns = N - (d == 0), Ms = M - (d == 1), Ks = K - (d == 2);
+    const long long nsm = (long long)Ns * Ms, ns = nsm * Ks;
+    const double* de = g.delta;
+    const double nu = g.nu;
+    const double S_ = a.bc[6 * d + 2], N_ = a.bc[6 * d + 3], B_ = a.bc[6 * d + 4], T_ = a.bc[6 * d + 5];
+    const double W_ = a.bc[6 * d];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ns;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % Ns);
+        const long long rest = i / Ns;
+        const int y = (int)(rest % Ms), z = (int)(rest / Ms);
+        const long long P = x + (long long)N * (y + (long long)M * z);
+        const int t = g.stype[i];
+        double f = 0.0;
+        if (x == 0) {
+            if (d == 0)
+                f = h_div(h_mul(a.u_w[y + (long long)z * M], h_mul(h_mul(nu, de[3 * P + 2]), de[3 * P + 1])), de[3 * P]);
+            else if (d == 1)
+                f = h_div(h_mul(W_, h_mul(h_mul(nu, de[3 * P + 2]), h_add(de[3 * P + 1], de[3 * (P + N) + 1]))),
+                          de[3 * P]);
+            else
+                f = h_div(h_mul(W_, h_mul(h_mul(nu, de[3 * P + 1]), h_add(de[3 * P + 2], de[3 * (P + NM) + 2]))),
+                          de[3 * P]);
+        }
+        if (y == 0 || y == Ms - 1) {
+            const long long b0 = (long long)z * NM;
+            const bool north = (y == Ms - 1);
+            double coef;
+            if (d == 0) {
+                const long long q = north ? (nsm * z + nsm - Ns) + (long long)z * M : b0;
+                coef = h_div(h_mul(h_mul(nu, north ? N_ : S_), de[3 * b0 + 2]), de[3 * q + 1]);
+            } else if (d == 1) {
+                const long long q = north ? b0 + (long long)N * (M - 2) : b0;
+                coef = h_div(h_mul(h_mul(nu, north ? N_ : S_), de[3 * b0 + 2]), de[3 * q + 1]);
+            } else {
+                const double dzz = h_add(de[3 * b0 + 2], de[3 * (b0 + NM) + 2]);
+                const long long q = north ? b0 + NM - N : b0;
+                coef = h_div(h_mul(h_mul(nu, north ? N_ : S_), dzz), de[3 * q + 1]);
+            }
+            const double c = d == 0 ? h_add(de[3 * (b0 + x)], de[3 * (b0 + x + 1)]) : de[3 * (b0 + x)];
+            f = h_add(f, h_mul(c, coef));
+        }
+        if ((z == 0 || z == Ks - 1) && t != 0) {
+            const long long b0 = (long long)N * y;
+            const bool top = (z == Ks - 1);
+            double coef;
+            if (d == 0) {
+                coef = h_div(h_mul(h_mul(nu, top ? T_ : B_), de[3 * b0 + 1]),
+                             de[3 * (top ? b0 + (long long)(K - 1) * NM : b0) + 2]);
+            } else if (d == 1) {
+                const double dyy = h_add(de[3 * b0 + 1], de[3 * (b0 + N) + 1]);
+                const long long numT = (long long)(Ks - 1) * nsm + (long long)y * Ns;
+                coef = h_div(h_mul(h_mul(nu, top ? T_ : B_), dyy),
+                             de[3 * (top ? numT + y + (long long)(K - 1) * N : b0) + 2]);
+            } else {
+                coef = h_div(h_mul(h_mul(nu, top ? T_ : B_), de[3 * b0 + 1]),
+                             de[3 * (top ? b0 + (long long)(K - 2) * NM : b0) + 2]);
+            }
+            const double c = d == 0 ? h_add(de[3 * (b0 + x)], de[3 * (b0 + x + 1)]) : de[3 * (b0 + x)];
+            f = h_add(f, h_mul(c, coef));
+        }
+        if (a.ib && y >= 1 && y <= Ms - 2) {
+            const long long up = d == 0 ? 1 : (d == 1 ? N : NM);
+            bool cut = t > 0 && t < 11111111;
+            if (t == -2 || t == -3) cut = helm_cut_face(a.side_type, P) || (d != 2 && helm_cut_face(a.side_type, P + up));
+            const double* th = g.theta;
+            const double* al = g.alpha;
+            const double ta = th[3 * P + d];
+            if (!cut || ta < 1e-5) {
+                f = 0.0;
+            } else {
+                const long long bnum = z ? NM : 0;
+                double a2, ib = 0.0, lo;
+                if (d == 0) {
+                    a2 = h_mul(de[3 * P + 1], de[3 * P + 2]);
+                    if (al[3 * P + 2] < 1e-5 || al[3 * (P - N) + 2] < 1e-5)
+                        ib = h_mul(h_mul(h_add(g.dib_en[3 * P + 1], g.dib_ws[3 * (P + 1) + 1]), g.inv_dib_ne[3 * P + 1]),
+                                   a.vyx[3 * P]);
+                    if (al[3 * P + 1] < 1e-5 || al[3 * (P - bnum) + 1] < 1e-5)
+                        ib = h_add(ib, h_mul(h_mul(h_add(g.dib_en[3 * P], g.dib_ws[3 * (P + 1)]), g.inv_dib_ne[3 * P + 2]),
+                                             a.vzy[3 * P]));
+                    lo = th[3 * (P - 1)];
+                } else if (d == 1) {
+                    a2 = h_mul(de[3 * P], de[3 * P + 2]);
+                    if (al[3 * P + 2] < 1e-5 || al[3 * (P - 1) + 2] < 1e-5)
+                        ib = h_mul(h_mul(h_add(g.dib_en[3 * P + 2], g.dib_ws[3 * (P + N) + 2]), g.inv_dib_ne[3 * P]),
+                                   a.vyx[3 * P + 1]);
+                    if (al[3 * P] < 1e-5 || al[3 * (P - bnum)] < 1e-5)
+                        ib = h_add(ib, h_mul(h_mul(h_add(g.dib_nb[3 * P], g.dib_st[3 * (P + N)]), g.inv_dib_tn[3 * P + 2]),
+                                             a.vzy[3 * P + 1]));
+                    lo = th[3 * (P - N) + 1];
+                } else {
+                    a2 = h_mul(de[3 * P], de[3 * P + 1]);
+                    if (al[3 * P + 1] < 1e-5 || al[3 * (P - 1) + 1] < 1e-5)
+                        ib = h_mul(h_mul(h_add(g.dib_st[3 * P + 2], g.dib_nb[3 * (P + NM) + 2]), g.inv_dib_tn[3 * P]),
+                                   a.vyx[3 * P + 2]);
+                    if (al[3 * P] < 1e-5 || al[3 * (P - N)] < 1e-5)
+                        ib = h_add(ib, h_mul(h_mul(h_add(g.dib_st[3 * P + 1], g.dib_nb[3 * (P + NM) + 1]),
+                                                   g.inv_dib_tn[3 * P + 1]),
+                                             a.vzy[3 * P + 2]));
+                    lo = th[3 * (P - bnum) + 2];
+                }
+                const double hi_t = h_mul(h_mul(h_sub(ta, th[3 * (P + up) + d]), a.vib[3 * (P + up) + d]), g.inv_vof[P + up]);
+                const double lo_t = h_mul(h_mul(h_sub(lo, ta), a.vib[3 * P + d]), g.inv_vof[P]);
+                f = h_mul(nu, h_add(ib, h_mul(h_mul(h_mul(ta, a2), a2), h_sub(hi_t, lo_t))));
+            }
+        }
+        a.flux[i] = f;
+    }
+}
+
+}  // namespace lsg

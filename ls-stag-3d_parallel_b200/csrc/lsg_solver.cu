@@ -1801,6 +1801,83 @@ int lsg_set_matrix_helmholtz(lsg_ctx* h, int dir, int N, int M, int K, const int
     LSG_API_END(h)
 }
 
+int lsg_helmholtz_flux(lsg_ctx* h, int dir, int N, int M, int K, const int* stype, const double* delta,
+                       const double* u_w, const double* bc, double nu, int ib, const int* side_type,
+                       const double* theta, const double* alpha, const double* inv_vof, const double* delta_ib_en,
+                       const double* delta_ib_ws, const double* delta_ib_nb, const double* delta_ib_st,
+                       const double* inv_delta_ib_ne, const double* inv_delta_ib_tn, const double* vib,
+                       const double* vib_yx, const double* vib_zy, double* flux)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z)");
+    LSG_REQUIRE(N >= 3 && M >= 3 && K >= 3, LSG_ERR_ARG, "grid must be at least 3 cells in every direction");
+    LSG_REQUIRE(stype && delta && u_w && bc && flux, LSG_ERR_ARG, "null argument");
+    LSG_REQUIRE(!ib || (side_type && theta && alpha && inv_vof && delta_ib_en && delta_ib_ws && delta_ib_nb &&
+                        delta_ib_st && inv_delta_ib_ne && inv_delta_ib_tn && vib && vib_yx && vib_zy),
+                LSG_ERR_ARG, "null immersed-boundary argument");
+    const long long n = (long long)N * M * K;
+    LSG_REQUIRE(n < (1LL << 31), LSG_ERR_ARG, "grid too large");
+    const int Ns = N - (dir == 0), Ms = M - (dir == 1), Ks = K - (dir == 2);
+    const long long ns = (long long)Ns * Ms * Ks;
+    LSG_CUDA(cudaSetDevice(C.device));
+    DevBuf<int> dt, dsd;
+    DevBuf<double> dde, duw, dout, dth, dal, dinv, den, dws, dnb, dst, dne, dtn, dv, dyx, dzy;
+    dt.alloc(ns);
+    dde.alloc(3 * n);
+    duw.alloc((size_t)M * K);
+    dout.alloc(ns);
+    LSG_CUDA(cudaMemcpyAsync(dt.p, stype, ns * sizeof(int), cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dde.p, delta, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(duw.p, u_w, (size_t)M * K * 8, cudaMemcpyHostToDevice, C.s));
+    HelmFluxArgs a;
+    memset(&a, 0, sizeof(a));
+    a.g.N = N;
+    a.g.M = M;
+    a.g.K = K;
+    a.g.d = dir;
+    a.g.stype = dt.p;
+    a.g.delta = dde.p;
+    a.g.nu = nu;
+    if (ib) {
+        dsd.alloc(3 * n);
+        LSG_CUDA(cudaMemcpyAsync(dsd.p, side_type, 3 * n * sizeof(int), cudaMemcpyHostToDevice, C.s));
+        const double* src3[11] = {theta, alpha, delta_ib_en, delta_ib_ws, delta_ib_nb, delta_ib_st,
+                                  inv_delta_ib_ne, inv_delta_ib_tn, vib, vib_yx, vib_zy};
+        DevBuf<double>* dst3[11] = {&dth, &dal, &den, &dws, &dnb, &dst, &dne, &dtn, &dv, &dyx, &dzy};
+        for (int q = 0; q < 11; q++) {
+            dst3[q]->alloc(3 * n);
+            LSG_CUDA(cudaMemcpyAsync(dst3[q]->p, src3[q], 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+        }
+        dinv.alloc(n);
+        LSG_CUDA(cudaMemcpyAsync(dinv.p, inv_vof, n * 8, cudaMemcpyHostToDevice, C.s));
+        a.g.theta = dth.p;
+        a.g.alpha = dal.p;
+        a.g.inv_vof = dinv.p;
+        a.g.dib_en = den.p;
+        a.g.dib_ws = dws.p;
+        a.g.dib_nb = dnb.p;
+        a.g.dib_st = dst.p;
+        a.g.inv_dib_ne = dne.p;
+        a.g.inv_dib_tn = dtn.p;
+        a.side_type = dsd.p;
+        a.vib = dv.p;
+        a.vyx = dyx.p;
+        a.vzy = dzy.p;
+    }
+    a.u_w = duw.p;
+    for (int q = 0; q < 18; q++) a.bc[q] = bc[q];
+    a.ib = ib ? 1 : 0;
+    a.flux = dout.p;
+    k_helmholtz_flux<<<grid_for(ns, 256), 256, 0, C.s>>>(a);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaMemcpyAsync(flux, dout.p, ns * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
 int lsg_set_staggered_types(lsg_ctx* h, const int* xtype, const int* ytype, const int* ztype)
 {
     if (!h) return LSG_ERR_ARG;

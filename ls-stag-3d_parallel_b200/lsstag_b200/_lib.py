@@ -55,6 +55,7 @@ EXPORTS = [
     "lsg_momentum_rhs", "lsg_convective_apply", "lsg_convective_apply_device", "lsg_version",
     "lsg_loads_set", "lsg_loads_calculate", "lsg_loads_calculate_device", "lsg_loads_reset_filter",
     "lsg_loads_adjoint", "lsg_loads_adjoint_device", "lsg_set_matrix_helmholtz",
+    "lsg_helmholtz_flux",
 ]
 
 _lib = None
@@ -123,6 +124,8 @@ def load() -> C.CDLL:
     lib.lsg_projection_correct_device.argtypes = [P] + [C.c_void_p] * 8 + [C.c_double, C.c_double, C.c_int]
     lib.lsg_set_matrix_helmholtz.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, ip] + [dp] * 11 + [
         C.c_double, C.c_double, C.c_int]
+    lib.lsg_helmholtz_flux.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, ip, dp, dp, dp, C.c_double, C.c_int,
+                                       ip] + [dp] * 12 + [dp]
     lib.lsg_loads_set.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip] + [dp] * 8 + [C.c_double,
                                                                                              C.c_double]
     lib.lsg_loads_calculate.argtypes = [P] + [dp] * 8 + [C.c_double, dp, C.POINTER(LoadsResult)]

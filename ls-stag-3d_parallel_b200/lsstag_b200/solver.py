@@ -128,6 +128,30 @@ class IterativeSolver:
         if setup:
             self._setup()
 
+    def helmholtz_flux(self, direction: int, base_dims, stype, delta, u_w, bc, nu: float, ib_geom: dict | None = None):
+        """Source term of the momentum operator of one direction as the
+        reference's build() leaves it (inflow, S/N and B/T walls); with
+        ib_geom (side_type, theta, alpha, inv_vof, dib_en, dib_ws, dib_nb,
+        dib_st, inv_dib_ne, inv_dib_tn, vib, vibyx, vibzy) the immersed-boundary
+        term is written over it as the reference does for moving bodies."""
+        N, M, K = (int(v) for v in base_dims)
+        d = int(direction)
+        ns = (N - (d == 0)) * (M - (d == 1)) * (K - (d == 2))
+        st = np.ascontiguousarray(stype, dtype=np.int32)
+        arr = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (delta, u_w, bc)]
+        out = np.empty(ns)
+        keys = ("theta", "alpha", "inv_vof", "dib_en", "dib_ws", "dib_nb", "dib_st", "inv_dib_ne", "inv_dib_tn",
+                "vib", "vibyx", "vibzy")
+        if ib_geom is not None:
+            sd = np.ascontiguousarray(ib_geom["side_type"], dtype=np.int32)
+            gg = [np.ascontiguousarray(ib_geom[k], dtype=np.float64).reshape(-1) for k in keys]
+            extra = [L.iptr(sd)] + [L.dptr(a) for a in gg]
+        else:
+            extra = [None] * 13
+        self.ctx.check(self.ctx.lib.lsg_helmholtz_flux(self.ctx.h, d, N, M, K, L.iptr(st), *(L.dptr(a) for a in arr),
+                                                       float(nu), int(ib_geom is not None), *extra, L.dptr(out)))
+        return out
+
     # -- pressure projection (needs set_geometry) -----------------------------
     def set_staggered_types(self, xtype, ytype, ztype):
         self._stypes = tuple(np.ascontiguousarray(t, dtype=np.int32) for t in (xtype, ytype, ztype))

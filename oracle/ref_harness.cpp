@@ -178,6 +178,18 @@ struct HarnessTask : FlowTaskDescription {
     }
 };
 
+/* The momentum operators with their immersed-boundary source term made
+   callable (ibFlux is run by the reference only for moving bodies). */
+struct HelmXProbe : HelmholtzDiscreteOperatorX {
+    void runIbFlux() { ibRecalcFlux = true; calcFlux(); }
+};
+struct HelmYProbe : HelmholtzDiscreteOperatorY {
+    void runIbFlux() { ibRecalcFlux = true; calcFlux(); }
+};
+struct HelmZProbe : HelmholtzDiscreteOperatorZ {
+    void runIbFlux() { ibRecalcFlux = true; calcFlux(); }
+};
+
 struct Dumper {
     std::string dir;
     std::ofstream man;
@@ -477,12 +489,25 @@ int main(int argc, char** argv)
             double* vofs[3] = {mm->xMesh.VOF, mm->yMesh.VOF, mm->zMesh.VOF};
             for (int d = 0; d < 3; d++)
                 for (long i = 0; i < ns[d]; i++) vofs[d][i] = 0.2 + 0.8 * U(rng);
+            // cell sizes, boundary velocities and immersed-boundary velocities too
+            const double hx = task->hx, hy = task->hy, hz = task->hz;
+            for (long i = 0; i < n; i++) {
+                mm->delta[i].set(hx * (0.5 + U(rng)), hy * (0.5 + U(rng)), hz * (0.5 + U(rng)));
+                mm->v_ib[i].set(U(rng) - 0.5, U(rng) - 0.5, U(rng) - 0.5);
+                mm->v_ib_yx[i].set(U(rng) - 0.5, U(rng) - 0.5, U(rng) - 0.5);
+                mm->v_ib_zy[i].set(U(rng) - 0.5, U(rng) - 0.5, U(rng) - 0.5);
+            }
+            for (long j = 0; j < (long)M * K; j++) task->pU_W[j] = 0.5 + U(rng);
+            double* bcs[18] = {&task->U_W, &task->U_E, &task->U_S, &task->U_N, &task->U_B, &task->U_T,
+                               &task->V_W, &task->V_E, &task->V_S, &task->V_N, &task->V_B, &task->V_T,
+                               &task->W_W, &task->W_E, &task->W_S, &task->W_N, &task->W_B, &task->W_T};
+            for (int b = 0; b < 18; b++) *bcs[b] = U(rng) - 0.5;
         }
         // the operators of a task that is not a flow (no outflow terms, walls on T/B)
         if ((int)cfg.get("helm_noflow", 0)) task->id = BaseTaskDescription::TASK_UNKNOWN;
-        HelmholtzDiscreteOperatorX* kx = new HelmholtzDiscreteOperatorX;   // not destroyed (see below)
-        HelmholtzDiscreteOperatorY* ky = new HelmholtzDiscreteOperatorY;
-        HelmholtzDiscreteOperatorZ* kz = new HelmholtzDiscreteOperatorZ;
+        HelmXProbe* kx = new HelmXProbe;   // not destroyed (see below)
+        HelmYProbe* ky = new HelmYProbe;
+        HelmZProbe* kz = new HelmZProbe;
         kx->init(task, &mm->xMesh);
         ky->init(task, &mm->yMesh);
         kz->init(task, &mm->zMesh);
@@ -494,6 +519,17 @@ int main(int argc, char** argv)
         out.d("hflux_x", kx->flux, ns[0]);
         out.d("hflux_y", ky->flux, ns[1]);
         out.d("hflux_z", kz->flux, ns[2]);
+        if ((int)cfg.get("helm_ibflux", 0)) {
+            // the immersed-boundary part of the source term, which the time
+            // step recomputes for moving bodies (ibFluxHelmX/Y/Z), applied
+            // over the boundary flux above
+            kx->runIbFlux();
+            ky->runIbFlux();
+            kz->runIbFlux();
+            out.d("hflux_ib_x", kx->flux, ns[0]);
+            out.d("hflux_ib_y", ky->flux, ns[1]);
+            out.d("hflux_ib_z", kz->flux, ns[2]);
+        }
         out.i("xtype", (const int*)mm->xMesh.typeOfCell, ns[0]);
         out.i("ytype", (const int*)mm->yMesh.typeOfCell, ns[1]);
         out.i("ztype", (const int*)mm->zMesh.typeOfCell, ns[2]);

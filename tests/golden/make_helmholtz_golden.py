@@ -12,8 +12,12 @@ helm_random14.npz: the same operators on a 14^3 grid with a sphere whose face fr
 edge fractions (15 % of them exactly 0, so that the immersed-boundary
 branches run on every cell type), cell volumes and immersed-boundary
 distances are seeded random numbers; the cell types are the mesh's own.
-Built once as a flow task (K*_flow) and once as a task that is not a flow
-(K*_noflow: no outflow terms, T/B walls).
+Cell sizes, boundary velocities, the inflow profile and the
+immersed-boundary velocities are seeded too.  Built once as a flow task
+(K*_flow) and once as a task that is not a flow (K*_noflow: no outflow
+terms, T/B walls); with the boundary source term of the operators (hflux_*)
+and the immersed-boundary source term written over it (hflux_ib_*,
+ibFluxHelmX/Y/Z, which the reference runs for moving bodies).
 """
 from __future__ import annotations
 
@@ -45,20 +49,26 @@ def main():
     h = 1.0 / 16
     case = rr.Case(16, 16, 16, h, h, h, spheres=[(0.5 + 0.3 * h, 0.5 + 0.2 * h, 0.5 + 0.1 * h, 0.18)])
     r = rr.run(case, threads=1, helm=1, dump_geometry=0)
-    keep = {k: r[k] for k in GEOM}
+    keep = {k: r[k] for k in GEOM + ["bc", "u_w"]}
     keep.update(ops(r))
     np.savez_compressed(os.path.join(HERE, "helm_sphere16.npz"), **keep)
 
     h = 1.0 / 14
     case = rr.Case(14, 14, 14, h, h, h, spheres=[(0.5 + 0.3 * h, 0.5 + 0.2 * h, 0.5 + 0.1 * h, 0.12)])
-    r1 = rr.run(case, threads=1, helm=1, helm_random=1, seed=5, dump_geometry=0)
-    r2 = rr.run(case, threads=1, helm=1, helm_random=1, helm_noflow=1, seed=5, dump_geometry=0)
-    for k in GEOM[:-1]:
+    r1 = rr.run(case, threads=1, helm=1, helm_random=1, helm_ibflux=1, seed=5, dump_geometry=0)
+    r2 = rr.run(case, threads=1, helm=1, helm_random=1, helm_ibflux=1, helm_noflow=1, seed=5, dump_geometry=0)
+    extra = ["side_type", "vib", "vibyx", "vibzy", "u_w", "bc"]
+    for k in GEOM[:-1] + extra:
         assert np.array_equal(r1[k], r2[k]), k
-    keep = {k: r1[k] for k in GEOM[:-1]}
+    keep = {k: r1[k] for k in GEOM[:-1] + extra}
     keep["nu_coef_dt"] = r1["nu_coef_isflow_dt"][[0, 1, 3]]
     keep.update(ops(r1, "_flow"))
     keep.update(ops(r2, "_noflow"))
+    for d in "xyz":
+        # the source term is the same for both task kinds at build time
+        assert np.array_equal(r1["hflux_" + d], r2["hflux_" + d])
+        keep["hflux_" + d] = r1["hflux_" + d]
+        keep["hflux_ib_" + d] = r1["hflux_ib_" + d]
     np.savez_compressed(os.path.join(HERE, "helm_random14.npz"), **keep)
     for f in ("helm_sphere16.npz", "helm_random14.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -92,3 +92,36 @@ def test_helmholtz_rejects_inconsistent_types():
         s.set_helmholtz(0, geom, g["dims"], 0.01, 150.0, True, setup=False)
     assert e.value.code == L.LSG_ERR_ARG
     s.close()
+
+
+@pytest.mark.parametrize("d", [0, 1, 2])
+def test_helmholtz_flux_bitwise(d):
+    """Boundary source term, then the immersed-boundary term written over it,
+    on seeded random geometry, cell sizes and boundary velocities: bitwise."""
+    from lsstag_b200 import solver as S
+    g = load_golden("helm_random14")
+    c = "xyz"[d]
+    nu = float(g["nu_coef_dt"][0])
+    s = S.ILUFGMRES()
+    f = s.helmholtz_flux(d, g["dims"], g[c + "type"], g["delta"], g["u_w"], g["bc"], nu)
+    assert np.array_equal(f, g["hflux_" + c])
+    keys = ("side_type", "theta", "alpha", "inv_vof", "dib_en", "dib_ws", "dib_nb", "dib_st", "inv_dib_ne",
+            "inv_dib_tn", "vib", "vibyx", "vibzy")
+    fi = s.helmholtz_flux(d, g["dims"], g[c + "type"], g["delta"], g["u_w"], g["bc"], nu,
+                          ib_geom={k: g[k] for k in keys})
+    assert np.array_equal(fi, g["hflux_ib_" + c])
+    s.close()
+
+
+def test_helmholtz_flux_on_sphere_matches_momentum_step_input():
+    """The source term the reference's momentum step used (the hflux input
+    of lsg_momentum_rhs in the momentum-step fixture) from the geometry."""
+    from lsstag_b200 import solver as S
+    h = load_golden("helm_sphere16")
+    g = load_golden("sphere16")
+    nu = float(h["nu_coef_isflow_dt"][0])
+    s = S.ILUFGMRES()
+    for d, c in enumerate("xyz"):
+        f = s.helmholtz_flux(d, h["dims"], h[c + "type"], h["delta"], h["u_w"], h["bc"], nu)
+        assert np.array_equal(f, g["mstep_hflux_" + c]), c
+    s.close()

@@ -40,3 +40,30 @@ def test_helmholtz_random_geometry_bitwise(d, flow):
     # every box-boundary family, fluid, solid and cut cells are present
     types = set(int(t) for t in g["xyz"[d] + "type"])
     assert set(range(-27, -1)) <= types and {0, 11111111} <= types and any(t > 0 and t != 11111111 for t in types)
+
+
+@pytest.mark.parametrize("d", [0, 1, 2])
+def test_helmholtz_flux_bitwise(d):
+    g = load_golden("helm_random14")
+    N, M, K = (int(v) for v in g["dims"])
+    nu = float(g["nu_coef_dt"][0])
+    c = "xyz"[d]
+    f = O.helmholtz_flux(d, N, M, K, g[c + "type"], g["delta"], g["u_w"], g["bc"], nu)
+    assert np.array_equal(f, g["hflux_" + c])
+    fi = O.helmholtz_ib_flux(d, N, M, K, g[c + "type"], g["side_type"], g["theta"], g["alpha"], g["delta"],
+                             g["inv_vof"], g["dib_en"], g["dib_ws"], g["dib_nb"], g["dib_st"], g["inv_dib_ne"],
+                             g["inv_dib_tn"], g["vib"], g["vibyx"], g["vibzy"], nu, f)
+    assert np.array_equal(fi, g["hflux_ib_" + c])
+    assert np.count_nonzero(fi != f) > 0            # the immersed-boundary rows changed
+
+
+def test_helmholtz_flux_sphere_is_the_momentum_step_input():
+    """On the sphere case the restated source term equals the hflux the
+    reference's momentum step used (momentum-step fixture)."""
+    h = load_golden("helm_sphere16")
+    g = load_golden("sphere16")
+    N, M, K = (int(v) for v in h["dims"])
+    nu = float(h["nu_coef_isflow_dt"][0])
+    for d, c in enumerate("xyz"):
+        f = O.helmholtz_flux(d, N, M, K, h[c + "type"], h["delta"], h["u_w"], h["bc"], nu)
+        assert np.array_equal(f, g["mstep_hflux_" + c]), c
