@@ -235,6 +235,25 @@ int lsg_helmholtz_flux(lsg_ctx* ctx, int dir, int N, int M, int K, const int* st
                        const double* inv_delta_ib_ne, const double* inv_delta_ib_tn, const double* vib,
                        const double* vib_yx, const double* vib_zy, double* flux);
 
+/* Source term of the convective operator of direction dir as the time step
+   recomputes it (SkewSymDiscreteOperator::recalc -> calcFlux -> baseFlux,
+   skew_sym_discrete_operator.h:244-249, :290-294), the flux2 input of
+   lsg_momentum_rhs.  For z: ConvectiveDiscreteOperatorZ::baseFlux
+   (convective_discrete_operator_z.h:748-757: inflow W_W with the x-inflow
+   profile, outflow from ux and uz, S/N walls W_S*V_S, W_N*V_N, B/T outflow
+   terms from uz), bitwise.  For x and y the reference's operators never run
+   their baseFluxX/baseFluxY (they do not override baseFlux), so the term is
+   0, reproduced.  theta, delta (3n) on the N x M x K base grid, ux/uz the
+   x/z-grid velocities, u_w the x-inflow profile (M*K), bc as for
+   lsg_helmholtz_flux.  Host pointers. */
+int lsg_convective_flux(lsg_ctx* ctx, int dir, int N, int M, int K, const double* theta, const double* delta,
+                        const double* ux, const double* uy, const double* uz, const double* u_w, const double* bc,
+                        double* flux);
+/* Same on device pointers (bc on the host). */
+int lsg_convective_flux_device(lsg_ctx* ctx, int dir, int N, int M, int K, const double* theta, const double* delta,
+                               const double* ux, const double* uy, const double* uz, const double* u_w,
+                               const double* bc, double* flux);
+
 /* ---- loads on the immersed boundary (LoadsCalculator, loads_calculator.h) ---- */
 
 typedef struct lsg_loads_result {

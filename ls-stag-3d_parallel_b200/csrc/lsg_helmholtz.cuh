@@ -414,3 +414,65 @@ __global__ void __launch_bounds__(256) k_helmholtz_flux(HelmFluxArgs a)
 }
 
 }  // namespace lsg
+
+namespace lsg {
+
+// Boundary source term of the z convective operator as the time step
+// recomputes it (ConvectiveDiscreteOperatorZ::baseFlux,
+// convective_discrete_operator_z.h:748-757: baseFluxz, addFluxNSz,
+// addFluxTBOutZ), one thread per z-grid cell, in the reference's order
+// (inflow / outflow value assigned, then the S/N and B/T terms added).  The
+// outflow value uses the row's first cell's sizes, as the reference does.
+// The x and y operators' source terms are 0 in the reference (their
+// baseFluxX/baseFluxY never run), so no kernel exists for them.
+struct ConvFluxArgs {
+    int N, M, K;
+    const double* theta;
+    const double* delta;
+    const double* ux;
+    const double* uz;
+    const double* u_w;
+    double W_W, VW_S, VW_N;       // W_W, W_S * V_S, W_N * V_N
+    double* flux;
+};
+
+__global__ void __launch_bounds__(256) k_convective_flux_z(ConvFluxArgs a)
+{
+    const int N = a.N, M = a.M, Ks = a.K - 1;
+    const long long NM = (long long)N * M, ns = NM * Ks;
+    const double* de = a.delta;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ns;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % N);
+        const long long rest = i / N;
+        const int y = (int)(rest % M), z = (int)(rest / M);
+        double f = 0.0;
+        if (x == 0 || x == N - 1) {
+            const long long numF = (long long)N * y + NM * z;       // the row's first cell
+            const long long numW = y + (long long)z * M;
+            const double dz = de[3 * numF + 2], dy = de[3 * numF + 1], dzz = de[3 * (numF + NM) + 2];
+            if (x == 0) {
+                f = h_mul(h_mul(h_mul(-0.25, h_add(h_mul(a.u_w[numW], dz), h_mul(a.u_w[numW + M], dzz))), a.W_W), dy);
+            } else {
+                const long long last = numF + N - 1, num2 = last - numW - 1;
+                f = h_mul(h_mul(h_mul(0.25, a.uz[last]),
+                                h_add(h_mul(a.ux[num2], dz), h_mul(a.ux[num2 + (long long)(N - 1) * M], dzz))),
+                          dy);
+            }
+        }
+        if (y == 0 || y == M - 1) {
+            const long long b0 = (long long)z * NM;
+            const double dzz = h_mul(0.25, h_add(de[3 * b0 + 2], de[3 * (b0 + NM) + 2]));
+            const double coef = h_mul(de[3 * (b0 + x)], dzz);
+            f = (y == 0) ? h_sub(f, h_mul(coef, a.VW_S)) : h_add(f, h_mul(coef, a.VW_N));
+        }
+        if (z == 0 || z == Ks - 1) {
+            const double w = a.uz[i];
+            const double t = h_mul(h_mul(h_mul(h_mul(h_mul(0.5, de[3 * i]), de[3 * i + 1]), a.theta[3 * i + 2]), w), w);
+            f = (z == 0) ? h_sub(f, t) : h_add(f, t);
+        }
+        a.flux[i] = f;
+    }
+}
+
+}  // namespace lsg

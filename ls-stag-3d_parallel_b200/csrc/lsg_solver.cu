@@ -1878,6 +1878,89 @@ int lsg_helmholtz_flux(lsg_ctx* h, int dir, int N, int M, int K, const int* styp
     LSG_API_END(h)
 }
 
+static void convective_flux_run(Context& C, int dir, int N, int M, int K, const double* theta, const double* delta,
+                                const double* ux, const double* uz, const double* u_w, const double* bc, double* flux)
+{
+    const int Ns = N - (dir == 0), Ms = M - (dir == 1), Ks = K - (dir == 2);
+    const long long ns = (long long)Ns * Ms * Ks;
+    if (dir != 2) {
+        // the reference's x and y convective operators keep a zero source term
+        LSG_CUDA(cudaMemsetAsync(flux, 0, ns * 8, C.s));
+        return;
+    }
+    ConvFluxArgs a;
+    a.N = N;
+    a.M = M;
+    a.K = K;
+    a.theta = theta;
+    a.delta = delta;
+    a.ux = ux;
+    a.uz = uz;
+    a.u_w = u_w;
+    a.W_W = bc[12];
+    a.VW_S = bc[14] * bc[8];
+    a.VW_N = bc[15] * bc[9];
+    a.flux = flux;
+    k_convective_flux_z<<<grid_for(ns, 256), 256, 0, C.s>>>(a);
+    LSG_CHECK_LAUNCH();
+}
+
+int lsg_convective_flux_device(lsg_ctx* h, int dir, int N, int M, int K, const double* theta, const double* delta,
+                               const double* ux, const double* uy, const double* uz, const double* u_w,
+                               const double* bc, double* flux)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z)");
+    LSG_REQUIRE(N >= 3 && M >= 3 && K >= 3, LSG_ERR_ARG, "grid must be at least 3 cells in every direction");
+    LSG_REQUIRE(flux && bc && (dir != 2 || (theta && delta && ux && uz && u_w)), LSG_ERR_ARG, "null argument");
+    (void)uy;
+    LSG_CUDA(cudaSetDevice(C.device));
+    convective_flux_run(C, dir, N, M, K, theta, delta, ux, uz, u_w, bc, flux);
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_convective_flux(lsg_ctx* h, int dir, int N, int M, int K, const double* theta, const double* delta,
+                        const double* ux, const double* uy, const double* uz, const double* u_w, const double* bc,
+                        double* flux)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z)");
+    LSG_REQUIRE(N >= 3 && M >= 3 && K >= 3, LSG_ERR_ARG, "grid must be at least 3 cells in every direction");
+    LSG_REQUIRE(flux && bc && (dir != 2 || (theta && delta && ux && uz && u_w)), LSG_ERR_ARG, "null argument");
+    (void)uy;
+    const long long n = (long long)N * M * K;
+    LSG_REQUIRE(n < (1LL << 31), LSG_ERR_ARG, "grid too large");
+    const int Ns = N - (dir == 0), Ms = M - (dir == 1), Ks = K - (dir == 2);
+    const long long ns = (long long)Ns * Ms * Ks;
+    LSG_CUDA(cudaSetDevice(C.device));
+    DevBuf<double> dth, dde, dux, duz, duw, dout;
+    dout.alloc(ns);
+    if (dir == 2) {
+        const long long nx = (long long)(N - 1) * M * K, nz = (long long)N * M * (K - 1);
+        dth.alloc(3 * n);
+        dde.alloc(3 * n);
+        dux.alloc(nx);
+        duz.alloc(nz);
+        duw.alloc((size_t)M * K);
+        LSG_CUDA(cudaMemcpyAsync(dth.p, theta, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+        LSG_CUDA(cudaMemcpyAsync(dde.p, delta, 3 * n * 8, cudaMemcpyHostToDevice, C.s));
+        LSG_CUDA(cudaMemcpyAsync(dux.p, ux, nx * 8, cudaMemcpyHostToDevice, C.s));
+        LSG_CUDA(cudaMemcpyAsync(duz.p, uz, nz * 8, cudaMemcpyHostToDevice, C.s));
+        LSG_CUDA(cudaMemcpyAsync(duw.p, u_w, (size_t)M * K * 8, cudaMemcpyHostToDevice, C.s));
+    }
+    convective_flux_run(C, dir, N, M, K, dth.p, dde.p, dux.p, duz.p, duw.p, bc, dout.p);
+    LSG_CUDA(cudaMemcpyAsync(flux, dout.p, ns * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
 int lsg_set_staggered_types(lsg_ctx* h, const int* xtype, const int* ytype, const int* ztype)
 {
     if (!h) return LSG_ERR_ARG;

@@ -152,6 +152,18 @@ class IterativeSolver:
                                                        float(nu), int(ib_geom is not None), *extra, L.dptr(out)))
         return out
 
+    def convective_flux(self, direction: int, base_dims, theta, delta, ux, uy, uz, u_w, bc):
+        """Source term (flux2) of the convective operator of one direction as
+        the reference's time step recomputes it (0 for x and y, as there)."""
+        N, M, K = (int(v) for v in base_dims)
+        d = int(direction)
+        ns = (N - (d == 0)) * (M - (d == 1)) * (K - (d == 2))
+        arr = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (theta, delta, ux, uy, uz, u_w, bc)]
+        out = np.empty(ns)
+        self.ctx.check(self.ctx.lib.lsg_convective_flux(self.ctx.h, d, N, M, K, *(L.dptr(a) for a in arr),
+                                                        L.dptr(out)))
+        return out
+
     # -- pressure projection (needs set_geometry) -----------------------------
     def set_staggered_types(self, xtype, ytype, ztype):
         self._stypes = tuple(np.ascontiguousarray(t, dtype=np.int32) for t in (xtype, ytype, ztype))

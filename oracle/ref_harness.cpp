@@ -519,6 +519,31 @@ int main(int argc, char** argv)
         out.d("hflux_x", kx->flux, ns[0]);
         out.d("hflux_y", ky->flux, ns[1]);
         out.d("hflux_z", kz->flux, ns[2]);
+        if ((int)cfg.get("helm_conv", 0)) {
+            // the convective operators' boundary source term (baseFlux of
+            // ConvectiveDiscreteOperatorX/Y/Z, built by init -> build -> calcFlux
+            // for flow tasks) on seeded velocities
+            std::mt19937_64 rng2((unsigned long long)cfg.get("seed", 1) + 17);
+            std::uniform_real_distribution<double> U2(-1.0, 1.0);
+            double* cur[3] = {mm->m_Ux, mm->m_Uy, mm->m_Uz};
+            for (int d = 0; d < 3; d++)
+                for (long i = 0; i < ns[d]; i++) cur[d][i] = U2(rng2);
+            ConvectiveDiscreteOperatorX* cx = new ConvectiveDiscreteOperatorX;   // not destroyed (see below)
+            ConvectiveDiscreteOperatorY* cy = new ConvectiveDiscreteOperatorY;
+            ConvectiveDiscreteOperatorZ* cz = new ConvectiveDiscreteOperatorZ;
+            cx->init(task, &mm->xMesh);
+            cy->init(task, &mm->yMesh);
+            cz->init(task, &mm->zMesh);
+            cx->recalc();
+            cy->recalc();
+            cz->recalc();
+            out.d("cflux_x", cx->flux, ns[0]);
+            out.d("cflux_y", cy->flux, ns[1]);
+            out.d("cflux_z", cz->flux, ns[2]);
+            out.d("ux", mm->m_Ux, ns[0]);
+            out.d("uy", mm->m_Uy, ns[1]);
+            out.d("uz", mm->m_Uz, ns[2]);
+        }
         if ((int)cfg.get("helm_ibflux", 0)) {
             // the immersed-boundary part of the source term, which the time
             // step recomputes for moving bodies (ibFluxHelmX/Y/Z), applied

@@ -17,7 +17,9 @@ immersed-boundary velocities are seeded too.  Built once as a flow task
 (K*_flow) and once as a task that is not a flow (K*_noflow: no outflow
 terms, T/B walls); with the boundary source term of the operators (hflux_*)
 and the immersed-boundary source term written over it (hflux_ib_*,
-ibFluxHelmX/Y/Z, which the reference runs for moving bodies).
+ibFluxHelmX/Y/Z, which the reference runs for moving bodies); and, on
+seeded velocities (ux, uy, uz), the convective operators' source term
+(cflux_*, ConvectiveDiscreteOperatorX/Y/Z::recalc).
 """
 from __future__ import annotations
 
@@ -55,7 +57,7 @@ def main():
 
     h = 1.0 / 14
     case = rr.Case(14, 14, 14, h, h, h, spheres=[(0.5 + 0.3 * h, 0.5 + 0.2 * h, 0.5 + 0.1 * h, 0.12)])
-    r1 = rr.run(case, threads=1, helm=1, helm_random=1, helm_ibflux=1, seed=5, dump_geometry=0)
+    r1 = rr.run(case, threads=1, helm=1, helm_random=1, helm_ibflux=1, helm_conv=1, seed=5, dump_geometry=0)
     r2 = rr.run(case, threads=1, helm=1, helm_random=1, helm_ibflux=1, helm_noflow=1, seed=5, dump_geometry=0)
     extra = ["side_type", "vib", "vibyx", "vibzy", "u_w", "bc"]
     for k in GEOM[:-1] + extra:
@@ -69,6 +71,8 @@ def main():
         assert np.array_equal(r1["hflux_" + d], r2["hflux_" + d])
         keep["hflux_" + d] = r1["hflux_" + d]
         keep["hflux_ib_" + d] = r1["hflux_ib_" + d]
+        keep["cflux_" + d] = r1["cflux_" + d]
+        keep["u" + d] = r1["u" + d]
     np.savez_compressed(os.path.join(HERE, "helm_random14.npz"), **keep)
     for f in ("helm_sphere16.npz", "helm_random14.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))

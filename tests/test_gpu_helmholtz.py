@@ -125,3 +125,25 @@ def test_helmholtz_flux_on_sphere_matches_momentum_step_input():
         f = s.helmholtz_flux(d, h["dims"], h[c + "type"], h["delta"], h["u_w"], h["bc"], nu)
         assert np.array_equal(f, g["mstep_hflux_" + c]), c
     s.close()
+
+
+@pytest.mark.parametrize("d", [0, 1, 2])
+def test_convective_flux_bitwise(d):
+    from lsstag_b200 import solver as S
+    g = load_golden("helm_random14")
+    s = S.ILUFGMRES()
+    f = s.convective_flux(d, g["dims"], g["theta"], g["delta"], g["ux"], g["uy"], g["uz"], g["u_w"], g["bc"])
+    assert np.array_equal(f, g["cflux_" + "xyz"[d]])
+    s.close()
+
+
+def test_convective_flux_sphere_is_the_momentum_step_input():
+    from lsstag_b200 import solver as S
+    h = load_golden("helm_sphere16")
+    g = load_golden("sphere16")
+    s = S.ILUFGMRES()
+    for d, c in enumerate("xyz"):
+        f = s.convective_flux(d, h["dims"], h["theta"], h["delta"], g["mstep_u_x"], g["mstep_u_y"], g["mstep_u_z"],
+                              h["u_w"], h["bc"])
+        assert np.array_equal(f, g["flux2_1" + c]), c
+    s.close()

@@ -67,3 +67,24 @@ def test_helmholtz_flux_sphere_is_the_momentum_step_input():
     for d, c in enumerate("xyz"):
         f = O.helmholtz_flux(d, N, M, K, h[c + "type"], h["delta"], h["u_w"], h["bc"], nu)
         assert np.array_equal(f, g["mstep_hflux_" + c]), c
+
+
+@pytest.mark.parametrize("d", [0, 1, 2])
+def test_convective_flux_bitwise(d):
+    """Source term of the convective operators (0 for x and y, as the
+    reference leaves it) on seeded geometry, velocities and boundary values."""
+    g = load_golden("helm_random14")
+    N, M, K = (int(v) for v in g["dims"])
+    f = O.convective_flux(d, N, M, K, g["theta"], g["delta"], g["ux"], g["uy"], g["uz"], g["u_w"], g["bc"])
+    assert np.array_equal(f, g["cflux_" + "xyz"[d]])
+    if d == 2:
+        assert np.count_nonzero(f) > 0
+
+
+def test_convective_flux_sphere_is_the_momentum_step_input():
+    h = load_golden("helm_sphere16")
+    g = load_golden("sphere16")
+    for d, c in enumerate("xyz"):
+        f = O.convective_flux(d, 16, 16, 16, h["theta"], h["delta"], g["mstep_u_x"], g["mstep_u_y"], g["mstep_u_z"],
+                              h["u_w"], h["bc"])
+        assert np.array_equal(f, g["flux2_1" + c]), c
