@@ -174,8 +174,10 @@ int lsg_laplace_flux_device(lsg_ctx* ctx, const int* side_type, const double* vi
      right = ((-2 u + 0.5 u_prev) VOF) coef2 - ((G p + flux) + prev_aux) + 2 aux,
    with G the pressure gradient applied from the geometry, flux the Helmholtz
    operator's source term, coef2 = 1/dt; aux is returned as the next step's
-   prev_aux.  Bit-identical to the reference.  Host pointers (staggered-grid
-   vectors, p on the base grid). */
+   prev_aux.  Bit-identical to the reference.  With rowptr == NULL (col and
+   val unused) flux2 already holds flux2 + C u, as lsg_convective_apply
+   returns it from the geometry.  Host pointers (staggered-grid vectors, p on
+   the base grid). */
 int lsg_momentum_rhs(lsg_ctx* ctx, int dir, const int* rowptr, const int* col, const double* val,
                      const double* flux2, const double* u, const double* uprev, const double* vof,
                      const double* hflux, const double* p, const double* prev_aux, double coef2, double* right,

@@ -285,6 +285,7 @@ __global__ void __launch_bounds__(256) k_gradient_apply(int dir, int N, int M, i
 // operator (ConvectiveDiscreteOperator*, rebuilt by the caller each step),
 // right = ((-2 u + 0.5 u_prev) VOF) coef2 - ((G p + flux) + prev_aux) + 2 aux;
 // aux is returned as the next step's prev_aux (Adams-Bashforth history).
+// Without a CSR (rowptr == NULL) flux2 already holds flux2 + C u.
 __global__ void __launch_bounds__(256) k_momentum_rhs(long long n, const int* __restrict__ rowptr,
                                                       const int* __restrict__ col, const double* __restrict__ val,
                                                       const double* __restrict__ flux2, const double* __restrict__ u,
@@ -298,7 +299,8 @@ __global__ void __launch_bounds__(256) k_momentum_rhs(long long n, const int* __
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         double aux = flux2[i];
-        for (int e = rowptr[i]; e < rowptr[i + 1]; e++) aux = add(aux, mul(val[e], u[col[e]]));
+        if (rowptr)
+            for (int e = rowptr[i]; e < rowptr[i + 1]; e++) aux = add(aux, mul(val[e], u[col[e]]));
         double r = mul(mul(add(mul(-2.0, u[i]), mul(0.5, uprev[i])), vof[i]), coef2);
         r = sub(r, add(add(gp[i], hflux[i]), prev_aux[i]));
         r = add(r, mul(aux, 2.0));

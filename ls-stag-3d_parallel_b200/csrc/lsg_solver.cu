@@ -2128,29 +2128,37 @@ int lsg_momentum_rhs(lsg_ctx* h, int dir, const int* rowptr, const int* col, con
     LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
                 "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
     LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z)");
-    LSG_REQUIRE(rowptr && col && val && flux2 && u && uprev && vof && hflux && p && prev_aux && right && aux,
+    // rowptr == NULL: flux2 already holds the convective term flux2 + C u
+    // (lsg_convective_apply with init = flux2)
+    LSG_REQUIRE((!rowptr || (col && val)) && flux2 && u && uprev && vof && hflux && p && prev_aux && right && aux,
                 LSG_ERR_ARG, "null argument");
     LSG_CUDA(cudaSetDevice(C.device));
     const Dims& d = C.d;
     const int Ns = d.N - (dir == 0), Ms = d.M - (dir == 1), Ks = d.K - (dir == 2);
     const long long ns = (long long)Ns * Ms * Ks, n = C.n;
-    const long long nnz = rowptr[ns];
-    LSG_REQUIRE(rowptr[0] == 0 && nnz >= 0, LSG_ERR_ARG, "bad CSR row pointer");
-    for (long long i = 0; i < ns; i++)
-        LSG_REQUIRE(rowptr[i] <= rowptr[i + 1], LSG_ERR_ARG, "CSR row pointer not monotone");
-    for (long long e = 0; e < nnz; e++)
-        LSG_REQUIRE(col[e] >= 0 && col[e] < ns, LSG_ERR_ARG, "CSR column outside the staggered grid");
+    const long long nnz = rowptr ? rowptr[ns] : 0;
+    if (rowptr) {
+        LSG_REQUIRE(rowptr[0] == 0 && nnz >= 0, LSG_ERR_ARG, "bad CSR row pointer");
+        for (long long i = 0; i < ns; i++)
+            LSG_REQUIRE(rowptr[i] <= rowptr[i + 1], LSG_ERR_ARG, "CSR row pointer not monotone");
+        for (long long e = 0; e < nnz; e++)
+            LSG_REQUIRE(col[e] >= 0 && col[e] < ns, LSG_ERR_ARG, "CSR column outside the staggered grid");
+    }
     DevBuf<int> drp, dcol;
     DevBuf<double> dval, dflux2, du, dup, dvof, dhf, dp, dprev, dgp, dr, da;
-    drp.alloc(ns + 1);
-    dcol.alloc(std::max<long long>(nnz, 1));
-    dval.alloc(std::max<long long>(nnz, 1));
+    if (rowptr) {
+        drp.alloc(ns + 1);
+        dcol.alloc(std::max<long long>(nnz, 1));
+        dval.alloc(std::max<long long>(nnz, 1));
+    }
     for (DevBuf<double>* b : {&dflux2, &du, &dup, &dvof, &dhf, &dprev, &dgp, &dr, &da}) b->alloc(ns);
     dp.alloc(n);
-    LSG_CUDA(cudaMemcpyAsync(drp.p, rowptr, (ns + 1) * sizeof(int), cudaMemcpyHostToDevice, C.s));
-    if (nnz) {
-        LSG_CUDA(cudaMemcpyAsync(dcol.p, col, nnz * sizeof(int), cudaMemcpyHostToDevice, C.s));
-        LSG_CUDA(cudaMemcpyAsync(dval.p, val, nnz * 8, cudaMemcpyHostToDevice, C.s));
+    if (rowptr) {
+        LSG_CUDA(cudaMemcpyAsync(drp.p, rowptr, (ns + 1) * sizeof(int), cudaMemcpyHostToDevice, C.s));
+        if (nnz) {
+            LSG_CUDA(cudaMemcpyAsync(dcol.p, col, nnz * sizeof(int), cudaMemcpyHostToDevice, C.s));
+            LSG_CUDA(cudaMemcpyAsync(dval.p, val, nnz * 8, cudaMemcpyHostToDevice, C.s));
+        }
     }
     const double* hsrc[6] = {flux2, u, uprev, vof, hflux, prev_aux};
     DevBuf<double>* dst[6] = {&dflux2, &du, &dup, &dvof, &dhf, &dprev};

@@ -1,0 +1,102 @@
+"""Time steps of the fixed-body flow task with every operator on the GPU:
+the counterpart of the reference's TimeSteppingMethodInterface::init/step
+(TimeSteppingMethod/time_stepping_method_interface.h:150-214) for a flow past
+bodies that do not move.
+
+One step, in the reference's order:
+  1. the pressure operator's source term from the current x-velocity
+     (pEq.m_A->calcFlux: lsg_laplace_flux);
+  2. for u, v, w: the convective operator of the current velocities applied
+     from the geometry with its source term (ConvectiveDiscreteOperator*
+     recalc: lsg_convective_flux + lsg_convective_apply), the right-hand side
+     (HelmholtzDiscreteEquation::recalcRightMember: lsg_momentum_rhs) and the
+     ILU(0)-FGMRES solve on the momentum operator assembled from the geometry
+     (lsg_set_matrix_helmholtz), started from the current velocity;
+  3. the pressure equation: b = D u* + flux (lsg_projection_rhs) and the
+     MG-FGMRES solve from 0;
+  4. the projection (SetSolutions::correction: lsg_projection_correct).
+The state (current and previous velocities, pressure, the Adams-Bashforth
+history of each momentum equation) lives on the host between the calls.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import solver as S
+
+
+class FlowStepper:
+    """geom: the mesh arrays (celltype, xtype, ytype, ztype, side_type, theta,
+    alpha, delta, inv_vof, vof_x/y/z, inv_mx/my/mz, dib_en/ws/nb/st,
+    inv_dib_ne/tn, vib, vibyx, vibzy, u_w, bc (18 boundary velocities), pins);
+    par: nu, coef (1.5/dt), coef2 (1/dt), coef_integr (COEF_INTEGR_TIME), eps
+    (absolute), vbase, max_it, restart_mom, restart_p."""
+
+    def __init__(self, geom: dict, dims, par: dict, u0, v0, w0, p0, device: int = 0):
+        self.g = geom
+        self.dims = tuple(int(v) for v in dims)
+        self.par = par
+        N, M, K = self.dims
+        bc = np.asarray(geom["bc"], dtype=np.float64)
+        self.bc = bc
+        # U_E, V_S, V_N, W_B, W_T of the pressure equation's source term
+        self.bc_lap = bc[[1, 8, 9, 16, 17]].copy()
+        ptask = S.Task(eps=par["eps"], MAX_ITER=int(par["max_it"]), FGMRES_RESTART_NUM=int(par["restart_p"]))
+        self.pres = S.MGFGMRES(device=device)
+        self.pres.set_geometry({k: geom[k] for k in ("celltype", "theta", "delta", "inv_mx", "inv_my", "inv_mz")},
+                               self.dims, geom["pins"], task=ptask)
+        self.pres.set_staggered_types(geom["xtype"], geom["ytype"], geom["ztype"])
+        mtask = S.Task(eps=par["eps"], MAX_ITER=int(par["max_it"]), FGMRES_RESTART_NUM=int(par["restart_mom"]))
+        self.mom, self.hflux = [], []
+        for d, c in enumerate("xyz"):
+            hg = {k: geom[k] for k in ("theta", "alpha", "delta", "inv_vof", "dib_en", "dib_ws", "dib_nb", "dib_st",
+                                       "inv_dib_ne", "inv_dib_tn")}
+            hg["stype"] = geom[c + "type"]
+            hg["vof"] = geom["vof_" + c]
+            s = S.ILUFGMRES(device=device)
+            s.set_helmholtz(d, hg, self.dims, par["nu"], par["coef_integr"], True, task=mtask)
+            self.mom.append(s)
+            self.hflux.append(s.helmholtz_flux(d, self.dims, geom[c + "type"], geom["delta"], geom["u_w"], bc,
+                                               par["nu"]))
+        self.u = [np.array(a, dtype=np.float64) for a in (u0, v0, w0)]
+        self.p = np.array(p0, dtype=np.float64)
+        # HelmholtzDiscreteEquation::set: previous velocity = current, history
+        # = flux2 + C(u) u of the initial state
+        self.uprev = [a.copy() for a in self.u]
+        self.prev_aux = [self._convective_term(d) for d in range(3)]
+        self.its = None
+
+    def _convective_term(self, d: int) -> np.ndarray:
+        g = self.g
+        flux2 = self.mom[d].convective_flux(d, self.dims, g["theta"], g["delta"], *self.u, g["u_w"], self.bc)
+        return self.pres.convective_apply(d, self.u, self.u[d], init=flux2)
+
+    def step(self):
+        g, par = self.g, self.par
+        flux_lap = self.pres.laplace_flux(g["side_type"], g["vib"], g["u_w"], self.bc_lap, self.u[0])
+        us, its = [], []
+        for d, c in enumerate("xyz"):
+            aux_in = self._convective_term(d)
+            right, aux = self.pres.momentum_rhs(d, None, aux_in, self.u[d], self.uprev[d], g["vof_" + c],
+                                                self.hflux[d], self.p, self.prev_aux[d], par["coef2"])
+            self.prev_aux[d] = aux
+            x = self.u[d].copy()
+            its.append(self.mom[d].solve(right, x))
+            us.append(x)
+        b = self.pres.projection_rhs(us[0], us[1], us[2], flux_lap)
+        phi = np.zeros_like(self.p)
+        its.append(self.pres.solve(b, phi))
+        self.uprev = [a.copy() for a in self.u]
+        p = self.p.copy()
+        u, v, w, _ = self.pres.projection_correct(phi, us[0], us[1], us[2], p, par["coef"], par["vbase"])
+        self.u = [u, v, w]
+        self.p = p
+        self.its = its
+        self.predictions = us
+        self.phi = phi
+        return its
+
+    def close(self):
+        for s in self.mom:
+            s.close()
+        self.pres.close()

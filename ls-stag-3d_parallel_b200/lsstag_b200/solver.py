@@ -193,14 +193,19 @@ class IterativeSolver:
     def momentum_rhs(self, direction: int, Cconv, flux2, u, uprev, vof, hflux, p, prev_aux, coef2):
         """(right, aux) of one momentum equation (HelmholtzDiscreteEquation::
         recalcRightMember); Cconv = (rowptr, col, val) of the convective
-        operator; aux is the next step's prev_aux."""
-        rp = np.ascontiguousarray(Cconv[0], dtype=np.int32)
-        col = np.ascontiguousarray(Cconv[1], dtype=np.int32)
-        val = np.ascontiguousarray(Cconv[2], dtype=np.float64)
+        operator; aux is the next step's prev_aux.  Cconv = None: flux2
+        already holds flux2 + C u (convective_apply with init=flux2)."""
+        if Cconv is None:
+            csr = (None, None, None)
+        else:
+            rp = np.ascontiguousarray(Cconv[0], dtype=np.int32)
+            col = np.ascontiguousarray(Cconv[1], dtype=np.int32)
+            val = np.ascontiguousarray(Cconv[2], dtype=np.float64)
+            csr = (L.iptr(rp), L.iptr(col), L.dptr(val))
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (flux2, u, uprev, vof, hflux, p, prev_aux)]
         right = np.empty_like(arrs[1])
         aux = np.empty_like(arrs[1])
-        self.ctx.check(self.ctx.lib.lsg_momentum_rhs(self.ctx.h, int(direction), L.iptr(rp), L.iptr(col), L.dptr(val),
+        self.ctx.check(self.ctx.lib.lsg_momentum_rhs(self.ctx.h, int(direction), *csr,
                                                      *(L.dptr(a) for a in arrs), float(coef2), L.dptr(right),
                                                      L.dptr(aux)))
         return right, aux

@@ -458,6 +458,101 @@ int main(int argc, char** argv)
             mm->v_ib[i].set(0.1 * sin(0.11 * i), 0.1 * cos(0.13 * i), 0.05 * sin(0.17 * i));
         for (long i = 0; i < (long)mm->xMesh.NMK; i++) mm->m_Ux[i] = 1.0 + 0.2 * sin(0.29 * i);
     }
+    if ((int)cfg.get("flow_steps", 0)) {
+        // whole time steps of the flow task as TimeSteppingMethodInterface::init
+        // and ::step run them (time_stepping_method_interface.h:150-214: the
+        // three momentum equations, the pressure equation, the projection),
+        // with every input of the GPU path and the state after each step
+        // dumped; no start-up pressure scaling (tScaleP < 0), solver
+        // tolerance task_eps (absolute)
+        LSSTAGUniformMesh* mm = task->m_mesh;
+        const int N = mm->baseMesh.N, M = mm->baseMesh.M, K = mm->baseMesh.K;
+        const long n = (long)N * M * K;
+        const long ns[3] = {(long)mm->xMesh.NMK, (long)mm->yMesh.NMK, (long)mm->zMesh.NMK};
+        task->tScaleP = -1.0;
+        task->eps = cfg.get("task_eps", task->eps);
+        PoissonDiscreteEquation* pE = new PoissonDiscreteEquation;   // not destroyed (see below)
+        pE->set(task, &(sol->prediction.p));
+        mm->U_ib = pE->m_A->flux;
+        HelmholtzDiscreteEquationX* uE = new HelmholtzDiscreteEquationX;
+        HelmholtzDiscreteEquationY* vE = new HelmholtzDiscreteEquationY;
+        HelmholtzDiscreteEquationZ* wE = new HelmholtzDiscreteEquationZ;
+        uE->set(task, &(sol->prediction.u));
+        vE->set(task, &(sol->prediction.v));
+        wE->set(task, &(sol->prediction.w));
+        sol->set((SparseMatrix*)(uE->m_grad), (SparseMatrix*)(vE->m_grad), (SparseMatrix*)(wE->m_grad), uE->coef);
+        int dd[3] = {N, M, K};
+        out.i("dims", dd, 3);
+        out.i("celltype", (const int*)mm->baseMesh.typeOfCell, n);
+        out.i("xtype", (const int*)mm->xMesh.typeOfCell, ns[0]);
+        out.i("ytype", (const int*)mm->yMesh.typeOfCell, ns[1]);
+        out.i("ztype", (const int*)mm->zMesh.typeOfCell, ns[2]);
+        out.i("side_type", (const int*)mm->baseSideTypes, 3 * n);
+        out.d("theta", (const double*)mm->theta, 3 * n);
+        out.d("alpha", (const double*)mm->alpha, 3 * n);
+        out.d("delta", (const double*)mm->delta, 3 * n);
+        out.d("inv_vof", mm->baseMesh.inv_VOF, n);
+        out.d("vof_x", mm->xMesh.VOF, ns[0]);
+        out.d("vof_y", mm->yMesh.VOF, ns[1]);
+        out.d("vof_z", mm->zMesh.VOF, ns[2]);
+        out.d("inv_mx", mm->xMesh.inv_VOF, ns[0]);
+        out.d("inv_my", mm->yMesh.inv_VOF, ns[1]);
+        out.d("inv_mz", mm->zMesh.inv_VOF, ns[2]);
+        out.d("dib_en", (const double*)mm->delta_ib_en, 3 * n);
+        out.d("dib_ws", (const double*)mm->delta_ib_ws, 3 * n);
+        out.d("dib_nb", (const double*)mm->delta_ib_nb, 3 * n);
+        out.d("dib_st", (const double*)mm->delta_ib_st, 3 * n);
+        out.d("inv_dib_ne", (const double*)mm->inv_delta_ib_ne, 3 * n);
+        out.d("inv_dib_tn", (const double*)mm->inv_delta_ib_tn, 3 * n);
+        out.d("vib", (const double*)mm->v_ib, 3 * n);
+        out.d("vibyx", (const double*)mm->v_ib_yx, 3 * n);
+        out.d("vibzy", (const double*)mm->v_ib_zy, 3 * n);
+        out.d("u_w", task->pU_W, (long)M * K);
+        double bc[18] = {task->U_W, task->U_E, task->U_S, task->U_N, task->U_B, task->U_T,
+                         task->V_W, task->V_E, task->V_S, task->V_N, task->V_B, task->V_T,
+                         task->W_W, task->W_E, task->W_S, task->W_N, task->W_B, task->W_T};
+        out.d("bc", bc, 18);
+        int pins[2] = {pE->A.fixPointNum, pE->A.fixPointFlowNum};
+        out.i("pins", pins, 2);
+        double par[8] = {task->nu, uE->coef, 1.0 / task->t, task->COEF_INTEGR_TIME, task->t, task->eps,
+                         task->V_BASE, (double)task->MAX_ITER};
+        out.d("nu_coef_coef2_integr_dt_eps_vbase_maxit", par, 8);
+        int rs[2] = {task->FGMRES_RESTART_NUM, task->FGMRES_RESTART_NUM_P};
+        out.i("restart_mom_p", rs, 2);
+        double *cu, *cv, *cw, *cp, *pu, *pv, *pw, *pp;
+        sol->current.getCopy(cu, cv, cw, cp);
+        sol->prediction.getCopy(pu, pv, pw, pp);
+        out.d("u_0", cu, ns[0]);
+        out.d("v_0", cv, ns[1]);
+        out.d("w_0", cw, ns[2]);
+        out.d("p_0", cp, n);
+        const int steps = (int)cfg.get("flow_steps", 0);
+        double curTime = 0.0;
+        for (int s = 1; s <= steps; s++) {
+            curTime += task->t;
+            sol->init();
+            task->rebuildMesh();
+            pE->m_A->calcFlux();
+            const std::string k = std::to_string(s);
+            out.d("lflux_" + k, pE->A.flux, n);
+            uE->solve();
+            vE->solve();
+            wE->solve();
+            pE->solve();
+            out.d("us_" + k, pu, ns[0]);
+            out.d("vs_" + k, pv, ns[1]);
+            out.d("ws_" + k, pw, ns[2]);
+            out.d("phi_" + k, pp, n);
+            int its[4] = {uE->solver.it, vE->solver.it, wE->solver.it, pE->solver.it};
+            out.i("its_" + k, its, 4);
+            sol->correction();
+            out.d("u_" + k, cu, ns[0]);
+            out.d("v_" + k, cv, ns[1]);
+            out.d("w_" + k, cw, ns[2]);
+            out.d("p_" + k, cp, n);
+        }
+        return 0;
+    }
     if ((int)cfg.get("helm", 0)) {
         // the momentum operators as the time step builds them
         // (HelmholtzDiscreteOperatorX/Y/Z::init -> build: calcFlux, calcHelm*,
