@@ -183,6 +183,14 @@ int lsg_momentum_rhs(lsg_ctx* ctx, int dir, const int* rowptr, const int* col, c
                      const double* hflux, const double* p, const double* prev_aux, double coef2, double* right,
                      double* aux);
 
+/* Device form of lsg_momentum_rhs without a CSR: conv holds flux2 + C u
+   (lsg_convective_apply_device with init = flux2), gp_work is a scratch
+   vector of the staggered grid (receives G p); right and aux as there; aux
+   may alias nothing else.  Device pointers. */
+int lsg_momentum_rhs_device(lsg_ctx* ctx, int dir, const double* conv, const double* u, const double* uprev,
+                            const double* vof, const double* hflux, const double* p, const double* prev_aux,
+                            double coef2, double* right, double* aux, double* gp_work);
+
 /* Convective operator of momentum component dir (0 x, 1 y, 2 z) applied
    from the geometry: out = init + C(u) v on the dir-grid, C the operator
    ConvectiveDiscreteOperatorX/Y/Z::calcConv* builds from the velocity

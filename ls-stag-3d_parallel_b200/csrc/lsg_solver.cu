@@ -2178,6 +2178,34 @@ int lsg_momentum_rhs(lsg_ctx* h, int dir, const int* rowptr, const int* col, con
     LSG_API_END(h)
 }
 
+int lsg_momentum_rhs_device(lsg_ctx* h, int dir, const double* conv, const double* u, const double* uprev,
+                            const double* vof, const double* hflux, const double* p, const double* prev_aux,
+                            double coef2, double* right, double* aux, double* gp_work)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z)");
+    LSG_REQUIRE(conv && u && uprev && vof && hflux && p && prev_aux && right && aux && gp_work, LSG_ERR_ARG,
+                "null argument");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const int Ns = d.N - (dir == 0), Ms = d.M - (dir == 1), Ks = d.K - (dir == 2);
+    const long long ns = (long long)Ns * Ms * Ks;
+    const Context::Geometry& g = C.geo;
+    k_gradient_apply<<<dim3((Ns + 31) / 32, (Ms + 7) / 8, Ks), dim3(32, 8), 0, C.s>>>(
+        dir, d.N, d.M, d.K, g.stype[dir].p, g.theta.p, g.delta.p, p, gp_work);
+    LSG_CHECK_LAUNCH();
+    k_momentum_rhs<<<grid_for(ns, 256), 256, 0, C.s>>>(ns, nullptr, nullptr, nullptr, conv, u, uprev, vof, hflux,
+                                                       prev_aux, gp_work, coef2, right, aux);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
 static void convective_apply(Context& C, int dir, const double* ux, const double* uy, const double* uz, const double* v,
                              const double* init, double* out, bool zquirk)
 {

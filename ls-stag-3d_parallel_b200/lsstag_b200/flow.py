@@ -100,3 +100,102 @@ class FlowStepper:
         for s in self.mom:
             s.close()
         self.pres.close()
+
+
+class FlowStepperDevice:
+    """The same time step with the state and every intermediate vector in
+    device memory (torch CUDA tensors as buffers, the library's *_device
+    entry points for the work): no host copies inside a step except the
+    iteration counts.  Same arguments as FlowStepper."""
+
+    def __init__(self, geom: dict, dims, par: dict, u0, v0, w0, p0, device: int = 0):
+        import ctypes as C
+        import torch
+        self.torch = torch
+        self.C = C
+        host = FlowStepper(geom, dims, par, u0, v0, w0, p0, device=device)
+        self.host = host                      # owns the contexts; its first state seeds this one
+        self.dims = host.dims
+        self.par = par
+        dev = torch.device("cuda", device)
+        f8 = dict(dtype=torch.float64, device=dev)
+        T = lambda a, **kw: torch.as_tensor(np.ascontiguousarray(a), device=dev, **kw).contiguous()  # noqa: E731
+        self.side_type = T(geom["side_type"], dtype=torch.int32)
+        self.vib = T(geom["vib"], dtype=torch.float64)
+        self.u_w = T(geom["u_w"], dtype=torch.float64)
+        self.theta = T(geom["theta"], dtype=torch.float64)
+        self.delta = T(geom["delta"], dtype=torch.float64)
+        self.vof = [T(geom["vof_" + c], dtype=torch.float64) for c in "xyz"]
+        self.hflux = [T(h, dtype=torch.float64) for h in host.hflux]
+        self.u = [T(a, dtype=torch.float64) for a in host.u]
+        self.uprev = [T(a, dtype=torch.float64) for a in host.uprev]
+        self.prev_aux = [T(a, dtype=torch.float64) for a in host.prev_aux]
+        self.p = T(host.p, dtype=torch.float64)
+        n = self.p.numel()
+        self.flux_lap = torch.empty(n, **f8)
+        self.b = torch.empty(n, **f8)
+        self.phi = torch.empty(n, **f8)
+        self.us = [torch.empty_like(a) for a in self.u]
+        self.unew = [torch.empty_like(a) for a in self.u]
+        self.flux2 = [torch.empty_like(a) for a in self.u]
+        self.conv = [torch.empty_like(a) for a in self.u]
+        self.right = [torch.empty_like(a) for a in self.u]
+        self.aux = [torch.empty_like(a) for a in self.u]
+        self.gp = [torch.empty_like(a) for a in self.u]
+        self.bc = np.ascontiguousarray(host.bc)
+        self.bc_lap = np.ascontiguousarray(host.bc_lap)
+        self.stats = None
+        torch.cuda.synchronize()
+
+    def _p(self, t):
+        return self.C.c_void_p(t.data_ptr())
+
+    def step(self):
+        from . import _lib as L
+        torch, C, par = self.torch, self.C, self.par
+        pres, mom = self.host.pres, self.host.mom
+        lib = pres.ctx.lib
+        N, M, K = self.dims
+        ck = pres.ctx.check
+        ck(lib.lsg_laplace_flux_device(pres.ctx.h, self._p(self.side_type), self._p(self.vib), self._p(self.u_w),
+                                       L.dptr(self.bc_lap), self._p(self.u[0]), self._p(self.flux_lap)))
+        its = []
+        for d in range(3):
+            m = mom[d]
+            m.ctx.check(lib.lsg_convective_flux_device(m.ctx.h, d, N, M, K, self._p(self.theta), self._p(self.delta),
+                                                       self._p(self.u[0]), self._p(self.u[1]), self._p(self.u[2]),
+                                                       self._p(self.u_w), L.dptr(self.bc), self._p(self.flux2[d])))
+            ck(lib.lsg_convective_apply_device(pres.ctx.h, d, self._p(self.u[0]), self._p(self.u[1]),
+                                               self._p(self.u[2]), self._p(self.u[d]), self._p(self.flux2[d]),
+                                               self._p(self.conv[d]), 1))
+            ck(lib.lsg_momentum_rhs_device(pres.ctx.h, d, self._p(self.conv[d]), self._p(self.u[d]),
+                                           self._p(self.uprev[d]), self._p(self.vof[d]), self._p(self.hflux[d]),
+                                           self._p(self.p), self._p(self.prev_aux[d]), float(par["coef2"]),
+                                           self._p(self.right[d]), self._p(self.aux[d]), self._p(self.gp[d])))
+            self.prev_aux[d], self.aux[d] = self.aux[d], self.prev_aux[d]
+            self.us[d].copy_(self.u[d])
+            torch.cuda.synchronize()
+            st = L.Stats()
+            rc = lib.lsg_solve_device(m.ctx.h, self._p(self.right[d]), self._p(self.us[d]), C.byref(st))
+            m.ctx.check(rc)
+            its.append(st.iterations)
+        ck(lib.lsg_projection_rhs_device(pres.ctx.h, self._p(self.us[0]), self._p(self.us[1]), self._p(self.us[2]),
+                                         self._p(self.flux_lap), self._p(self.b)))
+        self.phi.zero_()
+        torch.cuda.synchronize()
+        st = L.Stats()
+        ck(lib.lsg_solve_device(pres.ctx.h, self._p(self.b), self._p(self.phi), C.byref(st)))
+        its.append(st.iterations)
+        ck(lib.lsg_projection_correct_device(pres.ctx.h, self._p(self.phi), self._p(self.us[0]), self._p(self.us[1]),
+                                             self._p(self.us[2]), self._p(self.unew[0]), self._p(self.unew[1]),
+                                             self._p(self.unew[2]), self._p(self.p), float(par["coef"]),
+                                             float(par["vbase"]), 1))
+        # previous <- current, current <- corrected (buffer rotation)
+        self.uprev, self.u, self.unew = self.u, self.unew, self.uprev
+        return its
+
+    def state(self):
+        return [a.cpu().numpy() for a in self.u], self.p.cpu().numpy()
+
+    def close(self):
+        self.host.close()
