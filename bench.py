@@ -178,6 +178,87 @@ def run_reference_arm(args, world, rank):
     return 0
 
 
+FLOW_METRIC = "Flow past a sphere 128x64x64 FP64 (C0): ms per time step on 1 B200"
+
+
+def reference_flow_steps(steps, threads):
+    """The reference's own time step (oracle/_ref, TimeSteppingMethodInterface::
+    step order) on the flow case: per-step seconds and iteration counts."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner as rr
+    h = 1.0 / 16
+    case = rr.Case(128, 64, 64, h, h, h, spheres=[(2.0, 2.0 + 0.5 * h, 2.0 + 0.5 * h, 0.5)])
+    r = rr.run(case, threads=threads, flow_steps=steps, flow_no_dump=1, restart=30, dump_geometry=0, timeout=3600)
+    return [1e3 * t for t in r["step_s"]], [r[f"its_{k}"].tolist() for k in range(1, steps + 1)], int(r["omp_threads"][0])
+
+
+def run_flow(args, world, rank, local, pg):
+    """One step = one time step of the flow past a sphere (momentum equations,
+    pressure equation, projection) with every operator on the GPU."""
+    import torch
+
+    from lsstag_b200 import cases
+    from lsstag_b200.flow import FlowStepper, FlowStepperDevice
+    cfg = {"workload": "flow_sphere_128x64x64_fp64_dt0.01_Re100", "grid": [128, 64, 64],
+           "bodies": "sphere D=1 at (2, 2+h/2, 2+h/2) in [0,8]x[0,4]x[0,4]",
+           "solvers": "momentum ILU(0)-FGMRES(13), pressure MG-FGMRES(30), absolute eps 1e-5 (reference defaults)",
+           "l2": "state and operators larger than L2", "parallelism": "replicas" if world > 1 else "single GPU"}
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        threads = os.cpu_count() or 1
+        ms, its, th = reference_flow_steps(args.warmup + args.steps, threads)
+        timed = ms[args.warmup:] if len(ms) > args.warmup else ms
+        v = sum(timed) / len(timed)
+        print(json.dumps({"impl": "reference", "metric": FLOW_METRIC, "value": v, "unit": "ms/step", "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": cfg, "iterations_last": its[-1],
+                          "cpu_baseline": {"value": v, "unit": "ms/step", "cores": th, "kind": "reference",
+                                           "sample": f"{len(timed)} time steps after {args.warmup}"},
+                          "e2e": {"value": v, "unit": "ms/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return 0
+    torch.cuda.set_device(local)
+    g, dims, par, (u0, v0, w0, p0) = cases.load_flow_case()
+    fs = FlowStepperDevice(g, dims, par, u0, v0, w0, p0, device=local)
+    for _ in range(args.warmup):
+        fs.step()
+    barrier(pg)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    its = [fs.step() for _ in range(args.steps)]
+    t1.record()
+    torch.cuda.synchronize()
+    ms = barrier_max(pg, t0.elapsed_time(t1), local) / args.steps
+    fs.close()
+    # end to end through the host-array entry points (every vector copied in and out)
+    fh = FlowStepper(g, dims, par, u0, v0, w0, p0, device=local)
+    fh.step()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        fh.step()
+    e2e = barrier_max(pg, 1e3 * (time.perf_counter() - t), local) / args.steps
+    fh.close()
+    out = {"metric": FLOW_METRIC, "value": ms, "unit": "ms/step", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg, "iterations_last": its[-1],
+           "e2e": {"value": e2e, "unit": "ms/step", "note": "host-array entry points, every operand copied"}}
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            ref_ms, ref_its, th = reference_flow_steps(3, os.cpu_count() or 1)
+            out["cpu_baseline"] = {"value": sum(ref_ms[1:]) / 2, "unit": "ms/step", "cores": th, "kind": "reference",
+                                   "iterations_last": ref_its[-1],
+                                   "sample": "time steps 2-3 of the same case (reference OpenMP build)"}
+        except Exception as e:  # report, do not hide
+            out["cpu_baseline"] = {"error": str(e)}
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
 def config_dict(args, world):
     return {"workload": f"poisson_spheres4_{args.size}^3_mgfgmres30_rel1e-10",
             "grid": [args.size] * 3, "bodies": "4 seeded spheres (seed 3), Neumann walls, 2 pinned rows",
@@ -205,9 +286,17 @@ def main():
                     help="Gram-Schmidt form of both arms: the low-synchronisation form of the MGS "
                          "projections (default; two passes over the basis per step) or the reference's "
                          "pass-per-vector MGS")
+    ap.add_argument("--workload", default="poisson", choices=["poisson", "flow"],
+                    help="poisson: the 256^3 pressure solve (the headline); flow: time steps of the flow past "
+                         "a sphere at 128x64x64 (every operator of the step on the GPU)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
     world, rank, local, pg = dist_setup(args)
+    if args.workload == "flow":
+        rc = run_flow(args, world, rank, local, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return rc
     if args.impl == "reference":
         rc = run_reference_arm(args, world, rank)
         if pg is not None:

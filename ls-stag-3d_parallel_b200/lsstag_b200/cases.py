@@ -60,3 +60,31 @@ def load(n: int, seed: int = 3):
     ct = np.where(celltype, 0, 1)
     b = synth.poisson_rhs(seed, ct, pins, mask)
     return P, dims, pins, b
+
+
+# --------------------------------------------------------------------------
+# Flow past a sphere (the plain FP64 LS-STAG flow case): every mesh array of
+# the time step, stored sparsely (most frequent value + exceptions) by
+# cases/make_flow_case.py
+# --------------------------------------------------------------------------
+def flow_case_path() -> str:
+    return os.path.join(CASE_DIR, "flow_sphere_128x64x64.npz")
+
+
+def load_flow_case(path: str | None = None):
+    """(mesh arrays, dims, params, (u0, v0, w0, p0)) of the flow case, in the
+    form lsstag_b200.flow.FlowStepper takes them."""
+    z = np.load(path or flow_case_path())
+    g = {}
+    for k in z.files:
+        if k.endswith("__mode"):
+            name = k[:-6]
+            a = np.full(int(z[name + "__n"]), z[k], dtype=z[k].dtype)
+            a[z[name + "__idx"]] = z[name + "__val"]
+            g[name] = a
+        elif "__" not in k:
+            g[k] = z[k]
+    nu, coef, coef2, integr, dt, eps, vbase, maxit = (float(v) for v in g["nu_coef_coef2_integr_dt_eps_vbase_maxit"])
+    par = dict(nu=nu, coef=coef, coef2=coef2, coef_integr=integr, dt=dt, eps=eps, vbase=vbase, max_it=int(maxit),
+               restart_mom=int(g["restart_mom_p"][0]), restart_p=int(g["restart_mom_p"][1]))
+    return g, tuple(int(v) for v in g["dims"]), par, (g["u_0"], g["v_0"], g["w_0"], g["p_0"])

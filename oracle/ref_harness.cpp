@@ -458,7 +458,7 @@ int main(int argc, char** argv)
             mm->v_ib[i].set(0.1 * sin(0.11 * i), 0.1 * cos(0.13 * i), 0.05 * sin(0.17 * i));
         for (long i = 0; i < (long)mm->xMesh.NMK; i++) mm->m_Ux[i] = 1.0 + 0.2 * sin(0.29 * i);
     }
-    if ((int)cfg.get("flow_steps", 0)) {
+    if ((int)cfg.get("flow_steps", 0) || (int)cfg.get("flow_setup", 0)) {
         // whole time steps of the flow task as TimeSteppingMethodInterface::init
         // and ::step run them (time_stepping_method_interface.h:150-214: the
         // three momentum equations, the pressure equation, the projection),
@@ -528,29 +528,39 @@ int main(int argc, char** argv)
         out.d("p_0", cp, n);
         const int steps = (int)cfg.get("flow_steps", 0);
         double curTime = 0.0;
+        std::vector<double> step_s;
         for (int s = 1; s <= steps; s++) {
+            const double t_step = now_s();
             curTime += task->t;
             sol->init();
             task->rebuildMesh();
             pE->m_A->calcFlux();
             const std::string k = std::to_string(s);
-            out.d("lflux_" + k, pE->A.flux, n);
+            const bool dump = !(int)cfg.get("flow_no_dump", 0);   // timing runs write nothing inside the step
+            if (dump) out.d("lflux_" + k, pE->A.flux, n);
             uE->solve();
             vE->solve();
             wE->solve();
             pE->solve();
-            out.d("us_" + k, pu, ns[0]);
-            out.d("vs_" + k, pv, ns[1]);
-            out.d("ws_" + k, pw, ns[2]);
-            out.d("phi_" + k, pp, n);
+            if (dump) {
+                out.d("us_" + k, pu, ns[0]);
+                out.d("vs_" + k, pv, ns[1]);
+                out.d("ws_" + k, pw, ns[2]);
+                out.d("phi_" + k, pp, n);
+            }
             int its[4] = {uE->solver.it, vE->solver.it, wE->solver.it, pE->solver.it};
             out.i("its_" + k, its, 4);
             sol->correction();
+            step_s.push_back(now_s() - t_step);
+            if (!dump) continue;
             out.d("u_" + k, cu, ns[0]);
             out.d("v_" + k, cv, ns[1]);
             out.d("w_" + k, cw, ns[2]);
             out.d("p_" + k, cp, n);
         }
+        out.d("step_s", step_s.data(), (long)step_s.size());
+        int nthreads = omp_get_max_threads();
+        out.i("omp_threads", &nthreads, 1);
         return 0;
     }
     if ((int)cfg.get("helm", 0)) {
