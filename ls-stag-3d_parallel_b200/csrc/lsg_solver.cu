@@ -204,6 +204,10 @@ struct Context {
     // ILU(0)
     DevBuf<double> iluL, iluU;        // 3 lower planes (b s w) / 4 planes (p e n t), U diagonal = plane 0
     bool have_ilu = false;
+    // the level-scheduled ILU(0) solves as one CUDA graph (instantiated on
+    // first use, reading ilu_in and writing ilu_out)
+    cudaGraphExec_t ilu_exec = nullptr;
+    DevBuf<double> ilu_in, ilu_out;
     double bytes = 0;
     int vcycles = 0;
     bool own_stream = true;
@@ -244,6 +248,7 @@ struct lsg_ctx {
 namespace lsg {
 
 static void ilu_apply(Context& C, const double* b, double* x);
+static void ilu_graph_release(Context& C);
 
 // ---------------------------------------------------------------------------
 // row dictionary of an operator given as noff coefficient planes
@@ -1247,6 +1252,7 @@ static void ilu_setup(Context& C)
     const Dims& d = C.d;
     LSG_REQUIRE(d.N >= 3 && d.M >= 3 && d.K >= 3, LSG_ERR_ARG, "ILU(0) needs N, M, K >= 3");
     const long long n = C.n;
+    ilu_graph_release(C);              // factors and work buffers may move
     C.iluU.alloc(n);
     C.iluL.alloc(3 * n);
     const int planes = d.N + d.M + d.K - 2;
@@ -1262,7 +1268,7 @@ static void ilu_setup(Context& C)
 }
 
 // x = U^{-1} L^{-1} b ; uses C.t4 for the intermediate
-static void ilu_apply(Context& C, const double* b, double* x)
+static void ilu_sweeps(Context& C, const double* b, double* x)
 {
     const Dims& d = C.d;
     const int planes = d.N + d.M + d.K - 2;
@@ -1272,7 +1278,46 @@ static void ilu_apply(Context& C, const double* b, double* x)
         k_ilu_fwd<<<blocks, 256, 0, C.s>>>(lv, d.N, d.M, d.K, C.iluL.p, b, y);
     for (int lv = planes - 1; lv >= 0; lv--)
         k_ilu_bwd<<<blocks, 256, 0, C.s>>>(lv, d.N, d.M, d.K, C.A7.p, C.iluU.p, y, x);
-    LSG_CHECK_LAUNCH();
+}
+
+static void ilu_graph_release(Context& C)
+{
+    if (C.ilu_exec) cudaGraphExecDestroy(C.ilu_exec);
+    C.ilu_exec = nullptr;
+}
+
+// The 2 (N + M + K - 2) hyperplane launches of one application are replayed
+// as one CUDA graph: b is copied into a fixed input buffer, the graph runs,
+// the result is copied out (two device copies of n values against hundreds
+// of launch submissions).  A context on the legacy default stream launches
+// the sweeps directly.
+static void ilu_apply(Context& C, const double* b, double* x)
+{
+    if (!C.s) {
+        ilu_sweeps(C, b, x);
+        LSG_CHECK_LAUNCH();
+        return;
+    }
+    const long long n = C.n;
+    if (!C.ilu_exec) {
+        C.ilu_in.alloc(n);
+        C.ilu_out.alloc(n);
+        cudaGraph_t graph = nullptr;
+        LSG_CUDA(cudaStreamBeginCapture(C.s, cudaStreamCaptureModeThreadLocal));
+        ilu_sweeps(C, C.ilu_in.p, C.ilu_out.p);
+        const cudaError_t launch_err = cudaGetLastError();
+        const cudaError_t cap_err = cudaStreamEndCapture(C.s, &graph);
+        LSG_CUDA(launch_err);
+        LSG_CUDA(cap_err);
+        const cudaError_t inst_err = cudaGraphInstantiate(&C.ilu_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (inst_err != cudaSuccess) C.ilu_exec = nullptr;
+        LSG_CUDA(inst_err);
+    }
+    LSG_CUDA(cudaMemcpyAsync(C.ilu_in.p, b, n * sizeof(double), cudaMemcpyDeviceToDevice, C.s));
+    LSG_CUDA(cudaGraphLaunch(C.ilu_exec, C.s));
+    ::lsg::g_launches++;
+    LSG_CUDA(cudaMemcpyAsync(x, C.ilu_out.p, n * sizeof(double), cudaMemcpyDeviceToDevice, C.s));
 }
 
 // ---------------------------------------------------------------------------
@@ -1436,6 +1481,7 @@ static cudaStream_t context_release(Context& C)
         C.adj.reset();
     }
     if (C.s) cudaStreamSynchronize(C.s);
+    ilu_graph_release(C);
     if (C.hflag) cudaFreeHost(C.hflag);
     C.hflag = nullptr;
     if (C.ev0) cudaEventDestroy(C.ev0);
@@ -2344,6 +2390,7 @@ int lsg_setup(lsg_ctx* h, const lsg_options* opts)
     Context& C = h->c;
     LSG_REQUIRE(C.have_matrix, LSG_ERR_STATE, "lsg_set_matrix_csr must be called before lsg_setup");
     LSG_CUDA(cudaSetDevice(C.device));
+    ilu_graph_release(C);                  // work buffers are (re)allocated below
     if (opts) C.opt = *opts;
     LSG_REQUIRE(C.opt.method == LSG_METHOD_FGMRES || C.opt.method == LSG_METHOD_BICGSTAB, LSG_ERR_ARG, "bad method");
     LSG_REQUIRE(C.opt.precond >= 0 && C.opt.precond <= 2, LSG_ERR_ARG, "bad preconditioner");
