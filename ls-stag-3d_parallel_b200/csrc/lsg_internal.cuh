@@ -29,7 +29,7 @@ struct Error {
 
 // every kernel launch of the library is followed by this check, which also
 // counts launches (reported per solve in lsg_stats.kernel_launches)
-extern long long g_launches;
+extern thread_local long long g_launches;
 #define LSG_CHECK_LAUNCH()              \
     do {                                \
         ::lsg::g_launches++;            \

@@ -19,7 +19,7 @@
 
 namespace lsg {
 
-long long g_launches = 0;
+thread_local long long g_launches = 0;   // per host thread: solves on different contexts may run concurrently
 
 // ---------------------------------------------------------------------------
 // host-side tables and helpers

@@ -145,6 +145,8 @@ class FlowStepperDevice:
         self.bc = np.ascontiguousarray(host.bc)
         self.bc_lap = np.ascontiguousarray(host.bc_lap)
         self.stats = None
+        from concurrent.futures import ThreadPoolExecutor
+        self.pool = ThreadPoolExecutor(max_workers=3)
         torch.cuda.synchronize()
 
     def _p(self, t):
@@ -159,7 +161,6 @@ class FlowStepperDevice:
         ck = pres.ctx.check
         ck(lib.lsg_laplace_flux_device(pres.ctx.h, self._p(self.side_type), self._p(self.vib), self._p(self.u_w),
                                        L.dptr(self.bc_lap), self._p(self.u[0]), self._p(self.flux_lap)))
-        its = []
         for d in range(3):
             m = mom[d]
             m.ctx.check(lib.lsg_convective_flux_device(m.ctx.h, d, N, M, K, self._p(self.theta), self._p(self.delta),
@@ -174,11 +175,17 @@ class FlowStepperDevice:
                                            self._p(self.right[d]), self._p(self.aux[d]), self._p(self.gp[d])))
             self.prev_aux[d], self.aux[d] = self.aux[d], self.prev_aux[d]
             self.us[d].copy_(self.u[d])
-            torch.cuda.synchronize()
-            st = L.Stats()
-            rc = lib.lsg_solve_device(m.ctx.h, self._p(self.right[d]), self._p(self.us[d]), C.byref(st))
-            m.ctx.check(rc)
-            its.append(st.iterations)
+        torch.cuda.synchronize()
+        # the three momentum systems are independent given the current state:
+        # solved concurrently, each on its own context and stream (the calls
+        # release the interpreter lock while they wait on the device)
+        stats = [L.Stats() for _ in range(3)]
+        futs = [self.pool.submit(lib.lsg_solve_device, mom[d].ctx.h, self._p(self.right[d]), self._p(self.us[d]),
+                                 C.byref(stats[d])) for d in range(3)]
+        its = []
+        for d in range(3):
+            mom[d].ctx.check(futs[d].result())
+            its.append(stats[d].iterations)
         ck(lib.lsg_projection_rhs_device(pres.ctx.h, self._p(self.us[0]), self._p(self.us[1]), self._p(self.us[2]),
                                          self._p(self.flux_lap), self._p(self.b)))
         self.phi.zero_()
@@ -198,4 +205,5 @@ class FlowStepperDevice:
         return [a.cpu().numpy() for a in self.u], self.p.cpu().numpy()
 
     def close(self):
+        self.pool.shutdown()
         self.host.close()
