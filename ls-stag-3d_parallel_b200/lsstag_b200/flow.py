@@ -63,6 +63,7 @@ class FlowStepper:
         # HelmholtzDiscreteEquation::set: previous velocity = current, history
         # = flux2 + C(u) u of the initial state
         self.uprev = [a.copy() for a in self.u]
+        self.pprev = self.p.copy()
         self.prev_aux = [self._convective_term(d) for d in range(3)]
         self.its = None
 
@@ -87,6 +88,7 @@ class FlowStepper:
         phi = np.zeros_like(self.p)
         its.append(self.pres.solve(b, phi))
         self.uprev = [a.copy() for a in self.u]
+        self.pprev = self.p.copy()
         p = self.p.copy()
         u, v, w, _ = self.pres.projection_correct(phi, us[0], us[1], us[2], p, par["coef"], par["vbase"])
         self.u = [u, v, w]
@@ -95,6 +97,27 @@ class FlowStepper:
         self.predictions = us
         self.phi = phi
         return its
+
+    def save_state(self, path: str, it: int, time: float, centers, center_velocities, loads):
+        """Write the reference's continue-state file (lsstag_b200.state) for
+        this state; centers / center_velocities / loads per immersed body."""
+        from .state import FlowState, write_state
+        write_state(path, FlowState(int(it), float(time), np.asarray(centers, np.float64).reshape(-1, 3),
+                                    np.asarray(center_velocities, np.float64).reshape(-1, 3),
+                                    np.asarray(loads, np.float64).reshape(-1, 4),
+                                    (self.u[0], self.u[1], self.u[2], self.p),
+                                    (self.uprev[0], self.uprev[1], self.uprev[2], self.pprev)))
+
+    @classmethod
+    def from_state(cls, geom: dict, dims, par: dict, path: str, n_bodies: int = 1, device: int = 0):
+        """Continue from a continue-state file as the reference does
+        (TimeSteppingMethodInterface::init with continueSolveTask: the
+        equations are set up on the loaded current state, which also becomes
+        the previous one).  Returns (stepper, FlowState)."""
+        from .state import read_state
+        st = read_state(path, dims, n_bodies)
+        u, v, w, p = st.current
+        return cls(geom, dims, par, u, v, w, p, device=device), st
 
     def close(self):
         for s in self.mom:

@@ -28,6 +28,7 @@
 #include "Base/Solvers/BiCGStab/ilu_bicgstab.h"
 #include <chrono>
 #include <fstream>
+#include <filesystem>
 #include <map>
 #include <random>
 #include <sstream>
@@ -527,7 +528,6 @@ int main(int argc, char** argv)
         out.d("w_0", cw, ns[2]);
         out.d("p_0", cp, n);
         const int steps = (int)cfg.get("flow_steps", 0);
-        double curTime = 0.0;
         std::vector<double> step_s;
         for (int s = 1; s <= steps; s++) {
             const double t_step = now_s();
@@ -552,6 +552,7 @@ int main(int argc, char** argv)
             out.i("its_" + k, its, 4);
             sol->correction();
             step_s.push_back(now_s() - t_step);
+            if (s < steps) it++;
             if (!dump) continue;
             out.d("u_" + k, cu, ns[0]);
             out.d("v_" + k, cv, ns[1]);
@@ -559,6 +560,20 @@ int main(int argc, char** argv)
             out.d("p_" + k, cp, n);
         }
         out.d("step_s", step_s.data(), (long)step_s.size());
+        if ((int)cfg.get("save_state", 0)) {
+            // the reference's own continue-state file (SetSolutions::saveState,
+            // set_solutions.h:318-337), returned byte for byte
+            sol->saveState();
+            std::string found;
+            for (const auto& e : std::filesystem::directory_iterator(outdir))
+                if (e.path().filename().string().rfind("continueSolveTask__", 0) == 0) found = e.path().string();
+            std::ifstream sf(found, std::ios::binary);
+            std::vector<char> bytes((std::istreambuf_iterator<char>(sf)), std::istreambuf_iterator<char>());
+            out.put("state_bytes", (const unsigned char*)bytes.data(), (long)bytes.size(), "u1");
+            int itc = it;
+            out.i("state_it", &itc, 1);
+            out.scalar("state_time", curTime);
+        }
         int nthreads = omp_get_max_threads();
         out.i("omp_threads", &nthreads, 1);
         return 0;

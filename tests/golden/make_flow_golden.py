@@ -11,6 +11,9 @@ equations, pressure equation, projection) with absolute solver tolerance
 1e-11 and no start-up pressure scaling; every mesh array the GPU path reads,
 the initial state, and per step the predicted velocities, the pressure
 correction, the iteration counts and the new state.
+
+flow16_state.npz: the reference's own continue-state file
+(SetSolutions::saveState) after the first two of those steps, byte for byte.
 """
 from __future__ import annotations
 
@@ -34,6 +37,11 @@ def main():
     r = rr.run(case, threads=1, flow_steps=3, task_eps=1e-11, restart=30, dump_geometry=0)
     np.savez_compressed(os.path.join(HERE, "flow16_steps.npz"), **r)
     print("flow16_steps.npz", os.path.getsize(os.path.join(HERE, "flow16_steps.npz")))
+    # the reference's continue-state file after two of those steps
+    s = rr.run(case, threads=1, flow_steps=2, task_eps=1e-11, restart=30, dump_geometry=0, save_state=1)
+    np.savez_compressed(os.path.join(HERE, "flow16_state.npz"), state_bytes=s["state_bytes"],
+                        state_it=s["state_it"], state_time=s["state_time"])
+    print("flow16_state.npz", os.path.getsize(os.path.join(HERE, "flow16_state.npz")))
 
 
 if __name__ == "__main__":
