@@ -32,7 +32,7 @@ class FlowStepper:
     par: nu, coef (1.5/dt), coef2 (1/dt), coef_integr (COEF_INTEGR_TIME), eps
     (absolute), vbase, max_it, restart_mom, restart_p."""
 
-    def __init__(self, geom: dict, dims, par: dict, u0, v0, w0, p0, device: int = 0):
+    def __init__(self, geom: dict, dims, par: dict, u0, v0, w0, p0, device: int = 0, pressure_mg_fp32: bool = False):
         self.g = geom
         self.dims = tuple(int(v) for v in dims)
         self.par = par
@@ -42,7 +42,10 @@ class FlowStepper:
         # U_E, V_S, V_N, W_B, W_T of the pressure equation's source term
         self.bc_lap = bc[[1, 8, 9, 16, 17]].copy()
         ptask = S.Task(eps=par["eps"], MAX_ITER=int(par["max_it"]), FGMRES_RESTART_NUM=int(par["restart_p"]))
-        self.pres = S.MGFGMRES(device=device)
+        # pressure solve: MG-FGMRES, optionally with the FP32 multigrid inside
+        # the FP64 FGMRES (the mixed-precision preconditioner)
+        from . import _lib as L
+        self.pres = S.MGFGMRES(device=device, mg_precision=L.FP32 if pressure_mg_fp32 else L.FP64)
         self.pres.set_geometry({k: geom[k] for k in ("celltype", "theta", "delta", "inv_mx", "inv_my", "inv_mz")},
                                self.dims, geom["pins"], task=ptask)
         self.pres.set_staggered_types(geom["xtype"], geom["ytype"], geom["ztype"])
@@ -131,12 +134,12 @@ class FlowStepperDevice:
     entry points for the work): no host copies inside a step except the
     iteration counts.  Same arguments as FlowStepper."""
 
-    def __init__(self, geom: dict, dims, par: dict, u0, v0, w0, p0, device: int = 0):
+    def __init__(self, geom: dict, dims, par: dict, u0, v0, w0, p0, device: int = 0, pressure_mg_fp32: bool = False):
         import ctypes as C
         import torch
         self.torch = torch
         self.C = C
-        host = FlowStepper(geom, dims, par, u0, v0, w0, p0, device=device)
+        host = FlowStepper(geom, dims, par, u0, v0, w0, p0, device=device, pressure_mg_fp32=pressure_mg_fp32)
         self.host = host                      # owns the contexts; its first state seeds this one
         self.dims = host.dims
         self.par = par
