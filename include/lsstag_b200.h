@@ -320,6 +320,22 @@ int lsg_loads_adjoint(lsg_ctx* ctx, const double* weight, const double* nu_cell,
 int lsg_loads_adjoint_device(lsg_ctx* ctx, const double* weight, const double* nu_cell, double nu,
                              double* g_ux, double* g_uy, double* g_uz, double* g_p);
 
+/* Transposed Jacobian of the convective term out = init + C(U) v of
+   lsg_convective_apply: for a cotangent lam on the dir-grid, the gradients
+   of <lam, C(U) v> with respect to the three velocity grids (ux_bar, uy_bar,
+   uz_bar) and to v (v_bar).  No reference counterpart (the reference has no
+   adjoint); it is the nonlinear part of the momentum step's adjoint.  Host
+   pointers, outputs overwritten. */
+int lsg_convective_adjoint(lsg_ctx* ctx, int dir, const double* ux, const double* uy, const double* uz,
+                           const double* v, const double* lam, double* ux_bar, double* uy_bar, double* uz_bar,
+                           double* v_bar, int zconv_reference);
+/* Same on device pointers; the outputs accumulate (zero them first; for the
+   equation's own velocity v = U_dir the same buffer may serve as v_bar and
+   the dir component of U_bar). */
+int lsg_convective_adjoint_device(lsg_ctx* ctx, int dir, const double* ux, const double* uy, const double* uz,
+                                  const double* v, const double* lam, double* ux_bar, double* uy_bar, double* uz_bar,
+                                  double* v_bar, int zconv_reference);
+
 /* Staggered cell types (LSSTAGUniformMesh xMesh/yMesh/zMesh typeOfCell),
    needed by the staggered-grid entry points below.  Checked on the host like
    the base types (a kept face must lie inside the grid).  Host pointers. */

@@ -390,6 +390,83 @@ __global__ void __launch_bounds__(256) k_convective_apply(int d, int N, int M, i
     out[f] = acc;
 }
 
+// Transposed Jacobian of the convective term out = init + C(U) v
+// (k_convective_apply): out is bilinear in (U, v), so for a cotangent lam on
+// the d-grid
+//   v_bar[f + col_k]  += lam_f coef_k(U)
+//   U_bar[e][face]    += lam_f v[f + col_k] dcoef_k/dU_e[face]
+// for every face k of every non-solid row f, with the same face model,
+// absent faces and z-operator x-velocity indexing as the forward kernel.
+// Contributions of neighbouring rows meet in one unknown, so they are added
+// with atomics (their order is not fixed).  The outputs accumulate; for the
+// momentum equation's own velocity (v = U_d) pass the same buffer for v_bar
+// and U_bar[d].
+__global__ void __launch_bounds__(256) k_convective_adjoint(int d, int N, int M, int K, const int* __restrict__ stype,
+                                                            const double* __restrict__ theta,
+                                                            const double* __restrict__ delta,
+                                                            const double* __restrict__ Ux,
+                                                            const double* __restrict__ Uy,
+                                                            const double* __restrict__ Uz,
+                                                            const double* __restrict__ v,
+                                                            const double* __restrict__ lam, bool zquirk,
+                                                            double* Ux_bar, double* Uy_bar, double* Uz_bar,
+                                                            double* v_bar)
+{
+    const int Nd = N - (d == 0), Md = M - (d == 1);
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= Nd || y >= Md) return;
+    const long long f = x + (long long)Nd * (y + (long long)Md * z);
+    const int t = stype[f];
+    const double lf = lam[f];
+    if (t == 0 || lf == 0.0) return;
+    const long long NM = (long long)N * M;
+    const long long step[3] = {1, N, NM};
+    const long long P = x + (long long)N * (y + (long long)M * z), Q = P + step[d];
+    const int qx = x + (d == 0), qy = y + (d == 1), qz = z + (d == 2);
+    const double* U[3] = {Ux, Uy, Uz};
+    double* Ub[3] = {Ux_bar, Uy_bar, Uz_bar};
+    const long long dstride = d == 0 ? 1 : (d == 1 ? Nd : (long long)Nd * Md);
+    const long long cols[6] = {-(long long)Nd * Md, -Nd, -1, 1, Nd, (long long)Nd * Md};
+    const int fdir[6] = {2, 1, 0, 0, 1, 2};
+    const int miss = absent_faces(t);
+    for (int k = 0; k < 6; k++) {
+        if (miss & (1 << k)) continue;
+        const bool upper = k >= 3;
+        const int e = fdir[k];
+        const double sgn = upper ? 0.25 : -0.25;
+        const double vk = v[f + cols[k]];
+        const double lv = lf * vk;
+        double coef;
+        if (e == d) {
+            const int o0 = d == 0 ? 1 : 0, o1 = d == 2 ? 1 : 2;
+            const double area = delta[3 * P + o0] * delta[3 * P + o1];
+            const double th1 = theta[3 * P + d];
+            const double th2 = upper ? theta[3 * Q + d] : theta[3 * (P - step[d]) + d];
+            const long long f2 = upper ? f + dstride : f - dstride;
+            coef = sgn * area * (th1 * U[d][f] + th2 * U[d][f2]);
+            atomicAdd(Ub[d] + f, lv * sgn * area * th1);
+            atomicAdd(Ub[d] + f2, lv * sgn * area * th2);
+        } else {
+            const int third = 3 - d - e;
+            const double h = delta[3 * P + third];
+            const long long pc = upper ? P : P - step[e], qc = upper ? Q : Q - step[e];
+            const int px = x - (!upper && e == 0), py = y - (!upper && e == 1), pz = z - (!upper && e == 2);
+            const int cx = qx - (!upper && e == 0), cy = qy - (!upper && e == 1), cz = qz - (!upper && e == 2);
+            const long long shift = (zquirk && d == 2 && e == 0) ? z : 0;
+            const long long fp = face_index(e, N, M, px, py, pz) - shift;
+            const long long fq = face_index(e, N, M, cx, cy, cz) - shift;
+            const double ca = sgn * h * delta[3 * P + d] * theta[3 * pc + e];
+            const double cb = sgn * h * delta[3 * Q + d] * theta[3 * qc + e];
+            coef = ca * U[e][fp] + cb * U[e][fq];
+            atomicAdd(Ub[e] + fp, lv * ca);
+            atomicAdd(Ub[e] + fq, lv * cb);
+        }
+        atomicAdd(v_bar + f + cols[k], lf * coef);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Adjoint of the projection (outflow clamps off):
 //   b = Pi (Dx u + Dy v + Dz w + flux),  A phi = b,

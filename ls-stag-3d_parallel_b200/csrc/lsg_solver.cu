@@ -2263,6 +2263,73 @@ static void convective_apply(Context& C, int dir, const double* ux, const double
     LSG_CHECK_LAUNCH();
 }
 
+int lsg_convective_adjoint_device(lsg_ctx* h, int dir, const double* ux, const double* uy, const double* uz,
+                                  const double* v, const double* lam, double* ux_bar, double* uy_bar, double* uz_bar,
+                                  double* v_bar, int zconv_reference)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z)");
+    LSG_REQUIRE(ux && uy && uz && v && lam && ux_bar && uy_bar && uz_bar && v_bar, LSG_ERR_ARG, "null argument");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const Context::Geometry& g = C.geo;
+    const int Ns = d.N - (dir == 0), Ms = d.M - (dir == 1), Ks = d.K - (dir == 2);
+    k_convective_adjoint<<<dim3((Ns + 31) / 32, (Ms + 7) / 8, Ks), dim3(32, 8), 0, C.s>>>(
+        dir, d.N, d.M, d.K, g.stype[dir].p, g.theta.p, g.delta.p, ux, uy, uz, v, lam, zconv_reference != 0, ux_bar,
+        uy_bar, uz_bar, v_bar);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_convective_adjoint(lsg_ctx* h, int dir, const double* ux, const double* uy, const double* uz,
+                           const double* v, const double* lam, double* ux_bar, double* uy_bar, double* uz_bar,
+                           double* v_bar, int zconv_reference)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z)");
+    LSG_REQUIRE(ux && uy && uz && v && lam && ux_bar && uy_bar && uz_bar && v_bar, LSG_ERR_ARG, "null argument");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const long long cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
+                              (long long)d.N * d.M * (d.K - 1)};
+    DevBuf<double> du[3], db[3], dv, dl, dvb;
+    const double* hu[3] = {ux, uy, uz};
+    for (int e = 0; e < 3; e++) {
+        du[e].alloc(cnt[e]);
+        db[e].alloc(cnt[e]);
+        LSG_CUDA(cudaMemcpyAsync(du[e].p, hu[e], cnt[e] * 8, cudaMemcpyHostToDevice, C.s));
+        LSG_CUDA(cudaMemsetAsync(db[e].p, 0, cnt[e] * 8, C.s));
+    }
+    dv.alloc(cnt[dir]);
+    dl.alloc(cnt[dir]);
+    dvb.alloc(cnt[dir]);
+    LSG_CUDA(cudaMemcpyAsync(dv.p, v, cnt[dir] * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(dl.p, lam, cnt[dir] * 8, cudaMemcpyHostToDevice, C.s));
+    LSG_CUDA(cudaMemsetAsync(dvb.p, 0, cnt[dir] * 8, C.s));
+    const Context::Geometry& g = C.geo;
+    const int Ns = d.N - (dir == 0), Ms = d.M - (dir == 1), Ks = d.K - (dir == 2);
+    k_convective_adjoint<<<dim3((Ns + 31) / 32, (Ms + 7) / 8, Ks), dim3(32, 8), 0, C.s>>>(
+        dir, d.N, d.M, d.K, g.stype[dir].p, g.theta.p, g.delta.p, du[0].p, du[1].p, du[2].p, dv.p, dl.p,
+        zconv_reference != 0, db[0].p, db[1].p, db[2].p, dvb.p);
+    LSG_CHECK_LAUNCH();
+    double* hb[3] = {ux_bar, uy_bar, uz_bar};
+    for (int e = 0; e < 3; e++) LSG_CUDA(cudaMemcpyAsync(hb[e], db[e].p, cnt[e] * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaMemcpyAsync(v_bar, dvb.p, cnt[dir] * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
 int lsg_convective_apply_device(lsg_ctx* h, int dir, const double* ux, const double* uy, const double* uz,
                                 const double* v, const double* init, double* out, int zconv_reference)
 {

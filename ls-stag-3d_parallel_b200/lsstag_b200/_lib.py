@@ -56,6 +56,7 @@ EXPORTS = [
     "lsg_loads_set", "lsg_loads_calculate", "lsg_loads_calculate_device", "lsg_loads_reset_filter",
     "lsg_loads_adjoint", "lsg_loads_adjoint_device", "lsg_set_matrix_helmholtz",
     "lsg_helmholtz_flux", "lsg_convective_flux", "lsg_convective_flux_device", "lsg_momentum_rhs_device",
+    "lsg_convective_adjoint", "lsg_convective_adjoint_device",
 ]
 
 _lib = None
@@ -130,6 +131,8 @@ def load() -> C.CDLL:
     lib.lsg_convective_flux_device.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 6 + [
         dp, C.c_void_p]
     lib.lsg_momentum_rhs_device.argtypes = [P, C.c_int] + [C.c_void_p] * 7 + [C.c_double] + [C.c_void_p] * 3
+    lib.lsg_convective_adjoint.argtypes = [P, C.c_int] + [dp] * 9 + [C.c_int]
+    lib.lsg_convective_adjoint_device.argtypes = [P, C.c_int] + [C.c_void_p] * 9 + [C.c_int]
     lib.lsg_loads_set.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip] + [dp] * 8 + [C.c_double,
                                                                                              C.c_double]
     lib.lsg_loads_calculate.argtypes = [P] + [dp] * 8 + [C.c_double, dp, C.POINTER(LoadsResult)]

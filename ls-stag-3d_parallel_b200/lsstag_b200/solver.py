@@ -190,6 +190,19 @@ class IterativeSolver:
                                                          L.dptr(out), int(bool(zconv_reference))))
         return out
 
+    def convective_adjoint(self, direction: int, U, v, lam, zconv_reference: bool = True):
+        """(ux_bar, uy_bar, uz_bar, v_bar): gradients of <lam, C(U) v> in the
+        three velocity grids and in v."""
+        us = [np.ascontiguousarray(a, dtype=np.float64) for a in U]
+        vv = np.ascontiguousarray(v, dtype=np.float64)
+        ll = np.ascontiguousarray(lam, dtype=np.float64)
+        ub = [np.empty_like(a) for a in us]
+        vb = np.empty_like(vv)
+        self.ctx.check(self.ctx.lib.lsg_convective_adjoint(self.ctx.h, int(direction), *(L.dptr(a) for a in us),
+                                                           L.dptr(vv), L.dptr(ll), *(L.dptr(a) for a in ub),
+                                                           L.dptr(vb), int(bool(zconv_reference))))
+        return ub[0], ub[1], ub[2], vb
+
     def momentum_rhs(self, direction: int, Cconv, flux2, u, uprev, vof, hflux, p, prev_aux, coef2):
         """(right, aux) of one momentum equation (HelmholtzDiscreteEquation::
         recalcRightMember); Cconv = (rowptr, col, val) of the convective
