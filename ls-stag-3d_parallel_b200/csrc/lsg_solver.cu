@@ -171,6 +171,10 @@ struct MGData {
     int tail_l0 = -1;
     DevBuf<TailArgs<double>> tail64;
     DevBuf<TailArgs<float>> tail32;
+    // the ADLJ V-cycle as one CUDA graph per precision (instantiated on first
+    // use; it reads level 0's r and leaves the correction in level 0's ch)
+    cudaGraphExec_t cycle64 = nullptr, cycle32 = nullptr;
+    long long cycle64_nodes = 0, cycle32_nodes = 0;   // kernels per replay (launch accounting)
 };
 
 // ---------------------------------------------------------------------------
@@ -207,6 +211,7 @@ struct Context {
     // the level-scheduled ILU(0) solves as one CUDA graph (instantiated on
     // first use, reading ilu_in and writing ilu_out)
     cudaGraphExec_t ilu_exec = nullptr;
+    long long ilu_nodes = 0;
     DevBuf<double> ilu_in, ilu_out;
     double bytes = 0;
     int vcycles = 0;
@@ -510,8 +515,11 @@ static void tail_setup(Context& C)
     LSG_CUDA(cudaStreamSynchronize(C.s));    // the host copies of the arguments go out of scope
 }
 
+static void vcycle_graphs_release(MGData& mg);
+
 static void mg_setup(Context& C)
 {
+    vcycle_graphs_release(C.mg);           // the hierarchy's buffers are rebuilt below
     MGData& mg = C.mg;
     const lsg_options& o = C.opt;
     cudaStream_t s = C.s;
@@ -942,6 +950,59 @@ static void vcycle(Context& C, std::vector<LevelT<T>>& lev, T* ch0 = nullptr)
     C.vcycles++;
 }
 
+static void vcycle_graphs_release(MGData& mg)
+{
+    if (mg.cycle64) cudaGraphExecDestroy(mg.cycle64);
+    if (mg.cycle32) cudaGraphExecDestroy(mg.cycle32);
+    mg.cycle64 = mg.cycle32 = nullptr;
+}
+
+// One ADLJ V-cycle replayed from a CUDA graph: the cycle's launches (about 20
+// per level above the tail kernel) only touch the hierarchy's own buffers, so
+// they are captured once and submitted as one unit, which removes the host
+// submission gaps of the small coarse-level kernels.  The correction is left
+// in level 0's ch; ch0 (if given) receives a copy.  Contexts on the legacy
+// default stream and the Gauss-Seidel cycle run the launches directly.
+template <typename T>
+static void vcycle_run(Context& C, std::vector<LevelT<T>>& lev, T* ch0)
+{
+    if (!C.s || C.opt.smoother == LSG_SMOOTHER_RBGS) {
+        vcycle<T>(C, lev, ch0);
+        return;
+    }
+    cudaGraphExec_t& exec = sizeof(T) == 8 ? C.mg.cycle64 : C.mg.cycle32;
+    if (!exec) {
+        cudaGraph_t graph = nullptr;
+        LSG_CUDA(cudaStreamBeginCapture(C.s, cudaStreamCaptureModeThreadLocal));
+        Error captured{LSG_OK, ""};
+        try {
+            vcycle<T>(C, lev, nullptr);
+        } catch (const Error& e) {
+            captured = e;
+        }
+        const cudaError_t cap_err = cudaStreamEndCapture(C.s, &graph);
+        if (captured.code != LSG_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            throw captured;
+        }
+        LSG_CUDA(cap_err);
+        size_t nodes = 0;
+        cudaGraphGetNodes(graph, nullptr, &nodes);
+        (sizeof(T) == 8 ? C.mg.cycle64_nodes : C.mg.cycle32_nodes) = (long long)nodes;
+        const cudaError_t inst_err = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (inst_err != cudaSuccess) exec = nullptr;
+        LSG_CUDA(inst_err);
+        C.vcycles--;                       // the capture only recorded the cycle
+    }
+    LSG_CUDA(cudaGraphLaunch(exec, C.s));
+    // launch accounting counts the kernels the replay runs
+    ::lsg::g_launches += sizeof(T) == 8 ? C.mg.cycle64_nodes : C.mg.cycle32_nodes;
+    C.vcycles++;
+    if (ch0)
+        LSG_CUDA(cudaMemcpyAsync(ch0, lev[0].ch.p, (size_t)lev[0].d.n() * sizeof(T), cudaMemcpyDeviceToDevice, C.s));
+}
+
 // Algorithmic bytes of one V-cycle with element size w (documented model).
 static double vcycle_bytes(const MGData& mg, const lsg_options& o, double w)
 {
@@ -985,13 +1046,13 @@ static void precond_apply(Context& C, const double* v, double* z)
         auto& lev = C.mg.l32;
         k_convert<float, double><<<grid_for(n, 256), 256, 0, s>>>(n, v, lev[0].r.p);
         LSG_CHECK_LAUNCH();
-        vcycle<float>(C, lev);
+        vcycle_run<float>(C, lev, nullptr);
         k_convert<double, float><<<grid_for(n, 256), 256, 0, s>>>(n, lev[0].ch.p, z);
         LSG_CHECK_LAUNCH();
     } else {
         auto& lev = C.mg.l64;
         LSG_CUDA(cudaMemcpyAsync(lev[0].r.p, v, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-        vcycle<double>(C, lev);
+        vcycle_run<double>(C, lev, nullptr);
         LSG_CUDA(cudaMemcpyAsync(z, lev[0].ch.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     }
 }
@@ -1094,7 +1155,7 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
                     // w = A z_j below holds for the stored z_j)
                     k_scale_copy<float><<<grid_for(n, 256), 256, 0, s>>>(n, C.w.p, &ks->invNormW, vj, C.mg.l32[0].r.p);
                     LSG_CHECK_LAUNCH();
-                    vcycle<float>(C, C.mg.l32, zj32);
+                    vcycle_run<float>(C, C.mg.l32, zj32);
                     bytes += (8 + 8 + 4) * (double)n + vcycle_bytes(C.mg, C.opt, 4.0);
                 } else {
                     k_scale_copy<double><<<grid_for(n, 256), 256, 0, s>>>(n, C.w.p, &ks->invNormW, vj, C.t1.p);
@@ -1309,6 +1370,9 @@ static void ilu_apply(Context& C, const double* b, double* x)
         const cudaError_t cap_err = cudaStreamEndCapture(C.s, &graph);
         LSG_CUDA(launch_err);
         LSG_CUDA(cap_err);
+        size_t nodes = 0;
+        cudaGraphGetNodes(graph, nullptr, &nodes);
+        C.ilu_nodes = (long long)nodes;
         const cudaError_t inst_err = cudaGraphInstantiate(&C.ilu_exec, graph, 0);
         cudaGraphDestroy(graph);
         if (inst_err != cudaSuccess) C.ilu_exec = nullptr;
@@ -1316,7 +1380,7 @@ static void ilu_apply(Context& C, const double* b, double* x)
     }
     LSG_CUDA(cudaMemcpyAsync(C.ilu_in.p, b, n * sizeof(double), cudaMemcpyDeviceToDevice, C.s));
     LSG_CUDA(cudaGraphLaunch(C.ilu_exec, C.s));
-    ::lsg::g_launches++;
+    ::lsg::g_launches += C.ilu_nodes;
     LSG_CUDA(cudaMemcpyAsync(x, C.ilu_out.p, n * sizeof(double), cudaMemcpyDeviceToDevice, C.s));
 }
 
@@ -1482,6 +1546,7 @@ static cudaStream_t context_release(Context& C)
     }
     if (C.s) cudaStreamSynchronize(C.s);
     ilu_graph_release(C);
+    vcycle_graphs_release(C.mg);
     if (C.hflag) cudaFreeHost(C.hflag);
     C.hflag = nullptr;
     if (C.ev0) cudaEventDestroy(C.ev0);
