@@ -43,7 +43,9 @@ class FlowStepper:
         self.bc_lap = bc[[1, 8, 9, 16, 17]].copy()
         ptask = S.Task(eps=par["eps"], MAX_ITER=int(par["max_it"]), FGMRES_RESTART_NUM=int(par["restart_p"]))
         # pressure solve: MG-FGMRES, optionally with the FP32 multigrid inside
-        # the FP64 FGMRES (the mixed-precision preconditioner)
+        # the FP64 FGMRES (the mixed-precision preconditioner; on the 128x64x64
+        # sphere flow with the reference's absolute eps 1e-5 it did not
+        # converge within 200 iterations, so the flow runs the FP64 cycle)
         from . import _lib as L
         self.pres = S.MGFGMRES(device=device, mg_precision=L.FP32 if pressure_mg_fp32 else L.FP64)
         self.pres.set_geometry({k: geom[k] for k in ("celltype", "theta", "delta", "inv_mx", "inv_my", "inv_mz")},
