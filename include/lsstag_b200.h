@@ -390,7 +390,11 @@ int lsg_projection_correct_device(lsg_ctx* ctx, const double* phi, const double*
 int lsg_setup(lsg_ctx* ctx, const lsg_options* opts);
 
 /* Solve A x = b; x holds the initial guess on entry and the solution on exit
-   (IterativeSolverInterface::solve).  Host buffers of N*M*K doubles. */
+   (IterativeSolverInterface::solve).  Host buffers of N*M*K doubles.
+   The first preconditioner application after lsg_setup records the
+   multigrid V-cycle (or the ILU(0) sweeps) as a CUDA graph on the
+   context's own stream and later ones replay it; make that first solve
+   outside any stream capture of the caller's. */
 int lsg_solve(lsg_ctx* ctx, const double* b, double* x, lsg_stats* stats);
 /* Same with device buffers (no host copies). */
 int lsg_solve_device(lsg_ctx* ctx, const double* b, double* x, lsg_stats* stats);
