@@ -377,6 +377,14 @@ int lsg_projection_correct(lsg_ctx* ctx, const double* phi, const double* us, co
 int lsg_projection_adjoint(lsg_ctx* ctx, const double* ubar_out, const double* vbar_out, const double* wbar_out,
                            const double* pbar_out, double coef, double* ubar, double* vbar, double* wbar,
                            double* fluxbar, lsg_stats* st);
+/* out = Gx^T gx + Gy^T gy + Gz^T gz on the base grid: the transpose of the
+   pressure gradient GradientDiscreteOperatorX/Y/Z
+   (DiscreteOperators/Gradient/gradient_discrete_operator_x.h:58-77, _y.h:52-74,
+   _z.h:45-62) applied from the geometry, as lsg_projection_adjoint applies it
+   with unit weights.  It is the pressure cotangent of the G p term of the
+   momentum right-hand side (lsg_momentum_rhs).  No reference counterpart.
+   Host pointers (staggered-grid inputs). */
+int lsg_gradient_transpose(lsg_ctx* ctx, const double* gx, const double* gy, const double* gz, double* out);
 /* Same on device pointers. */
 int lsg_projection_correct_device(lsg_ctx* ctx, const double* phi, const double* us, const double* vs,
                                   const double* ws, double* u, double* v, double* w, double* p, double coef,

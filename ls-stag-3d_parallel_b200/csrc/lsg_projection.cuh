@@ -513,15 +513,17 @@ __global__ void __launch_bounds__(256) k_projection_adjoint_phi(int N, int M, in
     double acc = coef * pb[i];
     // x-faces: east (P = i) and west (P = i - 1); x-grid index numX = i - y - z M
     const long long fx = i - y - (long long)z * M;
-    if (x < N - 1 && xtype[fx] != 0) acc += grad_coef(0, theta, delta, i) * inv_x[fx] * ub[fx];
-    if (x > 0 && xtype[fx - 1] != 0) acc -= grad_coef(0, theta, delta, i - 1) * inv_x[fx - 1] * ub[fx - 1];
+    // inv_* == nullptr: unit weights (the plain transposed gradient)
+    auto w = [](const double* __restrict__ inv, long long f) { return inv ? inv[f] : 1.0; };
+    if (x < N - 1 && xtype[fx] != 0) acc += grad_coef(0, theta, delta, i) * w(inv_x, fx) * ub[fx];
+    if (x > 0 && xtype[fx - 1] != 0) acc -= grad_coef(0, theta, delta, i - 1) * w(inv_x, fx - 1) * ub[fx - 1];
     // y-faces: north (P = i) and south (P = i - N); y-grid index i - z N
     const long long fy = i - (long long)z * N;
-    if (y < M - 1 && ytype[fy] != 0) acc += grad_coef(1, theta, delta, i) * inv_y[fy] * vb[fy];
-    if (y > 0 && ytype[fy - N] != 0) acc -= grad_coef(1, theta, delta, i - N) * inv_y[fy - N] * vb[fy - N];
+    if (y < M - 1 && ytype[fy] != 0) acc += grad_coef(1, theta, delta, i) * w(inv_y, fy) * vb[fy];
+    if (y > 0 && ytype[fy - N] != 0) acc -= grad_coef(1, theta, delta, i - N) * w(inv_y, fy - N) * vb[fy - N];
     // z-faces: top (P = i) and bottom (P = i - NM); z-grid index i
-    if (z < K - 1 && ztype[i] != 0) acc += grad_coef(2, theta, delta, i) * inv_z[i] * wb[i];
-    if (z > 0 && ztype[i - NM] != 0) acc -= grad_coef(2, theta, delta, i - NM) * inv_z[i - NM] * wb[i - NM];
+    if (z < K - 1 && ztype[i] != 0) acc += grad_coef(2, theta, delta, i) * w(inv_z, i) * wb[i];
+    if (z > 0 && ztype[i - NM] != 0) acc -= grad_coef(2, theta, delta, i - NM) * w(inv_z, i - NM) * wb[i - NM];
     phib[i] = acc;
 }
 

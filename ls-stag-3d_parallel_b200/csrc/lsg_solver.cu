@@ -2789,6 +2789,38 @@ int lsg_projection_adjoint(lsg_ctx* h, const double* ubar_out, const double* vba
     LSG_API_END(h)
 }
 
+int lsg_gradient_transpose(lsg_ctx* h, const double* gx, const double* gy, const double* gz, double* out)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(gx && gy && gz && out, LSG_ERR_ARG, "null field");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const Context::Geometry& g = C.geo;
+    const long long n = C.n, cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
+                                       (long long)d.N * d.M * (d.K - 1)};
+    const double* hin[3] = {gx, gy, gz};
+    DevBuf<double> din[3], dzero, dout;
+    for (int k = 0; k < 3; k++) {
+        din[k].alloc(cnt[k]);
+        LSG_CUDA(cudaMemcpyAsync(din[k].p, hin[k], cnt[k] * 8, cudaMemcpyHostToDevice, C.s));
+    }
+    dzero.alloc(n);
+    dout.alloc(n);
+    LSG_CUDA(cudaMemsetAsync(dzero.p, 0, n * 8, C.s));
+    k_projection_adjoint_phi<<<dim3((d.N + 31) / 32, (d.M + 7) / 8, d.K), dim3(32, 8), 0, C.s>>>(
+        d.N, d.M, d.K, g.stype[0].p, g.stype[1].p, g.stype[2].p, g.theta.p, g.delta.p, nullptr, nullptr, nullptr,
+        din[0].p, din[1].p, din[2].p, dzero.p, 0.0, dout.p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaMemcpyAsync(out, dout.p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
 int lsg_solve_adjoint(lsg_ctx* h, const double* g, double* lambda, lsg_stats* st)
 {
     if (!h) return LSG_ERR_ARG;

@@ -253,6 +253,14 @@ class IterativeSolver:
                                                            L.C.byref(self.adj_stats)))
         return outs[0], outs[1], outs[2], fb, ins[3].copy()
 
+    def gradient_transpose(self, gx, gy, gz) -> np.ndarray:
+        """Gx^T gx + Gy^T gy + Gz^T gz on the base grid (the transposed
+        pressure gradient applied from the geometry)."""
+        ins = [np.ascontiguousarray(a, dtype=np.float64) for a in (gx, gy, gz)]
+        out = np.empty(int(np.prod(self.dims)))
+        self.ctx.check(self.ctx.lib.lsg_gradient_transpose(self.ctx.h, *(L.dptr(a) for a in ins), L.dptr(out)))
+        return out
+
     def planes(self) -> np.ndarray:
         n = int(np.prod(self.dims))
         P = np.empty((7, n))

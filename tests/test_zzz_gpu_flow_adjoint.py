@@ -1,0 +1,90 @@
+"""The flow adjoint with every operator on the GPU (flow_adjoint.GpuFlowOps
+through the C ABI): each transposed operator against the oracle operator set
+(tests/flow_oracle_ops.py, exact solves), the forward against the oracle's,
+and the checkpointed reverse sweep against the oracle-backed gradient and
+against central differences of the GPU forward.  Solves run to an absolute
+residual of 1e-12."""
+import numpy as np
+import pytest
+
+from flow_oracle_ops import OracleFlowOps, load_adjoint_case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def both():
+    from lsstag_b200 import flow_adjoint as FA
+    geom, dims, par = load_adjoint_case()
+    par = dict(par, eps=1e-12)
+    gpu = FA.GpuFlowOps(geom, dims, par)
+    cpu = OracleFlowOps(geom, dims, par)
+    yield geom, dims, par, gpu, cpu
+    gpu.close()
+
+
+def _rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300)
+
+
+def test_transposed_operators_match_oracle(both):
+    geom, dims, par, gpu, cpu = both
+    rng = np.random.default_rng(21)
+    fluid = [np.asarray(t) != 0 for t in cpu.stypes]
+    for d in range(3):
+        g = np.where(fluid[d], rng.standard_normal(fluid[d].size), 0.0)
+        assert _rel(gpu.helm_solve_T(d, g)[fluid[d]], cpu.helm_solve_T(d, g)[fluid[d]]) <= 1e-9, d
+    r = [rng.standard_normal(f.size) for f in fluid]
+    assert _rel(gpu.gradient_T(r), cpu.gradient_T(r)) <= 1e-13
+    U = [geom[k] + 0.1 * rng.standard_normal(geom[k].size) for k in ("u_1", "v_1", "w_1")]
+    for d in range(3):
+        cb = rng.standard_normal(U[d].size)
+        for a, b in zip(gpu.conv_adjoint(d, U, cb), cpu.conv_adjoint(d, U, cb)):
+            assert _rel(a, b) <= 1e-13, d
+    qb = [np.where(f, rng.standard_normal(f.size), 0.0) for f in fluid]
+    pb = rng.standard_normal(geom["p_0"].size)
+    sg, Lg = gpu.projection_adjoint(qb, pb)
+    sc, Lc = cpu.projection_adjoint(qb, pb)
+    for a, b in zip(sg, sc):
+        assert _rel(a, b) <= 1e-8
+    assert _rel(Lg[cpu.live], Lc[cpu.live]) <= 1e-8
+    for a, b in zip(gpu.drag_gradient()[0], cpu.drag_gradient()[0]):
+        assert _rel(a, b) <= 1e-13
+
+
+def test_forward_matches_oracle(both):
+    from lsstag_b200 import flow_adjoint as FA
+    geom, dims, par, gpu, cpu = both
+    u0, p0 = [geom["u_0"], geom["v_0"], geom["w_0"]], geom["p_0"]
+    th = 0.05 * np.random.default_rng(22).standard_normal(8)
+    fg, fc = FA.FlowAdjoint(gpu, 3), FA.FlowAdjoint(cpu, 3)
+    Jg, Jc = fg.forward(th, None, u0, p0), fc.forward(th, None, u0, p0)
+    assert abs(Jg - Jc) <= 1e-8 * abs(Jc)
+    for a, b in zip(fg.final[0], fc.final[0]):
+        assert _rel(a, b) <= 1e-8
+
+
+def test_gradient_matches_oracle_and_differences(both):
+    """4 steps, checkpoints every 2: the GPU gradient against the oracle's
+    (relative 1e-6) and against central differences of the GPU forward for
+    two inflow modes (relative 1e-5)."""
+    from lsstag_b200 import flow_adjoint as FA
+    geom, dims, par, gpu, cpu = both
+    u0, p0 = [geom["u_0"], geom["v_0"], geom["w_0"]], geom["p_0"]
+    rng = np.random.default_rng(23)
+    th0 = 0.05 * rng.standard_normal(8)
+    f0 = [0.01 * rng.standard_normal(a.size) for a in u0]
+    fg, fc = FA.FlowAdjoint(gpu, 4, every=2), FA.FlowAdjoint(cpu, 4, every=2)
+    Jg, gth, gf = fg.gradient(th0, f0, u0, p0)
+    Jc, cth, cf = fc.gradient(th0, f0, u0, p0)
+    assert fg.stats == {"recomputed_steps": 4, "checkpoints": 2}
+    assert abs(Jg - Jc) <= 1e-8 * abs(Jc)
+    assert _rel(gth, cth) <= 1e-6
+    for a, b in zip(gf, cf):
+        assert _rel(a, b) <= 1e-6
+    h = 1e-4
+    for k in (0, 4):
+        e = np.zeros(8)
+        e[k] = h
+        fd = (fg.forward(th0 + e, f0, u0, p0) - fg.forward(th0 - e, f0, u0, p0)) / (2 * h)
+        assert abs(gth[k] - fd) <= 1e-5 * abs(fd), (k, gth[k], fd)
