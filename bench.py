@@ -263,6 +263,74 @@ def run_flow(args, world, rank, local, pg):
     return 0
 
 
+ADJ_METRIC = "Drag gradient through 50 time steps of the 128x64x64 sphere flow (C3): ms per gradient on 1 B200"
+
+
+def run_adjoint(args, world, rank, local, pg):
+    """One step = one gradient of the mean drag coefficient over
+    --adjoint-steps time steps of the flow case (8 inflow modes and a forcing
+    field), checkpoints every --checkpoint-every steps: forward, one recompute
+    per segment and the reverse sweep, every operator and transposed
+    operator on the GPU, the sweep orchestrated on the host through the
+    host-array entry points (so the time is end to end)."""
+    import numpy as np
+    import torch
+
+    cfg = {"workload": f"adjoint_flow_sphere_128x64x64_{args.adjoint_steps}steps_ckpt{args.checkpoint_every}",
+           "grid": [128, 64, 64], "objective": "mean C_d over the steps (LoadsCalculator, unfiltered)",
+           "parameters": "8 inflow modes N(0,0.05) and a forcing field N(0,0.01), seed 7",
+           "solvers": "forward and transposed: momentum ILU(0)-FGMRES(13), pressure MG-FGMRES(30), "
+                      "absolute eps 1e-5 (reference defaults)",
+           "warmup": "gradients over 1 time step (contexts, graphs and transposed operators built)",
+           "parallelism": "replicas" if world > 1 else "single GPU"}
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "metric": ADJ_METRIC,
+                              "unavailable": "the reference has no adjoint (its forward time step is the flow "
+                                             "workload's reference arm)"}))
+        return 0
+    torch.cuda.set_device(local)
+    from lsstag_b200 import cases
+    from lsstag_b200 import flow_adjoint as FA
+    g, dims, par, (u0, v0, w0, p0) = cases.load_flow_case()
+    par = dict(par, fcoef=float(g["fcoef"]))
+    ops = FA.GpuFlowOps(g, dims, par, device=local)
+    rng = np.random.default_rng(7)
+    theta = 0.05 * rng.standard_normal(8)
+    forcing = [0.01 * rng.standard_normal(a.size) for a in (u0, v0, w0)]
+    for _ in range(args.warmup):
+        FA.FlowAdjoint(ops, 1, every=1).gradient(theta, forcing, (u0, v0, w0), p0)
+    fa = FA.FlowAdjoint(ops, args.adjoint_steps, every=args.checkpoint_every)
+    barrier(pg)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        J, gth, gf = fa.gradient(theta, forcing, (u0, v0, w0), p0)
+    torch.cuda.synchronize()
+    ms = barrier_max(pg, 1e3 * (time.perf_counter() - t), local) / args.steps
+    ops.close()
+    out = {"metric": ADJ_METRIC, "value": ms, "unit": "ms/gradient", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg, "J": J,
+           "dJ_dtheta": [float(v) for v in gth], "dJ_df_norm": float(np.sqrt(sum(a @ a for a in gf))),
+           "sweep": fa.stats,
+           "e2e": {"value": ms, "unit": "ms/gradient", "note": "host-orchestrated sweep: the timed value is "
+                   "already end to end (every operand copied in and out)"}}
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            ref_ms, _, th = reference_flow_steps(3, os.cpu_count() or 1)
+            out["cpu_baseline"] = {"value": args.adjoint_steps * sum(ref_ms[1:]) / 2,
+                                   "unit": f"ms per {args.adjoint_steps} forward time steps", "cores": th,
+                                   "kind": "reference",
+                                   "sample": "time steps 2-3 of the same case, scaled to the step count: the "
+                                             "reference has no adjoint, this is its forward cost alone"}
+        except Exception as e:  # report, do not hide
+            out["cpu_baseline"] = {"error": str(e)}
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
 def config_dict(args, world):
     return {"workload": f"poisson_spheres4_{args.size}^3_mgfgmres30_rel1e-10",
             "grid": [args.size] * 3, "bodies": "4 seeded spheres (seed 3), Neumann walls, 2 pinned rows",
@@ -290,14 +358,17 @@ def main():
                     help="Gram-Schmidt form of both arms: the low-synchronisation form of the MGS "
                          "projections (default; two passes over the basis per step) or the reference's "
                          "pass-per-vector MGS")
-    ap.add_argument("--workload", default="poisson", choices=["poisson", "flow"],
+    ap.add_argument("--workload", default="poisson", choices=["poisson", "flow", "adjoint"],
                     help="poisson: the 256^3 pressure solve (the headline); flow: time steps of the flow past "
-                         "a sphere at 128x64x64 (every operator of the step on the GPU)")
+                         "a sphere at 128x64x64 (every operator of the step on the GPU); adjoint: the drag "
+                         "gradient through time steps of that flow (use --steps 1)")
+    ap.add_argument("--adjoint-steps", type=int, default=50, help="time steps of one adjoint gradient")
+    ap.add_argument("--checkpoint-every", type=int, default=10, help="checkpoint interval of the adjoint sweep")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
     world, rank, local, pg = dist_setup(args)
-    if args.workload == "flow":
-        rc = run_flow(args, world, rank, local, pg)
+    if args.workload in ("flow", "adjoint"):
+        rc = (run_flow if args.workload == "flow" else run_adjoint)(args, world, rank, local, pg)
         if pg is not None:
             pg.destroy_process_group()
         return rc

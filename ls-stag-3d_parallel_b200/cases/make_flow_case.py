@@ -12,6 +12,11 @@ flow task's walls and convective outflow, dt = 0.01.  Every mesh array the
 GPU time step reads and the initial state are stored sparsely (the most
 frequent value of each array and the exceptions), which keeps the file
 small; lsstag_b200.cases.load_flow_case expands it.
+
+The loads inputs of the same mesh (LoadsCalculator's cut-cell list,
+delta_ib_max, inv_delta_ib_ne, inv_delta_ib_tn and fcoef, from the harness's
+loads mode; the geometry arrays of both runs are checked equal) are stored
+beside them for the drag objective of the time-step adjoint.
 """
 import os
 import sys
@@ -31,12 +36,11 @@ KEEP = ["dims", "celltype", "xtype", "ytype", "ztype", "side_type", "theta", "al
         "restart_mom_p", "u_0", "v_0", "w_0", "p_0"]
 
 
-def main():
-    h = 1.0 / 16
-    case = rr.Case(128, 64, 64, h, h, h, spheres=[(2.0, 2.0 + 0.5 * h, 2.0 + 0.5 * h, 0.5)])
-    r = rr.run(case, threads=os.cpu_count() or 1, flow_setup=1, restart=30, dump_geometry=0, timeout=3000)
-    out = {}
-    for k in KEEP:
+LOADS_KEEP = ["cells", "dmax", "dne", "dtn"]
+
+
+def _store(out, r, keys):
+    for k in keys:
         a = np.asarray(r[k])
         if a.size < 64:
             out[k] = a
@@ -48,6 +52,27 @@ def main():
         out[k + "__idx"] = idx
         out[k + "__val"] = a[idx]
         out[k + "__n"] = np.array(a.size)
+
+
+def loads_inputs(case, geom):
+    """The loads inputs of the case's mesh (harness loads mode), checked
+    against the flow run's geometry."""
+    r = rr.run_loads(case, threads=os.cpu_count() or 1, timeout=3000)
+    for k in ("celltype", "theta", "delta", "inv_vof"):
+        assert np.array_equal(np.asarray(r[k]).ravel(), np.asarray(geom[k]).ravel()), k
+    out = {}
+    _store(out, r, LOADS_KEEP)
+    out["fcoef"] = np.array(float(r["nu_fcoef_dt"][1]))
+    return out
+
+
+def main():
+    h = 1.0 / 16
+    case = rr.Case(128, 64, 64, h, h, h, spheres=[(2.0, 2.0 + 0.5 * h, 2.0 + 0.5 * h, 0.5)])
+    r = rr.run(case, threads=os.cpu_count() or 1, flow_setup=1, restart=30, dump_geometry=0, timeout=3000)
+    out = {}
+    _store(out, r, KEEP)
+    out.update(loads_inputs(case, r))
     path = cases.flow_case_path()
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes")

@@ -223,8 +223,9 @@ class GpuFlowOps:
     momentum operator, and the loads context for the drag and its gradient.
 
     geom: FlowStepper's mesh arrays plus the loads inputs cells, dmax (delta_ib_max),
-    dne (inv_delta_ib_ne), dtn (inv_delta_ib_tn), nodes, center; par:
-    FlowStepper's parameters plus fcoef and dt."""
+    dne (inv_delta_ib_ne), dtn (inv_delta_ib_tn) and, optionally, nodes and
+    center (they enter the moments only, not the drag); par: FlowStepper's
+    parameters plus fcoef and dt."""
 
     def __init__(self, geom: dict, dims, par: dict, device: int = 0):
         from .loads import LoadsCalculator
@@ -257,9 +258,10 @@ class GpuFlowOps:
                                              FGMRES_RESTART_NUM=int(par["restart_mom"])))
             self.momT.append(t)
         self.loads = LoadsCalculator(device=device)
+        n = int(np.prod(self.dims))
         self.loads.set(self.dims, geom["cells"], geom["celltype"], geom["theta"], geom["delta"], geom["inv_vof"],
-                       geom["dmax"], geom["dne"], geom["dtn"], geom["nodes"], geom["center"], par["fcoef"],
-                       par["dt"])
+                       geom["dmax"], geom["dne"], geom["dtn"], geom.get("nodes", np.zeros(3 * n)),
+                       geom.get("center", np.zeros(3)), par["fcoef"], par["dt"])
         self.set_inflow(geom["u_w"])
 
     def set_inflow(self, u_w):

@@ -206,3 +206,22 @@ def test_inflow_basis():
             for i in range(5):
                 assert B[k, j + i * 6] == pytest.approx(np.sin(a * np.pi * y[j]) * np.sin(b * np.pi * z[i]), abs=1e-15)
     assert np.linalg.matrix_rank(B) == 8
+
+
+def test_flow_case_carries_the_drag_inputs():
+    """The 128x64x64 case holds LoadsCalculator's inputs for the objective:
+    the cut-cell list (cut cells of the mesh only, each once) and its
+    immersed-boundary arrays; the oracle's drag gradient on them is finite
+    and nonzero."""
+    from lsstag_b200 import cases
+    g, dims, par, _ = cases.load_flow_case()
+    N, M, K = dims
+    cells = np.asarray(g["cells"])
+    ct = np.asarray(g["celltype"])[cells]
+    assert cells.size == np.unique(cells).size > 0
+    assert np.all((ct != lo.SOLID_CELL) & (ct != lo.FLUID_CELL))
+    assert float(g["fcoef"]) > 0
+    gx, gy, gz, gp = lo.loads_adjoint(N, M, K, cells, g["celltype"], g["theta"], g["delta"], g["inv_vof"],
+                                      g["dmax"], g["dne"], g["dtn"], (float(g["fcoef"]), 0.0, 0.0), par["nu"])
+    tot = sum(np.abs(a).sum() for a in (gx, gy, gz, gp))
+    assert np.isfinite(tot) and tot > 0
