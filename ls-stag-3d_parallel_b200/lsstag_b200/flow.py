@@ -42,15 +42,21 @@ class FlowStepper:
         # U_E, V_S, V_N, W_B, W_T of the pressure equation's source term
         self.bc_lap = bc[[1, 8, 9, 16, 17]].copy()
         ptask = S.Task(eps=par["eps"], MAX_ITER=int(par["max_it"]), FGMRES_RESTART_NUM=int(par["restart_p"]))
-        # pressure solve: MG-FGMRES, optionally with the FP32 multigrid inside
-        # the FP64 FGMRES (the mixed-precision preconditioner; on the 128x64x64
-        # sphere flow with the reference's absolute eps 1e-5 it did not
-        # converge within 200 iterations, so the flow runs the FP64 cycle)
+        # pressure: the operator assembled from the geometry (it also serves the
+        # projection entry points) solved by MG-FGMRES with the FP64 cycle, as
+        # the reference does; or, with pressure_mg_fp32, by MG-FGMRES with the
+        # FP32 cycle on the same operator with its pinned rows negated
+        # (pins_negated: same solution, a hierarchy without wrong-signed
+        # coarse rows, which the FP32 cycle needs)
         from . import _lib as L
-        self.pres = S.MGFGMRES(device=device, mg_precision=L.FP32 if pressure_mg_fp32 else L.FP64)
+        self.pres = S.MGFGMRES(device=device)
         self.pres.set_geometry({k: geom[k] for k in ("celltype", "theta", "delta", "inv_mx", "inv_my", "inv_mz")},
-                               self.dims, geom["pins"], task=ptask)
+                               self.dims, geom["pins"], task=ptask, setup=not pressure_mg_fp32)
         self.pres.set_staggered_types(geom["xtype"], geom["ytype"], geom["ztype"])
+        self.psolve = self.pres
+        if pressure_mg_fp32:
+            self.psolve = S.MGFGMRES(device=device, mg_precision=L.FP32)
+            self.psolve.set_planes(S.pins_negated(self.pres.planes(), geom["pins"]), self.dims, task=ptask)
         mtask = S.Task(eps=par["eps"], MAX_ITER=int(par["max_it"]), FGMRES_RESTART_NUM=int(par["restart_mom"]))
         self.mom, self.hflux = [], []
         for d, c in enumerate("xyz"):
@@ -91,7 +97,7 @@ class FlowStepper:
             us.append(x)
         b = self.pres.projection_rhs(us[0], us[1], us[2], flux_lap)
         phi = np.zeros_like(self.p)
-        its.append(self.pres.solve(b, phi))
+        its.append(self.psolve.solve(b, phi))
         self.uprev = [a.copy() for a in self.u]
         self.pprev = self.p.copy()
         p = self.p.copy()
@@ -127,6 +133,8 @@ class FlowStepper:
     def close(self):
         for s in self.mom:
             s.close()
+        if self.psolve is not self.pres:
+            self.psolve.close()
         self.pres.close()
 
 
@@ -219,7 +227,8 @@ class FlowStepperDevice:
         self.phi.zero_()
         torch.cuda.synchronize()
         st = L.Stats()
-        ck(lib.lsg_solve_device(pres.ctx.h, self._p(self.b), self._p(self.phi), C.byref(st)))
+        psolve = self.host.psolve
+        psolve.ctx.check(lib.lsg_solve_device(psolve.ctx.h, self._p(self.b), self._p(self.phi), C.byref(st)))
         its.append(st.iterations)
         ck(lib.lsg_projection_correct_device(pres.ctx.h, self._p(self.phi), self._p(self.us[0]), self._p(self.us[1]),
                                              self._p(self.us[2]), self._p(self.unew[0]), self._p(self.unew[1]),

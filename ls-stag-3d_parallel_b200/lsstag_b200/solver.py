@@ -31,6 +31,24 @@ class Task:
     n_post: int = 3
 
 
+def pins_negated(planes: np.ndarray, pins) -> np.ndarray:
+    """The seven coefficient planes with the pinned rows negated.  The
+    reference pins two rows of the pressure operator to the identity
+    (laplace_discrete_operator.h:809-821) while every other row has a
+    negative diagonal; the Galerkin hierarchy then holds, in the aggregates
+    of the pins, rows whose diagonal is positive or nearly zero next to
+    positive off-diagonals, and the line smoother divides by them: the
+    cycle's output grows to about 1e4 near a pin on the 128x64x64 sphere
+    flow while the solution is O(0.3), more than the FP32 cycle can carry.
+    Negated, the pins have the sign of the other rows.  The pressure
+    right-hand side is 0 at the pins, so S A x = b has the solution of
+    A x = b, and the residual norms are the same (S = diag(+-1))."""
+    P = np.array(planes, dtype=np.float64, copy=True)
+    for p in pins:
+        P[:, int(p)] = -P[:, int(p)]
+    return P
+
+
 class IterativeSolver:
     """Common part of the solver classes (IterativeSolverInterface)."""
 

@@ -1,0 +1,62 @@
+"""The flow's pressure solved with the FP32 multigrid cycle inside FP64 FGMRES
+on the operator with negated pins (FlowStepper / FlowStepperDevice with
+pressure_mg_fp32): on the 16^3 sphere flow against the reference's three
+steps, and on the 128x64x64 sphere flow, where the cycle on the reference's
+pins stalled, against the FP64 stepper."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def test_fp32_pressure_flow16_matches_reference_steps():
+    """Both sides solve to an absolute residual of 1e-11; the pressure
+    operator's smallest singular value (4.6e-5) bounds how far two such
+    solutions may lie apart: velocities 1e-7, pressure 1e-5 on the cells
+    that are neither solid nor empty rows."""
+    import lsg_oracle as lo
+    from flow_oracle_ops import planes_csr
+    from lsstag_b200.flow import FlowStepper
+    g = load_golden("flow16_steps")
+    dims = tuple(int(v) for v in g["dims"])
+    nu, coef, coef2, integr, dt, eps, vbase, maxit = (float(v) for v in g["nu_coef_coef2_integr_dt_eps_vbase_maxit"])
+    par = dict(nu=nu, coef=coef, coef2=coef2, coef_integr=integr, eps=eps, vbase=vbase, max_it=int(maxit),
+               restart_mom=int(g["restart_mom_p"][0]), restart_p=int(g["restart_mom_p"][1]))
+    fs = FlowStepper(g, dims, par, g["u_0"], g["v_0"], g["w_0"], g["p_0"], pressure_mg_fp32=True)
+    A = planes_csr(lo.laplace_from_geometry(*dims, g["celltype"], g["theta"], g["delta"], g["inv_mx"], g["inv_my"],
+                                            g["inv_mz"], g["pins"]), dims)
+    live = (np.asarray(abs(A).sum(axis=1)).ravel() != 0) & (np.asarray(g["celltype"]) != lo.SOLID_CELL)
+    for s in (1, 2, 3):
+        its = fs.step()
+        assert its[3] <= int(g[f"its_{s}"][3]) + 2, (s, its)
+        for name, mine in zip("uvw", fs.u):
+            assert _rel(mine, g[f"{name}_{s}"]) <= 1e-7, (s, name)
+        assert _rel(fs.p[live], g[f"p_{s}"][live]) <= 1e-5, s
+    fs.close()
+
+
+def test_fp32_pressure_flow_128x64x64_converges():
+    """Three steps of the 128x64x64 flow: the FP32-cycle pressure solve
+    converges to the reference's absolute eps 1e-5 in a few iterations (the
+    reference's FP64 cycle takes 5 on the first step) and the state follows
+    the FP64 stepper's to the solver tolerance."""
+    from lsstag_b200 import cases
+    from lsstag_b200.flow import FlowStepperDevice
+    g, dims, par, (u0, v0, w0, p0) = cases.load_flow_case()
+    states = []
+    for fp32 in (False, True):
+        fs = FlowStepperDevice(g, dims, par, u0, v0, w0, p0, pressure_mg_fp32=fp32)
+        its = [fs.step() for _ in range(3)]
+        if fp32:
+            assert all(i[3] <= 8 for i in its), its
+        states.append(fs.state())
+        fs.close()
+    (u64, p64), (u32, p32) = states
+    for a, b in zip(u32, u64):
+        assert _rel(a, b) <= 1e-4
