@@ -385,6 +385,13 @@ int lsg_projection_adjoint(lsg_ctx* ctx, const double* ubar_out, const double* v
    momentum right-hand side (lsg_momentum_rhs).  No reference counterpart.
    Host pointers (staggered-grid inputs). */
 int lsg_gradient_transpose(lsg_ctx* ctx, const double* gx, const double* gy, const double* gz, double* out);
+/* Same on device pointers (the context's device; the call returns when the
+   result is written). */
+int lsg_gradient_transpose_device(lsg_ctx* ctx, const double* gx, const double* gy, const double* gz, double* out);
+/* lsg_projection_adjoint on device pointers; outputs must not alias inputs. */
+int lsg_projection_adjoint_device(lsg_ctx* ctx, const double* ubar_out, const double* vbar_out,
+                                  const double* wbar_out, const double* pbar_out, double coef, double* ubar,
+                                  double* vbar, double* wbar, double* fluxbar, lsg_stats* st);
 /* Same on device pointers. */
 int lsg_projection_correct_device(lsg_ctx* ctx, const double* phi, const double* us, const double* vs,
                                   const double* ws, double* u, double* v, double* w, double* p, double coef,

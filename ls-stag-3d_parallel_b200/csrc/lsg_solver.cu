@@ -2789,6 +2789,69 @@ int lsg_projection_adjoint(lsg_ctx* h, const double* ubar_out, const double* vba
     LSG_API_END(h)
 }
 
+int lsg_projection_adjoint_device(lsg_ctx* h, const double* ubar_out, const double* vbar_out,
+                                  const double* wbar_out, const double* pbar_out, double coef, double* ubar,
+                                  double* vbar, double* wbar, double* fluxbar, lsg_stats* st)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(ubar_out && vbar_out && wbar_out && pbar_out && ubar && vbar && wbar && fluxbar, LSG_ERR_ARG,
+                "null field");
+    LSG_CUDA(cudaSetDevice(C.device));
+    Context& A = adjoint_context(C);
+    if (st) std::memset(st, 0, sizeof(*st));
+    const Dims& d = C.d;
+    const Context::Geometry& g = C.geo;
+    const long long n = C.n;
+    const double* dout[3] = {ubar_out, vbar_out, wbar_out};
+    double* din[3] = {ubar, vbar, wbar};
+    const dim3 blk(32, 8);
+    k_projection_adjoint_phi<<<dim3((d.N + 31) / 32, (d.M + 7) / 8, d.K), blk, 0, C.s>>>(
+        d.N, d.M, d.K, g.stype[0].p, g.stype[1].p, g.stype[2].p, g.theta.p, g.delta.p, g.inv[0].p, g.inv[1].p,
+        g.inv[2].p, dout[0], dout[1], dout[2], pbar_out, coef, A.bd.p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaMemsetAsync(A.xd.p, 0, n * 8, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    const int rc = solve_device(A, A.bd.p, A.xd.p, st);
+    for (int dir = 0; dir < 3; dir++) {
+        const int Ns = d.N - (dir == 0), Ms = d.M - (dir == 1), Ks = d.K - (dir == 2);
+        k_projection_adjoint_vel<<<dim3((Ns + 31) / 32, (Ms + 7) / 8, Ks), blk, 0, C.s>>>(
+            dir, d.N, d.M, d.K, g.type.p, g.theta.p, g.delta.p, A.xd.p, g.pin0, g.pin1, dout[dir], din[dir]);
+        LSG_CHECK_LAUNCH();
+    }
+    k_pin_zero_copy<<<grid_for(n, 256), 256, 0, C.s>>>(n, g.pin0, g.pin1, A.xd.p, fluxbar);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return rc;
+    LSG_API_END(h)
+}
+
+int lsg_gradient_transpose_device(lsg_ctx* h, const double* gx, const double* gy, const double* gz, double* out)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(gx && gy && gz && out, LSG_ERR_ARG, "null field");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const Context::Geometry& g = C.geo;
+    DevBuf<double> dzero;
+    dzero.alloc(C.n);
+    LSG_CUDA(cudaMemsetAsync(dzero.p, 0, C.n * 8, C.s));
+    k_projection_adjoint_phi<<<dim3((d.N + 31) / 32, (d.M + 7) / 8, d.K), dim3(32, 8), 0, C.s>>>(
+        d.N, d.M, d.K, g.stype[0].p, g.stype[1].p, g.stype[2].p, g.theta.p, g.delta.p, nullptr, nullptr, nullptr, gx,
+        gy, gz, dzero.p, 0.0, out);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
 int lsg_gradient_transpose(lsg_ctx* h, const double* gx, const double* gy, const double* gz, double* out)
 {
     if (!h) return LSG_ERR_ARG;

@@ -57,6 +57,7 @@ EXPORTS = [
     "lsg_loads_adjoint", "lsg_loads_adjoint_device", "lsg_set_matrix_helmholtz",
     "lsg_helmholtz_flux", "lsg_convective_flux", "lsg_convective_flux_device", "lsg_momentum_rhs_device",
     "lsg_convective_adjoint", "lsg_convective_adjoint_device", "lsg_gradient_transpose",
+    "lsg_gradient_transpose_device", "lsg_projection_adjoint_device",
 ]
 
 _lib = None
@@ -119,6 +120,9 @@ def load() -> C.CDLL:
     lib.lsg_momentum_rhs.argtypes = [P, C.c_int, ip, ip, dp, dp, dp, dp, dp, dp, dp, dp, C.c_double, dp, dp]
     lib.lsg_projection_adjoint.argtypes = [P, dp, dp, dp, dp, C.c_double, dp, dp, dp, dp, C.POINTER(Stats)]
     lib.lsg_gradient_transpose.argtypes = [P, dp, dp, dp, dp]
+    lib.lsg_gradient_transpose_device.argtypes = [P] + [C.c_void_p] * 4
+    lib.lsg_projection_adjoint_device.argtypes = ([P] + [C.c_void_p] * 4 + [C.c_double] + [C.c_void_p] * 4
+                                                  + [C.POINTER(Stats)])
     lib.lsg_laplace_flux_device.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p, dp, C.c_void_p, C.c_void_p]
     lib.lsg_projection_rhs.argtypes = [P, dp, dp, dp, dp, dp]
     lib.lsg_projection_rhs_device.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]

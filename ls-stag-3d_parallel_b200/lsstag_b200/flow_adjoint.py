@@ -456,3 +456,294 @@ class FlowAdjoint:
         uwb += src.convective_flux_T(pab[2], u0v[0], u0v[2])[2]
         self.stats = {"recomputed_steps": recomputed, "checkpoints": len(starts)}
         return J, self.B @ uwb, fb
+
+
+class FlowAdjointDevice:
+    """FlowAdjoint with the state, the checkpoints, the segment records and
+    every cotangent in device memory (torch CUDA tensors as buffers), the
+    work done by the *_device entry points on the contexts of a GpuFlowOps,
+    and the boundary transposes and clamp masks as index operations on the
+    device.  No host copies inside a step except the drag value and the
+    iteration counts.  Same arguments and results as FlowAdjoint."""
+
+    def __init__(self, ops: GpuFlowOps, steps: int, every: int = 10, device: int = 0):
+        import ctypes
+        import torch
+        self.torch, self.ct = torch, ctypes
+        self.ops = ops
+        self.S = int(steps)
+        self.every = max(1, int(every))
+        N, M, K = self.dims = ops.dims
+        self.dev = torch.device("cuda", device)
+        self.n = N * M * K
+        self.gsize = [int(np.prod(grid_dims(d, self.dims))) for d in range(3)]
+        g = ops.g
+        T = self._t
+        self.side_type = T(g["side_type"], torch.int32)
+        self.vib, self.vibyx, self.vibzy = T(g["vib"]), T(g["vibyx"]), T(g["vibzy"])
+        self.theta_g, self.delta_g = T(g["theta"]), T(g["delta"])
+        self.vof = [T(v) for v in ops.vof]
+        self.fluid = [T(np.asarray(t) != 0, torch.bool) for t in ops.stypes]
+        self.fvof = [torch.where(f, v, torch.zeros_like(v)) for f, v in zip(self.fluid, self.vof)]
+        self.B = T(inflow_basis(M, K))
+        self.u_w0 = T(g["u_w"])
+        self.bc = np.ascontiguousarray(ops.bc, dtype=np.float64)
+        self.bc_lap = np.ascontiguousarray(ops.bc_lap, dtype=np.float64)
+        self._index_setup(g["theta"], g["delta"], g["bc"], ops.nu)
+        gu, gp = ops.drag_gradient()
+        self.gu = [T(a) / self.S for a in gu]
+        self.gp = T(gp) / self.S
+        self.stats = {}
+
+    def _index_setup(self, theta, delta, bc, nu):
+        """Index sets and coefficients of the boundary transposes and of the
+        clamp masks, as device tensors."""
+        torch = self.torch
+        T = self._t
+        N, M, K = self.dims
+        src = SourceTermTransposes(self.dims, theta, delta, bc, nu)
+        self.src = {k: (T(v, torch.int64) if np.asarray(v).dtype.kind in "iu" else T(v))
+                    for k, v in vars(src).items() if k != "dims"}
+        NM = N * M
+        zz, yy = np.meshgrid(np.arange(1, K - 1), np.arange(1, M - 1), indexing="ij")
+        zz, yy = zz.ravel(), yy.ravel()
+        num = (yy + 1) * N - 1 + zz * NM
+        self.cl_num, self.cl_num2, self.cl_num3 = (T(a, torch.int64) for a in (num, num - yy - 1 - zz * M, num - zz * N))
+        yy, xx = np.meshgrid(np.arange(1, M), np.arange(1, N), indexing="ij")
+        nb = (xx + yy * N).ravel()
+        self.cl_nb, self.cl_nt = T(nb, torch.int64), T(nb + (K - 2) * NM, torch.int64)
+
+    # -- helpers ---------------------------------------------------------------
+    def _t(self, a, dtype=None):
+        torch = self.torch
+        t = torch.as_tensor(np.ascontiguousarray(a), device=self.dev)
+        return t.to(dtype or torch.float64).contiguous()
+
+    def _p(self, t, numel=None):
+        """Device pointer of a contiguous float64 (or int32) tensor of the
+        expected size on this device."""
+        assert t.is_contiguous() and t.device == self.dev
+        if numel is not None:
+            assert t.numel() == numel, (t.numel(), numel)
+        return self.ct.c_void_p(t.data_ptr())
+
+    def _sync(self):
+        self.torch.cuda.synchronize(self.dev)
+
+    def _empty(self, n):
+        return self.torch.empty(n, dtype=self.torch.float64, device=self.dev)
+
+    def _zeros(self, n):
+        return self.torch.zeros(n, dtype=self.torch.float64, device=self.dev)
+
+    def _vel(self, u):
+        return [self._p(u[d], self.gsize[d]) for d in range(3)]
+
+    def _solve(self, solver, b, x):
+        from . import _lib as L
+        st = L.Stats()
+        self._sync()
+        solver.ctx.check(solver.ctx.lib.lsg_solve_device(solver.ctx.h, self._p(b, x.numel()), self._p(x),
+                                                         self.ct.byref(st)))
+        self._sync()
+        return st.iterations
+
+    # -- forward ---------------------------------------------------------------
+    def _set_inflow(self, theta):
+        th = self._t(np.zeros(self.B.shape[0]) if theta is None else theta)
+        self.u_w = (self.u_w0 + th @ self.B).contiguous()
+        self.ops.set_inflow(self.u_w.cpu().numpy())
+        self.hflux = [self._t(h) for h in self.ops.hflux]
+
+    def _conv(self, d, u):
+        from . import _lib as L
+        ops = self.ops
+        N, M, K = self.dims
+        flux2, out = self._empty(self.gsize[d]), self._empty(self.gsize[d])
+        self._sync()
+        m = ops.mom[d]
+        m.ctx.check(m.ctx.lib.lsg_convective_flux_device(m.ctx.h, d, N, M, K, self._p(self.theta_g, 3 * self.n),
+                                                         self._p(self.delta_g, 3 * self.n), *self._vel(u),
+                                                         self._p(self.u_w), L.dptr(self.bc), self._p(flux2)))
+        pr = ops.pres
+        pr.ctx.check(pr.ctx.lib.lsg_convective_apply_device(pr.ctx.h, d, *self._vel(u), self._p(u[d]),
+                                                            self._p(flux2), self._p(out), 1))
+        self._sync()
+        return out
+
+    def _initial(self, u0, p0):
+        u = [self._t(a) for a in u0]
+        return (u, [a.clone() for a in u], self._t(p0), [self._conv(d, u) for d in range(3)])
+
+    def _masks(self, q):
+        torch = self.torch
+        mx, my, mz = (torch.zeros(n, dtype=torch.bool, device=self.dev) for n in self.gsize)
+        for sh in (0, 1):
+            hit = q[0][self.cl_num2 - sh] < 0.0
+            mx[(self.cl_num2 - sh)[hit]] = True
+            my[(self.cl_num3 - sh)[hit]] = True
+            mz[(self.cl_num - sh)[hit]] = True
+        mz[self.cl_nb[q[2][self.cl_nb] > 0.0]] = True
+        mz[self.cl_nt[q[2][self.cl_nt] < 0.0]] = True
+        return mx, my, mz
+
+    def _step(self, st, forcing, rec=None):
+        from . import _lib as L
+        ops, par = self.ops, self.ops.par
+        pr = ops.pres
+        lib = pr.ctx.lib
+        u, uprev, p, pa = st
+        Lf = self._empty(self.n)
+        self._sync()
+        pr.ctx.check(lib.lsg_laplace_flux_device(pr.ctx.h, self._p(self.side_type), self._p(self.vib),
+                                                 self._p(self.u_w), L.dptr(self.bc_lap), self._p(u[0]), self._p(Lf)))
+        s, c = [], []
+        for d in range(3):
+            cd = self._conv(d, u)
+            right, aux, gpw = (self._empty(self.gsize[d]) for _ in range(3))
+            pr.ctx.check(lib.lsg_momentum_rhs_device(pr.ctx.h, d, self._p(cd), self._p(u[d]), self._p(uprev[d]),
+                                                     self._p(self.vof[d]), self._p(self.hflux[d]),
+                                                     self._p(p, self.n), self._p(pa[d]), float(par["coef2"]),
+                                                     self._p(right), self._p(aux), self._p(gpw)))
+            self._sync()
+            if forcing is not None:
+                right += self.fvof[d] * forcing[d]
+            x = u[d].clone()
+            self._solve(ops.mom[d], right, x)
+            s.append(x)
+            c.append(cd)
+        b = self._empty(self.n)
+        pr.ctx.check(lib.lsg_projection_rhs_device(pr.ctx.h, *self._vel(s), self._p(Lf), self._p(b)))
+        phi = self._zeros(self.n)
+        self._solve(pr, b, phi)
+        unew = [self._empty(n) for n in self.gsize]
+        pnew = p.clone()
+        pr.ctx.check(lib.lsg_projection_correct_device(pr.ctx.h, self._p(phi), *self._vel(s), *self._vel(unew),
+                                                       self._p(pnew, self.n), float(par["coef"]), float(par["vbase"]),
+                                                       1))
+        if rec is not None:
+            q = [self._empty(n) for n in self.gsize]
+            pq = p.clone()
+            pr.ctx.check(lib.lsg_projection_correct_device(pr.ctx.h, self._p(phi), *self._vel(s), *self._vel(q),
+                                                           self._p(pq, self.n), float(par["coef"]),
+                                                           float(par["vbase"]), 0))
+            self._sync()
+            rec.append((u, self._masks(q)))
+        self._sync()
+        return (unew, u, pnew, c)
+
+    def _drag(self, u, p):
+        self._sync()
+        r = self.ops.loads.calculate_device(u[0].data_ptr(), u[1].data_ptr(), u[2].data_ptr(), p.data_ptr(),
+                                            self.vib.data_ptr(), self.vibyx.data_ptr(), self.vibzy.data_ptr(),
+                                            self.ops.nu)
+        return float(r.coef[0])
+
+    def _forcing(self, forcing):
+        return None if forcing is None else [self._t(f) for f in forcing]
+
+    def forward(self, theta, forcing, u0, p0) -> float:
+        self._set_inflow(theta)
+        fr = self._forcing(forcing)
+        st = self._initial(u0, p0)
+        self.checkpoints = {}
+        J = 0.0
+        for n in range(self.S):
+            if n % self.every == 0:
+                self.checkpoints[n] = st
+            st = self._step(st, fr)
+            J += self._drag(st[0], st[2]) / self.S
+        self.final = st
+        return J
+
+    # -- reverse ---------------------------------------------------------------
+    def _conv_flux_T(self, cbar, ux, uz, ub, uwb):
+        s = self.src
+        cin = cbar[s["cz_in"]]
+        uwb.index_add_(0, s["cz_in_w"], cin * s["cz_in_c0"])
+        uwb.index_add_(0, s["cz_in_w"] + self.dims[1], cin * s["cz_in_c1"])
+        cl = cbar[s["cz_last"]]
+        ub[2].index_add_(0, s["cz_last"], cl * 0.25 * (ux[s["cz_u0"]] * s["cz_dz"] + ux[s["cz_u1"]] * s["cz_dzz"])
+                         * s["cz_dy"])
+        w = cl * 0.25 * uz[s["cz_last"]] * s["cz_dy"]
+        ub[0].index_add_(0, s["cz_u0"], w * s["cz_dz"])
+        ub[0].index_add_(0, s["cz_u1"], w * s["cz_dzz"])
+        ub[2].index_add_(0, s["cz_nb"], cbar[s["cz_nb"]] * s["cz_cb"] * uz[s["cz_nb"]])
+        ub[2].index_add_(0, s["cz_nt"], cbar[s["cz_nt"]] * s["cz_ct"] * uz[s["cz_nt"]])
+
+    def gradient(self, theta, forcing, u0, p0):
+        """(J, dJ/dtheta, dJ/df): host numpy results, as FlowAdjoint.gradient."""
+        from . import _lib as L
+        torch = self.torch
+        ops = self.ops
+        pr = ops.pres
+        lib = pr.ctx.lib
+        s = self.src
+        J = self.forward(theta, forcing, u0, p0)
+        fr = self._forcing(forcing)
+        co2, coef = float(ops.par["coef2"]), float(ops.par["coef"])
+        z = lambda a: torch.zeros_like(a)                                    # noqa: E731
+        ub = [torch.where(f, a, z(a)) for f, a in zip(self.fluid, self.gu)]
+        upb = [z(a) for a in ub]
+        pb = self.gp.clone()
+        pab = [z(a) for a in ub]
+        uwb = self._zeros(self.u_w0.numel())
+        fb = [z(a) for a in ub]
+        starts = sorted(self.checkpoints)
+        recomputed = 0
+        for k in reversed(range(len(starts))):
+            n0 = starts[k]
+            n1 = starts[k + 1] if k + 1 < len(starts) else self.S
+            rec, st = [], self.checkpoints[n0]
+            for _ in range(n0, n1):
+                st = self._step(st, fr, rec)
+                recomputed += 1
+            for n in reversed(range(n0, n1)):
+                un, masks = rec[n - n0]
+                qb = [torch.where(m, z(a), a).contiguous() for m, a in zip(masks, ub)]
+                sb = [self._empty(m) for m in self.gsize]
+                Lb = self._empty(self.n)
+                stt = L.Stats()
+                self._sync()
+                pr.ctx.check(lib.lsg_projection_adjoint_device(pr.ctx.h, *self._vel(qb), self._p(pb, self.n), coef,
+                                                               *self._vel(sb), self._p(Lb), self.ct.byref(stt)))
+                ub_in = [a.clone() for a in upb]
+                cb = [a.clone() for a in pab]
+                rs = []
+                for d in range(3):
+                    g_ = torch.where(self.fluid[d], sb[d], z(sb[d])).contiguous()
+                    rb = z(g_)
+                    self._solve(ops.momT[d], g_, rb)
+                    rb = torch.where(self.fluid[d], rb, z(rb))
+                    fb[d] += self.fvof[d] * rb
+                    ub_in[d] += (-2.0 * co2) * self.vof[d] * rb
+                    upb[d] = (0.5 * co2) * self.vof[d] * rb
+                    pab[d] = -rb
+                    cb[d] += 2.0 * rb
+                    rs.append(rb.contiguous())
+                uwb.index_add_(0, s["hx_w"], (-rs[0])[s["hx_row"]] * s["hx_c"])
+                gT = self._empty(self.n)
+                self._sync()
+                pr.ctx.check(lib.lsg_gradient_transpose_device(pr.ctx.h, *self._vel(rs), self._p(gT)))
+                pb = pb - gT
+                for d in range(3):
+                    self._sync()
+                    pr.ctx.check(lib.lsg_convective_adjoint_device(pr.ctx.h, d, *self._vel(un), self._p(un[d]),
+                                                                   self._p(cb[d], self.gsize[d]),
+                                                                   *self._vel(ub_in), self._p(ub_in[d]), 1))
+                self._sync()
+                self._conv_flux_T(cb[2], un[0], un[2], ub_in, uwb)
+                ub_in[0].index_add_(0, s["lap_out_u"], Lb[s["lap_out"]] * s["lap_out_c"])
+                uwb.index_add_(0, s["lap_in_w"], Lb[s["lap_in"]] * s["lap_in_c"])
+                if n >= 1:
+                    for d in range(3):
+                        ub_in[d] += self.gu[d]
+                    pb = pb + self.gp
+                ub = [torch.where(f, a, z(a)).contiguous() for f, a in zip(self.fluid, ub_in)]
+                upb = [torch.where(f, a, z(a)) for f, a in zip(self.fluid, upb)]
+        u0v = self.checkpoints[0][0]
+        tmp = [z(a) for a in u0v]
+        self._conv_flux_T(pab[2], u0v[0], u0v[2], tmp, uwb)
+        self._sync()
+        self.stats = {"recomputed_steps": recomputed, "checkpoints": len(starts)}
+        return J, (self.B @ uwb).cpu().numpy(), [f.cpu().numpy() for f in fb]

@@ -225,3 +225,30 @@ def test_flow_case_carries_the_drag_inputs():
                                       g["dmax"], g["dne"], g["dtn"], (float(g["fcoef"]), 0.0, 0.0), par["nu"])
     tot = sum(np.abs(a).sum() for a in (gx, gy, gz, gp))
     assert np.isfinite(tot) and tot > 0
+
+
+def test_device_sweep_index_operations_match_host(case):
+    """FlowAdjointDevice's clamp masks and boundary transposes (torch index
+    operations) against the host versions, run here on CPU tensors."""
+    import torch
+    geom, dims, par, ops = case
+    N, M, K = dims
+    fd = object.__new__(FA.FlowAdjointDevice)           # the index state only, no contexts
+    fd.torch, fd.dev, fd.dims = torch, torch.device("cpu"), dims
+    fd.gsize = [int(np.prod(FA.grid_dims(d, dims))) for d in range(3)]
+    bc = np.array(geom["bc"], dtype=np.float64)
+    bc[12] = 0.7
+    fd._index_setup(geom["theta"], geom["delta"], bc, par["nu"])
+    src = FA.SourceTermTransposes(dims, geom["theta"], geom["delta"], bc, par["nu"])
+    rng = np.random.default_rng(9)
+    q = [rng.standard_normal(n) for n in fd.gsize]
+    for a, b in zip(fd._masks([fd._t(v) for v in q]), FA.outflow_clamp_mask(dims, *q)):
+        assert np.array_equal(a.numpy(), b)
+    cb, ux, uz = rng.standard_normal(fd.gsize[2]), rng.standard_normal(fd.gsize[0]), rng.standard_normal(fd.gsize[2])
+    ub = [torch.zeros(n, dtype=torch.float64) for n in fd.gsize]
+    uwb = torch.zeros(M * K, dtype=torch.float64)
+    fd._conv_flux_T(fd._t(cb), fd._t(ux), fd._t(uz), ub, uwb)
+    hx, hz, hw = src.convective_flux_T(cb, ux, uz)
+    assert np.allclose(ub[0].numpy(), hx, rtol=1e-13, atol=1e-15)
+    assert np.allclose(ub[2].numpy(), hz, rtol=1e-13, atol=1e-15)
+    assert np.allclose(uwb.numpy(), hw, rtol=1e-13, atol=1e-15)

@@ -96,3 +96,24 @@ def test_gradient_matches_oracle_and_differences(both):
         e[k] = h
         fd = (fg.forward(th0 + e, f0, u0, p0) - fg.forward(th0 - e, f0, u0, p0)) / (2 * h)
         assert abs(gth[k] - fd) <= 1e-4 * abs(fd), (k, gth[k], fd)
+
+
+def test_device_sweep_matches_host_sweep(both):
+    """FlowAdjointDevice (state, checkpoints and cotangents in device memory,
+    *_device entry points, boundary transposes as device index operations)
+    against FlowAdjoint on the same operators: the same solves on the same
+    inputs, so agreement to rounding (summation order of the index adds)."""
+    from lsstag_b200 import flow_adjoint as FA
+    geom, dims, par, gpu, cpu = both
+    u0, p0 = [geom["u_0"], geom["v_0"], geom["w_0"]], geom["p_0"]
+    rng = np.random.default_rng(24)
+    th0 = 0.05 * rng.standard_normal(8)
+    f0 = [0.01 * rng.standard_normal(a.size) for a in u0]
+    Jh, gh, fh = FA.FlowAdjoint(gpu, 4, every=2).gradient(th0, f0, u0, p0)
+    fd = FA.FlowAdjointDevice(gpu, 4, every=2)
+    Jd, gd, fdv = fd.gradient(th0, f0, u0, p0)
+    assert fd.stats == {"recomputed_steps": 4, "checkpoints": 2}
+    assert abs(Jd - Jh) <= 1e-10 * abs(Jh)
+    assert _rel(gd, gh) <= 1e-8
+    for a, b in zip(fdv, fh):
+        assert _rel(a, b) <= 1e-8
