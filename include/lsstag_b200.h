@@ -435,6 +435,32 @@ int lsg_precond_apply(lsg_ctx* ctx, const double* b, double* x);
    lsg_operator_gradient: grad[s*n + i] = -lambda_i x_{i + off_s} = dJ/dA for
      the seven planes of lsg_set_matrix_stencil7 (0 toward outside cells).
    Host buffers. */
+/* Tecplot solution file, byte for byte the file SolTecplotPrinter::printField
+   writes (Base/TecplotPrinters/sol_tecplot_printer.h:254-355, header of
+   BaseTecplotPrinter::init base_tecplot_printer.h:35-60): the (N+2) x (M+2)
+   x (K+2) points (walls, boundary rows, cell centres) with x y z P SPD_x
+   SPD_y SPD_z SPD in ostream's default format.  nodes: the cell-centre
+   coordinates (3 N M K, xyz interleaved, LSSTAGUniformMesh m_nodes); delta,
+   theta: as lsg_set_matrix_geometry; celltype: base cell types; u, v, w, p
+   the staggered velocities and the pressure; u_w the inflow profile (M K,
+   the task's pU_W; NULL: none); bc the 18 boundary velocities U_W U_E U_S
+   U_N U_B U_T V_W .. V_T W_W .. W_T; flow != 0 for a flow task (outflow
+   east, the B and T planes repeat the first and last layer).
+   lsg_tecplot_sol_write: host arrays, no context, no device work.
+   lsg_tecplot_sol_async: u, v, w, p on the device of a context holding the
+   base grid's geometry; the call copies them to pinned host memory (the
+   caller may overwrite them on return; they must be complete when the call
+   is made) and returns while a host thread formats and writes the file;
+   lsg_tecplot_wait joins that thread and returns its status.  One write in
+   flight per context (a second call waits for the first). */
+int lsg_tecplot_sol_write(const char* path, int N, int M, int K, const double* nodes, const double* delta,
+                          const double* theta, const int* celltype, const double* u, const double* v,
+                          const double* w, const double* p, const double* u_w, const double* bc, int flow);
+int lsg_tecplot_sol_async(lsg_ctx* ctx, const char* path, const double* nodes, const double* delta,
+                          const double* theta, const int* celltype, const double* u, const double* v,
+                          const double* w, const double* p, const double* u_w, const double* bc, int flow);
+int lsg_tecplot_wait(lsg_ctx* ctx);
+
 int lsg_apply_transpose(lsg_ctx* ctx, const double* x, double* y);
 int lsg_solve_adjoint(lsg_ctx* ctx, const double* g, double* lambda, lsg_stats* stats);
 int lsg_operator_gradient(lsg_ctx* ctx, const double* lambda, const double* x, double* grad);

@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <cstring>
 #include <memory>
+#include <thread>
 
 #include "lsg_coarse.cuh"
 #include "lsg_ilu.cuh"
@@ -16,6 +17,7 @@
 #include "lsg_helmholtz.cuh"
 #include "lsg_loads.cuh"
 #include "lsg_projection.cuh"
+#include "lsg_tecplot.cuh"
 
 namespace lsg {
 
@@ -180,6 +182,20 @@ struct MGData {
 // ---------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------
+// an asynchronous Tecplot write (lsg_tecplot_sol_async): pinned host copies
+// of u | v | w | p and the thread that formats and writes the file
+struct TecplotAsync {
+    std::thread th;
+    int status = 0;
+    double* pinned = nullptr;
+    size_t pinned_len = 0;
+    ~TecplotAsync()
+    {
+        if (th.joinable()) th.join();
+        if (pinned) cudaFreeHost(pinned);
+    }
+};
+
 struct Context {
     int device = 0;
     cudaStream_t s = nullptr;
@@ -219,6 +235,7 @@ struct Context {
     // adjoint: a second solver state for the transposed operator, built on
     // first use and dropped whenever the operator changes
     std::unique_ptr<Context> adj;
+    std::unique_ptr<TecplotAsync> tec;
     // cut-cell geometry kept on the device by lsg_set_matrix_geometry (the
     // projection kernels read it); staggered cell types from
     // lsg_set_staggered_types
@@ -2882,6 +2899,96 @@ int lsg_gradient_transpose(lsg_ctx* h, const double* gx, const double* gy, const
     LSG_CUDA(cudaStreamSynchronize(C.s));
     return LSG_OK;
     LSG_API_END(h)
+}
+
+int lsg_tecplot_sol_write(const char* path, int N, int M, int K, const double* nodes, const double* delta,
+                          const double* theta, const int* celltype, const double* u, const double* v,
+                          const double* w, const double* p, const double* u_w, const double* bc, int flow)
+{
+    if (!path || N < 2 || M < 2 || K < 3 || !nodes || !delta || !theta || !celltype || !u || !v || !w || !p || !bc)
+        return LSG_ERR_ARG;
+    try {
+        const std::string s = tecplot_sol_bytes(N, M, K, nodes, delta, theta, celltype, u, v, w, p, u_w, bc,
+                                                flow != 0);
+        FILE* f = std::fopen(path, "wb");
+        if (!f) return LSG_ERR_ARG;
+        const size_t wr = std::fwrite(s.data(), 1, s.size(), f);
+        const int cl = std::fclose(f);
+        return (wr == s.size() && cl == 0) ? LSG_OK : LSG_ERR_ARG;
+    } catch (const std::bad_alloc&) {
+        return LSG_ERR_NOMEM;
+    }
+}
+
+int lsg_tecplot_sol_async(lsg_ctx* h, const char* path, const double* nodes, const double* delta,
+                          const double* theta, const int* celltype, const double* u, const double* v,
+                          const double* w, const double* p, const double* u_w, const double* bc, int flow)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have, LSG_ERR_STATE, "a context holding the base grid's geometry is needed "
+                                           "(lsg_set_matrix_geometry)");
+    LSG_REQUIRE(path && nodes && delta && theta && celltype && u && v && w && p && bc, LSG_ERR_ARG, "null argument");
+    LSG_REQUIRE(C.d.N >= 2 && C.d.M >= 2 && C.d.K >= 3, LSG_ERR_ARG, "grid too small for the printer");
+    LSG_CUDA(cudaSetDevice(C.device));
+    if (!C.tec) C.tec.reset(new TecplotAsync);
+    TecplotAsync& T = *C.tec;
+    if (T.th.joinable()) T.th.join();                      // one write in flight per context
+    const int N = C.d.N, M = C.d.M, K = C.d.K;
+    const size_t n = (size_t)C.n, c0 = (size_t)(N - 1) * M * K, c1 = (size_t)N * (M - 1) * K,
+                 c2 = (size_t)N * M * (K - 1);
+    const size_t len = c0 + c1 + c2 + n;
+    if (T.pinned_len < len) {
+        if (T.pinned) cudaFreeHost(T.pinned);
+        T.pinned = nullptr;
+        T.pinned_len = 0;
+        LSG_CUDA(cudaMallocHost(&T.pinned, len * sizeof(double)));
+        T.pinned_len = len;
+    }
+    double* hp = T.pinned;
+    LSG_CUDA(cudaMemcpyAsync(hp, u, c0 * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaMemcpyAsync(hp + c0, v, c1 * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaMemcpyAsync(hp + c0 + c1, w, c2 * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaMemcpyAsync(hp + c0 + c1 + c2, p, n * 8, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));                  // the caller may overwrite the fields on return
+    std::vector<double> vn(nodes, nodes + 3 * n), vd(delta, delta + 3 * n), vt(theta, theta + 3 * n);
+    std::vector<int> vc(celltype, celltype + n);
+    std::vector<double> vw;
+    if (u_w) vw.assign(u_w, u_w + (size_t)M * K);
+    std::vector<double> vb(bc, bc + 18);
+    const std::string sp(path);
+    const bool fl = flow != 0;
+    T.status = LSG_OK;
+    TecplotAsync* tp = &T;
+    T.th = std::thread([tp, N, M, K, hp, c0, c1, c2, sp, fl, vn = std::move(vn), vd = std::move(vd),
+                        vt = std::move(vt), vc = std::move(vc), vw = std::move(vw), vb = std::move(vb)]() {
+        try {
+            const std::string s = tecplot_sol_bytes(N, M, K, vn.data(), vd.data(), vt.data(), vc.data(), hp, hp + c0,
+                                                    hp + c0 + c1, hp + c0 + c1 + c2,
+                                                    vw.empty() ? nullptr : vw.data(), vb.data(), fl);
+            FILE* f = std::fopen(sp.c_str(), "wb");
+            if (!f) {
+                tp->status = LSG_ERR_ARG;
+                return;
+            }
+            const size_t wr = std::fwrite(s.data(), 1, s.size(), f);
+            if (std::fclose(f) != 0 || wr != s.size()) tp->status = LSG_ERR_ARG;
+        } catch (const std::bad_alloc&) {
+            tp->status = LSG_ERR_NOMEM;
+        }
+    });
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_tecplot_wait(lsg_ctx* h)
+{
+    if (!h) return LSG_ERR_ARG;
+    if (!h->c.tec) return LSG_OK;
+    TecplotAsync& T = *h->c.tec;
+    if (T.th.joinable()) T.th.join();
+    return T.status;
 }
 
 int lsg_solve_adjoint(lsg_ctx* h, const double* g, double* lambda, lsg_stats* st)

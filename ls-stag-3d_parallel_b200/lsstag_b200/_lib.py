@@ -57,7 +57,8 @@ EXPORTS = [
     "lsg_loads_adjoint", "lsg_loads_adjoint_device", "lsg_set_matrix_helmholtz",
     "lsg_helmholtz_flux", "lsg_convective_flux", "lsg_convective_flux_device", "lsg_momentum_rhs_device",
     "lsg_convective_adjoint", "lsg_convective_adjoint_device", "lsg_gradient_transpose",
-    "lsg_gradient_transpose_device", "lsg_projection_adjoint_device",
+    "lsg_gradient_transpose_device", "lsg_projection_adjoint_device", "lsg_tecplot_sol_write",
+    "lsg_tecplot_sol_async", "lsg_tecplot_wait",
 ]
 
 _lib = None
@@ -121,6 +122,10 @@ def load() -> C.CDLL:
     lib.lsg_projection_adjoint.argtypes = [P, dp, dp, dp, dp, C.c_double, dp, dp, dp, dp, C.POINTER(Stats)]
     lib.lsg_gradient_transpose.argtypes = [P, dp, dp, dp, dp]
     lib.lsg_gradient_transpose_device.argtypes = [P] + [C.c_void_p] * 4
+    lib.lsg_tecplot_sol_write.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, dp, dp, dp, ip, dp, dp, dp, dp,
+                                          dp, dp, C.c_int]
+    lib.lsg_tecplot_sol_async.argtypes = [P, C.c_char_p, dp, dp, dp, ip] + [C.c_void_p] * 4 + [dp, dp, C.c_int]
+    lib.lsg_tecplot_wait.argtypes = [P]
     lib.lsg_projection_adjoint_device.argtypes = ([P] + [C.c_void_p] * 4 + [C.c_double] + [C.c_void_p] * 4
                                                   + [C.POINTER(Stats)])
     lib.lsg_laplace_flux_device.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p, dp, C.c_void_p, C.c_void_p]

@@ -441,6 +441,9 @@ int main(int argc, char** argv)
     double t0 = now_s();
     task->init(&curTime);
     SetSolutions* sol = new SetSolutions;
+    // print_sol: the solution printer (SolTecplotPrinter, set up by
+    // SetSolutions::init) prints on its first call
+    if ((int)cfg.get("print_sol", 0)) task->PeriodPrintSol = task->t;
     sol->init(task, &it);
     task->initSol(&(sol->current), &(sol->prediction), &(sol->previous));
     if ((int)cfg.get("flux_perturb", 0)) {
@@ -573,6 +576,24 @@ int main(int argc, char** argv)
             int itc = it;
             out.i("state_it", &itc, 1);
             out.scalar("state_time", curTime);
+        }
+        if ((int)cfg.get("print_sol", 0)) {
+            // the reference's own Tecplot solution file (SetSolutions::print ->
+            // SolTecplotPrinter::printField, sol_tecplot_printer.h:254-355) of
+            // the current state, returned byte for byte
+            sol->print();
+            std::string found;
+            for (const auto& e : std::filesystem::directory_iterator(outdir)) {
+                const std::string nm = e.path().filename().string();
+                if (nm.find("Sol") != std::string::npos && nm.rfind("continueSolveTask", 0) != 0 && nm.size() > 4 &&
+                    nm.substr(nm.size() - 4) == ".dat")
+                    found = e.path().string();
+            }
+            std::ifstream sf(found, std::ios::binary);
+            std::vector<char> bytes((std::istreambuf_iterator<char>(sf)), std::istreambuf_iterator<char>());
+            out.put("sol_bytes", (const unsigned char*)bytes.data(), (long)bytes.size(), "u1");
+            LSSTAGUniformMesh* pm = task->m_mesh;
+            out.d("nodes", (const double*)pm->nodes, 3L * pm->baseMesh.N * pm->baseMesh.M * pm->baseMesh.K);
         }
         int nthreads = omp_get_max_threads();
         out.i("omp_threads", &nthreads, 1);
