@@ -12,9 +12,12 @@
 // bytes equal the reference's file.
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <string>
+#include <thread>
+#include <vector>
 
 namespace lsg {
 
@@ -27,6 +30,7 @@ struct TecplotSol {
     long long num = 0, num2 = 0, num3 = 0, numW = 0, cur = 0;
     double tx = 0, ty = 0, tz = 0, tP = 0, Ux = 0, Uy = 0, Uz = 0;
     std::string out;
+    bool emit = true;   // false: the walk only advances the indices (the dry pass)
 
     static constexpr int kSolid = 0, kFluid = 11111111;
     static constexpr double kEq = 1e-5;   // EQ_DOUBLE (Base/ls_stag_real_constants.h)
@@ -34,6 +38,7 @@ struct TecplotSol {
     void setP() { tP = p[num]; }
     void node()
     {
+        if (!emit) return;
         const double U = std::sqrt(Ux * Ux + Uy * Uy + Uz * Uz);
         char buf[256];
         const int len = std::snprintf(buf, sizeof buf, "%g %g %g %g %g %g %g %g\n", tx, ty, tz, tP, Ux, Uy, Uz, U);
@@ -223,29 +228,22 @@ struct TecplotSol {
         ty += 0.5 * de[3 * num + 1];
         wall(V_N, U_N, W_N);
     }
-    void field()                                                 // printField
+    // the walk after the header is K + 2 segments, one per printed layer:
+    // 0 the bottom plane, 1 the first cell layer, 2 .. K-1 the interior
+    // layers, K the last cell layer, K + 1 the top plane; each starts from
+    // the running indices the previous one left (the top plane from those
+    // the last cell layer started with)
+    void segment(int sg)
     {
-        out.reserve((size_t)(N + 2) * (M + 2) * (K + 2) * 72 + 256);
-        out += "TITLE     = \"Velocity Vectors\" \n";
-        out += "VARIABLES = \"x\" \n";
-        for (const char* name : {"y", "z", "P", "SPD_x", "SPD_y", "SPD_z", "SPD"}) {
-            out += "\"";
-            out += name;
-            out += "\"\n";
-        }
-        out += "ZONE T=\"Data\" \n";
-        char buf[96];
-        std::snprintf(buf, sizeof buf, "I=%d, J=%d, K=%d, F=POINT\n", N + 2, M + 2, K + 2);
-        out += buf;
-        tx = ty = tz = 0.0;
-        num = 0;
-        cur = 0;
-        if (flow)
-            layer_b(true);
-        else
-            wall_plane(V_B, U_B, W_B);
-        layer_b(false);
-        for (int k = 1; k < zK; k++) {
+        if (sg == 0) {
+            if (flow)
+                layer_b(true);
+            else
+                wall_plane(V_B, U_B, W_B);
+        } else if (sg == 1) {
+            layer_b(false);
+        } else if (sg <= zK) {
+            const int k = sg - 1;
             ty = 0.0;
             tz = Z(cur);
             wall(V_S, U_S, W_S);
@@ -266,15 +264,9 @@ struct TecplotSol {
             tx = 0.0;
             ty += 0.5 * de[3 * num + 1];
             wall(V_N, U_N, W_N);
-        }
-        const long long s0 = num, s1 = num2, s2 = num3, s3 = numW, s4 = cur;
-        layer_t(false);
-        num = s0;
-        num2 = s1;
-        num3 = s2;
-        numW = s3;
-        cur = s4;
-        if (flow) {
+        } else if (sg == zK + 1) {
+            layer_t(false);
+        } else if (flow) {
             layer_t(true);
         } else {
             const long long nT = (long long)NMK - NM;
@@ -282,7 +274,85 @@ struct TecplotSol {
             wall_plane(V_T, U_T, W_T);
         }
     }
+    struct State {
+        long long num, num2, num3, numW, cur;
+        double tx, ty, tz, tP, Ux, Uy, Uz;
+    };
+    State state() const { return {num, num2, num3, numW, cur, tx, ty, tz, tP, Ux, Uy, Uz}; }
+    void set_state(const State& q)
+    {
+        num = q.num;
+        num2 = q.num2;
+        num3 = q.num3;
+        numW = q.numW;
+        cur = q.cur;
+        tx = q.tx;
+        ty = q.ty;
+        tz = q.tz;
+        tP = q.tP;
+        Ux = q.Ux;
+        Uy = q.Uy;
+        Uz = q.Uz;
+    }
+    static std::string header(int N, int M, int K)
+    {
+        std::string h = "TITLE     = \"Velocity Vectors\" \n";
+        h += "VARIABLES = \"x\" \n";
+        for (const char* name : {"y", "z", "P", "SPD_x", "SPD_y", "SPD_z", "SPD"}) {
+            h += "\"";
+            h += name;
+            h += "\"\n";
+        }
+        h += "ZONE T=\"Data\" \n";
+        char buf[96];
+        std::snprintf(buf, sizeof buf, "I=%d, J=%d, K=%d, F=POINT\n", N + 2, M + 2, K + 2);
+        h += buf;
+        return h;
+    }
 };
+
+// The file's bytes: a dry pass records the running indices at the start of
+// every segment, then groups of consecutive segments are formatted on up
+// to `threads` threads and joined in order (the same bytes as one walk).
+inline std::string tecplot_sol_text(const TecplotSol& proto, int threads)
+{
+    const int nseg = proto.K + 2;
+    std::vector<TecplotSol::State> start((size_t)nseg + 1);
+    TecplotSol dry = proto;
+    dry.emit = false;
+    dry.tx = dry.ty = dry.tz = 0.0;
+    dry.num = dry.cur = 0;
+    for (int sg = 0; sg < nseg; sg++) {
+        start[(size_t)sg] = dry.state();
+        if (sg == nseg - 1) dry.set_state(start[(size_t)nseg - 2]);   // the top plane restarts from the last layer
+        dry.segment(sg);
+    }
+    start[(size_t)nseg - 1] = start[(size_t)nseg - 2];
+    const int nt = std::max(1, std::min(threads, nseg));
+    std::vector<std::string> parts((size_t)nt);
+    auto work = [&](int t) {
+        const int s0 = (int)((long long)nseg * t / nt), s1 = (int)((long long)nseg * (t + 1) / nt);
+        TecplotSol w = proto;
+        w.emit = true;
+        w.out.clear();
+        w.out.reserve((size_t)(s1 - s0) * (w.N + 2) * (w.M + 2) * 72);
+        for (int sg = s0; sg < s1; sg++) {
+            w.set_state(start[(size_t)sg]);
+            w.segment(sg);
+        }
+        parts[(size_t)t] = std::move(w.out);
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
+    std::string out = TecplotSol::header(proto.N, proto.M, proto.K);
+    size_t total = out.size();
+    for (const auto& s : parts) total += s.size();
+    out.reserve(total);
+    for (const auto& s : parts) out += s;
+    return out;
+}
 
 // the file's bytes for host arrays (bc: U_W U_E U_S U_N U_B U_T, V_W .. V_T, W_W .. W_T)
 inline std::string tecplot_sol_bytes(int N, int M, int K, const double* nodes, const double* delta,
@@ -311,8 +381,8 @@ inline std::string tecplot_sol_bytes(int N, int M, int K, const double* nodes, c
                      &t.V_N, &t.V_B, &t.V_T, &t.W_W, &t.W_E, &t.W_S, &t.W_N, &t.W_B, &t.W_T};
     for (int i = 0; i < 18; i++) *f[i] = bc[i];
     t.flow = flow;
-    t.field();
-    return std::move(t.out);
+    const unsigned hc = std::thread::hardware_concurrency();
+    return tecplot_sol_text(t, (int)std::min(hc ? hc : 1u, 16u));
 }
 
 }  // namespace lsg
