@@ -350,6 +350,7 @@ def config_dict(args, world):
                         if getattr(args, "smoother", "adlj") == "rbgs"
                         else "Galerkin MG, ADLJ z/y/x line smoother V(0,3), omega 0.805"),
             "l2": "inputs larger than L2 (operator 0.94 GB FP64 + Krylov basis)",
+            "pins": getattr(args, "pins", "reference"),
             "parallelism": "replicas" if world > 1 else "single GPU"}
 
 
@@ -373,6 +374,9 @@ def main():
                     help="poisson: the 256^3 pressure solve (the headline); flow: time steps of the flow past "
                          "a sphere at 128x64x64 (every operator of the step on the GPU); adjoint: the drag "
                          "gradient through time steps of that flow (use --steps 1)")
+    ap.add_argument("--pins", default="reference", choices=["reference", "negated"],
+                    help="poisson workload, this arm: the reference's +1 identity pins (default) or the same "
+                         "system with the pinned rows negated")
     ap.add_argument("--adjoint-steps", type=int, default=50, help="time steps of one adjoint gradient")
     ap.add_argument("--checkpoint-every", type=int, default=10, help="checkpoint interval of the adjoint sweep")
     ap.add_argument("--adjoint-sweep", default="device", choices=["device", "host"],
@@ -401,6 +405,10 @@ def main():
 
     torch.cuda.set_device(local)
     P, dims, pins, b = cases.load(args.size)
+    if args.pins == "negated":
+        # the same system with the pinned rows negated (b is 0 there: same
+        # solution); the multigrid hierarchy then has no wrong-signed rows
+        P = S.pins_negated(P, pins)
     n = b.size
     bnorm = float(np.linalg.norm(b))
     task = S.Task(eps=1e-10 * bnorm, MAX_ITER=200, FGMRES_RESTART_NUM=args.restart,
