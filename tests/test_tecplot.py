@@ -52,3 +52,17 @@ def test_cell_centres_are_the_reference_nodes():
     from lsstag_b200 import tecplot
     t, g, dims = _case()
     assert np.array_equal(tecplot.cell_centres(dims, (1 / 16, 1 / 16, 1 / 16)), t["nodes"])
+
+
+def test_threaded_writer_at_full_size(tmp_path):
+    """The 128x64x64 flow case's initial state: the library formats the 66
+    layers on several threads from a dry walk's running indices; the bytes
+    equal the oracle's single walk (19 MB)."""
+    from lsstag_b200 import cases, tecplot
+    g, dims, par, (u, v, w, p) = cases.load_flow_case()
+    nodes = tecplot.cell_centres(dims, (1 / 16, 1 / 16, 1 / 16))
+    path = tmp_path / "sol.dat"
+    tecplot.write_sol(path, dims, nodes, g, u, v, w, p, flow=True)
+    ref = lo.tecplot_sol(*dims, nodes, g["delta"], g["theta"], g["celltype"], u, v, w, p, g["u_w"], g["bc"], True)
+    assert len(ref) > 18_000_000
+    assert path.read_bytes() == ref
