@@ -452,7 +452,9 @@ int lsg_precond_apply(lsg_ctx* ctx, const double* b, double* x);
    caller may overwrite them on return; they must be complete when the call
    is made) and returns while a host thread formats and writes the file;
    lsg_tecplot_wait joins that thread and returns its status.  One write in
-   flight per context (a second call waits for the first). */
+   flight per context (a second call waits for the first).  The status is
+   sticky: the first failure of any write since the last lsg_tecplot_wait is
+   what lsg_tecplot_wait returns, and that call clears it. */
 int lsg_tecplot_sol_write(const char* path, int N, int M, int K, const double* nodes, const double* delta,
                           const double* theta, const int* celltype, const double* u, const double* v,
                           const double* w, const double* p, const double* u_w, const double* bc, int flow);
@@ -494,7 +496,9 @@ int lsg_profile_kernel(lsg_ctx* ctx, int which, int reps, double* ms_per_launch,
    program).  All pointers are device pointers owned by the caller; r may be
    NULL (norm only); *norm2 receives ||b - A x||^2 (FP64).  Work is queued on
    `stream` (a cudaStream_t, NULL = legacy default stream); read *norm2 after
-   synchronising it.  Scratch is a file-scope device array of the library
+   synchronising it.  The stream must belong to the calling thread's current
+   device: the scratch address used is the current device's, and the
+   pointers must be that device's memory.  Scratch is a file-scope device array of the library
    (4096 block partials + a counter, about 32 KiB per GPU, held until the
    process exits), which caps the grid at 16,777,216 cells; larger grids are
    rejected with LSG_ERR_ARG and a message on stderr.  The first call on a

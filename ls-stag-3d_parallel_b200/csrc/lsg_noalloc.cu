@@ -101,14 +101,17 @@ extern "C" int lsg_residual_norm_noalloc(int N, int M, int K, const double* plan
                                          const double* b, double* r, double* norm2, void* stream)
 {
     if (N < 1 || M < 1 || K < 1 || !planes || !x || !b || !norm2) return LSG_ERR_ARG;
-    const long long n = (long long)N * M * K;
-    if (n > kMaxCells) {
+    // compare before multiplying all three: N*M*K of three large ints can
+    // overflow 64 bits, M*K (< 2^62) cannot
+    const long long MK = (long long)M * K;
+    if (MK > kMaxCells || (long long)N > kMaxCells / MK) {
         fprintf(stderr,
-                "lsg_residual_norm_noalloc: %lld cells exceed the fixed scratch capacity of %lld cells "
+                "lsg_residual_norm_noalloc: a %d x %d x %d grid exceeds the fixed scratch capacity of %lld cells "
                 "(%d blocks of %lld cells)\n",
-                n, kMaxCells, kMaxBlocks, kCellsPerBlock);
+                N, M, K, kMaxCells, kMaxBlocks, kCellsPerBlock);
         return LSG_ERR_ARG;
     }
+    const long long n = (long long)N * MK;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return LSG_ERR_CUDA;
     double* scratch = nullptr;

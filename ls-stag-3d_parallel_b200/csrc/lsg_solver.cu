@@ -673,6 +673,16 @@ static void mg_setup(Context& C)
             }
             first0[i] = (firstcol == 0);
         }
+        // the reference's pivot clamp (1e-13 max|A|) keeps any nonzero
+        // coarsest matrix factorable; a zero or non-finite one is not
+        double amax = 0.0;
+        bool finite = true;
+        for (const double v : A) {
+            finite = finite && std::isfinite(v);
+            amax = std::max(amax, std::fabs(v));
+        }
+        LSG_REQUIRE(finite && amax > 0.0, LSG_ERR_SINGULAR,
+                    "coarsest multigrid operator is zero or holds NaN/Inf: no LU factorisation");
         std::vector<double> Lh, Uh, sc;
         std::vector<int> pm;
         coarse_lu(nc, A, first0, Lh, Uh, sc, pm);
@@ -1148,7 +1158,10 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
     double norm_r = std::sqrt(nrm2);
     int it = 0;
     int status = LSG_OK;
-    if (norm_r > C.opt.eps) {
+    // a NaN or Inf in b, x or the operator: no iteration can help (the
+    // reference would iterate to MAX_ITER on NaNs and report nothing)
+    if (!std::isfinite(norm_r)) status = LSG_BREAKDOWN;
+    else if (norm_r > C.opt.eps) {
         it = 1;
         // initialise device scalars: norm_r, invNormW = 1/norm_r, it
         KrylovScalars h;
@@ -1430,7 +1443,8 @@ static int bicgstab(Context& C, double* x, const double* b, lsg_stats* st)
     LSG_CUDA(cudaStreamSynchronize(s));
     double norm_r = std::sqrt(nr2);
     int status = LSG_OK;
-    if (norm_r > C.opt.eps) {
+    if (!std::isfinite(norm_r)) status = LSG_BREAKDOWN;
+    else if (norm_r > C.opt.eps) {
         LSG_CUDA(cudaMemcpyAsync(rr, r, n * 8, cudaMemcpyDeviceToDevice, s));
         LSG_CUDA(cudaMemcpyAsync(p, r, n * 8, cudaMemcpyDeviceToDevice, s));
         do {
@@ -1451,7 +1465,7 @@ static int bicgstab(Context& C, double* x, const double* b, lsg_stats* st)
             norm_r = std::sqrt(nr2);
             it++;
             bytes += 8.0 * n * (10 + 4 + 10 + 10 + 5) + (C.opt.precond == LSG_PC_ILU0 ? 2 * 8.0 * n * 12 : 0.0);
-            if (std::isnan(norm_r)) {
+            if (!std::isfinite(norm_r)) {
                 status = LSG_BREAKDOWN;
                 break;
             }
@@ -2959,7 +2973,8 @@ int lsg_tecplot_sol_async(lsg_ctx* h, const char* path, const double* nodes, con
     std::vector<double> vb(bc, bc + 18);
     const std::string sp(path);
     const bool fl = flow != 0;
-    T.status = LSG_OK;
+    // the status stays sticky: an error of an earlier write that nobody
+    // collected with lsg_tecplot_wait survives this new write
     TecplotAsync* tp = &T;
     T.th = std::thread([tp, N, M, K, hp, c0, c1, c2, sp, fl, vn = std::move(vn), vd = std::move(vd),
                         vt = std::move(vt), vc = std::move(vc), vw = std::move(vw), vb = std::move(vb)]() {
@@ -2976,6 +2991,9 @@ int lsg_tecplot_sol_async(lsg_ctx* h, const char* path, const double* nodes, con
             if (std::fclose(f) != 0 || wr != s.size()) tp->status = LSG_ERR_ARG;
         } catch (const std::bad_alloc&) {
             tp->status = LSG_ERR_NOMEM;
+        } catch (...) {
+            // nothing may escape a std::thread (it would end the process)
+            tp->status = LSG_ERR_ARG;
         }
     });
     return LSG_OK;
@@ -2988,7 +3006,9 @@ int lsg_tecplot_wait(lsg_ctx* h)
     if (!h->c.tec) return LSG_OK;
     TecplotAsync& T = *h->c.tec;
     if (T.th.joinable()) T.th.join();
-    return T.status;
+    const int st = T.status;
+    T.status = LSG_OK;       // collected: the next write starts clean
+    return st;
 }
 
 int lsg_solve_adjoint(lsg_ctx* h, const double* g, double* lambda, lsg_stats* st)

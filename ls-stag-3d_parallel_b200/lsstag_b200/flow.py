@@ -30,7 +30,8 @@ class FlowStepper:
     alpha, delta, inv_vof, vof_x/y/z, inv_mx/my/mz, dib_en/ws/nb/st,
     inv_dib_ne/tn, vib, vibyx, vibzy, u_w, bc (18 boundary velocities), pins);
     par: nu, coef (1.5/dt), coef2 (1/dt), coef_integr (COEF_INTEGR_TIME), eps
-    (absolute), vbase, max_it, restart_mom, restart_p."""
+    (absolute), vbase, max_it, restart_mom, restart_p; optional eps_p, an
+    absolute tolerance of the pressure solve alone (default eps)."""
 
     def __init__(self, geom: dict, dims, par: dict, u0, v0, w0, p0, device: int = 0, pressure_mg_fp32: bool = False):
         self.g = geom
@@ -41,7 +42,8 @@ class FlowStepper:
         self.bc = bc
         # U_E, V_S, V_N, W_B, W_T of the pressure equation's source term
         self.bc_lap = bc[[1, 8, 9, 16, 17]].copy()
-        ptask = S.Task(eps=par["eps"], MAX_ITER=int(par["max_it"]), FGMRES_RESTART_NUM=int(par["restart_p"]))
+        ptask = S.Task(eps=par.get("eps_p", par["eps"]), MAX_ITER=int(par["max_it"]),
+                       FGMRES_RESTART_NUM=int(par["restart_p"]))
         # pressure: the operator assembled from the geometry (it also serves the
         # projection entry points) solved by MG-FGMRES with the FP64 cycle, as
         # the reference does; or, with pressure_mg_fp32, by MG-FGMRES with the

@@ -42,22 +42,45 @@ def test_fp32_pressure_flow16_matches_reference_steps():
 
 
 def test_fp32_pressure_flow_128x64x64_converges():
-    """Three steps of the 128x64x64 flow: the FP32-cycle pressure solve
-    converges to the reference's absolute eps 1e-5 in a few iterations (the
-    reference's FP64 cycle takes 5 on the first step) and the state follows
-    the FP64 stepper's within 1e-3 (both stop at an absolute residual of
-    1e-5, a relative one of about 1.6e-4 on this right-hand side)."""
+    """Three steps of the 128x64x64 flow with the reference's absolute eps
+    1e-5: the FP32-cycle pressure solve converges in a few iterations (the
+    reference's FP64 cycle takes 5 on the first step; on the reference's
+    own pins the FP32 cycle stalled at the 200-iteration cap)."""
     from lsstag_b200 import cases
     from lsstag_b200.flow import FlowStepperDevice
     g, dims, par, (u0, v0, w0, p0) = cases.load_flow_case()
-    states = []
+    fs = FlowStepperDevice(g, dims, par, u0, v0, w0, p0, pressure_mg_fp32=True)
+    its = [fs.step() for _ in range(3)]
+    fs.close()
+    assert all(0 < i[3] <= 8 for i in its), its
+
+
+def test_fp32_pressure_flow_128x64x64_state_matches_fp64():
+    """The FP32-cycle and FP64-cycle steppers reach the same state when the
+    pressure is solved tightly.  At the reference's eps 1e-5 (a relative
+    residual of about 1.6e-4) two stopped solutions may differ by up to
+    2e-5 / sigma_min in phi (sigma_min of the pressure operator about
+    4e-5): a 2.4e-3 relative gap in u was measured there, which says
+    nothing about either path.  With the pressure stopped at an absolute
+    1e-11 instead, ||dphi|| <= 2e-11 / 4e-5 = 5e-7, the correction
+    M^-1 G dphi moves u by at most 2/h * 5e-7 = 1.6e-5 (h = 1/16) against
+    ||u|| of about 700, i.e. 2.3e-8 per step relative; the momentum solves
+    (same eps 1e-5 on both sides, started from states that differ by that)
+    carry it over three steps.  1e-6 leaves a factor of 40."""
+    from lsstag_b200 import cases
+    from lsstag_b200.flow import FlowStepperDevice
+    g, dims, par, (u0, v0, w0, p0) = cases.load_flow_case()
+    par = dict(par, eps_p=1e-11)
+    states, iters = [], []
     for fp32 in (False, True):
         fs = FlowStepperDevice(g, dims, par, u0, v0, w0, p0, pressure_mg_fp32=fp32)
-        its = [fs.step() for _ in range(3)]
-        if fp32:
-            assert all(i[3] <= 8 for i in its), its
+        iters.append([fs.step()[3] for _ in range(3)])
         states.append(fs.state())
+        planes = fs.host.pres.planes()
         fs.close()
+    live = (np.abs(planes).sum(axis=0) != 0) & (np.asarray(g["celltype"]) != 0)
     (u64, p64), (u32, p32) = states
-    for a, b in zip(u32, u64):
-        assert _rel(a, b) <= 1e-3
+    errs = [_rel(a, b) for a, b in zip(u32, u64)] + [_rel(p32[live], p64[live])]
+    print("fp32 vs fp64 pressure, 128x64x64, eps_p 1e-11: iterations", iters, "rel u, v, w, p", errs)
+    assert max(errs[:3]) <= 1e-6, errs
+    assert errs[3] <= 1e-6, errs

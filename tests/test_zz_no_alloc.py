@@ -5,8 +5,9 @@ that is recording a CUDA graph, or a solver embedded under a device-memory
 budget its host application owns -- so it takes every buffer from the
 caller and keeps its only scratch in a fixed device array of the library.
 This checks it, through the C ABI, against the context-based operator apply
-on two calls in a row.  The file sorts last so that a run stopping at the
-first failure has already run every other test."""
+on two calls in a row, with and without the residual vector.  Its file name
+puts it after every other test file in pytest's collection order, so a run
+that stops at the first failure has already run the rest."""
 import ctypes
 
 import numpy as np
@@ -64,6 +65,14 @@ def test_residual_norm_noalloc_matches_context_apply():
         assert np.linalg.norm(r - r_ref) <= 1e-14 * np.linalg.norm(r_ref), call
         nrm = float(nrm_d.item())
         assert nrm == pytest.approx(float(np.dot(r_ref, r_ref)), rel=1e-12), call
+        # norm only (r = NULL): the same partial sums, so the same bits
+        nrm_d.zero_()
+        rc = lib.lsg_residual_norm_noalloc(N, M, K, ctypes.c_void_p(planes_d.data_ptr()),
+                                           ctypes.c_void_p(x_d.data_ptr()), ctypes.c_void_p(b_d.data_ptr()),
+                                           None, ctypes.c_void_p(nrm_d.data_ptr()), ctypes.c_void_p(stream))
+        assert rc == L.LSG_OK
+        torch.cuda.synchronize()
+        assert float(nrm_d.item()) == nrm, call
     s.close()
 
 
@@ -72,4 +81,8 @@ def test_residual_norm_noalloc_rejects_oversize_grid():
     lib = L.load()
     one = ctypes.c_void_p(8)   # never dereferenced: the size check comes first
     rc = lib.lsg_residual_norm_noalloc(512, 256, 256, one, one, one, None, one, None)
+    assert rc == L.LSG_ERR_ARG
+    # N*M*K beyond 2^63: rejected, not wrapped to a small or negative count
+    big = 2**31 - 1
+    rc = lib.lsg_residual_norm_noalloc(big, big, big, one, one, one, None, one, None)
     assert rc == L.LSG_ERR_ARG
