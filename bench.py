@@ -146,7 +146,7 @@ def reference_solve_ms(P, dims, b, threads, repeats):
     import ref_runner as rr
     r = rr.run_planes(P, dims, b, threads=threads, fgmres=1, bicgstab=0, restart=30, rel_tol=1e-10,
                       max_it=200, repeats=repeats, timeout=3600)
-    return [1e3 * t for t in r["fgmres_time_s"]], int(r["fgmres_it"][0]), int(r["omp_threads"][0])
+    return [1e3 * t for t in r["fgmres_time_s"]], int(r["fgmres_it"][0]), int(r["omp_threads"][0]), r["fgmres_x"]
 
 
 def run_reference_arm(args, world, rank):
@@ -163,7 +163,7 @@ def run_reference_arm(args, world, rank):
                           "reference sources at build time)"}))
         return 0
     warm = min(args.warmup, 1)
-    times, it, th = reference_solve_ms(P, dims, b, threads, warm + args.steps)
+    times, it, th, _ = reference_solve_ms(P, dims, b, threads, warm + args.steps)
     timed = times[warm:]
     ms = sum(timed) / len(timed)
     out = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms/solve", "n_gpus": world,
@@ -172,7 +172,8 @@ def run_reference_arm(args, world, rank):
            "iterations": it,
            "cpu_baseline": {"value": ms, "unit": "ms/solve", "cores": th, "kind": "reference",
                             "sample": f"{len(timed)} full {args.size}^3 MG-FGMRES(30) solves to 1e-10 "
-                                      f"(reference LS-STAG-3D OpenMP build, {th} threads)"},
+                                      f"(reference LS-STAG-3D OpenMP build, g++ -O2, {th} threads)"},
+           "gram_schmidt": "modified Gram-Schmidt, one pass per basis vector (the reference's own)",
            "e2e": {"value": ms, "unit": "ms/solve", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
@@ -345,7 +346,7 @@ def run_adjoint(args, world, rank, local, pg):
 def config_dict(args, world):
     return {"workload": f"poisson_spheres4_{args.size}^3_mgfgmres30_rel1e-10",
             "grid": [args.size] * 3, "bodies": "4 seeded spheres (seed 3), Neumann walls, 2 pinned rows",
-            "krylov": f"FGMRES({getattr(args, 'restart', 30)}) FP64, modified Gram-Schmidt ({getattr(args, 'gs', 'mgs')} form)",
+            "krylov": f"FGMRES({getattr(args, 'restart', 30)}) FP64, modified Gram-Schmidt projections",
             "precond": ("Galerkin MG, red-black / 8-colour Gauss-Seidel V(2,2)"
                         if getattr(args, "smoother", "adlj") == "rbgs"
                         else "Galerkin MG, ADLJ z/y/x line smoother V(0,3), omega 0.805"),
@@ -405,6 +406,24 @@ def main():
 
     torch.cuda.set_device(local)
     P, dims, pins, b = cases.load(args.size)
+    # the operator as the product builds it: the flow task's mesh build and
+    # the Laplace assembly on the GPU from the seeded spheres alone; it must
+    # equal, bit for bit, the reference's own assembly stored in the case file
+    from lsstag_b200 import mesh as MS
+    from lsstag_b200 import synth
+    hcell = (1.0 / args.size,) * 3
+    sph = synth.four_spheres(3)
+    sm = S.MGFGMRES(device=local)
+    t0 = time.perf_counter()
+    mesh_ms = sm.build_mesh(dims, hcell, MS.flow_block(dims, hcell, sph), bodies=MS.bodies_array(sph))
+    sm.set_from_mesh(pins, setup=False)
+    torch.cuda.synchronize()
+    setup_wall_ms = 1e3 * (time.perf_counter() - t0)
+    P_gpu = sm.planes()
+    sm.close()
+    operator_bitwise = bool(P_gpu.tobytes() == P.tobytes())
+    P = P_gpu
+    del P_gpu
     if args.pins == "negated":
         # the same system with the pinned rows negated (b is 0 there: same
         # solution); the multigrid hierarchy then has no wrong-signed rows
@@ -505,6 +524,9 @@ def main():
         "iterations": {"fp32": results["fp32"]["it"], "fp64": results["fp64"]["it"]},
         "true_rel_residual": {"fp32": results["fp32"]["true_res"] / bnorm, "fp64": results["fp64"]["true_res"] / bnorm},
         "rel_l2_fp32_vs_fp64": err,
+        "gram_schmidt": f"modified Gram-Schmidt, {args.gs} schedule",
+        "operator": {"built_on_gpu_from_seed": True, "bitwise_equal_to_reference_assembly": operator_bitwise,
+                     "mesh_build_ms": mesh_ms, "mesh_and_assembly_wall_ms": setup_wall_ms},
         "solve_algorithmic_gbs": results["fp32"]["bytes"] / results["fp32"]["ms_per_solve"] / 1e6,
         "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
@@ -521,11 +543,16 @@ def main():
             import ref_runner as rr
             if rr.available():
                 threads = os.cpu_count() or 1
-                times, it, th = reference_solve_ms(P, dims, b, threads, 1)
+                times, it, th, x_ref = reference_solve_ms(P, dims, b, threads, 1)
                 out["cpu_baseline"] = {"value": times[0], "unit": "ms/solve", "cores": th, "kind": "reference",
                                        "iterations": it,
                                        "sample": f"one full {args.size}^3 MG-FGMRES(30) solve to 1e-10 on the same "
-                                                 f"operator and right-hand side (reference OpenMP build, {th} threads)"}
+                                                 f"operator and right-hand side (reference OpenMP build, g++ -O2, "
+                                                 f"{th} threads)"}
+                rn = float(np.linalg.norm(x_ref))
+                out["rel_l2_vs_reference"] = {"fp32": float(np.linalg.norm(x32 - x_ref) / rn),
+                                              "fp64": float(np.linalg.norm(x64 - x_ref) / rn),
+                                              "reference_iterations": it}
             else:
                 out["cpu_baseline"] = None
         except Exception as e:  # report, do not hide

@@ -508,6 +508,68 @@ int lsg_profile_kernel(lsg_ctx* ctx, int which, int reps, double* ms_per_launch,
 int lsg_residual_norm_noalloc(int N, int M, int K, const double* planes, const double* x, const double* b,
                               double* r, double* norm2, void* stream);
 
+/* Mesh build of the flow task on the device: the restatement, for a uniform
+   grid, of BaseTaskDescription::buildMesh (base_task_description.h:330-371)
+   for a flow past fixed bodies -- the level set (the task's buildLS, e.g.
+   FlowSphereTaskDescription::calcLevelSetSphere,
+   flow_sphere_task_description.h:57-74), the edge fractions alpha with the
+   in-place oscillation fix (FlowTaskDescription::calcAlpha,
+   flow_task_description.h:102-136; checkOscLS / BuildAlpha,
+   ls_stag_uniform_mesh.h:2906-2963), face and cell types (calcTypeOfCells,
+   flow_task_description.h:175-230; TypeOfSide / TypeOfCell,
+   ls_stag_uniform_mesh.h:2969-2977, :3624-3675), face fractions theta
+   (calcTheta; getThetaZ / BuildTheta / tbBuildTheta, :1652-1837), cell
+   volumes (kernel v, :1838-2714) and their inverses
+   (ls_stag_base_mesh_params.h:77-85), staggered cell types (cvu / cvv / cvw,
+   :108-136), staggered volumes (mx / my / mz, :2804-2826) and their inverses.
+   Bit-identical to the reference's arrays.
+     N, M, K    base grid; h[3] the uniform cell sizes (nodes at (i + 1/2) h);
+     block[4]   the level-set block hs, hf, vs, vf of the task (the reference's
+                hs_loc .. vf_loc, flow_task_description.h:388-398): cells
+                [hs, hf) x [vs, vf) x [0, K) are built from the level set, all
+                others are plain fluid / box-border cells;
+                1 <= hs < hf <= N-1, 1 <= vs < vf <= M-1;
+     bodies     n_bodies records of 17 doubles (kind 0 sphere / 1 ellipsoid,
+                centre[3], radius, semi-axes[3], rotation[9] row major, body
+                frame = R (x - c)), merged by max (phi > 0 inside); or
+     phi        (host, N*M*K doubles, used when not NULL) the task's own level
+                set at the upper cell corners; values outside the block are
+                taken as 0, as the reference's walks find them;
+     *ms        (may be NULL) device time of the build.
+   The mesh stays on the device of the context. */
+int lsg_mesh_build(lsg_ctx* ctx, int N, int M, int K, const double* h, const int* block, int n_bodies,
+                   const double* bodies, const double* phi, double* ms);
+/* Copy one array of the built mesh to host memory `out` (the reference's
+   layouts: coord triples x, y, z per cell for alpha, theta, delta and the
+   side types (east, north, top faces); staggered arrays on the x-grid
+   (N-1)MK, y-grid N(M-1)K, z-grid NM(K-1)). */
+#define LSG_MESH_PHI_LS 0     /* level set as evaluated (double n) */
+#define LSG_MESH_PHI 1        /* after the oscillation fix (double n) */
+#define LSG_MESH_ALPHA 2      /* double 3n */
+#define LSG_MESH_SIDE_TYPE 3  /* int 3n (SideTypes codes) */
+#define LSG_MESH_CELL_TYPE 4  /* int n (CellTypes codes) */
+#define LSG_MESH_THETA 5      /* double 3n */
+#define LSG_MESH_DELTA 6      /* double 3n */
+#define LSG_MESH_VOF 7        /* double n */
+#define LSG_MESH_INV_VOF 8    /* double n */
+#define LSG_MESH_XTYPE 9      /* int, x-grid */
+#define LSG_MESH_YTYPE 10     /* int, y-grid */
+#define LSG_MESH_ZTYPE 11     /* int, z-grid */
+#define LSG_MESH_VOF_X 12     /* double, x-grid */
+#define LSG_MESH_VOF_Y 13
+#define LSG_MESH_VOF_Z 14
+#define LSG_MESH_INV_MX 15    /* double, x-grid: 1 / M_x */
+#define LSG_MESH_INV_MY 16
+#define LSG_MESH_INV_MZ 17
+int lsg_mesh_get(lsg_ctx* ctx, int field, void* out);
+/* Fixed-point sweeps the oscillation fix took in the last build (>= 1). */
+int lsg_mesh_osc_sweeps(const lsg_ctx* ctx);
+/* Set the context's operator to the Laplace operator assembled from the
+   built mesh (lsg_set_matrix_geometry on the device-resident arrays, with
+   the staggered types of lsg_set_staggered_types), pin0 / pin1 the pinned
+   rows (N-1 and NM-1 for the flow task). */
+int lsg_set_matrix_mesh(lsg_ctx* ctx, long long pin0, long long pin1);
+
 /* Library build string (version, arch). */
 const char* lsg_version(void);
 

@@ -16,6 +16,7 @@
 #include "lsg_krylov.cuh"
 #include "lsg_helmholtz.cuh"
 #include "lsg_loads.cuh"
+#include "lsg_mesh.cuh"
 #include "lsg_projection.cuh"
 #include "lsg_tecplot.cuh"
 
@@ -245,6 +246,15 @@ struct Context {
         long long pin0 = -1, pin1 = -1;
         bool have = false, have_stypes = false;
     } geo;
+    // the mesh built on the device by lsg_mesh_build (the flow task's mesh
+    // build: level set to staggered inverse volumes)
+    struct Mesh {
+        int N = 0, M = 0, K = 0;
+        DevBuf<double> phi_ls, phi, alpha, theta, delta, vof, inv_vof, svof[3], sinv[3];
+        DevBuf<int> side, type, stype[3];
+        int osc_sweeps = 0;
+        bool have = false;
+    } mesh;
     // cut-cell loads: packed per-cut-cell records from lsg_loads_set, the
     // reduction scratch, and the state of the three moment filters
     struct Loads {
@@ -1813,6 +1823,34 @@ static void check_cell_types(int N, int M, int K, const int* t)
             }
 }
 
+// The Laplace operator from the context's geometry (C.geo type, theta,
+// delta, inverse staggered volumes), the row dictionary, and the context's
+// operator state.
+static void assemble_laplace(Context& C, int N, int M, int K, long long pin0, long long pin1)
+{
+    Context::Geometry& g = C.geo;
+    const long long n = (long long)N * M * K;
+    g.pin0 = pin0;
+    g.pin1 = pin1;
+    C.d.N = N;
+    C.d.M = M;
+    C.d.K = K;
+    C.n = n;
+    C.A7.alloc(7 * n);
+    k_laplace_from_geometry<<<grid_for(n, 256), 256, 0, C.s>>>(N, M, K, g.type.p, g.theta.p, g.delta.p, g.inv[0].p,
+                                                              g.inv[1].p, g.inv[2].p, pin0, pin1, C.A7.p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    C.nclass0 = build_dict(C.s, C.A7.p, 7, n, C.cls0, C.dict0);
+    if (C.adj) {
+        context_release(*C.adj);
+        C.adj.reset();
+    }
+    g.have = true;
+    C.have_matrix = true;
+    C.have_setup = false;
+}
+
 int lsg_set_matrix_geometry(lsg_ctx* h, int N, int M, int K, const int* celltype, const double* theta,
                             const double* delta, const double* inv_mx, const double* inv_my, const double* inv_mz,
                             long long pin0, long long pin1)
@@ -1843,25 +1881,7 @@ int lsg_set_matrix_geometry(lsg_ctx* h, int N, int M, int K, const int* celltype
     LSG_CUDA(cudaMemcpyAsync(g.inv[0].p, inv_mx, nx * 8, cudaMemcpyHostToDevice, C.s));
     LSG_CUDA(cudaMemcpyAsync(g.inv[1].p, inv_my, ny * 8, cudaMemcpyHostToDevice, C.s));
     LSG_CUDA(cudaMemcpyAsync(g.inv[2].p, inv_mz, nz * 8, cudaMemcpyHostToDevice, C.s));
-    g.pin0 = pin0;
-    g.pin1 = pin1;
-    C.d.N = N;
-    C.d.M = M;
-    C.d.K = K;
-    C.n = n;
-    C.A7.alloc(7 * n);
-    k_laplace_from_geometry<<<grid_for(n, 256), 256, 0, C.s>>>(N, M, K, g.type.p, g.theta.p, g.delta.p, g.inv[0].p,
-                                                              g.inv[1].p, g.inv[2].p, pin0, pin1, C.A7.p);
-    LSG_CHECK_LAUNCH();
-    LSG_CUDA(cudaStreamSynchronize(C.s));
-    C.nclass0 = build_dict(C.s, C.A7.p, 7, n, C.cls0, C.dict0);
-    if (C.adj) {
-        context_release(*C.adj);
-        C.adj.reset();
-    }
-    g.have = true;
-    C.have_matrix = true;
-    C.have_setup = false;
+    assemble_laplace(C, N, M, K, pin0, pin1);
     return LSG_OK;
     LSG_API_END(h)
 }
@@ -2126,6 +2146,218 @@ int lsg_set_staggered_types(lsg_ctx* h, const int* xtype, const int* ytype, cons
     }
     LSG_CUDA(cudaStreamSynchronize(C.s));
     C.geo.have_stypes = true;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+// ---------------------------------------------------------------------------
+// mesh build on the device (level set -> ... -> staggered inverse volumes)
+// ---------------------------------------------------------------------------
+int lsg_mesh_build(lsg_ctx* h, int N, int M, int K, const double* hstep, const int* block, int n_bodies,
+                   const double* bodies, const double* phi, double* ms)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(N >= 4 && M >= 4 && K >= 3, LSG_ERR_ARG, "grid must be at least 4 x 4 x 3 cells");
+    LSG_REQUIRE(hstep && block, LSG_ERR_ARG, "null cell size or block");
+    LSG_REQUIRE(hstep[0] > 0 && hstep[1] > 0 && hstep[2] > 0, LSG_ERR_ARG, "cell sizes must be positive");
+    const long long n = (long long)N * M * K;
+    LSG_REQUIRE(n < (1LL << 31), LSG_ERR_ARG, "grid too large");
+    const mesh::Block b{block[0], block[1], block[2], block[3]};
+    // the walks read one corner value back and one ahead along x and y: the
+    // block keeps off the box's first and last column and row
+    LSG_REQUIRE(b.hs >= 1 && b.hs < b.hf && b.hf <= N - 1 && b.vs >= 1 && b.vs < b.vf && b.vf <= M - 1, LSG_ERR_ARG,
+                "level-set block must satisfy 1 <= hs < hf <= N-1 and 1 <= vs < vf <= M-1");
+    LSG_REQUIRE(phi || (n_bodies > 0 && bodies), LSG_ERR_ARG, "need a level set (phi) or at least one body");
+    if (!phi) {
+        for (int q = 0; q < n_bodies; q++) {
+            const double* bq = bodies + (size_t)q * mesh::kBodyWords;
+            LSG_REQUIRE(bq[0] == 0.0 || bq[0] == 1.0, LSG_ERR_ARG, "body kind must be 0 (sphere) or 1 (ellipsoid)");
+            LSG_REQUIRE(bq[0] == 0.0 ? bq[4] > 0 : (bq[5] > 0 && bq[6] > 0 && bq[7] > 0), LSG_ERR_ARG,
+                        "body radius / semi-axes must be positive");
+        }
+    }
+    LSG_CUDA(cudaSetDevice(C.device));
+    Context::Mesh& m = C.mesh;
+    m.have = false;
+    m.N = N;
+    m.M = M;
+    m.K = K;
+    const long long ns[3] = {(long long)(N - 1) * M * K, (long long)N * (M - 1) * K, (long long)N * M * (K - 1)};
+    m.phi_ls.alloc(n);
+    m.phi.alloc(n);
+    m.alpha.alloc(3 * n);
+    m.theta.alloc(3 * n);
+    m.delta.alloc(3 * n);
+    m.vof.alloc(n);
+    m.inv_vof.alloc(n);
+    m.side.alloc(3 * n);
+    m.type.alloc(n);
+    for (int d = 0; d < 3; d++) {
+        m.svof[d].alloc(ns[d]);
+        m.sinv[d].alloc(ns[d]);
+        m.stype[d].alloc(ns[d]);
+    }
+    cudaEvent_t e0, e1;
+    LSG_CUDA(cudaEventCreate(&e0));
+    LSG_CUDA(cudaEventCreate(&e1));
+    struct Ev {
+        cudaEvent_t a, b;
+        ~Ev() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    } ev{e0, e1};
+    LSG_CUDA(cudaEventRecord(e0, C.s));
+    const int gsz = grid_for(n, 256);
+    mesh::k_mesh_init<<<gsz, 256, 0, C.s>>>(N, M, K, hstep[0], hstep[1], hstep[2], m.phi_ls.p, m.alpha.p, m.theta.p,
+                                      m.delta.p, m.side.p, m.type.p);
+    LSG_CHECK_LAUNCH();
+    DevBuf<double> scratch;
+    if (phi) {
+        scratch.alloc(n);
+        LSG_CUDA(cudaMemcpyAsync(scratch.p, phi, n * 8, cudaMemcpyHostToDevice, C.s));
+        mesh::k_mesh_phi_block<<<gsz, 256, 0, C.s>>>(N, M, K, b, scratch.p, m.phi_ls.p);
+        LSG_CHECK_LAUNCH();
+    } else {
+        DevBuf<double> db;
+        db.alloc((size_t)n_bodies * mesh::kBodyWords);
+        LSG_CUDA(cudaMemcpyAsync(db.p, bodies, (size_t)n_bodies * mesh::kBodyWords * 8, cudaMemcpyHostToDevice, C.s));
+        const long long rows = (long long)(b.vf - b.vs) * K;
+        mesh::k_mesh_levelset<<<(unsigned)((rows + 127) / 128), 128, 0, C.s>>>(N, M, K, b, hstep[0], hstep[1], hstep[2],
+                                                                          n_bodies, db.p, m.phi_ls.p);
+        LSG_CHECK_LAUNCH();
+        LSG_CUDA(cudaStreamSynchronize(C.s));   // db is released on return of this scope
+    }
+    // oscillation fix: fixed-point sweeps of the reference's walk until no
+    // value moves; each sweep settles at least the next cell of every chain of
+    // edits, so the count is bounded by the longest chain (a few cells)
+    LSG_CUDA(cudaMemcpyAsync(m.phi.p, m.phi_ls.p, n * 8, cudaMemcpyDeviceToDevice, C.s));
+    if (!scratch.p) scratch.alloc(n);
+    LSG_CUDA(cudaMemcpyAsync(scratch.p, m.phi_ls.p, n * 8, cudaMemcpyDeviceToDevice, C.s));
+    unsigned int* changed = (unsigned int*)(C.scal.p + 8);
+    const long long bcells = (long long)(b.hf - b.hs) * (b.vf - b.vs) * K;
+    const unsigned bgrid = (unsigned)((bcells + 255) / 256);
+    const long long max_sweeps = bcells + 1;
+    double* cur = m.phi.p;
+    double* nxt = scratch.p;
+    m.osc_sweeps = 0;
+    for (;;) {
+        LSG_REQUIRE(m.osc_sweeps < max_sweeps, LSG_ERR_STATE, "level-set oscillation fix did not settle");
+        LSG_CUDA(cudaMemsetAsync(changed, 0, sizeof(unsigned int), C.s));
+        mesh::k_mesh_osc<<<bgrid, 256, 0, C.s>>>(N, M, K, b, m.phi_ls.p, cur, nxt, changed);
+        LSG_CHECK_LAUNCH();
+        unsigned int hc = 0;
+        LSG_CUDA(cudaMemcpyAsync(&hc, changed, sizeof(hc), cudaMemcpyDeviceToHost, C.s));
+        LSG_CUDA(cudaStreamSynchronize(C.s));
+        m.osc_sweeps++;
+        std::swap(cur, nxt);
+        if (hc == 0) break;
+    }
+    if (cur != m.phi.p) std::swap(m.phi, scratch);      // keep the settled values in m.phi
+    mesh::k_mesh_alpha_types<<<bgrid, 256, 0, C.s>>>(N, M, K, b, m.phi.p, m.alpha.p, m.side.p, m.type.p);
+    LSG_CHECK_LAUNCH();
+    mesh::k_mesh_theta<<<bgrid, 256, 0, C.s>>>(N, M, K, b, m.side.p, m.alpha.p, m.theta.p);
+    LSG_CHECK_LAUNCH();
+    mesh::k_mesh_volume<<<gsz, 256, 0, C.s>>>(N, M, K, m.type.p, m.delta.p, m.theta.p, m.alpha.p, m.vof.p, m.inv_vof.p);
+    LSG_CHECK_LAUNCH();
+    mesh::k_mesh_staggered<<<gsz, 256, 0, C.s>>>(N, M, K, m.type.p, m.theta.p, m.vof.p, m.stype[0].p, m.stype[1].p,
+                                           m.stype[2].p, m.svof[0].p, m.svof[1].p, m.svof[2].p, m.sinv[0].p,
+                                           m.sinv[1].p, m.sinv[2].p);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaEventRecord(e1, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    float t = 0;
+    LSG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    if (ms) *ms = t;
+    m.have = true;
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_mesh_get(lsg_ctx* h, int field, void* out)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    Context::Mesh& m = C.mesh;
+    LSG_REQUIRE(m.have, LSG_ERR_STATE, "no mesh built (lsg_mesh_build)");
+    LSG_REQUIRE(out, LSG_ERR_ARG, "null output");
+    const void* src = nullptr;
+    size_t bytes = 0;
+    const long long n = (long long)m.N * m.M * m.K;
+    const long long ns[3] = {(long long)(m.N - 1) * m.M * m.K, (long long)m.N * (m.M - 1) * m.K,
+                             (long long)m.N * m.M * (m.K - 1)};
+    switch (field) {
+    case LSG_MESH_PHI_LS: src = m.phi_ls.p; bytes = n * 8; break;
+    case LSG_MESH_PHI: src = m.phi.p; bytes = n * 8; break;
+    case LSG_MESH_ALPHA: src = m.alpha.p; bytes = 3 * n * 8; break;
+    case LSG_MESH_SIDE_TYPE: src = m.side.p; bytes = 3 * n * 4; break;
+    case LSG_MESH_CELL_TYPE: src = m.type.p; bytes = n * 4; break;
+    case LSG_MESH_THETA: src = m.theta.p; bytes = 3 * n * 8; break;
+    case LSG_MESH_DELTA: src = m.delta.p; bytes = 3 * n * 8; break;
+    case LSG_MESH_VOF: src = m.vof.p; bytes = n * 8; break;
+    case LSG_MESH_INV_VOF: src = m.inv_vof.p; bytes = n * 8; break;
+    case LSG_MESH_XTYPE: case LSG_MESH_YTYPE: case LSG_MESH_ZTYPE: {
+        const int d = field - LSG_MESH_XTYPE;
+        src = m.stype[d].p;
+        bytes = ns[d] * 4;
+        break;
+    }
+    case LSG_MESH_VOF_X: case LSG_MESH_VOF_Y: case LSG_MESH_VOF_Z: {
+        const int d = field - LSG_MESH_VOF_X;
+        src = m.svof[d].p;
+        bytes = ns[d] * 8;
+        break;
+    }
+    case LSG_MESH_INV_MX: case LSG_MESH_INV_MY: case LSG_MESH_INV_MZ: {
+        const int d = field - LSG_MESH_INV_MX;
+        src = m.sinv[d].p;
+        bytes = ns[d] * 8;
+        break;
+    }
+    default: throw Error{LSG_ERR_ARG, "unknown mesh field"};
+    }
+    LSG_CUDA(cudaSetDevice(C.device));
+    LSG_CUDA(cudaMemcpyAsync(out, src, bytes, cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_mesh_osc_sweeps(const lsg_ctx* h)
+{
+    if (!h || !h->c.mesh.have) return LSG_ERR_STATE;
+    return h->c.mesh.osc_sweeps;
+}
+
+int lsg_set_matrix_mesh(lsg_ctx* h, long long pin0, long long pin1)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    Context::Mesh& m = C.mesh;
+    LSG_REQUIRE(m.have, LSG_ERR_STATE, "no mesh built (lsg_mesh_build)");
+    const long long n = (long long)m.N * m.M * m.K;
+    LSG_REQUIRE(pin0 >= -1 && pin0 < n && pin1 >= -1 && pin1 < n, LSG_ERR_ARG, "pinned row outside the grid");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const long long ns[3] = {(long long)(m.N - 1) * m.M * m.K, (long long)m.N * (m.M - 1) * m.K,
+                             (long long)m.N * m.M * (m.K - 1)};
+    Context::Geometry& g = C.geo;
+    g.have = false;
+    g.have_stypes = false;
+    g.type.alloc(n);
+    g.theta.alloc(3 * n);
+    g.delta.alloc(3 * n);
+    LSG_CUDA(cudaMemcpyAsync(g.type.p, m.type.p, n * 4, cudaMemcpyDeviceToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(g.theta.p, m.theta.p, 3 * n * 8, cudaMemcpyDeviceToDevice, C.s));
+    LSG_CUDA(cudaMemcpyAsync(g.delta.p, m.delta.p, 3 * n * 8, cudaMemcpyDeviceToDevice, C.s));
+    for (int d = 0; d < 3; d++) {
+        g.inv[d].alloc(ns[d]);
+        g.stype[d].alloc(ns[d]);
+        LSG_CUDA(cudaMemcpyAsync(g.inv[d].p, m.sinv[d].p, ns[d] * 8, cudaMemcpyDeviceToDevice, C.s));
+        LSG_CUDA(cudaMemcpyAsync(g.stype[d].p, m.stype[d].p, ns[d] * 4, cudaMemcpyDeviceToDevice, C.s));
+    }
+    assemble_laplace(C, m.N, m.M, m.K, pin0, pin1);
+    g.have_stypes = true;
     return LSG_OK;
     LSG_API_END(h)
 }

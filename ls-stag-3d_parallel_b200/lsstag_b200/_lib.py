@@ -22,6 +22,7 @@ LSG_ERR_CUDA = -2
 LSG_ERR_NOMEM = -3
 LSG_ERR_STATE = -4
 LSG_ERR_PATTERN = -5
+LSG_ERR_SINGULAR = -6
 
 METHOD_FGMRES, METHOD_BICGSTAB = 0, 1
 PC_MG, PC_ILU0, PC_NONE = 0, 1, 2
@@ -58,6 +59,7 @@ EXPORTS = [
     "lsg_helmholtz_flux", "lsg_convective_flux", "lsg_convective_flux_device", "lsg_momentum_rhs_device",
     "lsg_convective_adjoint", "lsg_convective_adjoint_device", "lsg_gradient_transpose",
     "lsg_gradient_transpose_device", "lsg_projection_adjoint_device", "lsg_tecplot_sol_write",
+    "lsg_mesh_build", "lsg_mesh_get", "lsg_mesh_osc_sweeps", "lsg_set_matrix_mesh",
     "lsg_tecplot_sol_async", "lsg_tecplot_wait",
 ]
 
@@ -151,6 +153,10 @@ def load() -> C.CDLL:
     lib.lsg_loads_reset_filter.argtypes = [P, C.c_double]
     lib.lsg_loads_adjoint.argtypes = [P, dp, dp, C.c_double, dp, dp, dp, dp]
     lib.lsg_loads_adjoint_device.argtypes = [P, dp, C.c_void_p, C.c_double] + [C.c_void_p] * 4
+    lib.lsg_mesh_build.argtypes = [P, C.c_int, C.c_int, C.c_int, dp, ip, C.c_int, dp, dp, dp]
+    lib.lsg_mesh_get.argtypes = [P, C.c_int, C.c_void_p]
+    lib.lsg_mesh_osc_sweeps.argtypes = [P]
+    lib.lsg_set_matrix_mesh.argtypes = [P, C.c_longlong, C.c_longlong]
     lib.lsg_version.restype = C.c_char_p
     _lib = lib
     return lib

@@ -123,6 +123,46 @@ class IterativeSolver:
         if setup:
             self._setup()
 
+    def build_mesh(self, dims, h, block, bodies=None, phi=None) -> float:
+        """The flow task's mesh build on this context's device
+        (lsg_mesh_build): ``bodies`` from lsstag_b200.mesh.bodies_array, or
+        ``phi`` the task's own level set at the upper cell corners.  Returns
+        the device time in ms."""
+        N, M, K = (int(v) for v in dims)
+        hh = np.ascontiguousarray(h, dtype=np.float64).reshape(3)
+        blk = np.ascontiguousarray(block, dtype=np.int32).reshape(4)
+        ms = L.C.c_double(0.0)
+        if phi is not None:
+            ph = np.ascontiguousarray(phi, dtype=np.float64).reshape(-1)
+            rc = self.ctx.lib.lsg_mesh_build(self.ctx.h, N, M, K, L.dptr(hh), L.iptr(blk), 0, None, L.dptr(ph),
+                                             L.C.byref(ms))
+        else:
+            b = np.ascontiguousarray(bodies, dtype=np.float64).reshape(-1)
+            rc = self.ctx.lib.lsg_mesh_build(self.ctx.h, N, M, K, L.dptr(hh), L.iptr(blk), b.size // 17, L.dptr(b),
+                                             None, L.C.byref(ms))
+        self.ctx.check(rc)
+        self.mesh_dims = (N, M, K)
+        return float(ms.value)
+
+    def mesh_get(self, name: str) -> np.ndarray:
+        """One array of the built mesh (names: lsstag_b200.mesh.FIELDS)."""
+        from . import mesh as MS
+        code, dt, _ = MS.FIELDS[name]
+        out = np.empty(MS.field_size(name, self.mesh_dims), dtype=dt)
+        self.ctx.check(self.ctx.lib.lsg_mesh_get(self.ctx.h, code, out.ctypes.data_as(L.C.c_void_p)))
+        return out
+
+    def set_from_mesh(self, pins, task: Task | None = None, setup: bool = True):
+        """Same as set() with the pressure operator assembled on the GPU from
+        the mesh this context built (lsg_set_matrix_mesh), pins = the two
+        pinned rows; the staggered types for the projection come with it."""
+        self.task = task or Task()
+        self.eps = float(self.task.eps)
+        self.dims = self.mesh_dims
+        self.ctx.check(self.ctx.lib.lsg_set_matrix_mesh(self.ctx.h, int(pins[0]), int(pins[1])))
+        if setup:
+            self._setup()
+
     def set_helmholtz(self, direction: int, geom: dict, base_dims, nu: float, coef: float, is_flow: bool = True,
                       task: Task | None = None, setup: bool = True):
         """The momentum operator of one direction (HelmholtzDiscreteOperator

@@ -176,7 +176,15 @@ struct HarnessTask : FlowTaskDescription {
                     p.x += d->x;
                 }
             }
+        // the level set as evaluated, before calcAlpha's oscillation fix
+        // (checkOscLS, ls_stag_uniform_mesh.h:2906-2916) edits it in place
+        const long n = (long)N * mesh.baseMesh.M * mesh.baseMesh.K;
+        phi_ls.assign(mesh.phi, mesh.phi + n);
     }
+    std::vector<double> phi_ls;
+    // the block FlowTaskDescription::buildBaseMesh walks (its hs_loc .. vf_loc:
+    // the level-set block widened by 3 cells, flow_task_description.h:388-398)
+    void lsBlock(int b[4]) const { b[0] = mesh.hs - 3; b[1] = mesh.hf + 3; b[2] = mesh.vs - 3; b[3] = mesh.vf + 3; }
 };
 
 /* The momentum operators with their immersed-boundary source term made
@@ -461,6 +469,51 @@ int main(int argc, char** argv)
         for (long i = 0; i < nb; i++)
             mm->v_ib[i].set(0.1 * sin(0.11 * i), 0.1 * cos(0.13 * i), 0.05 * sin(0.17 * i));
         for (long i = 0; i < (long)mm->xMesh.NMK; i++) mm->m_Ux[i] = 1.0 + 0.2 * sin(0.29 * i);
+    }
+    if ((int)cfg.get("mesh_dump", 0)) {
+        // the whole mesh build of the flow task (BaseTaskDescription::buildMesh,
+        // base_task_description.h:330-371): level set as evaluated, level set
+        // after the oscillation fix, edge fractions alpha, face types, cell
+        // types, face fractions theta, cell volumes, staggered types, volumes
+        // and inverse volumes, with the level-set block the walks used
+        LSSTAGUniformMesh* mm = task->m_mesh;
+        const int N = mm->baseMesh.N, M = mm->baseMesh.M, K = mm->baseMesh.K;
+        const long n = (long)N * M * K;
+        const long ns[3] = {(long)mm->xMesh.NMK, (long)mm->yMesh.NMK, (long)mm->zMesh.NMK};
+        int dd[3] = {N, M, K};
+        out.i("dims", dd, 3);
+        int blk[4];
+        task->lsBlock(blk);
+        out.i("ls_block", blk, 4);
+        double hh[3] = {task->hx, task->hy, task->hz};
+        out.d("h", hh, 3);
+        out.d("phi_ls", task->phi_ls.data(), n);
+        out.d("phi", mm->phi, n);
+        out.d("alpha", (const double*)mm->alpha, 3 * n);
+        out.i("side_type", (const int*)mm->baseSideTypes, 3 * n);
+        out.i("celltype", (const int*)mm->baseMesh.typeOfCell, n);
+        out.d("theta", (const double*)mm->theta, 3 * n);
+        out.d("delta", (const double*)mm->delta, 3 * n);
+        out.d("nodes", (const double*)mm->nodes, 3 * n);
+        out.d("vof", mm->baseMesh.VOF, n);
+        out.d("inv_vof", mm->baseMesh.inv_VOF, n);
+        out.i("xtype", (const int*)mm->xMesh.typeOfCell, ns[0]);
+        out.i("ytype", (const int*)mm->yMesh.typeOfCell, ns[1]);
+        out.i("ztype", (const int*)mm->zMesh.typeOfCell, ns[2]);
+        out.d("vof_x", mm->xMesh.VOF, ns[0]);
+        out.d("vof_y", mm->yMesh.VOF, ns[1]);
+        out.d("vof_z", mm->zMesh.VOF, ns[2]);
+        out.d("inv_mx", mm->xMesh.inv_VOF, ns[0]);
+        out.d("inv_my", mm->yMesh.inv_VOF, ns[1]);
+        out.d("inv_mz", mm->zMesh.inv_VOF, ns[2]);
+        out.d("dib_en", (const double*)mm->delta_ib_en, 3 * n);
+        out.d("dib_ws", (const double*)mm->delta_ib_ws, 3 * n);
+        out.d("dib_nb", (const double*)mm->delta_ib_nb, 3 * n);
+        out.d("dib_st", (const double*)mm->delta_ib_st, 3 * n);
+        out.d("dib_max", (const double*)mm->delta_ib_max, 3 * n);
+        out.d("inv_dib_ne", (const double*)mm->inv_delta_ib_ne, 3 * n);
+        out.d("inv_dib_tn", (const double*)mm->inv_delta_ib_tn, 3 * n);
+        return 0;
     }
     if ((int)cfg.get("flow_steps", 0) || (int)cfg.get("flow_setup", 0)) {
         // whole time steps of the flow task as TimeSteppingMethodInterface::init
