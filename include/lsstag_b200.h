@@ -369,11 +369,14 @@ int lsg_projection_correct(lsg_ctx* ctx, const double* phi, const double* us, co
    solve and lsg_projection_correct with outflow = 0): given the cotangents of
    the outputs, returns those of the inputs,
      phi_bar = Gx^T S_x ubar_out + Gy^T S_y vbar_out + Gz^T S_z wbar_out + coef pbar_out,
+               set to 0 on solid rows and on empty rows (cut cells whose
+               faces are all closed): the forward solve never excites them
+               and no velocity reads their pressure,
      A^T lambda = phi_bar (lsg_solve_adjoint's solver),  b_bar = lambda with the pins zeroed,
      ubar = ubar_out + Dx^T b_bar (likewise v, w),  fluxbar = b_bar,
    the pressure cotangent passing through unchanged.  No counterpart in the
-   reference (the north star's adjoint of the projection step).  Host
-   pointers; st receives the adjoint solve's statistics (may be NULL). */
+   reference (the adjoint of its projection step).  Host pointers; st
+   receives the adjoint solve's statistics (may be NULL). */
 int lsg_projection_adjoint(lsg_ctx* ctx, const double* ubar_out, const double* vbar_out, const double* wbar_out,
                            const double* pbar_out, double coef, double* ubar, double* vbar, double* wbar,
                            double* fluxbar, lsg_stats* st);
@@ -482,7 +485,10 @@ int lsg_mg_level_tridiag(lsg_ctx* ctx, int level, char dir, double* c, double* d
    events (after a warm-up launch): `which` = 0/1/2 the finest-level x/y/z
    line solve of the multigrid smoother, 3 the finest-level residual update
    r -= A c, 4 the FP64 operator apply fused with a dot product (Krylov),
-   5 the residual update of the first coarse level (Galerkin stencil).
+   5 the residual update of the first coarse level (Galerkin stencil),
+   6 the operator apply fused with a dot product on an FP32 preconditioned
+   vector (the Krylov product of the FP32-multigrid solve), 7 the same
+   product by the one-thread-per-cell kernel the solve uses on wide grids.
    Returns the mean duration of one launch and the algorithmic HBM bytes one
    launch moves (compulsory traffic of its inputs and outputs).  Needs
    lsg_setup with the multigrid preconditioner. */

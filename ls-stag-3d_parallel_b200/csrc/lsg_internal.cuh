@@ -42,6 +42,45 @@ extern thread_local long long g_launches;
     } while (0)
 
 // ---------------------------------------------------------------------------
+// per-call temporaries: stream-ordered allocations from a context's own memory
+// pool, released on the context's stream when they go out of scope.  The
+// pool keeps freed memory (release threshold: never), so a call that repeats
+// every time step reuses its blocks instead of a cudaMalloc / cudaFree pair
+// (cudaFree synchronises the device).
+// ---------------------------------------------------------------------------
+template <typename T>
+struct TmpBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    cudaMemPool_t pool = nullptr;
+    TmpBuf(cudaStream_t stream, cudaMemPool_t mp) : s(stream), pool(mp) {}
+    TmpBuf(const TmpBuf&) = delete;
+    TmpBuf& operator=(const TmpBuf&) = delete;
+    ~TmpBuf() { release(); }
+    void alloc(size_t count)
+    {
+        if (count == n && p) return;
+        release();
+        if (count == 0) return;
+        cudaError_t e = cudaMallocFromPoolAsync((void**)&p, count * sizeof(T), pool, s);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            throw Error{LSG_ERR_NOMEM, std::string("stream-ordered allocation of ") +
+                                           std::to_string(count * sizeof(T)) + " bytes: " + cudaGetErrorString(e)};
+        }
+        n = count;
+    }
+    void release()
+    {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---------------------------------------------------------------------------
 // device buffers
 // ---------------------------------------------------------------------------
 template <typename T>

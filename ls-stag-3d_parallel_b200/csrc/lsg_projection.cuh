@@ -585,4 +585,26 @@ __global__ void k_pin_zero_copy(long long n, long long pin0, long long pin1, con
         out[i] = (i == pin0 || i == pin1) ? 0.0 : lambda[i];
 }
 
+// The adjoint right-hand side restricted to the rows the forward solve can
+// excite.  Solid rows (a decoupled 1e-16 diagonal) and empty rows (cut cells
+// whose faces are all closed) see a zero right-hand side in every forward
+// projection, and no velocity reads their pressure, so the forward map does
+// not depend on the pressure cotangent there; dropping it keeps a
+// 1e16-scaled component out of the transposed Krylov solve.
+__global__ void k_adjoint_live_rows(long long n, const int* __restrict__ type, const double* __restrict__ A7,
+                                    double* __restrict__ v)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        bool live = type[i] != 0;
+        if (live) {
+            bool any = false;
+#pragma unroll
+            for (int s = 0; s < 7; s++) any = any || (A7[(size_t)s * n + i] != 0.0);
+            live = any;
+        }
+        if (!live) v[i] = 0.0;
+    }
+}
+
 }  // namespace lsg

@@ -200,6 +200,7 @@ struct TecplotAsync {
 struct Context {
     int device = 0;
     cudaStream_t s = nullptr;
+    cudaMemPool_t pool = nullptr;   // per-call temporaries (TmpBuf)
     std::string err;
     Dims d;
     long long n = 0;
@@ -772,10 +773,14 @@ static void apply_resid(const LevelT<T>& lv, const T* x, T* r, cudaStream_t s, i
         else
             k_apply7z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict, x, r);
     } else if (lv.ol.n == 27 && lv.dict28.p) {
+        // shared-memory staged planes; longer z-chunks amortise the two extra
+        // planes (z0 - 1, z1) each CTA stages
+        const int zs = n >= (8LL << 20) ? 16 : (n >= (1LL << 20) ? 8 : 4);
+        const dim3 sg(zg.x, zg.y, (lv.d.K + zs - 1) / zs);
         if (mode == 0)
-            k_apply27z<T, 0><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict28.p, x, r);
+            k_apply27s<T, 0><<<sg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zs, lv.cls, lv.dict28.p, x, r);
         else
-            k_apply27z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict28.p, x, r);
+            k_apply27s<T, 1><<<sg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zs, lv.cls, lv.dict28.p, x, r);
     } else {
         if (mode == 0)
             k_applyboxd<T, 0><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.ol, lv.cls, lv.dict, x, r);
@@ -1569,6 +1574,16 @@ static void context_init(Context& C, int device, cudaStream_t stream)
     }
     LSG_CUDA(cudaEventCreate(&C.ev0));
     LSG_CUDA(cudaEventCreate(&C.ev1));
+    {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        LSG_CUDA(cudaMemPoolCreate(&C.pool, &props));
+        uint64_t keep = UINT64_MAX;          // freed blocks stay with the pool
+        LSG_CUDA(cudaMemPoolSetAttribute(C.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     C.red.init();
     C.scal.alloc(64);
     LSG_CUDA(cudaMemset(C.scal.p, 0, C.scal.bytes()));
@@ -1593,6 +1608,8 @@ static cudaStream_t context_release(Context& C)
     if (C.ev0) cudaEventDestroy(C.ev0);
     if (C.ev1) cudaEventDestroy(C.ev1);
     C.ev0 = C.ev1 = nullptr;
+    if (C.pool) cudaMemPoolDestroy(C.pool);
+    C.pool = nullptr;
     return C.own_stream ? C.s : nullptr;
 }
 
@@ -1708,8 +1725,8 @@ static int set_matrix_impl(lsg_ctx* h, int N, int M, int K, const int* rowptr, c
     LSG_CUDA(cudaSetDevice(C.device));
     const long long n = (long long)N * M * K;
     LSG_REQUIRE(n < (1LL << 31), LSG_ERR_ARG, "grid too large for 32-bit CSR indices");
-    DevBuf<int> drp, dcol;
-    DevBuf<double> dval;
+    TmpBuf<int> drp(C.s, C.pool), dcol(C.s, C.pool);
+    TmpBuf<double> dval(C.s, C.pool);
     const int* prp = rowptr;
     const int* pcol = col;
     const double* pval = val;
@@ -1908,13 +1925,13 @@ int lsg_set_matrix_helmholtz(lsg_ctx* h, int dir, int N, int M, int K, const int
     check_cell_types(Ns, Ms, Ks, stype);
     C.geo.have = C.geo.have_stypes = false;    // geometry of an earlier operator no longer applies
     LSG_CUDA(cudaSetDevice(C.device));
-    DevBuf<int> dt;
-    DevBuf<double> dth, dal, dde, dinv, dvof, den, dws, dnb, dst, dne, dtn;
+    TmpBuf<int> dt(C.s, C.pool);
+    TmpBuf<double> dth(C.s, C.pool), dal(C.s, C.pool), dde(C.s, C.pool), dinv(C.s, C.pool), dvof(C.s, C.pool), den(C.s, C.pool), dws(C.s, C.pool), dnb(C.s, C.pool), dst(C.s, C.pool), dne(C.s, C.pool), dtn(C.s, C.pool);
     dt.alloc(ns);
     LSG_CUDA(cudaMemcpyAsync(dt.p, stype, ns * sizeof(int), cudaMemcpyHostToDevice, C.s));
     const double* src3[9] = {theta, alpha, delta, delta_ib_en, delta_ib_ws, delta_ib_nb, delta_ib_st,
                              inv_delta_ib_ne, inv_delta_ib_tn};
-    DevBuf<double>* dst3[9] = {&dth, &dal, &dde, &den, &dws, &dnb, &dst, &dne, &dtn};
+    TmpBuf<double>* dst3[9] = {&dth, &dal, &dde, &den, &dws, &dnb, &dst, &dne, &dtn};
     for (int a = 0; a < 9; a++) {
         dst3[a]->alloc(3 * n);
         LSG_CUDA(cudaMemcpyAsync(dst3[a]->p, src3[a], 3 * n * 8, cudaMemcpyHostToDevice, C.s));
@@ -1984,8 +2001,8 @@ int lsg_helmholtz_flux(lsg_ctx* h, int dir, int N, int M, int K, const int* styp
     const int Ns = N - (dir == 0), Ms = M - (dir == 1), Ks = K - (dir == 2);
     const long long ns = (long long)Ns * Ms * Ks;
     LSG_CUDA(cudaSetDevice(C.device));
-    DevBuf<int> dt, dsd;
-    DevBuf<double> dde, duw, dout, dth, dal, dinv, den, dws, dnb, dst, dne, dtn, dv, dyx, dzy;
+    TmpBuf<int> dt(C.s, C.pool), dsd(C.s, C.pool);
+    TmpBuf<double> dde(C.s, C.pool), duw(C.s, C.pool), dout(C.s, C.pool), dth(C.s, C.pool), dal(C.s, C.pool), dinv(C.s, C.pool), den(C.s, C.pool), dws(C.s, C.pool), dnb(C.s, C.pool), dst(C.s, C.pool), dne(C.s, C.pool), dtn(C.s, C.pool), dv(C.s, C.pool), dyx(C.s, C.pool), dzy(C.s, C.pool);
     dt.alloc(ns);
     dde.alloc(3 * n);
     duw.alloc((size_t)M * K);
@@ -2007,7 +2024,7 @@ int lsg_helmholtz_flux(lsg_ctx* h, int dir, int N, int M, int K, const int* styp
         LSG_CUDA(cudaMemcpyAsync(dsd.p, side_type, 3 * n * sizeof(int), cudaMemcpyHostToDevice, C.s));
         const double* src3[11] = {theta, alpha, delta_ib_en, delta_ib_ws, delta_ib_nb, delta_ib_st,
                                   inv_delta_ib_ne, inv_delta_ib_tn, vib, vib_yx, vib_zy};
-        DevBuf<double>* dst3[11] = {&dth, &dal, &den, &dws, &dnb, &dst, &dne, &dtn, &dv, &dyx, &dzy};
+        TmpBuf<double>* dst3[11] = {&dth, &dal, &den, &dws, &dnb, &dst, &dne, &dtn, &dv, &dyx, &dzy};
         for (int q = 0; q < 11; q++) {
             dst3[q]->alloc(3 * n);
             LSG_CUDA(cudaMemcpyAsync(dst3[q]->p, src3[q], 3 * n * 8, cudaMemcpyHostToDevice, C.s));
@@ -2101,7 +2118,7 @@ int lsg_convective_flux(lsg_ctx* h, int dir, int N, int M, int K, const double* 
     const int Ns = N - (dir == 0), Ms = M - (dir == 1), Ks = K - (dir == 2);
     const long long ns = (long long)Ns * Ms * Ks;
     LSG_CUDA(cudaSetDevice(C.device));
-    DevBuf<double> dth, dde, dux, duz, duw, dout;
+    TmpBuf<double> dth(C.s, C.pool), dde(C.s, C.pool), dux(C.s, C.pool), duz(C.s, C.pool), duw(C.s, C.pool), dout(C.s, C.pool);
     dout.alloc(ns);
     if (dir == 2) {
         const long long nx = (long long)(N - 1) * M * K, nz = (long long)N * M * (K - 1);
@@ -2211,14 +2228,14 @@ int lsg_mesh_build(lsg_ctx* h, int N, int M, int K, const double* hstep, const i
     mesh::k_mesh_init<<<gsz, 256, 0, C.s>>>(N, M, K, hstep[0], hstep[1], hstep[2], m.phi_ls.p, m.alpha.p, m.theta.p,
                                       m.delta.p, m.side.p, m.type.p);
     LSG_CHECK_LAUNCH();
-    DevBuf<double> scratch;
+    TmpBuf<double> scratch(C.s, C.pool);
     if (phi) {
         scratch.alloc(n);
         LSG_CUDA(cudaMemcpyAsync(scratch.p, phi, n * 8, cudaMemcpyHostToDevice, C.s));
         mesh::k_mesh_phi_block<<<gsz, 256, 0, C.s>>>(N, M, K, b, scratch.p, m.phi_ls.p);
         LSG_CHECK_LAUNCH();
     } else {
-        DevBuf<double> db;
+        TmpBuf<double> db(C.s, C.pool);
         db.alloc((size_t)n_bodies * mesh::kBodyWords);
         LSG_CUDA(cudaMemcpyAsync(db.p, bodies, (size_t)n_bodies * mesh::kBodyWords * 8, cudaMemcpyHostToDevice, C.s));
         const long long rows = (long long)(b.vf - b.vs) * K;
@@ -2252,7 +2269,8 @@ int lsg_mesh_build(lsg_ctx* h, int N, int M, int K, const double* hstep, const i
         std::swap(cur, nxt);
         if (hc == 0) break;
     }
-    if (cur != m.phi.p) std::swap(m.phi, scratch);      // keep the settled values in m.phi
+    if (cur != m.phi.p)                                   // keep the settled values in m.phi
+        LSG_CUDA(cudaMemcpyAsync(m.phi.p, cur, n * 8, cudaMemcpyDeviceToDevice, C.s));
     mesh::k_mesh_alpha_types<<<bgrid, 256, 0, C.s>>>(N, M, K, b, m.phi.p, m.alpha.p, m.side.p, m.type.p);
     LSG_CHECK_LAUNCH();
     mesh::k_mesh_theta<<<bgrid, 256, 0, C.s>>>(N, M, K, b, m.side.p, m.alpha.p, m.theta.p);
@@ -2421,7 +2439,7 @@ int lsg_projection_rhs(lsg_ctx* h, const double* u, const double* v, const doubl
     const Dims& d = C.d;
     const long long n = C.n, cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
                                        (long long)d.N * d.M * (d.K - 1)};
-    DevBuf<double> du, dv, dw, df, db;
+    TmpBuf<double> du(C.s, C.pool), dv(C.s, C.pool), dw(C.s, C.pool), df(C.s, C.pool), db(C.s, C.pool);
     du.alloc(cnt[0]);
     dv.alloc(cnt[1]);
     dw.alloc(cnt[2]);
@@ -2474,8 +2492,8 @@ int lsg_laplace_flux(lsg_ctx* h, const int* side_type, const double* vib, const 
     LSG_CUDA(cudaSetDevice(C.device));
     const Dims& d = C.d;
     const long long n = C.n, nx = (long long)(d.N - 1) * d.M * d.K, nmk = (long long)d.M * d.K;
-    DevBuf<int> ds;
-    DevBuf<double> dv, dw, dux, df;
+    TmpBuf<int> ds(C.s, C.pool);
+    TmpBuf<double> dv(C.s, C.pool), dw(C.s, C.pool), dux(C.s, C.pool), df(C.s, C.pool);
     ds.alloc(3 * n);
     dv.alloc(3 * n);
     dw.alloc(nmk);
@@ -2518,14 +2536,14 @@ int lsg_momentum_rhs(lsg_ctx* h, int dir, const int* rowptr, const int* col, con
         for (long long e = 0; e < nnz; e++)
             LSG_REQUIRE(col[e] >= 0 && col[e] < ns, LSG_ERR_ARG, "CSR column outside the staggered grid");
     }
-    DevBuf<int> drp, dcol;
-    DevBuf<double> dval, dflux2, du, dup, dvof, dhf, dp, dprev, dgp, dr, da;
+    TmpBuf<int> drp(C.s, C.pool), dcol(C.s, C.pool);
+    TmpBuf<double> dval(C.s, C.pool), dflux2(C.s, C.pool), du(C.s, C.pool), dup(C.s, C.pool), dvof(C.s, C.pool), dhf(C.s, C.pool), dp(C.s, C.pool), dprev(C.s, C.pool), dgp(C.s, C.pool), dr(C.s, C.pool), da(C.s, C.pool);
     if (rowptr) {
         drp.alloc(ns + 1);
         dcol.alloc(std::max<long long>(nnz, 1));
         dval.alloc(std::max<long long>(nnz, 1));
     }
-    for (DevBuf<double>* b : {&dflux2, &du, &dup, &dvof, &dhf, &dprev, &dgp, &dr, &da}) b->alloc(ns);
+    for (TmpBuf<double>* b : {&dflux2, &du, &dup, &dvof, &dhf, &dprev, &dgp, &dr, &da}) b->alloc(ns);
     dp.alloc(n);
     if (rowptr) {
         LSG_CUDA(cudaMemcpyAsync(drp.p, rowptr, (ns + 1) * sizeof(int), cudaMemcpyHostToDevice, C.s));
@@ -2535,7 +2553,7 @@ int lsg_momentum_rhs(lsg_ctx* h, int dir, const int* rowptr, const int* col, con
         }
     }
     const double* hsrc[6] = {flux2, u, uprev, vof, hflux, prev_aux};
-    DevBuf<double>* dst[6] = {&dflux2, &du, &dup, &dvof, &dhf, &dprev};
+    TmpBuf<double>* dst[6] = {&dflux2, &du, &dup, &dvof, &dhf, &dprev};
     for (int k = 0; k < 6; k++) LSG_CUDA(cudaMemcpyAsync(dst[k]->p, hsrc[k], ns * 8, cudaMemcpyHostToDevice, C.s));
     LSG_CUDA(cudaMemcpyAsync(dp.p, p, n * 8, cudaMemcpyHostToDevice, C.s));
     const Context::Geometry& g = C.geo;
@@ -2630,7 +2648,7 @@ int lsg_convective_adjoint(lsg_ctx* h, int dir, const double* ux, const double* 
     const Dims& d = C.d;
     const long long cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
                               (long long)d.N * d.M * (d.K - 1)};
-    DevBuf<double> du[3], db[3], dv, dl, dvb;
+    TmpBuf<double> du[3] = {TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool)}, db[3] = {TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool)}, dv(C.s, C.pool), dl(C.s, C.pool), dvb(C.s, C.pool);
     const double* hu[3] = {ux, uy, uz};
     for (int e = 0; e < 3; e++) {
         du[e].alloc(cnt[e]);
@@ -2690,7 +2708,7 @@ int lsg_convective_apply(lsg_ctx* h, int dir, const double* ux, const double* uy
     const long long cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
                               (long long)d.N * d.M * (d.K - 1)};
     const double* hu[3] = {ux, uy, uz};
-    DevBuf<double> du[3], dv, di, dout;
+    TmpBuf<double> du[3] = {TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool)}, dv(C.s, C.pool), di(C.s, C.pool), dout(C.s, C.pool);
     for (int k = 0; k < 3; k++) {
         du[k].alloc(cnt[k]);
         LSG_CUDA(cudaMemcpyAsync(du[k].p, hu[k], cnt[k] * 8, cudaMemcpyHostToDevice, C.s));
@@ -2740,7 +2758,7 @@ int lsg_projection_correct(lsg_ctx* h, const double* phi, const double* us, cons
     const Dims& d = C.d;
     const long long n = C.n, cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
                                        (long long)d.N * d.M * (d.K - 1)};
-    DevBuf<double> dphi, dp, dpred[3], dout[3];
+    TmpBuf<double> dphi(C.s, C.pool), dp(C.s, C.pool), dpred[3] = {TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool)}, dout[3] = {TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool)};
     dphi.alloc(n);
     dp.alloc(n);
     const double* hpred[3] = {us, vs, ws};
@@ -2845,7 +2863,7 @@ int lsg_apply(lsg_ctx* h, const double* x, double* y)
     LSG_REQUIRE(x && y, LSG_ERR_ARG, "null vector");
     LSG_CUDA(cudaSetDevice(C.device));
     const long long n = C.n;
-    DevBuf<double> dx, dy;
+    TmpBuf<double> dx(C.s, C.pool), dy(C.s, C.pool);
     dx.alloc(n);
     dy.alloc(n);
     LSG_CUDA(cudaMemcpyAsync(dx.p, x, n * 8, cudaMemcpyHostToDevice, C.s));
@@ -2985,7 +3003,7 @@ int lsg_apply_transpose(lsg_ctx* h, const double* x, double* y)
     LSG_REQUIRE(x && y, LSG_ERR_ARG, "null vector");
     LSG_CUDA(cudaSetDevice(C.device));
     const long long n = C.n;
-    DevBuf<double> AT, dx, dy;
+    TmpBuf<double> AT(C.s, C.pool), dx(C.s, C.pool), dy(C.s, C.pool);
     AT.alloc(7 * n);
     dx.alloc(n);
     dy.alloc(n);
@@ -3020,7 +3038,7 @@ int lsg_projection_adjoint(lsg_ctx* h, const double* ubar_out, const double* vba
                                        (long long)d.N * d.M * (d.K - 1)};
     const double* hout[3] = {ubar_out, vbar_out, wbar_out};
     double* hin[3] = {ubar, vbar, wbar};
-    DevBuf<double> dout[3], din[3], dp, df;
+    TmpBuf<double> dout[3] = {TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool)}, din[3] = {TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool)}, dp(C.s, C.pool), df(C.s, C.pool);
     for (int k = 0; k < 3; k++) {
         dout[k].alloc(cnt[k]);
         din[k].alloc(cnt[k]);
@@ -3033,6 +3051,8 @@ int lsg_projection_adjoint(lsg_ctx* h, const double* ubar_out, const double* vba
     k_projection_adjoint_phi<<<dim3((d.N + 31) / 32, (d.M + 7) / 8, d.K), blk, 0, C.s>>>(
         d.N, d.M, d.K, g.stype[0].p, g.stype[1].p, g.stype[2].p, g.theta.p, g.delta.p, g.inv[0].p, g.inv[1].p,
         g.inv[2].p, dout[0].p, dout[1].p, dout[2].p, dp.p, coef, A.bd.p);
+    LSG_CHECK_LAUNCH();
+    k_adjoint_live_rows<<<grid_for(n, 256), 256, 0, C.s>>>(n, g.type.p, C.A7.p, A.bd.p);
     LSG_CHECK_LAUNCH();
     LSG_CUDA(cudaMemsetAsync(A.xd.p, 0, n * 8, C.s));
     LSG_CUDA(cudaStreamSynchronize(C.s));
@@ -3076,6 +3096,8 @@ int lsg_projection_adjoint_device(lsg_ctx* h, const double* ubar_out, const doub
         d.N, d.M, d.K, g.stype[0].p, g.stype[1].p, g.stype[2].p, g.theta.p, g.delta.p, g.inv[0].p, g.inv[1].p,
         g.inv[2].p, dout[0], dout[1], dout[2], pbar_out, coef, A.bd.p);
     LSG_CHECK_LAUNCH();
+    k_adjoint_live_rows<<<grid_for(n, 256), 256, 0, C.s>>>(n, g.type.p, C.A7.p, A.bd.p);
+    LSG_CHECK_LAUNCH();
     LSG_CUDA(cudaMemsetAsync(A.xd.p, 0, n * 8, C.s));
     LSG_CUDA(cudaStreamSynchronize(C.s));
     const int rc = solve_device(A, A.bd.p, A.xd.p, st);
@@ -3103,7 +3125,7 @@ int lsg_gradient_transpose_device(lsg_ctx* h, const double* gx, const double* gy
     LSG_CUDA(cudaSetDevice(C.device));
     const Dims& d = C.d;
     const Context::Geometry& g = C.geo;
-    DevBuf<double> dzero;
+    TmpBuf<double> dzero(C.s, C.pool);
     dzero.alloc(C.n);
     LSG_CUDA(cudaMemsetAsync(dzero.p, 0, C.n * 8, C.s));
     k_projection_adjoint_phi<<<dim3((d.N + 31) / 32, (d.M + 7) / 8, d.K), dim3(32, 8), 0, C.s>>>(
@@ -3129,7 +3151,7 @@ int lsg_gradient_transpose(lsg_ctx* h, const double* gx, const double* gy, const
     const long long n = C.n, cnt[3] = {(long long)(d.N - 1) * d.M * d.K, (long long)d.N * (d.M - 1) * d.K,
                                        (long long)d.N * d.M * (d.K - 1)};
     const double* hin[3] = {gx, gy, gz};
-    DevBuf<double> din[3], dzero, dout;
+    TmpBuf<double> din[3] = {TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool), TmpBuf<double>(C.s, C.pool)}, dzero(C.s, C.pool), dout(C.s, C.pool);
     for (int k = 0; k < 3; k++) {
         din[k].alloc(cnt[k]);
         LSG_CUDA(cudaMemcpyAsync(din[k].p, hin[k], cnt[k] * 8, cudaMemcpyHostToDevice, C.s));
@@ -3271,7 +3293,7 @@ int lsg_operator_gradient(lsg_ctx* h, const double* lambda, const double* x, dou
     LSG_REQUIRE(lambda && x && grad, LSG_ERR_ARG, "null vector");
     LSG_CUDA(cudaSetDevice(C.device));
     const long long n = C.n;
-    DevBuf<double> dl, dx, dg;
+    TmpBuf<double> dl(C.s, C.pool), dx(C.s, C.pool), dg(C.s, C.pool);
     dl.alloc(n);
     dx.alloc(n);
     dg.alloc(7 * n);
@@ -3308,6 +3330,16 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
             else apply_resid<double>(C.mg.l64[1], C.mg.l64[1].c.p, C.mg.l64[1].r.p, C.s, 0);
         } else if (which == 4) {
             krylov7<double, 0>(C, C.Z.p, C.V.p, C.w.p, C.scal.p + 48);
+        } else if (which == 6) {
+            LSG_REQUIRE(f32 && C.Z32.p, LSG_ERR_STATE, "needs the FP32 multigrid");
+            krylov7<float, 0>(C, C.Z32.p, C.V.p, C.w.p, C.scal.p + 48);
+        } else if (which == 7) {
+            LSG_REQUIRE(f32 && C.Z32.p, LSG_ERR_STATE, "needs the FP32 multigrid");
+            const Dims& d = C.d;
+            k_spmv_dot7<float><<<grid_for(n, 256, Reducer::kMaxBlocks), 256, 0, C.s>>>(
+                d.N, d.M, d.K, C.cls0.p, C.dict0.p, C.Z32.p, C.V.p, C.w.p, C.red.partial.p, C.red.counter.p,
+                C.scal.p + 48);
+            LSG_CHECK_LAUNCH();
         } else {
             throw Error{LSG_ERR_ARG, "unknown kernel id"};
         }
@@ -3316,6 +3348,7 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
     if (which <= 2) bytes = 7.0 * w * n;              // r, lo, dinv, up, ch read; c, ch written
     else if (which == 3) bytes = (3.0 * w + 4.0) * n; // c, r read/write, row class
     else if (which == 5) bytes = (3.0 * w + 4.0) * (double)C.mg.dims[1].n();
+    else if (which == 6 || which == 7) bytes = (4.0 + 8.0 + 8.0 + 4.0) * n;   // FP32 z, v0 read, w written, class
     else bytes = (3.0 * 8.0 + 4.0) * n;               // z, v0 read, w written, row class
     // defined inputs for the timed launches
     if (which == 5) {
@@ -3339,6 +3372,10 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
     }
     if (which == 4) {
         LSG_CUDA(cudaMemsetAsync(C.Z.p, 0, n * 8, C.s));
+        LSG_CUDA(cudaMemsetAsync(C.V.p, 0, n * 8, C.s));
+    }
+    if (which == 6 || which == 7) {
+        LSG_CUDA(cudaMemsetAsync(C.Z32.p, 0, n * 4, C.s));
         LSG_CUDA(cudaMemsetAsync(C.V.p, 0, n * 8, C.s));
     }
     launch();
@@ -3529,7 +3566,7 @@ int lsg_loads_calculate(lsg_ctx* h, const double* ux, const double* uy, const do
     LSG_CUDA(cudaSetDevice(C.device));
     const long long N = L.N, M = L.M, K = L.K, n = N * M * K;
     const long long nx = (N - 1) * M * K, ny = N * (M - 1) * K, nz = N * M * (K - 1);
-    DevBuf<double> du, dv, dw, dp, dvib, dyx, dzy, dnu, df;
+    TmpBuf<double> du(C.s, C.pool), dv(C.s, C.pool), dw(C.s, C.pool), dp(C.s, C.pool), dvib(C.s, C.pool), dyx(C.s, C.pool), dzy(C.s, C.pool), dnu(C.s, C.pool), df(C.s, C.pool);
     du.alloc(nx);
     dv.alloc(ny);
     dw.alloc(nz);
@@ -3625,7 +3662,7 @@ int lsg_loads_adjoint(lsg_ctx* h, const double* weight, const double* nu_cell, d
     LSG_CUDA(cudaSetDevice(C.device));
     const long long N = L.N, M = L.M, K = L.K, n = N * M * K;
     const long long nx = (N - 1) * M * K, ny = N * (M - 1) * K, nz = N * M * (K - 1);
-    DevBuf<double> gx, gy, gz, gpd, dnu;
+    TmpBuf<double> gx(C.s, C.pool), gy(C.s, C.pool), gz(C.s, C.pool), gpd(C.s, C.pool), dnu(C.s, C.pool);
     gx.alloc(nx);
     gy.alloc(ny);
     gz.alloc(nz);

@@ -62,6 +62,32 @@ def load(n: int, seed: int = 3):
     return P, dims, pins, b
 
 
+def build_on_device(n: int, seed: int = 3, device: int = 0):
+    """(planes, dims, pins, rhs, mesh_ms) of the n^3 four-sphere case with the
+    operator built on the GPU from the seeded spheres alone: the flow task's
+    mesh build (lsg_mesh_build) and the Laplace assembly from it
+    (lsg_set_matrix_mesh), pins N-1 and NM-1 as in the reference's flow task
+    (laplace_discrete_operator.h:809-821).  For the sizes with a case file
+    the planes equal the file's, bit for bit."""
+    from . import mesh as MS
+    from . import solver as S
+    dims = (n, n, n)
+    h = (1.0 / n,) * 3
+    sph = synth.four_spheres(seed)
+    pins = np.array([n - 1, n * n - 1], dtype=np.int64)
+    s = S.MGFGMRES(device=device)
+    try:
+        ms = s.build_mesh(dims, h, MS.flow_block(dims, h, sph), bodies=MS.bodies_array(sph))
+        s.set_from_mesh(pins, setup=False)
+        P = s.planes()
+        solid = s.mesh_get("celltype") == 0
+    finally:
+        s.close()
+    mask = fluid_mask_from_planes(P, dims, pins)
+    b = synth.poisson_rhs(seed, np.where(solid, 0, 1), pins, mask)
+    return P, dims, pins, b, ms
+
+
 # --------------------------------------------------------------------------
 # Flow past a sphere (the plain FP64 LS-STAG flow case): every mesh array of
 # the time step, stored sparsely (most frequent value + exceptions) by

@@ -27,3 +27,34 @@ g++ -std=c++17 -O2 -fopenmp -fpermissive -w \
     "$HERE/ref_harness.cpp" "$SCRATCH/ref/src/Base/profiler.cpp" \
     -o "$OUT/ref_harness"
 echo "built $OUT/ref_harness"
+
+# The drop-in build: the same harness with PoissonDiscreteEquation's solver
+# ladder given the one branch a maintainer adds for the B200 library
+# (include/lsstag_b200_adapter.hpp): -DLS_STAG_USE_B200 selects
+# B200MGFGMRES, which calls liblsstag_b200.so through the C ABI.  Built only
+# when the library has been built (make -C ls-stag-3d_parallel_b200).
+REPO="$(cd "$HERE/.." && pwd)"
+LIBDIR="$REPO/ls-stag-3d_parallel_b200/lib"
+if [ -f "$LIBDIR/liblsstag_b200.so" ]; then
+    python3 - "$SCRATCH/ref/src/DiscreteEquations/poisson_discrete_equation.h" <<'PY'
+import sys
+p = sys.argv[1]
+s = open(p, encoding='utf-8', errors='surrogateescape').read()
+inc = '// ================================================================== SYNOPSIS'
+i = s.index(inc)
+s = s[:i] + '#ifdef LS_STAG_USE_B200\n#include "lsstag_b200_adapter.hpp"\n#endif\n' + s[i:]
+ladder = '#ifdef LS_STAG_USE_CUDA'
+first = s.index(ladder)
+second = s.index(ladder, first + 1)          # the solver member's ladder
+s = s[:second] + '#if defined(LS_STAG_USE_B200)\n    B200MGFGMRES solver;\n#elif defined(LS_STAG_USE_CUDA)' + \
+    s[second + len(ladder):]
+open(p, 'w', encoding='utf-8', errors='surrogateescape').write(s)
+PY
+    g++ -std=c++17 -O2 -fopenmp -fpermissive -w -DLS_STAG_USE_B200 \
+        -include "$HERE/ref_compat.h" -DCONFIG_PATH=\"/tmp\" \
+        -I"$SCRATCH/ref/src" -I"$REPO/include" \
+        "$HERE/ref_harness.cpp" "$SCRATCH/ref/src/Base/profiler.cpp" \
+        -L"$LIBDIR" -llsstag_b200 -Wl,-rpath,'$ORIGIN/../../ls-stag-3d_parallel_b200/lib' \
+        -o "$OUT/ref_harness_b200"
+    echo "built $OUT/ref_harness_b200"
+fi

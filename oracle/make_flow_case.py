@@ -1,8 +1,9 @@
-"""Generate the flow-past-a-sphere case file of this directory from the
+"""TEST INFRASTRUCTURE: generate the flow-past-a-sphere case file
+(ls-stag-3d_parallel_b200/cases/flow_sphere_128x64x64.npz) from the
 reference's own mesh build and equation set-up (oracle/_ref/ref_harness,
 built by oracle/build_ref.sh).  Run from the repository root:
 
-    python ls-stag-3d_parallel_b200/cases/make_flow_case.py
+    python oracle/make_flow_case.py
 
 Domain [0,8] x [0,4] x [0,4] on a uniform 128 x 64 x 64 staggered grid
 (h = 1/16), a sphere of diameter 1 centred at (2, 2 + h/2, 2 + h/2) (the
@@ -23,7 +24,7 @@ import sys
 
 import numpy as np
 
-ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "ls-stag-3d_parallel_b200"))
 

@@ -1074,7 +1074,7 @@ int main(int argc, char** argv)
     }
     // --- MG-FGMRES ---
     if ((int)cfg.get("fgmres", 1)) {
-        MGFGMRES& s = pEq->solver;
+        auto& s = pEq->solver;       // MGFGMRES, or the B200 adapter in the drop-in build
         s.eps = eps;
         std::vector<double> ts;
         for (int r = 0; r < reps; r++) {

@@ -16,10 +16,13 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_BIN = os.path.join(HERE, "_ref", "ref_harness")
+# the same harness built with the reference's pressure solver swapped for the
+# B200 library through include/lsstag_b200_adapter.hpp (-DLS_STAG_USE_B200)
+DROPIN_BIN = os.path.join(HERE, "_ref", "ref_harness_b200")
 
 
-def available() -> bool:
-    return os.path.isfile(REF_BIN) and os.access(REF_BIN, os.X_OK)
+def available(binary: str = REF_BIN) -> bool:
+    return os.path.isfile(binary) and os.access(binary, os.X_OK)
 
 
 @dataclass
@@ -56,12 +59,12 @@ def load_dir(d: str) -> dict:
 
 
 def run(case: Case, rhs: np.ndarray | None = None, *, threads: int = 0, workdir: str | None = None,
-        timeout: float = 3600, **opts) -> dict:
+        timeout: float = 3600, binary: str = REF_BIN, **opts) -> dict:
     """Run the harness once.  ``opts`` become config keys (restart, max_it,
     rel_tol, abs_tol, fgmres, bicgstab, dump_mg, dump_geometry, dump_matrix,
-    repeats, n_post)."""
-    if not available():
-        raise FileNotFoundError(REF_BIN)
+    repeats, n_post).  ``binary`` = DROPIN_BIN runs the drop-in build."""
+    if not available(binary):
+        raise FileNotFoundError(binary)
     own = workdir is None
     d = tempfile.mkdtemp(prefix="lsg_ref_") if own else workdir
     os.makedirs(d, exist_ok=True)
@@ -77,7 +80,7 @@ def run(case: Case, rhs: np.ndarray | None = None, *, threads: int = 0, workdir:
     cfg = os.path.join(d, "case.cfg")
     with open(cfg, "w") as f:
         f.write("\n".join(lines) + "\n")
-    subprocess.run([REF_BIN, cfg, d], check=True, timeout=timeout,
+    subprocess.run([binary, cfg, d], check=True, timeout=timeout,
                    stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
     res = load_dir(d)
     if own:

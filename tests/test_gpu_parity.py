@@ -114,18 +114,29 @@ def test_mg_fgmres_fp32_preconditioner(golden):
 
 
 def test_ilu_bicgstab(golden):
-    """BiCGStab's count moves with reduction order (the reference itself:
-    49..51 on sphere16 for 1..8 threads): a 15% window, and the solution."""
+    """ILU(0)-BiCGStab to a 1e-10 relative residual, held to the bar the
+    reference sets against itself: BiCGStab amplifies the summation order of
+    its dot products, so the reference's own count and solution move with
+    its OpenMP thread count (tests/golden/bicgstab_band.npz: 1, 2, 4, 8
+    threads; e.g. 66..71 iterations and 2.7e-7 relative L2 on spheres4_24,
+    49..51 and 1.9e-9 on sphere16).  The GPU's reduction order is one more
+    such order: its count must lie within the reference's band +-1 and its
+    solution within max(4 x the reference's largest spread, 1e-10) of the
+    reference's 1-thread solve (the fixture's)."""
     from lsstag_b200 import solver as S
-    _, g = golden
+    name, g = golden
+    band = load_golden("bicgstab_band")
+    its, spread = band[f"{name}_its"], band[f"{name}_spread"]
     s = _solver(g, cls=S.ILUBiCGStab)
     x = np.zeros_like(g["b"])
     it = s.solve(g["b"], x)
-    it_ref = int(g["bicgstab_it"][0])
-    assert abs(it - it_ref) <= max(2, int(0.15 * it_ref))
+    assert int(its.min()) - 1 <= it <= int(its.max()) + 1, (it, its)
     assert s.norm_r <= float(g["eps"][0])
     ref = g["bicgstab_x"]
-    assert np.linalg.norm(x - ref) <= 1e-6 * np.linalg.norm(ref)
+    err = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+    print(f"{name}: BiCGStab {it} iterations (reference {its.tolist()}), rel L2 {err:.3e} "
+          f"(reference spread {spread.max():.3e})")
+    assert err <= max(4.0 * float(spread.max()), 1e-10)
     s.close()
 
 
