@@ -488,7 +488,8 @@ int lsg_mg_level_tridiag(lsg_ctx* ctx, int level, char dir, double* c, double* d
    5 the residual update of the first coarse level (Galerkin stencil),
    6 the operator apply fused with a dot product on an FP32 preconditioned
    vector (the Krylov product of the FP32-multigrid solve), 7 the same
-   product by the one-thread-per-cell kernel the solve uses on wide grids.
+   product by the one-thread-per-cell kernel the solve uses on wide grids,
+   8 the same product with the z planes staged in shared memory.
    Returns the mean duration of one launch and the algorithmic HBM bytes one
    launch moves (compulsory traffic of its inputs and outputs).  Needs
    lsg_setup with the multigrid preconditioner. */
@@ -514,6 +515,13 @@ int lsg_profile_kernel(lsg_ctx* ctx, int which, int reps, double* ms_per_launch,
 int lsg_residual_norm_noalloc(int N, int M, int K, const double* planes, const double* x, const double* b,
                               double* r, double* norm2, void* stream);
 
+/* Change the absolute stopping tolerance of the next solves without a new
+   set-up (the hierarchy, factors and graphs stay): what the reference's
+   equations do when they set solver.eps before a solve
+   (IterativeSolverInterface::eps, iterative_solver_interface.h:66), e.g. a
+   tolerance relative to each right-hand side's norm. */
+int lsg_set_tolerance(lsg_ctx* ctx, double eps);
+
 /* Mesh build of the flow task on the device: the restatement, for a uniform
    grid, of BaseTaskDescription::buildMesh (base_task_description.h:330-371)
    for a flow past fixed bodies -- the level set (the task's buildLS, e.g.
@@ -527,8 +535,10 @@ int lsg_residual_norm_noalloc(int N, int M, int K, const double* planes, const d
    (calcTheta; getThetaZ / BuildTheta / tbBuildTheta, :1652-1837), cell
    volumes (kernel v, :1838-2714) and their inverses
    (ls_stag_base_mesh_params.h:77-85), staggered cell types (cvu / cvv / cvw,
-   :108-136), staggered volumes (mx / my / mz, :2804-2826) and their inverses.
-   Bit-identical to the reference's arrays.
+   :108-136), staggered volumes (mx / my / mz, :2804-2826) and their inverses,
+   the immersed-boundary face areas (buildDelta_ib: calcDeltaIB, :186-1650)
+   and inverse distances (buildInvBaseDelta_ib: calcInvBaseDeltaIb,
+   :3395-3620).  Bit-identical to the reference's arrays.
      N, M, K    base grid; h[3] the uniform cell sizes (nodes at (i + 1/2) h);
      block[4]   the level-set block hs, hf, vs, vf of the task (the reference's
                 hs_loc .. vf_loc, flow_task_description.h:388-398): cells
@@ -567,6 +577,15 @@ int lsg_mesh_build(lsg_ctx* ctx, int N, int M, int K, const double* h, const int
 #define LSG_MESH_INV_MX 15    /* double, x-grid: 1 / M_x */
 #define LSG_MESH_INV_MY 16
 #define LSG_MESH_INV_MZ 17
+/* immersed-boundary face areas (calcDeltaIB, ls_stag_uniform_mesh.h:186-1650)
+   and inverse distances (calcInvBaseDeltaIb, :3395-3620), double 3n each */
+#define LSG_MESH_DIB_EN 18
+#define LSG_MESH_DIB_WS 19
+#define LSG_MESH_DIB_NB 20
+#define LSG_MESH_DIB_ST 21
+#define LSG_MESH_DIB_MAX 22
+#define LSG_MESH_INV_DIB_NE 23
+#define LSG_MESH_INV_DIB_TN 24
 int lsg_mesh_get(lsg_ctx* ctx, int field, void* out);
 /* Fixed-point sweeps the oscillation fix took in the last build (>= 1). */
 int lsg_mesh_osc_sweeps(const lsg_ctx* ctx);

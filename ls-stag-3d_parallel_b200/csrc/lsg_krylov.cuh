@@ -136,6 +136,100 @@ __global__ void __launch_bounds__(256, 3) k_krylov7z(int N, int M, int K, int zc
     grid_reduce<1>(s, partial, counter, out);
 }
 
+// The same Krylov products with the z planes staged in shared memory, as
+// k_apply27s does: a CTA marches a 32 x 8 (x, y) tile along z with the tile's
+// planes z-1, z, z+1 and their one-cell halo in a ring of three shared
+// buffers, each plane read once per CTA by coalesced loads issued one plane
+// ahead; the seven neighbours of a cell then come from shared memory.  Row
+// class and v stream from DRAM one step ahead.  Same summation order and
+// neighbour guards as k_krylov7z.
+template <typename Tz, int MODE>
+__global__ void __launch_bounds__(256) k_krylov7s(int N, int M, int K, int zc, const int* __restrict__ cls,
+                                                   const double* __restrict__ dict, const Tz* __restrict__ z,
+                                                   const double* __restrict__ v, double* __restrict__ w,
+                                                   double* partial, unsigned int* counter, double* out)
+{
+    constexpr int TW = 34, TH = 10, TP = TW * TH;
+    __shared__ Tz sp[3][TP];
+    double s[1] = {0.0};
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const int ix = blockIdx.x * 32 + threadIdx.x;
+    const int iy = blockIdx.y * 8 + threadIdx.y;
+    const bool own = ix < N && iy < M;
+    const int NM = N * M;                                  // grids hold fewer than 2^31 cells
+    const int z0 = blockIdx.z * zc;
+    const int z1 = min(z0 + zc, K);
+    const int gx0 = blockIdx.x * 32 - 1, gy0 = blockIdx.y * 8 - 1;
+    int goff[2];
+    bool gin[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int e = tid + 256 * q;
+        const int ly = e / TW, lx = e - ly * TW;
+        const int gx = gx0 + lx, gy = gy0 + ly;
+        gin[q] = (e < TP) && gx >= 0 && gx < N && gy >= 0 && gy < M;
+        goff[q] = gx + N * gy;
+    }
+    auto fetch = [&](int zz, Tz (&t)[2]) {
+        const bool zin = zz >= 0 && zz < K;
+#pragma unroll
+        for (int q = 0; q < 2; q++) t[q] = (zin && gin[q]) ? z[goff[q] + NM * zz] : (Tz)0;
+    };
+    auto stage = [&](int slot, const Tz (&t)[2]) {
+        sp[slot][tid] = t[0];
+        if (tid + 256 < TP) sp[slot][tid + 256] = t[1];
+    };
+    Tz t[2];
+    fetch(z0 - 1, t);
+    stage(0, t);
+    fetch(z0, t);
+    stage(1, t);
+    fetch(z0 + 1, t);
+    const int col = ix + N * iy;
+    int cn = own ? cls[col + NM * z0] : 0;
+    double vn = own ? v[col + NM * z0] : 0.0;
+    const bool hasw = ix > 0, hase = ix < N - 1, hass = iy > 0, hasn = iy < M - 1;
+    int sm = 0, sc = 1, sn = 2;
+    const int c0 = (threadIdx.y + 1) * TW + threadIdx.x + 1;
+    for (int zz = z0; zz < z1; zz++) {
+        stage(sn, t);
+        __syncthreads();
+        if (zz + 2 <= z1) fetch(zz + 2, t);
+        const int cl = cn;
+        const double vv = vn;
+        if (own && zz + 1 < z1) {
+            cn = cls[col + NM * (zz + 1)];
+            vn = v[col + NM * (zz + 1)];
+        }
+        if (own) {
+            const double* a = dict + (size_t)cl * 7;
+            const Tz* pc = sp[sc];
+            double acc = a[3] * (double)pc[c0];
+            acc += a[0] * (double)sp[sm][c0];
+            if (hass) acc += a[1] * (double)pc[c0 - TW];
+            if (hasw) acc += a[2] * (double)pc[c0 - 1];
+            if (hase) acc += a[4] * (double)pc[c0 + 1];
+            if (hasn) acc += a[5] * (double)pc[c0 + TW];
+            acc += a[6] * (double)sp[sn][c0];
+            const int i = col + NM * zz;
+            if (MODE == 0) {
+                w[i] = acc;
+                s[0] += acc * vv;
+            } else {
+                const double r = vv - acc;
+                w[i] = r;
+                s[0] += r * r;
+            }
+        }
+        __syncthreads();
+        const int tt = sm;
+        sm = sc;
+        sc = sn;
+        sn = tt;
+    }
+    grid_reduce<1>(s, partial, counter, out);
+}
+
 // One modified Gram-Schmidt step fused with the next dot:
 //   w -= h_prev * vprev ;  out = (w, vnext)   (vnext == w gives ||w||^2)
 __global__ void __launch_bounds__(256) k_mgs_step(long long n, const double* __restrict__ hprev,

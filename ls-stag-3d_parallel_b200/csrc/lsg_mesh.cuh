@@ -491,6 +491,753 @@ LSG_MHD int staggered_type(int tc, int te, double face_theta)
 }
 
 // ---------------------------------------------------------------------------
+// immersed-boundary face areas (calcDeltaIB, ls_stag_uniform_mesh.h:186-1650):
+// per cell five coordinate triples -- delta_ib_en, _ws, _nb, _st and _max,
+// the areas of the cut surface seen from the east/north, west/south,
+// north/bottom and south/top sides -- from theta and delta.  The reference
+// writes one block of assignments per cell type (and, for the bottom and
+// top border cells, per top-face side type); each block is restated here as a
+// short program for a stack machine: push theta (component, back-offset mask
+// 1 = x-1, 2 = y-1, 4 = z-1), push delta (component), push a constant, load or
+// store a local, add / subtract / multiply / absolute value / negate in the
+// block's own order, write one output component, or copy one output triple
+// into another.  Types without a block keep their arrays untouched (0).
+// ---------------------------------------------------------------------------
+enum DibOp : unsigned char {
+    DIB_END = 0, DIB_T, DIB_D, DIB_C, DIB_LD, DIB_ST, DIB_ADD, DIB_SUB, DIB_MUL, DIB_ABS, DIB_NEG, DIB_OUT, DIB_COPY
+};
+struct DibCase {
+    int type;      // cell type
+    int side_z;    // top-face side type (bottom / top border cells), else -1
+    int at;        // offset of the program in the code blob
+};
+constexpr int kDibCases = 156;
+constexpr int kDibCode = 13094;
+#define LSG_DIB_TABLE { \
+    {-27, -1, 0}, {-26, -1, 46}, {-25, -1, 92}, \
+    {-24, -1, 138}, {-23, -1, 184}, {-22, -1, 230}, \
+    {-21, -1, 276}, {-20, -1, 322}, {-19, -1, 368}, \
+    {-18, -1, 406}, {-17, -1, 444}, {-16, -1, 482}, \
+    {-15, -1, 520}, {-14, -1, 558}, {-13, -1, 596}, \
+    {-12, -1, 634}, {-11, -1, 672}, {-10, -1, 710}, \
+    {-9, -1, 748}, {-8, -1, 786}, {-7, -1, 824}, \
+    {-6, -1, 854}, {-5, -1, 884}, {-4, -1, 914}, \
+    {-3, 0, 944}, {-3, 1, 966}, {-3, 10, 1024}, \
+    {-3, 11, 1082}, {-3, 100, 1142}, {-3, 110, 1200}, \
+    {-3, 111, 1260}, {-3, 1000, 1354}, {-3, 1001, 1412}, \
+    {-3, 1011, 1472}, {-3, 1100, 1576}, {-3, 1101, 1636}, \
+    {-3, 1110, 1730}, {-3, 1111, 1834}, {-2, 0, 1856}, \
+    {-2, 1, 1878}, {-2, 10, 1936}, {-2, 11, 1994}, \
+    {-2, 100, 2054}, {-2, 110, 2112}, {-2, 111, 2172}, \
+    {-2, 1000, 2266}, {-2, 1001, 2324}, {-2, 1011, 2384}, \
+    {-2, 1100, 2488}, {-2, 1101, 2548}, {-2, 1110, 2642}, \
+    {-2, 1111, 2746}, {0, -1, 2768}, {1, -1, 2814}, \
+    {10, -1, 2884}, {11, -1, 2954}, {100, -1, 3042}, \
+    {110, -1, 3112}, {111, -1, 3200}, {1000, -1, 3294}, \
+    {1001, -1, 3364}, {1011, -1, 3452}, {1100, -1, 3546}, \
+    {1101, -1, 3634}, {1110, -1, 3728}, {1111, -1, 3822}, \
+    {10000, -1, 3912}, {10001, -1, 3982}, {10011, -1, 4070}, \
+    {11001, -1, 4164}, {11011, -1, 4258}, {11111, -1, 4358}, \
+    {100000, -1, 4456}, {100010, -1, 4526}, {100011, -1, 4614}, \
+    {100110, -1, 4708}, {100111, -1, 4802}, {101111, -1, 4902}, \
+    {110000, -1, 5000}, {110001, -1, 5088}, {110010, -1, 5182}, \
+    {110011, -1, 5276}, {110111, -1, 5366}, {111011, -1, 5464}, \
+    {111111, -1, 5562}, {1000000, -1, 5706}, {1000100, -1, 5776}, \
+    {1000110, -1, 5864}, {1001100, -1, 5958}, {1001110, -1, 6052}, \
+    {1001111, -1, 6152}, {1100000, -1, 6250}, {1100010, -1, 6338}, \
+    {1100100, -1, 6432}, {1100110, -1, 6526}, {1100111, -1, 6616}, \
+    {1101110, -1, 6714}, {1101111, -1, 6812}, {1110000, -1, 6956}, \
+    {1110010, -1, 7050}, {1110011, -1, 7150}, {1110110, -1, 7248}, \
+    {1110111, -1, 7346}, {1111111, -1, 7490}, {10000000, -1, 7612}, \
+    {10001000, -1, 7682}, {10001001, -1, 7770}, {10001100, -1, 7864}, \
+    {10001101, -1, 7958}, {10001111, -1, 8058}, {10010000, -1, 8156}, \
+    {10010001, -1, 8244}, {10011000, -1, 8338}, {10011001, -1, 8432}, \
+    {10011011, -1, 8522}, {10011101, -1, 8620}, {10011111, -1, 8718}, \
+    {10110000, -1, 8862}, {10110001, -1, 8956}, {10110011, -1, 9056}, \
+    {10111001, -1, 9154}, {10111011, -1, 9252}, {10111111, -1, 9396}, \
+    {11000000, -1, 9518}, {11000100, -1, 9606}, {11001000, -1, 9700}, \
+    {11001100, -1, 9794}, {11001101, -1, 9884}, {11001110, -1, 9982}, \
+    {11001111, -1, 10080}, {11010000, -1, 10214}, {11011000, -1, 10308}, \
+    {11011001, -1, 10408}, {11011100, -1, 10506}, {11011101, -1, 10604}, \
+    {11011111, -1, 10738}, {11100000, -1, 10850}, {11100100, -1, 10944}, \
+    {11100110, -1, 11044}, {11101100, -1, 11142}, {11101110, -1, 11240}, \
+    {11101111, -1, 11384}, {11110000, -1, 11506}, {11110001, -1, 11596}, \
+    {11110010, -1, 11694}, {11110011, -1, 11792}, {11110100, -1, 11926}, \
+    {11110110, -1, 12024}, {11110111, -1, 12168}, {11111000, -1, 12280}, \
+    {11111001, -1, 12378}, {11111011, -1, 12522}, {11111100, -1, 12644}, \
+    {11111101, -1, 12788}, {11111110, -1, 12910}, {11111111, -1, 13032}, \
+}
+#define LSG_DIB_CODE { \
+    3, 0, 2, 0, 8, 0, 2, 1, 8, 0, 11, 0, 3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, \
+    3, 0, 2, 1, 8, 0, 2, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 0, \
+    2, 0, 8, 0, 2, 1, 8, 0, 11, 0, 3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 0, \
+    2, 1, 8, 0, 2, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 0, 2, 0, \
+    8, 0, 2, 1, 8, 0, 11, 0, 3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 0, 2, 1, \
+    8, 0, 2, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 0, 2, 0, 8, 0, \
+    2, 1, 8, 0, 11, 0, 3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 0, 2, 1, 8, 0, \
+    2, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 0, 2, 0, 8, 0, 2, 1, \
+    8, 0, 11, 0, 3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 0, 2, 1, 8, 0, 2, 2, \
+    8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 0, 2, 0, 8, 0, 2, 1, 8, 0, \
+    11, 0, 3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 0, 2, 1, 8, 0, 2, 2, 8, 0, \
+    11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 0, 2, 0, 8, 0, 2, 1, 8, 0, 11, 0, \
+    3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 0, 2, 1, 8, 0, 2, 2, 8, 0, 11, 2, \
+    12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 0, 2, 0, 8, 0, 2, 1, 8, 0, 11, 0, 3, 0, \
+    2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 0, 2, 1, 8, 0, 2, 2, 8, 0, 11, 2, 12, 8, \
+    12, 16, 12, 24, 12, 32, 0, 0, 3, 1, 11, 0, 3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, \
+    3, 0, 2, 1, 8, 0, 2, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 1, \
+    11, 0, 3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 0, 2, 1, 8, 0, 2, 2, 8, 0, \
+    11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 1, 11, 0, 3, 0, 2, 0, 8, 0, 2, 2, \
+    8, 0, 11, 1, 3, 0, 2, 1, 8, 0, 2, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, \
+    0, 0, 3, 1, 11, 0, 3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 0, 2, 1, 8, 0, \
+    2, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 0, 2, 0, 8, 0, 2, 1, \
+    8, 0, 11, 0, 3, 1, 11, 1, 3, 0, 2, 1, 8, 0, 2, 2, 8, 0, 11, 2, 12, 8, 12, 16, \
+    12, 24, 12, 32, 0, 0, 3, 0, 2, 0, 8, 0, 2, 1, 8, 0, 11, 0, 3, 1, 11, 1, 3, 0, \
+    2, 1, 8, 0, 2, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 0, 2, 0, \
+    8, 0, 2, 1, 8, 0, 11, 0, 3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 1, 11, 2, \
+    12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 0, 2, 0, 8, 0, 2, 1, 8, 0, 11, 0, 3, 0, \
+    2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 1, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, \
+    3, 0, 2, 0, 8, 0, 2, 1, 8, 0, 11, 0, 3, 1, 11, 1, 3, 0, 2, 1, 8, 0, 2, 2, \
+    8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 0, 2, 0, 8, 0, 2, 1, 8, 0, \
+    11, 0, 3, 1, 11, 1, 3, 0, 2, 1, 8, 0, 2, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, \
+    12, 32, 0, 0, 3, 0, 2, 0, 8, 0, 2, 1, 8, 0, 11, 0, 3, 0, 2, 0, 8, 0, 2, 2, \
+    8, 0, 11, 1, 3, 1, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 0, 2, 0, 8, 0, \
+    2, 1, 8, 0, 11, 0, 3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 1, 11, 2, 12, 8, \
+    12, 16, 12, 24, 12, 32, 0, 0, 3, 1, 11, 0, 3, 1, 11, 1, 3, 0, 2, 1, 8, 0, 2, 2, \
+    8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 1, 11, 0, 3, 1, 11, 1, 3, 0, \
+    2, 1, 8, 0, 2, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 3, 1, 11, 0, \
+    3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 1, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, \
+    0, 0, 3, 1, 11, 0, 3, 0, 2, 0, 8, 0, 2, 2, 8, 0, 11, 1, 3, 1, 11, 2, 12, 8, \
+    12, 16, 12, 24, 12, 32, 0, 0, 3, 1, 11, 0, 3, 1, 11, 1, 3, 1, 11, 2, 12, 8, 12, 16, \
+    12, 24, 12, 32, 0, 0, 2, 2, 5, 0, 3, 0, 1, 9, 8, 0, 2, 0, 8, 0, 4, 0, 8, 0, \
+    5, 1, 3, 0, 1, 0, 8, 0, 2, 1, 8, 0, 4, 0, 8, 0, 5, 2, 3, 1, 11, 0, 4, 1, \
+    11, 1, 4, 2, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 2, 5, 0, 3, 0, 1, 9, \
+    8, 0, 2, 0, 8, 0, 4, 0, 8, 0, 5, 1, 3, 0, 1, 4, 8, 0, 2, 1, 8, 0, 4, 0, \
+    8, 0, 5, 2, 3, 1, 11, 0, 4, 1, 11, 1, 4, 2, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, \
+    0, 0, 2, 2, 5, 0, 3, 0, 2, 0, 8, 0, 4, 0, 8, 0, 5, 1, 3, 0, 1, 4, 1, 0, \
+    7, 0, 9, 0, 8, 0, 2, 1, 8, 0, 4, 0, 8, 0, 5, 2, 3, 1, 11, 0, 4, 1, 11, 1, \
+    4, 2, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 2, 5, 0, 3, 0, 1, 1, 8, 0, \
+    2, 0, 8, 0, 4, 0, 8, 0, 5, 1, 3, 0, 1, 4, 8, 0, 2, 1, 8, 0, 4, 0, 8, 0, \
+    5, 2, 3, 1, 11, 0, 4, 1, 11, 1, 4, 2, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, \
+    2, 2, 5, 0, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 2, 0, 8, 0, 4, 0, 8, 0, \
+    5, 1, 3, 0, 2, 1, 8, 0, 4, 0, 8, 0, 5, 2, 3, 1, 11, 0, 4, 1, 11, 1, 4, 2, \
+    11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 2, 5, 0, 3, 2, 1, 1, 7, 0, 2, 0, \
+    8, 0, 4, 0, 8, 0, 5, 1, 3, 0, 4, 1, 8, 0, 5, 2, 3, 2, 1, 0, 7, 0, 2, 1, \
+    8, 0, 4, 0, 8, 0, 5, 3, 3, 0, 4, 3, 8, 0, 5, 4, 3, 1, 11, 0, 4, 1, 11, 1, \
+    4, 3, 11, 2, 3, 1, 11, 3, 3, 1, 11, 4, 3, 1, 11, 5, 3, 1, 11, 6, 4, 2, 11, 7, \
+    4, 4, 11, 8, 12, 26, 12, 32, 0, 0, 2, 2, 5, 0, 3, 0, 1, 1, 8, 0, 2, 0, 8, 0, \
+    4, 0, 8, 0, 5, 1, 3, 0, 1, 0, 8, 0, 2, 1, 8, 0, 4, 0, 8, 0, 5, 2, 3, 1, \
+    11, 0, 4, 1, 11, 1, 4, 2, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 2, 5, 0, \
+    3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 2, 0, 8, 0, 4, 0, 8, 0, 5, 1, 3, 0, \
+    2, 1, 8, 0, 4, 0, 8, 0, 5, 2, 3, 1, 11, 0, 4, 1, 11, 1, 4, 2, 11, 2, 12, 8, \
+    12, 16, 12, 24, 12, 32, 0, 0, 2, 2, 5, 0, 3, 2, 1, 1, 7, 0, 2, 0, 8, 0, 4, 0, \
+    8, 0, 5, 1, 3, 0, 4, 1, 8, 0, 5, 2, 3, 2, 1, 4, 7, 0, 2, 1, 8, 0, 4, 0, \
+    8, 0, 5, 3, 3, 0, 4, 3, 8, 0, 5, 4, 3, 1, 11, 0, 3, 1, 11, 1, 4, 3, 11, 2, \
+    3, 1, 11, 3, 4, 1, 11, 4, 3, 1, 11, 5, 3, 1, 11, 6, 4, 2, 11, 7, 4, 4, 11, 8, \
+    12, 26, 3, 1, 11, 12, 4, 1, 11, 13, 4, 3, 11, 14, 0, 0, 2, 2, 5, 0, 3, 0, 2, 0, \
+    8, 0, 4, 0, 8, 0, 5, 1, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 2, 1, 8, 0, \
+    4, 0, 8, 0, 5, 2, 3, 1, 11, 0, 4, 1, 11, 1, 4, 2, 11, 2, 12, 8, 12, 16, 12, 24, \
+    12, 32, 0, 0, 2, 2, 5, 0, 3, 2, 1, 9, 7, 0, 2, 0, 8, 0, 4, 0, 8, 0, 5, 1, \
+    3, 0, 4, 1, 8, 0, 5, 2, 3, 2, 1, 4, 7, 0, 2, 1, 8, 0, 4, 0, 8, 0, 5, 3, \
+    3, 0, 4, 3, 8, 0, 5, 4, 3, 1, 11, 0, 3, 1, 11, 1, 3, 1, 11, 2, 3, 1, 11, 3, \
+    4, 1, 11, 4, 4, 3, 11, 5, 3, 1, 11, 6, 4, 2, 11, 7, 4, 4, 11, 8, 12, 26, 12, 33, \
+    0, 0, 2, 2, 5, 0, 3, 2, 1, 9, 7, 0, 2, 0, 8, 0, 4, 0, 8, 0, 5, 1, 3, 0, \
+    4, 1, 8, 0, 5, 2, 3, 2, 1, 0, 7, 0, 2, 1, 8, 0, 4, 0, 8, 0, 5, 3, 3, 0, \
+    4, 3, 8, 0, 5, 4, 3, 1, 11, 0, 4, 1, 11, 1, 3, 1, 11, 2, 3, 1, 11, 3, 3, 1, \
+    11, 4, 4, 3, 11, 5, 3, 1, 11, 6, 4, 2, 11, 7, 4, 4, 11, 8, 12, 26, 3, 1, 11, 12, \
+    4, 1, 11, 13, 4, 3, 11, 14, 0, 0, 3, 1, 11, 0, 3, 1, 11, 1, 3, 1, 11, 2, 12, 8, \
+    12, 16, 12, 24, 12, 32, 0, 0, 3, 1, 11, 0, 3, 1, 11, 1, 3, 1, 11, 2, 12, 8, 12, 16, \
+    12, 24, 12, 32, 0, 0, 2, 2, 5, 0, 3, 0, 1, 9, 8, 0, 2, 0, 8, 0, 4, 0, 8, 0, \
+    5, 1, 3, 0, 1, 0, 8, 0, 2, 1, 8, 0, 4, 0, 8, 0, 5, 2, 3, 1, 11, 0, 4, 1, \
+    11, 1, 4, 2, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 2, 5, 0, 3, 0, 1, 9, \
+    8, 0, 2, 0, 8, 0, 4, 0, 8, 0, 5, 1, 3, 0, 1, 4, 8, 0, 2, 1, 8, 0, 4, 0, \
+    8, 0, 5, 2, 3, 1, 11, 0, 4, 1, 11, 1, 4, 2, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, \
+    0, 0, 2, 2, 5, 0, 3, 0, 2, 0, 8, 0, 4, 0, 8, 0, 5, 1, 3, 0, 1, 4, 1, 0, \
+    7, 0, 9, 0, 8, 0, 2, 1, 8, 0, 4, 0, 8, 0, 5, 2, 3, 1, 11, 0, 4, 1, 11, 1, \
+    4, 2, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 2, 5, 0, 3, 0, 1, 1, 8, 0, \
+    2, 0, 8, 0, 4, 0, 8, 0, 5, 1, 3, 0, 1, 4, 8, 0, 2, 1, 8, 0, 4, 0, 8, 0, \
+    5, 2, 3, 1, 11, 0, 4, 1, 11, 1, 4, 2, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, \
+    2, 2, 5, 0, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 2, 0, 8, 0, 4, 0, 8, 0, \
+    5, 1, 3, 0, 2, 1, 8, 0, 4, 0, 8, 0, 5, 2, 3, 1, 11, 0, 4, 1, 11, 1, 4, 2, \
+    11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 2, 5, 0, 3, 2, 1, 1, 7, 0, 2, 0, \
+    8, 0, 4, 0, 8, 0, 5, 1, 3, 0, 4, 1, 8, 0, 5, 2, 3, 2, 1, 0, 7, 0, 2, 1, \
+    8, 0, 4, 0, 8, 0, 5, 3, 3, 0, 4, 3, 8, 0, 5, 4, 3, 1, 11, 0, 4, 1, 11, 1, \
+    4, 3, 11, 2, 3, 1, 11, 3, 3, 1, 11, 4, 3, 1, 11, 5, 3, 1, 11, 6, 4, 2, 11, 7, \
+    4, 4, 11, 8, 12, 26, 12, 32, 0, 0, 2, 2, 5, 0, 3, 0, 1, 1, 8, 0, 2, 0, 8, 0, \
+    4, 0, 8, 0, 5, 1, 3, 0, 1, 0, 8, 0, 2, 1, 8, 0, 4, 0, 8, 0, 5, 2, 3, 1, \
+    11, 0, 4, 1, 11, 1, 4, 2, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 2, 5, 0, \
+    3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 2, 0, 8, 0, 4, 0, 8, 0, 5, 1, 3, 0, \
+    2, 1, 8, 0, 4, 0, 8, 0, 5, 2, 3, 1, 11, 0, 4, 1, 11, 1, 4, 2, 11, 2, 12, 8, \
+    12, 16, 12, 24, 12, 32, 0, 0, 2, 2, 5, 0, 3, 2, 1, 1, 7, 0, 2, 0, 8, 0, 4, 0, \
+    8, 0, 5, 1, 3, 0, 4, 1, 8, 0, 5, 2, 3, 2, 1, 4, 7, 0, 2, 1, 8, 0, 4, 0, \
+    8, 0, 5, 3, 3, 0, 4, 3, 8, 0, 5, 4, 3, 1, 11, 0, 3, 1, 11, 1, 4, 3, 11, 2, \
+    3, 1, 11, 3, 4, 1, 11, 4, 3, 1, 11, 5, 3, 1, 11, 6, 4, 2, 11, 7, 4, 4, 11, 8, \
+    12, 26, 3, 1, 11, 12, 4, 1, 11, 13, 4, 3, 11, 14, 0, 0, 2, 2, 5, 0, 3, 0, 2, 0, \
+    8, 0, 4, 0, 8, 0, 5, 1, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 2, 1, 8, 0, \
+    4, 0, 8, 0, 5, 2, 3, 1, 11, 0, 4, 1, 11, 1, 4, 2, 11, 2, 12, 8, 12, 16, 12, 24, \
+    12, 32, 0, 0, 2, 2, 5, 0, 3, 2, 1, 9, 7, 0, 2, 0, 8, 0, 4, 0, 8, 0, 5, 1, \
+    3, 0, 4, 1, 8, 0, 5, 2, 3, 2, 1, 4, 7, 0, 2, 1, 8, 0, 4, 0, 8, 0, 5, 3, \
+    3, 0, 4, 3, 8, 0, 5, 4, 3, 1, 11, 0, 3, 1, 11, 1, 3, 1, 11, 2, 3, 1, 11, 3, \
+    4, 1, 11, 4, 4, 3, 11, 5, 3, 1, 11, 6, 4, 2, 11, 7, 4, 4, 11, 8, 12, 26, 12, 33, \
+    0, 0, 2, 2, 5, 0, 3, 2, 1, 9, 7, 0, 2, 0, 8, 0, 4, 0, 8, 0, 5, 1, 3, 0, \
+    4, 1, 8, 0, 5, 2, 3, 2, 1, 0, 7, 0, 2, 1, 8, 0, 4, 0, 8, 0, 5, 3, 3, 0, \
+    4, 3, 8, 0, 5, 4, 3, 1, 11, 0, 4, 1, 11, 1, 3, 1, 11, 2, 3, 1, 11, 3, 3, 1, \
+    11, 4, 4, 3, 11, 5, 3, 1, 11, 6, 4, 2, 11, 7, 4, 4, 11, 8, 12, 26, 3, 1, 11, 12, \
+    4, 1, 11, 13, 4, 3, 11, 14, 0, 0, 3, 1, 11, 0, 3, 1, 11, 1, 3, 1, 11, 2, 12, 8, \
+    12, 16, 12, 24, 12, 32, 0, 0, 3, 0, 2, 1, 8, 0, 2, 2, 8, 0, 11, 0, 3, 0, 2, 0, \
+    8, 0, 2, 2, 8, 0, 11, 1, 3, 0, 2, 0, 8, 0, 2, 1, 8, 0, 11, 2, 12, 8, 12, 16, \
+    12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 18, 8, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 11, 0, 3, 0, 1, 9, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, \
+    11, 1, 3, 0, 1, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, \
+    12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 18, 8, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 11, 0, 3, 0, 1, 9, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 11, 1, \
+    3, 0, 1, 4, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, \
+    0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 8, 0, 4, 0, 8, 0, \
+    4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, \
+    8, 0, 5, 4, 3, 0, 1, 18, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, \
+    4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, \
+    5, 1, 2, 2, 5, 2, 3, 0, 1, 18, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 11, 0, 3, 0, \
+    1, 1, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 11, 1, 3, 0, 1, 4, 8, 0, 4, 1, 8, 0, \
+    4, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, \
+    2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, \
+    5, 3, 3, 0, 1, 4, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 8, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, \
+    12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, \
+    1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, \
+    7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 8, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, \
+    12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 18, 8, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 11, 0, 3, 0, 1, 1, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, \
+    11, 1, 3, 0, 1, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, \
+    12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, \
+    9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 8, 0, 4, 1, 8, 0, \
+    4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, \
+    11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, \
+    2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, \
+    4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, \
+    8, 0, 5, 4, 3, 0, 1, 18, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, \
+    4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, \
+    5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, \
+    1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, \
+    8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, \
+    12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, \
+    1, 1, 1, 9, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, \
+    1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 8, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, \
+    12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, \
+    1, 9, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, \
+    7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 8, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, \
+    12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, \
+    7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, \
+    9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 4, 0, 8, 0, 4, 1, 8, 0, \
+    5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, \
+    2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 2, 8, 0, 4, 0, 8, 0, 4, 1, \
+    8, 0, 11, 0, 3, 0, 1, 9, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 11, 1, 3, 0, 1, 0, \
+    8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, \
+    5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, \
+    5, 3, 3, 0, 1, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, \
+    7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, \
+    4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, \
+    5, 2, 3, 0, 1, 9, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 1, 4, \
+    7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, \
+    9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, \
+    11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, \
+    3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, \
+    1, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, \
+    8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, \
+    12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, \
+    1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, \
+    1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, \
+    7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, \
+    4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, \
+    5, 2, 3, 0, 1, 1, 1, 9, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, \
+    3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, \
+    3, 2, 1, 2, 7, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, \
+    11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, \
+    2, 2, 5, 2, 3, 0, 1, 2, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 11, 0, 3, 0, 1, 9, \
+    8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 11, 1, 3, 0, 1, 4, 8, 0, 4, 1, 8, 0, 4, 2, \
+    8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, \
+    5, 2, 3, 0, 1, 9, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 8, 0, \
+    4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, \
+    12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 8, 0, \
+    4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, \
+    8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, \
+    4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, \
+    12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, \
+    9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 8, 0, 4, 1, 8, 0, \
+    4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, \
+    8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, \
+    0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, \
+    8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, \
+    4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, \
+    12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 1, 9, \
+    7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 1, 4, 7, 0, \
+    9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 3, 2, 1, 2, 7, 0, 8, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, \
+    12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, \
+    8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, \
+    4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, \
+    5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, \
+    2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 8, 0, 4, 0, 8, 0, 4, 2, \
+    8, 0, 5, 3, 3, 0, 1, 0, 1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, \
+    5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, \
+    4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, \
+    5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, \
+    5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, \
+    3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, \
+    11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, \
+    2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, \
+    1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, \
+    7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, \
+    4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, \
+    5, 2, 3, 0, 3, 2, 1, 9, 7, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, \
+    1, 0, 1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, \
+    1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, \
+    11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, \
+    2, 2, 5, 2, 3, 0, 3, 2, 1, 9, 7, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, \
+    3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, \
+    1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, \
+    4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, \
+    5, 1, 2, 2, 5, 2, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, \
+    8, 0, 5, 3, 3, 2, 1, 1, 7, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 4, 4, \
+    8, 0, 5, 5, 3, 2, 1, 2, 7, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 6, 3, 0, 4, 6, \
+    8, 0, 5, 7, 4, 7, 11, 0, 4, 5, 11, 1, 4, 3, 11, 2, 4, 7, 11, 3, 4, 5, 11, 4, \
+    4, 3, 11, 5, 4, 6, 11, 6, 3, 1, 11, 7, 4, 3, 11, 8, 3, 1, 11, 9, 4, 4, 11, 10, \
+    4, 3, 11, 11, 4, 6, 11, 12, 4, 4, 11, 13, 4, 3, 11, 14, 0, 0, 2, 0, 5, 0, 2, 1, \
+    5, 1, 2, 2, 5, 2, 3, 0, 1, 2, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 11, 0, 3, 0, \
+    1, 1, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 11, 1, 3, 0, 1, 4, 8, 0, 4, 1, 8, 0, \
+    4, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, \
+    2, 2, 5, 2, 3, 0, 1, 1, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, \
+    8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, \
+    12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, \
+    1, 9, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 8, 0, \
+    4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, \
+    12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 8, 0, \
+    4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, \
+    8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, \
+    4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, \
+    12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 1, 9, 7, 0, \
+    9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, \
+    8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, \
+    12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, \
+    1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 1, 4, \
+    7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 3, 2, 1, 2, 7, 0, \
+    8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, \
+    12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, \
+    1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, \
+    8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 8, 0, 4, 0, 8, 0, 4, 1, \
+    8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, \
+    0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, \
+    8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 8, 0, 4, 1, 8, 0, 4, 2, \
+    8, 0, 5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, \
+    5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, \
+    2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 1, 9, 7, 0, 9, 0, 8, 0, \
+    4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, \
+    5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, \
+    4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, \
+    5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, \
+    8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, \
+    1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, \
+    11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, \
+    2, 2, 5, 2, 3, 0, 1, 1, 1, 9, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, \
+    5, 3, 3, 0, 3, 2, 1, 0, 7, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, \
+    1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, \
+    4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, \
+    5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, \
+    8, 0, 5, 3, 3, 0, 3, 2, 1, 0, 7, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, \
+    3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, \
+    11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, \
+    2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, \
+    4, 2, 8, 0, 5, 3, 3, 2, 1, 0, 7, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, \
+    4, 4, 8, 0, 5, 5, 3, 2, 1, 2, 7, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 6, 3, 0, \
+    4, 6, 8, 0, 5, 7, 4, 6, 11, 0, 4, 3, 11, 1, 4, 5, 11, 2, 3, 1, 11, 3, 4, 3, \
+    11, 4, 4, 5, 11, 5, 4, 7, 11, 6, 4, 3, 11, 7, 3, 1, 11, 8, 4, 7, 11, 9, 4, 3, \
+    11, 10, 4, 4, 11, 11, 4, 6, 11, 12, 4, 3, 11, 13, 4, 4, 11, 14, 0, 0, 2, 0, 5, 0, \
+    2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, \
+    4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, \
+    8, 0, 5, 4, 3, 0, 1, 2, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, \
+    4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, \
+    5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, \
+    8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, \
+    5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, \
+    4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, \
+    5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 3, 2, 1, 9, 7, 0, 8, 0, 4, 0, 8, 0, \
+    4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, \
+    8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, \
+    5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, \
+    2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 1, 9, 7, 0, 9, 0, 8, 0, \
+    4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 3, 2, 1, 0, 7, 0, 8, 0, 4, 1, 8, 0, \
+    4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, \
+    8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, \
+    0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, \
+    8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 3, 3, 2, 1, 1, 7, 0, 4, 0, 8, 0, 4, 2, \
+    8, 0, 5, 4, 3, 0, 4, 4, 8, 0, 5, 5, 3, 2, 1, 0, 7, 0, 4, 1, 8, 0, 4, 2, \
+    8, 0, 5, 6, 3, 0, 4, 6, 8, 0, 5, 7, 4, 3, 11, 0, 4, 4, 11, 1, 4, 6, 11, 2, \
+    4, 3, 11, 3, 3, 1, 11, 4, 3, 1, 11, 5, 4, 3, 11, 6, 4, 5, 11, 7, 4, 7, 11, 8, \
+    4, 3, 11, 9, 4, 5, 11, 10, 4, 7, 11, 11, 4, 3, 11, 12, 4, 4, 11, 13, 4, 6, 11, 14, \
+    0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 2, 1, 1, 7, 0, 4, 0, 8, 0, \
+    4, 2, 8, 0, 5, 3, 3, 2, 1, 0, 7, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 2, \
+    1, 2, 7, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, \
+    11, 2, 3, 1, 11, 3, 3, 1, 11, 4, 3, 1, 11, 5, 4, 5, 11, 6, 3, 1, 11, 7, 3, 1, \
+    11, 8, 3, 1, 11, 9, 4, 3, 11, 10, 4, 4, 11, 11, 3, 1, 11, 12, 3, 1, 11, 13, 3, 1, \
+    11, 14, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 2, 8, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 11, 0, 3, 0, 1, 1, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 11, 1, \
+    3, 0, 1, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, \
+    0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 8, 0, 4, 0, 8, 0, \
+    4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, \
+    1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, \
+    4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, \
+    5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 1, 9, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, \
+    8, 0, 5, 3, 3, 0, 1, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, \
+    1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, \
+    11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, \
+    2, 2, 5, 2, 3, 0, 1, 1, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, \
+    1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, \
+    7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, \
+    4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, \
+    5, 2, 3, 0, 1, 1, 1, 9, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, \
+    3, 0, 1, 0, 1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, \
+    1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, \
+    4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, \
+    5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, \
+    8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, \
+    5, 4, 3, 0, 3, 2, 1, 2, 7, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, \
+    11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, \
+    2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, \
+    4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, \
+    1, 2, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, \
+    11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, \
+    3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, \
+    1, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, \
+    8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, \
+    12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, \
+    1, 1, 1, 9, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, \
+    8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, \
+    12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, \
+    1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 4, 1, 8, 0, \
+    4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, \
+    8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, \
+    0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 1, 9, 7, 0, 9, 0, \
+    8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 3, 2, 1, 4, 7, 0, 8, 0, 4, 1, \
+    8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, \
+    4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, \
+    12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, \
+    9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 3, 2, 1, 4, 7, 0, 8, 0, \
+    4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, \
+    12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, \
+    7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 2, 1, 4, 7, 0, 4, 1, \
+    8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 4, 4, 8, 0, 5, 5, 3, 2, 1, 2, 7, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 5, 6, 3, 0, 4, 6, 8, 0, 5, 7, 3, 1, 11, 0, 4, 3, 11, 1, \
+    4, 5, 11, 2, 4, 6, 11, 3, 4, 3, 11, 4, 4, 5, 11, 5, 4, 7, 11, 6, 4, 3, 11, 7, \
+    3, 1, 11, 8, 4, 7, 11, 9, 4, 3, 11, 10, 4, 4, 11, 11, 4, 6, 11, 12, 4, 3, 11, 13, \
+    4, 4, 11, 14, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, \
+    7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 1, 4, 7, 0, \
+    9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 8, 0, 4, 0, 8, 0, \
+    4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, \
+    12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, \
+    9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 1, 4, 7, 0, 9, 0, \
+    8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, \
+    12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 3, 2, \
+    1, 9, 7, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, \
+    9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, \
+    8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, \
+    12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, \
+    1, 1, 1, 9, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 3, 2, \
+    1, 4, 7, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, \
+    9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, \
+    11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, \
+    3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 3, 3, 2, \
+    1, 1, 7, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 4, 4, 8, 0, 5, 5, 3, 2, \
+    1, 4, 7, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 6, 3, 0, 4, 6, 8, 0, 5, 7, 4, 3, \
+    11, 0, 3, 1, 11, 1, 4, 6, 11, 2, 4, 3, 11, 3, 4, 4, 11, 4, 3, 1, 11, 5, 4, 3, \
+    11, 6, 4, 5, 11, 7, 4, 7, 11, 8, 4, 3, 11, 9, 4, 5, 11, 10, 4, 7, 11, 11, 4, 3, \
+    11, 12, 4, 4, 11, 13, 4, 6, 11, 14, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, \
+    3, 2, 1, 1, 7, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 2, 1, 4, 7, 0, 4, 1, \
+    8, 0, 4, 2, 8, 0, 5, 4, 3, 2, 1, 2, 7, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, \
+    3, 1, 11, 0, 3, 1, 11, 1, 4, 4, 11, 2, 4, 5, 11, 3, 4, 3, 11, 4, 3, 1, 11, 5, \
+    4, 5, 11, 6, 3, 1, 11, 7, 3, 1, 11, 8, 3, 1, 11, 9, 4, 3, 11, 10, 4, 4, 11, 11, \
+    3, 1, 11, 12, 3, 1, 11, 13, 3, 1, 11, 14, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, \
+    5, 2, 3, 0, 1, 1, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, \
+    7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 8, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, \
+    12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 8, 0, \
+    4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, \
+    8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, \
+    4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, \
+    12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 8, 0, 4, 0, \
+    8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, \
+    4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, \
+    8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, \
+    0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 4, 0, 8, 0, 4, 2, 8, 0, \
+    5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, \
+    3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, \
+    11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, \
+    2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 3, 2, 1, 1, 7, 0, 8, 0, 4, 0, 8, 0, 4, 2, \
+    8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, \
+    5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, \
+    4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, \
+    5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 3, 2, 1, 1, 7, 0, 8, 0, 4, 0, 8, 0, \
+    4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, \
+    8, 0, 5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, \
+    5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, \
+    2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, \
+    4, 1, 8, 0, 4, 2, 8, 0, 5, 3, 3, 2, 1, 9, 7, 0, 4, 0, 8, 0, 4, 2, 8, 0, \
+    5, 4, 3, 0, 4, 4, 8, 0, 5, 5, 3, 2, 1, 2, 7, 0, 4, 0, 8, 0, 4, 1, 8, 0, \
+    5, 6, 3, 0, 4, 6, 8, 0, 5, 7, 4, 7, 11, 0, 4, 5, 11, 1, 4, 3, 11, 2, 4, 7, \
+    11, 3, 4, 5, 11, 4, 4, 3, 11, 5, 3, 1, 11, 6, 3, 1, 11, 7, 4, 3, 11, 8, 4, 6, \
+    11, 9, 4, 4, 11, 10, 4, 3, 11, 11, 12, 35, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, \
+    5, 2, 3, 0, 1, 1, 1, 9, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, \
+    3, 0, 1, 0, 1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, \
+    1, 2, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, \
+    11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, \
+    3, 0, 1, 1, 1, 9, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, \
+    1, 0, 1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, \
+    1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, \
+    11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, 12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, \
+    2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, \
+    5, 3, 3, 0, 3, 2, 1, 4, 7, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, \
+    1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, \
+    4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, \
+    5, 1, 2, 2, 5, 2, 3, 0, 3, 2, 1, 1, 7, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, \
+    5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, \
+    3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, \
+    11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, \
+    2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, \
+    4, 1, 8, 0, 5, 3, 3, 2, 1, 9, 7, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, \
+    4, 4, 8, 0, 5, 5, 3, 2, 1, 4, 7, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 6, 3, 0, \
+    4, 6, 8, 0, 5, 7, 4, 3, 11, 0, 3, 1, 11, 1, 3, 1, 11, 2, 4, 3, 11, 3, 4, 4, \
+    11, 4, 4, 6, 11, 5, 4, 3, 11, 6, 4, 5, 11, 7, 4, 7, 11, 8, 4, 3, 11, 9, 4, 5, \
+    11, 10, 4, 7, 11, 11, 12, 33, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 2, \
+    1, 9, 7, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 2, 1, 4, 7, 0, 4, 1, 8, 0, \
+    4, 2, 8, 0, 5, 4, 3, 2, 1, 2, 7, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 3, 1, \
+    11, 0, 3, 1, 11, 1, 3, 1, 11, 2, 4, 5, 11, 3, 4, 3, 11, 4, 4, 4, 11, 5, 3, 1, \
+    11, 6, 3, 1, 11, 7, 3, 1, 11, 8, 12, 25, 3, 1, 11, 12, 3, 1, 11, 13, 3, 1, 11, 14, \
+    0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 1, 9, 7, 0, 9, 0, \
+    8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, \
+    4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, \
+    5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, \
+    2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 1, 9, 7, 0, 9, 0, 8, 0, \
+    4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, \
+    8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 2, 1, 18, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, \
+    4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, \
+    12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, \
+    9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 3, 2, 1, 0, 7, 0, 8, 0, \
+    4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, \
+    12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 3, 2, 1, 1, \
+    7, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 1, 4, 7, 0, 9, 0, \
+    8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 1, 18, 1, 2, 7, 0, 9, 0, 8, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, \
+    12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 18, \
+    1, 2, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 3, 3, 2, 1, 9, 7, 0, \
+    4, 0, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 4, 4, 8, 0, 5, 5, 3, 2, 1, 0, 7, 0, \
+    4, 1, 8, 0, 4, 2, 8, 0, 5, 6, 3, 0, 4, 6, 8, 0, 5, 7, 4, 3, 11, 0, 4, 4, \
+    11, 1, 3, 1, 11, 2, 4, 3, 11, 3, 3, 1, 11, 4, 4, 6, 11, 5, 4, 3, 11, 6, 4, 5, \
+    11, 7, 4, 7, 11, 8, 4, 3, 11, 9, 4, 5, 11, 10, 4, 7, 11, 11, 4, 3, 11, 12, 4, 4, \
+    11, 13, 4, 6, 11, 14, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 2, 1, 9, \
+    7, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 2, 1, 0, 7, 0, 4, 1, 8, 0, 4, 2, \
+    8, 0, 5, 4, 3, 2, 1, 2, 7, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, \
+    4, 3, 11, 1, 3, 1, 11, 2, 3, 1, 11, 3, 3, 1, 11, 4, 4, 4, 11, 5, 3, 1, 11, 6, \
+    3, 1, 11, 7, 3, 1, 11, 8, 4, 5, 11, 9, 4, 3, 11, 10, 4, 4, 11, 11, 3, 1, 11, 12, \
+    3, 1, 11, 13, 3, 1, 11, 14, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, \
+    1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, \
+    1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 4, 0, 8, 0, \
+    4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 8, 12, 16, 12, 24, \
+    12, 32, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 1, 9, 7, 0, \
+    9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, \
+    8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 3, 2, 1, 18, 7, 0, 8, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, \
+    12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 1, 1, 9, \
+    7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 1, 4, 7, 0, \
+    9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 3, 2, 1, 18, 7, 0, 8, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, \
+    12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 4, \
+    1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 3, 3, 2, 1, 1, 7, 0, \
+    4, 0, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, 4, 4, 8, 0, 5, 5, 3, 2, 1, 18, 7, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 5, 6, 3, 0, 4, 6, 8, 0, 5, 7, 4, 7, 11, 0, 4, 5, \
+    11, 1, 4, 3, 11, 2, 4, 7, 11, 3, 4, 5, 11, 4, 4, 3, 11, 5, 4, 6, 11, 6, 4, 4, \
+    11, 7, 4, 3, 11, 8, 3, 1, 11, 9, 3, 1, 11, 10, 4, 3, 11, 11, 12, 34, 0, 0, 2, 0, \
+    5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, \
+    8, 0, 4, 2, 8, 0, 5, 3, 3, 0, 1, 0, 1, 4, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, \
+    4, 2, 8, 0, 5, 4, 3, 0, 3, 2, 1, 18, 7, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, \
+    5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, \
+    2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, \
+    4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 2, 1, 0, 7, 0, 4, 1, 8, 0, 4, 2, 8, 0, \
+    5, 4, 3, 0, 4, 4, 8, 0, 5, 5, 3, 2, 1, 18, 7, 0, 4, 0, 8, 0, 4, 1, 8, 0, \
+    5, 6, 3, 0, 4, 6, 8, 0, 5, 7, 4, 6, 11, 0, 4, 3, 11, 1, 4, 5, 11, 2, 3, 1, \
+    11, 3, 4, 3, 11, 4, 4, 5, 11, 5, 4, 7, 11, 6, 4, 3, 11, 7, 4, 4, 11, 8, 4, 7, \
+    11, 9, 4, 3, 11, 10, 3, 1, 11, 11, 4, 6, 11, 12, 4, 3, 11, 13, 4, 4, 11, 14, 0, 0, \
+    2, 0, 5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 2, 1, 1, 7, 0, 4, 0, 8, 0, 4, 2, \
+    8, 0, 5, 3, 3, 2, 1, 0, 7, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 2, 1, 18, \
+    7, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 4, 4, 11, 2, \
+    3, 1, 11, 3, 3, 1, 11, 4, 3, 1, 11, 5, 12, 16, 3, 1, 11, 9, 3, 1, 11, 10, 3, 1, \
+    11, 11, 3, 1, 11, 12, 3, 1, 11, 13, 3, 1, 11, 14, 0, 0, 2, 0, 5, 0, 2, 1, 5, 1, \
+    2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, 8, 0, \
+    5, 3, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, \
+    3, 0, 3, 2, 1, 18, 7, 0, 8, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, \
+    4, 3, 11, 1, 4, 4, 11, 2, 12, 32, 12, 8, 12, 16, 12, 24, 0, 0, 2, 0, 5, 0, 2, 1, \
+    5, 1, 2, 2, 5, 2, 3, 0, 1, 9, 1, 1, 7, 0, 9, 0, 8, 0, 4, 0, 8, 0, 4, 2, \
+    8, 0, 5, 3, 3, 2, 1, 4, 7, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 2, 1, 18, \
+    7, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 3, 0, 4, 4, 8, 0, 5, 6, 3, 0, 4, 5, \
+    8, 0, 5, 7, 3, 1, 11, 0, 4, 3, 11, 1, 4, 6, 11, 2, 4, 5, 11, 3, 4, 3, 11, 4, \
+    4, 6, 11, 5, 4, 7, 11, 6, 4, 3, 11, 7, 4, 4, 11, 8, 4, 7, 11, 9, 4, 3, 11, 10, \
+    3, 1, 11, 11, 4, 5, 11, 12, 4, 3, 11, 13, 4, 4, 11, 14, 0, 0, 2, 0, 5, 0, 2, 1, \
+    5, 1, 2, 2, 5, 2, 3, 2, 1, 1, 7, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, 3, 2, \
+    1, 4, 7, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 2, 1, 18, 7, 0, 4, 0, 8, 0, \
+    4, 1, 8, 0, 5, 5, 3, 1, 11, 0, 3, 1, 11, 1, 4, 4, 11, 2, 4, 5, 11, 3, 4, 3, \
+    11, 4, 3, 1, 11, 5, 4, 5, 11, 6, 4, 3, 11, 7, 4, 4, 11, 8, 3, 1, 11, 9, 3, 1, \
+    11, 10, 3, 1, 11, 11, 3, 1, 11, 12, 3, 1, 11, 13, 3, 1, 11, 14, 0, 0, 2, 0, 5, 0, \
+    2, 1, 5, 1, 2, 2, 5, 2, 3, 0, 1, 4, 1, 0, 7, 0, 9, 0, 8, 0, 4, 1, 8, 0, \
+    4, 2, 8, 0, 5, 3, 3, 2, 1, 9, 7, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 4, 3, 0, \
+    4, 4, 8, 0, 5, 5, 3, 2, 1, 18, 7, 0, 4, 0, 8, 0, 4, 1, 8, 0, 5, 6, 3, 0, \
+    4, 6, 8, 0, 5, 7, 4, 7, 11, 0, 4, 5, 11, 1, 4, 3, 11, 2, 4, 7, 11, 3, 4, 5, \
+    11, 4, 4, 3, 11, 5, 3, 1, 11, 6, 4, 4, 11, 7, 4, 3, 11, 8, 4, 6, 11, 9, 3, 1, \
+    11, 10, 4, 3, 11, 11, 4, 6, 11, 12, 4, 4, 11, 13, 4, 3, 11, 14, 0, 0, 2, 0, 5, 0, \
+    2, 1, 5, 1, 2, 2, 5, 2, 3, 2, 1, 9, 7, 0, 4, 0, 8, 0, 4, 2, 8, 0, 5, 3, \
+    3, 2, 1, 4, 7, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 2, 1, 18, 7, 0, 4, 0, \
+    8, 0, 4, 1, 8, 0, 5, 5, 3, 1, 11, 0, 3, 1, 11, 1, 3, 1, 11, 2, 4, 5, 11, 3, \
+    4, 3, 11, 4, 4, 4, 11, 5, 3, 1, 11, 6, 4, 3, 11, 7, 4, 4, 11, 8, 4, 5, 11, 9, \
+    3, 1, 11, 10, 3, 1, 11, 11, 3, 1, 11, 12, 3, 1, 11, 13, 3, 1, 11, 14, 0, 0, 2, 0, \
+    5, 0, 2, 1, 5, 1, 2, 2, 5, 2, 3, 2, 1, 9, 7, 0, 4, 0, 8, 0, 4, 2, 8, 0, \
+    5, 3, 3, 2, 1, 0, 7, 0, 4, 1, 8, 0, 4, 2, 8, 0, 5, 4, 3, 2, 1, 18, 7, 0, \
+    4, 0, 8, 0, 4, 1, 8, 0, 5, 5, 4, 5, 11, 0, 4, 3, 11, 1, 3, 1, 11, 2, 3, 1, \
+    11, 3, 3, 1, 11, 4, 4, 4, 11, 5, 3, 1, 11, 6, 4, 3, 11, 7, 4, 4, 11, 8, 4, 5, \
+    11, 9, 3, 1, 11, 10, 3, 1, 11, 11, 3, 1, 11, 12, 3, 1, 11, 13, 3, 1, 11, 14, 0, 0, \
+    3, 1, 11, 0, 3, 1, 11, 1, 3, 1, 11, 2, 3, 1, 11, 3, 3, 1, 11, 4, 3, 1, 11, 5, \
+    3, 1, 11, 6, 3, 1, 11, 7, 3, 1, 11, 8, 3, 1, 11, 9, 3, 1, 11, 10, 3, 1, 11, 11, \
+    3, 1, 11, 12, 3, 1, 11, 13, 3, 1, 11, 14, 0, 0, \
+}
+static const DibCase kDibCaseHost[kDibCases] = LSG_DIB_TABLE;
+static const unsigned char kDibCodeHost[kDibCode] = LSG_DIB_CODE;
+static const double kDibConstHost[3] = {0.5, 0.0, 1.0};
+#ifdef __CUDACC__
+__constant__ DibCase kDibCaseDev[kDibCases] = LSG_DIB_TABLE;
+__device__ const unsigned char kDibCodeDev[kDibCode] = LSG_DIB_CODE;
+__constant__ double kDibConstDev[3] = {0.5, 0.0, 1.0};
+#endif
+#undef LSG_DIB_TABLE
+#undef LSG_DIB_CODE
+
+// out: the cell's five triples (en, ws, nb, st, max), left as given when the
+// type has no block
+LSG_MHD void dib_cell(long long c, int type, int side_z, long long N, long long NM, const double* theta,
+                      const double* delta, double (&out)[15])
+{
+#ifdef __CUDA_ARCH__
+    const DibCase* cs = kDibCaseDev;
+    const unsigned char* code = kDibCodeDev;
+    const double* kc = kDibConstDev;
+#else
+    const DibCase* cs = kDibCaseHost;
+    const unsigned char* code = kDibCodeHost;
+    const double* kc = kDibConstHost;
+#endif
+    const int sz = (type == B_Border || type == T_Border) ? side_z : -1;
+    int lo = 0, hi = kDibCases - 1, at = -1;
+    while (lo <= hi) {
+        const int mid = (lo + hi) >> 1;
+        const int cmp = (cs[mid].type != type) ? (cs[mid].type < type ? -1 : 1) : (cs[mid].side_z < sz ? -1 :
+                                                                                   (cs[mid].side_z > sz ? 1 : 0));
+        if (cmp == 0) {
+            at = cs[mid].at;
+            break;
+        }
+        if (cmp < 0) lo = mid + 1;
+        else hi = mid - 1;
+    }
+    if (at < 0) return;
+    double st[8], loc[8];
+    int sp = 0;
+    for (const unsigned char* p = code + at;; p += 2) {
+        const unsigned char op = p[0], a = p[1];
+        switch (op) {
+        case DIB_END: return;
+        case DIB_T: st[sp++] = opnd(theta, c, a, N, NM); break;
+        case DIB_D: st[sp++] = delta[3 * c + a]; break;
+        case DIB_C: st[sp++] = kc[a]; break;
+        case DIB_LD: st[sp++] = loc[a]; break;
+        case DIB_ST: loc[a] = st[--sp]; break;
+        case DIB_ADD: sp--; st[sp - 1] = add(st[sp - 1], st[sp]); break;
+        case DIB_SUB: sp--; st[sp - 1] = sub(st[sp - 1], st[sp]); break;
+        case DIB_MUL: sp--; st[sp - 1] = mul(st[sp - 1], st[sp]); break;
+        case DIB_ABS: st[sp - 1] = fabs(st[sp - 1]); break;
+        case DIB_NEG: st[sp - 1] = -st[sp - 1]; break;
+        case DIB_OUT: out[a] = st[--sp]; break;
+        case DIB_COPY: {
+            const int d = a >> 3, s = a & 7;
+            for (int q = 0; q < 3; q++) out[3 * d + q] = out[3 * s + q];
+            break;
+        }
+        default: return;
+        }
+    }
+}
+
+// inverse distances to the cut surface (calcInvBaseDeltaIb,
+// ls_stag_uniform_mesh.h:3395-3620) across the east, north and top faces:
+// for each face, by its side type, the edge fractions of its two in-plane
+// directions P and Q at the cell and one cell back give 2 / delta next to a
+// closed edge of a fluid face, 3 / (alpha delta) on triangles, and
+// 3 (a1 + a2) / ((a1 (a1 + a2) + a2 a2) delta) on trapezoids.  Returns the
+// two values of the face (P direction, Q direction).
+LSG_MHD void inv_dib_face(int st, const double* alpha, long long c, int cp, long long bp, int cq, long long bq,
+                          const double* d, int dp, int dq, double& outp, double& outq)
+{
+    const double pc = alpha[3 * c + cp], pb = alpha[3 * bp + cp];
+    const double qc = alpha[3 * c + cq], qb = alpha[3 * bq + cq];
+    auto tri = [&](double a, int di, double& o) {
+        if (a > kEq) o = dvd(3.0, mul(a, d[di]));
+    };
+    auto trap = [&](double a1, double a2, int di, double& o) {
+        const double s = add(a1, a2);
+        const double den = add(mul(a1, s), mul(a2, a2));
+        if (den > kEq) o = dvd(mul(3.0, s), mul(den, d[di]));
+    };
+    switch (st) {
+    case kFluidSide:
+        if (pc < kEq || pb < kEq) outq = dvd(2.0, d[dq]);
+        if (qc < kEq || qb < kEq) outp = dvd(2.0, d[dp]);
+        break;
+    case 10: tri(pb, dp, outp); tri(qb, dq, outq); break;       // NE triangle
+    case 1: tri(pb, dp, outp); tri(qc, dq, outq); break;        // NW triangle
+    case 100: tri(pc, dp, outp); tri(qb, dq, outq); break;      // SE triangle
+    case 1000: tri(pc, dp, outp); tri(qc, dq, outq); break;     // SW triangle
+    case 1001: case 110: trap(pb, pc, dp, outp); break;         // W, E trapezoids
+    case 1100: case 11: trap(qb, qc, dq, outq); break;          // S, N trapezoids
+    default: break;
+    }
+}
+
+// inv_dib_ne = (x_N, y_E, z_E), inv_dib_tn = (x_T, y_T, z_N); zero outside
+// the bottom / top borders and the cut cells
+LSG_MHD void inv_dib_cell(long long c, int type, const int* side, const double* alpha, const double* delta,
+                          long long N, long long NM, double* ne, double* tn)
+{
+    double xN = 0, yE = 0, zE = 0, zN = 0, xT = 0, yT = 0;
+    if (type > N_Border && type < kFluid && type != kSolid) {
+        const long long nb = (c < NM) ? c : c - NM;
+        const double* d = delta + 3 * c;
+        inv_dib_face(side[3 * c], alpha, c, 1, nb, 2, c - N, d, 1, 2, yE, zE);        // east face: P = y, Q = z
+        inv_dib_face(side[3 * c + 1], alpha, c, 0, nb, 2, c - 1, d, 0, 2, xN, zN);    // north face: P = x, Q = z
+        inv_dib_face(side[3 * c + 2], alpha, c, 0, c - N, 1, c - 1, d, 0, 1, xT, yT); // top face: P = x, Q = y
+    }
+    ne[3 * c] = xN;
+    ne[3 * c + 1] = yE;
+    ne[3 * c + 2] = zE;
+    tn[3 * c] = xT;
+    tn[3 * c + 1] = yT;
+    tn[3 * c + 2] = zN;
+}
+
+// ---------------------------------------------------------------------------
 // kernels (one thread per cell unless stated; the level-set block is
 // [hs, hf) x [vs, vf) x [0, K))
 // ---------------------------------------------------------------------------
@@ -642,6 +1389,27 @@ __global__ void __launch_bounds__(256) k_mesh_staggered(int N, int M, int K, con
             vz[c] = m;
             iz[c] = inverse_volume(m);
         }
+    }
+}
+// immersed-boundary face areas and inverse distances of every cell
+__global__ void __launch_bounds__(256) k_mesh_ib(int N, int M, int K, const int* __restrict__ type,
+                                                 const int* __restrict__ side, const double* __restrict__ theta,
+                                                 const double* __restrict__ alpha, const double* __restrict__ delta,
+                                                 double* en, double* ws, double* nb, double* st, double* mx,
+                                                 double* ne, double* tn)
+{
+    const long long n = (long long)N * M * K, NM = (long long)N * M;
+    double* arr[5] = {en, ws, nb, st, mx};
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        double o[15];
+#pragma unroll
+        for (int q = 0; q < 15; q++) o[q] = 0.0;
+        dib_cell(c, type[c], side[3 * c + 2], N, NM, theta, delta, o);
+#pragma unroll
+        for (int a = 0; a < 5; a++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) arr[a][3 * c + q] = o[3 * a + q];
+        inv_dib_cell(c, type[c], side, alpha, delta, N, NM, ne, tn);
     }
 }
 #endif  // __CUDACC__

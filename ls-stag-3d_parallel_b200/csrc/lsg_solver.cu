@@ -252,6 +252,7 @@ struct Context {
     struct Mesh {
         int N = 0, M = 0, K = 0;
         DevBuf<double> phi_ls, phi, alpha, theta, delta, vof, inv_vof, svof[3], sinv[3];
+        DevBuf<double> dib[5], inv_dib_ne, inv_dib_tn;   // immersed-boundary areas, inverse distances
         DevBuf<int> side, type, stype[3];
         int osc_sweeps = 0;
         bool have = false;
@@ -2216,6 +2217,9 @@ int lsg_mesh_build(lsg_ctx* h, int N, int M, int K, const double* hstep, const i
         m.sinv[d].alloc(ns[d]);
         m.stype[d].alloc(ns[d]);
     }
+    for (int a = 0; a < 5; a++) m.dib[a].alloc(3 * n);
+    m.inv_dib_ne.alloc(3 * n);
+    m.inv_dib_tn.alloc(3 * n);
     cudaEvent_t e0, e1;
     LSG_CUDA(cudaEventCreate(&e0));
     LSG_CUDA(cudaEventCreate(&e1));
@@ -2281,6 +2285,10 @@ int lsg_mesh_build(lsg_ctx* h, int N, int M, int K, const double* hstep, const i
                                            m.stype[2].p, m.svof[0].p, m.svof[1].p, m.svof[2].p, m.sinv[0].p,
                                            m.sinv[1].p, m.sinv[2].p);
     LSG_CHECK_LAUNCH();
+    mesh::k_mesh_ib<<<gsz, 256, 0, C.s>>>(N, M, K, m.type.p, m.side.p, m.theta.p, m.alpha.p, m.delta.p, m.dib[0].p,
+                                          m.dib[1].p, m.dib[2].p, m.dib[3].p, m.dib[4].p, m.inv_dib_ne.p,
+                                          m.inv_dib_tn.p);
+    LSG_CHECK_LAUNCH();
     LSG_CUDA(cudaEventRecord(e1, C.s));
     LSG_CUDA(cudaStreamSynchronize(C.s));
     float t = 0;
@@ -2332,6 +2340,12 @@ int lsg_mesh_get(lsg_ctx* h, int field, void* out)
         bytes = ns[d] * 8;
         break;
     }
+    case LSG_MESH_DIB_EN: case LSG_MESH_DIB_WS: case LSG_MESH_DIB_NB: case LSG_MESH_DIB_ST: case LSG_MESH_DIB_MAX:
+        src = m.dib[field - LSG_MESH_DIB_EN].p;
+        bytes = 3 * n * 8;
+        break;
+    case LSG_MESH_INV_DIB_NE: src = m.inv_dib_ne.p; bytes = 3 * n * 8; break;
+    case LSG_MESH_INV_DIB_TN: src = m.inv_dib_tn.p; bytes = 3 * n * 8; break;
     default: throw Error{LSG_ERR_ARG, "unknown mesh field"};
     }
     LSG_CUDA(cudaSetDevice(C.device));
@@ -2794,6 +2808,14 @@ int lsg_get_matrix_stencil7(lsg_ctx* h, double* planes)
     LSG_CUDA(cudaStreamSynchronize(C.s));
     return LSG_OK;
     LSG_API_END(h)
+}
+
+int lsg_set_tolerance(lsg_ctx* h, double eps)
+{
+    if (!h) return LSG_ERR_ARG;
+    if (!(eps >= 0.0)) return LSG_ERR_ARG;
+    h->c.opt.eps = eps;
+    return LSG_OK;
 }
 
 int lsg_setup(lsg_ctx* h, const lsg_options* opts)
@@ -3333,6 +3355,17 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
         } else if (which == 6) {
             LSG_REQUIRE(f32 && C.Z32.p, LSG_ERR_STATE, "needs the FP32 multigrid");
             krylov7<float, 0>(C, C.Z32.p, C.V.p, C.w.p, C.scal.p + 48);
+        } else if (which == 8) {
+            LSG_REQUIRE(f32 && C.Z32.p, LSG_ERR_STATE, "needs the FP32 multigrid");
+            const Dims& d = C.d;
+            const long long gx = (d.N + 31) / 32, gy = (d.M + 7) / 8;
+            int zc = 16;
+            while (gx * gy * ((d.K + zc - 1) / zc) > 4096) zc *= 2;
+            const dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)((d.K + zc - 1) / zc));
+            k_krylov7s<float, 0><<<grid, dim3(32, 8), 0, C.s>>>(d.N, d.M, d.K, zc, C.cls0.p, C.dict0.p, C.Z32.p,
+                                                                  C.V.p, C.w.p, C.red.partial.p, C.red.counter.p,
+                                                                  C.scal.p + 48);
+            LSG_CHECK_LAUNCH();
         } else if (which == 7) {
             LSG_REQUIRE(f32 && C.Z32.p, LSG_ERR_STATE, "needs the FP32 multigrid");
             const Dims& d = C.d;
@@ -3348,7 +3381,7 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
     if (which <= 2) bytes = 7.0 * w * n;              // r, lo, dinv, up, ch read; c, ch written
     else if (which == 3) bytes = (3.0 * w + 4.0) * n; // c, r read/write, row class
     else if (which == 5) bytes = (3.0 * w + 4.0) * (double)C.mg.dims[1].n();
-    else if (which == 6 || which == 7) bytes = (4.0 + 8.0 + 8.0 + 4.0) * n;   // FP32 z, v0 read, w written, class
+    else if (which >= 6) bytes = (4.0 + 8.0 + 8.0 + 4.0) * n;   // FP32 z, v0 read, w written, row class
     else bytes = (3.0 * 8.0 + 4.0) * n;               // z, v0 read, w written, row class
     // defined inputs for the timed launches
     if (which == 5) {
@@ -3374,7 +3407,7 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
         LSG_CUDA(cudaMemsetAsync(C.Z.p, 0, n * 8, C.s));
         LSG_CUDA(cudaMemsetAsync(C.V.p, 0, n * 8, C.s));
     }
-    if (which == 6 || which == 7) {
+    if (which >= 6) {
         LSG_CUDA(cudaMemsetAsync(C.Z32.p, 0, n * 4, C.s));
         LSG_CUDA(cudaMemsetAsync(C.V.p, 0, n * 8, C.s));
     }

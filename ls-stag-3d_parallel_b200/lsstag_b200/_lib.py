@@ -59,7 +59,7 @@ EXPORTS = [
     "lsg_helmholtz_flux", "lsg_convective_flux", "lsg_convective_flux_device", "lsg_momentum_rhs_device",
     "lsg_convective_adjoint", "lsg_convective_adjoint_device", "lsg_gradient_transpose",
     "lsg_gradient_transpose_device", "lsg_projection_adjoint_device", "lsg_tecplot_sol_write",
-    "lsg_mesh_build", "lsg_mesh_get", "lsg_mesh_osc_sweeps", "lsg_set_matrix_mesh",
+    "lsg_mesh_build", "lsg_mesh_get", "lsg_mesh_osc_sweeps", "lsg_set_matrix_mesh", "lsg_set_tolerance",
     "lsg_tecplot_sol_async", "lsg_tecplot_wait",
 ]
 
@@ -157,6 +157,7 @@ def load() -> C.CDLL:
     lib.lsg_mesh_get.argtypes = [P, C.c_int, C.c_void_p]
     lib.lsg_mesh_osc_sweeps.argtypes = [P]
     lib.lsg_set_matrix_mesh.argtypes = [P, C.c_longlong, C.c_longlong]
+    lib.lsg_set_tolerance.argtypes = [P, C.c_double]
     lib.lsg_version.restype = C.c_char_p
     _lib = lib
     return lib

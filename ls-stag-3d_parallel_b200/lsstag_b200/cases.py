@@ -114,3 +114,53 @@ def load_flow_case(path: str | None = None):
     par = dict(nu=nu, coef=coef, coef2=coef2, coef_integr=integr, dt=dt, eps=eps, vbase=vbase, max_it=int(maxit),
                restart_mom=int(g["restart_mom_p"][0]), restart_p=int(g["restart_mom_p"][1]))
     return g, tuple(int(v) for v in g["dims"]), par, (g["u_0"], g["v_0"], g["w_0"], g["p_0"])
+
+
+def flow_case_on_device(dims, h, spheres=(), ellipsoids=(), Re: float = 100.0, dt: float = 0.01,
+                        eps: float = 1e-5, restart_p: int = 30, restart_mom: int = 13, max_it: int = 200,
+                        device: int = 0):
+    """(mesh arrays, dims, params, (u0, v0, w0, p0)) of a flow past fixed
+    bodies on a uniform grid, in the form load_flow_case returns them, with
+    the whole mesh built on the GPU from the bodies (lsg_mesh_build) instead of
+    read from a case file.  The rest is the reference's flow task set-up:
+    uniform inflow U_W = V_BASE = 1 (base_task_description.h:313-315),
+    N/S walls u = 1 and W/E u = 1 (flow_task_description.h:79-96), every other
+    boundary velocity 0, immersed-boundary velocities 0 (fixed bodies), the
+    pinned rows N - 1 and N M - 1 (laplace_discrete_operator.h:809-821), the
+    initial state u = 1 on the x-grid cells that are not solid, v = w = p = 0,
+    nu = 1 / Re, the BDF2 coefficients 1.5 / dt and 1 / dt.  The loads inputs
+    of the drag objective (cut-cell list in the reference's order, delta_ib_max,
+    inverse immersed-boundary distances, fcoef = 2) come with it."""
+    from . import mesh as MS
+    from . import solver as S
+    N, M, K = (int(v) for v in dims)
+    s = S.MGFGMRES(device=device)
+    try:
+        s.build_mesh((N, M, K), h, MS.flow_block((N, M, K), h, spheres, ellipsoids),
+                     bodies=MS.bodies_array(spheres, ellipsoids))
+        g = {k: s.mesh_get(k) for k in ("celltype", "xtype", "ytype", "ztype", "side_type", "theta", "alpha",
+                                         "delta", "inv_vof", "vof_x", "vof_y", "vof_z", "inv_mx", "inv_my",
+                                         "inv_mz", "dib_en", "dib_ws", "dib_nb", "dib_st", "inv_dib_ne",
+                                         "inv_dib_tn", "dib_max")}
+    finally:
+        s.close()
+    n = N * M * K
+    g["dims"] = np.array([N, M, K], dtype=np.int32)
+    for k in ("vib", "vibyx", "vibzy"):
+        g[k] = np.zeros(3 * n)
+    g["u_w"] = np.ones(M * K)
+    bc = np.zeros(18)
+    bc[[0, 1, 2, 3]] = 1.0          # U_W, U_E, U_S, U_N
+    g["bc"] = bc
+    g["pins"] = np.array([N - 1, N * M - 1], dtype=np.int32)
+    ct = g["celltype"]
+    g["cells"] = np.nonzero((ct > 0) & (ct < 11111111))[0].astype(np.int32)
+    g["dmax"], g["dne"], g["dtn"] = g["dib_max"], g["inv_dib_ne"], g["inv_dib_tn"]
+    g["fcoef"] = np.array(2.0)
+    par = dict(nu=1.0 / Re, coef=1.5 / dt, coef2=1.0 / dt, coef_integr=1.5 / dt, dt=dt, eps=eps, vbase=1.0,
+               max_it=int(max_it), restart_mom=int(restart_mom), restart_p=int(restart_p))
+    u0 = np.where(g["xtype"] != 0, 1.0, 0.0)
+    v0 = np.zeros(N * (M - 1) * K)
+    w0 = np.zeros(N * M * (K - 1))
+    p0 = np.zeros(n)
+    return g, (N, M, K), par, (u0, v0, w0, p0)

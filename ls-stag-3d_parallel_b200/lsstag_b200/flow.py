@@ -146,9 +146,14 @@ class FlowStepperDevice:
     entry points for the work): no host copies inside a step except the
     iteration counts.  Same arguments as FlowStepper."""
 
-    def __init__(self, geom: dict, dims, par: dict, u0, v0, w0, p0, device: int = 0, pressure_mg_fp32: bool = False):
+    def __init__(self, geom: dict, dims, par: dict, u0, v0, w0, p0, device: int = 0, pressure_mg_fp32: bool = False,
+                 p_rel_tol: float | None = None):
+        """p_rel_tol: stop each pressure solve at p_rel_tol times the norm of
+        its right-hand side (lsg_set_tolerance before the solve) instead of
+        the absolute eps."""
         import ctypes as C
         import torch
+        self.p_rel_tol = p_rel_tol
         self.torch = torch
         self.C = C
         host = FlowStepper(geom, dims, par, u0, v0, w0, p0, device=device, pressure_mg_fp32=pressure_mg_fp32)
@@ -227,9 +232,12 @@ class FlowStepperDevice:
         ck(lib.lsg_projection_rhs_device(pres.ctx.h, self._p(self.us[0]), self._p(self.us[1]), self._p(self.us[2]),
                                          self._p(self.flux_lap), self._p(self.b)))
         self.phi.zero_()
+        psolve = self.host.psolve
+        if self.p_rel_tol is not None:
+            bn = float(torch.linalg.vector_norm(self.b))
+            psolve.ctx.check(lib.lsg_set_tolerance(psolve.ctx.h, self.p_rel_tol * bn))
         torch.cuda.synchronize()
         st = L.Stats()
-        psolve = self.host.psolve
         psolve.ctx.check(lib.lsg_solve_device(psolve.ctx.h, self._p(self.b), self._p(self.phi), C.byref(st)))
         its.append(st.iterations)
         ck(lib.lsg_projection_correct_device(pres.ctx.h, self._p(self.phi), self._p(self.us[0]), self._p(self.us[1]),

@@ -26,6 +26,9 @@ FIELDS = {
     "xtype": (9, np.int32, "x"), "ytype": (10, np.int32, "y"), "ztype": (11, np.int32, "z"),
     "vof_x": (12, np.float64, "x"), "vof_y": (13, np.float64, "y"), "vof_z": (14, np.float64, "z"),
     "inv_mx": (15, np.float64, "x"), "inv_my": (16, np.float64, "y"), "inv_mz": (17, np.float64, "z"),
+    "dib_en": (18, np.float64, "3n"), "dib_ws": (19, np.float64, "3n"), "dib_nb": (20, np.float64, "3n"),
+    "dib_st": (21, np.float64, "3n"), "dib_max": (22, np.float64, "3n"), "inv_dib_ne": (23, np.float64, "3n"),
+    "inv_dib_tn": (24, np.float64, "3n"),
 }
 
 

@@ -12,7 +12,8 @@ Cases: one sphere off the grid lines (16^3), one sphere centred on a cell
 corner so that its poles put phi = 0 exactly on corners (16^3, the
 degenerate case the reference's own sphere task avoids by a half-cell shift),
 a flat box 20x12x10, four seeded spheres (24^3), three seeded rotated
-ellipsoids (64x32x32), and the 128x64x64 sphere flow box.
+ellipsoids (64x32x32), two spheres cutting the bottom and top walls
+(16x16x12), and the 128x64x64 sphere flow box.
 """
 from __future__ import annotations
 
@@ -53,7 +54,12 @@ def cases():
     ell = synth.ellipsoids(5, 3, (8.0, 4.0, 4.0), amin=0.3, amax=0.8)
     ell = [(np.asarray(c, float) + np.array([1.0, 0.0, 0.0]), a, rot) for (c, a, rot) in ell]
     out.append(("ellipsoids3_64x32x32", rr.Case(64, 32, 32, h, h, h, ellipsoids=ell)))
+    # spheres cutting the bottom and top walls: the first and last layers'
+    # own walks (bottom- / topBuildAlpha, bottom- / topTypeOfCell,
+    # tbBuildTheta) and the border cells' face-shape cases
     h = 1.0 / 16
+    out.append(("walls16x16x12", rr.Case(16, 16, 12, h, h, h, spheres=[(0.5 + 0.01, 0.5 - 0.02, 0.03, 0.15),
+                                                                        (0.47, 0.52, 0.74, 0.14)])))
     out.append(("flow_sphere_128x64x64", rr.Case(128, 64, 64, h, h, h,
                                                  spheres=[(2.0, 2.0 + 0.5 * h, 2.0 + 0.5 * h, 0.5)])))
     return out

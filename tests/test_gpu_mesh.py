@@ -3,10 +3,12 @@ reference's own mesh build, array by array and bit for bit
 (tests/golden/mesh_*.npz, dumped by the reference harness's mesh_dump mode:
 level set as evaluated and after the oscillation fix, alpha, face and cell
 types, theta, cell volumes and their inverses, staggered types, volumes and
-inverse volumes).  Cases: spheres off and on the grid lines (a pole on a
-cell corner), four spheres, three rotated ellipsoids, the 128x64x64 flow
-box; together they reach all 106 volume formulas and two oscillation-fix
-chains.  Then the pressure operator assembled from the device mesh
+inverse volumes, immersed-boundary face areas and inverse distances).
+Cases: spheres off and on the grid lines (a pole on a cell corner), four
+spheres, three rotated ellipsoids, two spheres cutting the bottom and top
+walls, the 128x64x64 flow box; together they reach all 106 volume formulas,
+the border cells' face shapes and oscillation-fix chains of up to three
+cells.  Then the pressure operator assembled from the device mesh
 (lsg_set_matrix_mesh) against the reference's own CSR."""
 import glob
 import os
@@ -20,7 +22,8 @@ pytestmark = pytest.mark.gpu
 
 CASES = sorted(glob.glob(os.path.join(GOLDEN, "mesh_*.npz")))
 FIELDS = ["phi_ls", "phi", "alpha", "side_type", "celltype", "theta", "delta", "vof", "inv_vof", "xtype", "ytype",
-          "ztype", "vof_x", "vof_y", "vof_z", "inv_mx", "inv_my", "inv_mz"]
+          "ztype", "vof_x", "vof_y", "vof_z", "inv_mx", "inv_my", "inv_mz", "dib_en", "dib_ws", "dib_nb", "dib_st",
+          "dib_max", "inv_dib_ne", "inv_dib_tn"]
 
 
 def _bodies(g):
@@ -105,3 +108,28 @@ def test_four_spheres_128_operator_from_seed():
     print(f"128^3 four-sphere mesh build: {ms:.3f} ms on the device")
     assert mine.tobytes() == P.tobytes()
     s.close()
+
+
+def test_flow_case_from_bodies_matches_reference_case():
+    """The 128x64x64 sphere flow set up from the sphere alone
+    (cases.flow_case_on_device: mesh built on the GPU) equals the case file
+    made from the reference's own mesh build and equation set-up, array by
+    array and bit for bit, parameters and initial state included."""
+    from lsstag_b200 import cases
+    g_ref, dims_ref, par_ref, st_ref = cases.load_flow_case()
+    h = 1.0 / 16
+    g, dims, par, st = cases.flow_case_on_device((128, 64, 64), (h, h, h),
+                                                 spheres=[(2.0, 2.0 + 0.5 * h, 2.0 + 0.5 * h, 0.5)])
+    assert dims == tuple(dims_ref)
+    bad = [k for k in ("celltype", "xtype", "ytype", "ztype", "side_type", "theta", "alpha", "delta", "inv_vof",
+                       "vof_x", "vof_y", "vof_z", "inv_mx", "inv_my", "inv_mz", "dib_en", "dib_ws", "dib_nb",
+                       "dib_st", "inv_dib_ne", "inv_dib_tn", "vib", "vibyx", "vibzy", "u_w", "bc", "pins", "cells",
+                       "dmax", "dne", "dtn")
+           if np.asarray(g[k]).reshape(-1).astype(np.asarray(g_ref[k]).dtype).tobytes()
+           != np.asarray(g_ref[k]).reshape(-1).tobytes()]
+    assert bad == []
+    assert float(g["fcoef"]) == float(g_ref["fcoef"])
+    for k in ("nu", "coef", "coef2", "coef_integr", "dt", "eps", "vbase", "max_it", "restart_mom", "restart_p"):
+        assert par[k] == par_ref[k], k
+    for a, b in zip(st, st_ref):
+        assert a.tobytes() == np.asarray(b, dtype=np.float64).tobytes()

@@ -192,3 +192,26 @@ def test_mg_fgmres_rbgs(golden, prec):
     ref = g["fgmres_x"]
     assert np.linalg.norm((x - ref)[mask]) <= 1e-7 * np.linalg.norm(ref[mask])
     s.close()
+
+
+def test_set_tolerance_without_new_setup(golden):
+    """lsg_set_tolerance changes the stopping tolerance of the next solves
+    (the reference's equations set solver.eps before a solve): the same
+    context, no new set-up, stops at the new absolute residual, with the
+    reference's iteration count when set to the fixture's eps."""
+    from lsstag_b200 import solver as S
+    _, g = golden
+    eps = float(g["eps"][0])
+    s = _solver(g)
+    s.ctx.check(s.ctx.lib.lsg_set_tolerance(s.ctx.h, 1e3 * eps))
+    x = np.zeros_like(g["b"])
+    it_loose = s.solve(g["b"], x)
+    assert s.norm_r <= 1e3 * eps
+    s.ctx.check(s.ctx.lib.lsg_set_tolerance(s.ctx.h, eps))
+    x = np.zeros_like(g["b"])
+    it = s.solve(g["b"], x)
+    assert it_loose < it and abs(it - int(g["fgmres_it"][0])) <= 1
+    assert s.norm_r <= eps
+    assert s.ctx.lib.lsg_set_tolerance(s.ctx.h, -1.0) < 0
+    assert isinstance(S.Task(), S.Task)
+    s.close()
