@@ -338,7 +338,7 @@ def run_flow_large(args, world, rank, local, pg):
            "max_rel_velocity_diff_fp32_vs_fp64": dv,
            "mesh_and_case_setup_s": setup_s, "operators_setup_s": {k: res[k]["operators_setup_s"] for k in res},
            "cut_cells": int(g["cells"].size),
-           "e2e": {"value": v, "unit": "ms/step", "note": "device-resident state; the mesh is built on the device"}}
+           "e2e": None, "e2e_note": "no host-array arm at this size: state and mesh are built and stay on the device"}
     if rank == 0:
         print(json.dumps(out))
     return 0

@@ -391,6 +391,23 @@ int lsg_gradient_transpose(lsg_ctx* ctx, const double* gx, const double* gy, con
 /* Same on device pointers (the context's device; the call returns when the
    result is written). */
 int lsg_gradient_transpose_device(lsg_ctx* ctx, const double* gx, const double* gy, const double* gz, double* out);
+/* Reverse sweep of the time steps, per momentum equation dir (device
+   pointers on the dir staggered grid, a context holding the geometry and
+   the staggered types): with r = rsol on fluid faces and 0 on solid ones
+   (written to r),
+     fbar += vof r,  ubar += (-2 coef2) vof r,  uprevbar = (coef2 / 2) vof r,
+     histbar = -r,   convbar += 2 r,
+   the cotangents of the forcing, the current and previous velocity, the
+   Adams-Bashforth history and the convective term, given the transposed
+   momentum solve's solution rsol (coef2 = 1/dt): the transpose of the BDF2 /
+   Adams-Bashforth right-hand side of HelmholtzDiscreteEquation
+   (helmholtz_discrete_equation.h:213-254).  No reference counterpart. */
+int lsg_momentum_cotangents_device(lsg_ctx* ctx, int dir, const double* vof, const double* rsol, double coef2,
+                                   double* r, double* fbar, double* ubar, double* uprevbar, double* histbar,
+                                   double* convbar);
+/* out = in on the fluid faces of staggered grid dir, 0 on its solid faces
+   (device pointers; in and out may alias). */
+int lsg_fluid_faces_device(lsg_ctx* ctx, int dir, const double* in, double* out);
 /* lsg_projection_adjoint on device pointers; outputs must not alias inputs. */
 int lsg_projection_adjoint_device(lsg_ctx* ctx, const double* ubar_out, const double* vbar_out,
                                   const double* wbar_out, const double* pbar_out, double coef, double* ubar,
@@ -487,9 +504,10 @@ int lsg_mg_level_tridiag(lsg_ctx* ctx, int level, char dir, double* c, double* d
    r -= A c, 4 the FP64 operator apply fused with a dot product (Krylov),
    5 the residual update of the first coarse level (Galerkin stencil),
    6 the operator apply fused with a dot product on an FP32 preconditioned
-   vector (the Krylov product of the FP32-multigrid solve), 7 the same
-   product by the one-thread-per-cell kernel the solve uses on wide grids,
-   8 the same product with the z planes staged in shared memory.
+   vector (the Krylov product of the FP32-multigrid solve, z planes staged in
+   shared memory), 7 the same product by the one-thread-per-cell kernel the
+   solve uses on wide grids, 8 the same product by the register z-marching
+   kernel (no staging; for comparison).
    Returns the mean duration of one launch and the algorithmic HBM bytes one
    launch moves (compulsory traffic of its inputs and outputs).  Needs
    lsg_setup with the multigrid preconditioner. */

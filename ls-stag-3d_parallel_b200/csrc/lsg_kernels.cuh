@@ -513,97 +513,6 @@ __global__ void __launch_bounds__(256) k_apply27z(int N, int M, int K, int zc, c
     }
 }
 
-// 27-point apply with the x planes staged in shared memory: the CTA owns a
-// 32 x 8 (x, y) tile and marches it along z, keeping the tile's planes z-1,
-// z, z+1 with their one-cell halo (34 x 10 values each) in a ring of three
-// shared buffers.  Each plane is read from global memory once per CTA (two
-// coalesced loads per thread, issued one plane ahead so they overlap the
-// arithmetic of the current plane) instead of nine register gathers per
-// thread; the 27 neighbours of a cell then come from shared memory.  Values
-// outside the grid are staged as 0, like the zero coefficients they meet.
-// Same summation order as k_apply27z (z-1, z, z+1 planes; y, x within).
-template <typename T, int MODE>
-__global__ void __launch_bounds__(256) k_apply27s(int N, int M, int K, int zc, const int* __restrict__ cls,
-                                                   const T* __restrict__ dict28, const T* __restrict__ x,
-                                                   T* __restrict__ r)
-{
-    constexpr int TW = 34, TH = 10, TP = TW * TH;          // tile plane with halo
-    __shared__ T sp[3][TP];
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-    const int ix = blockIdx.x * 32 + threadIdx.x;
-    const int iy = blockIdx.y * 8 + threadIdx.y;
-    const bool own = ix < N && iy < M;
-    const int NM = N * M;                                  // grids hold fewer than 2^31 cells
-    const int z0 = blockIdx.z * zc;
-    const int z1 = min(z0 + zc, K);
-    const int gx0 = blockIdx.x * 32 - 1, gy0 = blockIdx.y * 8 - 1;
-    // the two staging slots of this thread in a tile plane (tid and tid + 256)
-    int goff[2];
-    bool gin[2];
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-        const int e = tid + 256 * q;
-        const int ly = e / TW, lx = e - ly * TW;
-        const int gx = gx0 + lx, gy = gy0 + ly;
-        gin[q] = (e < TP) && gx >= 0 && gx < N && gy >= 0 && gy < M;
-        goff[q] = gx + N * gy;
-    }
-    auto fetch = [&](int z, T (&v)[2]) {
-        const bool zin = z >= 0 && z < K;
-#pragma unroll
-        for (int q = 0; q < 2; q++) v[q] = (zin && gin[q]) ? x[goff[q] + NM * z] : (T)0;
-    };
-    auto stage = [&](int slot, const T (&v)[2]) {
-        sp[slot][tid] = v[0];
-        if (tid + 256 < TP) sp[slot][tid + 256] = v[1];
-    };
-    T v[2];
-    fetch(z0 - 1, v);
-    stage(0, v);
-    fetch(z0, v);
-    stage(1, v);
-    fetch(z0 + 1, v);                                      // plane z0+1, staged at the top of the loop
-    const int col = ix + N * iy;
-    int cn = own ? cls[col + NM * z0] : 0;
-    T rn = (MODE == 0 && own) ? r[col + NM * z0] : (T)0;
-    int sm = 0, sc = 1, sn = 2;                            // ring slots of z-1, z, z+1
-    const int c0 = (threadIdx.y + 1) * TW + threadIdx.x + 1;   // this cell in the tile plane
-    for (int z = z0; z < z1; z++) {
-        stage(sn, v);
-        __syncthreads();
-        if (z + 2 <= z1) fetch(z + 2, v);                  // next plane, in flight during this one
-        const int cl = cn;
-        const T rv = rn;
-        if (own && z + 1 < z1) {
-            cn = cls[col + NM * (z + 1)];
-            if (MODE == 0) rn = r[col + NM * (z + 1)];
-        }
-        if (own) {
-            T a[28];
-            load_row28(dict28 + (size_t)cl * 28, a);
-            T acc = 0;
-            const int slots[3] = {sm, sc, sn};
-#pragma unroll
-            for (int pz = 0; pz < 3; pz++) {
-                const T* pl = sp[slots[pz]];
-#pragma unroll
-                for (int dy = -1; dy <= 1; dy++)
-#pragma unroll
-                    for (int dx = -1; dx <= 1; dx++)
-                        acc += a[pz * 9 + (dy + 1) * 3 + (dx + 1)] * pl[c0 + dy * TW + dx];
-            }
-            const int i = col + NM * z;
-            if (MODE == 0) r[i] = rv - acc;
-            else r[i] = acc;
-        }
-        __syncthreads();                                   // slot sm is overwritten next
-        const int t = sm;
-        sm = sc;
-        sc = sn;
-        sn = t;
-    }
-}
-
 __global__ void k_pad_rows(long long nrows, int w, int wpad, const double* __restrict__ src, double* __restrict__ dst)
 {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nrows * wpad;

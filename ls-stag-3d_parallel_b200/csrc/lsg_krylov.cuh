@@ -136,13 +136,15 @@ __global__ void __launch_bounds__(256, 3) k_krylov7z(int N, int M, int K, int zc
     grid_reduce<1>(s, partial, counter, out);
 }
 
-// The same Krylov products with the z planes staged in shared memory, as
-// k_apply27s does: a CTA marches a 32 x 8 (x, y) tile along z with the tile's
-// planes z-1, z, z+1 and their one-cell halo in a ring of three shared
-// buffers, each plane read once per CTA by coalesced loads issued one plane
-// ahead; the seven neighbours of a cell then come from shared memory.  Row
-// class and v stream from DRAM one step ahead.  Same summation order and
-// neighbour guards as k_krylov7z.
+// The same Krylov products with the z planes staged in shared memory (the
+// kernel the solve launches; k_krylov7z stays for timing comparisons): a CTA
+// marches a 32 x 8 (x, y) tile along z with the tile's planes z-1, z, z+1 and
+// their one-cell halo (34 x 10 values) in a ring of three shared buffers, each
+// plane read once per CTA by two coalesced loads per thread issued one plane
+// ahead; the seven neighbours of a cell then come from shared memory instead
+// of four lateral gathers per cell through L1.  Row class and v stream from
+// DRAM one step ahead.  Values outside the grid are staged as 0.  Same
+// summation order and neighbour guards as k_krylov7z.
 template <typename Tz, int MODE>
 __global__ void __launch_bounds__(256) k_krylov7s(int N, int M, int K, int zc, const int* __restrict__ cls,
                                                    const double* __restrict__ dict, const Tz* __restrict__ z,

@@ -607,4 +607,41 @@ __global__ void k_adjoint_live_rows(long long n, const int* __restrict__ type, c
     }
 }
 
+// Cotangent algebra of one momentum equation in the reverse sweep of the
+// time steps (the transposes of HelmholtzDiscreteEquation::recalcRightMember's
+// BDF2 / Adams-Bashforth terms, helmholtz_discrete_equation.h:213-254), for
+// r = the transposed momentum solve's solution on the fluid faces (0 on solid
+// faces):
+//   fb += vof r          forcing cotangent (forcing enters as vof f)
+//   ub += (-2 c2) vof r  current velocity (the 2 u^n / dt mass term)
+//   upb = (c2 / 2) vof r previous velocity (the -u^{n-1} / (2 dt) term)
+//   pab = -r             Adams-Bashforth history a^{n-1}
+//   cb += 2 r            convective term of this step
+__global__ void k_momentum_cotangents(long long n, const int* __restrict__ stype, const double* __restrict__ vof,
+                                      const double* __restrict__ rsol, double c2, double* __restrict__ r,
+                                      double* __restrict__ fb, double* __restrict__ ub, double* __restrict__ upb,
+                                      double* __restrict__ pab, double* __restrict__ cb)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double rv = (stype[i] != 0) ? rsol[i] : 0.0;
+        const double v = vof[i];
+        r[i] = rv;
+        fb[i] += ((stype[i] != 0) ? v : 0.0) * rv;
+        ub[i] += ((-2.0 * c2) * v) * rv;
+        upb[i] = ((0.5 * c2) * v) * rv;
+        pab[i] = -rv;
+        cb[i] += 2.0 * rv;
+    }
+}
+
+// out = in on the staggered grid's fluid faces, 0 on its solid faces
+__global__ void k_fluid_faces(long long n, const int* __restrict__ stype, const double* __restrict__ in,
+                              double* __restrict__ out)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = (stype[i] != 0) ? in[i] : 0.0;
+}
+
 }  // namespace lsg

@@ -774,14 +774,10 @@ static void apply_resid(const LevelT<T>& lv, const T* x, T* r, cudaStream_t s, i
         else
             k_apply7z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict, x, r);
     } else if (lv.ol.n == 27 && lv.dict28.p) {
-        // shared-memory staged planes; longer z-chunks amortise the two extra
-        // planes (z0 - 1, z1) each CTA stages
-        const int zs = n >= (8LL << 20) ? 16 : (n >= (1LL << 20) ? 8 : 4);
-        const dim3 sg(zg.x, zg.y, (lv.d.K + zs - 1) / zs);
         if (mode == 0)
-            k_apply27s<T, 0><<<sg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zs, lv.cls, lv.dict28.p, x, r);
+            k_apply27z<T, 0><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict28.p, x, r);
         else
-            k_apply27s<T, 1><<<sg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zs, lv.cls, lv.dict28.p, x, r);
+            k_apply27z<T, 1><<<zg, zb, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, zc, lv.cls, lv.dict28.p, x, r);
     } else {
         if (mode == 0)
             k_applyboxd<T, 0><<<grid_for(n, 256), 256, 0, s>>>(lv.d.N, lv.d.M, lv.d.K, lv.ol, lv.cls, lv.dict, x, r);
@@ -1111,9 +1107,11 @@ static void launch_givens(Context& C, int j)
 
 // Low-synchronisation MGS for Arnoldi step j: one pass for V^T w and the new
 // row of V^T V, a triangular correction, one update pass (with ||w||^2).
-// Fine-grid Krylov product fused with one dot (k_krylov7z): MODE 0 w = A z,
-// out = (w, v); MODE 1 w = v - A z, out = ||w||^2.  The z-chunk is sized so the
-// grid has at most 4096 blocks; wider grids use the one-thread-per-cell kernels.
+// Fine-grid Krylov product fused with one dot (k_krylov7s, z planes staged in
+// shared memory): MODE 0 w = A z, out = (w, v); MODE 1 w = v - A z,
+// out = ||w||^2.  The z-chunk is at least 8 planes (each CTA stages two planes
+// beyond its chunk) and doubles until the grid has at most 4096 blocks; wider
+// grids use the one-thread-per-cell kernels.
 template <typename Tz, int MODE>
 static void krylov7(Context& C, const Tz* z, const double* v, double* w, double* out)
 {
@@ -1121,10 +1119,10 @@ static void krylov7(Context& C, const Tz* z, const double* v, double* w, double*
     const long long gx = (d.N + 31) / 32, gy = (d.M + 7) / 8;
     constexpr long long cap = 4096;
     if (gx * gy <= cap) {
-        int zc = zchunk_for(C.n);
+        int zc = std::max(zchunk_for(C.n), 8);
         while (gx * gy * ((d.K + zc - 1) / zc) > cap) zc *= 2;
         const dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)((d.K + zc - 1) / zc));
-        k_krylov7z<Tz, MODE><<<grid, dim3(32, 8), 0, C.s>>>(d.N, d.M, d.K, zc, C.cls0.p, C.dict0.p, z, v, w,
+        k_krylov7s<Tz, MODE><<<grid, dim3(32, 8), 0, C.s>>>(d.N, d.M, d.K, zc, C.cls0.p, C.dict0.p, z, v, w,
                                                              C.red.partial.p, C.red.counter.p, out);
     } else {
         const int gb = grid_for(C.n, 256, Reducer::kMaxBlocks);
@@ -3136,6 +3134,47 @@ int lsg_projection_adjoint_device(lsg_ctx* h, const double* ubar_out, const doub
     LSG_API_END(h)
 }
 
+int lsg_momentum_cotangents_device(lsg_ctx* h, int dir, const double* vof, const double* rsol, double coef2,
+                                   double* r, double* fbar, double* ubar, double* uprevbar, double* histbar,
+                                   double* convbar)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0, 1 or 2");
+    LSG_REQUIRE(vof && rsol && r && fbar && ubar && uprevbar && histbar && convbar, LSG_ERR_ARG, "null field");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const long long ns = (long long)(d.N - (dir == 0)) * (d.M - (dir == 1)) * (d.K - (dir == 2));
+    k_momentum_cotangents<<<grid_for(ns, 256), 256, 0, C.s>>>(ns, C.geo.stype[dir].p, vof, rsol, coef2, r, fbar,
+                                                                ubar, uprevbar, histbar, convbar);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_fluid_faces_device(lsg_ctx* h, int dir, const double* in, double* out)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.geo.have && C.geo.have_stypes, LSG_ERR_STATE,
+                "geometry and staggered types needed (lsg_set_matrix_geometry, lsg_set_staggered_types)");
+    LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0, 1 or 2");
+    LSG_REQUIRE(in && out, LSG_ERR_ARG, "null field");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    const long long ns = (long long)(d.N - (dir == 0)) * (d.M - (dir == 1)) * (d.K - (dir == 2));
+    k_fluid_faces<<<grid_for(ns, 256), 256, 0, C.s>>>(ns, C.geo.stype[dir].p, in, out);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
 int lsg_gradient_transpose_device(lsg_ctx* h, const double* gx, const double* gy, const double* gz, double* out)
 {
     if (!h) return LSG_ERR_ARG;
@@ -3359,10 +3398,11 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
             LSG_REQUIRE(f32 && C.Z32.p, LSG_ERR_STATE, "needs the FP32 multigrid");
             const Dims& d = C.d;
             const long long gx = (d.N + 31) / 32, gy = (d.M + 7) / 8;
-            int zc = 16;
+            LSG_REQUIRE(gx * gy <= 4096, LSG_ERR_STATE, "grid too wide for the z-marching kernel");
+            int zc = zchunk_for(n);
             while (gx * gy * ((d.K + zc - 1) / zc) > 4096) zc *= 2;
             const dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)((d.K + zc - 1) / zc));
-            k_krylov7s<float, 0><<<grid, dim3(32, 8), 0, C.s>>>(d.N, d.M, d.K, zc, C.cls0.p, C.dict0.p, C.Z32.p,
+            k_krylov7z<float, 0><<<grid, dim3(32, 8), 0, C.s>>>(d.N, d.M, d.K, zc, C.cls0.p, C.dict0.p, C.Z32.p,
                                                                   C.V.p, C.w.p, C.red.partial.p, C.red.counter.p,
                                                                   C.scal.p + 48);
             LSG_CHECK_LAUNCH();

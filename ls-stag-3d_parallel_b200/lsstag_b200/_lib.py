@@ -60,6 +60,7 @@ EXPORTS = [
     "lsg_convective_adjoint", "lsg_convective_adjoint_device", "lsg_gradient_transpose",
     "lsg_gradient_transpose_device", "lsg_projection_adjoint_device", "lsg_tecplot_sol_write",
     "lsg_mesh_build", "lsg_mesh_get", "lsg_mesh_osc_sweeps", "lsg_set_matrix_mesh", "lsg_set_tolerance",
+    "lsg_momentum_cotangents_device", "lsg_fluid_faces_device",
     "lsg_tecplot_sol_async", "lsg_tecplot_wait",
 ]
 
@@ -158,6 +159,8 @@ def load() -> C.CDLL:
     lib.lsg_mesh_osc_sweeps.argtypes = [P]
     lib.lsg_set_matrix_mesh.argtypes = [P, C.c_longlong, C.c_longlong]
     lib.lsg_set_tolerance.argtypes = [P, C.c_double]
+    lib.lsg_momentum_cotangents_device.argtypes = [P, C.c_int, P, P, C.c_double] + [P] * 6
+    lib.lsg_fluid_faces_device.argtypes = [P, C.c_int, P, P]
     lib.lsg_version.restype = C.c_char_p
     _lib = lib
     return lib

@@ -711,16 +711,18 @@ class FlowAdjointDevice:
                 cb = [a.clone() for a in pab]
                 rs = []
                 for d in range(3):
-                    g_ = torch.where(self.fluid[d], sb[d], z(sb[d])).contiguous()
-                    rb = z(g_)
-                    self._solve(ops.momT[d], g_, rb)
-                    rb = torch.where(self.fluid[d], rb, z(rb))
-                    fb[d] += self.fvof[d] * rb
-                    ub_in[d] += (-2.0 * co2) * self.vof[d] * rb
-                    upb[d] = (0.5 * co2) * self.vof[d] * rb
-                    pab[d] = -rb
-                    cb[d] += 2.0 * rb
-                    rs.append(rb.contiguous())
+                    # the momentum equation's transposed solve on its fluid
+                    # faces, then the cotangents of its right-hand side's
+                    # terms in one library kernel
+                    g_ = self._empty(self.gsize[d])
+                    pr.ctx.check(lib.lsg_fluid_faces_device(pr.ctx.h, d, self._p(sb[d]), self._p(g_)))
+                    rsol = self._zeros(self.gsize[d])
+                    self._solve(ops.momT[d], g_, rsol)
+                    rb = self._empty(self.gsize[d])
+                    pr.ctx.check(lib.lsg_momentum_cotangents_device(
+                        pr.ctx.h, d, self._p(self.vof[d]), self._p(rsol), co2, self._p(rb), self._p(fb[d]),
+                        self._p(ub_in[d]), self._p(upb[d]), self._p(pab[d]), self._p(cb[d])))
+                    rs.append(rb)
                 uwb.index_add_(0, s["hx_w"], (-rs[0])[s["hx_row"]] * s["hx_c"])
                 gT = self._empty(self.n)
                 self._sync()
@@ -739,8 +741,10 @@ class FlowAdjointDevice:
                     for d in range(3):
                         ub_in[d] += self.gu[d]
                     pb = pb + self.gp
-                ub = [torch.where(f, a, z(a)).contiguous() for f, a in zip(self.fluid, ub_in)]
-                upb = [torch.where(f, a, z(a)) for f, a in zip(self.fluid, upb)]
+                ub = [self._empty(n) for n in self.gsize]
+                for d in range(3):
+                    pr.ctx.check(lib.lsg_fluid_faces_device(pr.ctx.h, d, self._p(ub_in[d]), self._p(ub[d])))
+                    pr.ctx.check(lib.lsg_fluid_faces_device(pr.ctx.h, d, self._p(upb[d]), self._p(upb[d])))
         u0v = self.checkpoints[0][0]
         tmp = [z(a) for a in u0v]
         self._conv_flux_T(pab[2], u0v[0], u0v[2], tmp, uwb)

@@ -26,6 +26,19 @@ def both():
     gpu.close()
 
 
+@pytest.fixture(scope="module")
+def tight():
+    """The GPU operator set with every solve stopped at an absolute residual
+    of 1e-14: a difference quotient of the forward divides the solve error
+    of J by the step, and the pressure operator's smallest singular value
+    (4.6e-5) turns a residual of 1e-12 into pressure errors up to 2e-8."""
+    from lsstag_b200 import flow_adjoint as FA
+    geom, dims, par = load_adjoint_case()
+    gpu = FA.GpuFlowOps(geom, dims, dict(par, eps=1e-14))
+    yield geom, gpu
+    gpu.close()
+
+
 def _rel(a, b):
     return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300)
 
@@ -70,29 +83,33 @@ def test_forward_matches_oracle(both):
         assert _rel(a, b) <= 1e-7
 
 
-def _richardson(f, x0, e, h):
-    """Central difference of f at x0 along e, Richardson-extrapolated from
-    steps h and h/2: (4 D(h/2) - D(h)) / 3 cancels the h^2 term, leaving
-    O(h^4) plus the forward's solver noise divided by h."""
-    d1 = (f(x0 + h * e) - f(x0 - h * e)) / (2 * h)
-    d2 = (f(x0 + 0.5 * h * e) - f(x0 - 0.5 * h * e)) / h
-    return (4.0 * d2 - d1) / 3.0
+def _central(f, x0, e, h):
+    return (f(x0 + h * e) - f(x0 - h * e)) / (2 * h)
 
 
-def test_gradient_matches_oracle_and_differences(both):
+# J is only piecewise smooth: the outflow clamps (SetSolutions::correction)
+# switch where an outflow velocity changes sign, and the discrete gradient is
+# the derivative of the branch taken.  At the point of seed 25 (9 or 10 steps)
+# a clamp switches less than 1e-6 above theta_0 along inflow mode 0: central
+# differences of the oracle's exact-solve forward there miss the adjoint by
+# 2e-5 at every step from 1e-3 to 1e-5, while the backward difference at 1e-6
+# agrees to 2e-8 (9 steps).  The
+# seeds below are points with no switch within the steps used: there central
+# differences of the oracle's forward agree with the oracle's gradient to
+# 4e-10 (seed 29, 4 steps, step 1e-4; seed 30, 10 steps, step 1e-4 for the
+# inflow modes and 3e-2 for the forcing direction).
+
+
+def test_gradient_matches_oracle_and_differences(both, tight):
     """4 steps, checkpoints every 2: the GPU gradient against the oracle's
     (relative 1e-5) and against central differences of the GPU forward for
-    two inflow modes.  The differences are Richardson-extrapolated from
-    steps 1e-3 and 5e-4: a plain step of 1e-3 leaves a truncation error of
-    h^2/6 times the third derivative, 1.8e-4 relative for mode 4
-    (measured), and a step of 1e-6 would divide the forward's solver noise
-    (absolute residual 1e-12 on a pressure operator whose smallest singular
-    value is 4.6e-5) by 1e-6; the exact-solve check at step 1e-6 is the CPU
-    test (tests/test_flow_adjoint.py)."""
+    two inflow modes, on the operator set solved to 1e-14 (fixture tight),
+    step 1e-4; the exact-solve check at step 1e-6 is the CPU test
+    (tests/test_flow_adjoint.py)."""
     from lsstag_b200 import flow_adjoint as FA
     geom, dims, par, gpu, cpu = both
     u0, p0 = [geom["u_0"], geom["v_0"], geom["w_0"]], geom["p_0"]
-    rng = np.random.default_rng(23)
+    rng = np.random.default_rng(29)
     th0 = 0.05 * rng.standard_normal(8)
     f0 = [0.01 * rng.standard_normal(a.size) for a in u0]
     fg, fc = FA.FlowAdjoint(gpu, 4, every=2), FA.FlowAdjoint(cpu, 4, every=2)
@@ -103,12 +120,15 @@ def test_gradient_matches_oracle_and_differences(both):
     assert _rel(gth, cth) <= 1e-5
     for a, b in zip(gf, cf):
         assert _rel(a, b) <= 1e-5
+    _, tgpu = tight
+    ft = FA.FlowAdjoint(tgpu, 4, every=2)
+    _, tth, _ = ft.gradient(th0, f0, u0, p0)
     for k in (0, 4):
         e = np.zeros(8)
         e[k] = 1.0
-        fd = _richardson(lambda th: fg.forward(th, f0, u0, p0), th0, e, 1e-3)
-        print(f"mode {k}: adjoint {gth[k]:.10e}, Richardson difference {fd:.10e}")
-        assert abs(gth[k] - fd) <= 1e-5 * abs(fd), (k, gth[k], fd)
+        fd = _central(lambda th: ft.forward(th, f0, u0, p0), th0, e, 1e-4)
+        print(f"mode {k}: adjoint {tth[k]:.10e}, central difference {fd:.10e}")
+        assert abs(tth[k] - fd) <= 1e-5 * abs(fd), (k, tth[k], fd)
 
 
 def test_device_sweep_matches_host_sweep(both):
@@ -132,16 +152,20 @@ def test_device_sweep_matches_host_sweep(both):
         assert _rel(a, b) <= 1e-8
 
 
-def test_gradient_ten_steps_checkpoints_every_five(both):
+def test_gradient_ten_steps_checkpoints_every_five(both, tight):
     """The device sweep over 10 time steps with checkpoints every 5 (two
-    segments, each recomputed once) against Richardson-extrapolated central
-    differences of the GPU forward: two inflow modes and one random
-    direction of the forcing field, relative 1e-5; and the same sweep with
-    checkpoints every 2 gives the same gradient (the recompute is exact)."""
+    segments, each recomputed once) on the operator set solved to 1e-14,
+    against central differences of the GPU forward: two inflow modes (step
+    1e-4) and one random unit direction of the forcing field (step 3e-2: J
+    moves 1e-4 as much per unit of forcing as per unit of inflow mode and is
+    close to quadratic in the forcing), relative 1e-5; and the same sweep
+    with checkpoints every 2 gives the same gradient (the recompute is
+    exact)."""
     from lsstag_b200 import flow_adjoint as FA
-    geom, dims, par, gpu, cpu = both
+    geom, dims, par, _, cpu = both
+    _, gpu = tight
     u0, p0 = [geom["u_0"], geom["v_0"], geom["w_0"]], geom["p_0"]
-    rng = np.random.default_rng(25)
+    rng = np.random.default_rng(30)
     th0 = 0.05 * rng.standard_normal(8)
     f0 = [0.01 * rng.standard_normal(a.size) for a in u0]
     fa = FA.FlowAdjointDevice(gpu, 10, every=5)
@@ -153,14 +177,14 @@ def test_gradient_ten_steps_checkpoints_every_five(both):
     for k in (0, 4):
         e = np.zeros(8)
         e[k] = 1.0
-        fd = _richardson(lambda th: fwd.forward(th, f0, u0, p0), th0, e, 1e-3)
-        print(f"10 steps, mode {k}: adjoint {gth[k]:.10e}, Richardson difference {fd:.10e}")
+        fd = _central(lambda th: fwd.forward(th, f0, u0, p0), th0, e, 1e-4)
+        print(f"10 steps, mode {k}: adjoint {gth[k]:.10e}, central difference {fd:.10e}")
         assert abs(gth[k] - fd) <= 1e-5 * abs(fd), (k, gth[k], fd)
     # a random forcing direction: d/ds J(f0 + s df) = <dJ/df, df>
     df = [rng.standard_normal(a.size) * (np.asarray(t) != 0) for a, t in zip(u0, cpu.stypes)]
     dfn = np.sqrt(sum(a @ a for a in df))
     df = [a / dfn for a in df]
-    fdf = _richardson(lambda s: fwd.forward(th0, [a + s * b for a, b in zip(f0, df)], u0, p0), 0.0, 1.0, 1e-3)
+    fdf = _central(lambda s: fwd.forward(th0, [a + s * b for a, b in zip(f0, df)], u0, p0), 0.0, 1.0, 3e-2)
     ad = sum(a @ b for a, b in zip(gf, df))
-    print(f"10 steps, forcing direction: adjoint {ad:.10e}, Richardson difference {fdf:.10e}")
+    print(f"10 steps, forcing direction: adjoint {ad:.10e}, central difference {fdf:.10e}")
     assert abs(ad - fdf) <= 1e-5 * abs(fdf), (ad, fdf)
