@@ -510,6 +510,7 @@ def main():
         else:
             s = S.MGFGMRES(device=local, mg_precision=prec, gram_schmidt=gs)
         s.set_planes(P, dims, task)
+        setup_ms = s.setup_times()
         x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
         st = L.Stats()
         def one():
@@ -536,15 +537,21 @@ def main():
         ms_max = barrier_max(pg, ms, local)
         results[name] = {"ms_total": ms_max, "ms_per_solve": ms_max / args.steps, "it": recs[-1][1],
                          "launches": sum(r[2] for r in recs), "bytes": recs[-1][3], "true_res": recs[-1][4],
-                         "norm_r": recs[-1][5], "x": x_dev.cpu().numpy(), "clocks": sampler.summary() if sampler else None}
+                         "norm_r": recs[-1][5], "x": x_dev.cpu().numpy(), "clocks": sampler.summary() if sampler else None,
+                         "setup": {"operator_and_row_dictionary_ms": setup_ms[0], "hierarchy_ms": setup_ms[1]}}
         if name == "fp32":
             # dominant-kernel roofline (finest-level smoother/residual kernels)
             prof = {}
             nv = recs[-1][1]
-            per_solve = {0: 3 * nv, 1: 3 * nv, 2: 3 * nv, 3: 9 * nv, 5: 9 * nv}
+            per_solve = {0: 3 * nv, 1: 3 * nv, 2: 3 * nv, 3: 9 * nv, 5: 9 * nv, 9: 3 * nv, 10: 3 * nv, 11: 3 * nv}
             names = {0: "adlj_xline_fp32", 1: "adlj_yline_fp32", 2: "adlj_zline_fp32", 3: "residual7_fp32",
-                     5: "residual27_level1_fp32"}
-            for k in (0, 1, 2, 3, 5):
+                     5: "residual27_level1_fp32", 9: "adlj_fused_x_fp32", 10: "adlj_fused_y_fp32",
+                     11: "adlj_fused_z_fp32"}
+            # the finest level runs the fused direction steps (ids 9-11) unless
+            # its shape needs the separate residual and line-solve kernels
+            msk, byk = L.C.c_double(0), L.C.c_double(0)
+            fused = s.ctx.lib.lsg_profile_kernel(s.ctx.h, 9, 1, L.C.byref(msk), L.C.byref(byk)) == L.LSG_OK
+            for k in ((9, 10, 11, 5) if fused else (0, 1, 2, 3, 5)):
                 msk = L.C.c_double(0)
                 byk = L.C.c_double(0)
                 s.ctx.check(s.ctx.lib.lsg_profile_kernel(s.ctx.h, k, 20, L.C.byref(msk), L.C.byref(byk)))
@@ -600,6 +607,10 @@ def main():
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": dbytes, "ms_per_launch": dms},
         "kernels": results["prof"],
+        "setup_ms": {k: results[k]["setup"] for k in ("fp32", "fp64")},
+        "adlj_schedule": "fused direction steps on the finest level (residual formed in the line solve)"
+                         if any(k.startswith("adlj_fused") for k in results["prof"]) else
+                         "reference schedule (r -= A c, then the line solve)",
         "e2e": {"value": results["e2e_ms"] / world, "unit": "ms/solve", "h2d_bytes_per_step": 2 * 8 * n,
                 "d2h_bytes_per_step": 8 * n},
         "gpu_launches": results["fp32"]["launches"],

@@ -61,6 +61,8 @@ extern "C" {
 /* lsg_options.smoother */
 #define LSG_SMOOTHER_ADLJ 0   /* reference: damped z,y,x line Jacobi */
 #define LSG_SMOOTHER_RBGS 1   /* red-black point Gauss-Seidel (new variant) */
+#define LSG_ADLJ_FUSED 0      /* ADLJ direction step as one kernel (residual formed in the line solve) */
+#define LSG_ADLJ_REFERENCE 1  /* the reference's schedule: r -= A c, then the line solve */
 
 typedef struct lsg_options {
     int method;          /* LSG_METHOD_*; reference default FGMRES */
@@ -81,7 +83,15 @@ typedef struct lsg_options {
                             LSG_GS_LOWSYNC: the same MGS projections computed as
                             h = (I + L)^{-1} V^T w with L the strictly lower part of
                             V^T V (inverse compact WY form), two passes per step */
-    int reserved[7];
+    int adlj_schedule;   /* LSG_ADLJ_FUSED (default): every ADLJ direction step
+                            ch' = ch + omega T_d^{-1} (b - A ch) as one kernel on
+                            levels with the 7-point stencil (other levels keep
+                            the separate kernels); LSG_ADLJ_REFERENCE: the
+                            reference's r -= A c, c = omega T_d^{-1} r, ch += c
+                            (smoother_adlj_interface.h:66-77) everywhere.  The
+                            two are equal in exact arithmetic (r = b - A ch
+                            before every direction) and differ by rounding. */
+    int reserved[6];
 } lsg_options;
 
 typedef struct lsg_stats {
@@ -423,6 +433,20 @@ int lsg_projection_correct_device(lsg_ctx* ctx, const double* phi, const double*
    ilu_decomposition_sparse_matrix.h:138-148).  Call again after
    lsg_set_matrix_csr to rebuild (rebuildPreconditioner). */
 int lsg_setup(lsg_ctx* ctx, const lsg_options* opts);
+/* Wall times (host clock, ms) of the context's last lsg_set_matrix_* call
+   (operator upload or assembly and the row-dictionary build, both on the
+   device) and of its last lsg_setup (Galerkin products and dictionaries of
+   the coarse levels, line factorisations, coarsest LU, FP32 copies, Krylov
+   buffers).  The reference rebuilds the same in
+   IterativeSolverInterface::set / rebuildPreconditioner
+   (iterative_solver_interface.h:46-70, coarse_grid.h:93-106). */
+int lsg_setup_times(const lsg_ctx* ctx, double* matrix_ms, double* setup_ms);
+/* The row dictionary of multigrid level `level` (0 = the operator itself,
+   needs an operator; 1..lsg_mg_num_levels() need lsg_setup): *nclass
+   distinct rows of *noff coefficients (7, or 27 on Galerkin levels) in
+   first-seen row order, and each row's index into them.  cls (n ints) and
+   dict (nclass * noff doubles) may be null to query the sizes first. */
+int lsg_row_classes(lsg_ctx* ctx, int level, int* cls, double* dict, int* nclass, int* noff);
 
 /* Solve A x = b; x holds the initial guess on entry and the solution on exit
    (IterativeSolverInterface::solve).  Host buffers of N*M*K doubles.
@@ -507,7 +531,9 @@ int lsg_mg_level_tridiag(lsg_ctx* ctx, int level, char dir, double* c, double* d
    vector (the Krylov product of the FP32-multigrid solve, z planes staged in
    shared memory), 7 the same product by the one-thread-per-cell kernel the
    solve uses on wide grids, 8 the same product by the register z-marching
-   kernel (no staging; for comparison).
+   kernel (no staging; for comparison), 9/10/11 the fused ADLJ direction
+   step (residual formed inside the line solve) along x/y/z on the finest
+   level (LSG_ADLJ_FUSED; needs a level that runs it).
    Returns the mean duration of one launch and the algorithmic HBM bytes one
    launch moves (compulsory traffic of its inputs and outputs).  Needs
    lsg_setup with the multigrid preconditioner. */

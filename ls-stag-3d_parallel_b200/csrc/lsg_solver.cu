@@ -11,6 +11,8 @@
 #include <memory>
 #include <thread>
 
+#include "lsg_adlj_fused.cuh"
+#include "lsg_dict.cuh"
 #include "lsg_coarse.cuh"
 #include "lsg_ilu.cuh"
 #include "lsg_krylov.cuh"
@@ -209,6 +211,7 @@ struct Context {
     DevBuf<double> dict0;
     int nclass0 = 0;
     bool have_matrix = false, have_setup = false;
+    double matrix_ms = 0.0, setup_ms = 0.0;   // wall time of the last lsg_set_matrix_* / lsg_setup
     lsg_options opt;
     MGData mg;
     Reducer red;
@@ -294,10 +297,10 @@ __global__ void k_planes_to_rows(int noff, long long n, const double* __restrict
         for (int o = 0; o < noff; o++) rows[i * noff + o] = planes[(size_t)o * n + i];
 }
 
-// Assign every row a class id (first-seen order) and collect the distinct
-// rows; rows are compared bit for bit, so the format is lossless.
-static int build_dict(cudaStream_t s, const double* planes, int noff, long long n, DevBuf<int>& cls,
-                      DevBuf<double>& dict)
+// Host build of the same dictionary (serial first-seen dedup); taken only
+// when the device build meets two different rows with one 64-bit hash.
+static int build_dict_host(cudaStream_t s, const double* planes, int noff, long long n, DevBuf<int>& cls,
+                           DevBuf<double>& dict)
 {
     DevBuf<double> rows;
     rows.alloc((size_t)noff * n);
@@ -358,6 +361,56 @@ static int build_dict(cudaStream_t s, const double* planes, int noff, long long 
     dict.alloc(hd.size());
     LSG_CUDA(cudaMemcpyAsync(cls.p, hc.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
     LSG_CUDA(cudaMemcpyAsync(dict.p, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    LSG_CUDA(cudaStreamSynchronize(s));
+    return nclass;
+}
+
+// Assign every row a class id (first-seen order) and collect the distinct
+// rows; rows are compared bit for bit, so the format is lossless.  Built on
+// the device (lsg_dict.cuh); the result equals the host build's.
+static int build_dict(cudaStream_t s, const double* planes, int noff, long long n, DevBuf<int>& cls,
+                      DevBuf<double>& dict)
+{
+    LSG_REQUIRE(n >= 1 && n < 0x7F7F7F7FLL, LSG_ERR_ARG, "row count out of range for the dictionary build");
+    unsigned long long cap = 1;
+    while (cap < 2ull * (unsigned long long)n) cap <<= 1;
+    int nclass = 0, flag = 0;
+    DevBuf<int> repidx, number, tiles, out;
+    const long long ntiles = (n + kDictTile - 1) / kDictTile;
+    {
+        DevBuf<unsigned long long> keys;
+        DevBuf<int> rep;
+        keys.alloc(cap);
+        rep.alloc(cap);
+        repidx.alloc(n);
+        number.alloc(n);
+        tiles.alloc(ntiles);
+        out.alloc(2);
+        LSG_CUDA(cudaMemsetAsync(keys.p, 0xFF, cap * sizeof(unsigned long long), s));
+        LSG_CUDA(cudaMemsetAsync(rep.p, 0x7F, cap * sizeof(int), s));     // 0x7F7F7F7F > every row index
+        LSG_CUDA(cudaMemsetAsync(out.p, 0, 2 * sizeof(int), s));
+        k_dict_insert<<<grid_for(n, 256), 256, 0, s>>>(noff, n, planes, keys.p, rep.p, cap - 1);
+        LSG_CHECK_LAUNCH();
+        k_dict_lookup<<<grid_for(n, 256), 256, 0, s>>>(noff, n, planes, keys.p, rep.p, cap - 1, repidx.p, number.p,
+                                                       out.p);
+        LSG_CHECK_LAUNCH();
+        k_dict_tile_count<<<(unsigned)ntiles, kDictTile, 0, s>>>(n, number.p, tiles.p);
+        LSG_CHECK_LAUNCH();
+        k_dict_scan_tiles<<<1, kDictTile, 0, s>>>((int)ntiles, tiles.p, out.p + 1);
+        LSG_CHECK_LAUNCH();
+        int h[2];
+        LSG_CUDA(cudaMemcpyAsync(h, out.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        LSG_CUDA(cudaStreamSynchronize(s));
+        flag = h[0];
+        nclass = h[1];
+    }
+    if (flag) return build_dict_host(s, planes, noff, n, cls, dict);
+    dict.alloc((size_t)nclass * noff);
+    cls.alloc(n);
+    k_dict_number<<<(unsigned)ntiles, kDictTile, 0, s>>>(noff, n, planes, tiles.p, number.p, dict.p);
+    LSG_CHECK_LAUNCH();
+    k_dict_classes<<<grid_for(n, 256), 256, 0, s>>>(n, repidx.p, number.p, cls.p);
+    LSG_CHECK_LAUNCH();
     LSG_CUDA(cudaStreamSynchronize(s));
     return nclass;
 }
@@ -850,6 +903,82 @@ static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStr
     LSG_CHECK_LAUNCH();
 }
 
+// y/z-line shapes of the segmented kernels: 8-cell segments (two CTAs of
+// MAXT threads per SM) where a line has at most 32 of them or 12-cell ones
+// would not fit either, else 12-cell segments (FP32 only); 0 = neither.
+template <typename T>
+static int seg_cells(int L)
+{
+    constexpr int MAXT = sizeof(T) == 4 ? 512 : 256;
+    const int S8 = (L + 7) / 8, S12 = (L + 11) / 12;
+    if (8 * S8 <= MAXT && (S8 <= 32 || 8 * S12 > MAXT)) return 8;
+    if (sizeof(T) == 4 && 8 * S12 <= MAXT) return 12;
+    return 0;
+}
+
+// Whether a level with these dimensions and stencil runs the fused ADLJ
+// direction steps: the fine 7-point stencil (offsets b, s, w, p, e, n, t),
+// x-lines of 8-cell segments on P <= 32 lanes (P a power of two), y- and
+// z-lines in the segmented kernel's shapes.
+template <typename T>
+static bool adlj_fused_level(const Dims& g, int noff, const std::vector<int>& off, const lsg_options& o)
+{
+    if (o.smoother != LSG_SMOOTHER_ADLJ || o.adlj_schedule != LSG_ADLJ_FUSED) return false;
+    if (noff != 7 || off.size() < 3 || off[0] != 0 || off[1] != 0 || off[2] != -1) return false;
+    if (g.N < 2 || g.M < 2 || g.K < 2 || g.N % 8) return false;
+    const int P = g.N / 8;
+    if (P > 32 || (P & (P - 1))) return false;
+    return seg_cells<T>(g.M) != 0 && seg_cells<T>(g.K) != 0;
+}
+
+// One fused ADLJ direction step on level lv:  xout = xin + omega T_d^{-1} (b - A xin),
+// b = the level's right-hand side (lv.r, left unchanged).
+template <typename T>
+static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStream_t s, const T* xin, T* xout)
+{
+    const Dims& g = lv.d;
+    const T* b = lv.r.p;
+    const T* dinv = lv.dinv[d].p;
+    if (d == 0) {
+        const int P = g.N / 8;
+        const long long threads = (long long)g.M * g.K * P;
+        k_adlj_fused_xseg<T, 8><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g.N, g.M, g.K, P, lv.cls, lv.dict,
+                                                                                dinv, b, xin, xout, omega);
+    } else {
+        constexpr int MAXT = sizeof(T) == 4 ? 512 : 256;
+        const int L = d == 1 ? g.M : g.K;
+        const long long rows = d == 1 ? g.K : g.M;
+        const int seg = seg_cells<T>(L);
+        const int S = (L + seg - 1) / seg;
+        int W = 8;
+        while (W < 32 && 2 * W * S <= MAXT) W *= 2;
+        const unsigned blocks = (unsigned)((long long)((g.N + W - 1) / W) * rows);
+        const dim3 blk(W, S);
+        const size_t sm = 2 * (size_t)W * S * sizeof(T);
+        const bool zq = d == 2 && zquirk;
+        if (seg == 8) {
+            if (d == 1)
+                k_adlj_fused_seg<T, 1, 8, MAXT, 2><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, false, lv.cls, lv.dict, dinv,
+                                                                           b, xin, xout, omega);
+            else
+                k_adlj_fused_seg<T, 2, 8, MAXT, 2><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls, lv.dict, dinv,
+                                                                           b, xin, xout, omega);
+        } else {
+            if constexpr (sizeof(T) == 4) {
+                if (d == 1)
+                    k_adlj_fused_seg<T, 1, 12, MAXT, 1><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, false, lv.cls, lv.dict,
+                                                                                dinv, b, xin, xout, omega);
+                else
+                    k_adlj_fused_seg<T, 2, 12, MAXT, 1><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls, lv.dict,
+                                                                                dinv, b, xin, xout, omega);
+            } else {
+                throw Error{LSG_ERR_STATE, "no fused line kernel for this line length"};
+            }
+        }
+    }
+    LSG_CHECK_LAUNCH();
+}
+
 // One smoothing sweep of the multi-colour Gauss-Seidel variant on level lv:
 // colours in increasing order (forward) or decreasing order (backward, for
 // the post-smoothing of a symmetric cycle).
@@ -978,12 +1107,26 @@ static void vcycle(Context& C, std::vector<LevelT<T>>& lev, T* ch0 = nullptr)
         k_prolong<T, PZ><<<dim3((f.N + 31) / 32, (f.M + 7) / 8, (f.K + PZ - 1) / PZ), dim3(32, 8), 0, s>>>(
             f.N, f.M, f.K, lev[l + 1].d.N, lev[l + 1].d.M, t.P(0), t.P(1), t.P(2), lev[l + 1].ch.p, chl, lv.c.p);
         LSG_CHECK_LAUNCH();
-        for (int it = 0; it < C.opt.n_post; it++) {
-            const int order[3] = {2, 1, 0};       // SmootherADLJ::solve: z, y, x
-            for (int q = 0; q < 3; q++) {
-                apply_resid<T>(lv, lv.c.p, lv.r.p, s, 0);        // calcRes: r -= A c
-                line_solve<T>(lv, order[q], zq, omega, s, chl);  // c = omega T^-1 r ; ch += c
-            }
+        const int order[3] = {2, 1, 0};           // SmootherADLJ::solve: z, y, x
+        const int steps = 3 * C.opt.n_post;
+        const bool aligned = ((reinterpret_cast<uintptr_t>(chl) | reinterpret_cast<uintptr_t>(lv.c.p) |
+                               reinterpret_cast<uintptr_t>(lv.r.p) | reinterpret_cast<uintptr_t>(lv.cls)) & 15) == 0;
+        if (steps > 0 && aligned && adlj_fused_level<T>(f, lv.ol.n, lv.off, C.opt)) {
+            // the iterate alternates between c and chl (both hold P c_H after the
+            // prolongation); the first buffer is chosen so the last step writes chl
+            T* buf[2] = {chl, lv.c.p};
+            int cur = steps % 2;
+            for (int it = 0; it < C.opt.n_post; it++)
+                for (int q = 0; q < 3; q++) {
+                    adlj_fused_step<T>(lv, order[q], zq, omega, s, buf[cur], buf[cur ^ 1]);
+                    cur ^= 1;
+                }
+        } else {
+            for (int it = 0; it < C.opt.n_post; it++)
+                for (int q = 0; q < 3; q++) {
+                    apply_resid<T>(lv, lv.c.p, lv.r.p, s, 0);        // calcRes: r -= A c
+                    line_solve<T>(lv, order[q], zq, omega, s, chl);  // c = omega T^-1 r ; ch += c
+                }
         }
     }
     C.vcycles++;
@@ -1057,9 +1200,14 @@ static double vcycle_bytes(const MGData& mg, const lsg_options& o, double w)
                 b += (o.n_pre + o.n_post) * (3.0 * w + 4.0) * n;
                 if (o.n_pre > 0) b += (5.0 * w + 4.0) * n;
             } else {
-                // per direction: residual (r rw, c; row class 4 B; the distinct-row
-                // table is L2 resident) + line solve (r, lo, dinv, up, ch read; c, ch written)
-                b += 3.0 * o.n_post * ((3.0 * w + 4.0) + 7.0 * w) * n;
+                // per direction, fused step: b, iterate, dinv read, iterate written,
+                // row class 4 B (the distinct-row table is L2 resident); otherwise
+                // residual (r rw, c; row class) + line solve (r, lo, dinv, up, ch
+                // read; c, ch written)
+                const LevelT<double>& lv = mg.l64[l];
+                const bool fused = w == 4.0 ? adlj_fused_level<float>(mg.dims[l], lv.ol.n, lv.off, o)
+                                            : adlj_fused_level<double>(mg.dims[l], lv.ol.n, lv.off, o);
+                b += 3.0 * o.n_post * (fused ? 4.0 * w + 4.0 : (3.0 * w + 4.0) + 7.0 * w) * n;
             }
         }
     }
@@ -1714,10 +1862,20 @@ int lsg_destroy(lsg_ctx* h)
 
 const char* lsg_last_error(const lsg_ctx* h) { return h ? h->c.err.c_str() : "null context"; }
 
+// Wall time of an entry point into *out (host clock; the entry points below
+// end with a stream synchronisation).
+struct WallTimer {
+    double& out;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    explicit WallTimer(double& o) : out(o) {}
+    ~WallTimer() { out = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); }
+};
+
 static int set_matrix_impl(lsg_ctx* h, int N, int M, int K, const int* rowptr, const int* col, const double* val,
                            long long nnz, bool host)
 {
     Context& C = h->c;
+    WallTimer wt(C.matrix_ms);
     LSG_REQUIRE(N >= 1 && M >= 1 && K >= 1, LSG_ERR_ARG, "grid dimensions must be positive");
     LSG_REQUIRE(rowptr && col && val, LSG_ERR_ARG, "null CSR pointer");
     C.geo.have = C.geo.have_stypes = false;    // geometry of an earlier operator no longer applies
@@ -1792,6 +1950,7 @@ int lsg_set_matrix_stencil7(lsg_ctx* h, int N, int M, int K, const double* plane
     if (!h) return LSG_ERR_ARG;
     LSG_API_BEGIN
     Context& C = h->c;
+    WallTimer wt(C.matrix_ms);
     LSG_REQUIRE(N >= 1 && M >= 1 && K >= 1, LSG_ERR_ARG, "grid dimensions must be positive");
     LSG_REQUIRE(planes, LSG_ERR_ARG, "null planes");
     C.geo.have = C.geo.have_stypes = false;    // geometry of an earlier operator no longer applies
@@ -1874,6 +2033,7 @@ int lsg_set_matrix_geometry(lsg_ctx* h, int N, int M, int K, const int* celltype
     if (!h) return LSG_ERR_ARG;
     LSG_API_BEGIN
     Context& C = h->c;
+    WallTimer wt(C.matrix_ms);
     LSG_REQUIRE(N >= 2 && M >= 2 && K >= 2, LSG_ERR_ARG, "grid dimensions must be >= 2");
     LSG_REQUIRE(celltype && theta && delta && inv_mx && inv_my && inv_mz, LSG_ERR_ARG, "null geometry array");
     const long long n = (long long)N * M * K;
@@ -1911,6 +2071,7 @@ int lsg_set_matrix_helmholtz(lsg_ctx* h, int dir, int N, int M, int K, const int
     if (!h) return LSG_ERR_ARG;
     LSG_API_BEGIN
     Context& C = h->c;
+    WallTimer wt(C.matrix_ms);
     LSG_REQUIRE(dir >= 0 && dir <= 2, LSG_ERR_ARG, "dir must be 0 (x), 1 (y) or 2 (z)");
     LSG_REQUIRE(N >= 3 && M >= 3 && K >= 3, LSG_ERR_ARG, "grid must be at least 3 cells in every direction");
     LSG_REQUIRE(stype && theta && alpha && delta && inv_vof && vof && delta_ib_en && delta_ib_ws && delta_ib_nb &&
@@ -2364,6 +2525,7 @@ int lsg_set_matrix_mesh(lsg_ctx* h, long long pin0, long long pin1)
     if (!h) return LSG_ERR_ARG;
     LSG_API_BEGIN
     Context& C = h->c;
+    WallTimer wt(C.matrix_ms);
     Context::Mesh& m = C.mesh;
     LSG_REQUIRE(m.have, LSG_ERR_STATE, "no mesh built (lsg_mesh_build)");
     const long long n = (long long)m.N * m.M * m.K;
@@ -2821,6 +2983,7 @@ int lsg_setup(lsg_ctx* h, const lsg_options* opts)
     if (!h) return LSG_ERR_ARG;
     LSG_API_BEGIN
     Context& C = h->c;
+    WallTimer wt(C.setup_ms);
     LSG_REQUIRE(C.have_matrix, LSG_ERR_STATE, "lsg_set_matrix_csr must be called before lsg_setup");
     LSG_CUDA(cudaSetDevice(C.device));
     ilu_graph_release(C);                  // work buffers are (re)allocated below
@@ -2834,13 +2997,58 @@ int lsg_setup(lsg_ctx* h, const lsg_options* opts)
                 "smoother not supported");
     LSG_REQUIRE(C.opt.n_pre >= 0 && C.opt.n_post >= 0 && (C.opt.smoother == LSG_SMOOTHER_RBGS || C.opt.n_pre == 0),
                 LSG_ERR_ARG, "pre-smoothing needs the Gauss-Seidel smoother (the ADLJ cycle is V(0, n_post))");
+    LSG_REQUIRE(C.opt.adlj_schedule == LSG_ADLJ_FUSED || C.opt.adlj_schedule == LSG_ADLJ_REFERENCE, LSG_ERR_ARG,
+                "bad ADLJ schedule");
     C.have_setup = false;
     if (C.opt.precond == LSG_PC_MG) mg_setup(C);
     if (C.opt.precond == LSG_PC_ILU0) ilu_setup(C);
     krylov_alloc(C);
+    LSG_CUDA(cudaStreamSynchronize(C.s));
     C.have_setup = true;
     return LSG_OK;
     LSG_API_END(h)
+}
+
+int lsg_row_classes(lsg_ctx* h, int level, int* cls, double* dict, int* nclass, int* noff)
+{
+    if (!h || !nclass || !noff) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.have_matrix, LSG_ERR_STATE, "no operator");
+    const int* c = nullptr;
+    const double* d = nullptr;
+    long long n = 0;
+    if (level == 0) {
+        c = C.cls0.p;
+        d = C.dict0.p;
+        n = C.n;
+        *nclass = C.nclass0;
+        *noff = 7;
+    } else {
+        LSG_REQUIRE(C.have_setup && C.opt.precond == LSG_PC_MG && level >= 1 && level <= C.mg.L, LSG_ERR_ARG,
+                    "level out of range (needs the multigrid setup)");
+        const LevelT<double>& lv = C.mg.l64[level];
+        c = lv.cls;
+        d = lv.dict;
+        n = lv.d.n();
+        *nclass = lv.nclass;
+        *noff = lv.ol.n;
+    }
+    LSG_CUDA(cudaSetDevice(C.device));
+    if (cls) LSG_CUDA(cudaMemcpyAsync(cls, c, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, C.s));
+    if (dict)
+        LSG_CUDA(cudaMemcpyAsync(dict, d, (size_t)*nclass * *noff * sizeof(double), cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_setup_times(const lsg_ctx* h, double* matrix_ms, double* setup_ms)
+{
+    if (!h || !matrix_ms || !setup_ms) return LSG_ERR_ARG;
+    *matrix_ms = h->c.matrix_ms;
+    *setup_ms = h->c.setup_ms;
+    return LSG_OK;
 }
 
 int lsg_solve_device(lsg_ctx* h, const double* b, double* x, lsg_stats* st)
@@ -3413,12 +3621,27 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
                 d.N, d.M, d.K, C.cls0.p, C.dict0.p, C.Z32.p, C.V.p, C.w.p, C.red.partial.p, C.red.counter.p,
                 C.scal.p + 48);
             LSG_CHECK_LAUNCH();
+        } else if (which >= 9 && which <= 11) {
+            const int d = which - 9;
+            const bool zq = C.opt.zline_reference != 0;
+            if (f32) {
+                const LevelT<float>& lv = C.mg.l32[0];
+                LSG_REQUIRE(adlj_fused_level<float>(lv.d, lv.ol.n, lv.off, C.opt), LSG_ERR_STATE,
+                            "the finest level does not run the fused ADLJ steps");
+                adlj_fused_step<float>(lv, d, zq, (float)C.opt.omega, C.s, lv.ch.p, lv.c.p);
+            } else {
+                const LevelT<double>& lv = C.mg.l64[0];
+                LSG_REQUIRE(adlj_fused_level<double>(lv.d, lv.ol.n, lv.off, C.opt), LSG_ERR_STATE,
+                            "the finest level does not run the fused ADLJ steps");
+                adlj_fused_step<double>(lv, d, zq, C.opt.omega, C.s, lv.ch.p, lv.c.p);
+            }
         } else {
             throw Error{LSG_ERR_ARG, "unknown kernel id"};
         }
     };
     double bytes;
-    if (which <= 2) bytes = 7.0 * w * n;              // r, lo, dinv, up, ch read; c, ch written
+    if (which >= 9) bytes = (4.0 * w + 4.0) * n;      // b, iterate, dinv read; iterate written; row class
+    else if (which <= 2) bytes = 7.0 * w * n;         // r, lo, dinv, up, ch read; c, ch written
     else if (which == 3) bytes = (3.0 * w + 4.0) * n; // c, r read/write, row class
     else if (which == 5) bytes = (3.0 * w + 4.0) * (double)C.mg.dims[1].n();
     else if (which >= 6) bytes = (4.0 + 8.0 + 8.0 + 4.0) * n;   // FP32 z, v0 read, w written, row class

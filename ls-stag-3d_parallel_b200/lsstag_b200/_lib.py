@@ -29,13 +29,14 @@ PC_MG, PC_ILU0, PC_NONE = 0, 1, 2
 FP64, FP32 = 0, 1
 SMOOTHER_ADLJ, SMOOTHER_RBGS = 0, 1
 GS_MGS, GS_LOWSYNC = 0, 1
+ADLJ_FUSED, ADLJ_REFERENCE = 0, 1
 
 
 class Options(C.Structure):
     _fields_ = [("method", C.c_int), ("precond", C.c_int), ("mg_precision", C.c_int), ("smoother", C.c_int),
                 ("n_pre", C.c_int), ("n_post", C.c_int), ("max_levels", C.c_int), ("restart", C.c_int),
                 ("max_it", C.c_int), ("zline_reference", C.c_int), ("eps", C.c_double), ("omega", C.c_double),
-                ("gram_schmidt", C.c_int), ("reserved", C.c_int * 7)]
+                ("gram_schmidt", C.c_int), ("adlj_schedule", C.c_int), ("reserved", C.c_int * 6)]
 
 
 class Stats(C.Structure):
@@ -60,6 +61,7 @@ EXPORTS = [
     "lsg_convective_adjoint", "lsg_convective_adjoint_device", "lsg_gradient_transpose",
     "lsg_gradient_transpose_device", "lsg_projection_adjoint_device", "lsg_tecplot_sol_write",
     "lsg_mesh_build", "lsg_mesh_get", "lsg_mesh_osc_sweeps", "lsg_set_matrix_mesh", "lsg_set_tolerance",
+    "lsg_setup_times", "lsg_row_classes",
     "lsg_momentum_cotangents_device", "lsg_fluid_faces_device",
     "lsg_tecplot_sol_async", "lsg_tecplot_wait",
 ]
@@ -159,6 +161,8 @@ def load() -> C.CDLL:
     lib.lsg_mesh_osc_sweeps.argtypes = [P]
     lib.lsg_set_matrix_mesh.argtypes = [P, C.c_longlong, C.c_longlong]
     lib.lsg_set_tolerance.argtypes = [P, C.c_double]
+    lib.lsg_setup_times.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.lsg_row_classes.argtypes = [P, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.lsg_momentum_cotangents_device.argtypes = [P, C.c_int, P, P, C.c_double] + [P] * 6
     lib.lsg_fluid_faces_device.argtypes = [P, C.c_int, P, P]
     lib.lsg_version.restype = C.c_char_p

@@ -57,9 +57,10 @@ class IterativeSolver:
 
     def __init__(self, device: int = 0, mg_precision: int = L.FP64, zline_reference: bool = True,
                  max_levels: int = 0, omega: float = 0.805, gram_schmidt: int = L.GS_MGS,
-                 smoother: int = L.SMOOTHER_ADLJ, n_pre: int = 0):
+                 smoother: int = L.SMOOTHER_ADLJ, n_pre: int = 0, adlj_schedule: int = L.ADLJ_FUSED):
         self.ctx = L.Context(device)
         self.mg_precision = mg_precision
+        self.adlj_schedule = adlj_schedule
         self.smoother = smoother
         self.n_pre = n_pre
         self.gram_schmidt = gram_schmidt
@@ -331,7 +332,8 @@ class IterativeSolver:
                                  n_post=int(self.task.n_post), eps=float(self.eps),
                                  zline_reference=int(self.zline_reference), max_levels=int(self.max_levels),
                                  omega=float(self.omega), gram_schmidt=int(self.gram_schmidt),
-                                 smoother=int(self.smoother), n_pre=int(self.n_pre))
+                                 smoother=int(self.smoother), n_pre=int(self.n_pre),
+                                 adlj_schedule=int(self.adlj_schedule))
 
     def _setup(self):
         o = self.options()
@@ -364,6 +366,26 @@ class IterativeSolver:
         self.ctx.check(self.ctx.lib.lsg_apply(self.ctx.h, L.dptr(np.ascontiguousarray(x, dtype=np.float64)),
                                               L.dptr(y)))
         return y
+
+    def setup_times(self):
+        """(matrix_ms, setup_ms): wall times of the last operator upload or
+        assembly with its row-dictionary build, and of the last setup."""
+        a, b = L.C.c_double(), L.C.c_double()
+        self.ctx.check(self.ctx.lib.lsg_setup_times(self.ctx.h, L.C.byref(a), L.C.byref(b)))
+        return a.value, b.value
+
+    def row_classes(self, level: int = 0):
+        """(cls, dict) of multigrid level `level` (0 = the operator): each
+        row's index into the table of distinct rows (nclass x noff,
+        first-seen order)."""
+        nc, no = L.C.c_int(), L.C.c_int()
+        self.ctx.check(self.ctx.lib.lsg_row_classes(self.ctx.h, level, None, None, L.C.byref(nc), L.C.byref(no)))
+        n = int(np.prod(self.level_dims(level) if level > 0 else self.dims))
+        cls = np.empty(n, dtype=np.int32)
+        dct = np.empty((nc.value, no.value), dtype=np.float64)
+        self.ctx.check(self.ctx.lib.lsg_row_classes(self.ctx.h, level, cls.ctypes.data, dct.ctypes.data,
+                                                    L.C.byref(nc), L.C.byref(no)))
+        return cls, dct
 
     def precondition(self, b: np.ndarray) -> np.ndarray:
         x = np.empty(b.size, dtype=np.float64)
