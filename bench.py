@@ -199,7 +199,7 @@ def run_flow(args, world, rank, local, pg):
     import torch
 
     from lsstag_b200 import cases
-    from lsstag_b200.flow import FlowStepper, FlowStepperDevice
+    from lsstag_b200.flow import FlowStepper, FlowStepperNative
     cfg = {"workload": "flow_sphere_128x64x64_fp64_dt0.01_Re100", "grid": [128, 64, 64],
            "bodies": "sphere D=1 at (2, 2+h/2, 2+h/2) in [0,8]x[0,4]x[0,4]",
            "solvers": "momentum ILU(0)-FGMRES(13), pressure MG-FGMRES(30), absolute eps 1e-5 (reference defaults)",
@@ -222,7 +222,7 @@ def run_flow(args, world, rank, local, pg):
     torch.cuda.set_device(local)
     g, dims, par, (u0, v0, w0, p0) = cases.load_flow_case()
     def timed(fp32):
-        fs = FlowStepperDevice(g, dims, par, u0, v0, w0, p0, device=local, pressure_mg_fp32=fp32)
+        fs = FlowStepperNative(g, dims, par, u0, v0, w0, p0, device=local, pressure_mg_fp32=fp32)
         for _ in range(args.warmup):
             fs.step()
         barrier(pg)
@@ -254,6 +254,7 @@ def run_flow(args, world, rank, local, pg):
     out = {"metric": FLOW_METRIC, "value": ms, "unit": "ms/step", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg, "iterations_last": its[-1],
+           "driver": "native C++ time step (lsg_flow_step; momentum solves on library threads)",
            "fp32_mg_pressure": {"ms_per_step": ms32, "iterations_last": its32[-1],
                                 "max_rel_velocity_diff_vs_fp64": dv,
                                 "note": "pressure MG cycle in FP32 on the operator with negated pins"},
@@ -287,7 +288,7 @@ def run_flow_large(args, world, rank, local, pg):
     import torch
 
     from lsstag_b200 import cases, synth
-    from lsstag_b200.flow import FlowStepperDevice
+    from lsstag_b200.flow import FlowStepperNative
     dims = (512, 256, 256)
     h = 1.0 / 32
     ell = synth.ellipsoids(11, 3, (16.0, 8.0, 8.0), amin=0.3, amax=0.8)
@@ -308,7 +309,7 @@ def run_flow_large(args, world, rank, local, pg):
     res = {}
     for name, fp32 in (("fp32", True), ("fp64", False)):
         t1 = time.perf_counter()
-        fs = FlowStepperDevice(g, dims, par, *st, device=local, pressure_mg_fp32=fp32, p_rel_tol=1e-9)
+        fs = FlowStepperNative(g, dims, par, *st, device=local, pressure_mg_fp32=fp32, p_rel_tol=1e-9)
         init_s = time.perf_counter() - t1
         for _ in range(args.warmup):
             fs.step()

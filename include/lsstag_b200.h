@@ -640,6 +640,59 @@ int lsg_mesh_osc_sweeps(const lsg_ctx* ctx);
 int lsg_set_matrix_mesh(lsg_ctx* ctx, long long pin0, long long pin1);
 
 /* Library build string (version, arch). */
+/* ---- native fixed-body flow time step ------------------------------------
+   TimeSteppingMethodInterface::step (time_stepping_method_interface.h:180-214)
+   for a flow past bodies that do not move, over the contexts the caller set
+   up: the pressure-equation context (geometry from lsg_set_matrix_geometry or
+   lsg_set_matrix_mesh, staggered types from lsg_set_staggered_types: fluxes,
+   convective operator, right-hand sides, projection), the pressure solver
+   context (the same context, or one holding the same operator with its pins
+   negated for the FP32 cycle), and the three momentum solver contexts
+   (lsg_set_matrix_helmholtz + lsg_setup).  One step: pressure source term;
+   per component the convective term, right-hand side with its
+   Adams-Bashforth history and the ILU-FGMRES solve from the current velocity
+   (the three solves concurrently, one host thread and context each);
+   b = D u* + flux and the pressure solve from 0; the projection.  The state
+   lives in device memory owned by the stepper.  The contexts must outlive
+   it and are not used by anyone else during a step. */
+typedef struct lsg_flow lsg_flow;
+typedef struct lsg_flow_desc {
+    int N, M, K;              /* base grid */
+    int device;               /* CUDA device of the contexts */
+    lsg_ctx* pres;            /* pressure equation (geometry, staggered types) */
+    lsg_ctx* psolve;          /* pressure solver (may be pres) */
+    lsg_ctx* mom[3];          /* momentum solvers x, y, z */
+    /* copied at creation; host or device pointers */
+    const int* side_type;     /* 3n, as for lsg_laplace_flux */
+    const double* vib;        /* 3n */
+    const double* u_w;        /* M*K inflow profile */
+    const double* theta;      /* 3n */
+    const double* delta;      /* 3n */
+    const double* vof[3];     /* staggered volumes, x/y/z grids */
+    const double* hflux[3];   /* Helmholtz source terms (lsg_helmholtz_flux) */
+    double bc[18];            /* boundary velocities, as for lsg_helmholtz_flux */
+    double bc_lap[5];         /* U_E, V_S, V_N, W_B, W_T */
+    double coef, coef2, vbase;
+    double p_rel_tol;         /* > 0: each pressure solve to p_rel_tol * ||b||; 0: the context's eps */
+    int zconv_reference;      /* as for lsg_convective_apply */
+    int reserved[7];
+} lsg_flow_desc;
+int lsg_flow_create(const lsg_flow_desc* desc, lsg_flow** out);
+int lsg_flow_destroy(lsg_flow* flow);
+const char* lsg_flow_last_error(const lsg_flow* flow);
+/* The current and previous velocities and the pressure (host or device
+   pointers); prev_aux = the three momentum histories, or null to form them
+   from the state as HelmholtzDiscreteEquation::set does (flux2 + C(u) u). */
+int lsg_flow_set_state(lsg_flow* flow, const double* const u[3], const double* const uprev[3], const double* p,
+                       const double* const prev_aux[3]);
+/* One time step; its[4] = iterations of the x, y, z momentum and pressure
+   solves.  Returns LSG_OK, a solve's LSG_NOT_CONVERGED / LSG_BREAKDOWN
+   (the step completes), or a negative error. */
+int lsg_flow_step(lsg_flow* flow, int its[4]);
+/* Copy the current velocities, pressure and previous velocities out (any
+   pointer may be null; host or device). */
+int lsg_flow_state(lsg_flow* flow, double* const u[3], double* p, double* const uprev[3]);
+
 const char* lsg_version(void);
 
 #ifdef __cplusplus

@@ -46,6 +46,17 @@ class Stats(C.Structure):
                 ("reserved", C.c_int * 4)]
 
 
+class FlowDesc(C.Structure):
+    """lsg_flow_desc (include/lsstag_b200.h)."""
+    _fields_ = [("N", C.c_int), ("M", C.c_int), ("K", C.c_int), ("device", C.c_int),
+                ("pres", C.c_void_p), ("psolve", C.c_void_p), ("mom", C.c_void_p * 3),
+                ("side_type", C.c_void_p), ("vib", C.c_void_p), ("u_w", C.c_void_p), ("theta", C.c_void_p),
+                ("delta", C.c_void_p), ("vof", C.c_void_p * 3), ("hflux", C.c_void_p * 3),
+                ("bc", C.c_double * 18), ("bc_lap", C.c_double * 5), ("coef", C.c_double), ("coef2", C.c_double),
+                ("vbase", C.c_double), ("p_rel_tol", C.c_double), ("zconv_reference", C.c_int),
+                ("reserved", C.c_int * 7)]
+
+
 EXPORTS = [
     "lsg_default_options", "lsg_create", "lsg_destroy", "lsg_last_error", "lsg_set_matrix_csr",
     "lsg_set_matrix_csr_device", "lsg_set_matrix_stencil7", "lsg_setup", "lsg_solve", "lsg_solve_device", "lsg_apply",
@@ -62,6 +73,8 @@ EXPORTS = [
     "lsg_gradient_transpose_device", "lsg_projection_adjoint_device", "lsg_tecplot_sol_write",
     "lsg_mesh_build", "lsg_mesh_get", "lsg_mesh_osc_sweeps", "lsg_set_matrix_mesh", "lsg_set_tolerance",
     "lsg_setup_times", "lsg_row_classes",
+    "lsg_flow_create", "lsg_flow_destroy", "lsg_flow_last_error", "lsg_flow_set_state", "lsg_flow_step",
+    "lsg_flow_state",
     "lsg_momentum_cotangents_device", "lsg_fluid_faces_device",
     "lsg_tecplot_sol_async", "lsg_tecplot_wait",
 ]
@@ -163,6 +176,13 @@ def load() -> C.CDLL:
     lib.lsg_set_tolerance.argtypes = [P, C.c_double]
     lib.lsg_setup_times.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.lsg_row_classes.argtypes = [P, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    lib.lsg_flow_create.argtypes = [C.POINTER(FlowDesc), C.POINTER(C.c_void_p)]
+    lib.lsg_flow_destroy.argtypes = [P]
+    lib.lsg_flow_last_error.argtypes = [P]
+    lib.lsg_flow_last_error.restype = C.c_char_p
+    lib.lsg_flow_set_state.argtypes = [P, C.c_void_p * 3, C.c_void_p * 3, C.c_void_p, C.c_void_p]
+    lib.lsg_flow_step.argtypes = [P, C.POINTER(C.c_int)]
+    lib.lsg_flow_state.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.lsg_momentum_cotangents_device.argtypes = [P, C.c_int, P, P, C.c_double] + [P] * 6
     lib.lsg_fluid_faces_device.argtypes = [P, C.c_int, P, P]
     lib.lsg_version.restype = C.c_char_p

@@ -140,6 +140,84 @@ class FlowStepper:
         self.pres.close()
 
 
+class FlowStepperNative:
+    """The same time step run by the library's native stepper
+    (lsg_flow_create / lsg_flow_step, csrc/lsg_flow.cu): C++ drives every
+    phase, the three momentum solves run concurrently on host threads of the
+    library, the state stays in the stepper's device memory.  Same arguments
+    as FlowStepperDevice."""
+
+    def __init__(self, geom: dict, dims, par: dict, u0, v0, w0, p0, device: int = 0, pressure_mg_fp32: bool = False,
+                 p_rel_tol: float | None = None):
+        import ctypes as C
+
+        from . import _lib as L
+        self.C, self.L = C, L
+        host = FlowStepper(geom, dims, par, u0, v0, w0, p0, device=device, pressure_mg_fp32=pressure_mg_fp32)
+        self.host = host
+        self.dims = host.dims
+        self.ns = [a.size for a in host.u]
+        self.lib = host.pres.ctx.lib
+        f8 = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        self._keep = {"side_type": np.ascontiguousarray(geom["side_type"], dtype=np.int32), "vib": f8(geom["vib"]),
+                      "u_w": f8(geom["u_w"]), "theta": f8(geom["theta"]), "delta": f8(geom["delta"]),
+                      "vof": [f8(geom["vof_" + c]) for c in "xyz"], "hflux": [f8(h) for h in host.hflux]}
+        k = self._keep
+        d = L.FlowDesc()
+        d.N, d.M, d.K = self.dims
+        d.device = device
+        d.pres, d.psolve = host.pres.ctx.h, host.psolve.ctx.h
+        for i in range(3):
+            d.mom[i] = host.mom[i].ctx.h
+            d.vof[i] = k["vof"][i].ctypes.data
+            d.hflux[i] = k["hflux"][i].ctypes.data
+        d.side_type, d.vib, d.u_w = k["side_type"].ctypes.data, k["vib"].ctypes.data, k["u_w"].ctypes.data
+        d.theta, d.delta = k["theta"].ctypes.data, k["delta"].ctypes.data
+        for i in range(18):
+            d.bc[i] = float(host.bc[i])
+        for i in range(5):
+            d.bc_lap[i] = float(host.bc_lap[i])
+        d.coef, d.coef2, d.vbase = float(par["coef"]), float(par["coef2"]), float(par["vbase"])
+        d.p_rel_tol = float(p_rel_tol or 0.0)
+        d.zconv_reference = 1
+        self.desc = d
+        self.h = C.c_void_p()
+        rc = self.lib.lsg_flow_create(C.byref(d), C.byref(self.h))
+        if rc != L.LSG_OK:
+            raise L.LsgError(rc, "lsg_flow_create failed")
+        arr3 = C.c_void_p * 3
+        u = [f8(a) for a in host.u]
+        up = [f8(a) for a in host.uprev]
+        aux = [f8(a) for a in host.prev_aux]
+        self._check(self.lib.lsg_flow_set_state(self.h, arr3(*[a.ctypes.data for a in u]),
+                                                arr3(*[a.ctypes.data for a in up]), f8(host.p).ctypes.data,
+                                                arr3(*[a.ctypes.data for a in aux])))
+
+    def _check(self, rc):
+        if rc < 0:
+            raise self.L.LsgError(rc, self.lib.lsg_flow_last_error(self.h).decode())
+        return rc
+
+    def step(self):
+        its = (self.C.c_int * 4)()
+        self._check(self.lib.lsg_flow_step(self.h, its))
+        return list(its)
+
+    def state(self):
+        """((u, v, w), p) copied to the host."""
+        u = [np.empty(n) for n in self.ns]
+        p = np.empty(int(np.prod(self.dims)))
+        arr3 = self.C.c_void_p * 3
+        self._check(self.lib.lsg_flow_state(self.h, arr3(*[a.ctypes.data for a in u]), p.ctypes.data, None))
+        return u, p
+
+    def close(self):
+        if self.h:
+            self.lib.lsg_flow_destroy(self.h)
+            self.h = self.C.c_void_p()
+        self.host.close()
+
+
 class FlowStepperDevice:
     """The same time step with the state and every intermediate vector in
     device memory (torch CUDA tensors as buffers, the library's *_device
