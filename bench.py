@@ -609,9 +609,10 @@ def main():
                      "algorithmic_bytes_per_launch": dbytes, "ms_per_launch": dms},
         "kernels": results["prof"],
         "setup_ms": {k: results[k]["setup"] for k in ("fp32", "fp64")},
-        "adlj_schedule": "fused direction steps on the finest level (residual formed in the line solve)"
-                         if any(k.startswith("adlj_fused") for k in results["prof"]) else
-                         "reference schedule (r -= A c, then the line solve)",
+        "adlj_schedule": {"fp32": "fused direction steps on the finest level (residual formed in the line solve)"
+                          if any(k.startswith("adlj_fused") for k in results["prof"]) else
+                          "reference schedule (r -= A c, then the line solve)",
+                          "fp64": "reference schedule (r -= A c, then the line solve)"},
         "e2e": {"value": results["e2e_ms"] / world, "unit": "ms/solve", "h2d_bytes_per_step": 2 * 8 * n,
                 "d2h_bytes_per_step": 8 * n},
         "gpu_launches": results["fp32"]["launches"],

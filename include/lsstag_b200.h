@@ -61,8 +61,9 @@ extern "C" {
 /* lsg_options.smoother */
 #define LSG_SMOOTHER_ADLJ 0   /* reference: damped z,y,x line Jacobi */
 #define LSG_SMOOTHER_RBGS 1   /* red-black point Gauss-Seidel (new variant) */
-#define LSG_ADLJ_FUSED 0      /* ADLJ direction step as one kernel (residual formed in the line solve) */
+#define LSG_ADLJ_AUTO 0       /* fused for the FP32 cycle, the reference's schedule for the FP64 cycle */
 #define LSG_ADLJ_REFERENCE 1  /* the reference's schedule: r -= A c, then the line solve */
+#define LSG_ADLJ_FUSED 2      /* ADLJ direction step as one kernel (residual formed in the line solve) */
 
 typedef struct lsg_options {
     int method;          /* LSG_METHOD_*; reference default FGMRES */
@@ -83,14 +84,16 @@ typedef struct lsg_options {
                             LSG_GS_LOWSYNC: the same MGS projections computed as
                             h = (I + L)^{-1} V^T w with L the strictly lower part of
                             V^T V (inverse compact WY form), two passes per step */
-    int adlj_schedule;   /* LSG_ADLJ_FUSED (default): every ADLJ direction step
+    int adlj_schedule;   /* LSG_ADLJ_FUSED: every ADLJ direction step
                             ch' = ch + omega T_d^{-1} (b - A ch) as one kernel on
                             levels with the 7-point stencil (other levels keep
                             the separate kernels); LSG_ADLJ_REFERENCE: the
                             reference's r -= A c, c = omega T_d^{-1} r, ch += c
                             (smoother_adlj_interface.h:66-77) everywhere.  The
                             two are equal in exact arithmetic (r = b - A ch
-                            before every direction) and differ by rounding. */
+                            before every direction) and differ by rounding.
+                            LSG_ADLJ_AUTO (default): fused in the FP32 cycle,
+                            the reference's schedule in the FP64 cycle. */
     int reserved[6];
 } lsg_options;
 
@@ -533,7 +536,8 @@ int lsg_mg_level_tridiag(lsg_ctx* ctx, int level, char dir, double* c, double* d
    solve uses on wide grids, 8 the same product by the register z-marching
    kernel (no staging; for comparison), 9/10/11 the fused ADLJ direction
    step (residual formed inside the line solve) along x/y/z on the finest
-   level (LSG_ADLJ_FUSED; needs a level that runs it).
+   level (needs a level that runs it: LSG_ADLJ_FUSED, or LSG_ADLJ_AUTO in
+   FP32), 12 the x step reading the unpadded 7-value rows (for comparison).
    Returns the mean duration of one launch and the algorithmic HBM bytes one
    launch moves (compulsory traffic of its inputs and outputs).  Needs
    lsg_setup with the multigrid preconditioner. */

@@ -9,7 +9,8 @@
 //     ch' = ch + omega T_d^{-1} (b - A ch)
 // computed here by one kernel per direction: each thread forms the residual
 // of its cells from b, the row class and the current iterate (its line
-// neighbours from registers, the lateral ones through L1/L2), then runs the
+// neighbours from registers, the lateral ones by shuffles or coalesced
+// loads issued with its own), then runs the
 // segmented Thomas recurrence of k_tdma_seg / k_tdma_xseg on it.  The line
 // tridiagonal is read from the operator's own rows (lo, up = the row's
 // couplings along d) and the stored inverse pivots dinv_d (the factorisation
@@ -23,26 +24,47 @@
 // against 10w + 4 for the separate residual update and line solve (r, c read
 // and r written; r, lo, dinv, up, ch read and c, ch written).
 //
-// The operator is the fine 7-point stencil in the row-dictionary form: dict
-// holds each distinct row as (b, s, w, p, e, n, t), cls[i] its index.
+// The operator is the fine 7-point stencil in the row-dictionary form: dict8
+// holds each distinct row as (b, s, w, p, e, n, t, 0), cls[i] its index.
 #pragma once
 
 #include "lsg_kernels.cuh"
 
 namespace lsg {
 
+// Row of the 7-point stencil stored with stride 8 (b, s, w, p, e, n, t, 0):
+// two 16-byte loads in FP32, four in FP64.
+template <typename T>
+__device__ __forceinline__ void load_row8(const T* __restrict__ p, T (&a)[8])
+{
+    if constexpr (sizeof(T) == 4) {
+        const float4 u = __ldg(reinterpret_cast<const float4*>(p));
+        const float4 v = __ldg(reinterpret_cast<const float4*>(p) + 1);
+        a[0] = u.x; a[1] = u.y; a[2] = u.z; a[3] = u.w;
+        a[4] = v.x; a[5] = v.y; a[6] = v.z; a[7] = v.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const double2 u = __ldg(reinterpret_cast<const double2*>(p) + k);
+            a[2 * k] = u.x;
+            a[2 * k + 1] = u.y;
+        }
+    }
+}
+
 // b - A x at flat cell q, every neighbour read from memory (the z-line
 // quirk's right-hand side cell).  Terms summed p, b, s, w, e, n, t.
 template <typename T>
-__device__ __forceinline__ T resid7_at(int N, int M, int K, long long q, const int* __restrict__ cls,
-                                       const T* __restrict__ dict, const T* __restrict__ b,
-                                       const T* __restrict__ x)
+__device__ __forceinline__ T resid7_at8(int N, int M, int K, long long q, const int* __restrict__ cls,
+                                        const T* __restrict__ dict8, const T* __restrict__ b,
+                                        const T* __restrict__ x)
 {
     const int NM = N * M;
     const int qz = (int)(q / NM);
     const int rem = (int)(q - (long long)qz * NM);
     const int qy = rem / N, qx = rem - qy * N;
-    const T* a = dict + (size_t)cls[q] * 7;
+    T a[8];
+    load_row8(dict8 + (size_t)cls[q] * 8, a);
     T acc = a[3] * x[q];
     if (qz > 0) acc += a[0] * x[q - NM];
     if (qy > 0) acc += a[1] * x[q - N];
@@ -53,27 +75,72 @@ __device__ __forceinline__ T resid7_at(int N, int M, int K, long long q, const i
     return b[q] - acc;
 }
 
+// Inclusive scan of the segment maps y = A + B y_in along the segment index
+// (threadIdx.y) of each line (threadIdx.x), Kogge-Stone in shared memory
+// with two buffers: log2(S) steps.  REV scans from the last segment down
+// (backward recurrence).  Returns the composed map of the segments before
+// this one (exclusive), as (A, B).
+template <typename T, bool REV>
+__device__ __forceinline__ void seg_scan(T& a, T& b, T* sA, T* sB)
+{
+    const int W = blockDim.x, S = blockDim.y;
+    const int w = threadIdx.x, sg = threadIdx.y;
+    const int q = REV ? S - 1 - sg : sg;                  // position along the scan
+    int cur = 0;
+    sA[sg * W + w] = a;
+    sB[sg * W + w] = b;
+    __syncthreads();
+    for (int off = 1; off < S; off <<= 1) {
+        T na = a, nb = b;
+        if (q >= off) {
+            const int src = (REV ? sg + off : sg - off) * W + w;
+            const T pa = sA[cur * W * S + src], pb = sB[cur * W * S + src];
+            na = a + b * pa;
+            nb = b * pb;
+        }
+        a = na;
+        b = nb;
+        cur ^= 1;
+        sA[cur * W * S + sg * W + w] = a;
+        sB[cur * W * S + sg * W + w] = b;
+        __syncthreads();
+    }
+    // exclusive: the inclusive result of the neighbour before this segment
+    if (q == 0) {
+        a = 0;
+        b = 1;
+    } else {
+        const int src = (REV ? sg + 1 : sg - 1) * W + w;
+        a = sA[cur * W * S + src];
+        b = sB[cur * W * S + src];
+    }
+}
+
 // y-lines (DIR 1) and z-lines (DIR 2), segmented like k_tdma_seg: a CTA holds
 // W neighbouring lines (consecutive x) split into S = ceil(L/SEG) segments,
-// one thread per (line, segment).  Phase 1 loads the segment's row classes,
-// right-hand sides, pivots and iterate values (plus the iterate just before
-// and after the segment); phase 2 forms the residuals with the lateral
-// neighbours (x +- 1 and the other cross direction); then the affine segment
-// maps of the forward and backward recurrences are chained through shared
-// memory.  zquirk (DIR 2): the first right-hand side of the z-line (x, y) is
-// the residual at cell y*N*K + x, where the reference reads it
+// one thread per (line, segment).  All loads of a thread are issued before
+// any arithmetic: its segment's row classes, right-hand sides, pivots and
+// iterate values, the iterate just before and after the segment, and the
+// iterate of the same cells in the two neighbouring rows of the other cross
+// direction (coalesced along x like the rest); the x-neighbours come from the
+// adjacent lanes by shuffles (width W), the two lanes at the CTA's x edges
+// load theirs.  The residual rows use the stencil rows padded to 8 values
+// (two 16-byte loads in FP32).  The affine segment maps of the forward and
+// backward recurrences are then composed by log-step scans in shared memory.
+// zquirk (DIR 2): the first right-hand side of the z-line (x, y) is the
+// residual at cell y*N*K + x, where the reference reads it
 // (smoother_adlj_z.h:54-58).
 template <typename T, int DIR, int SEG, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
-    k_adlj_fused_seg(int N, int M, int K, bool zquirk, const int* __restrict__ cls, const T* __restrict__ dict,
+    k_adlj_fused_seg(int N, int M, int K, bool zquirk, const int* __restrict__ cls, const T* __restrict__ dict8,
                      const T* __restrict__ dinv, const T* __restrict__ b, const T* __restrict__ xin,
                      T* __restrict__ xout, T omega)
 {
     static_assert(DIR == 1 || DIR == 2, "y- or z-lines");
     extern __shared__ __align__(16) unsigned char fseg_smem[];
     const int W = blockDim.x, S = blockDim.y;
-    T* sA = reinterpret_cast<T*>(fseg_smem);
-    T* sB = sA + W * S;
+    T* sA = reinterpret_cast<T*>(fseg_smem);               // 2 buffers of W*S each
+    T* sB = sA + 2 * W * S;
     const int w = threadIdx.x, sg = threadIdx.y;
     const int NM = N * M;                                  // grids hold fewer than 2^31 cells
     const int L = DIR == 1 ? M : K;
@@ -87,9 +154,11 @@ __global__ void __launch_bounds__(MAXT, MINB)
     const int xs = valid ? x : N - 1;                      // idle lanes load a valid line, store nothing
     const int i0 = DIR == 1 ? row * NM + xs : row * N + xs;
     const int t0 = sg * SEG;
-    // phase 1: the segment's own streams
+    const bool hw = xs > 0, he = xs < N - 1, hm = row > 0, hp = row < rows - 1;
+    const bool edge_w = w == 0 && hw, edge_e = w == W - 1 && he;   // x-neighbour outside the CTA's lines
+    // phase 1: every load of the thread
     int cl[SEG];
-    T rv[SEG], dv[SEG], xc[SEG];
+    T rv[SEG], dv[SEG], xc[SEG], xm[SEG], xq[SEG], xo[SEG];
 #pragma unroll
     for (int u = 0; u < SEG; u++) {
         const int t = min(t0 + u, L - 1);
@@ -98,43 +167,45 @@ __global__ void __launch_bounds__(MAXT, MINB)
         rv[u] = b[i];
         dv[u] = dinv[i];
         xc[u] = xin[i];
+        xm[u] = hm ? xin[i - sb] : (T)0;
+        xq[u] = hp ? xin[i + sb] : (T)0;
+        xo[u] = edge_w ? xin[i - 1] : (edge_e ? xin[i + 1] : (T)0);
     }
     const T xprev = t0 > 0 ? xin[i0 + (t0 - 1) * st] : (T)0;
     const T xnext = t0 + SEG < L ? xin[i0 + (t0 + SEG) * st] : (T)0;
     // phase 2: residuals; lv <- lower coupling, uv <- scaled upper coupling
     T lv[SEG], uv[SEG];
-    const bool hw = xs > 0, he = xs < N - 1, hm = row > 0, hp = row < rows - 1;
 #pragma unroll
     for (int u = 0; u < SEG; u++) {
         const int t = t0 + u;
+        const T fromw = __shfl_up_sync(0xffffffffu, xc[u], 1, W);     // lane w-1: x - 1
+        const T frome = __shfl_down_sync(0xffffffffu, xc[u], 1, W);   // lane w+1: x + 1
+        const T xw = w == 0 ? xo[u] : fromw;
+        const T xe = w == W - 1 ? xo[u] : frome;
         lv[u] = 0;
         uv[u] = 0;
         if (t < L) {
-            const int i = i0 + t * st;
-            const T* a = dict + (size_t)cl[u] * 7;
-            const T xw = hw ? xin[i - 1] : (T)0;
-            const T xe = he ? xin[i + 1] : (T)0;
-            const T xm = hm ? xin[i - sb] : (T)0;
-            const T xq = hp ? xin[i + sb] : (T)0;
+            T a[8];
+            load_row8(dict8 + (size_t)cl[u] * 8, a);
             const T xa = u == 0 ? xprev : xc[u > 0 ? u - 1 : 0];           // previous along the line
             const T xb = u == SEG - 1 ? xnext : xc[u < SEG - 1 ? u + 1 : 0];   // next along the line
             const bool ha = t > 0, hb = t < L - 1;
             T acc = a[3] * xc[u];
             if (DIR == 1) {
-                if (hm) acc += a[0] * xm;                  // z - 1
+                if (hm) acc += a[0] * xm[u];               // z - 1
                 if (ha) acc += a[1] * xa;                  // y - 1
                 if (hw) acc += a[2] * xw;
                 if (he) acc += a[4] * xe;
                 if (hb) acc += a[5] * xb;                  // y + 1
-                if (hp) acc += a[6] * xq;                  // z + 1
+                if (hp) acc += a[6] * xq[u];               // z + 1
                 lv[u] = a[1];
                 uv[u] = a[5] * dv[u];
             } else {
                 if (ha) acc += a[0] * xa;                  // z - 1
-                if (hm) acc += a[1] * xm;                  // y - 1
+                if (hm) acc += a[1] * xm[u];               // y - 1
                 if (hw) acc += a[2] * xw;
                 if (he) acc += a[4] * xe;
-                if (hp) acc += a[5] * xq;                  // y + 1
+                if (hp) acc += a[5] * xq[u];               // y + 1
                 if (hb) acc += a[6] * xb;                  // z + 1
                 lv[u] = a[0];
                 uv[u] = a[6] * dv[u];
@@ -142,7 +213,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
             rv[u] = rv[u] - acc;
         }
     }
-    if (DIR == 2 && zquirk && sg == 0) rv[0] = resid7_at<T>(N, M, K, (long long)row * N * K + xs, cls, dict, b, xin);
+    if (DIR == 2 && zquirk && sg == 0) rv[0] = resid7_at8<T>(N, M, K, (long long)row * N * K + xs, cls, dict8, b, xin);
     // forward, relative to y_in
     T fa = 0, fb = 1;
 #pragma unroll
@@ -160,12 +231,9 @@ __global__ void __launch_bounds__(MAXT, MINB)
         rv[u] = fa;
         lv[u] = fb;
     }
-    sA[sg * W + w] = fa;
-    sB[sg * W + w] = fb;
-    __syncthreads();
-    T yin = 0;
-    for (int q = 0; q < sg; q++) yin = sA[q * W + w] + sB[q * W + w] * yin;
-    __syncthreads();
+    seg_scan<T, false>(fa, fb, sA, sB);
+    const T yin = fa;                                      // y entering this segment (line start: 0)
+    __syncthreads();                                       // the scan buffers are reused below
     // backward, relative to x_out
     T gg = 0, hh = 1;
 #pragma unroll
@@ -184,17 +252,14 @@ __global__ void __launch_bounds__(MAXT, MINB)
         rv[u] = gg;
         lv[u] = hh;
     }
-    sA[sg * W + w] = gg;
-    sB[sg * W + w] = hh;
-    __syncthreads();
-    T xo = 0;
-    for (int q = S - 1; q > sg; q--) xo = sA[q * W + w] + sB[q * W + w] * xo;
+    seg_scan<T, true>(gg, hh, sA, sB);
+    const T xout0 = gg;                                    // x leaving the next segment (line end: 0)
     if (valid) {
 #pragma unroll
         for (int u = 0; u < SEG; u++) {
             const int t = t0 + u;
             if (t < L) {
-                const T cv = omega * (rv[u] + lv[u] * xo);
+                const T cv = omega * (rv[u] + lv[u] * xout0);
                 xout[i0 + t * st] = xc[u] + cv;
             }
         }
@@ -206,8 +271,9 @@ __global__ void __launch_bounds__(MAXT, MINB)
 // loads (b, iterate, pivots, row classes, and the four lateral rows y +- 1,
 // z +- 1 of the iterate), the x neighbours across segment ends come from the
 // adjacent lanes by shuffles, and the segment maps are chained across the P
-// lanes of a line by warp scans.
-template <typename T, int SEG>
+// lanes of a line by warp scans.  ROW8: stencil rows padded to 8 values
+// (vector loads), else the plain 7-value rows.
+template <typename T, int SEG, bool ROW8>
 __global__ void __launch_bounds__(256) k_adlj_fused_xseg(int N, int M, int K, int P, const int* __restrict__ cls,
                                                           const T* __restrict__ dict, const T* __restrict__ dinv,
                                                           const T* __restrict__ b, const T* __restrict__ xin,
@@ -249,7 +315,13 @@ __global__ void __launch_bounds__(256) k_adlj_fused_xseg(int N, int M, int K, in
 #pragma unroll
     for (int u = 0; u < SEG; u++) {
         const int xx = q * SEG + u;
-        const T* a = dict + (size_t)cl[u] * 7;
+        T a[8];
+        if constexpr (ROW8) {
+            load_row8(dict + (size_t)cl[u] * 8, a);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 7; k++) a[k] = dict[(size_t)cl[u] * 7 + k];
+        }
         T acc = a[3] * xc[u];
         if (hzm) acc += a[0] * zm[u];
         if (hym) acc += a[1] * ym[u];

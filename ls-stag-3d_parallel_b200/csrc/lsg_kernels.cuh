@@ -451,7 +451,10 @@ __device__ __forceinline__ void load_row28(const T* __restrict__ p, T (&a)[28])
 
 // 27-point apply (Galerkin levels) marching along z.  dict28 holds each
 // distinct row with stride 28 (the 27 box coefficients in z, y, x order and a
-// zero), so a row is seven (FP32) or fourteen (FP64) vector loads.
+// zero), so a row is seven (FP32) or fourteen (FP64) vector loads.  The row
+// stays in registers from one z-step to the next and a warp reloads only
+// when one of its cells changes class (the kernel is bound by load
+// instructions, and along z most columns keep their class).
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) k_apply27z(int N, int M, int K, int zc, const int* __restrict__ cls,
                                                    const T* __restrict__ dict28, const T* __restrict__ x,
@@ -485,6 +488,9 @@ __global__ void __launch_bounds__(256) k_apply27z(int N, int M, int K, int zc, c
     load_plane(z0, pc);
     int cn = cls[col + NM * z0];
     T rn = (MODE == 0) ? r[col + NM * z0] : (T)0;
+    T a[28];
+    int cprev = -1;
+    const unsigned active = __activemask();               // lanes past the grid edge returned above
     for (int z = z0; z < z1; z++) {
         const int i = col + NM * z;
         const int cl = cn;
@@ -494,8 +500,10 @@ __global__ void __launch_bounds__(256) k_apply27z(int N, int M, int K, int zc, c
             cn = cls[i + NM];
             if (MODE == 0) rn = r[i + NM];
         }
-        T a[28];
-        load_row28(dict28 + (size_t)cl * 28, a);
+        if (__any_sync(active, cl != cprev)) {
+            if (cl != cprev) load_row28(dict28 + (size_t)cl * 28, a);
+            cprev = cl;
+        }
         T acc = 0;
 #pragma unroll
         for (int q = 0; q < 9; q++) acc += a[q] * pm[q];

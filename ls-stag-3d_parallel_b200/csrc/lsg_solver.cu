@@ -153,6 +153,7 @@ struct LevelT {
     const T* dict = nullptr;
     DevBuf<T> dictown;
     DevBuf<T> dict28;         // 27-point levels: rows padded to stride 28 for vector loads
+    DevBuf<T> dict8;          // 7-point levels: rows padded to stride 8 for vector loads
     int nclass = 0;
     DevBuf<T> lo[3], dinv[3], up[3];
     DevBuf<T> gsdinv;         // Gauss-Seidel smoother: 1 / a_ii, 0 below the tiny pivot threshold
@@ -623,6 +624,10 @@ static void mg_setup(Context& C)
     mg.l64[0].cls = C.cls0.p;
     mg.l64[0].dict = C.dict0.p;
     mg.l64[0].nclass = C.nclass0;
+    mg.l64[0].dict8.alloc((size_t)C.nclass0 * 8);
+    k_pad_rows<<<grid_for((long long)C.nclass0 * 8, 256), 256, 0, s>>>(C.nclass0, 7, 8, C.dict0.p,
+                                                                        mg.l64[0].dict8.p);
+    LSG_CHECK_LAUNCH();
     std::vector<int> rad = {1, 1, 1};
     for (int l = 0; l < L; l++) {
         const Dims f = mg.dims[l];
@@ -782,6 +787,12 @@ static void mg_setup(Context& C)
             b.dict = b.dictown.p;
             k_convert<float, double><<<grid_for(nd, 256), 256, 0, s>>>(nd, a.dict, b.dictown.p);
             LSG_CHECK_LAUNCH();
+            if (a.dict8.p) {
+                const long long n8 = (long long)a.nclass * 8;
+                b.dict8.alloc(n8);
+                k_convert<float, double><<<grid_for(n8, 256), 256, 0, s>>>(n8, a.dict8.p, b.dict8.p);
+                LSG_CHECK_LAUNCH();
+            }
             if (a.ol.n == 27) {
                 const long long n28 = (long long)a.nclass * 28;
                 b.dict28.alloc(n28);
@@ -916,6 +927,17 @@ static int seg_cells(int L)
     return 0;
 }
 
+// Segment length of the fused y/z-line kernel (CTAs of 256 threads, at most
+// 32 segments per line): 8 cells, or 12 in FP32 for lines of 257..384
+// cells; 0 = the fused kernel does not take this length.
+template <typename T>
+static int fused_seg_cells(int L)
+{
+    if ((L + 7) / 8 <= 32) return 8;
+    if (sizeof(T) == 4 && (L + 11) / 12 <= 32) return 12;
+    return 0;
+}
+
 // Whether a level with these dimensions and stencil runs the fused ADLJ
 // direction steps: the fine 7-point stencil (offsets b, s, w, p, e, n, t),
 // x-lines of 8-cell segments on P <= 32 lanes (P a power of two), y- and
@@ -923,18 +945,20 @@ static int seg_cells(int L)
 template <typename T>
 static bool adlj_fused_level(const Dims& g, int noff, const std::vector<int>& off, const lsg_options& o)
 {
-    if (o.smoother != LSG_SMOOTHER_ADLJ || o.adlj_schedule != LSG_ADLJ_FUSED) return false;
+    if (o.smoother != LSG_SMOOTHER_ADLJ) return false;
+    if (!(o.adlj_schedule == LSG_ADLJ_FUSED || (o.adlj_schedule == LSG_ADLJ_AUTO && sizeof(T) == 4))) return false;
     if (noff != 7 || off.size() < 3 || off[0] != 0 || off[1] != 0 || off[2] != -1) return false;
     if (g.N < 2 || g.M < 2 || g.K < 2 || g.N % 8) return false;
     const int P = g.N / 8;
     if (P > 32 || (P & (P - 1))) return false;
-    return seg_cells<T>(g.M) != 0 && seg_cells<T>(g.K) != 0;
+    return fused_seg_cells<T>(g.M) != 0 && fused_seg_cells<T>(g.K) != 0;
 }
 
 // One fused ADLJ direction step on level lv:  xout = xin + omega T_d^{-1} (b - A xin),
 // b = the level's right-hand side (lv.r, left unchanged).
 template <typename T>
-static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStream_t s, const T* xin, T* xout)
+static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStream_t s, const T* xin, T* xout,
+                            bool row8 = true)
 {
     const Dims& g = lv.d;
     const T* b = lv.r.p;
@@ -942,35 +966,41 @@ static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cu
     if (d == 0) {
         const int P = g.N / 8;
         const long long threads = (long long)g.M * g.K * P;
-        k_adlj_fused_xseg<T, 8><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g.N, g.M, g.K, P, lv.cls, lv.dict,
-                                                                                dinv, b, xin, xout, omega);
+        if (row8)
+            k_adlj_fused_xseg<T, 8, true><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
+                g.N, g.M, g.K, P, lv.cls, lv.dict8.p, dinv, b, xin, xout, omega);
+        else
+            k_adlj_fused_xseg<T, 8, false><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
+                g.N, g.M, g.K, P, lv.cls, lv.dict, dinv, b, xin, xout, omega);
     } else {
-        constexpr int MAXT = sizeof(T) == 4 ? 512 : 256;
+        constexpr int MAXT = 256;
         const int L = d == 1 ? g.M : g.K;
         const long long rows = d == 1 ? g.K : g.M;
-        const int seg = seg_cells<T>(L);
+        const int seg = fused_seg_cells<T>(L);
         const int S = (L + seg - 1) / seg;
-        int W = 8;
+        int W = 8;                                         // lanes per line row: a divisor of 32
         while (W < 32 && 2 * W * S <= MAXT) W *= 2;
         const unsigned blocks = (unsigned)((long long)((g.N + W - 1) / W) * rows);
         const dim3 blk(W, S);
-        const size_t sm = 2 * (size_t)W * S * sizeof(T);
+        const size_t sm = 4 * (size_t)W * S * sizeof(T);     // two scan buffers of (A, B)
         const bool zq = d == 2 && zquirk;
         if (seg == 8) {
             if (d == 1)
-                k_adlj_fused_seg<T, 1, 8, MAXT, 2><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, false, lv.cls, lv.dict, dinv,
-                                                                           b, xin, xout, omega);
+                k_adlj_fused_seg<T, 1, 8, MAXT, 2><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, false, lv.cls, lv.dict8.p,
+                                                                           dinv, b, xin, xout, omega);
             else
-                k_adlj_fused_seg<T, 2, 8, MAXT, 2><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls, lv.dict, dinv,
-                                                                           b, xin, xout, omega);
+                k_adlj_fused_seg<T, 2, 8, MAXT, 2><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls, lv.dict8.p,
+                                                                           dinv, b, xin, xout, omega);
         } else {
             if constexpr (sizeof(T) == 4) {
                 if (d == 1)
-                    k_adlj_fused_seg<T, 1, 12, MAXT, 1><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, false, lv.cls, lv.dict,
-                                                                                dinv, b, xin, xout, omega);
+                    k_adlj_fused_seg<T, 1, 12, MAXT, 1><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, false, lv.cls,
+                                                                                lv.dict8.p, dinv, b, xin, xout,
+                                                                                omega);
                 else
-                    k_adlj_fused_seg<T, 2, 12, MAXT, 1><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls, lv.dict,
-                                                                                dinv, b, xin, xout, omega);
+                    k_adlj_fused_seg<T, 2, 12, MAXT, 1><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls,
+                                                                                lv.dict8.p, dinv, b, xin, xout,
+                                                                                omega);
             } else {
                 throw Error{LSG_ERR_STATE, "no fused line kernel for this line length"};
             }
@@ -2997,7 +3027,7 @@ int lsg_setup(lsg_ctx* h, const lsg_options* opts)
                 "smoother not supported");
     LSG_REQUIRE(C.opt.n_pre >= 0 && C.opt.n_post >= 0 && (C.opt.smoother == LSG_SMOOTHER_RBGS || C.opt.n_pre == 0),
                 LSG_ERR_ARG, "pre-smoothing needs the Gauss-Seidel smoother (the ADLJ cycle is V(0, n_post))");
-    LSG_REQUIRE(C.opt.adlj_schedule == LSG_ADLJ_FUSED || C.opt.adlj_schedule == LSG_ADLJ_REFERENCE, LSG_ERR_ARG,
+    LSG_REQUIRE(C.opt.adlj_schedule >= LSG_ADLJ_AUTO && C.opt.adlj_schedule <= LSG_ADLJ_FUSED, LSG_ERR_ARG,
                 "bad ADLJ schedule");
     C.have_setup = false;
     if (C.opt.precond == LSG_PC_MG) mg_setup(C);
@@ -3621,19 +3651,20 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
                 d.N, d.M, d.K, C.cls0.p, C.dict0.p, C.Z32.p, C.V.p, C.w.p, C.red.partial.p, C.red.counter.p,
                 C.scal.p + 48);
             LSG_CHECK_LAUNCH();
-        } else if (which >= 9 && which <= 11) {
-            const int d = which - 9;
+        } else if (which >= 9 && which <= 12) {
+            const int d = which == 12 ? 0 : which - 9;
+            const bool row8 = which != 12;
             const bool zq = C.opt.zline_reference != 0;
             if (f32) {
                 const LevelT<float>& lv = C.mg.l32[0];
                 LSG_REQUIRE(adlj_fused_level<float>(lv.d, lv.ol.n, lv.off, C.opt), LSG_ERR_STATE,
                             "the finest level does not run the fused ADLJ steps");
-                adlj_fused_step<float>(lv, d, zq, (float)C.opt.omega, C.s, lv.ch.p, lv.c.p);
+                adlj_fused_step<float>(lv, d, zq, (float)C.opt.omega, C.s, lv.ch.p, lv.c.p, row8);
             } else {
                 const LevelT<double>& lv = C.mg.l64[0];
                 LSG_REQUIRE(adlj_fused_level<double>(lv.d, lv.ol.n, lv.off, C.opt), LSG_ERR_STATE,
                             "the finest level does not run the fused ADLJ steps");
-                adlj_fused_step<double>(lv, d, zq, C.opt.omega, C.s, lv.ch.p, lv.c.p);
+                adlj_fused_step<double>(lv, d, zq, C.opt.omega, C.s, lv.ch.p, lv.c.p, row8);
             }
         } else {
             throw Error{LSG_ERR_ARG, "unknown kernel id"};
@@ -3670,7 +3701,7 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
         LSG_CUDA(cudaMemsetAsync(C.Z.p, 0, n * 8, C.s));
         LSG_CUDA(cudaMemsetAsync(C.V.p, 0, n * 8, C.s));
     }
-    if (which >= 6) {
+    if (which >= 6 && which <= 8) {
         LSG_CUDA(cudaMemsetAsync(C.Z32.p, 0, n * 4, C.s));
         LSG_CUDA(cudaMemsetAsync(C.V.p, 0, n * 8, C.s));
     }

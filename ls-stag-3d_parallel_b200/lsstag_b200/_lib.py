@@ -29,7 +29,7 @@ PC_MG, PC_ILU0, PC_NONE = 0, 1, 2
 FP64, FP32 = 0, 1
 SMOOTHER_ADLJ, SMOOTHER_RBGS = 0, 1
 GS_MGS, GS_LOWSYNC = 0, 1
-ADLJ_FUSED, ADLJ_REFERENCE = 0, 1
+ADLJ_AUTO, ADLJ_REFERENCE, ADLJ_FUSED = 0, 1, 2
 
 
 class Options(C.Structure):

@@ -57,7 +57,7 @@ class IterativeSolver:
 
     def __init__(self, device: int = 0, mg_precision: int = L.FP64, zline_reference: bool = True,
                  max_levels: int = 0, omega: float = 0.805, gram_schmidt: int = L.GS_MGS,
-                 smoother: int = L.SMOOTHER_ADLJ, n_pre: int = 0, adlj_schedule: int = L.ADLJ_FUSED):
+                 smoother: int = L.SMOOTHER_ADLJ, n_pre: int = 0, adlj_schedule: int = L.ADLJ_AUTO):
         self.ctx = L.Context(device)
         self.mg_precision = mg_precision
         self.adlj_schedule = adlj_schedule
