@@ -575,6 +575,27 @@ def main():
             results["e2e_ms"] = barrier_max(pg, sum(e2e), local) / args.steps
         s.close()
         del x_dev
+    # the mixed-precision configuration's point smoother: red-black / 8-colour
+    # Gauss-Seidel V(2,2) with the FP32 cycle, same operator and tolerance
+    rb = None
+    if args.smoother == "adlj":
+        s = S.MGFGMRES(device=local, mg_precision=L.FP32, gram_schmidt=gs, smoother=L.SMOOTHER_RBGS, n_pre=2)
+        s.set_planes(P, dims, S.Task(eps=1e-10 * bnorm, MAX_ITER=200, FGMRES_RESTART_NUM=args.restart, n_post=2))
+        x_dev = torch.zeros(n, dtype=torch.float64, device=dev)
+        st = L.Stats()
+        rms = []
+        for rep in range(2 + 3):
+            x_dev.zero_()
+            torch.cuda.synchronize()
+            s.ctx.check(s.ctx.lib.lsg_solve_device(s.ctx.h, L.C.c_void_p(b_dev.data_ptr()),
+                                                   L.C.c_void_p(x_dev.data_ptr()), L.C.byref(st)))
+            if rep >= 2:
+                rms.append(st.ms)
+        rb = {"ms_per_solve": barrier_max(pg, sum(rms), local) / len(rms), "iterations": st.iterations,
+              "true_rel_residual": st.true_residual / bnorm, "solves_timed": len(rms),
+              "smoother": "red-black (7-point level) / 8-colour (27-point levels) Gauss-Seidel V(2,2), FP32 cycle"}
+        s.close()
+        del x_dev
     x32, x64 = results["fp32"]["x"], results["fp64"]["x"]
     err = float(np.linalg.norm(x32 - x64) / np.linalg.norm(x64))
     peak, peak_kind = measured_hbm_gbs()
@@ -609,6 +630,7 @@ def main():
                      "algorithmic_bytes_per_launch": dbytes, "ms_per_launch": dms},
         "kernels": results["prof"],
         "setup_ms": {k: results[k]["setup"] for k in ("fp32", "fp64")},
+        "rbgs_v22_fp32": rb,
         "adlj_schedule": {"fp32": "fused direction steps on the finest level (residual formed in the line solve)"
                           if any(k.startswith("adlj_fused") for k in results["prof"]) else
                           "reference schedule (r -= A c, then the line solve)",

@@ -53,18 +53,18 @@ __device__ __forceinline__ void load_row8(const T* __restrict__ p, T (&a)[8])
 }
 
 // b - A x at flat cell q, every neighbour read from memory (the z-line
-// quirk's right-hand side cell).  Terms summed p, b, s, w, e, n, t.
-template <typename T>
-__device__ __forceinline__ T resid7_at8(int N, int M, int K, long long q, const int* __restrict__ cls,
-                                        const T* __restrict__ dict8, const T* __restrict__ b,
-                                        const T* __restrict__ x)
+// quirk's right-hand side cell); stencil rows stored with stride RS (7 or 8).
+// Terms summed p, b, s, w, e, n, t.
+template <typename T, int RS>
+__device__ __forceinline__ T resid7_at(int N, int M, int K, long long q, const int* __restrict__ cls,
+                                       const T* __restrict__ dict, const T* __restrict__ b,
+                                       const T* __restrict__ x)
 {
     const int NM = N * M;
     const int qz = (int)(q / NM);
     const int rem = (int)(q - (long long)qz * NM);
     const int qy = rem / N, qx = rem - qy * N;
-    T a[8];
-    load_row8(dict8 + (size_t)cls[q] * 8, a);
+    const T* a = dict + (size_t)cls[q] * RS;
     T acc = a[3] * x[q];
     if (qz > 0) acc += a[0] * x[q - NM];
     if (qy > 0) acc += a[1] * x[q - N];
@@ -118,25 +118,25 @@ __device__ __forceinline__ void seg_scan(T& a, T& b, T* sA, T* sB)
 
 // y-lines (DIR 1) and z-lines (DIR 2), segmented like k_tdma_seg: a CTA holds
 // W neighbouring lines (consecutive x) split into S = ceil(L/SEG) segments,
-// one thread per (line, segment).  All loads of a thread are issued before
-// any arithmetic: its segment's row classes, right-hand sides, pivots and
-// iterate values, the iterate just before and after the segment, and the
-// iterate of the same cells in the two neighbouring rows of the other cross
-// direction (coalesced along x like the rest); the x-neighbours come from the
-// adjacent lanes by shuffles (width W), the two lanes at the CTA's x edges
-// load theirs.  The residual rows use the stencil rows padded to 8 values
-// (two 16-byte loads in FP32).  The affine segment maps of the forward and
-// backward recurrences are then composed by log-step scans in shared memory.
-// zquirk (DIR 2): the first right-hand side of the z-line (x, y) is the
-// residual at cell y*N*K + x, where the reference reads it
-// (smoother_adlj_z.h:54-58).
-template <typename T, int DIR, int SEG, int MAXT, int MINB>
+// one thread per (line, segment).  Phase 1 loads the segment's row classes,
+// right-hand sides, pivots and iterate values (plus the iterate just before
+// and after the segment); phase 2 forms the residuals with the lateral
+// neighbours: the other cross direction's rows by coalesced loads, x +- 1
+// from the adjacent lanes by shuffles (width W; the CTA's edge lanes load
+// theirs) when VAR & 2, else by loads; then the affine segment maps of the
+// forward and backward recurrences are composed across the segments, by
+// log-step scans in shared memory when VAR & 1, else by each thread walking
+// the maps before its own.  zquirk (DIR 2): the first right-hand side of
+// the z-line (x, y) is the residual at cell y*N*K + x, where the reference
+// reads it (smoother_adlj_z.h:54-58).  Shared memory: 4 W S values.
+template <typename T, int DIR, int SEG, int MAXT, int MINB, int VAR>
 __global__ void __launch_bounds__(MAXT, MINB)
-    k_adlj_fused_seg(int N, int M, int K, bool zquirk, const int* __restrict__ cls, const T* __restrict__ dict8,
+    k_adlj_fused_seg(int N, int M, int K, bool zquirk, const int* __restrict__ cls, const T* __restrict__ dict,
                      const T* __restrict__ dinv, const T* __restrict__ b, const T* __restrict__ xin,
                      T* __restrict__ xout, T omega)
 {
     static_assert(DIR == 1 || DIR == 2, "y- or z-lines");
+    constexpr bool LOGSCAN = (VAR & 1) != 0, SHFL = (VAR & 2) != 0;
     extern __shared__ __align__(16) unsigned char fseg_smem[];
     const int W = blockDim.x, S = blockDim.y;
     T* sA = reinterpret_cast<T*>(fseg_smem);               // 2 buffers of W*S each
@@ -155,10 +155,9 @@ __global__ void __launch_bounds__(MAXT, MINB)
     const int i0 = DIR == 1 ? row * NM + xs : row * N + xs;
     const int t0 = sg * SEG;
     const bool hw = xs > 0, he = xs < N - 1, hm = row > 0, hp = row < rows - 1;
-    const bool edge_w = w == 0 && hw, edge_e = w == W - 1 && he;   // x-neighbour outside the CTA's lines
-    // phase 1: every load of the thread
+    // phase 1: the segment's own streams
     int cl[SEG];
-    T rv[SEG], dv[SEG], xc[SEG], xm[SEG], xq[SEG], xo[SEG];
+    T rv[SEG], dv[SEG], xc[SEG];
 #pragma unroll
     for (int u = 0; u < SEG; u++) {
         const int t = min(t0 + u, L - 1);
@@ -167,9 +166,6 @@ __global__ void __launch_bounds__(MAXT, MINB)
         rv[u] = b[i];
         dv[u] = dinv[i];
         xc[u] = xin[i];
-        xm[u] = hm ? xin[i - sb] : (T)0;
-        xq[u] = hp ? xin[i + sb] : (T)0;
-        xo[u] = edge_w ? xin[i - 1] : (edge_e ? xin[i + 1] : (T)0);
     }
     const T xprev = t0 > 0 ? xin[i0 + (t0 - 1) * st] : (T)0;
     const T xnext = t0 + SEG < L ? xin[i0 + (t0 + SEG) * st] : (T)0;
@@ -178,34 +174,45 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
     for (int u = 0; u < SEG; u++) {
         const int t = t0 + u;
-        const T fromw = __shfl_up_sync(0xffffffffu, xc[u], 1, W);     // lane w-1: x - 1
-        const T frome = __shfl_down_sync(0xffffffffu, xc[u], 1, W);   // lane w+1: x + 1
-        const T xw = w == 0 ? xo[u] : fromw;
-        const T xe = w == W - 1 ? xo[u] : frome;
+        T fromw = 0, frome = 0;
+        if constexpr (SHFL) {
+            fromw = __shfl_up_sync(0xffffffffu, xc[u], 1, W);             // lane w-1: x - 1
+            frome = __shfl_down_sync(0xffffffffu, xc[u], 1, W);           // lane w+1: x + 1
+        }
         lv[u] = 0;
         uv[u] = 0;
         if (t < L) {
-            T a[8];
-            load_row8(dict8 + (size_t)cl[u] * 8, a);
+            const int i = i0 + t * st;
+            T xw, xe;
+            if constexpr (SHFL) {
+                xw = w == 0 ? (hw ? xin[i - 1] : (T)0) : fromw;
+                xe = w == W - 1 ? (he ? xin[i + 1] : (T)0) : frome;
+            } else {
+                xw = hw ? xin[i - 1] : (T)0;
+                xe = he ? xin[i + 1] : (T)0;
+            }
+            const T* a = dict + (size_t)cl[u] * 7;
+            const T xm = hm ? xin[i - sb] : (T)0;
+            const T xq = hp ? xin[i + sb] : (T)0;
             const T xa = u == 0 ? xprev : xc[u > 0 ? u - 1 : 0];           // previous along the line
             const T xb = u == SEG - 1 ? xnext : xc[u < SEG - 1 ? u + 1 : 0];   // next along the line
             const bool ha = t > 0, hb = t < L - 1;
             T acc = a[3] * xc[u];
             if (DIR == 1) {
-                if (hm) acc += a[0] * xm[u];               // z - 1
+                if (hm) acc += a[0] * xm;                  // z - 1
                 if (ha) acc += a[1] * xa;                  // y - 1
                 if (hw) acc += a[2] * xw;
                 if (he) acc += a[4] * xe;
                 if (hb) acc += a[5] * xb;                  // y + 1
-                if (hp) acc += a[6] * xq[u];               // z + 1
+                if (hp) acc += a[6] * xq;                  // z + 1
                 lv[u] = a[1];
                 uv[u] = a[5] * dv[u];
             } else {
                 if (ha) acc += a[0] * xa;                  // z - 1
-                if (hm) acc += a[1] * xm[u];               // y - 1
+                if (hm) acc += a[1] * xm;                  // y - 1
                 if (hw) acc += a[2] * xw;
                 if (he) acc += a[4] * xe;
-                if (hp) acc += a[5] * xq[u];               // y + 1
+                if (hp) acc += a[5] * xq;                  // y + 1
                 if (hb) acc += a[6] * xb;                  // z + 1
                 lv[u] = a[0];
                 uv[u] = a[6] * dv[u];
@@ -213,7 +220,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
             rv[u] = rv[u] - acc;
         }
     }
-    if (DIR == 2 && zquirk && sg == 0) rv[0] = resid7_at8<T>(N, M, K, (long long)row * N * K + xs, cls, dict8, b, xin);
+    if (DIR == 2 && zquirk && sg == 0)
+        rv[0] = resid7_at<T, 7>(N, M, K, (long long)row * N * K + xs, cls, dict, b, xin);
     // forward, relative to y_in
     T fa = 0, fb = 1;
 #pragma unroll
@@ -231,9 +239,17 @@ __global__ void __launch_bounds__(MAXT, MINB)
         rv[u] = fa;
         lv[u] = fb;
     }
-    seg_scan<T, false>(fa, fb, sA, sB);
-    const T yin = fa;                                      // y entering this segment (line start: 0)
-    __syncthreads();                                       // the scan buffers are reused below
+    T yin = 0;
+    if constexpr (LOGSCAN) {
+        seg_scan<T, false>(fa, fb, sA, sB);
+        yin = fa;                                          // y entering this segment (line start: 0)
+    } else {
+        sA[sg * W + w] = fa;
+        sB[sg * W + w] = fb;
+        __syncthreads();
+        for (int q = 0; q < sg; q++) yin = sA[q * W + w] + sB[q * W + w] * yin;
+    }
+    __syncthreads();                                       // the shared buffers are reused below
     // backward, relative to x_out
     T gg = 0, hh = 1;
 #pragma unroll
@@ -252,14 +268,22 @@ __global__ void __launch_bounds__(MAXT, MINB)
         rv[u] = gg;
         lv[u] = hh;
     }
-    seg_scan<T, true>(gg, hh, sA, sB);
-    const T xout0 = gg;                                    // x leaving the next segment (line end: 0)
+    T xo = 0;
+    if constexpr (LOGSCAN) {
+        seg_scan<T, true>(gg, hh, sA, sB);
+        xo = gg;                                           // x leaving the next segment (line end: 0)
+    } else {
+        sA[sg * W + w] = gg;
+        sB[sg * W + w] = hh;
+        __syncthreads();
+        for (int q = S - 1; q > sg; q--) xo = sA[q * W + w] + sB[q * W + w] * xo;
+    }
     if (valid) {
 #pragma unroll
         for (int u = 0; u < SEG; u++) {
             const int t = t0 + u;
             if (t < L) {
-                const T cv = omega * (rv[u] + lv[u] * xout0);
+                const T cv = omega * (rv[u] + lv[u] * xo);
                 xout[i0 + t * st] = xc[u] + cv;
             }
         }

@@ -927,17 +927,6 @@ static int seg_cells(int L)
     return 0;
 }
 
-// Segment length of the fused y/z-line kernel (CTAs of 256 threads, at most
-// 32 segments per line): 8 cells, or 12 in FP32 for lines of 257..384
-// cells; 0 = the fused kernel does not take this length.
-template <typename T>
-static int fused_seg_cells(int L)
-{
-    if ((L + 7) / 8 <= 32) return 8;
-    if (sizeof(T) == 4 && (L + 11) / 12 <= 32) return 12;
-    return 0;
-}
-
 // Whether a level with these dimensions and stencil runs the fused ADLJ
 // direction steps: the fine 7-point stencil (offsets b, s, w, p, e, n, t),
 // x-lines of 8-cell segments on P <= 32 lanes (P a power of two), y- and
@@ -951,14 +940,47 @@ static bool adlj_fused_level(const Dims& g, int noff, const std::vector<int>& of
     if (g.N < 2 || g.M < 2 || g.K < 2 || g.N % 8) return false;
     const int P = g.N / 8;
     if (P > 32 || (P & (P - 1))) return false;
-    return fused_seg_cells<T>(g.M) != 0 && fused_seg_cells<T>(g.K) != 0;
+    return seg_cells<T>(g.M) != 0 && seg_cells<T>(g.K) != 0;
 }
 
 // One fused ADLJ direction step on level lv:  xout = xin + omega T_d^{-1} (b - A xin),
 // b = the level's right-hand side (lv.r, left unchanged).
+template <typename T, int DIR, int VAR>
+static void launch_fused_seg(const LevelT<T>& lv, bool zq, T omega, cudaStream_t s, const T* dinv, const T* xin,
+                             T* xout)
+{
+    constexpr int MAXT = sizeof(T) == 4 ? 512 : 256;
+    const Dims& g = lv.d;
+    const int L = DIR == 1 ? g.M : g.K;
+    const long long rows = DIR == 1 ? g.K : g.M;
+    const int seg = seg_cells<T>(L);
+    const int S = (L + seg - 1) / seg;
+    int W = 8;                                             // lanes per line row: a divisor of 32
+    while (W < 32 && 2 * W * S <= MAXT) W *= 2;
+    const unsigned blocks = (unsigned)((long long)((g.N + W - 1) / W) * rows);
+    const dim3 blk(W, S);
+    const size_t sm = 4 * (size_t)W * S * sizeof(T);       // scan buffers
+    if (seg == 8) {
+        k_adlj_fused_seg<T, DIR, 8, MAXT, 2, VAR><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls, lv.dict, dinv,
+                                                                         lv.r.p, xin, xout, omega);
+    } else {
+        if constexpr (sizeof(T) == 4)
+            k_adlj_fused_seg<T, DIR, 12, MAXT, 1, VAR><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls, lv.dict,
+                                                                              dinv, lv.r.p, xin, xout, omega);
+        else
+            throw Error{LSG_ERR_STATE, "no fused line kernel for this line length"};
+    }
+}
+
+// One fused ADLJ direction step on level lv:  xout = xin + omega T_d^{-1} (b - A xin),
+// b = the level's right-hand side (lv.r, left unchanged).  var selects the
+// y/z kernel's form (bit 0: log-step segment scans, bit 1: x-neighbours by
+// shuffles); row8: the x kernel reads the stencil rows padded to 8 values.
+constexpr int kFusedVar = 1;                               // the solve's y/z form (profile ids 13..20)
+
 template <typename T>
 static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStream_t s, const T* xin, T* xout,
-                            bool row8 = true)
+                            int var = kFusedVar, bool row8 = false)
 {
     const Dims& g = lv.d;
     const T* b = lv.r.p;
@@ -973,38 +995,17 @@ static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cu
             k_adlj_fused_xseg<T, 8, false><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
                 g.N, g.M, g.K, P, lv.cls, lv.dict, dinv, b, xin, xout, omega);
     } else {
-        constexpr int MAXT = 256;
-        const int L = d == 1 ? g.M : g.K;
-        const long long rows = d == 1 ? g.K : g.M;
-        const int seg = fused_seg_cells<T>(L);
-        const int S = (L + seg - 1) / seg;
-        int W = 8;                                         // lanes per line row: a divisor of 32
-        while (W < 32 && 2 * W * S <= MAXT) W *= 2;
-        const unsigned blocks = (unsigned)((long long)((g.N + W - 1) / W) * rows);
-        const dim3 blk(W, S);
-        const size_t sm = 4 * (size_t)W * S * sizeof(T);     // two scan buffers of (A, B)
         const bool zq = d == 2 && zquirk;
-        if (seg == 8) {
-            if (d == 1)
-                k_adlj_fused_seg<T, 1, 8, MAXT, 2><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, false, lv.cls, lv.dict8.p,
-                                                                           dinv, b, xin, xout, omega);
-            else
-                k_adlj_fused_seg<T, 2, 8, MAXT, 2><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls, lv.dict8.p,
-                                                                           dinv, b, xin, xout, omega);
-        } else {
-            if constexpr (sizeof(T) == 4) {
-                if (d == 1)
-                    k_adlj_fused_seg<T, 1, 12, MAXT, 1><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, false, lv.cls,
-                                                                                lv.dict8.p, dinv, b, xin, xout,
-                                                                                omega);
-                else
-                    k_adlj_fused_seg<T, 2, 12, MAXT, 1><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls,
-                                                                                lv.dict8.p, dinv, b, xin, xout,
-                                                                                omega);
-            } else {
-                throw Error{LSG_ERR_STATE, "no fused line kernel for this line length"};
-            }
+#define LSG_FUSED_SEG(V)                                                                    \
+    (d == 1 ? launch_fused_seg<T, 1, V>(lv, false, omega, s, dinv, xin, xout)              \
+            : launch_fused_seg<T, 2, V>(lv, zq, omega, s, dinv, xin, xout))
+        switch (var) {
+        case 0: LSG_FUSED_SEG(0); break;
+        case 1: LSG_FUSED_SEG(1); break;
+        case 2: LSG_FUSED_SEG(2); break;
+        default: LSG_FUSED_SEG(3); break;
         }
+#undef LSG_FUSED_SEG
     }
     LSG_CHECK_LAUNCH();
 }
@@ -1133,19 +1134,27 @@ static void vcycle(Context& C, std::vector<LevelT<T>>& lev, T* ch0 = nullptr)
         const Dims& f = lv.d;
         const TransferTabs& t = mg.tabs[l];
         T* chl = (l == 0 && ch0) ? ch0 : lv.ch.p;
-        constexpr int PZ = 4;
-        k_prolong<T, PZ><<<dim3((f.N + 31) / 32, (f.M + 7) / 8, (f.K + PZ - 1) / PZ), dim3(32, 8), 0, s>>>(
-            f.N, f.M, f.K, lev[l + 1].d.N, lev[l + 1].d.M, t.P(0), t.P(1), t.P(2), lev[l + 1].ch.p, chl, lv.c.p);
-        LSG_CHECK_LAUNCH();
         const int order[3] = {2, 1, 0};           // SmootherADLJ::solve: z, y, x
         const int steps = 3 * C.opt.n_post;
         const bool aligned = ((reinterpret_cast<uintptr_t>(chl) | reinterpret_cast<uintptr_t>(lv.c.p) |
                                reinterpret_cast<uintptr_t>(lv.r.p) | reinterpret_cast<uintptr_t>(lv.cls)) & 15) == 0;
-        if (steps > 0 && aligned && adlj_fused_level<T>(f, lv.ol.n, lv.off, C.opt)) {
-            // the iterate alternates between c and chl (both hold P c_H after the
-            // prolongation); the first buffer is chosen so the last step writes chl
-            T* buf[2] = {chl, lv.c.p};
-            int cur = steps % 2;
+        const bool fused = steps > 0 && aligned && adlj_fused_level<T>(f, lv.ol.n, lv.off, C.opt);
+        // the fused steps alternate the iterate between c and chl, starting from
+        // the buffer that makes the last step write chl: the prolongation fills
+        // that one only; the reference schedule needs P c_H in both
+        T* buf[2] = {chl, lv.c.p};
+        int cur = steps % 2;
+        constexpr int ZP = 8;
+        const dim3 pg(((f.N + 1) / 2 + 31) / 32, ((f.M + 1) / 2 + 3) / 4, (f.K + ZP - 1) / ZP);
+        const Dims& cd = lev[l + 1].d;
+        if (fused)
+            k_prolong_blk<T, ZP><<<pg, dim3(32, 4), 0, s>>>(f.N, f.M, f.K, cd.N, cd.M, cd.K, t.P(0), t.P(1), t.P(2),
+                                                            lev[l + 1].ch.p, buf[cur], nullptr);
+        else
+            k_prolong_blk<T, ZP><<<pg, dim3(32, 4), 0, s>>>(f.N, f.M, f.K, cd.N, cd.M, cd.K, t.P(0), t.P(1), t.P(2),
+                                                            lev[l + 1].ch.p, chl, lv.c.p);
+        LSG_CHECK_LAUNCH();
+        if (fused) {
             for (int it = 0; it < C.opt.n_post; it++)
                 for (int q = 0; q < 3; q++) {
                     adlj_fused_step<T>(lv, order[q], zq, omega, s, buf[cur], buf[cur ^ 1]);
@@ -1223,7 +1232,13 @@ static double vcycle_bytes(const MGData& mg, const lsg_options& o, double w)
         const double n = (double)mg.dims[l].n();
         if (l < mg.L) {
             b += (1.0 + 0.125) * w * n;                      // restriction read fine + write coarse
-            b += (0.125 + 2.0) * w * n;                      // prolongation read coarse + write ch, c (or ch rw)
+            const LevelT<double>& lp = mg.l64[l];
+            const bool fused_l = o.smoother == LSG_SMOOTHER_ADLJ && o.n_post > 0 &&
+                                 (w == 4.0 ? adlj_fused_level<float>(mg.dims[l], lp.ol.n, lp.off, o)
+                                           : adlj_fused_level<double>(mg.dims[l], lp.ol.n, lp.off, o));
+            // prolongation: read coarse, write ch and c (one of them ahead of
+            // the fused smoother; ch read and written in the Gauss-Seidel cycle)
+            b += (0.125 + (fused_l ? 1.0 : 2.0)) * w * n;
             if (o.smoother == LSG_SMOOTHER_RBGS) {
                 // full colour sweep: b, x read, x written, row class 4 B; pre-smoothed
                 // levels also form their residual (copy 2w + apply 3w + 4)
@@ -3651,20 +3666,24 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
                 d.N, d.M, d.K, C.cls0.p, C.dict0.p, C.Z32.p, C.V.p, C.w.p, C.red.partial.p, C.red.counter.p,
                 C.scal.p + 48);
             LSG_CHECK_LAUNCH();
-        } else if (which >= 9 && which <= 12) {
-            const int d = which == 12 ? 0 : which - 9;
-            const bool row8 = which != 12;
+        } else if (which >= 9 && which <= 20) {
+            // 9/10/11: the solve's form; 12: x with padded rows; 13..20: y/z
+            // with var = (which - 13) / 2 (0 walk + loads, 1 scans + loads,
+            // 2 walk + shuffles, 3 scans + shuffles)
+            const int d = which <= 11 ? which - 9 : (which == 12 ? 0 : 1 + (which - 13) % 2);
+            const bool row8 = which == 12;
+            const int var = which >= 13 ? (which - 13) / 2 : kFusedVar;
             const bool zq = C.opt.zline_reference != 0;
             if (f32) {
                 const LevelT<float>& lv = C.mg.l32[0];
                 LSG_REQUIRE(adlj_fused_level<float>(lv.d, lv.ol.n, lv.off, C.opt), LSG_ERR_STATE,
                             "the finest level does not run the fused ADLJ steps");
-                adlj_fused_step<float>(lv, d, zq, (float)C.opt.omega, C.s, lv.ch.p, lv.c.p, row8);
+                adlj_fused_step<float>(lv, d, zq, (float)C.opt.omega, C.s, lv.ch.p, lv.c.p, var, row8);
             } else {
                 const LevelT<double>& lv = C.mg.l64[0];
                 LSG_REQUIRE(adlj_fused_level<double>(lv.d, lv.ol.n, lv.off, C.opt), LSG_ERR_STATE,
                             "the finest level does not run the fused ADLJ steps");
-                adlj_fused_step<double>(lv, d, zq, C.opt.omega, C.s, lv.ch.p, lv.c.p, row8);
+                adlj_fused_step<double>(lv, d, zq, C.opt.omega, C.s, lv.ch.p, lv.c.p, var, row8);
             }
         } else {
             throw Error{LSG_ERR_ARG, "unknown kernel id"};
