@@ -537,10 +537,8 @@ int lsg_mg_level_tridiag(lsg_ctx* ctx, int level, char dir, double* c, double* d
    kernel (no staging; for comparison), 9/10/11 the fused ADLJ direction
    step (residual formed inside the line solve) along x/y/z on the finest
    level (needs a level that runs it: LSG_ADLJ_FUSED, or LSG_ADLJ_AUTO in
-   FP32), 12 the x step reading the stencil rows padded to 8 values, 13..20
-   the y/z steps in their four forms ((id - 13) / 2: segment maps composed
-   by each thread walking them or by log-step scans, x-neighbours by loads
-   or by shuffles; for comparison).
+   FP32), 12/13 the y/z steps with the segment maps walked by each thread
+   instead of composed by log-step scans (for comparison).
    Returns the mean duration of one launch and the algorithmic HBM bytes one
    launch moves (compulsory traffic of its inputs and outputs).  Needs
    lsg_setup with the multigrid preconditioner. */

@@ -9,8 +9,7 @@
 //     ch' = ch + omega T_d^{-1} (b - A ch)
 // computed here by one kernel per direction: each thread forms the residual
 // of its cells from b, the row class and the current iterate (its line
-// neighbours from registers, the lateral ones by shuffles or coalesced
-// loads issued with its own), then runs the
+// neighbours from registers, the lateral ones through L1/L2), then runs the
 // segmented Thomas recurrence of k_tdma_seg / k_tdma_xseg on it.  The line
 // tridiagonal is read from the operator's own rows (lo, up = the row's
 // couplings along d) and the stored inverse pivots dinv_d (the factorisation
@@ -24,37 +23,16 @@
 // against 10w + 4 for the separate residual update and line solve (r, c read
 // and r written; r, lo, dinv, up, ch read and c, ch written).
 //
-// The operator is the fine 7-point stencil in the row-dictionary form: dict8
-// holds each distinct row as (b, s, w, p, e, n, t, 0), cls[i] its index.
+// The operator is the fine 7-point stencil in the row-dictionary form: dict
+// holds each distinct row as (b, s, w, p, e, n, t), cls[i] its index.
 #pragma once
 
 #include "lsg_kernels.cuh"
 
 namespace lsg {
 
-// Row of the 7-point stencil stored with stride 8 (b, s, w, p, e, n, t, 0):
-// two 16-byte loads in FP32, four in FP64.
-template <typename T>
-__device__ __forceinline__ void load_row8(const T* __restrict__ p, T (&a)[8])
-{
-    if constexpr (sizeof(T) == 4) {
-        const float4 u = __ldg(reinterpret_cast<const float4*>(p));
-        const float4 v = __ldg(reinterpret_cast<const float4*>(p) + 1);
-        a[0] = u.x; a[1] = u.y; a[2] = u.z; a[3] = u.w;
-        a[4] = v.x; a[5] = v.y; a[6] = v.z; a[7] = v.w;
-    } else {
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const double2 u = __ldg(reinterpret_cast<const double2*>(p) + k);
-            a[2 * k] = u.x;
-            a[2 * k + 1] = u.y;
-        }
-    }
-}
-
 // b - A x at flat cell q, every neighbour read from memory (the z-line
-// quirk's right-hand side cell); stencil rows stored with stride RS (7 or 8).
-// Terms summed p, b, s, w, e, n, t.
+// quirk's right-hand side cell).  Terms summed p, b, s, w, e, n, t.
 template <typename T, int RS>
 __device__ __forceinline__ T resid7_at(int N, int M, int K, long long q, const int* __restrict__ cls,
                                        const T* __restrict__ dict, const T* __restrict__ b,
@@ -120,15 +98,14 @@ __device__ __forceinline__ void seg_scan(T& a, T& b, T* sA, T* sB)
 // W neighbouring lines (consecutive x) split into S = ceil(L/SEG) segments,
 // one thread per (line, segment).  Phase 1 loads the segment's row classes,
 // right-hand sides, pivots and iterate values (plus the iterate just before
-// and after the segment); phase 2 forms the residuals with the lateral
-// neighbours: the other cross direction's rows by coalesced loads, x +- 1
-// from the adjacent lanes by shuffles (width W; the CTA's edge lanes load
-// theirs) when VAR & 2, else by loads; then the affine segment maps of the
-// forward and backward recurrences are composed across the segments, by
-// log-step scans in shared memory when VAR & 1, else by each thread walking
-// the maps before its own.  zquirk (DIR 2): the first right-hand side of
-// the z-line (x, y) is the residual at cell y*N*K + x, where the reference
-// reads it (smoother_adlj_z.h:54-58).  Shared memory: 4 W S values.
+// and after the segment); phase 2 forms the residuals with the four lateral
+// neighbours (coalesced loads, mostly L1/L2 hits); then the affine segment
+// maps of the forward and backward recurrences are composed across the
+// segments: by log-step scans in shared memory when VAR & 1 (the solve's
+// form), else by each thread walking the maps before its own (timing
+// comparison).  zquirk (DIR 2): the first right-hand side of the z-line
+// (x, y) is the residual at cell y*N*K + x, where the reference reads it
+// (smoother_adlj_z.h:54-58).  Shared memory: 4 W S values.
 template <typename T, int DIR, int SEG, int MAXT, int MINB, int VAR>
 __global__ void __launch_bounds__(MAXT, MINB)
     k_adlj_fused_seg(int N, int M, int K, bool zquirk, const int* __restrict__ cls, const T* __restrict__ dict,
@@ -136,7 +113,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
                      T* __restrict__ xout, T omega)
 {
     static_assert(DIR == 1 || DIR == 2, "y- or z-lines");
-    constexpr bool LOGSCAN = (VAR & 1) != 0, SHFL = (VAR & 2) != 0;
+    constexpr bool LOGSCAN = (VAR & 1) != 0;
     extern __shared__ __align__(16) unsigned char fseg_smem[];
     const int W = blockDim.x, S = blockDim.y;
     T* sA = reinterpret_cast<T*>(fseg_smem);               // 2 buffers of W*S each
@@ -174,24 +151,13 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
     for (int u = 0; u < SEG; u++) {
         const int t = t0 + u;
-        T fromw = 0, frome = 0;
-        if constexpr (SHFL) {
-            fromw = __shfl_up_sync(0xffffffffu, xc[u], 1, W);             // lane w-1: x - 1
-            frome = __shfl_down_sync(0xffffffffu, xc[u], 1, W);           // lane w+1: x + 1
-        }
         lv[u] = 0;
         uv[u] = 0;
         if (t < L) {
             const int i = i0 + t * st;
-            T xw, xe;
-            if constexpr (SHFL) {
-                xw = w == 0 ? (hw ? xin[i - 1] : (T)0) : fromw;
-                xe = w == W - 1 ? (he ? xin[i + 1] : (T)0) : frome;
-            } else {
-                xw = hw ? xin[i - 1] : (T)0;
-                xe = he ? xin[i + 1] : (T)0;
-            }
             const T* a = dict + (size_t)cl[u] * 7;
+            const T xw = hw ? xin[i - 1] : (T)0;
+            const T xe = he ? xin[i + 1] : (T)0;
             const T xm = hm ? xin[i - sb] : (T)0;
             const T xq = hp ? xin[i + sb] : (T)0;
             const T xa = u == 0 ? xprev : xc[u > 0 ? u - 1 : 0];           // previous along the line
@@ -295,9 +261,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
 // loads (b, iterate, pivots, row classes, and the four lateral rows y +- 1,
 // z +- 1 of the iterate), the x neighbours across segment ends come from the
 // adjacent lanes by shuffles, and the segment maps are chained across the P
-// lanes of a line by warp scans.  ROW8: stencil rows padded to 8 values
-// (vector loads), else the plain 7-value rows.
-template <typename T, int SEG, bool ROW8>
+// lanes of a line by warp scans.
+template <typename T, int SEG>
 __global__ void __launch_bounds__(256) k_adlj_fused_xseg(int N, int M, int K, int P, const int* __restrict__ cls,
                                                           const T* __restrict__ dict, const T* __restrict__ dinv,
                                                           const T* __restrict__ b, const T* __restrict__ xin,
@@ -339,13 +304,7 @@ __global__ void __launch_bounds__(256) k_adlj_fused_xseg(int N, int M, int K, in
 #pragma unroll
     for (int u = 0; u < SEG; u++) {
         const int xx = q * SEG + u;
-        T a[8];
-        if constexpr (ROW8) {
-            load_row8(dict + (size_t)cl[u] * 8, a);
-        } else {
-#pragma unroll
-            for (int k = 0; k < 7; k++) a[k] = dict[(size_t)cl[u] * 7 + k];
-        }
+        const T* a = dict + (size_t)cl[u] * 7;
         T acc = a[3] * xc[u];
         if (hzm) acc += a[0] * zm[u];
         if (hym) acc += a[1] * ym[u];

@@ -153,7 +153,6 @@ struct LevelT {
     const T* dict = nullptr;
     DevBuf<T> dictown;
     DevBuf<T> dict28;         // 27-point levels: rows padded to stride 28 for vector loads
-    DevBuf<T> dict8;          // 7-point levels: rows padded to stride 8 for vector loads
     int nclass = 0;
     DevBuf<T> lo[3], dinv[3], up[3];
     DevBuf<T> gsdinv;         // Gauss-Seidel smoother: 1 / a_ii, 0 below the tiny pivot threshold
@@ -624,10 +623,6 @@ static void mg_setup(Context& C)
     mg.l64[0].cls = C.cls0.p;
     mg.l64[0].dict = C.dict0.p;
     mg.l64[0].nclass = C.nclass0;
-    mg.l64[0].dict8.alloc((size_t)C.nclass0 * 8);
-    k_pad_rows<<<grid_for((long long)C.nclass0 * 8, 256), 256, 0, s>>>(C.nclass0, 7, 8, C.dict0.p,
-                                                                        mg.l64[0].dict8.p);
-    LSG_CHECK_LAUNCH();
     std::vector<int> rad = {1, 1, 1};
     for (int l = 0; l < L; l++) {
         const Dims f = mg.dims[l];
@@ -787,12 +782,6 @@ static void mg_setup(Context& C)
             b.dict = b.dictown.p;
             k_convert<float, double><<<grid_for(nd, 256), 256, 0, s>>>(nd, a.dict, b.dictown.p);
             LSG_CHECK_LAUNCH();
-            if (a.dict8.p) {
-                const long long n8 = (long long)a.nclass * 8;
-                b.dict8.alloc(n8);
-                k_convert<float, double><<<grid_for(n8, 256), 256, 0, s>>>(n8, a.dict8.p, b.dict8.p);
-                LSG_CHECK_LAUNCH();
-            }
             if (a.ol.n == 27) {
                 const long long n28 = (long long)a.nclass * 28;
                 b.dict28.alloc(n28);
@@ -960,12 +949,13 @@ static void launch_fused_seg(const LevelT<T>& lv, bool zq, T omega, cudaStream_t
     const unsigned blocks = (unsigned)((long long)((g.N + W - 1) / W) * rows);
     const dim3 blk(W, S);
     const size_t sm = 4 * (size_t)W * S * sizeof(T);       // scan buffers
+    const T* dict = lv.dict;
     if (seg == 8) {
-        k_adlj_fused_seg<T, DIR, 8, MAXT, 2, VAR><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls, lv.dict, dinv,
+        k_adlj_fused_seg<T, DIR, 8, MAXT, 2, VAR><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls, dict, dinv,
                                                                          lv.r.p, xin, xout, omega);
     } else {
         if constexpr (sizeof(T) == 4)
-            k_adlj_fused_seg<T, DIR, 12, MAXT, 1, VAR><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls, lv.dict,
+            k_adlj_fused_seg<T, DIR, 12, MAXT, 1, VAR><<<blocks, blk, sm, s>>>(g.N, g.M, g.K, zq, lv.cls, dict,
                                                                               dinv, lv.r.p, xin, xout, omega);
         else
             throw Error{LSG_ERR_STATE, "no fused line kernel for this line length"};
@@ -973,14 +963,12 @@ static void launch_fused_seg(const LevelT<T>& lv, bool zq, T omega, cudaStream_t
 }
 
 // One fused ADLJ direction step on level lv:  xout = xin + omega T_d^{-1} (b - A xin),
-// b = the level's right-hand side (lv.r, left unchanged).  var selects the
-// y/z kernel's form (bit 0: log-step segment scans, bit 1: x-neighbours by
-// shuffles); row8: the x kernel reads the stencil rows padded to 8 values.
-constexpr int kFusedVar = 1;                               // the solve's y/z form (profile ids 13..20)
-
+// b = the level's right-hand side (lv.r, left unchanged).  scan: the y/z
+// kernel composes its segment maps by log-step scans (the solve's form;
+// false: each thread walks them, kept for timing comparisons).
 template <typename T>
 static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStream_t s, const T* xin, T* xout,
-                            int var = kFusedVar, bool row8 = false)
+                            bool scan = true)
 {
     const Dims& g = lv.d;
     const T* b = lv.r.p;
@@ -988,24 +976,17 @@ static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cu
     if (d == 0) {
         const int P = g.N / 8;
         const long long threads = (long long)g.M * g.K * P;
-        if (row8)
-            k_adlj_fused_xseg<T, 8, true><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-                g.N, g.M, g.K, P, lv.cls, lv.dict8.p, dinv, b, xin, xout, omega);
-        else
-            k_adlj_fused_xseg<T, 8, false><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(
-                g.N, g.M, g.K, P, lv.cls, lv.dict, dinv, b, xin, xout, omega);
+        k_adlj_fused_xseg<T, 8><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g.N, g.M, g.K, P, lv.cls, lv.dict,
+                                                                                dinv, b, xin, xout, omega);
     } else {
         const bool zq = d == 2 && zquirk;
-#define LSG_FUSED_SEG(V)                                                                    \
-    (d == 1 ? launch_fused_seg<T, 1, V>(lv, false, omega, s, dinv, xin, xout)              \
-            : launch_fused_seg<T, 2, V>(lv, zq, omega, s, dinv, xin, xout))
-        switch (var) {
-        case 0: LSG_FUSED_SEG(0); break;
-        case 1: LSG_FUSED_SEG(1); break;
-        case 2: LSG_FUSED_SEG(2); break;
-        default: LSG_FUSED_SEG(3); break;
+        if (scan) {
+            if (d == 1) launch_fused_seg<T, 1, 1>(lv, false, omega, s, dinv, xin, xout);
+            else launch_fused_seg<T, 2, 1>(lv, zq, omega, s, dinv, xin, xout);
+        } else {
+            if (d == 1) launch_fused_seg<T, 1, 0>(lv, false, omega, s, dinv, xin, xout);
+            else launch_fused_seg<T, 2, 0>(lv, zq, omega, s, dinv, xin, xout);
         }
-#undef LSG_FUSED_SEG
     }
     LSG_CHECK_LAUNCH();
 }
@@ -3666,24 +3647,22 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
                 d.N, d.M, d.K, C.cls0.p, C.dict0.p, C.Z32.p, C.V.p, C.w.p, C.red.partial.p, C.red.counter.p,
                 C.scal.p + 48);
             LSG_CHECK_LAUNCH();
-        } else if (which >= 9 && which <= 20) {
-            // 9/10/11: the solve's form; 12: x with padded rows; 13..20: y/z
-            // with var = (which - 13) / 2 (0 walk + loads, 1 scans + loads,
-            // 2 walk + shuffles, 3 scans + shuffles)
-            const int d = which <= 11 ? which - 9 : (which == 12 ? 0 : 1 + (which - 13) % 2);
-            const bool row8 = which == 12;
-            const int var = which >= 13 ? (which - 13) / 2 : kFusedVar;
+        } else if (which >= 9 && which <= 13) {
+            // 9/10/11: the solve's x/y/z steps; 12/13: y/z with the segment maps
+            // walked by each thread instead of scanned
+            const int d = which <= 11 ? which - 9 : which - 11;
+            const bool scan = which <= 11;
             const bool zq = C.opt.zline_reference != 0;
             if (f32) {
                 const LevelT<float>& lv = C.mg.l32[0];
                 LSG_REQUIRE(adlj_fused_level<float>(lv.d, lv.ol.n, lv.off, C.opt), LSG_ERR_STATE,
                             "the finest level does not run the fused ADLJ steps");
-                adlj_fused_step<float>(lv, d, zq, (float)C.opt.omega, C.s, lv.ch.p, lv.c.p, var, row8);
+                adlj_fused_step<float>(lv, d, zq, (float)C.opt.omega, C.s, lv.ch.p, lv.c.p, scan);
             } else {
                 const LevelT<double>& lv = C.mg.l64[0];
                 LSG_REQUIRE(adlj_fused_level<double>(lv.d, lv.ol.n, lv.off, C.opt), LSG_ERR_STATE,
                             "the finest level does not run the fused ADLJ steps");
-                adlj_fused_step<double>(lv, d, zq, C.opt.omega, C.s, lv.ch.p, lv.c.p, var, row8);
+                adlj_fused_step<double>(lv, d, zq, C.opt.omega, C.s, lv.ch.p, lv.c.p, scan);
             }
         } else {
             throw Error{LSG_ERR_ARG, "unknown kernel id"};
