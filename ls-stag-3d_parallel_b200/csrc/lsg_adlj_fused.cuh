@@ -53,47 +53,6 @@ __device__ __forceinline__ T resid7_at(int N, int M, int K, long long q, const i
     return b[q] - acc;
 }
 
-// Inclusive scan of the segment maps y = A + B y_in along the segment index
-// (threadIdx.y) of each line (threadIdx.x), Kogge-Stone in shared memory
-// with two buffers: log2(S) steps.  REV scans from the last segment down
-// (backward recurrence).  Returns the composed map of the segments before
-// this one (exclusive), as (A, B).
-template <typename T, bool REV>
-__device__ __forceinline__ void seg_scan(T& a, T& b, T* sA, T* sB)
-{
-    const int W = blockDim.x, S = blockDim.y;
-    const int w = threadIdx.x, sg = threadIdx.y;
-    const int q = REV ? S - 1 - sg : sg;                  // position along the scan
-    int cur = 0;
-    sA[sg * W + w] = a;
-    sB[sg * W + w] = b;
-    __syncthreads();
-    for (int off = 1; off < S; off <<= 1) {
-        T na = a, nb = b;
-        if (q >= off) {
-            const int src = (REV ? sg + off : sg - off) * W + w;
-            const T pa = sA[cur * W * S + src], pb = sB[cur * W * S + src];
-            na = a + b * pa;
-            nb = b * pb;
-        }
-        a = na;
-        b = nb;
-        cur ^= 1;
-        sA[cur * W * S + sg * W + w] = a;
-        sB[cur * W * S + sg * W + w] = b;
-        __syncthreads();
-    }
-    // exclusive: the inclusive result of the neighbour before this segment
-    if (q == 0) {
-        a = 0;
-        b = 1;
-    } else {
-        const int src = (REV ? sg + 1 : sg - 1) * W + w;
-        a = sA[cur * W * S + src];
-        b = sB[cur * W * S + src];
-    }
-}
-
 // y-lines (DIR 1) and z-lines (DIR 2), segmented like k_tdma_seg: a CTA holds
 // W neighbouring lines (consecutive x) split into S = ceil(L/SEG) segments,
 // one thread per (line, segment).  Phase 1 loads the segment's row classes,

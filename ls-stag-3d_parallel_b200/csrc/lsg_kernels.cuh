@@ -1126,6 +1126,47 @@ __global__ void __launch_bounds__(128) k_tdma_strided(LineGeom g, bool zquirk, c
     }
 }
 
+// Inclusive scan of the segment maps y = A + B y_in along the segment index
+// (threadIdx.y) of each line (threadIdx.x), Kogge-Stone in shared memory
+// with two buffers: log2(S) steps.  REV scans from the last segment down
+// (backward recurrence).  Returns the composed map of the segments before
+// this one (exclusive), as (A, B).
+template <typename T, bool REV>
+__device__ __forceinline__ void seg_scan(T& a, T& b, T* sA, T* sB)
+{
+    const int W = blockDim.x, S = blockDim.y;
+    const int w = threadIdx.x, sg = threadIdx.y;
+    const int q = REV ? S - 1 - sg : sg;                  // position along the scan
+    int cur = 0;
+    sA[sg * W + w] = a;
+    sB[sg * W + w] = b;
+    __syncthreads();
+    for (int off = 1; off < S; off <<= 1) {
+        T na = a, nb = b;
+        if (q >= off) {
+            const int src = (REV ? sg + off : sg - off) * W + w;
+            const T pa = sA[cur * W * S + src], pb = sB[cur * W * S + src];
+            na = a + b * pa;
+            nb = b * pb;
+        }
+        a = na;
+        b = nb;
+        cur ^= 1;
+        sA[cur * W * S + sg * W + w] = a;
+        sB[cur * W * S + sg * W + w] = b;
+        __syncthreads();
+    }
+    // exclusive: the inclusive result of the neighbour before this segment
+    if (q == 0) {
+        a = 0;
+        b = 1;
+    } else {
+        const int src = (REV ? sg + 1 : sg - 1) * W + w;
+        a = sA[cur * W * S + src];
+        b = sB[cur * W * S + src];
+    }
+}
+
 // y- and z-lines, segmented.  A CTA holds W neighbouring lines (consecutive
 // x, so each warp load is a contiguous row piece) split into S = ceil(L/SEG)
 // segments, one thread per (line, segment).  Every thread issues all loads of
@@ -1134,8 +1175,10 @@ __global__ void __launch_bounds__(128) k_tdma_strided(LineGeom g, bool zquirk, c
 //   y_t = (r_t - lo_t y_{t-1}) dinv_t
 // is kept as affine maps of the value entering the segment, y_t = A_t + B_t y_in,
 // and the backward one x_t = y_t - up_t x_{t+1} as x_t = G_t + H_t x_out; the
-// S segment maps of a line are chained through shared memory.
-template <typename T, int SEG, int MAXT, int MINB>
+// S segment maps of a line are composed through shared memory by log-step
+// scans (SCAN), or by each thread walking the maps before its own.  Shared
+// memory: 4 W S values.
+template <typename T, int SEG, int MAXT, int MINB, bool SCAN = true>
 __global__ void __launch_bounds__(MAXT, MINB) k_tdma_seg(LineGeom g, bool zquirk, const T* __restrict__ lo,
                                                          const T* __restrict__ dinv, const T* __restrict__ up,
                                                          const T* __restrict__ r, T* __restrict__ c,
@@ -1184,11 +1227,16 @@ __global__ void __launch_bounds__(MAXT, MINB) k_tdma_seg(LineGeom g, bool zquirk
         rv[u] = a;
         lv[u] = b;
     }
-    sA[sg * W + w] = a;
-    sB[sg * W + w] = b;
-    __syncthreads();
     T yin = 0;
-    for (int q = 0; q < sg; q++) yin = sA[q * W + w] + sB[q * W + w] * yin;
+    if constexpr (SCAN) {
+        seg_scan<T, false>(a, b, sA, sA + 2 * W * S);
+        yin = a;
+    } else {
+        sA[sg * W + w] = a;
+        sB[sg * W + w] = b;
+        __syncthreads();
+        for (int q = 0; q < sg; q++) yin = sA[q * W + w] + sB[q * W + w] * yin;
+    }
     __syncthreads();
     // backward, relative to x_out
     T gg = 0, hh = 1;
@@ -1208,11 +1256,16 @@ __global__ void __launch_bounds__(MAXT, MINB) k_tdma_seg(LineGeom g, bool zquirk
         rv[u] = gg;
         lv[u] = hh;
     }
-    sA[sg * W + w] = gg;
-    sB[sg * W + w] = hh;
-    __syncthreads();
     T xo = 0;
-    for (int q = S - 1; q > sg; q--) xo = sA[q * W + w] + sB[q * W + w] * xo;
+    if constexpr (SCAN) {
+        seg_scan<T, true>(gg, hh, sA, sA + 2 * W * S);
+        xo = gg;
+    } else {
+        sA[sg * W + w] = gg;
+        sB[sg * W + w] = hh;
+        __syncthreads();
+        for (int q = S - 1; q > sg; q--) xo = sA[q * W + w] + sB[q * W + w] * xo;
+    }
     if (valid) {
 #pragma unroll
         for (int u = 0; u < SEG; u++) {

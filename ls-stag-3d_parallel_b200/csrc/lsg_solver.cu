@@ -841,7 +841,8 @@ static void apply_resid(const LevelT<T>& lv, const T* x, T* r, cudaStream_t s, i
 }
 
 template <typename T>
-static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStream_t s, T* ch = nullptr)
+static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStream_t s, T* ch = nullptr,
+                       bool walk = false)
 {
     if (!ch) ch = const_cast<T*>(lv.ch.p);
     const Dims& g = lv.d;
@@ -888,12 +889,16 @@ static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStr
         if (8 * S8 <= MAXT && (S8 <= 32 || 8 * S12 > MAXT)) {
             const int W = pick_w(S8);
             const long long blocks = (long long)((g.N + W - 1) / W) * rows;
-            k_tdma_seg<T, 8, MAXT, 2><<<(unsigned)blocks, dim3(W, S8), 2 * (size_t)W * S8 * sizeof(T), s>>>(
-                lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, ch, omega);
+            if (walk)
+                k_tdma_seg<T, 8, MAXT, 2, false><<<(unsigned)blocks, dim3(W, S8), 4 * (size_t)W * S8 * sizeof(T), s>>>(
+                    lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, ch, omega);
+            else
+                k_tdma_seg<T, 8, MAXT, 2><<<(unsigned)blocks, dim3(W, S8), 4 * (size_t)W * S8 * sizeof(T), s>>>(
+                    lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, ch, omega);
         } else if (sizeof(T) == 4 && 8 * S12 <= MAXT) {
             const int W = pick_w(S12);
             const long long blocks = (long long)((g.N + W - 1) / W) * rows;
-            k_tdma_seg<T, 12, MAXT, 1><<<(unsigned)blocks, dim3(W, S12), 2 * (size_t)W * S12 * sizeof(T), s>>>(
+            k_tdma_seg<T, 12, MAXT, 1><<<(unsigned)blocks, dim3(W, S12), 4 * (size_t)W * S12 * sizeof(T), s>>>(
                 lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, ch, omega);
         } else {
             k_tdma_strided<T><<<grid_for(lg.nlines(), 128, 148 * 64), 128, 0, s>>>(
@@ -3647,6 +3652,12 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
                 d.N, d.M, d.K, C.cls0.p, C.dict0.p, C.Z32.p, C.V.p, C.w.p, C.red.partial.p, C.red.counter.p,
                 C.scal.p + 48);
             LSG_CHECK_LAUNCH();
+        } else if (which == 14 || which == 15) {
+            // the reference-schedule y/z line solve with the segment maps walked
+            if (f32) line_solve<float>(C.mg.l32[0], which - 13, C.opt.zline_reference != 0, (float)C.opt.omega, C.s,
+                                       nullptr, true);
+            else line_solve<double>(C.mg.l64[0], which - 13, C.opt.zline_reference != 0, C.opt.omega, C.s, nullptr,
+                                    true);
         } else if (which >= 9 && which <= 13) {
             // 9/10/11: the solve's x/y/z steps; 12/13: y/z with the segment maps
             // walked by each thread instead of scanned
@@ -3669,7 +3680,8 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
         }
     };
     double bytes;
-    if (which >= 9) bytes = (4.0 * w + 4.0) * n;      // b, iterate, dinv read; iterate written; row class
+    if (which == 14 || which == 15) bytes = 7.0 * w * n;
+    else if (which >= 9) bytes = (4.0 * w + 4.0) * n; // b, iterate, dinv read; iterate written; row class
     else if (which <= 2) bytes = 7.0 * w * n;         // r, lo, dinv, up, ch read; c, ch written
     else if (which == 3) bytes = (3.0 * w + 4.0) * n; // c, r read/write, row class
     else if (which == 5) bytes = (3.0 * w + 4.0) * (double)C.mg.dims[1].n();
