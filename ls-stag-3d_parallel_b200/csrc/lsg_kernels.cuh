@@ -630,104 +630,6 @@ __global__ void __launch_bounds__(256) k_prolong(int N, int M, int K, int Nc, in
     }
 }
 
-// The same prolongation with each thread on a 2 x 2 block of fine (x, y)
-// cells marching ZP fine z-planes: the fine cells 2I, 2I+1 of a dimension
-// draw on the coarse cells I-1, I, I+1 only (both 1-D factors, even and odd),
-// so a thread loads the 3 x 3 coarse columns of one new coarse plane per fine
-// z-pair (nine loads for eight fine cells instead of eight gathers per fine
-// cell) into a ring of three planes in shared memory, which it indexes by the
-// table's coarse indices.  Weights, skipped zero weights and summation order
-// are those of k_prolong (z, y, x ascending), so the results are the same
-// bits.  Block (32, 4); c may be null (only ch is written).
-template <typename T, int ZP>
-__global__ void __launch_bounds__(128) k_prolong_blk(int N, int M, int K, int Nc, int Mc, int Kc, PTab px, PTab py,
-                                                     PTab pz, const T* __restrict__ coarse, T* __restrict__ ch,
-                                                     T* __restrict__ c)
-{
-    static_assert(ZP % 2 == 0, "fine z-planes in pairs");
-    __shared__ T ring[3][9][128];                           // [plane slot][window cell][thread]
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-    const int I = blockIdx.x * 32 + threadIdx.x;           // fine x 2I, 2I+1
-    const int J = blockIdx.y * 4 + threadIdx.y;            // fine y 2J, 2J+1
-    if (2 * I >= N || 2 * J >= M) return;                  // no barrier below: each thread reads its own slots
-    const int z0 = blockIdx.z * ZP;                        // even
-    const int z1 = min(z0 + ZP, K);
-    const int NMc = Nc * Mc;
-    // x and y: weights and window cells (coarse index - (I-1)) of the two fine cells
-    float wx[2][2], wy[2][2];
-    int kx[2][2], ky[2][2];
-#pragma unroll
-    for (int s = 0; s < 2; s++) {
-        const int fx = min(2 * I + s, N - 1), fy = min(2 * J + s, M - 1);
-#pragma unroll
-        for (int q = 0; q < 2; q++) {
-            wx[s][q] = px.w[2 * fx + q];
-            kx[s][q] = wx[s][q] != 0.f ? px.c[2 * fx + q] - (I - 1) : 1;
-            wy[s][q] = py.w[2 * fy + q];
-            ky[s][q] = wy[s][q] != 0.f ? py.c[2 * fy + q] - (J - 1) : 1;
-        }
-    }
-    const bool vx1 = 2 * I + 1 < N, vy1 = 2 * J + 1 < M;
-    // the 3 x 3 coarse columns (clamped: a clamped cell carries no weight)
-    int col[9];
-#pragma unroll
-    for (int b = 0; b < 3; b++)
-#pragma unroll
-        for (int a = 0; a < 3; a++)
-            col[b * 3 + a] = min(max(I - 1 + a, 0), Nc - 1) + Nc * min(max(J - 1 + b, 0), Mc - 1);
-    // coarse plane kz lives in ring slot (kz + 3) % 3
-    auto load_plane = [&](int kz) {
-        const int z = min(max(kz, 0), Kc - 1);
-        const int slot = (kz + 3) % 3;
-        T v[9];
-#pragma unroll
-        for (int e = 0; e < 9; e++) v[e] = coarse[col[e] + NMc * z];
-#pragma unroll
-        for (int e = 0; e < 9; e++) ring[slot][e][tid] = v[e];
-    };
-    const int Kz0 = z0 / 2;
-    load_plane(Kz0 - 1);
-    load_plane(Kz0);
-    for (int zf = z0; zf < z1; zf += 2) {
-        const int Kz = zf / 2;
-        load_plane(Kz + 1);
-#pragma unroll
-        for (int sz = 0; sz < 2; sz++) {
-            const int z = zf + sz;
-            if (z >= z1) break;
-            float wz[2];
-            int slot[2];
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                wz[q] = pz.w[2 * z + q];
-                const int kz = wz[q] != 0.f ? pz.c[2 * z + q] : Kz;
-                slot[q] = (kz + 3) % 3;
-            }
-#pragma unroll
-            for (int sy = 0; sy < 2; sy++) {
-                if (sy == 1 && !vy1) break;
-#pragma unroll
-                for (int sx = 0; sx < 2; sx++) {
-                    if (sx == 1 && !vx1) break;
-                    T acc = 0;
-#pragma unroll
-                    for (int a = 0; a < 2; a++)
-#pragma unroll
-                        for (int b = 0; b < 2; b++)
-#pragma unroll
-                            for (int q = 0; q < 2; q++)
-                                if (wz[a] != 0.f && wy[sy][b] != 0.f && wx[sx][q] != 0.f)
-                                    acc += (T)(wz[a] * wy[sy][b] * wx[sx][q]) *
-                                           ring[slot[a]][ky[sy][b] * 3 + kx[sx][q]][tid];
-                    const int i = (2 * I + sx) + N * ((2 * J + sy) + M * z);   // grids hold fewer than 2^31 cells
-                    ch[i] = acc;
-                    if (c) c[i] = acc;
-                }
-            }
-        }
-    }
-}
-
 // coarse = R fine.  agglomerate: 1/8 of the 2x2x2 block (even-even-even
 // class, summed in the reference's CSR order); otherwise R = P^T via tables.
 template <typename T>
