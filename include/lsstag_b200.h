@@ -539,8 +539,7 @@ int lsg_mg_level_tridiag(lsg_ctx* ctx, int level, char dir, double* c, double* d
    level (needs a level that runs it: LSG_ADLJ_FUSED, or LSG_ADLJ_AUTO in
    FP32), 12/13 the y/z steps with the segment maps walked by each thread
    instead of composed by log-step scans, 14/15 the same for the y/z line
-   solves of the reference schedule, 16/17 the fused y/z steps with the
-   next cell's lateral neighbours loaded ahead (for comparison).
+   solves of the reference schedule (for comparison).
    Returns the mean duration of one launch and the algorithmic HBM bytes one
    launch moves (compulsory traffic of its inputs and outputs).  Needs
    lsg_setup with the multigrid preconditioner. */

@@ -58,12 +58,11 @@ __device__ __forceinline__ T resid7_at(int N, int M, int K, long long q, const i
 // one thread per (line, segment).  Phase 1 loads the segment's row classes,
 // right-hand sides, pivots and iterate values (plus the iterate just before
 // and after the segment); phase 2 forms the residuals with the four lateral
-// neighbours (coalesced loads, mostly L1/L2 hits; with VAR & 2 those of
-// the next cell are in flight while a cell's residual is formed); then the
-// affine segment maps of the forward and backward recurrences are composed
-// across the segments: by log-step scans in shared memory when VAR & 1 (the
-// solve's form), else by each thread walking the maps before its own
-// (timing comparison).  zquirk (DIR 2): the first right-hand side of the z-line
+// neighbours (coalesced loads, mostly L1/L2 hits); then the affine segment
+// maps of the forward and backward recurrences are composed across the
+// segments: by log-step scans in shared memory when VAR & 1 (the solve's
+// form), else by each thread walking the maps before its own (timing
+// comparison).  zquirk (DIR 2): the first right-hand side of the z-line
 // (x, y) is the residual at cell y*N*K + x, where the reference reads it
 // (smoother_adlj_z.h:54-58).  Shared memory: 4 W S values.
 template <typename T, int DIR, int SEG, int MAXT, int MINB, int VAR>
@@ -73,7 +72,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
                      T* __restrict__ xout, T omega)
 {
     static_assert(DIR == 1 || DIR == 2, "y- or z-lines");
-    constexpr bool LOGSCAN = (VAR & 1) != 0, PIPE = (VAR & 2) != 0;
+    constexpr bool LOGSCAN = (VAR & 1) != 0;
     extern __shared__ __align__(16) unsigned char fseg_smem[];
     const int W = blockDim.x, S = blockDim.y;
     T* sA = reinterpret_cast<T*>(fseg_smem);               // 2 buffers of W*S each
@@ -106,37 +105,20 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
     const T xprev = t0 > 0 ? xin[i0 + (t0 - 1) * st] : (T)0;
     const T xnext = t0 + SEG < L ? xin[i0 + (t0 + SEG) * st] : (T)0;
-    // phase 2: residuals; lv <- lower coupling, uv <- scaled upper coupling.
-    // PIPE: the four lateral neighbours of the next cell are loaded while
-    // this cell's residual is formed.
+    // phase 2: residuals; lv <- lower coupling, uv <- scaled upper coupling
     T lv[SEG], uv[SEG];
-    T nw = 0, ne = 0, nm = 0, nq = 0;
-    auto laterals = [&](int u) {
-        const int i = i0 + min(t0 + u, L - 1) * st;
-        nw = hw ? xin[i - 1] : (T)0;
-        ne = he ? xin[i + 1] : (T)0;
-        nm = hm ? xin[i - sb] : (T)0;
-        nq = hp ? xin[i + sb] : (T)0;
-    };
-    if constexpr (PIPE) laterals(0);
 #pragma unroll
     for (int u = 0; u < SEG; u++) {
         const int t = t0 + u;
-        T xw = nw, xe = ne, xm = nm, xq = nq;
-        if constexpr (PIPE) {
-            if (u + 1 < SEG) laterals(u + 1);
-        }
         lv[u] = 0;
         uv[u] = 0;
         if (t < L) {
             const int i = i0 + t * st;
             const T* a = dict + (size_t)cl[u] * 7;
-            if constexpr (!PIPE) {
-                xw = hw ? xin[i - 1] : (T)0;
-                xe = he ? xin[i + 1] : (T)0;
-                xm = hm ? xin[i - sb] : (T)0;
-                xq = hp ? xin[i + sb] : (T)0;
-            }
+            const T xw = hw ? xin[i - 1] : (T)0;
+            const T xe = he ? xin[i + 1] : (T)0;
+            const T xm = hm ? xin[i - sb] : (T)0;
+            const T xq = hp ? xin[i + sb] : (T)0;
             const T xa = u == 0 ? xprev : xc[u > 0 ? u - 1 : 0];           // previous along the line
             const T xb = u == SEG - 1 ? xnext : xc[u < SEG - 1 ? u + 1 : 0];   // next along the line
             const bool ha = t > 0, hb = t < L - 1;

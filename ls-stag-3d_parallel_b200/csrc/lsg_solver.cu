@@ -973,7 +973,7 @@ static void launch_fused_seg(const LevelT<T>& lv, bool zq, T omega, cudaStream_t
 // false: each thread walks them, kept for timing comparisons).
 template <typename T>
 static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStream_t s, const T* xin, T* xout,
-                            bool scan = true, bool pipe = false)
+                            bool scan = true)
 {
     const Dims& g = lv.d;
     const T* b = lv.r.p;
@@ -985,10 +985,7 @@ static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cu
                                                                                 dinv, b, xin, xout, omega);
     } else {
         const bool zq = d == 2 && zquirk;
-        if (scan && pipe) {
-            if (d == 1) launch_fused_seg<T, 1, 3>(lv, false, omega, s, dinv, xin, xout);
-            else launch_fused_seg<T, 2, 3>(lv, zq, omega, s, dinv, xin, xout);
-        } else if (scan) {
+        if (scan) {
             if (d == 1) launch_fused_seg<T, 1, 1>(lv, false, omega, s, dinv, xin, xout);
             else launch_fused_seg<T, 2, 1>(lv, zq, omega, s, dinv, xin, xout);
         } else {
@@ -3660,24 +3657,22 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
                                        nullptr, true);
             else line_solve<double>(C.mg.l64[0], which - 13, C.opt.zline_reference != 0, C.opt.omega, C.s, nullptr,
                                     true);
-        } else if ((which >= 9 && which <= 13) || which == 16 || which == 17) {
+        } else if (which >= 9 && which <= 13) {
             // 9/10/11: the solve's x/y/z steps; 12/13: y/z with the segment maps
-            // walked by each thread instead of scanned; 16/17: y/z with the next
-            // cell's lateral neighbours loaded ahead
-            const int d = which <= 11 ? which - 9 : (which <= 13 ? which - 11 : which - 15);
-            const bool scan = which <= 11 || which >= 16;
-            const bool pipe = which >= 16;
+            // walked by each thread instead of scanned
+            const int d = which <= 11 ? which - 9 : which - 11;
+            const bool scan = which <= 11;
             const bool zq = C.opt.zline_reference != 0;
             if (f32) {
                 const LevelT<float>& lv = C.mg.l32[0];
                 LSG_REQUIRE(adlj_fused_level<float>(lv.d, lv.ol.n, lv.off, C.opt), LSG_ERR_STATE,
                             "the finest level does not run the fused ADLJ steps");
-                adlj_fused_step<float>(lv, d, zq, (float)C.opt.omega, C.s, lv.ch.p, lv.c.p, scan, pipe);
+                adlj_fused_step<float>(lv, d, zq, (float)C.opt.omega, C.s, lv.ch.p, lv.c.p, scan);
             } else {
                 const LevelT<double>& lv = C.mg.l64[0];
                 LSG_REQUIRE(adlj_fused_level<double>(lv.d, lv.ol.n, lv.off, C.opt), LSG_ERR_STATE,
                             "the finest level does not run the fused ADLJ steps");
-                adlj_fused_step<double>(lv, d, zq, C.opt.omega, C.s, lv.ch.p, lv.c.p, scan, pipe);
+                adlj_fused_step<double>(lv, d, zq, C.opt.omega, C.s, lv.ch.p, lv.c.p, scan);
             }
         } else {
             throw Error{LSG_ERR_ARG, "unknown kernel id"};
