@@ -539,7 +539,9 @@ int lsg_mg_level_tridiag(lsg_ctx* ctx, int level, char dir, double* c, double* d
    level (needs a level that runs it: LSG_ADLJ_FUSED, or LSG_ADLJ_AUTO in
    FP32), 12/13 the y/z steps with the segment maps walked by each thread
    instead of composed by log-step scans, 14/15 the same for the y/z line
-   solves of the reference schedule (for comparison).
+   solves of the reference schedule, 16/17 those line solves with 4-cell
+   segments (the FP64 z-line solve's own form), 18/19 the first coarse
+   level's residual with 8 / 16 z-planes per thread (for comparison).
    Returns the mean duration of one launch and the algorithmic HBM bytes one
    launch moves (compulsory traffic of its inputs and outputs).  Needs
    lsg_setup with the multigrid preconditioner. */

@@ -816,10 +816,13 @@ static void mg_setup(Context& C)
 // Input: right-hand side already in lev[0].r.  Output: lev[0].ch.
 // ---------------------------------------------------------------------------
 template <typename T>
-static void apply_resid(const LevelT<T>& lv, const T* x, T* r, cudaStream_t s, int mode)
+static void apply_resid(const LevelT<T>& lv, const T* x, T* r, cudaStream_t s, int mode, int zc27 = 0)
 {
     const long long n = lv.d.n();
-    const int zc = zchunk_for(n);
+    // 27-point levels of a million cells or more march 8 z-planes a thread (the
+    // two planes loaded ahead of each chunk weigh less; 14.9 against 16.5 us
+    // at 128^3 in FP32, measured)
+    const int zc = lv.ol.n == 27 ? (zc27 > 0 ? zc27 : (n >= (1LL << 20) ? 8 : zchunk_for(n))) : zchunk_for(n);
     const dim3 zb(32, 8), zg((lv.d.N + 31) / 32, (lv.d.M + 7) / 8, (lv.d.K + zc - 1) / zc);
     if (lv.ol.n == 7 && lv.off[0] == 0 && lv.off[2] == -1) {
         if (mode == 0)
@@ -842,8 +845,9 @@ static void apply_resid(const LevelT<T>& lv, const T* x, T* r, cudaStream_t s, i
 
 template <typename T>
 static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStream_t s, T* ch = nullptr,
-                       bool walk = false)
+                       int form = 0)
 {
+    const bool walk = form == 1;
     if (!ch) ch = const_cast<T*>(lv.ch.p);
     const Dims& g = lv.d;
     if (d == 0) {
@@ -885,8 +889,16 @@ static void line_solve(const LevelT<T>& lv, int d, bool zquirk, T omega, cudaStr
             while (W < 32 && 2 * W * S <= MAXT) W *= 2;
             return W;
         };
-        const int S8 = (L + 7) / 8, S12 = (L + 11) / 12;
-        if (8 * S8 <= MAXT && (S8 <= 32 || 8 * S12 > MAXT)) {
+        const int S8 = (L + 7) / 8, S12 = (L + 11) / 12, S4 = (L + 3) / 4;
+        // FP64 z-lines: 4-cell segments in 512-thread CTAs (59 registers, two
+        // CTAs per SM instead of one 126-register CTA of 8-cell segments:
+        // 246 against 276 us at 256^3, measured); form 2 forces them
+        const bool seg4 = (form == 2 || (form == 0 && sizeof(T) == 8 && d == 2)) && 8 * S4 <= 512;
+        if (seg4) {
+            const long long blocks = (long long)((g.N + 7) / 8) * rows;
+            k_tdma_seg<T, 4, 512, 2><<<(unsigned)blocks, dim3(8, S4), 4 * (size_t)8 * S4 * sizeof(T), s>>>(
+                lg, d == 2 && zquirk, lv.lo[d].p, lv.dinv[d].p, lv.up[d].p, lv.r.p, lv.c.p, ch, omega);
+        } else if (8 * S8 <= MAXT && (S8 <= 32 || 8 * S12 > MAXT)) {
             const int W = pick_w(S8);
             const long long blocks = (long long)((g.N + W - 1) / W) * rows;
             if (walk)
@@ -3651,12 +3663,20 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
                 d.N, d.M, d.K, C.cls0.p, C.dict0.p, C.Z32.p, C.V.p, C.w.p, C.red.partial.p, C.red.counter.p,
                 C.scal.p + 48);
             LSG_CHECK_LAUNCH();
-        } else if (which == 14 || which == 15) {
+        } else if (which >= 14 && which <= 17) {
             // the reference-schedule y/z line solve with the segment maps walked
-            if (f32) line_solve<float>(C.mg.l32[0], which - 13, C.opt.zline_reference != 0, (float)C.opt.omega, C.s,
-                                       nullptr, true);
-            else line_solve<double>(C.mg.l64[0], which - 13, C.opt.zline_reference != 0, C.opt.omega, C.s, nullptr,
-                                    true);
+            // (14/15) or with 4-cell segments (16/17)
+            const int form = which <= 15 ? 1 : 2;
+            const int d = 1 + (which - 14) % 2;
+            if (f32) line_solve<float>(C.mg.l32[0], d, C.opt.zline_reference != 0, (float)C.opt.omega, C.s,
+                                       nullptr, form);
+            else line_solve<double>(C.mg.l64[0], d, C.opt.zline_reference != 0, C.opt.omega, C.s, nullptr, form);
+        } else if (which == 18 || which == 19) {
+            // the first coarse level's residual update with 8 / 16 z-planes per thread
+            LSG_REQUIRE(C.mg.L >= 2, LSG_ERR_STATE, "no smoothed coarse level");
+            const int zc = which == 18 ? 8 : 16;
+            if (f32) apply_resid<float>(C.mg.l32[1], C.mg.l32[1].c.p, C.mg.l32[1].r.p, C.s, 0, zc);
+            else apply_resid<double>(C.mg.l64[1], C.mg.l64[1].c.p, C.mg.l64[1].r.p, C.s, 0, zc);
         } else if (which >= 9 && which <= 13) {
             // 9/10/11: the solve's x/y/z steps; 12/13: y/z with the segment maps
             // walked by each thread instead of scanned
@@ -3679,7 +3699,8 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
         }
     };
     double bytes;
-    if (which == 14 || which == 15) bytes = 7.0 * w * n;
+    if (which >= 14 && which <= 17) bytes = 7.0 * w * n;
+    else if (which == 18 || which == 19) bytes = (3.0 * w + 4.0) * (double)C.mg.dims[1].n();
     else if (which >= 9) bytes = (4.0 * w + 4.0) * n; // b, iterate, dinv read; iterate written; row class
     else if (which <= 2) bytes = 7.0 * w * n;         // r, lo, dinv, up, ch read; c, ch written
     else if (which == 3) bytes = (3.0 * w + 4.0) * n; // c, r read/write, row class
@@ -3687,7 +3708,7 @@ int lsg_profile_kernel(lsg_ctx* h, int which, int reps, double* ms_per_launch, d
     else if (which >= 6) bytes = (4.0 + 8.0 + 8.0 + 4.0) * n;   // FP32 z, v0 read, w written, row class
     else bytes = (3.0 * 8.0 + 4.0) * n;               // z, v0 read, w written, row class
     // defined inputs for the timed launches
-    if (which == 5) {
+    if (which == 5 || which == 18 || which == 19) {
         const long long n1 = C.mg.dims[1].n();
         if (f32) {
             LSG_CUDA(cudaMemsetAsync(C.mg.l32[1].r.p, 0, n1 * 4, C.s));
