@@ -949,8 +949,8 @@ static bool adlj_fused_level(const Dims& g, int noff, const std::vector<int>& of
     return seg_cells<T>(g.M) != 0 && seg_cells<T>(g.K) != 0;
 }
 
-// One fused ADLJ direction step on level lv:  xout = xin + omega T_d^{-1} (b - A xin),
-// b = the level's right-hand side (lv.r, left unchanged).
+// The fused y (DIR 1) or z (DIR 2) step in the form VAR of k_adlj_fused_seg:
+// W lines x S segments per CTA of at most MAXT threads.
 template <typename T, int DIR, int VAR>
 static void launch_fused_seg(const LevelT<T>& lv, bool zq, T omega, cudaStream_t s, const T* dinv, const T* xin,
                              T* xout)
