@@ -104,8 +104,8 @@ def test_gradient_matches_oracle_and_differences(both, tight):
     """4 steps, checkpoints every 2: the GPU gradient against the oracle's
     (relative 1e-5) and against central differences of the GPU forward for
     two inflow modes, on the operator set solved to 1e-14 (fixture tight),
-    step 1e-4; the exact-solve check at step 1e-6 is the CPU test
-    (tests/test_flow_adjoint.py)."""
+    step 1e-4, relative 1e-6 (measured on the B200: 4e-10 and 1e-10); the
+    exact-solve check at step 1e-6 is the CPU test (tests/test_flow_adjoint.py)."""
     from lsstag_b200 import flow_adjoint as FA
     geom, dims, par, gpu, cpu = both
     u0, p0 = [geom["u_0"], geom["v_0"], geom["w_0"]], geom["p_0"]
@@ -128,7 +128,7 @@ def test_gradient_matches_oracle_and_differences(both, tight):
         e[k] = 1.0
         fd = _central(lambda th: ft.forward(th, f0, u0, p0), th0, e, 1e-4)
         print(f"mode {k}: adjoint {tth[k]:.10e}, central difference {fd:.10e}")
-        assert abs(tth[k] - fd) <= 1e-5 * abs(fd), (k, tth[k], fd)
+        assert abs(tth[k] - fd) <= 1e-6 * abs(fd), (k, tth[k], fd)
 
 
 def test_device_sweep_matches_host_sweep(both):
@@ -158,9 +158,9 @@ def test_gradient_ten_steps_checkpoints_every_five(both, tight):
     against central differences of the GPU forward: two inflow modes (step
     1e-4) and one random unit direction of the forcing field (step 3e-2: J
     moves 1e-4 as much per unit of forcing as per unit of inflow mode and is
-    close to quadratic in the forcing), relative 1e-5; and the same sweep
-    with checkpoints every 2 gives the same gradient (the recompute is
-    exact)."""
+    close to quadratic in the forcing), relative 1e-6 (measured on the B200:
+    1.4e-10, 1e-11, 4.5e-11); and the same sweep with checkpoints every 2
+    gives the same gradient (the recompute is exact)."""
     from lsstag_b200 import flow_adjoint as FA
     geom, dims, par, _, cpu = both
     _, gpu = tight
@@ -179,7 +179,7 @@ def test_gradient_ten_steps_checkpoints_every_five(both, tight):
         e[k] = 1.0
         fd = _central(lambda th: fwd.forward(th, f0, u0, p0), th0, e, 1e-4)
         print(f"10 steps, mode {k}: adjoint {gth[k]:.10e}, central difference {fd:.10e}")
-        assert abs(gth[k] - fd) <= 1e-5 * abs(fd), (k, gth[k], fd)
+        assert abs(gth[k] - fd) <= 1e-6 * abs(fd), (k, gth[k], fd)
     # a random forcing direction: d/ds J(f0 + s df) = <dJ/df, df>
     df = [rng.standard_normal(a.size) * (np.asarray(t) != 0) for a, t in zip(u0, cpu.stypes)]
     dfn = np.sqrt(sum(a @ a for a in df))
@@ -187,4 +187,4 @@ def test_gradient_ten_steps_checkpoints_every_five(both, tight):
     fdf = _central(lambda s: fwd.forward(th0, [a + s * b for a, b in zip(f0, df)], u0, p0), 0.0, 1.0, 3e-2)
     ad = sum(a @ b for a, b in zip(gf, df))
     print(f"10 steps, forcing direction: adjoint {ad:.10e}, central difference {fdf:.10e}")
-    assert abs(ad - fdf) <= 1e-5 * abs(fdf), (ad, fdf)
+    assert abs(ad - fdf) <= 1e-6 * abs(fdf), (ad, fdf)
