@@ -421,6 +421,25 @@ int lsg_momentum_cotangents_device(lsg_ctx* ctx, int dir, const double* vof, con
 /* out = in on the fluid faces of staggered grid dir, 0 on its solid faces
    (device pointers; in and out may alias). */
 int lsg_fluid_faces_device(lsg_ctx* ctx, int dir, const double* in, double* out);
+/* Transpose of the outflow clamps of SetSolutions::correction
+   (Base/set_solutions.h:87-118, :297-304) for the adjoint sweep: o = b with
+   the entries the clamps overwrite set to 0, decided from qx, qz (the x- and
+   z-velocities before the clamps): per interior (y, z) row of the east
+   outflow whose last or next-to-last x-face is negative, that x-face and
+   the matching y- and z-faces; bottom z-faces with positive and top ones
+   with negative velocity.  o may equal b.  Device pointers; needs the
+   context's grid (an operator). */
+int lsg_clamp_transpose_device(lsg_ctx* ctx, const double* qx, const double* qz, const double* bx,
+                               const double* by, const double* bz, double* ox, double* oy, double* oz);
+/* dst[dst_idx[e]] += coef[e] * src[src_idx[e]] * (src2 ? src2[src2_idx[e]] : 1)
+   for e < count: the boundary source terms' transposes of the adjoint sweep
+   (index sets built once by the caller).  FP64 atomic adds: entries sharing
+   a destination add in an unspecified order.  Device pointers. */
+int lsg_scatter_add_device(lsg_ctx* ctx, long long count, double* dst, const long long* dst_idx,
+                           const double* src, const long long* src_idx, const double* coef,
+                           const double* src2, const long long* src2_idx);
+/* y += alpha x on device vectors of n doubles. */
+int lsg_axpy_device(lsg_ctx* ctx, long long n, double alpha, const double* x, double* y);
 /* lsg_projection_adjoint on device pointers; outputs must not alias inputs. */
 int lsg_projection_adjoint_device(lsg_ctx* ctx, const double* ubar_out, const double* vbar_out,
                                   const double* wbar_out, const double* pbar_out, double coef, double* ubar,

@@ -644,4 +644,70 @@ __global__ void k_fluid_faces(long long n, const int* __restrict__ stype, const 
         out[i] = (stype[i] != 0) ? in[i] : 0.0;
 }
 
+// Transpose of the outflow clamps of SetSolutions::correction
+// (Base/set_solutions.h:87-118, :297-304): the clamps overwrite entries with
+// constants, so their transpose zeroes the cotangents of those entries.  q =
+// the velocities before the clamps decides which: per interior (y, z) row of
+// the east outflow (y in 1..M-2, z in 1..K-2), if the x-face value at the
+// row's last or next-to-last face is negative, that x-face and the matching
+// y- and z-faces; a bottom z-face (k = 0) with positive and a top one
+// (k = K-2) with negative velocity.  out holds a copy of the cotangents; the
+// two kernels zero the clamped entries in place.
+__global__ void k_clamp_transpose_east(int N, int M, int K, const double* __restrict__ qx, double* __restrict__ ox,
+                                       double* __restrict__ oy, double* __restrict__ oz)
+{
+    const long long rows = (long long)(M - 2) * (K - 2);
+    const int NM = N * M;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < 2 * rows;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int sh = (int)(e / rows);
+        const long long r = e - sh * rows;
+        const int zz = 1 + (int)(r / (M - 2)), yy = 1 + (int)(r % (M - 2));
+        const int num = (yy + 1) * N - 1 + zz * NM;         // last base cell of the row
+        const int num2 = num - yy - 1 - zz * M;             // its x-face
+        const int num3 = num - zz * N;                      // its y-face
+        if (qx[num2 - sh] < 0.0) {
+            ox[num2 - sh] = 0.0;
+            oy[num3 - sh] = 0.0;
+            oz[num - sh] = 0.0;
+        }
+    }
+}
+
+__global__ void k_clamp_transpose_tb(int N, int M, int K, const double* __restrict__ qz, double* __restrict__ oz)
+{
+    const long long faces = (long long)(N - 1) * (M - 1);
+    const int NM = N * M;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < faces;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int yy = 1 + (int)(e / (N - 1)), xx = 1 + (int)(e % (N - 1));
+        const int nb = xx + yy * N, nt = nb + (K - 2) * NM;
+        if (qz[nb] > 0.0) oz[nb] = 0.0;
+        if (qz[nt] < 0.0) oz[nt] = 0.0;
+    }
+}
+
+// dst[di[e]] += coef[e] * src[si[e]] * (src2 ? src2[s2i[e]] : 1): the
+// boundary source terms' transposes (index sets built once on the host).
+// FP64 atomic adds: entries that share a destination add in an unspecified
+// order.
+__global__ void k_scatter_add(long long count, double* dst, const long long* __restrict__ di,
+                              const double* __restrict__ src, const long long* __restrict__ si,
+                              const double* __restrict__ coef, const double* __restrict__ src2,
+                              const long long* __restrict__ s2i)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+         e += (long long)gridDim.x * blockDim.x) {
+        double v = coef[e] * src[si[e]];
+        if (src2) v *= src2[s2i[e]];
+        atomicAdd(dst + di[e], v);
+    }
+}
+
+__global__ void k_axpy(long long n, double alpha, const double* __restrict__ x, double* __restrict__ y)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] += alpha * x[i];
+}
+
 }  // namespace lsg

@@ -3425,6 +3425,67 @@ int lsg_fluid_faces_device(lsg_ctx* h, int dir, const double* in, double* out)
     LSG_API_END(h)
 }
 
+int lsg_clamp_transpose_device(lsg_ctx* h, const double* qx, const double* qz, const double* bx, const double* by,
+                               const double* bz, double* ox, double* oy, double* oz)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.have_matrix, LSG_ERR_STATE, "no grid (set an operator first)");
+    LSG_REQUIRE(qx && qz && bx && by && bz && ox && oy && oz, LSG_ERR_ARG, "null field");
+    LSG_CUDA(cudaSetDevice(C.device));
+    const Dims& d = C.d;
+    LSG_REQUIRE(d.N >= 2 && d.M >= 3 && d.K >= 3, LSG_ERR_ARG, "grid too small for the outflow clamps");
+    const long long nx = (long long)(d.N - 1) * d.M * d.K, ny = (long long)d.N * (d.M - 1) * d.K,
+                    nz = (long long)d.N * d.M * (d.K - 1);
+    if (ox != bx) LSG_CUDA(cudaMemcpyAsync(ox, bx, nx * sizeof(double), cudaMemcpyDeviceToDevice, C.s));
+    if (oy != by) LSG_CUDA(cudaMemcpyAsync(oy, by, ny * sizeof(double), cudaMemcpyDeviceToDevice, C.s));
+    if (oz != bz) LSG_CUDA(cudaMemcpyAsync(oz, bz, nz * sizeof(double), cudaMemcpyDeviceToDevice, C.s));
+    const long long rows = 2LL * (d.M - 2) * (d.K - 2);
+    k_clamp_transpose_east<<<grid_for(rows, 256), 256, 0, C.s>>>(d.N, d.M, d.K, qx, ox, oy, oz);
+    LSG_CHECK_LAUNCH();
+    const long long faces = (long long)(d.N - 1) * (d.M - 1);
+    k_clamp_transpose_tb<<<grid_for(faces, 256), 256, 0, C.s>>>(d.N, d.M, d.K, qz, oz);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_scatter_add_device(lsg_ctx* h, long long count, double* dst, const long long* dst_idx, const double* src,
+                           const long long* src_idx, const double* coef, const double* src2,
+                           const long long* src2_idx)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(count >= 0, LSG_ERR_ARG, "negative count");
+    if (count == 0) return LSG_OK;
+    LSG_REQUIRE(dst && dst_idx && src && src_idx && coef && (!src2 || src2_idx), LSG_ERR_ARG, "null array");
+    LSG_CUDA(cudaSetDevice(C.device));
+    k_scatter_add<<<grid_for(count, 256), 256, 0, C.s>>>(count, dst, dst_idx, src, src_idx, coef, src2, src2_idx);
+    LSG_CHECK_LAUNCH();
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_axpy_device(lsg_ctx* h, long long n, double alpha, const double* x, double* y)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(n >= 0 && x && y, LSG_ERR_ARG, "bad vector");
+    LSG_CUDA(cudaSetDevice(C.device));
+    if (n > 0) {
+        k_axpy<<<grid_for(n, 256), 256, 0, C.s>>>(n, alpha, x, y);
+        LSG_CHECK_LAUNCH();
+    }
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
 int lsg_gradient_transpose_device(lsg_ctx* h, const double* gx, const double* gy, const double* gz, double* out)
 {
     if (!h) return LSG_ERR_ARG;

@@ -75,7 +75,8 @@ EXPORTS = [
     "lsg_setup_times", "lsg_row_classes",
     "lsg_flow_create", "lsg_flow_destroy", "lsg_flow_last_error", "lsg_flow_set_state", "lsg_flow_step",
     "lsg_flow_state",
-    "lsg_momentum_cotangents_device", "lsg_fluid_faces_device",
+    "lsg_momentum_cotangents_device", "lsg_fluid_faces_device", "lsg_clamp_transpose_device",
+    "lsg_scatter_add_device", "lsg_axpy_device",
     "lsg_tecplot_sol_async", "lsg_tecplot_wait",
 ]
 
@@ -185,6 +186,9 @@ def load() -> C.CDLL:
     lib.lsg_flow_state.argtypes = [P, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.lsg_momentum_cotangents_device.argtypes = [P, C.c_int, P, P, C.c_double] + [P] * 6
     lib.lsg_fluid_faces_device.argtypes = [P, C.c_int, P, P]
+    lib.lsg_clamp_transpose_device.argtypes = [P] + [C.c_void_p] * 8
+    lib.lsg_scatter_add_device.argtypes = [P, C.c_longlong] + [C.c_void_p] * 7
+    lib.lsg_axpy_device.argtypes = [P, C.c_longlong, C.c_double, C.c_void_p, C.c_void_p]
     lib.lsg_version.restype = C.c_char_p
     _lib = lib
     return lib

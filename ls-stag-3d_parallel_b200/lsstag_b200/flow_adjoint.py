@@ -461,10 +461,13 @@ class FlowAdjoint:
 class FlowAdjointDevice:
     """FlowAdjoint with the state, the checkpoints, the segment records and
     every cotangent in device memory (torch CUDA tensors as buffers), the
-    work done by the *_device entry points on the contexts of a GpuFlowOps,
-    and the boundary transposes and clamp masks as index operations on the
-    device.  No host copies inside a step except the drag value and the
-    iteration counts.  Same arguments and results as FlowAdjoint."""
+    work done by the *_device entry points on the contexts of a GpuFlowOps:
+    the outflow clamps' transpose (lsg_clamp_transpose_device), the boundary
+    source terms' transposes as scatter-adds over index sets built once
+    (lsg_scatter_add_device) and the cotangent updates (lsg_axpy_device) are
+    library kernels too; torch only allocates the buffers.  No host copies
+    inside a step except the drag value and the iteration counts.  Same
+    arguments and results as FlowAdjoint."""
 
     def __init__(self, ops: GpuFlowOps, steps: int, every: int = 10, device: int = 0):
         import ctypes
@@ -483,10 +486,8 @@ class FlowAdjointDevice:
         self.vib, self.vibyx, self.vibzy = T(g["vib"]), T(g["vibyx"]), T(g["vibzy"])
         self.theta_g, self.delta_g = T(g["theta"]), T(g["delta"])
         self.vof = [T(v) for v in ops.vof]
-        self.fluid = [T(np.asarray(t) != 0, torch.bool) for t in ops.stypes]
-        self.fvof = [torch.where(f, v, torch.zeros_like(v)) for f, v in zip(self.fluid, self.vof)]
-        self.B = T(inflow_basis(M, K))
-        self.u_w0 = T(g["u_w"])
+        self.B = inflow_basis(M, K)
+        self.u_w0 = np.asarray(g["u_w"], dtype=np.float64)
         self.bc = np.ascontiguousarray(ops.bc, dtype=np.float64)
         self.bc_lap = np.ascontiguousarray(ops.bc_lap, dtype=np.float64)
         self._index_setup(g["theta"], g["delta"], g["bc"], ops.nu)
@@ -496,22 +497,33 @@ class FlowAdjointDevice:
         self.stats = {}
 
     def _index_setup(self, theta, delta, bc, nu):
-        """Index sets and coefficients of the boundary transposes and of the
-        clamp masks, as device tensors."""
+        """Index sets and coefficients of the boundary transposes, as device
+        tensors."""
         torch = self.torch
         T = self._t
         N, M, K = self.dims
         src = SourceTermTransposes(self.dims, theta, delta, bc, nu)
-        self.src = {k: (T(v, torch.int64) if np.asarray(v).dtype.kind in "iu" else T(v))
-                    for k, v in vars(src).items() if k != "dims"}
-        NM = N * M
-        zz, yy = np.meshgrid(np.arange(1, K - 1), np.arange(1, M - 1), indexing="ij")
-        zz, yy = zz.ravel(), yy.ravel()
-        num = (yy + 1) * N - 1 + zz * NM
-        self.cl_num, self.cl_num2, self.cl_num3 = (T(a, torch.int64) for a in (num, num - yy - 1 - zz * M, num - zz * N))
-        yy, xx = np.meshgrid(np.arange(1, M), np.arange(1, N), indexing="ij")
-        nb = (xx + yy * N).ravel()
-        self.cl_nb, self.cl_nt = T(nb, torch.int64), T(nb + (K - 2) * NM, torch.int64)
+        # the boundary source terms' transposes as scatter-adds (dst index,
+        # src index, coefficient, optional second factor's index), run by
+        # lsg_scatter_add_device
+        sc = {"cz_in0": (src.cz_in_w, src.cz_in, src.cz_in_c0, None),
+              "cz_in1": (src.cz_in_w + M, src.cz_in, src.cz_in_c1, None),
+              "cz_last_u0": (src.cz_last, src.cz_last, 0.25 * src.cz_dz * src.cz_dy, src.cz_u0),
+              "cz_last_u1": (src.cz_last, src.cz_last, 0.25 * src.cz_dzz * src.cz_dy, src.cz_u1),
+              "cz_u0": (src.cz_u0, src.cz_last, 0.25 * src.cz_dy * src.cz_dz, src.cz_last),
+              "cz_u1": (src.cz_u1, src.cz_last, 0.25 * src.cz_dy * src.cz_dzz, src.cz_last),
+              "cz_nb": (src.cz_nb, src.cz_nb, src.cz_cb, src.cz_nb),
+              "cz_nt": (src.cz_nt, src.cz_nt, src.cz_ct, src.cz_nt),
+              "hx": (src.hx_w, src.hx_row, -src.hx_c, None),
+              "lap_out": (src.lap_out_u, src.lap_out, src.lap_out_c, None),
+              "lap_in": (src.lap_in_w, src.lap_in, src.lap_in_c, None)}
+        self.sc = {k: (T(di, torch.int64), T(si, torch.int64), T(c), None if s2 is None else T(s2, torch.int64))
+                   for k, (di, si, c, s2) in sc.items()}
+        # (smallest index, end of each index set) for the host-side bounds
+        # check of every scatter
+        rng_ = lambda a: (int(np.min(a)), int(np.max(a)) + 1) if np.size(a) else (0, 0)   # noqa: E731
+        self.sc_bounds = {k: (rng_(di), rng_(si), None if s2 is None else rng_(s2))
+                          for k, (di, si, c, s2) in sc.items()}
 
     # -- helpers ---------------------------------------------------------------
     def _t(self, a, dtype=None):
@@ -536,6 +548,22 @@ class FlowAdjointDevice:
     def _zeros(self, n):
         return self.torch.zeros(n, dtype=self.torch.float64, device=self.dev)
 
+    def _scatter(self, key, dst, src, src2=None):
+        """dst[di] += coef * src[si] (* src2[s2i]) with the index set `key`."""
+        pr = self.ops.pres
+        di, si, c, s2i = self.sc[key]
+        bd, bs, bs2 = self.sc_bounds[key]
+        assert bd[0] >= 0 and bd[1] <= dst.numel() and bs[0] >= 0 and bs[1] <= src.numel(), key
+        assert (src2 is None) == (s2i is None), key
+        assert src2 is None or (bs2[0] >= 0 and bs2[1] <= src2.numel()), key
+        pr.ctx.check(pr.ctx.lib.lsg_scatter_add_device(
+            pr.ctx.h, di.numel(), self._p(dst), self._p(di), self._p(src), self._p(si), self._p(c),
+            None if src2 is None else self._p(src2), None if src2 is None else self._p(s2i)))
+
+    def _axpy(self, alpha, x, y):
+        pr = self.ops.pres
+        pr.ctx.check(pr.ctx.lib.lsg_axpy_device(pr.ctx.h, y.numel(), float(alpha), self._p(x), self._p(y)))
+
     def _vel(self, u):
         return [self._p(u[d], self.gsize[d]) for d in range(3)]
 
@@ -550,9 +578,9 @@ class FlowAdjointDevice:
 
     # -- forward ---------------------------------------------------------------
     def _set_inflow(self, theta):
-        th = self._t(np.zeros(self.B.shape[0]) if theta is None else theta)
-        self.u_w = (self.u_w0 + th @ self.B).contiguous()
-        self.ops.set_inflow(self.u_w.cpu().numpy())
+        u_w = self.u_w0 if theta is None else self.u_w0 + np.asarray(theta, dtype=np.float64) @ self.B
+        self.u_w = self._t(u_w)
+        self.ops.set_inflow(u_w)
         self.hflux = [self._t(h) for h in self.ops.hflux]
 
     def _conv(self, d, u):
@@ -575,18 +603,6 @@ class FlowAdjointDevice:
         u = [self._t(a) for a in u0]
         return (u, [a.clone() for a in u], self._t(p0), [self._conv(d, u) for d in range(3)])
 
-    def _masks(self, q):
-        torch = self.torch
-        mx, my, mz = (torch.zeros(n, dtype=torch.bool, device=self.dev) for n in self.gsize)
-        for sh in (0, 1):
-            hit = q[0][self.cl_num2 - sh] < 0.0
-            mx[(self.cl_num2 - sh)[hit]] = True
-            my[(self.cl_num3 - sh)[hit]] = True
-            mz[(self.cl_num - sh)[hit]] = True
-        mz[self.cl_nb[q[2][self.cl_nb] > 0.0]] = True
-        mz[self.cl_nt[q[2][self.cl_nt] < 0.0]] = True
-        return mx, my, mz
-
     def _step(self, st, forcing, rec=None):
         from . import _lib as L
         ops, par = self.ops, self.ops.par
@@ -607,7 +623,7 @@ class FlowAdjointDevice:
                                                      self._p(right), self._p(aux), self._p(gpw)))
             self._sync()
             if forcing is not None:
-                right += self.fvof[d] * forcing[d]
+                self._axpy(1.0, forcing[d], right)         # forcing[d] = vof-weighted forcing field
             x = u[d].clone()
             self._solve(ops.mom[d], right, x)
             s.append(x)
@@ -628,7 +644,7 @@ class FlowAdjointDevice:
                                                            self._p(pq, self.n), float(par["coef"]),
                                                            float(par["vbase"]), 0))
             self._sync()
-            rec.append((u, self._masks(q)))
+            rec.append((u, q))
         self._sync()
         return (unew, u, pnew, c)
 
@@ -640,7 +656,12 @@ class FlowAdjointDevice:
         return float(r.coef[0])
 
     def _forcing(self, forcing):
-        return None if forcing is None else [self._t(f) for f in forcing]
+        """The forcing field weighted by the fluid faces' volumes (the term the
+        momentum right-hand side adds), uploaded once per call."""
+        if forcing is None:
+            return None
+        return [self._t(np.where(np.asarray(f_) != 0, v, 0.0) * np.asarray(f, dtype=np.float64))
+                for f_, v, f in zip(self.ops.stypes, self.ops.vof, forcing)]
 
     def forward(self, theta, forcing, u0, p0) -> float:
         self._set_inflow(theta)
@@ -658,18 +679,16 @@ class FlowAdjointDevice:
 
     # -- reverse ---------------------------------------------------------------
     def _conv_flux_T(self, cbar, ux, uz, ub, uwb):
-        s = self.src
-        cin = cbar[s["cz_in"]]
-        uwb.index_add_(0, s["cz_in_w"], cin * s["cz_in_c0"])
-        uwb.index_add_(0, s["cz_in_w"] + self.dims[1], cin * s["cz_in_c1"])
-        cl = cbar[s["cz_last"]]
-        ub[2].index_add_(0, s["cz_last"], cl * 0.25 * (ux[s["cz_u0"]] * s["cz_dz"] + ux[s["cz_u1"]] * s["cz_dzz"])
-                         * s["cz_dy"])
-        w = cl * 0.25 * uz[s["cz_last"]] * s["cz_dy"]
-        ub[0].index_add_(0, s["cz_u0"], w * s["cz_dz"])
-        ub[0].index_add_(0, s["cz_u1"], w * s["cz_dzz"])
-        ub[2].index_add_(0, s["cz_nb"], cbar[s["cz_nb"]] * s["cz_cb"] * uz[s["cz_nb"]])
-        ub[2].index_add_(0, s["cz_nt"], cbar[s["cz_nt"]] * s["cz_ct"] * uz[s["cz_nt"]])
+        """(u_x, u_z, u_w) cotangents of <cbar, flux2_z(u, u_w)> added into
+        (ub[0], ub[2], uwb), as SourceTermTransposes.convective_flux_T."""
+        self._scatter("cz_in0", uwb, cbar)
+        self._scatter("cz_in1", uwb, cbar)
+        self._scatter("cz_last_u0", ub[2], cbar, ux)
+        self._scatter("cz_last_u1", ub[2], cbar, ux)
+        self._scatter("cz_u0", ub[0], cbar, uz)
+        self._scatter("cz_u1", ub[0], cbar, uz)
+        self._scatter("cz_nb", ub[2], cbar, uz)
+        self._scatter("cz_nt", ub[2], cbar, uz)
 
     def gradient(self, theta, forcing, u0, p0):
         """(J, dJ/dtheta, dJ/df): host numpy results, as FlowAdjoint.gradient."""
@@ -678,16 +697,17 @@ class FlowAdjointDevice:
         ops = self.ops
         pr = ops.pres
         lib = pr.ctx.lib
-        s = self.src
         J = self.forward(theta, forcing, u0, p0)
         fr = self._forcing(forcing)
         co2, coef = float(ops.par["coef2"]), float(ops.par["coef"])
         z = lambda a: torch.zeros_like(a)                                    # noqa: E731
-        ub = [torch.where(f, a, z(a)) for f, a in zip(self.fluid, self.gu)]
+        ub = [self._empty(n) for n in self.gsize]
+        for d in range(3):
+            pr.ctx.check(lib.lsg_fluid_faces_device(pr.ctx.h, d, self._p(self.gu[d]), self._p(ub[d])))
         upb = [z(a) for a in ub]
         pb = self.gp.clone()
         pab = [z(a) for a in ub]
-        uwb = self._zeros(self.u_w0.numel())
+        uwb = self._zeros(self.u_w0.size)
         fb = [z(a) for a in ub]
         starts = sorted(self.checkpoints)
         recomputed = 0
@@ -699,8 +719,10 @@ class FlowAdjointDevice:
                 st = self._step(st, fr, rec)
                 recomputed += 1
             for n in reversed(range(n0, n1)):
-                un, masks = rec[n - n0]
-                qb = [torch.where(m, z(a), a).contiguous() for m, a in zip(masks, ub)]
+                un, q = rec[n - n0]
+                qb = [self._empty(m) for m in self.gsize]
+                pr.ctx.check(lib.lsg_clamp_transpose_device(pr.ctx.h, self._p(q[0]), self._p(q[2]), *self._vel(ub),
+                                                            *self._vel(qb)))
                 sb = [self._empty(m) for m in self.gsize]
                 Lb = self._empty(self.n)
                 stt = L.Stats()
@@ -723,11 +745,11 @@ class FlowAdjointDevice:
                         pr.ctx.h, d, self._p(self.vof[d]), self._p(rsol), co2, self._p(rb), self._p(fb[d]),
                         self._p(ub_in[d]), self._p(upb[d]), self._p(pab[d]), self._p(cb[d])))
                     rs.append(rb)
-                uwb.index_add_(0, s["hx_w"], (-rs[0])[s["hx_row"]] * s["hx_c"])
+                self._scatter("hx", uwb, rs[0])
                 gT = self._empty(self.n)
                 self._sync()
                 pr.ctx.check(lib.lsg_gradient_transpose_device(pr.ctx.h, *self._vel(rs), self._p(gT)))
-                pb = pb - gT
+                self._axpy(-1.0, gT, pb)
                 for d in range(3):
                     self._sync()
                     pr.ctx.check(lib.lsg_convective_adjoint_device(pr.ctx.h, d, *self._vel(un), self._p(un[d]),
@@ -735,12 +757,12 @@ class FlowAdjointDevice:
                                                                    *self._vel(ub_in), self._p(ub_in[d]), 1))
                 self._sync()
                 self._conv_flux_T(cb[2], un[0], un[2], ub_in, uwb)
-                ub_in[0].index_add_(0, s["lap_out_u"], Lb[s["lap_out"]] * s["lap_out_c"])
-                uwb.index_add_(0, s["lap_in_w"], Lb[s["lap_in"]] * s["lap_in_c"])
+                self._scatter("lap_out", ub_in[0], Lb)
+                self._scatter("lap_in", uwb, Lb)
                 if n >= 1:
                     for d in range(3):
-                        ub_in[d] += self.gu[d]
-                    pb = pb + self.gp
+                        self._axpy(1.0, self.gu[d], ub_in[d])
+                    self._axpy(1.0, self.gp, pb)
                 ub = [self._empty(n) for n in self.gsize]
                 for d in range(3):
                     pr.ctx.check(lib.lsg_fluid_faces_device(pr.ctx.h, d, self._p(ub_in[d]), self._p(ub[d])))
@@ -750,4 +772,4 @@ class FlowAdjointDevice:
         self._conv_flux_T(pab[2], u0v[0], u0v[2], tmp, uwb)
         self._sync()
         self.stats = {"recomputed_steps": recomputed, "checkpoints": len(starts)}
-        return J, (self.B @ uwb).cpu().numpy(), [f.cpu().numpy() for f in fb]
+        return J, self.B @ uwb.cpu().numpy(), [f.cpu().numpy() for f in fb]

@@ -227,9 +227,11 @@ def test_flow_case_carries_the_drag_inputs():
     assert np.isfinite(tot) and tot > 0
 
 
-def test_device_sweep_index_operations_match_host(case):
-    """FlowAdjointDevice's clamp masks and boundary transposes (torch index
-    operations) against the host versions, run here on CPU tensors."""
+def test_device_sweep_scatter_sets_match_host(case):
+    """FlowAdjointDevice's boundary transposes are scatter-adds
+    dst[di] += coef * src[si] (* src2[s2i]) run by lsg_scatter_add_device;
+    the index sets it builds, applied here with numpy on the CPU, give
+    SourceTermTransposes' laplace, helmholtz and convective flux transposes."""
     import torch
     geom, dims, par, ops = case
     N, M, K = dims
@@ -240,15 +242,39 @@ def test_device_sweep_index_operations_match_host(case):
     bc[12] = 0.7
     fd._index_setup(geom["theta"], geom["delta"], bc, par["nu"])
     src = FA.SourceTermTransposes(dims, geom["theta"], geom["delta"], bc, par["nu"])
+
+    def scatter(key, dst, v, v2=None):
+        di, si, c, s2i = (None if t is None else t.numpy() for t in fd.sc[key])
+        # every index inside its buffer (the device kernel does no bounds check)
+        assert di.min() >= 0 and di.max() < dst.size and si.min() >= 0 and si.max() < v.size, key
+        assert (v2 is None) == (s2i is None) and (v2 is None or (s2i.min() >= 0 and s2i.max() < v2.size)), key
+        assert di.size == si.size == c.size
+        w = c * v[si]
+        if v2 is not None:
+            w = w * v2[s2i]
+        np.add.at(dst, di, w)
+
     rng = np.random.default_rng(9)
-    q = [rng.standard_normal(n) for n in fd.gsize]
-    for a, b in zip(fd._masks([fd._t(v) for v in q]), FA.outflow_clamp_mask(dims, *q)):
-        assert np.array_equal(a.numpy(), b)
     cb, ux, uz = rng.standard_normal(fd.gsize[2]), rng.standard_normal(fd.gsize[0]), rng.standard_normal(fd.gsize[2])
-    ub = [torch.zeros(n, dtype=torch.float64) for n in fd.gsize]
-    uwb = torch.zeros(M * K, dtype=torch.float64)
-    fd._conv_flux_T(fd._t(cb), fd._t(ux), fd._t(uz), ub, uwb)
-    hx, hz, hw = src.convective_flux_T(cb, ux, uz)
-    assert np.allclose(ub[0].numpy(), hx, rtol=1e-13, atol=1e-15)
-    assert np.allclose(ub[2].numpy(), hz, rtol=1e-13, atol=1e-15)
-    assert np.allclose(uwb.numpy(), hw, rtol=1e-13, atol=1e-15)
+    uxb, uzb, uwb = np.zeros(fd.gsize[0]), np.zeros(fd.gsize[2]), np.zeros(M * K)
+    scatter("cz_in0", uwb, cb)
+    scatter("cz_in1", uwb, cb)
+    scatter("cz_last_u0", uzb, cb, ux)
+    scatter("cz_last_u1", uzb, cb, ux)
+    scatter("cz_u0", uxb, cb, uz)
+    scatter("cz_u1", uxb, cb, uz)
+    scatter("cz_nb", uzb, cb, uz)
+    scatter("cz_nt", uzb, cb, uz)
+    for a, b in zip((uxb, uzb, uwb), src.convective_flux_T(cb, ux, uz)):
+        assert np.allclose(a, b, rtol=1e-13, atol=1e-15)
+    Lb = rng.standard_normal(N * M * K)
+    lx, lw = np.zeros(fd.gsize[0]), np.zeros(M * K)
+    scatter("lap_out", lx, Lb)
+    scatter("lap_in", lw, Lb)
+    hx_, hw_ = src.laplace_flux_T(Lb)
+    assert np.allclose(lx, hx_, rtol=1e-13, atol=1e-15) and np.allclose(lw, hw_, rtol=1e-13, atol=1e-15)
+    hb = rng.standard_normal(fd.gsize[0])
+    hw = np.zeros(M * K)
+    scatter("hx", hw, hb)
+    # FlowAdjointDevice subtracts the x-momentum cotangents' flux term
+    assert np.allclose(hw, -src.helmholtz_flux_T(hb), rtol=1e-13, atol=1e-15)
