@@ -933,24 +933,37 @@ static int seg_cells(int L)
     return 0;
 }
 
+// Segment length of the fused x-line step: N = SEG * P with P <= 32 lanes, P a
+// power of two, 8-cell segments where they fit (lines of 8..256), else 12-cell
+// ones (12..384); 0 = neither.
+static int xseg_cells(int N)
+{
+    for (int seg : {8, 12}) {
+        if (N % seg) continue;
+        const int P = N / seg;
+        if (P <= 32 && (P & (P - 1)) == 0) return seg;
+    }
+    return 0;
+}
+
 // Whether a level with these dimensions and stencil runs the fused ADLJ
 // direction steps: the fine 7-point stencil (offsets b, s, w, p, e, n, t),
-// x-lines of 8-cell segments on P <= 32 lanes (P a power of two), y- and
-// z-lines in the segmented kernel's shapes.
+// x-lines of 8- or 12-cell segments on P <= 32 lanes (P a power of two), y-
+// and z-lines in the segmented kernel's shapes.
 template <typename T>
 static bool adlj_fused_level(const Dims& g, int noff, const std::vector<int>& off, const lsg_options& o)
 {
     if (o.smoother != LSG_SMOOTHER_ADLJ) return false;
     if (!(o.adlj_schedule == LSG_ADLJ_FUSED || (o.adlj_schedule == LSG_ADLJ_AUTO && sizeof(T) == 4))) return false;
     if (noff != 7 || off.size() < 3 || off[0] != 0 || off[1] != 0 || off[2] != -1) return false;
-    if (g.N < 2 || g.M < 2 || g.K < 2 || g.N % 8) return false;
-    const int P = g.N / 8;
-    if (P > 32 || (P & (P - 1))) return false;
+    if (g.N < 2 || g.M < 2 || g.K < 2 || !xseg_cells(g.N)) return false;
     return seg_cells<T>(g.M) != 0 && seg_cells<T>(g.K) != 0;
 }
 
 // The fused y (DIR 1) or z (DIR 2) step in the form VAR of k_adlj_fused_seg:
-// W lines x S segments per CTA of at most MAXT threads.
+// W lines x S segments per CTA of at most MAXT threads.  FP32 y-lines of more
+// than 32 8-cell segments keep 8-cell segments while they fit (at 384^3: 558
+// against 868 us with 12-cell ones; z-lines the other way, 587 against 830 us).
 template <typename T, int DIR, int VAR>
 static void launch_fused_seg(const LevelT<T>& lv, bool zq, T omega, cudaStream_t s, const T* dinv, const T* xin,
                              T* xout)
@@ -959,7 +972,7 @@ static void launch_fused_seg(const LevelT<T>& lv, bool zq, T omega, cudaStream_t
     const Dims& g = lv.d;
     const int L = DIR == 1 ? g.M : g.K;
     const long long rows = DIR == 1 ? g.K : g.M;
-    const int seg = seg_cells<T>(L);
+    const int seg = (sizeof(T) == 4 && DIR == 1 && 8 * ((L + 7) / 8) <= MAXT) ? 8 : seg_cells<T>(L);
     const int S = (L + seg - 1) / seg;
     int W = 8;                                             // lanes per line row: a divisor of 32
     while (W < 32 && 2 * W * S <= MAXT) W *= 2;
@@ -991,10 +1004,16 @@ static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cu
     const T* b = lv.r.p;
     const T* dinv = lv.dinv[d].p;
     if (d == 0) {
-        const int P = g.N / 8;
+        const int seg = xseg_cells(g.N);
+        const int P = g.N / seg;
         const long long threads = (long long)g.M * g.K * P;
-        k_adlj_fused_xseg<T, 8><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g.N, g.M, g.K, P, lv.cls, lv.dict,
-                                                                                dinv, b, xin, xout, omega);
+        if (seg == 8)
+            k_adlj_fused_xseg<T, 8><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g.N, g.M, g.K, P, lv.cls,
+                                                                                    lv.dict, dinv, b, xin, xout, omega);
+        else
+            k_adlj_fused_xseg<T, 12><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g.N, g.M, g.K, P, lv.cls,
+                                                                                     lv.dict, dinv, b, xin, xout,
+                                                                                     omega);
     } else {
         const bool zq = d == 2 && zquirk;
         if (scan) {

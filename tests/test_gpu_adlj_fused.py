@@ -22,11 +22,14 @@ def _csr(g):
     return (g["A_rowptr"], g["A_col"], g["A_val"], tuple(int(v) for v in g["dims"]))
 
 
+@pytest.mark.parametrize("case", ["sphere16", "spheres4_24"])
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
-def test_vcycle_matches_reference_schedule_sphere16(prec):
+def test_vcycle_matches_reference_schedule_sphere16(prec, case):
+    """sphere16 splits its x-lines into 8-cell segments (2 lanes), spheres4_24
+    into 12-cell ones (2 lanes)."""
     from lsstag_b200 import _lib as L
     from lsstag_b200 import solver as S
-    g = load_golden("sphere16")
+    g = load_golden(case)
     p = L.FP64 if prec == "fp64" else L.FP32
     out, its = [], []
     for sched in (L.ADLJ_FUSED, L.ADLJ_REFERENCE):
@@ -37,7 +40,7 @@ def test_vcycle_matches_reference_schedule_sphere16(prec):
         its.append(s.solve(g["b"], x))
         s.close()
     rel = np.linalg.norm(out[0] - out[1]) / np.linalg.norm(out[1])
-    print(f"sphere16 {prec}: one V-cycle, fused vs reference schedule, relative {rel:.2e}; iterations {its}")
+    print(f"{case} {prec}: one V-cycle, fused vs reference schedule, relative {rel:.2e}; iterations {its}")
     assert rel <= (1e-12 if prec == "fp64" else 1e-5)
     assert abs(its[0] - its[1]) <= 1
     assert its[1] == int(g["fgmres_it"][0]) or prec == "fp32"
