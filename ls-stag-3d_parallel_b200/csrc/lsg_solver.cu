@@ -935,10 +935,10 @@ static int seg_cells(int L)
 
 // Segment length of the fused x-line step: N = SEG * P with P <= 32 lanes, P a
 // power of two, 8-cell segments where they fit (lines of 8..256), else 12-cell
-// ones (12..384); 0 = neither.
+// ones (12..384), else 16-cell ones (16..512); 0 = none.
 static int xseg_cells(int N)
 {
-    for (int seg : {8, 12}) {
+    for (int seg : {8, 12, 16}) {
         if (N % seg) continue;
         const int P = N / seg;
         if (P <= 32 && (P & (P - 1)) == 0) return seg;
@@ -948,8 +948,8 @@ static int xseg_cells(int N)
 
 // Whether a level with these dimensions and stencil runs the fused ADLJ
 // direction steps: the fine 7-point stencil (offsets b, s, w, p, e, n, t),
-// x-lines of 8- or 12-cell segments on P <= 32 lanes (P a power of two), y-
-// and z-lines in the segmented kernel's shapes.
+// x-lines of 8-, 12- or 16-cell segments on P <= 32 lanes (P a power of two),
+// y- and z-lines in the segmented kernel's shapes.
 template <typename T>
 static bool adlj_fused_level(const Dims& g, int noff, const std::vector<int>& off, const lsg_options& o)
 {
@@ -1010,8 +1010,12 @@ static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cu
         if (seg == 8)
             k_adlj_fused_xseg<T, 8><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g.N, g.M, g.K, P, lv.cls,
                                                                                     lv.dict, dinv, b, xin, xout, omega);
-        else
+        else if (seg == 12)
             k_adlj_fused_xseg<T, 12><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g.N, g.M, g.K, P, lv.cls,
+                                                                                     lv.dict, dinv, b, xin, xout,
+                                                                                     omega);
+        else
+            k_adlj_fused_xseg<T, 16><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(g.N, g.M, g.K, P, lv.cls,
                                                                                      lv.dict, dinv, b, xin, xout,
                                                                                      omega);
     } else {

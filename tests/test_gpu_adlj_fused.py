@@ -81,6 +81,53 @@ def test_vcycle_and_solve_128(case128, prec):
     assert dx <= 1e-6
 
 
+def _long_case(dims, seed=3):
+    """(planes, rhs) of the four seeded spheres in the unit cube on an
+    N x M x K grid, operator built on the GPU (as cases.build_on_device)."""
+    from lsstag_b200 import cases, mesh as MS, solver as S, synth
+    N, M, K = dims
+    h = (1.0 / N, 1.0 / M, 1.0 / K)
+    sph = synth.four_spheres(seed)
+    pins = np.array([N - 1, N * M - 1], dtype=np.int64)
+    s = S.MGFGMRES()
+    try:
+        s.build_mesh(dims, h, MS.flow_block(dims, h, sph), bodies=MS.bodies_array(sph))
+        s.set_from_mesh(pins, setup=False)
+        P = s.planes()
+        solid = s.mesh_get("celltype") == 0
+    finally:
+        s.close()
+    mask = cases.fluid_mask_from_planes(P, dims, pins)
+    return P, synth.poisson_rhs(seed, np.where(solid, 0, 1), pins, mask)
+
+
+@pytest.mark.parametrize("dims", [(512, 16, 16), (384, 16, 16), (16, 384, 16), (16, 16, 384)])
+def test_long_lines_fused_match_reference_schedule(dims):
+    """Lines longer than 256 cells in the FP32 cycle: x-lines of 512 in
+    16-cell segments and of 384 in 12-cell ones (32 lanes), y-lines of 384 in
+    8-cell segments (48 per line), z-lines of 384 in 12-cell ones; one
+    V-cycle against the reference's schedule to FP32 rounding, the same
+    iterations to the same 1e-10 relative residual."""
+    from lsstag_b200 import _lib as L
+    from lsstag_b200 import solver as S
+    P, b = _long_case(dims)
+    tol = 1e-10 * float(np.linalg.norm(b))
+    out, its = [], []
+    for sched in (L.ADLJ_FUSED, L.ADLJ_REFERENCE):
+        s = S.MGFGMRES(mg_precision=L.FP32, adlj_schedule=sched)
+        s.set_planes(P, dims, S.Task(eps=tol, FGMRES_RESTART_NUM=30, MAX_ITER=200))
+        out.append(s.precondition(b))
+        x = np.zeros(b.size)
+        its.append(s.solve(b, x))
+        assert s.status == L.LSG_OK
+        assert s.stats.true_residual <= 1.5 * tol
+        s.close()
+    rel = np.linalg.norm(out[0] - out[1]) / np.linalg.norm(out[1])
+    print(f"{dims} FP32: one V-cycle, fused vs reference schedule, relative {rel:.2e}; iterations {its}")
+    assert rel <= 1e-5
+    assert abs(its[0] - its[1]) <= 1
+
+
 def test_fused_steps_profiled_128(case128):
     """Kernel ids 9/10/11 (the fused x/y/z steps on the finest level) run
     and report their algorithmic bytes (4w + 4 per cell); the reference
