@@ -62,7 +62,9 @@ __device__ __forceinline__ T resid7_at(int N, int M, int K, long long q, const i
 // maps of the forward and backward recurrences are composed across the
 // segments: by log-step scans in shared memory when VAR & 1 (the solve's
 // form), else by each thread walking the maps before its own (timing
-// comparison).  zquirk (DIR 2): the first right-hand side of the z-line
+// comparison).  VAR & 2: the line splits into whole segments (L = S SEG),
+// so no cell lies past its end and the line-end guards go.  zquirk (DIR 2):
+// the first right-hand side of the z-line
 // (x, y) is the residual at cell y*N*K + x, where the reference reads it
 // (smoother_adlj_z.h:54-58).  Shared memory: 4 W S values.
 template <typename T, int DIR, int SEG, int MAXT, int MINB, int VAR>
@@ -73,6 +75,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 {
     static_assert(DIR == 1 || DIR == 2, "y- or z-lines");
     constexpr bool LOGSCAN = (VAR & 1) != 0;
+    constexpr bool EXACT = (VAR & 2) != 0;                 // L = S * SEG: no cell past the line end
     extern __shared__ __align__(16) unsigned char fseg_smem[];
     const int W = blockDim.x, S = blockDim.y;
     T* sA = reinterpret_cast<T*>(fseg_smem);               // 2 buffers of W*S each
@@ -96,7 +99,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
     T rv[SEG], dv[SEG], xc[SEG];
 #pragma unroll
     for (int u = 0; u < SEG; u++) {
-        const int t = min(t0 + u, L - 1);
+        const int t = EXACT ? t0 + u : min(t0 + u, L - 1);
         const int i = i0 + t * st;
         cl[u] = cls[i];
         rv[u] = b[i];
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
         const int t = t0 + u;
         lv[u] = 0;
         uv[u] = 0;
-        if (t < L) {
+        if (EXACT || t < L) {
             const int i = i0 + t * st;
             const T* a = dict + (size_t)cl[u] * 7;
             const T xw = hw ? xin[i - 1] : (T)0;
@@ -152,7 +155,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
     for (int u = 0; u < SEG; u++) {
         const int t = t0 + u;
-        if (t < L) {
+        if (EXACT || t < L) {
             if (t == 0) {
                 fa = rv[u] * dv[u];
                 fb = 0;
@@ -180,7 +183,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
     for (int u = SEG - 1; u >= 0; u--) {
         const int t = t0 + u;
-        if (t < L) {
+        if (EXACT || t < L) {
             const T yv = rv[u] + lv[u] * yin;
             if (t == L - 1) {
                 gg = yv;
@@ -207,7 +210,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
         for (int u = 0; u < SEG; u++) {
             const int t = t0 + u;
-            if (t < L) {
+            if (EXACT || t < L) {
                 const T cv = omega * (rv[u] + lv[u] * xo);
                 xout[i0 + t * st] = xc[u] + cv;
             }

@@ -1021,8 +1021,17 @@ static void adlj_fused_step(const LevelT<T>& lv, int d, bool zquirk, T omega, cu
     } else {
         const bool zq = d == 2 && zquirk;
         if (scan) {
-            if (d == 1) launch_fused_seg<T, 1, 1>(lv, false, omega, s, dinv, xin, xout);
-            else launch_fused_seg<T, 2, 1>(lv, zq, omega, s, dinv, xin, xout);
+            // y-lines that split into whole segments drop the line-end guards
+            // (256^3 FP32: 112 against 131 us; the z step measured 140
+            // against 135 us that way and keeps them)
+            const int L = g.M;
+            const int sgl = (sizeof(T) == 4 && 8 * ((L + 7) / 8) <= 512) ? 8 : seg_cells<T>(L);
+            if (d == 1) {
+                if (L % sgl == 0) launch_fused_seg<T, 1, 3>(lv, false, omega, s, dinv, xin, xout);
+                else launch_fused_seg<T, 1, 1>(lv, false, omega, s, dinv, xin, xout);
+            } else {
+                launch_fused_seg<T, 2, 1>(lv, zq, omega, s, dinv, xin, xout);
+            }
         } else {
             if (d == 1) launch_fused_seg<T, 1, 0>(lv, false, omega, s, dinv, xin, xout);
             else launch_fused_seg<T, 2, 0>(lv, zq, omega, s, dinv, xin, xout);
