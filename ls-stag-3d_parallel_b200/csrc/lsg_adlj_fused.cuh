@@ -31,18 +31,17 @@
 
 namespace lsg {
 
-// b - A x at flat cell q, every neighbour read from memory (the z-line
-// quirk's right-hand side cell).  Terms summed p, b, s, w, e, n, t.
+// b - A x at flat cell q with row class c, every neighbour read from memory
+// (the z-line quirk's right-hand side cell).  Terms summed p, b, s, w, e, n, t.
 template <typename T, int RS>
-__device__ __forceinline__ T resid7_at(int N, int M, int K, long long q, const int* __restrict__ cls,
-                                       const T* __restrict__ dict, const T* __restrict__ b,
-                                       const T* __restrict__ x)
+__device__ __forceinline__ T resid7_at_class(int N, int M, int K, long long q, int c, const T* __restrict__ dict,
+                                             const T* __restrict__ b, const T* __restrict__ x)
 {
     const int NM = N * M;
     const int qz = (int)(q / NM);
     const int rem = (int)(q - (long long)qz * NM);
     const int qy = rem / N, qx = rem - qy * N;
-    const T* a = dict + (size_t)cls[q] * RS;
+    const T* a = dict + (size_t)c * RS;
     T acc = a[3] * x[q];
     if (qz > 0) acc += a[0] * x[q - NM];
     if (qy > 0) acc += a[1] * x[q - N];
@@ -51,6 +50,14 @@ __device__ __forceinline__ T resid7_at(int N, int M, int K, long long q, const i
     if (qy < M - 1) acc += a[5] * x[q + N];
     if (qz < K - 1) acc += a[6] * x[q + NM];
     return b[q] - acc;
+}
+
+template <typename T, int RS>
+__device__ __forceinline__ T resid7_at(int N, int M, int K, long long q, const int* __restrict__ cls,
+                                       const T* __restrict__ dict, const T* __restrict__ b,
+                                       const T* __restrict__ x)
+{
+    return resid7_at_class<T, RS>(N, M, K, q, cls[q], dict, b, x);
 }
 
 // y-lines (DIR 1) and z-lines (DIR 2), segmented like k_tdma_seg: a CTA holds
@@ -94,6 +101,10 @@ __global__ void __launch_bounds__(MAXT, MINB)
     const int i0 = DIR == 1 ? row * NM + xs : row * N + xs;
     const int t0 = sg * SEG;
     const bool hw = xs > 0, he = xs < N - 1, hm = row > 0, hp = row < rows - 1;
+    // the z-line quirk's cell y*N*K + x: its row class is read now, so the
+    // residual there (after phase 2) starts from a class already in hand
+    int qcl = 0;
+    if (DIR == 2 && zquirk && sg == 0) qcl = cls[(long long)row * N * K + xs];
     // phase 1: the segment's own streams
     int cl[SEG];
     T rv[SEG], dv[SEG], xc[SEG];
@@ -149,7 +160,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
         }
     }
     if (DIR == 2 && zquirk && sg == 0)
-        rv[0] = resid7_at<T, 7>(N, M, K, (long long)row * N * K + xs, cls, dict, b, xin);
+        rv[0] = resid7_at_class<T, 7>(N, M, K, (long long)row * N * K + xs, qcl, dict, b, xin);
     // forward, relative to y_in
     T fa = 0, fb = 1;
 #pragma unroll
