@@ -134,4 +134,141 @@ __global__ void k_ilu_bwd(int level, int N, int M, int K, const double* __restri
     }
 }
 
+// Both triangular sweeps of one ILU(0) application in one cooperative launch
+// (every CTA resident): the hyperplanes of the forward sweep, then those of
+// the backward sweep, each thread owning the (x, y) columns t, t + T, ...
+// (at most CMAX) for every plane, with the arithmetic of k_ilu_fwd /
+// k_ilu_bwd (so the same bits) and a grid-wide barrier between consecutive
+// planes instead of a kernel boundary.  A plane's operands that do not
+// depend on the previous plane (b or y, the factor entries, the pivot) are
+// loaded before the barrier that ends the previous plane, so after it only
+// the neighbours just written remain to fetch (through L2, __ldcg: other
+// CTAs wrote them).  The barrier counts arrivals on bar[0] (zeroed before
+// the launch) and gives up after one second, setting *err.
+__device__ __forceinline__ bool ilu_grid_barrier(unsigned int* bar, unsigned int target, int* err)
+{
+    __syncthreads();
+    __shared__ int ok;
+    if (threadIdx.x == 0) {
+        // arrive (release: this CTA's stores first), then poll with acquire
+        // loads; every 256 polls look at the clock and at the error flag
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
+        ok = 1;
+        unsigned long long t0 = 0;
+        for (unsigned it = 0;; it++) {
+            unsigned int v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+            if (v >= target) break;
+            if ((it & 255) == 0) {
+                unsigned long long now;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+                if (it == 0) t0 = now;
+                else if (now - t0 > 1000000000ull || *(volatile int*)err != 0) {
+                    atomicExch(err, 1);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+template <int CMAX>
+__global__ void __launch_bounds__(256, CMAX == 4 ? 3 : (CMAX == 2 ? 4 : 5)) k_ilu_sweep_coop(int N, int M, int K, const double* __restrict__ Lp,
+                                                         const double* __restrict__ A, const double* __restrict__ U,
+                                                         const double* __restrict__ b, double* y, double* xo,
+                                                         unsigned int* bar, int* err)
+{
+    const long long n = (long long)N * M * K;
+    const int NM = N * M;
+    const int planes = N + M + K - 2;
+    const int T = gridDim.x * blockDim.x;                 // T * CMAX >= N * M (host)
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    // the (x, y) columns of this thread, fixed for every plane
+    int cx[CMAX], cy[CMAX];
+#pragma unroll
+    for (int k = 0; k < CMAX; k++) {
+        const int t = tid + k * T;
+        cy[k] = t < NM ? t / N : M;                        // y = M: no column
+        cx[k] = t < NM ? t - cy[k] * N : 0;
+    }
+    // operands of a plane that do not depend on the previous plane, loaded
+    // before the barrier that ends the previous plane
+    double p0[CMAX], p1[CMAX], p2[CMAX], p3[CMAX], p4[CMAX];
+    long long ci[CMAX];
+    bool act[CMAX];
+    auto cell = [&](int level, int k) {
+        const int z = level - cx[k] - cy[k];
+        act[k] = cy[k] < M && z >= 0 && z < K;
+        ci[k] = act[k] ? (long long)z * NM + (long long)cy[k] * N + cx[k] : 0;
+        return z;
+    };
+    auto fwd_operands = [&](int level) {
+#pragma unroll
+        for (int k = 0; k < CMAX; k++) {
+            const int z = cell(level, k);
+            if (act[k]) {
+                const long long i = ci[k];
+                p0[k] = b[i];
+                p1[k] = z > 0 ? Lp[i] : 0.0;
+                p2[k] = cy[k] > 0 ? Lp[n + i] : 0.0;
+                p3[k] = cx[k] > 0 ? Lp[2 * n + i] : 0.0;
+            }
+        }
+    };
+    auto bwd_operands = [&](int level) {
+#pragma unroll
+        for (int k = 0; k < CMAX; k++) {
+            const int z = cell(level, k);
+            if (act[k]) {
+                const long long i = ci[k];
+                p0[k] = __ldcg(y + i);
+                p1[k] = cx[k] < N - 1 ? A[4 * n + i] : 0.0;
+                p2[k] = cy[k] < M - 1 ? A[5 * n + i] : 0.0;
+                p3[k] = z < K - 1 ? A[6 * n + i] : 0.0;
+                p4[k] = U[i];
+            }
+        }
+    };
+    unsigned int target = 0;
+    fwd_operands(0);
+    for (int level = 0; level < planes; level++) {
+#pragma unroll
+        for (int k = 0; k < CMAX; k++) {
+            if (!act[k]) continue;
+            const long long i = ci[k];
+            const int z = level - cx[k] - cy[k];
+            double aux = p0[k];
+            if (z > 0) aux -= p1[k] * __ldcg(y + i - NM);
+            if (cy[k] > 0) aux -= p2[k] * __ldcg(y + i - N);
+            if (cx[k] > 0) aux -= p3[k] * __ldcg(y + i - 1);
+            y[i] = aux;
+        }
+        if (level + 1 < planes) fwd_operands(level + 1);
+        target += gridDim.x;
+        if (!ilu_grid_barrier(bar, target, err)) return;
+    }
+    bwd_operands(planes - 1);
+    for (int level = planes - 1; level >= 0; level--) {
+#pragma unroll
+        for (int k = 0; k < CMAX; k++) {
+            if (!act[k]) continue;
+            const long long i = ci[k];
+            const int z = level - cx[k] - cy[k];
+            double aux = p0[k];
+            if (cx[k] < N - 1) aux -= p1[k] * __ldcg(xo + i + 1);
+            if (cy[k] < M - 1) aux -= p2[k] * __ldcg(xo + i + N);
+            if (z < K - 1) aux -= p3[k] * __ldcg(xo + i + NM);
+            xo[i] = aux / p4[k];
+        }
+        if (level > 0) {
+            bwd_operands(level - 1);
+            target += gridDim.x;
+            if (!ilu_grid_barrier(bar, target, err)) return;
+        }
+    }
+}
+
 }  // namespace lsg

@@ -234,6 +234,12 @@ struct Context {
     cudaGraphExec_t ilu_exec = nullptr;
     long long ilu_nodes = 0;
     DevBuf<double> ilu_in, ilu_out;
+    // the one-launch ILU sweep (k_ilu_sweep_coop): its barrier counter, the
+    // flag its bounded barrier sets when it gives up, and its grid size
+    DevBuf<unsigned int> ilu_bar;
+    DevBuf<int> ilu_err;
+    int ilu_blocks = 0;
+    int ilu_cmax = 0;
     double bytes = 0;
     int vcycles = 0;
     bool own_stream = true;
@@ -286,6 +292,7 @@ namespace lsg {
 
 static void ilu_apply(Context& C, const double* b, double* x);
 static void ilu_graph_release(Context& C);
+static void ilu_check(Context& C);
 
 // ---------------------------------------------------------------------------
 // row dictionary of an operator given as noff coefficient planes
@@ -1505,6 +1512,7 @@ static int fgmres(Context& C, double* x, const double* b, lsg_stats* st)
         if (hs.breakdown) status = LSG_BREAKDOWN;
         else if (!(norm_r <= C.opt.eps)) status = LSG_NOT_CONVERGED;
     }
+    ilu_check(C);
     if (st) {
         st->iterations = it;
         st->norm_r = norm_r;
@@ -1613,6 +1621,70 @@ static void ilu_graph_release(Context& C)
     C.ilu_exec = nullptr;
 }
 
+// Both sweeps of one ILU(0) application as one cooperative launch
+// (k_ilu_sweep_coop: a grid barrier between hyperplanes instead of a kernel
+// boundary, one launch instead of 2 (N + M + K - 2)).  The grid covers the
+// (x, y) columns of a plane, at most a third of the CTAs that fit on the GPU
+// at once, so the three momentum equations' solves still run side by side.
+// false = not available (the caller replays the per-plane graph).
+static bool ilu_coop(Context& C, const double* b, double* x)
+{
+    const Dims& d = C.d;
+    if (C.ilu_blocks == 0) {
+        int dev = 0, sms = 0, coop = 0, per_sm[3] = {0, 0, 0};
+        LSG_CUDA(cudaGetDevice(&dev));
+        LSG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        LSG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        LSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_ilu_sweep_coop<1>, 256, 0));
+        LSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_ilu_sweep_coop<2>, 256, 0));
+        LSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_ilu_sweep_coop<4>, 256, 0));
+        // the fewest columns per thread (1, 2 or 4) for which the grid fits a
+        // third of the CTAs the GPU holds at once
+        const long long cols = (long long)d.N * d.M;
+        C.ilu_cmax = 0;
+        for (int q = 0; q < 3 && !C.ilu_cmax; q++) {
+            const int c = 1 << q;
+            if ((cols + 256LL * c - 1) / (256LL * c) <= (long long)sms * per_sm[q] / 3) C.ilu_cmax = c;
+        }
+        const long long need = C.ilu_cmax ? (cols + 256LL * C.ilu_cmax - 1) / (256LL * C.ilu_cmax) : 0;
+        C.ilu_blocks = (coop && C.ilu_cmax && d.n() < (1LL << 40)) ? (int)std::max(1LL, need) : -1;
+        if (C.ilu_blocks > 0) {
+            C.ilu_bar.alloc(1);
+            C.ilu_err.alloc(1);
+            LSG_CUDA(cudaMemsetAsync(C.ilu_err.p, 0, sizeof(int), C.s));
+        }
+    }
+    if (C.ilu_blocks < 0) return false;
+    LSG_CUDA(cudaMemsetAsync(C.ilu_bar.p, 0, sizeof(unsigned int), C.s));
+    int N = d.N, M = d.M, K = d.K;
+    const double* Lp = C.iluL.p;
+    const double* A = C.A7.p;
+    const double* U = C.iluU.p;
+    double* y = C.t4.p;
+    unsigned int* bar = C.ilu_bar.p;
+    int* err = C.ilu_err.p;
+    void* args[] = {&N, &M, &K, (void*)&Lp, (void*)&A, (void*)&U, (void*)&b, &y, &x, &bar, &err};
+    const void* fn = C.ilu_cmax == 1   ? (const void*)k_ilu_sweep_coop<1>
+                     : C.ilu_cmax == 2 ? (const void*)k_ilu_sweep_coop<2>
+                                       : (const void*)k_ilu_sweep_coop<4>;
+    LSG_CUDA(cudaLaunchCooperativeKernel(fn, dim3(C.ilu_blocks), dim3(256), args, 0, C.s));
+    LSG_CHECK_LAUNCH();
+    return true;
+}
+
+// Raises the failure of a cooperative ILU sweep whose barrier gave up.
+static void ilu_check(Context& C)
+{
+    if (C.opt.precond != LSG_PC_ILU0 || C.ilu_blocks <= 0) return;
+    int e = 0;
+    LSG_CUDA(cudaMemcpyAsync(&e, C.ilu_err.p, sizeof(int), cudaMemcpyDeviceToHost, C.s));
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    if (e) {
+        LSG_CUDA(cudaMemsetAsync(C.ilu_err.p, 0, sizeof(int), C.s));
+        throw Error{LSG_ERR_CUDA, "an ILU sweep's grid barrier gave up waiting"};
+    }
+}
+
 // The 2 (N + M + K - 2) hyperplane launches of one application are replayed
 // as one CUDA graph: b is copied into a fixed input buffer, the graph runs,
 // the result is copied out (two device copies of n values against hundreds
@@ -1625,6 +1697,7 @@ static void ilu_apply(Context& C, const double* b, double* x)
         LSG_CHECK_LAUNCH();
         return;
     }
+    if (ilu_coop(C, b, x)) return;
     const long long n = C.n;
     if (!C.ilu_exec) {
         C.ilu_in.alloc(n);
@@ -1708,6 +1781,7 @@ static int bicgstab(Context& C, double* x, const double* b, lsg_stats* st)
         } while (norm_r > C.opt.eps && it < C.opt.max_it);
         if (status == LSG_OK && !(norm_r <= C.opt.eps)) status = LSG_NOT_CONVERGED;
     }
+    ilu_check(C);
     if (st) {
         st->iterations = it;
         st->norm_r = norm_r;
