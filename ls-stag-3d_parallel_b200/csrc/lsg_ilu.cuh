@@ -134,17 +134,10 @@ __global__ void k_ilu_bwd(int level, int N, int M, int K, const double* __restri
     }
 }
 
-// Both triangular sweeps of one ILU(0) application in one cooperative launch
-// (every CTA resident): the hyperplanes of the forward sweep, then those of
-// the backward sweep, each thread owning the (x, y) columns t, t + T, ...
-// (at most CMAX) for every plane, with the arithmetic of k_ilu_fwd /
-// k_ilu_bwd (so the same bits) and a grid-wide barrier between consecutive
-// planes instead of a kernel boundary.  A plane's operands that do not
-// depend on the previous plane (b or y, the factor entries, the pivot) are
-// loaded before the barrier that ends the previous plane, so after it only
-// the neighbours just written remain to fetch (through L2, __ldcg: other
-// CTAs wrote them).  The barrier counts arrivals on bar[0] (zeroed before
-// the launch) and gives up after one second, setting *err.
+// Grid-wide barrier of the cooperative ILU sweep (every CTA resident):
+// arrivals are counted on bar[0] (zeroed before the launch); it gives up
+// after one second, setting *err.  Values other CTAs wrote before the
+// barrier are read after it through L2 (__ldcg).
 __device__ __forceinline__ bool ilu_grid_barrier(unsigned int* bar, unsigned int target, int* err)
 {
     __syncthreads();
@@ -175,60 +168,103 @@ __device__ __forceinline__ bool ilu_grid_barrier(unsigned int* bar, unsigned int
     return ok != 0;
 }
 
-template <int CMAX>
-__global__ void __launch_bounds__(256, CMAX == 4 ? 3 : (CMAX == 2 ? 4 : 5)) k_ilu_sweep_coop(int N, int M, int K, const double* __restrict__ Lp,
-                                                         const double* __restrict__ A, const double* __restrict__ U,
-                                                         const double* __restrict__ b, double* y, double* xo,
-                                                         unsigned int* bar, int* err)
+// Position of cell (x, y, z) in the hyperplane order: planes l = x + y + z in
+// turn, inside a plane by z, then y (x = l - y - z).  start[l] is the first
+// position of plane l, rowstart[l K + z] the first of its row z.
+__device__ __forceinline__ int ilu_hpos(int x, int y, int z, int N, int K, const int* __restrict__ start,
+                                        const int* __restrict__ rowstart)
+{
+    const int l = x + y + z;
+    const int ymin = max(0, l - z - (N - 1));
+    return start[l] + rowstart[(long long)l * K + z] + (y - ymin);
+}
+
+// The factors and neighbour positions in hyperplane order: perm[p] = i for
+// the cell i at position p; fac = L_b, L_s, L_w, U_e, U_n, U_t, U_p (7 arrays
+// of n); nbr = the positions of the cells below (z-1, y-1, x-1) and above
+// (x+1, y+1, z+1), -1 outside the grid (6 arrays of n).
+__global__ void k_ilu_perm_build(int N, int M, int K, const int* __restrict__ start, const int* __restrict__ rowstart,
+                                 const double* __restrict__ Lp, const double* __restrict__ A,
+                                 const double* __restrict__ U, int* __restrict__ perm, double* __restrict__ fac,
+                                 int* __restrict__ nbr)
 {
     const long long n = (long long)N * M * K;
     const int NM = N * M;
-    const int planes = N + M + K - 2;
-    const int T = gridDim.x * blockDim.x;                 // T * CMAX >= N * M (host)
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    // the (x, y) columns of this thread, fixed for every plane
-    int cx[CMAX], cy[CMAX];
-#pragma unroll
-    for (int k = 0; k < CMAX; k++) {
-        const int t = tid + k * T;
-        cy[k] = t < NM ? t / N : M;                        // y = M: no column
-        cx[k] = t < NM ? t - cy[k] * N : 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        cell_xyz(i, N, NM, x, y, z);
+        const int p = ilu_hpos(x, y, z, N, K, start, rowstart);
+        perm[p] = (int)i;
+        fac[p] = Lp[i];
+        fac[n + p] = Lp[n + i];
+        fac[2 * n + p] = Lp[2 * n + i];
+        fac[3 * n + p] = A[4 * n + i];
+        fac[4 * n + p] = A[5 * n + i];
+        fac[5 * n + p] = A[6 * n + i];
+        fac[6 * n + p] = U[i];
+        nbr[p] = z > 0 ? ilu_hpos(x, y, z - 1, N, K, start, rowstart) : -1;
+        nbr[n + p] = y > 0 ? ilu_hpos(x, y - 1, z, N, K, start, rowstart) : -1;
+        nbr[2 * n + p] = x > 0 ? ilu_hpos(x - 1, y, z, N, K, start, rowstart) : -1;
+        nbr[3 * n + p] = x < N - 1 ? ilu_hpos(x + 1, y, z, N, K, start, rowstart) : -1;
+        nbr[4 * n + p] = y < M - 1 ? ilu_hpos(x, y + 1, z, N, K, start, rowstart) : -1;
+        nbr[5 * n + p] = z < K - 1 ? ilu_hpos(x, y, z + 1, N, K, start, rowstart) : -1;
     }
-    // operands of a plane that do not depend on the previous plane, loaded
-    // before the barrier that ends the previous plane
-    double p0[CMAX], p1[CMAX], p2[CMAX], p3[CMAX], p4[CMAX];
-    long long ci[CMAX];
-    bool act[CMAX];
-    auto cell = [&](int level, int k) {
-        const int z = level - cx[k] - cy[k];
-        act[k] = cy[k] < M && z >= 0 && z < K;
-        ci[k] = act[k] ? (long long)z * NM + (long long)cy[k] * N + cx[k] : 0;
-        return z;
-    };
+}
+
+// Both triangular sweeps of one ILU(0) application in one cooperative launch
+// over the hyperplane-ordered factors (k_ilu_perm_build): the cells of a
+// plane are contiguous, so every stream of a plane is read coalesced, and
+// their neighbours in the previous plane lie close together.  Each thread
+// takes positions t, t + T, ... (at most CMAX) of every plane, with the
+// arithmetic of k_ilu_fwd / k_ilu_bwd (the same bits); b is gathered and x
+// scattered through perm inside the sweeps.  A plane's operands that do not
+// depend on the previous plane are loaded before the barrier that ends it.
+template <int CMAX>
+__global__ void __launch_bounds__(256) k_ilu_sweep_perm(int planes, long long n, const int* __restrict__ start,
+                                                         const int* __restrict__ perm, const double* __restrict__ fac,
+                                                         const int* __restrict__ nbr, const double* __restrict__ b,
+                                                         double* yp, double* xp, double* __restrict__ x,
+                                                         unsigned int* bar, int* err)
+{
+    const int T = gridDim.x * blockDim.x;                 // T * CMAX >= the largest plane (host)
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    int pos[CMAX], n0[CMAX], n1[CMAX], n2[CMAX];
+    double v0[CMAX], v1[CMAX], v2[CMAX], v3[CMAX], v4[CMAX];
     auto fwd_operands = [&](int level) {
+        const int s0 = start[level], cnt = start[level + 1] - s0;
 #pragma unroll
         for (int k = 0; k < CMAX; k++) {
-            const int z = cell(level, k);
-            if (act[k]) {
-                const long long i = ci[k];
-                p0[k] = b[i];
-                p1[k] = z > 0 ? Lp[i] : 0.0;
-                p2[k] = cy[k] > 0 ? Lp[n + i] : 0.0;
-                p3[k] = cx[k] > 0 ? Lp[2 * n + i] : 0.0;
+            const int q = tid + k * T;
+            pos[k] = q < cnt ? s0 + q : -1;
+            if (pos[k] >= 0) {
+                const int p = pos[k];
+                v0[k] = b[perm[p]];
+                v1[k] = fac[p];
+                v2[k] = fac[n + p];
+                v3[k] = fac[2 * n + p];
+                n0[k] = nbr[p];
+                n1[k] = nbr[n + p];
+                n2[k] = nbr[2 * n + p];
             }
         }
     };
     auto bwd_operands = [&](int level) {
+        const int s0 = start[level], cnt = start[level + 1] - s0;
 #pragma unroll
         for (int k = 0; k < CMAX; k++) {
-            const int z = cell(level, k);
-            if (act[k]) {
-                const long long i = ci[k];
-                p0[k] = __ldcg(y + i);
-                p1[k] = cx[k] < N - 1 ? A[4 * n + i] : 0.0;
-                p2[k] = cy[k] < M - 1 ? A[5 * n + i] : 0.0;
-                p3[k] = z < K - 1 ? A[6 * n + i] : 0.0;
-                p4[k] = U[i];
+            const int q = tid + k * T;
+            pos[k] = q < cnt ? s0 + q : -1;
+            if (pos[k] >= 0) {
+                const int p = pos[k];
+                v0[k] = __ldcg(yp + p);
+                v1[k] = fac[3 * n + p];
+                v2[k] = fac[4 * n + p];
+                v3[k] = fac[5 * n + p];
+                v4[k] = fac[6 * n + p];
+                n0[k] = nbr[3 * n + p];
+                n1[k] = nbr[4 * n + p];
+                n2[k] = nbr[5 * n + p];
             }
         }
     };
@@ -237,14 +273,12 @@ __global__ void __launch_bounds__(256, CMAX == 4 ? 3 : (CMAX == 2 ? 4 : 5)) k_il
     for (int level = 0; level < planes; level++) {
 #pragma unroll
         for (int k = 0; k < CMAX; k++) {
-            if (!act[k]) continue;
-            const long long i = ci[k];
-            const int z = level - cx[k] - cy[k];
-            double aux = p0[k];
-            if (z > 0) aux -= p1[k] * __ldcg(y + i - NM);
-            if (cy[k] > 0) aux -= p2[k] * __ldcg(y + i - N);
-            if (cx[k] > 0) aux -= p3[k] * __ldcg(y + i - 1);
-            y[i] = aux;
+            if (pos[k] < 0) continue;
+            double aux = v0[k];
+            if (n0[k] >= 0) aux -= v1[k] * __ldcg(yp + n0[k]);
+            if (n1[k] >= 0) aux -= v2[k] * __ldcg(yp + n1[k]);
+            if (n2[k] >= 0) aux -= v3[k] * __ldcg(yp + n2[k]);
+            yp[pos[k]] = aux;
         }
         if (level + 1 < planes) fwd_operands(level + 1);
         target += gridDim.x;
@@ -254,14 +288,14 @@ __global__ void __launch_bounds__(256, CMAX == 4 ? 3 : (CMAX == 2 ? 4 : 5)) k_il
     for (int level = planes - 1; level >= 0; level--) {
 #pragma unroll
         for (int k = 0; k < CMAX; k++) {
-            if (!act[k]) continue;
-            const long long i = ci[k];
-            const int z = level - cx[k] - cy[k];
-            double aux = p0[k];
-            if (cx[k] < N - 1) aux -= p1[k] * __ldcg(xo + i + 1);
-            if (cy[k] < M - 1) aux -= p2[k] * __ldcg(xo + i + N);
-            if (z < K - 1) aux -= p3[k] * __ldcg(xo + i + NM);
-            xo[i] = aux / p4[k];
+            if (pos[k] < 0) continue;
+            double aux = v0[k];
+            if (n0[k] >= 0) aux -= v1[k] * __ldcg(xp + n0[k]);
+            if (n1[k] >= 0) aux -= v2[k] * __ldcg(xp + n1[k]);
+            if (n2[k] >= 0) aux -= v3[k] * __ldcg(xp + n2[k]);
+            const double v = aux / v4[k];
+            xp[pos[k]] = v;
+            x[perm[pos[k]]] = v;
         }
         if (level > 0) {
             bwd_operands(level - 1);

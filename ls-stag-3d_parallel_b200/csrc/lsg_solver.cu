@@ -234,8 +234,13 @@ struct Context {
     cudaGraphExec_t ilu_exec = nullptr;
     long long ilu_nodes = 0;
     DevBuf<double> ilu_in, ilu_out;
-    // the one-launch ILU sweep (k_ilu_sweep_coop): its barrier counter, the
-    // flag its bounded barrier sets when it gives up, and its grid size
+    // the one-launch ILU sweep (k_ilu_sweep_perm): factors, neighbour
+    // positions and work vectors in hyperplane order, the plane offsets, its
+    // barrier counter, the flag its bounded barrier sets when it gives up,
+    // its grid size and positions per thread
+    DevBuf<int> ilu_start, ilu_rowstart, ilu_perm, ilu_nbr;
+    DevBuf<double> ilu_fac, ilu_yp, ilu_xp;
+    int ilu_planes = 0, ilu_maxplane = 0;
     DevBuf<unsigned int> ilu_bar;
     DevBuf<int> ilu_err;
     int ilu_blocks = 0;
@@ -1598,6 +1603,46 @@ static void ilu_setup(Context& C)
     LSG_CHECK_LAUNCH();
     k_ilu_lower<<<grid_for(n, 256), 256, 0, C.s>>>(d.N, d.M, d.K, C.A7.p, C.iluU.p, C.iluL.p);
     LSG_CHECK_LAUNCH();
+    // the factors in hyperplane order for the one-launch sweep (grids of fewer
+    // than 2^31 cells): plane offsets and row offsets on the host, the rest
+    // on the device
+    C.ilu_blocks = 0;
+    C.ilu_planes = 0;
+    if (n < (1LL << 31) && C.s) {
+        const int P = planes, N = d.N, M = d.M, K = d.K;
+        std::vector<int> start(P + 1, 0), rowstart((size_t)P * K, 0);
+        int maxplane = 0;
+        for (int l = 0; l < P; l++) {
+            long long acc = 0;
+            for (int z = 0; z < K; z++) {
+                rowstart[(size_t)l * K + z] = (int)acc;
+                const int lz = l - z;
+                if (lz < 0) continue;
+                const int ylo = std::max(0, lz - (N - 1)), yhi = std::min(M - 1, lz);
+                if (yhi >= ylo) acc += yhi - ylo + 1;
+            }
+            start[l + 1] = start[l] + (int)acc;
+            maxplane = std::max(maxplane, (int)acc);
+        }
+        LSG_REQUIRE(start[P] == n, LSG_ERR_STATE, "hyperplane count mismatch");
+        C.ilu_planes = P;
+        C.ilu_maxplane = maxplane;
+        C.ilu_start.alloc(P + 1);
+        C.ilu_rowstart.alloc((size_t)P * K);
+        C.ilu_perm.alloc(n);
+        C.ilu_nbr.alloc(6 * (size_t)n);
+        C.ilu_fac.alloc(7 * (size_t)n);
+        C.ilu_yp.alloc(n);
+        C.ilu_xp.alloc(n);
+        LSG_CUDA(cudaMemcpyAsync(C.ilu_start.p, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                 C.s));
+        LSG_CUDA(cudaMemcpyAsync(C.ilu_rowstart.p, rowstart.data(), rowstart.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, C.s));
+        k_ilu_perm_build<<<grid_for(n, 256), 256, 0, C.s>>>(N, M, K, C.ilu_start.p, C.ilu_rowstart.p, C.iluL.p,
+                                                            C.A7.p, C.iluU.p, C.ilu_perm.p, C.ilu_fac.p,
+                                                            C.ilu_nbr.p);
+        LSG_CHECK_LAUNCH();
+    }
     LSG_CUDA(cudaStreamSynchronize(C.s));
     C.have_ilu = true;
 }
@@ -1622,32 +1667,32 @@ static void ilu_graph_release(Context& C)
 }
 
 // Both sweeps of one ILU(0) application as one cooperative launch
-// (k_ilu_sweep_coop: a grid barrier between hyperplanes instead of a kernel
-// boundary, one launch instead of 2 (N + M + K - 2)).  The grid covers the
-// (x, y) columns of a plane, at most a third of the CTAs that fit on the GPU
-// at once, so the three momentum equations' solves still run side by side.
-// false = not available (the caller replays the per-plane graph).
+// (k_ilu_sweep_perm over the hyperplane-ordered factors: a grid barrier
+// between hyperplanes instead of a kernel boundary, one launch instead of
+// 2 (N + M + K - 2)).  The grid covers the largest plane with at most a third
+// of the CTAs that fit on the GPU at once, so the three momentum equations'
+// solves still run side by side.  false = not available (the caller replays
+// the per-plane graph).
 static bool ilu_coop(Context& C, const double* b, double* x)
 {
-    const Dims& d = C.d;
     if (C.ilu_blocks == 0) {
         int dev = 0, sms = 0, coop = 0, per_sm[3] = {0, 0, 0};
         LSG_CUDA(cudaGetDevice(&dev));
         LSG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
         LSG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        LSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_ilu_sweep_coop<1>, 256, 0));
-        LSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_ilu_sweep_coop<2>, 256, 0));
-        LSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_ilu_sweep_coop<4>, 256, 0));
-        // the fewest columns per thread (1, 2 or 4) for which the grid fits a
-        // third of the CTAs the GPU holds at once
-        const long long cols = (long long)d.N * d.M;
+        LSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_ilu_sweep_perm<1>, 256, 0));
+        LSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_ilu_sweep_perm<2>, 256, 0));
+        LSG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_ilu_sweep_perm<4>, 256, 0));
+        // the fewest positions per thread (1, 2 or 4) for which the grid, as
+        // wide as the largest plane, fits a third of the CTAs the GPU holds
+        const long long cols = C.ilu_maxplane;
         C.ilu_cmax = 0;
         for (int q = 0; q < 3 && !C.ilu_cmax; q++) {
             const int c = 1 << q;
             if ((cols + 256LL * c - 1) / (256LL * c) <= (long long)sms * per_sm[q] / 3) C.ilu_cmax = c;
         }
         const long long need = C.ilu_cmax ? (cols + 256LL * C.ilu_cmax - 1) / (256LL * C.ilu_cmax) : 0;
-        C.ilu_blocks = (coop && C.ilu_cmax && d.n() < (1LL << 40)) ? (int)std::max(1LL, need) : -1;
+        C.ilu_blocks = (coop && C.ilu_cmax && C.ilu_planes > 0) ? (int)std::max(1LL, need) : -1;
         if (C.ilu_blocks > 0) {
             C.ilu_bar.alloc(1);
             C.ilu_err.alloc(1);
@@ -1656,17 +1701,21 @@ static bool ilu_coop(Context& C, const double* b, double* x)
     }
     if (C.ilu_blocks < 0) return false;
     LSG_CUDA(cudaMemsetAsync(C.ilu_bar.p, 0, sizeof(unsigned int), C.s));
-    int N = d.N, M = d.M, K = d.K;
-    const double* Lp = C.iluL.p;
-    const double* A = C.A7.p;
-    const double* U = C.iluU.p;
-    double* y = C.t4.p;
+    int planes = C.ilu_planes;
+    long long nn = C.n;
+    const int* start = C.ilu_start.p;
+    const int* perm = C.ilu_perm.p;
+    const double* fac = C.ilu_fac.p;
+    const int* nbr = C.ilu_nbr.p;
+    double* yp = C.ilu_yp.p;
+    double* xp = C.ilu_xp.p;
     unsigned int* bar = C.ilu_bar.p;
     int* err = C.ilu_err.p;
-    void* args[] = {&N, &M, &K, (void*)&Lp, (void*)&A, (void*)&U, (void*)&b, &y, &x, &bar, &err};
-    const void* fn = C.ilu_cmax == 1   ? (const void*)k_ilu_sweep_coop<1>
-                     : C.ilu_cmax == 2 ? (const void*)k_ilu_sweep_coop<2>
-                                       : (const void*)k_ilu_sweep_coop<4>;
+    void* args[] = {&planes, &nn, (void*)&start, (void*)&perm, (void*)&fac, (void*)&nbr, (void*)&b, &yp, &xp, &x,
+                    &bar, &err};
+    const void* fn = C.ilu_cmax == 1   ? (const void*)k_ilu_sweep_perm<1>
+                     : C.ilu_cmax == 2 ? (const void*)k_ilu_sweep_perm<2>
+                                       : (const void*)k_ilu_sweep_perm<4>;
     LSG_CUDA(cudaLaunchCooperativeKernel(fn, dim3(C.ilu_blocks), dim3(256), args, 0, C.s));
     LSG_CHECK_LAUNCH();
     return true;
