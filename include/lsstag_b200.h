@@ -566,6 +566,15 @@ int lsg_mg_level_tridiag(lsg_ctx* ctx, int level, char dir, double* c, double* d
    lsg_setup with the multigrid preconditioner. */
 int lsg_profile_kernel(lsg_ctx* ctx, int which, int reps, double* ms_per_launch, double* bytes_per_launch);
 
+/* Self-test of the bounded waits: runs the one-launch ILU(0) sweep of an
+   ILU(0) context with one CTA leaving before its first barrier arrival, so
+   the other CTAs' first wait runs out (after about one second) and the
+   kernel returns with its error flag set.  Returns LSG_ERR_CUDA with
+   lsg_last_error describing it (the expected result); the context stays
+   usable.  Needs lsg_setup with LSG_PC_ILU0 on a grid whose sweep has two
+   CTAs or more. */
+int lsg_selftest_wait_limit(lsg_ctx* ctx);
+
 /* Residual r = b - A x and its squared 2-norm for a 7-point operator given
    as seven coefficient planes (layout of lsg_set_matrix_stencil7), without
    allocating device memory.  No counterpart in the reference: it is for

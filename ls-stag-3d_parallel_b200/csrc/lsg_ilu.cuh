@@ -225,8 +225,11 @@ __global__ void __launch_bounds__(256) k_ilu_sweep_perm(int planes, long long n,
                                                          const int* __restrict__ perm, const double* __restrict__ fac,
                                                          const int* __restrict__ nbr, const double* __restrict__ b,
                                                          double* yp, double* xp, double* __restrict__ x,
-                                                         unsigned int* bar, int* err)
+                                                         unsigned int* bar, int* err, int withhold)
 {
+    // withhold >= 0 (the wait-limit self-test only): that CTA leaves before its
+    // first barrier arrival, so the others' first wait runs out
+    if ((int)blockIdx.x == withhold) return;
     const int T = gridDim.x * blockDim.x;                 // T * CMAX >= the largest plane (host)
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     int pos[CMAX], n0[CMAX], n1[CMAX], n2[CMAX];

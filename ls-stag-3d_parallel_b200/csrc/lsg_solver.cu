@@ -1673,7 +1673,7 @@ static void ilu_graph_release(Context& C)
 // of the CTAs that fit on the GPU at once, so the three momentum equations'
 // solves still run side by side.  false = not available (the caller replays
 // the per-plane graph).
-static bool ilu_coop(Context& C, const double* b, double* x)
+static bool ilu_coop(Context& C, const double* b, double* x, int withhold = -1)
 {
     if (C.ilu_blocks == 0) {
         int dev = 0, sms = 0, coop = 0, per_sm[3] = {0, 0, 0};
@@ -1712,7 +1712,7 @@ static bool ilu_coop(Context& C, const double* b, double* x)
     unsigned int* bar = C.ilu_bar.p;
     int* err = C.ilu_err.p;
     void* args[] = {&planes, &nn, (void*)&start, (void*)&perm, (void*)&fac, (void*)&nbr, (void*)&b, &yp, &xp, &x,
-                    &bar, &err};
+                    &bar, &err, &withhold};
     const void* fn = C.ilu_cmax == 1   ? (const void*)k_ilu_sweep_perm<1>
                      : C.ilu_cmax == 2 ? (const void*)k_ilu_sweep_perm<2>
                                        : (const void*)k_ilu_sweep_perm<4>;
@@ -3830,6 +3830,23 @@ int lsg_operator_gradient(lsg_ctx* h, const double* lambda, const double* x, dou
     LSG_CHECK_LAUNCH();
     LSG_CUDA(cudaMemcpyAsync(grad, dg.p, 7 * n * 8, cudaMemcpyDeviceToHost, C.s));
     LSG_CUDA(cudaStreamSynchronize(C.s));
+    return LSG_OK;
+    LSG_API_END(h)
+}
+
+int lsg_selftest_wait_limit(lsg_ctx* h)
+{
+    if (!h) return LSG_ERR_ARG;
+    LSG_API_BEGIN
+    Context& C = h->c;
+    LSG_REQUIRE(C.have_setup && C.opt.precond == LSG_PC_ILU0, LSG_ERR_STATE, "needs lsg_setup with ILU(0)");
+    LSG_CUDA(cudaSetDevice(C.device));
+    LSG_CUDA(cudaMemsetAsync(C.t1.p, 0, C.n * sizeof(double), C.s));
+    if (C.ilu_blocks == 0) ilu_coop(C, C.t1.p, C.t2.p);   // sizes the sweep (a normal run)
+    LSG_REQUIRE(C.ilu_blocks >= 2, LSG_ERR_STATE, "the self-test needs a one-launch sweep of two CTAs or more");
+    LSG_CUDA(cudaStreamSynchronize(C.s));
+    ilu_coop(C, C.t1.p, C.t2.p, 0);                // CTA 0 withholds its first arrival
+    ilu_check(C);                                  // throws: the others' wait ran out
     return LSG_OK;
     LSG_API_END(h)
 }

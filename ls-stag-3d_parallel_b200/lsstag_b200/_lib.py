@@ -71,7 +71,7 @@ EXPORTS = [
     "lsg_helmholtz_flux", "lsg_convective_flux", "lsg_convective_flux_device", "lsg_momentum_rhs_device",
     "lsg_convective_adjoint", "lsg_convective_adjoint_device", "lsg_gradient_transpose",
     "lsg_gradient_transpose_device", "lsg_projection_adjoint_device", "lsg_tecplot_sol_write",
-    "lsg_mesh_build", "lsg_mesh_get", "lsg_mesh_osc_sweeps", "lsg_set_matrix_mesh", "lsg_set_tolerance",
+    "lsg_mesh_build", "lsg_mesh_get", "lsg_mesh_osc_sweeps", "lsg_set_matrix_mesh", "lsg_set_tolerance", "lsg_selftest_wait_limit",
     "lsg_setup_times", "lsg_row_classes",
     "lsg_flow_create", "lsg_flow_destroy", "lsg_flow_last_error", "lsg_flow_set_state", "lsg_flow_step",
     "lsg_flow_state",
@@ -175,6 +175,7 @@ def load() -> C.CDLL:
     lib.lsg_mesh_osc_sweeps.argtypes = [P]
     lib.lsg_set_matrix_mesh.argtypes = [P, C.c_longlong, C.c_longlong]
     lib.lsg_set_tolerance.argtypes = [P, C.c_double]
+    lib.lsg_selftest_wait_limit.argtypes = [P]
     lib.lsg_setup_times.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.lsg_row_classes.argtypes = [P, C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     lib.lsg_flow_create.argtypes = [C.POINTER(FlowDesc), C.POINTER(C.c_void_p)]

@@ -1,6 +1,8 @@
 """Failure detection of the solver entry points, every failure made on the
-host (bad inputs, a call out of order, an iteration cap); nothing here
-faults or stalls the GPU, and the context stays usable after each one.
+host (bad inputs, a call out of order, an iteration cap), plus the bounded
+waits of the device code: a wait that runs out (a barrier arrival nobody
+makes) ends its kernel with an error flag the host reports.  Nothing here
+faults or hangs the GPU, and the context stays usable after each one.
 
 The reference reports none of these: a capped solve returns silently after
 MAX_ITER (base_task_description.h:45, fgmres_interface.h:123), NaNs run to
@@ -141,3 +143,37 @@ def test_operator_outside_the_stencil_is_rejected():
     assert e.value.code == L.LSG_ERR_PATTERN
     assert N > 2
     s.close()
+
+
+def test_bounded_wait_runs_out_and_is_reported():
+    """The one-launch ILU(0) sweep waits at a grid barrier between
+    hyperplanes for one second at most.  The self-test entry point runs it
+    with one CTA leaving before its first arrival: the others' wait runs
+    out, the kernel ends with its flag set, the call returns LSG_ERR_CUDA
+    with the reason, and the same context then solves normally."""
+    import time
+
+    from lsstag_b200 import _lib as L
+    from lsstag_b200 import cases
+    from lsstag_b200 import solver as S
+    P, dims, pins, b = cases.load(128)
+    s = S.ILUFGMRES()
+    s.set_planes(P, dims, S.Task(eps=1e-8 * float(np.linalg.norm(b))))
+    t0 = time.perf_counter()
+    rc = s.ctx.lib.lsg_selftest_wait_limit(s.ctx.h)
+    dt = time.perf_counter() - t0
+    msg = s.ctx.lib.lsg_last_error(s.ctx.h).decode()
+    print(f"wait-limit self-test: rc {rc} after {dt:.2f} s: {msg}")
+    assert rc == L.LSG_ERR_CUDA and "barrier" in msg
+    assert 0.5 < dt < 60
+    # the context then solves as a fresh one does, to the bit
+    x = np.zeros(b.size)
+    its = s.solve(b, x)
+    s.close()
+    f = S.ILUFGMRES()
+    f.set_planes(P, dims, S.Task(eps=1e-8 * float(np.linalg.norm(b))))
+    xf = np.zeros(b.size)
+    itf = f.solve(b, xf)
+    f.close()
+    assert its == itf and np.array_equal(x, xf) and np.all(np.isfinite(x))
+
